@@ -1,0 +1,145 @@
+/*
+ * Test infrastructure: a thin harness around the reference's OWN compiled
+ * solver (oracle/_ref/libsfr3d_ref.so).  Only tests/, the smoke check and
+ * bench.py's CPU-baseline leg load it, and only as the checker or the timed
+ * CPU arm -- never as the product path.
+ *
+ * It calls the reference's solverC (Solv.c:64-501) exactly as the SIMPLE and
+ * diffusion drivers do (Simple.c:2983, Diffusion.c:145), with a Memoria arena
+ * (Memoria.c:21 initMem) for its workspace and, for the OpenMP path, the
+ * BufferOmp that pMatrixSolverOmp builds (HccaOpenMp.c:24-40 ->
+ * partitionCsrByNonzeros, Csr.c:1827).  The iteration count, xKx and ||x||
+ * are read back from the one log line the solver writes (Cg.c:201-208,
+ * Bicgstab.c:235-242).  exit() is wrapped at link time so that the
+ * reference's fatal non-convergence path (Cg.c:195-200, Bicgstab.c:225-231)
+ * returns here with its exit code.
+ */
+#define _GNU_SOURCE
+#include <setjmp.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#include <Solv.h>
+
+extern Omp ompVar;
+extern Mpi mpiVar;
+extern FILE *fileLogExc, *fileLogDebug;
+extern iptx nmax; /* arena capacity that alloc() checks (Memoria.c:97-160) */
+void partitionCsrByNonzeros(INT *ia, INT *ja, INT const neq, int nThreads,
+                            INT *thBegin, INT *thEnd, INT *thSize,
+                            INT *thHeight, short type);
+
+void __real_exit(int code);
+
+static jmp_buf g_jump;
+static volatile int g_armed = 0;
+static volatile int g_exit_code = 0;
+
+void __wrap_exit(int code)
+{
+  if (g_armed) {
+    g_armed = 0;
+    g_exit_code = code;
+    longjmp(g_jump, 1);
+  }
+  __real_exit(code);
+}
+
+static void parse_log(const char *buf, int *iters, double *xKx, double *normx)
+{
+  const char *s;
+  if ((s = strstr(buf, "iteration ")) != NULL) sscanf(s + 10, "%d", iters);
+  if ((s = strstr(buf, "xKx ")) != NULL) sscanf(s + 4, "%le", xKx);
+  if ((s = strstr(buf, "norma(x*x) ")) != NULL) sscanf(s + 11, "%le", normx);
+  else if ((s = strstr(buf, "||x*x|| ")) != NULL) sscanf(s + 8, "%le", normx);
+}
+
+/*
+ * Solve one system with the reference's solverC.
+ *   solver : PCG=1 | PBICGSTAB=2 (Define.h:392-393)
+ *   storage: CSRD=2 | CSRC=3 | ELLPACK=4 (Define.h:407-410)
+ *   nthreads: 0 -> serial pcg/pbicgstab, >=1 -> pcgOmp/pbicgstabOmp
+ * Returns 0 when the solver converged, otherwise the code it passed to
+ * exit().  x is updated in place (newX != 0 zeroes it first).
+ */
+int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
+                  double *au, double *b, double *x, double tol,
+                  unsigned maxit, int storage, int solver, int newX,
+                  int unsym, int nthreads, int *iters, double *xKx,
+                  double *normx, double *seconds)
+{
+  Memoria mem;
+  BufferOmp omp;
+  char *logbuf = NULL;
+  size_t loglen = 0;
+  FILE *flog;
+  double t0;
+  int rc = 0, nvec;
+
+  memset(&omp, 0, sizeof(omp));
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  mpiVar.nPrcs = 1;
+  mpiVar.myId = 0;
+  ompVar.fSolver = nthreads > 0;
+  ompVar.nThreadsSolver = (unsigned short)(nthreads > 0 ? nthreads : 1);
+
+  /* workspace: pc + 6 Krylov vectors at most, plus the arena's alignment */
+  nvec = 8;
+  nmax = (iptx)nvec * (iptx)(neq + 64) * (iptx)sizeof(double) + 65536;
+  initMem(&mem, nmax, false);
+  /* dalloc (Memoria.c:280) refuses to release the only vector of an arena;
+   * in the application the mesh always sits below the solver workspace */
+  {
+    DOUBLE *base = NULL;
+    HccaAlloc(DOUBLE, &mem, base, 8, "harness_base", false);
+    (void)base;
+  }
+
+  flog = open_memstream(&logbuf, &loglen);
+  *iters = -1;
+  *xKx = 0.0;
+  *normx = 0.0;
+  *seconds = 0.0;
+
+  if (setjmp(g_jump) == 0) {
+    g_armed = 1;
+    if (nthreads > 0) {
+      omp_set_num_threads(nthreads);
+      omp.thBegin = calloc(nthreads, sizeof(INT));
+      omp.thEnd = calloc(nthreads, sizeof(INT));
+      omp.thSize = calloc(nthreads, sizeof(INT));
+      omp.thHeight = calloc(nthreads, sizeof(INT));
+      omp.thY = calloc((size_t)nthreads * (size_t)neq, sizeof(double));
+      partitionCsrByNonzeros(ia, ja, neq, nthreads, omp.thBegin, omp.thEnd,
+                             omp.thSize, omp.thHeight, (short)storage);
+    }
+    t0 = omp_get_wtime();
+    solverC(&mem, neq, neq, nad, 0, ia, ja, al, ad, au, b, x, NULL,
+            nthreads > 0 ? &omp : NULL, tol, maxit, (short)storage,
+            (short)solver, flog, true, newX != 0, unsym != 0, "oracle");
+    *seconds = omp_get_wtime() - t0;
+    g_armed = 0;
+    rc = 0;
+  } else {
+    rc = g_exit_code == 0 ? -1000 : g_exit_code;
+    *iters = (int)maxit;
+  }
+  fclose(flog);
+  if (rc == 0 && logbuf) parse_log(logbuf, iters, xKx, normx);
+  free(logbuf);
+  free(omp.thBegin);
+  free(omp.thEnd);
+  free(omp.thSize);
+  free(omp.thHeight);
+  free(omp.thY);
+  finalizeMem(&mem, false);
+  return rc;
+}
+
+/* Machine epsilon as the reference computes it for tol = 0 (Solv.c:614). */
+double sfr_ref_smachn(void) { return smachn(); }
+
+int sfr_ref_max_threads(void) { return omp_get_max_threads(); }

@@ -1,0 +1,44 @@
+/*
+ * Test infrastructure, not product code: a plain-C restatement of SFR3D's
+ * linear-solve path used as the parity oracle.  Only tests/, the smoke check
+ * and bench.py's CPU-baseline leg load it.  Every function cites the
+ * reference lines it restates; the arithmetic is done in the same order as
+ * the reference so that results are bit-identical to the reference's own
+ * compiled solver (checked by tests/test_oracle.py against oracle/_ref).
+ */
+#ifndef SFR3D_ORACLE_H
+#define SFR3D_ORACLE_H
+
+/* storage codes, Define.h:407-410 */
+#define ORC_CSRD 2
+#define ORC_CSRC 3
+#define ORC_ELLPACK 4
+
+typedef struct {
+  int iters;        /* j+1 as the reference reports it */
+  int status;       /* 0 converged, 1 reached maxIt (the reference exits) */
+  double xKx;       /* x^T A x */
+  double norm_x;    /* ||x||_2 */
+  double norm_r;    /* ||b - A x||_2 */
+  double norm_r_m;  /* ||b - A x||_M (PCG only) */
+  double conv;      /* tol * norm of b used by the stopping test */
+} orc_stats;
+
+/* y = A x for the storage/unsym pair solverC would see (setMatVec,
+ * Solv.c:732-919).  For ELLPACK, ia[0] is the row width (EllPack.c:35). */
+void orc_matvec(int storage, int unsym, int neq, const int *ia, const int *ja,
+                const double *al, const double *ad, const double *x,
+                double *y);
+
+double orc_dot(const double *a, const double *b, int n);
+
+int orc_pcg(int storage, int unsym, int neq, const int *ia, const int *ja,
+            const double *al, const double *ad, const double *b, double *x,
+            double tol, unsigned maxit, int newx, orc_stats *st);
+
+int orc_pbicgstab(int storage, int unsym, int neq, const int *ia,
+                  const int *ja, const double *al, const double *ad,
+                  const double *b, double *x, double tol, unsigned maxit,
+                  int newx, orc_stats *st);
+
+#endif
