@@ -1,0 +1,172 @@
+/*
+ * sfr3d_b200.h -- C ABI of the B200 (sm_100a) linear-solve path.
+ *
+ * Drop-in for SFR3D's solver entry points (include/Solv.h of the reference):
+ * the Jacobi-preconditioned CG (Cg.c) and Jacobi right-preconditioned
+ * BiCGSTAB (Bicgstab.c) over the CSRD, CSRC and ELLPACK layouts that
+ * dataStruct (Datastruct.c:28) builds.  Plain pointers and sizes only; every
+ * entry returns an int status (SFR_OK = 0) instead of calling exit() as the
+ * reference does, except sfr_solverC which keeps the reference's behaviour.
+ *
+ * Arrays named ia/ja/al/ad/au/b/x follow the reference's meaning:
+ *   CSRD  (storage 2): ia[neq+1], ja[nad] ascending per row, al[nad]
+ *                      off-diagonals, ad[neq] diagonal.  unsym = 0 stores the
+ *                      strict lower part only (Datastruct.c:117-335).
+ *   CSRC  (storage 3): strict lower pattern; al[nad] lower values and, when
+ *                      unsym, au[nad] = A(ja[k], i) (Csr.c:736-1022).  As in
+ *                      solverC, au may be NULL with the upper values stored at
+ *                      al + nad (HccaBlas.c:4233-4236).
+ *   ELLPACK (storage 4): ia = {width, neq*width}; ja, al row-major
+ *                      neq x width; padded slots have ja = i, al = 0
+ *                      (EllPack.c:26-149).
+ * Indices are 0-based int32 (INT, Define.h:429); values are double.
+ */
+#ifndef SFR3D_B200_H
+#define SFR3D_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* solver codes, Define.h:392-393 */
+#define SFR_PCG 1
+#define SFR_PBICGSTAB 2
+/* storage codes, Define.h:407-410 */
+#define SFR_CSRD 2
+#define SFR_CSRC 3
+#define SFR_ELLPACK 4
+
+/* status codes */
+#define SFR_OK 0
+#define SFR_MAXIT 1          /* maxIt reached without convergence */
+#define SFR_BREAKDOWN 2      /* zero or non-finite Krylov scalar */
+#define SFR_BAD_INPUT -1     /* rejected before any device work */
+#define SFR_CUDA_ERROR -2    /* a CUDA call failed */
+#define SFR_TIMEOUT -3       /* a bounded grid-wide wait gave up */
+#define SFR_UNSUPPORTED -4   /* solver/storage pair not handled here */
+
+/* precision modes */
+#define SFR_FP64 0           /* plain FP64: the reference's arithmetic */
+#define SFR_MIXED 1          /* FP32 matrix + inner Krylov, FP64 refinement */
+
+typedef struct sfr_system sfr_system; /* one pattern resident on a device */
+
+/* Per-solve report; the first fields are what the reference's log line and
+ * post-processing report (Cg.c:155-208, Bicgstab.c:188-242). */
+typedef struct {
+  int32_t iters;        /* j+1 as the reference counts (sum of inner its) */
+  int32_t status;       /* SFR_* */
+  double xKx;           /* x^T A x */
+  double norm_x;        /* ||x||_2 */
+  double norm_r;        /* ||b - A x||_2 (true residual, FP64) */
+  double norm_r_m;      /* ||b - A x||_M (PCG) */
+  double conv;          /* stopping threshold tol*||b|| (M-norm for PCG) */
+  double seconds;       /* device time of the solve (CUDA events) */
+  int32_t refinements;  /* MIXED: outer FP64 refinement steps */
+  int32_t inner_iters;  /* MIXED: inner FP32 iterations, all cycles */
+  double relres;        /* ||b - A x||_2 / ||b||_2 at exit */
+} sfr_solve_info;
+
+/* ---- handle API ------------------------------------------------------ */
+
+/* Upload a pattern (replaces dataStruct's product for the device; the
+ * pattern is fixed for the life of the handle).  For ELLPACK, ia is the
+ * two-entry header.  Replaces: the pattern half of solverC's inputs,
+ * Solv.h:59-70. */
+int sfr_gpu_create(int32_t neq, int32_t nad, const int32_t *ia,
+                   const int32_t *ja, int32_t storage, int32_t unsym,
+                   int32_t device, sfr_system **out);
+
+/* Upload values (al/ad/au as solverC receives them, Solv.h:59-70); rewritten
+ * every outer iteration in the application. */
+int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad,
+                       const double *au);
+
+/* Replace only the diagonal (the u/v/w momentum solves share al/au and
+ * differ in ad, Simple.c:2736-2750). */
+int sfr_gpu_set_diagonal(sfr_system *s, const double *ad);
+
+/* Solve A x = b with host b and x (copies inside).  Same semantics as
+ * callCg (Solv.c:936) / callBicgStab (Solv.c:1052): newX zeroes x, tol is
+ * the reference's relative tolerance.  info may be NULL. */
+int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x,
+                  double tol, uint32_t maxit, int32_t newx, int32_t precision,
+                  sfr_solve_info *info);
+
+/* Same with device-resident b and x (no host copies) on `stream`
+ * (cudaStream_t, NULL = legacy default). */
+int sfr_gpu_solve_device(sfr_system *s, int32_t solver, const double *d_b,
+                         double *d_x, double tol, uint32_t maxit,
+                         int32_t newx, int32_t precision, void *stream,
+                         sfr_solve_info *info);
+
+/* k right-hand sides sharing the matrix (the momentum u,v,w batch,
+ * Simple.c:2983-3040): b and x are k*neq, RHS r at offset r*neq; ad_k is
+ * NULL (shared diagonal) or k*neq per-RHS diagonals.  Solved in one
+ * persistent launch.  info has k entries. */
+int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
+                        const double *ad_k, const double *b, double *x,
+                        double tol, uint32_t maxit, int32_t newx,
+                        int32_t precision, sfr_solve_info *info);
+
+int sfr_gpu_destroy(sfr_system *s);
+
+/* ---- kernels for measurement and tests (device pointers) ------------- */
+
+/* y = A x on the device (the matVec* family, HccaBlas.c:2620-4755). */
+int sfr_gpu_spmv(sfr_system *s, const double *d_x, double *d_y,
+                 void *stream);
+/* y = A^T x on the device (the transpose the adjoint solve uses; the
+ * reference has no transpose product). */
+int sfr_gpu_spmv_transpose(sfr_system *s, const double *d_x, double *d_y,
+                           void *stream);
+/* y = A x and returns (y, x) through *dot_out (host), the fused SpMV+dot
+ * of the CG step (Cg.c:103-108). */
+int sfr_gpu_spmv_dot(sfr_system *s, const double *d_x, double *d_y,
+                     double *dot_out, void *stream);
+/* (a, b) with the device's deterministic reduction (dot, HccaBlas.c:393). */
+int sfr_gpu_dot(const double *d_a, const double *d_b, int32_t n,
+                double *dot_out, void *stream);
+
+/* Device memory the handle holds (bytes) and its SELL slot count. */
+int sfr_gpu_stats(const sfr_system *s, int64_t *bytes, int64_t *slots,
+                  int32_t *bandwidth);
+
+const char *sfr_status_string(int status);
+/* Text of the last failure on the calling thread (validation or CUDA). */
+const char *sfr_last_error(void);
+/* Compute capability of the GPU this library was built for and of `device`;
+ * returns SFR_OK when the device can run it. */
+int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor);
+
+/* ---- drop-in for the reference entry point --------------------------- */
+
+/* Same arguments and meaning as solverC (Solv.h:59-70, Solv.c:64-501).
+ * Memoria*, Interface* and BufferOmp* are accepted as opaque pointers and
+ * unused.  PCG and PBICGSTAB over CSRD/CSRC/ELLPACK run on the GPU; the
+ * pattern is cached per (ia, ja, storage) so a repeated call uploads only
+ * al/ad/au/b.  Writes the reference's log line to fSolvLog when fLog is
+ * set.  On non-convergence prints the reference's message and calls
+ * exit(EXIT_FAILURE) for PCG and exit(-2) for BiCGSTAB (Cg.c:195-200,
+ * Bicgstab.c:225-231) unless sfr_set_exit_on_failure(0) was called, in which
+ * case it returns the status. */
+int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
+                int32_t nAdR, int32_t *ia, int32_t *ja, double *al,
+                double *ad, double *au, double *b, double *x, void *iNeq,
+                void *bOmp, double tol, uint32_t maxIt, int16_t storage,
+                int16_t solver, FILE *fSolvLog, bool fLog, bool newX,
+                bool unSym, const char *name);
+void sfr_set_exit_on_failure(int32_t flag);
+/* Precision used by sfr_solverC (SFR_FP64 default). */
+void sfr_set_precision(int32_t precision);
+/* Release every pattern sfr_solverC cached. */
+void sfr_solverC_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

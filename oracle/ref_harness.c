@@ -36,6 +36,7 @@ void __real_exit(int code);
 static jmp_buf g_jump;
 static volatile int g_armed = 0;
 static volatile int g_exit_code = 0;
+static volatile double g_t0 = 0.0;
 
 void __wrap_exit(int code)
 {
@@ -104,6 +105,7 @@ int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
   *normx = 0.0;
   *seconds = 0.0;
 
+  g_t0 = 0.0;
   if (setjmp(g_jump) == 0) {
     g_armed = 1;
     if (nthreads > 0) {
@@ -117,6 +119,7 @@ int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
                              omp.thSize, omp.thHeight, (short)storage);
     }
     t0 = omp_get_wtime();
+    g_t0 = t0;
     solverC(&mem, neq, neq, nad, 0, ia, ja, al, ad, au, b, x, NULL,
             nthreads > 0 ? &omp : NULL, tol, maxit, (short)storage,
             (short)solver, flog, true, newX != 0, unsym != 0, "oracle");
@@ -126,6 +129,8 @@ int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
   } else {
     rc = g_exit_code == 0 ? -1000 : g_exit_code;
     *iters = (int)maxit;
+    /* the solve ran to maxIt before exiting: its wall time is still valid */
+    if (g_t0 > 0.0) *seconds = omp_get_wtime() - g_t0;
   }
   fclose(flog);
   if (rc == 0 && logbuf) parse_log(logbuf, iters, xKx, normx);

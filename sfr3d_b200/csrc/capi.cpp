@@ -1,0 +1,414 @@
+// extern "C" entry points of libsfr3d_b200.so (declared in
+// include/sfr3d_b200.h) and the solverC drop-in.
+#include <cuda_runtime.h>
+
+#include <cinttypes>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "internal.h"
+
+using sfr::HostSell;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int cuda_fail(cudaError_t e) {
+  g_last_error = cudaGetErrorString(e);
+  return SFR_CUDA_ERROR;
+}
+
+#define SFR_CU(expr)                           \
+  do {                                         \
+    cudaError_t e_ = (expr);                   \
+    if (e_ != cudaSuccess) return cuda_fail(e_); \
+  } while (0)
+
+struct IoBuffers {
+  double *b = nullptr, *x = nullptr, *diag = nullptr;
+  size_t cap = 0;  // doubles per buffer
+};
+std::map<const sfr_system *, IoBuffers> g_io;
+std::mutex g_io_mu;
+
+int io_for(sfr_system *s, size_t doubles, IoBuffers **out) {
+  std::lock_guard<std::mutex> lk(g_io_mu);
+  IoBuffers &io = g_io[s];
+  if (io.cap < doubles) {
+    cudaFree(io.b);
+    cudaFree(io.x);
+    cudaFree(io.diag);
+    io = IoBuffers{};
+    SFR_CU(cudaMalloc(&io.b, sizeof(double) * doubles));
+    SFR_CU(cudaMalloc(&io.x, sizeof(double) * doubles));
+    SFR_CU(cudaMalloc(&io.diag, sizeof(double) * doubles));
+    io.cap = doubles;
+  }
+  *out = &io;
+  return SFR_OK;
+}
+
+void io_release(const sfr_system *s) {
+  std::lock_guard<std::mutex> lk(g_io_mu);
+  auto it = g_io.find(s);
+  if (it == g_io.end()) return;
+  cudaFree(it->second.b);
+  cudaFree(it->second.x);
+  cudaFree(it->second.diag);
+  g_io.erase(it);
+}
+
+int ensure_transpose(sfr_system *s) {
+  if (s->at_ready) return SFR_OK;
+  if (!s->have_at_host) return SFR_UNSUPPORTED;
+  int rc = sfr::upload_sell(s->host_at, &s->At, &s->bytes);
+  if (rc != SFR_OK) return rc;
+  s->host_at = HostSell{};
+  s->have_at_host = false;
+  s->at_ready = true;
+  if (s->values_set) return sfr::gather_values(s, &s->At, s->stream);
+  return SFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *sfr_status_string(int status) {
+  switch (status) {
+    case SFR_OK: return "converged";
+    case SFR_MAXIT: return "maximum iterations reached";
+    case SFR_BREAKDOWN: return "Krylov breakdown (zero or non-finite scalar)";
+    case SFR_BAD_INPUT: return "bad input";
+    case SFR_CUDA_ERROR: return "CUDA error";
+    case SFR_TIMEOUT: return "grid barrier timed out";
+    case SFR_UNSUPPORTED: return "unsupported solver/storage/precision";
+    default: return "unknown status";
+  }
+}
+
+const char *sfr_last_error(void) { return g_last_error.c_str(); }
+
+int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    g_last_error = "no CUDA device";
+    return SFR_CUDA_ERROR;
+  }
+  if (device < 0 || device >= n) return SFR_BAD_INPUT;
+  int ma = 0, mi = 0;
+  SFR_CU(cudaDeviceGetAttribute(&ma, cudaDevAttrComputeCapabilityMajor, device));
+  SFR_CU(cudaDeviceGetAttribute(&mi, cudaDevAttrComputeCapabilityMinor, device));
+  if (major) *major = ma;
+  if (minor) *minor = mi;
+  return (ma == 10 && mi == 0) ? SFR_OK : SFR_UNSUPPORTED;
+}
+
+int sfr_gpu_create(int32_t neq, int32_t nad, const int32_t *ia, const int32_t *ja,
+                   int32_t storage, int32_t unsym, int32_t device, sfr_system **out) {
+  if (!out) return SFR_BAD_INPUT;
+  *out = nullptr;
+  auto s = std::make_unique<sfr_system>();
+  HostSell a;
+  std::string why;
+  int32_t nsrc = 0;
+  int rc = sfr::build_sell(neq, nad, ia, ja, storage, unsym, &a, &s->host_at, &nsrc, &why);
+  if (rc != SFR_OK) {
+    g_last_error = why;
+    return rc;
+  }
+  s->have_at_host = true;
+  s->device = device;
+  s->n = neq;
+  s->storage = storage;
+  s->unsym = unsym;
+  s->nad = nad;
+  s->nsrc = nsrc;
+  s->bandwidth = a.bandwidth;
+  SFR_CU(cudaSetDevice(device));
+  SFR_CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  rc = sfr::upload_sell(a, &s->A, &s->bytes);
+  if (rc != SFR_OK) return rc;
+  SFR_CU(cudaMalloc(&s->d_stage, sizeof(double) * std::max(nsrc, 1)));
+  SFR_CU(cudaMalloc(&s->d_diag, sizeof(double) * neq));
+  SFR_CU(cudaMalloc(&s->d_diag32, sizeof(float) * neq));
+  s->bytes += static_cast<int64_t>(sizeof(double) * std::max(nsrc, 1) + 12 * static_cast<size_t>(neq));
+  *out = s.release();
+  return SFR_OK;
+}
+
+int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const double *au) {
+  if (!s || !ad || (!al && s->nsrc > 0)) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  const bool split = s->storage == SFR_CSRC && s->unsym;
+  if (split && au) {
+    const size_t half = static_cast<size_t>(s->nsrc) / 2;
+    SFR_CU(cudaMemcpyAsync(s->d_stage, al, sizeof(double) * half, cudaMemcpyHostToDevice, s->stream));
+    SFR_CU(cudaMemcpyAsync(s->d_stage + half, au, sizeof(double) * half, cudaMemcpyHostToDevice,
+                           s->stream));
+  } else if (s->nsrc > 0) {
+    SFR_CU(cudaMemcpyAsync(s->d_stage, al, sizeof(double) * s->nsrc, cudaMemcpyHostToDevice,
+                           s->stream));
+  }
+  SFR_CU(cudaMemcpyAsync(s->d_diag, ad, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
+  int rc = sfr::gather_values(s, &s->A, s->stream);
+  if (rc != SFR_OK) return rc;
+  if (s->at_ready) {
+    rc = sfr::gather_values(s, &s->At, s->stream);
+    if (rc != SFR_OK) return rc;
+  }
+  SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
+  SFR_CU(cudaStreamSynchronize(s->stream));
+  s->values_set = true;
+  return SFR_OK;
+}
+
+int sfr_gpu_set_diagonal(sfr_system *s, const double *ad) {
+  if (!s || !ad) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  SFR_CU(cudaMemcpyAsync(s->d_diag, ad, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
+  SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
+  SFR_CU(cudaStreamSynchronize(s->stream));
+  return SFR_OK;
+}
+
+int sfr_gpu_solve_device(sfr_system *s, int32_t solver, const double *d_b, double *d_x,
+                         double tol, uint32_t maxit, int32_t newx, int32_t precision,
+                         void *stream, sfr_solve_info *info) {
+  if (!s || !d_b || !d_x) return SFR_BAD_INPUT;
+  if (!s->values_set) {
+    g_last_error = "sfr_gpu_set_values was not called";
+    return SFR_BAD_INPUT;
+  }
+  SFR_CU(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  return sfr::solve_device(s, solver, 1, nullptr, d_b, d_x, tol, maxit, newx, precision, st, info);
+}
+
+int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k, const double *ad_k,
+                        const double *b, double *x, double tol, uint32_t maxit, int32_t newx,
+                        int32_t precision, sfr_solve_info *info) {
+  if (!s || !b || !x || k < 1) return SFR_BAD_INPUT;
+  if (!s->values_set) {
+    g_last_error = "sfr_gpu_set_values was not called";
+    return SFR_BAD_INPUT;
+  }
+  SFR_CU(cudaSetDevice(s->device));
+  IoBuffers *io = nullptr;
+  const size_t total = static_cast<size_t>(s->n) * k;
+  int rc = io_for(s, total, &io);
+  if (rc != SFR_OK) return rc;
+  SFR_CU(cudaMemcpyAsync(io->b, b, sizeof(double) * total, cudaMemcpyHostToDevice, s->stream));
+  if (!newx)
+    SFR_CU(cudaMemcpyAsync(io->x, x, sizeof(double) * total, cudaMemcpyHostToDevice, s->stream));
+  if (ad_k)
+    SFR_CU(cudaMemcpyAsync(io->diag, ad_k, sizeof(double) * total, cudaMemcpyHostToDevice,
+                           s->stream));
+  rc = sfr::solve_device(s, solver, k, ad_k ? io->diag : nullptr, io->b, io->x, tol, maxit, newx,
+                         precision, s->stream, info);
+  if (rc == SFR_CUDA_ERROR || rc == SFR_BAD_INPUT || rc == SFR_UNSUPPORTED || rc == SFR_TIMEOUT)
+    return rc;
+  SFR_CU(cudaMemcpyAsync(x, io->x, sizeof(double) * total, cudaMemcpyDeviceToHost, s->stream));
+  SFR_CU(cudaStreamSynchronize(s->stream));
+  return rc;
+}
+
+int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x, double tol,
+                  uint32_t maxit, int32_t newx, int32_t precision, sfr_solve_info *info) {
+  return sfr_gpu_solve_multi(s, solver, 1, nullptr, b, x, tol, maxit, newx, precision, info);
+}
+
+int sfr_gpu_destroy(sfr_system *s) {
+  if (!s) return SFR_OK;
+  cudaSetDevice(s->device);
+  io_release(s);
+  sfr::free_sell(&s->A);
+  sfr::free_sell(&s->At);
+  cudaFree(s->d_stage);
+  cudaFree(s->d_diag);
+  cudaFree(s->d_diag32);
+  cudaFree(s->ws.base);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return SFR_OK;
+}
+
+int sfr_gpu_spmv(sfr_system *s, const double *d_x, double *d_y, void *stream) {
+  if (!s || !d_x || !d_y) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  return sfr::spmv_device(s, s->A, s->d_diag, d_x, d_y, nullptr, st);
+}
+
+int sfr_gpu_spmv_transpose(sfr_system *s, const double *d_x, double *d_y, void *stream) {
+  if (!s || !d_x || !d_y) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  int rc = ensure_transpose(s);
+  if (rc != SFR_OK) return rc;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  return sfr::spmv_device(s, s->At, s->d_diag, d_x, d_y, nullptr, st);
+}
+
+int sfr_gpu_spmv_dot(sfr_system *s, const double *d_x, double *d_y, double *dot_out,
+                     void *stream) {
+  if (!s || !d_x || !d_y) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  IoBuffers *io = nullptr;
+  int rc = io_for(s, 1, &io);
+  if (rc != SFR_OK) return rc;
+  rc = sfr::spmv_device(s, s->A, s->d_diag, d_x, d_y, io->diag, st);
+  if (rc != SFR_OK) return rc;
+  if (dot_out) {
+    SFR_CU(cudaMemcpyAsync(dot_out, io->diag, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SFR_CU(cudaStreamSynchronize(st));
+  }
+  return SFR_OK;
+}
+
+int sfr_gpu_dot(const double *d_a, const double *d_b, int32_t n, double *dot_out,
+                void *stream) {
+  if (!d_a || !d_b || n < 0 || !dot_out) return SFR_BAD_INPUT;
+  return sfr::dot_host(d_a, d_b, n, dot_out, static_cast<cudaStream_t>(stream));
+}
+
+int sfr_gpu_stats(const sfr_system *s, int64_t *bytes, int64_t *slots, int32_t *bandwidth) {
+  if (!s) return SFR_BAD_INPUT;
+  if (bytes) *bytes = s->bytes;
+  if (slots) *slots = s->A.nslots;
+  if (bandwidth) *bandwidth = s->bandwidth;
+  return SFR_OK;
+}
+
+// ------------------------------------------------------------ solverC ----
+
+namespace {
+
+std::mutex g_shim_mu;
+bool g_exit_on_failure = true;
+int g_precision = SFR_FP64;
+
+struct PatternKey {
+  const int32_t *ia, *ja;
+  int32_t neq, storage, unsym;
+  bool operator<(const PatternKey &o) const {
+    return std::tie(ia, ja, neq, storage, unsym) < std::tie(o.ia, o.ja, o.neq, o.storage, o.unsym);
+  }
+};
+struct Cached {
+  sfr_system *sys = nullptr;
+  uint64_t hash = 0;
+};
+std::map<PatternKey, Cached> g_cache;
+
+uint64_t pattern_hash(const int32_t *ia, const int32_t *ja, int32_t n_ia, int64_t n_ja) {
+  uint64_t h = 1469598103934665603ULL;  // FNV-1a
+  auto mix = [&](const int32_t *p, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+      h ^= static_cast<uint32_t>(p[i]);
+      h *= 1099511628211ULL;
+    }
+  };
+  mix(ia, n_ia);
+  if (ja) mix(ja, n_ja);
+  return h;
+}
+
+}  // namespace
+
+void sfr_set_exit_on_failure(int32_t flag) { g_exit_on_failure = flag != 0; }
+void sfr_set_precision(int32_t precision) { g_precision = precision; }
+
+void sfr_solverC_release(void) {
+  std::lock_guard<std::mutex> lk(g_shim_mu);
+  for (auto &kv : g_cache) sfr_gpu_destroy(kv.second.sys);
+  g_cache.clear();
+}
+
+int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR, int32_t *ia,
+                int32_t *ja, double *al, double *ad, double *au, double *b, double *x,
+                void *iNeq, void *bOmp, double tol, uint32_t maxIt, int16_t storage,
+                int16_t solver, FILE *fSolvLog, bool fLog, bool newX, bool unSym,
+                const char *name) {
+  (void)m;
+  (void)nAdR;
+  (void)iNeq;
+  (void)bOmp;
+  std::lock_guard<std::mutex> lk(g_shim_mu);
+  int rc = SFR_OK;
+  if ((solver != SFR_PCG && solver != SFR_PBICGSTAB) || nEqNov != nEq) {
+    // the reference's ERRO_OP (Erro.h:17-20) for an option this path lacks
+    fprintf(stderr, "Opcao %d e invalida!!\n", solver);
+    fprintf(stderr, "Arquivo:%s\nFonte:  %s\n", __FILE__, "sfr_solverC");
+    if (g_exit_on_failure) exit(EXIT_FAILURE);
+    return SFR_UNSUPPORTED;
+  }
+  const int32_t n_ia = storage == SFR_ELLPACK ? 2 : nEq + 1;
+  int64_t n_ja = 0;
+  if (storage == SFR_ELLPACK)
+    n_ja = static_cast<int64_t>(nEq) * ia[0];
+  else
+    n_ja = static_cast<int64_t>(ia[nEq]) - ia[0];
+  const uint64_t h = pattern_hash(ia, ja, n_ia, n_ja);
+  PatternKey key{ia, ja, nEq, storage, unSym ? 1 : 0};
+  Cached &c = g_cache[key];
+  if (!c.sys || c.hash != h) {
+    if (c.sys) sfr_gpu_destroy(c.sys);
+    c.sys = nullptr;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    rc = sfr_gpu_create(nEq, nAd, ia, ja, storage, unSym ? 1 : 0, dev, &c.sys);
+    if (rc != SFR_OK) {
+      g_cache.erase(key);
+      fprintf(stderr, "sfr_solverC: %s (%s)\n", sfr_status_string(rc), g_last_error.c_str());
+      if (g_exit_on_failure) exit(EXIT_FAILURE);
+      return rc;
+    }
+    c.hash = h;
+  }
+  sfr_system *s = c.sys;
+  rc = sfr_gpu_set_values(s, al, ad, au);
+  sfr_solve_info info;
+  std::memset(&info, 0, sizeof(info));
+  if (rc == SFR_OK)
+    rc = sfr_gpu_solve(s, solver, b, x, tol, maxIt, newX ? 1 : 0, g_precision, &info);
+  if (rc == SFR_MAXIT) {
+    // Cg.c:195-200 / Bicgstab.c:225-231
+    printf("name : %s\n", name ? name : "");
+    if (solver == SFR_PCG)
+      printf("PCG: *** WARNING: no convergende reached !\n");
+    else
+      printf(" PBICGSTAB *** WARNING: no convergende reached !\n");
+    printf("MAXIT = %d \n", maxIt);
+    if (g_exit_on_failure) exit(solver == SFR_PCG ? EXIT_FAILURE : -2);
+    return rc;
+  }
+  if (rc != SFR_OK) {
+    fprintf(stderr, "sfr_solverC: %s (%s)\n", sfr_status_string(rc), g_last_error.c_str());
+    if (g_exit_on_failure) exit(solver == SFR_PCG ? EXIT_FAILURE : -2);
+    return rc;
+  }
+  if (fLog && fSolvLog) {
+    // Cg.c:201-208 / Bicgstab.c:235-242
+    if (solver == SFR_PCG)
+      fprintf(fSolvLog,
+              "PCG: tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e time %20.5lf\n", tol,
+              info.iters, info.xKx, info.norm_x, info.seconds);
+    else
+      fprintf(fSolvLog,
+              "PBICGSTAB: tol %20.2e iteration %d xKx %20.12e ||x*x|| %20.12e time %20.5lf\n",
+              tol, info.iters, info.xKx, info.norm_x, info.seconds);
+  }
+  return SFR_OK;
+}
+
+}  // extern "C"

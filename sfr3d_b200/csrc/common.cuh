@@ -1,0 +1,185 @@
+// Shared device utilities of the sm_100a solve path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda/atomic>
+#include <cstdint>
+
+#include "sfr3d_b200.h"
+
+namespace sfr {
+
+constexpr int kWarp = 32;
+
+// ----------------------------------------------------------------------
+// Loads.  The matrix is read once per sweep: streaming (evict-first) loads
+// keep it from pushing the Krylov vectors out of L2.  Vectors written inside
+// a persistent launch are read with .cg (L2, never a stale L1 line).
+// ----------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
+template <typename T>
+__device__ __forceinline__ T ld_vec(const T *p) { return __ldcg(p); }
+template <typename T>
+__device__ __forceinline__ void st_vec(T *p, T v) { __stcg(p, v); }
+
+// ----------------------------------------------------------------------
+// Arithmetic that rounds exactly as the reference's host code does (one
+// rounding per multiply and per add; no FMA contraction).  Used by the FP64
+// path so that every SpMV row and vector update is bit-identical to
+// HccaBlas.c / Cg.c / Bicgstab.c.
+// ----------------------------------------------------------------------
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+
+// ----------------------------------------------------------------------
+// Deterministic reductions: fixed shuffle tree inside a warp, fixed tree
+// over the warps of a block, fixed sequential+tree order over the blocks.
+// ----------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;  // valid in lane 0
+}
+
+// Reduce NV per-thread values over the block; thread 0 writes
+// part[v * stride + blockIdx.x].  `sm` holds NV * 32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_partials(const double (&acc)[NV], double *part,
+                                               int stride, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = warp_sum(acc[v]);
+    if (lane == 0) sm[v * 32 + warp] = w;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double w = lane < nwarps ? sm[v * 32 + lane] : 0.0;
+      w = warp_sum(w);
+      if (lane == 0) st_vec(part + v * stride + blockIdx.x, w);
+    }
+  }
+  __syncthreads();
+}
+
+// Every block sums the nblocks partials of each value in the same order, so
+// all blocks hold bit-identical totals.  Result broadcast through `sm`.
+template <int NV>
+__device__ __forceinline__ void grid_totals(const double *part, int stride, int nblocks,
+                                            double (&out)[NV], double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double s = 0.0;
+      for (int b = lane; b < nblocks; b += 32) s += ld_vec(part + v * stride + b);
+      s = warp_sum(s);
+      if (lane == 0) sm[v] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] = sm[v];
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------------
+// Grid-wide barrier for a cooperative (co-resident) launch.  Every wait is
+// bounded: after `spin_limit` polls the block records SFR_TIMEOUT in *err and
+// returns false; a block that sees *err set stops waiting at once, so every
+// block leaves the kernel in bounded time.
+// ----------------------------------------------------------------------
+struct GridSync {
+  unsigned int *count;
+  unsigned int *gen;
+  int *err;
+  unsigned int nblocks;
+  unsigned int spin_limit;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridSync &g) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(*g.gen);
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(*g.count);
+    cuda::atomic_ref<int, cuda::thread_scope_device> err(*g.err);
+    int ok = 1;
+    const unsigned int my = gen.load(cuda::memory_order_relaxed);
+    const unsigned int prev = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    if (prev == g.nblocks - 1) {
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.store(my + 1u, cuda::memory_order_release);
+    } else {
+      unsigned int spins = 0;
+      while (gen.load(cuda::memory_order_acquire) == my) {
+        if (err.load(cuda::memory_order_relaxed) != 0) { ok = 0; break; }
+        if (++spins > g.spin_limit) {
+          int expected = 0;
+          err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    if (ok && err.load(cuda::memory_order_relaxed) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ----------------------------------------------------------------------
+// Sliced ELLPACK (SELL-32) view.  Rows are grouped in slices of 32; slice s
+// holds w_s = (sptr[s+1]-sptr[s])/32 slots, stored slot-major so that lane l
+// of a warp reads row 32s+l.  Slot k of a row is its k-th off-diagonal in the
+// reference's summation order; the diagonal is separate and summed first.
+// Padded slots have col = row and val = 0.
+// ----------------------------------------------------------------------
+template <typename V>
+struct SellView {
+  int n;
+  int nslices;
+  const int *sptr;
+  const int *col;
+  const V *val;
+  const V *diag;
+};
+
+// Row r = 32*s + lane of A*x with the reference's rounding: diagonal product
+// first, then each slot's product added in order.
+template <typename V, typename XV>
+__device__ __forceinline__ double row_spmv_exact(const SellView<V> &A, int s, int lane,
+                                                 const XV *x) {
+  const int r = s * kWarp + lane;
+  const int base = __ldg(A.sptr + s);
+  const int w = (__ldg(A.sptr + s + 1) - base) >> 5;
+  double t = xmul(static_cast<double>(ld_stream(A.diag + r)), static_cast<double>(ld_vec(x + r)));
+  const int *c = A.col + base + lane;
+  const V *v = A.val + base + lane;
+#pragma unroll 4
+  for (int k = 0; k < w; ++k) {
+    const int j = ld_stream(c + k * kWarp);
+    const double a = static_cast<double>(ld_stream(v + k * kWarp));
+    t = xadd(t, xmul(a, static_cast<double>(ld_vec(x + j))));
+  }
+  return t;
+}
+
+// Block-contiguous slice range of this block.
+__device__ __forceinline__ void block_slices(int nslices, int *first, int *last) {
+  const long long G = gridDim.x;
+  *first = static_cast<int>((static_cast<long long>(nslices) * blockIdx.x) / G);
+  *last = static_cast<int>((static_cast<long long>(nslices) * (blockIdx.x + 1)) / G);
+}
+
+}  // namespace sfr

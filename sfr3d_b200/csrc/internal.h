@@ -1,0 +1,96 @@
+// Internal host-side structures of libsfr3d_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sfr3d_b200.h"
+
+namespace sfr {
+
+constexpr int kWarpHost = 32;  // rows per SELL slice (one warp)
+
+// SELL-32 layout built on the host from one of the reference's layouts.
+// src[e] is the index of slot e's value in the value source the caller
+// passes (al, or al|au for CSRC unsym), or -1 for a padded slot.
+struct HostSell {
+  int32_t n = 0;
+  int32_t nslices = 0;
+  std::vector<int32_t> sptr;  // nslices + 1, in slots
+  std::vector<int32_t> col;
+  std::vector<int32_t> src;
+  int32_t bandwidth = 0;
+  int32_t max_width = 0;
+  int64_t nnz = 0;  // real (non-padded) off-diagonal slots
+};
+
+// Validates the reference layout and builds the SELL copy of A (and, when
+// `transpose` is set, of A^T).  Returns SFR_OK or SFR_BAD_INPUT with a
+// message in *why.
+int build_sell(int32_t neq, int32_t nad, const int32_t *ia, const int32_t *ja,
+               int32_t storage, int32_t unsym, HostSell *a, HostSell *at,
+               int32_t *nsrc, std::string *why);
+
+// Device copy of one SELL matrix.
+struct DevSell {
+  int32_t n = 0, nslices = 0;
+  int64_t nslots = 0;
+  int32_t *sptr = nullptr, *col = nullptr, *src = nullptr;
+  double *val = nullptr;  // FP64 values
+  float *val32 = nullptr; // FP32 copy (mixed precision)
+};
+
+struct SolveOut;  // device-side result record (krylov.cu)
+
+struct Workspace {
+  size_t bytes = 0;
+  void *base = nullptr;
+};
+
+}  // namespace sfr
+
+struct sfr_system {
+  int32_t device = 0;
+  int32_t n = 0;
+  int32_t storage = 0;
+  int32_t unsym = 0;
+  int32_t nad = 0;
+  int32_t nsrc = 0;  // length of the value source (al[, au])
+  int32_t bandwidth = 0;
+  sfr::HostSell host_at;    // kept until A^T is first needed
+  bool have_at_host = false;
+  sfr::DevSell A, At;
+  bool at_ready = false;
+  double *d_stage = nullptr;   // raw al|au
+  double *d_diag = nullptr;    // ad
+  float *d_diag32 = nullptr;
+  bool values_set = false;
+  cudaStream_t stream = nullptr;
+  sfr::Workspace ws;
+  int64_t bytes = 0;
+};
+
+namespace sfr {
+int upload_sell(const HostSell &h, DevSell *d, int64_t *bytes);
+void free_sell(DevSell *d);
+int ensure_workspace(sfr_system *s, size_t bytes);
+int gather_values(sfr_system *s, DevSell *d, cudaStream_t st);
+cudaError_t convert_diag32(const double *src, float *dst, int n, cudaStream_t st);
+
+// kernels / solvers (krylov.cu)
+int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
+                 const double *d_b, double *d_x, double tol, uint32_t maxit,
+                 int32_t newx, int32_t precision, cudaStream_t st,
+                 sfr_solve_info *info);
+int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag,
+                const double *d_x, double *d_y, double *d_dot, cudaStream_t st);
+int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
+               cudaStream_t st);
+// (a, b) into host memory through the device's per-device scratch
+int dot_host(const double *d_a, const double *d_b, int32_t n, double *h_out,
+             cudaStream_t st);
+int num_sms(int device);
+}  // namespace sfr

@@ -1,0 +1,271 @@
+"""Host-side mirror of SFR3D's solver interface over libsfr3d_b200.so.
+
+``solverC`` keeps the argument list and meaning of the reference entry point
+(Solv.h:59-70, Solv.c:64-501); ``GpuSystem`` is the explicit handle API
+(create / set_values / solve / destroy) that keeps a pattern resident on the
+GPU.  Every call goes through the C ABI declared in include/sfr3d_b200.h;
+there is no CPU implementation behind it.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+# solver / storage / status codes (include/sfr3d_b200.h; Define.h:392-412)
+PCG, PBICGSTAB = 1, 2
+CSRD, CSRC, ELLPACK = 2, 3, 4
+OK, MAXIT, BREAKDOWN = 0, 1, 2
+BAD_INPUT, CUDA_ERROR, TIMEOUT, UNSUPPORTED = -1, -2, -3, -4
+FP64, MIXED = 0, 1
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+
+
+class SolveInfoC(ctypes.Structure):
+    _fields_ = [("iters", _I32), ("status", _I32), ("xKx", ctypes.c_double),
+                ("norm_x", ctypes.c_double), ("norm_r", ctypes.c_double),
+                ("norm_r_m", ctypes.c_double), ("conv", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("refinements", _I32),
+                ("inner_iters", _I32), ("relres", ctypes.c_double)]
+
+
+@dataclass
+class SolveInfo:
+    iters: int
+    status: int
+    xKx: float
+    norm_x: float
+    norm_r: float
+    norm_r_m: float
+    conv: float
+    seconds: float
+    refinements: int
+    inner_iters: int
+    relres: float
+
+    @classmethod
+    def from_c(cls, c: SolveInfoC) -> "SolveInfo":
+        return cls(**{f: getattr(c, f) for f, _ in SolveInfoC._fields_})
+
+
+class SolverError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what}: {status_string(status)} ({last_error()})")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    L = _native.load("libsfr3d_b200.so")
+    if getattr(L, "_typed", False):
+        return L
+    L.sfr_status_string.restype = ctypes.c_char_p
+    L.sfr_status_string.argtypes = [ctypes.c_int]
+    L.sfr_last_error.restype = ctypes.c_char_p
+    L.sfr_gpu_check_device.argtypes = [_I32, _P, _P]
+    L.sfr_gpu_create.argtypes = [_I32, _I32, _P, _P, _I32, _I32, _I32,
+                                 ctypes.POINTER(_P)]
+    L.sfr_gpu_set_values.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_set_diagonal.argtypes = [_P, _P]
+    L.sfr_gpu_solve.argtypes = [_P, _I32, _P, _P, ctypes.c_double,
+                                ctypes.c_uint32, _I32, _I32, _P]
+    L.sfr_gpu_solve_device.argtypes = [_P, _I32, _P, _P, ctypes.c_double,
+                                       ctypes.c_uint32, _I32, _I32, _P, _P]
+    L.sfr_gpu_solve_multi.argtypes = [_P, _I32, _I32, _P, _P, _P,
+                                      ctypes.c_double, ctypes.c_uint32, _I32,
+                                      _I32, _P]
+    L.sfr_gpu_destroy.argtypes = [_P]
+    L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_spmv_transpose.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_spmv_dot.argtypes = [_P, _P, _P, _P, _P]
+    L.sfr_gpu_dot.argtypes = [_P, _P, _I32, _P, _P]
+    L.sfr_gpu_stats.argtypes = [_P, _P, _P, _P]
+    L.sfr_solverC.argtypes = [_P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P,
+                              _P, _P, _P, _P, ctypes.c_double, ctypes.c_uint32,
+                              ctypes.c_int16, ctypes.c_int16, _P, ctypes.c_bool,
+                              ctypes.c_bool, ctypes.c_bool, ctypes.c_char_p]
+    L.sfr_set_exit_on_failure.argtypes = [_I32]
+    L.sfr_set_exit_on_failure.restype = None
+    L.sfr_set_precision.argtypes = [_I32]
+    L.sfr_set_precision.restype = None
+    L.sfr_solverC_release.restype = None
+    L.sfr_solverC_release.argtypes = []
+    L._typed = True
+    return L
+
+
+def status_string(status: int) -> str:
+    return lib().sfr_status_string(status).decode()
+
+
+def last_error() -> str:
+    return lib().sfr_last_error().decode()
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def check_device(device: int = 0) -> tuple[int, int, int]:
+    ma, mi = ctypes.c_int32(), ctypes.c_int32()
+    rc = lib().sfr_gpu_check_device(device, ctypes.byref(ma), ctypes.byref(mi))
+    return rc, ma.value, mi.value
+
+
+class GpuSystem:
+    """One sparse pattern resident on a GPU (sfr_gpu_create ... destroy)."""
+
+    def __init__(self, neq: int, ia, ja, storage: int, unsym: bool,
+                 nad: int | None = None, device: int = 0):
+        self._ia = _i32(ia)
+        self._ja = _i32(ja) if ja is not None else None
+        if nad is None:
+            nad = (int(self._ia[1]) if storage == ELLPACK
+                   else int(self._ia[neq] - self._ia[0]))
+        self.neq, self.nad, self.storage, self.unsym = neq, nad, storage, unsym
+        h = _P()
+        rc = lib().sfr_gpu_create(neq, nad, _ptr(self._ia), _ptr(self._ja),
+                                  storage, int(unsym), device, ctypes.byref(h))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sfr_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_values(self, al, ad, au=None):
+        al, ad, au = _f64(al), _f64(ad), _f64(au)
+        rc = lib().sfr_gpu_set_values(self.h, _ptr(al), _ptr(ad), _ptr(au))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_values")
+
+    def set_diagonal(self, ad):
+        ad = _f64(ad)
+        rc = lib().sfr_gpu_set_diagonal(self.h, _ptr(ad))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_diagonal")
+
+    def solve(self, solver: int, b, x0=None, tol: float = 1e-10,
+              maxit: int = 100000, newx: bool = True, precision: int = FP64,
+              raise_on_error: bool = True):
+        """Host-buffer solve (sfr_gpu_solve).  Returns (x, SolveInfo)."""
+        b = _f64(b)
+        x = np.zeros(self.neq) if x0 is None else np.array(x0, dtype=np.float64)
+        info = SolveInfoC()
+        rc = lib().sfr_gpu_solve(self.h, solver, _ptr(b), _ptr(x), tol, maxit,
+                                 int(newx), precision, ctypes.byref(info))
+        if rc < 0 and raise_on_error:
+            raise SolverError(rc, "sfr_gpu_solve")
+        return x, SolveInfo.from_c(info)
+
+    def solve_multi(self, solver: int, b, x0=None, ad_k=None, tol=1e-10,
+                    maxit=100000, newx=True, precision=FP64,
+                    raise_on_error=True):
+        """k right-hand sides sharing the matrix; b is (k, neq)."""
+        b = _f64(b)
+        k = b.shape[0]
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64)
+        ad_k = _f64(ad_k)
+        infos = (SolveInfoC * k)()
+        rc = lib().sfr_gpu_solve_multi(self.h, solver, k, _ptr(ad_k), _ptr(b),
+                                       _ptr(x), tol, maxit, int(newx),
+                                       precision, infos)
+        if rc < 0 and raise_on_error:
+            raise SolverError(rc, "sfr_gpu_solve_multi")
+        return x, [SolveInfo.from_c(infos[i]) for i in range(k)]
+
+    # device-pointer entry points (pointers are plain integers)
+    def solve_device(self, solver, d_b: int, d_x: int, tol=1e-10,
+                     maxit=100000, newx=True, precision=FP64, stream: int = 0):
+        info = SolveInfoC()
+        rc = lib().sfr_gpu_solve_device(self.h, solver, d_b, d_x, tol, maxit,
+                                        int(newx), precision, stream or None,
+                                        ctypes.byref(info))
+        if rc < 0:
+            raise SolverError(rc, "sfr_gpu_solve_device")
+        return SolveInfo.from_c(info)
+
+    def spmv(self, d_x: int, d_y: int, stream: int = 0):
+        rc = lib().sfr_gpu_spmv(self.h, d_x, d_y, stream or None)
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_spmv")
+
+    def spmv_transpose(self, d_x: int, d_y: int, stream: int = 0):
+        rc = lib().sfr_gpu_spmv_transpose(self.h, d_x, d_y, stream or None)
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_spmv_transpose")
+
+    def spmv_dot(self, d_x: int, d_y: int, stream: int = 0) -> float:
+        out = ctypes.c_double()
+        rc = lib().sfr_gpu_spmv_dot(self.h, d_x, d_y, ctypes.byref(out),
+                                    stream or None)
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_spmv_dot")
+        return out.value
+
+    def stats(self):
+        b, s, w = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        lib().sfr_gpu_stats(self.h, ctypes.byref(b), ctypes.byref(s),
+                            ctypes.byref(w))
+        return {"device_bytes": b.value, "slots": s.value, "bandwidth": w.value}
+
+
+def dot(d_a: int, d_b: int, n: int, stream: int = 0) -> float:
+    out = ctypes.c_double()
+    rc = lib().sfr_gpu_dot(d_a, d_b, n, ctypes.byref(out), stream or None)
+    if rc != OK:
+        raise SolverError(rc, "sfr_gpu_dot")
+    return out.value
+
+
+def solverC(nEq, nEqNov, nAd, nAdR, ia, ja, al, ad, au, b, x, tol, maxIt,
+            storage, solver, fSolvLog=None, fLog=False, newX=True,
+            unSym=False, name="system", exit_on_failure=False) -> int:
+    """The reference's solverC (Solv.c:64) through sfr_solverC: x is updated
+    in place, b is left unchanged.  fSolvLog is a C FILE* (integer) or None.
+    Returns the status (the reference returns nothing and exits on failure;
+    pass exit_on_failure=True for that behaviour)."""
+    L = lib()
+    L.sfr_set_exit_on_failure(int(exit_on_failure))
+    ia, ja = _i32(ia), _i32(ja)
+    al, ad, au, b = _f64(al), _f64(ad), _f64(au), _f64(b)
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+        raise TypeError("x must be a C-contiguous float64 array (updated in place)")
+    return L.sfr_solverC(None, nEq, nEqNov, nAd, nAdR, _ptr(ia), _ptr(ja),
+                         _ptr(al), _ptr(ad), _ptr(au), _ptr(b), _ptr(x), None,
+                         None, tol, maxIt, storage, solver, fSolvLog,
+                         bool(fLog), bool(newX), bool(unSym), name.encode())
+
+
+def set_precision(precision: int) -> None:
+    lib().sfr_set_precision(precision)
+
+
+def release_cache() -> None:
+    lib().sfr_solverC_release()

@@ -1,0 +1,238 @@
+"""GPU parity against the oracle (FP64 plain path), through the C ABI.
+
+Bar: SpMV rows bit-identical to the reference's kernels; PCG / BiCGSTAB
+solutions within 1e-12 relative (2-norm) of the reference's FP64 solver at
+equal iteration count (+-1).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from helpers import layouts, rel
+from oracle import oracle as O
+from sfr3d_b200 import solver as sv
+from sfr3d_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+TOL_X = 1e-12  # relative 2-norm error in x, FP64 path vs reference
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_solves.npz"))
+
+
+def gpu_system(sysx, lname):
+    st, un, ia, ja, al, au = layouts(sysx)[lname]
+    g = sv.GpuSystem(sysx.neq, ia, ja, st, un)
+    g.set_values(al, sysx.ad, au)
+    return g, (st, un, ia, ja, al)
+
+
+def reference(solver, st, un, ia, ja, al, ad, b, **kw):
+    if O.ref_available():
+        return O.ref_solve(solver, st, un, ia, ja, al, ad, b, **kw)
+    fn = O.pcg if solver == O.PCG else O.pbicgstab
+    return fn(st, un, ia, ja, al, ad, b, **kw)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "jittered", "momentum"])
+def test_spmv_bit_identical(cuda, kind):
+    torch = cuda
+    s = {"uniform": lambda: S.poisson_uniform(12, seed=31),
+         "jittered": lambda: S.poisson_jittered(13, seed=32),
+         "momentum": lambda: S.momentum(11, seed=33, nrhs=1)}[kind]()
+    x = np.random.default_rng(1).standard_normal(s.neq)
+    dx = torch.tensor(x, device="cuda")
+    for lname in layouts(s):
+        g, (st, un, ia, ja, al) = gpu_system(s, lname)
+        dy = torch.empty_like(dx)
+        g.spmv(dx.data_ptr(), dy.data_ptr())
+        torch.cuda.synchronize()
+        want = O.matvec(st, un, ia, ja, al, s.ad, x)
+        assert np.array_equal(dy.cpu().numpy(), want), lname
+        dot = g.spmv_dot(dx.data_ptr(), dy.data_ptr())
+        assert abs(dot - float(np.dot(want, x))) <= 1e-13 * abs(dot)
+        g.close()
+
+
+def test_dot_deterministic(cuda):
+    torch = cuda
+    a = torch.randn(3_000_001, dtype=torch.float64, device="cuda")
+    b = torch.randn(3_000_001, dtype=torch.float64, device="cuda")
+    v1 = sv.dot(a.data_ptr(), b.data_ptr(), a.numel())
+    v2 = sv.dot(a.data_ptr(), b.data_ptr(), a.numel())
+    assert v1 == v2
+    assert abs(v1 - float(torch.dot(a, b))) < 1e-10 * a.numel() ** 0.5
+
+
+@pytest.mark.parametrize("name", [str(c) for c in GOLD["cases"]])
+def test_solver_against_reference_fixture(cuda, name):
+    g = {k.split("/", 1)[1]: GOLD[k] for k in GOLD.files if k.startswith(name + "/")}
+    solver, st, un, maxit, newx = (int(v) for v in g["meta"])
+    iters, status = (int(v) for v in g["res"])
+    n = len(g["ad"])
+    sysg = sv.GpuSystem(n, g["ia"], g["ja"], st, bool(un))
+    sysg.set_values(g["al"], g["ad"])
+    x, info = sysg.solve(solver, g["b"], x0=g["x0"], tol=float(g["tol"][0]),
+                         maxit=maxit, newx=bool(newx))
+    if status == 0:
+        assert info.status == sv.OK
+        assert abs(info.iters - iters) <= 1
+        assert rel(x, g["x"]) < TOL_X
+    else:
+        assert info.status == sv.MAXIT
+        assert info.iters == iters + 1 or info.iters == maxit + 1
+        assert rel(x, g["x"]) < 1e-10
+
+
+@pytest.mark.parametrize("lname", ["csrd_full", "csrd_sym", "csrc_sym", "ellpack"])
+def test_pcg_uniform_32(cuda, lname):
+    s = S.poisson_uniform(32, seed=1)
+    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    x, info = g.solve(sv.PCG, s.b[0], tol=1e-10)
+    ref = reference(O.PCG, st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
+    assert info.status == sv.OK and ref.status == 0
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(x, ref.x) < TOL_X
+    assert abs(info.xKx - ref.xKx) <= 1e-11 * abs(ref.xKx)
+
+
+def test_pcg_jittered_contrast(cuda):
+    s = S.poisson_jittered(40, seed=2)
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full")
+    x, info = g.solve(sv.PCG, s.b[0], tol=1e-10)
+    ref = O.pcg(st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
+    assert info.status == sv.OK
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(x, ref.x) < TOL_X
+
+
+def steady_system(n=24, seed=41):
+    """Nearly steady upwind convection-diffusion (dt = 1e3, Peclet 50)."""
+    return S.build(S.params(kind=S.SFR_SYS_CONVDIFF, n=n, lengths=(np.pi,) * 3,
+                            dirichlet=S.ALL_FACES, nrhs=1, rhs_normal=True,
+                            peclet=50.0, nu=1e-3, dt=1e3, seed=seed))
+
+
+@pytest.mark.parametrize("lname", ["csrd_full", "csrc_unsym", "ellpack"])
+def test_bicgstab_momentum(cuda, lname):
+    # the momentum system as the SIMPLE loop sees it (dt = 1e-2)
+    s = S.momentum(24, seed=41, nrhs=1)
+    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    x, info = g.solve(sv.PBICGSTAB, s.b[0], tol=1e-10)
+    ref = reference(O.PBICGSTAB, st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
+    assert info.status == sv.OK and ref.status == 0
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(x, ref.x) < TOL_X
+
+
+def reference_spread(solver, s, b):
+    """How far the reference moves from its own serial result when only the
+    reduction order changes: its OpenMP path (dotOmp reductions, per-thread
+    SpMV buffers) at 2, 4 and 8 threads on the CSRD layout."""
+    ser = O.ref_solve(solver, O.CSRD, True, s.ia, s.ja, s.al, s.ad, b)
+    its, errs = [ser.iters], [0.0]
+    for nt in (2, 4, 8):
+        o = O.ref_solve(solver, O.CSRD, True, s.ia, s.ja, s.al, s.ad, b, nthreads=nt)
+        its.append(o.iters)
+        errs.append(rel(o.x, ser.x))
+    return ser, min(its), max(its), max(errs)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("lname", ["csrd_full", "csrc_unsym", "ellpack"])
+def test_bicgstab_steady_within_reference_spread(cuda, lname):
+    # Convection-dominated and nearly steady: the BiCGSTAB residual history
+    # is irregular near the threshold, so any change of summation order moves
+    # the iteration count by a few and x by up to ~1e-9 -- the reference's
+    # own OpenMP path does.  Bar: stay inside that spread (+1 iteration, x 4x).
+    s = steady_system()
+    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    x, info = g.solve(sv.PBICGSTAB, s.b[0], tol=1e-10)
+    ser, lo, hi, err = reference_spread(O.PBICGSTAB, s, s.b[0])
+    assert info.status == sv.OK
+    assert lo - 1 <= info.iters <= hi + 1
+    assert rel(x, ser.x) <= max(TOL_X, 4 * err)
+
+
+@pytest.mark.parametrize("solver", [sv.PCG, sv.PBICGSTAB])
+def test_multi_rhs_matches_single(cuda, solver):
+    s = (S.poisson_jittered(16, seed=51) if solver == sv.PCG
+         else S.momentum(16, seed=52, nrhs=3))
+    b = np.stack([s.b[0], -0.5 * s.b[0] + 0.1, np.cos(np.arange(s.neq))]) \
+        if solver == sv.PCG else s.b
+    g, _ = gpu_system(s, "csrd_full")
+    xs, infos = g.solve_multi(solver, b, tol=1e-10)
+    for k in range(3):
+        x1, i1 = g.solve(solver, b[k], tol=1e-10)
+        assert infos[k].iters == i1.iters
+        assert np.array_equal(xs[k], x1)
+
+
+def test_multi_rhs_per_component_diagonal(cuda):
+    # u, v, w share al/au and differ in ad (Simple.c:2736-2750)
+    s = S.momentum(14, seed=53, nrhs=3)
+    ad_k = np.stack([s.ad, 1.1 * s.ad, 0.95 * s.ad])
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full")
+    xs, infos = g.solve_multi(sv.PBICGSTAB, s.b, ad_k=ad_k, tol=1e-10)
+    for k in range(3):
+        ref = O.pbicgstab(st, un, ia, ja, al, ad_k[k], s.b[k], tol=1e-10)
+        assert abs(infos[k].iters - ref.iters) <= 1
+        assert rel(xs[k], ref.x) < TOL_X
+
+
+def test_warm_start_and_repeatability(cuda):
+    s = S.poisson_uniform(20, seed=61)
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_sym")
+    x0 = np.linspace(-1, 1, s.neq)
+    x1, i1 = g.solve(sv.PCG, s.b[0], x0=x0, newx=False, tol=1e-9)
+    x2, i2 = g.solve(sv.PCG, s.b[0], x0=x0, newx=False, tol=1e-9)
+    assert np.array_equal(x1, x2) and i1.iters == i2.iters
+    ref = O.pcg(st, un, ia, ja, al, s.ad, s.b[0], x0=x0, newx=False, tol=1e-9)
+    assert abs(i1.iters - ref.iters) <= 1
+    assert rel(x1, ref.x) < TOL_X
+
+
+def test_breakdown_and_maxit_are_statuses_not_hangs(cuda):
+    s = S.poisson_uniform(10, seed=71)
+    g, _ = gpu_system(s, "csrd_full")
+    b = s.b[0].copy()
+    b[5] = np.nan
+    _, info = g.solve(sv.PCG, b, tol=1e-10, maxit=50)
+    assert info.status in (sv.BREAKDOWN, sv.MAXIT)
+    _, info = g.solve(sv.PCG, s.b[0], tol=1e-10, maxit=3)
+    assert info.status == sv.MAXIT and info.iters == 4
+
+
+def test_solverC_dropin_log_line(cuda):
+    s = S.poisson_uniform(16, seed=81)
+    il, jl, al = s.csrd_lower()
+    x = np.zeros(s.neq)
+    libc = ctypes.CDLL(None)
+    libc.fopen.restype = ctypes.c_void_p
+    libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    libc.fclose.argtypes = [ctypes.c_void_p]
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "solv_log.txt")
+        f = libc.fopen(path.encode(), b"w")
+        b = s.b[0].copy()
+        rc = sv.solverC(s.neq, s.neq, len(jl), 0, il, jl, al, s.ad, None, b, x,
+                        1e-10, 1000, sv.CSRD, sv.PCG, fSolvLog=f, fLog=True,
+                        newX=True, unSym=False, name="pres")
+        libc.fclose(f)
+        line = open(path).read()
+    assert rc == sv.OK
+    assert np.array_equal(b, s.b[0])          # b unchanged (Cg.c:41)
+    ref = O.pcg(O.CSRD, False, il, jl, al, s.ad, s.b[0], tol=1e-10)
+    assert line.startswith("PCG: tol") and f"iteration {ref.iters} " in line
+    assert rel(x, ref.x) < TOL_X
+    # second call reuses the cached pattern
+    x2 = np.zeros(s.neq)
+    assert sv.solverC(s.neq, s.neq, len(jl), 0, il, jl, al, s.ad, None, s.b[0],
+                      x2, 1e-10, 1000, sv.CSRD, sv.PCG) == sv.OK
+    assert np.array_equal(x, x2)
+    sv.release_cache()
