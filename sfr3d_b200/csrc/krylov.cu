@@ -592,8 +592,11 @@ __global__ void __launch_bounds__(256) spmv_dot_kernel(SellView<double> A, const
 __global__ void __launch_bounds__(256) dot_kernel(const double *a, const double *b, int n,
                                                   double *part, unsigned *counter, double *out) {
   double acc = 0.0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) acc += a[i] * b[i];
+  // 64-bit index: i + stride must not overflow for n close to INT32_MAX
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += stride)
+    acc += a[i] * b[i];
   last_block_total(acc, part, counter, out);
 }
 
