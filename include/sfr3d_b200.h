@@ -132,6 +132,19 @@ int sfr_gpu_spmv_dot(sfr_system *s, const double *d_x, double *d_y,
 int sfr_gpu_dot(const double *d_a, const double *d_b, int32_t n,
                 double *dot_out, void *stream);
 
+/* (a, b) like sfr_gpu_dot, for callers that cannot let this library
+ * allocate device memory (a program that reserves its GPU memory once and
+ * parcels it out itself, as SFR3D does with its host arena, or one running
+ * while another allocator holds the memory).  No counterpart in the
+ * reference.  Never calls cudaMalloc/cudaFree: its scratch is a fixed
+ * 4,752-byte device array (592 block partials, result, counter) that every
+ * GPU loading the library keeps until exit.  The first call on a device
+ * looks up that array's address; make it before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race.  n < 0 is
+ * rejected with SFR_BAD_INPUT. */
+int sfr_gpu_dot_noalloc(const double *d_a, const double *d_b, int32_t n,
+                        double *dot_out, void *stream);
+
 /* Device memory the handle holds (bytes) and its SELL slot count. */
 int sfr_gpu_stats(const sfr_system *s, int64_t *bytes, int64_t *slots,
                   int32_t *bandwidth);
