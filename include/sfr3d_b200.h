@@ -174,6 +174,10 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
                 int16_t solver, FILE *fSolvLog, bool fLog, bool newX,
                 bool unSym, const char *name);
 void sfr_set_exit_on_failure(int32_t flag);
+/* SFR_MIXED: the inner FP32 residual must fall by this factor (0 < delta
+ * < 1, default 0.1) before the FP64 solution is refreshed and the true
+ * residual recomputed. */
+void sfr_set_reliable_delta(double delta);
 /* Precision used by sfr_solverC (SFR_FP64 default). */
 void sfr_set_precision(int32_t precision);
 /* Release every pattern sfr_solverC cached. */

@@ -85,6 +85,10 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
                  const double *d_b, double *d_x, double tol, uint32_t maxit,
                  int32_t newx, int32_t precision, cudaStream_t st,
                  sfr_solve_info *info);
+// FP32 inner Krylov with FP64 reliable updates (mixed.cu)
+int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
+                const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
+                cudaStream_t st, sfr_solve_info *info);
 int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag,
                 const double *d_x, double *d_y, double *d_dot, cudaStream_t st);
 int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,

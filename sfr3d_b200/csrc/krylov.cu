@@ -20,19 +20,9 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "persist.cuh"
 
 namespace sfr {
-
-constexpr int kMaxK = 4;
-constexpr int kThreads = 512;
-constexpr int kMaxNV = 4 * kMaxK;
-
-struct SolveOut {
-  int iters;
-  int status;
-  double xKx, norm_x, norm_r, norm_r_m, conv;
-  double bnorm;
-};
 
 struct KrylovArgs {
   SellView<double> A;
@@ -55,22 +45,11 @@ struct KrylovArgs {
   int newx;
 };
 
-#define SFR_FOR_OWN_ROWS(s0, s1)                                          \
-  for (int s_ = (s0) + (threadIdx.x >> 5); s_ < (s1); s_ += (blockDim.x >> 5)) \
-    for (int row_ = s_ * kWarp + (threadIdx.x & 31), once_ = 1; once_; once_ = 0) \
-      if (row_ < n)
-
-// Reduce NV values: write partials into the next slot, barrier, total.
+// Reduce NV values of a FP64 solve: partials, barrier, totals.
 template <int NV>
 __device__ __forceinline__ bool reduce_all(const KrylovArgs &a, int &slot, double (&acc)[NV],
                                            double (&tot)[NV], double *sm) {
-  const int G = gridDim.x;
-  double *base = a.part + static_cast<size_t>(slot) * kMaxNV * G;
-  block_partials<NV>(acc, base, G, sm);
-  if (!grid_sync(a.gs)) return false;
-  grid_totals<NV>(base, G, G, tot, sm);
-  slot ^= 1;
-  return true;
+  return reduce_step<NV>(a.part, a.gs, slot, acc, tot, sm);
 }
 
 // y_k[row] for K right-hand sides from a gather functor g(k, col).
@@ -283,6 +262,8 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         o.norm_r = sqrt(tot[4 * k + 3]);
         o.conv = conv[k];
         o.bnorm = 0.0;
+        o.refinements = 0;
+        o.inner_iters = iters[k];
         a.out[k] = o;
       }
     }
@@ -529,6 +510,8 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         o.norm_r_m = 0.0;
         o.conv = conv[k];
         o.bnorm = 0.0;
+        o.refinements = 0;
+        o.inner_iters = iters[k];
         a.out[k] = o;
       }
     }
@@ -794,6 +777,8 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
                  int32_t precision, cudaStream_t st, sfr_solve_info *info) {
   if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
+  if (precision == SFR_MIXED)
+    return solve_mixed(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);
   if (precision != SFR_FP64) return SFR_UNSUPPORTED;
   SolveOut out[kMaxK];
   float ms = 0.f;
