@@ -73,10 +73,10 @@ def test_mixed_multi_rhs_per_component_diagonal(cuda):
         assert infos[k].status == sv.OK
         r = s.b[k] - O.matvec(O.CSRD, True, s.ia, s.ja, s.al, ad_k[k], xs[k])
         assert np.linalg.norm(r) < TOL * np.linalg.norm(s.b[k])
-        x1, i1 = g.solve(sv.PBICGSTAB, s.b[k], tol=TOL, precision=sv.MIXED) \
-            if k == 0 else (None, None)
-    # K=1 with the shared diagonal equals the first component
-    assert np.array_equal(x1, xs[0])
+    # the single-RHS solve of the first component (shared diagonal = ad_k[0])
+    x1, i1 = g.solve(sv.PBICGSTAB, s.b[0], tol=TOL, precision=sv.MIXED)
+    assert i1.status == sv.OK
+    assert rel(x1, xs[0]) < 1e-8
 
 
 def test_mixed_iteration_cap_folds_correction(cuda):

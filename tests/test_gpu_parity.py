@@ -161,16 +161,20 @@ def test_bicgstab_steady_within_reference_spread(cuda, lname):
 
 @pytest.mark.parametrize("solver", [sv.PCG, sv.PBICGSTAB])
 def test_multi_rhs_matches_single(cuda, solver):
-    s = (S.poisson_jittered(16, seed=51) if solver == sv.PCG
-         else S.momentum(16, seed=52, nrhs=3))
+    # K right-hand sides in one launch against K single solves.  The K-RHS
+    # kernel may run a different grid (occupancy), i.e. another reduction
+    # order, so the bar is the parity bar, not bit equality.
+    s = (S.poisson_jittered(24, seed=51) if solver == sv.PCG
+         else S.momentum(24, seed=52, nrhs=3))
     b = np.stack([s.b[0], -0.5 * s.b[0] + 0.1, np.cos(np.arange(s.neq))]) \
         if solver == sv.PCG else s.b
     g, _ = gpu_system(s, "csrd_full")
     xs, infos = g.solve_multi(solver, b, tol=1e-10)
     for k in range(3):
         x1, i1 = g.solve(solver, b[k], tol=1e-10)
-        assert infos[k].iters == i1.iters
-        assert np.array_equal(xs[k], x1)
+        assert infos[k].status == sv.OK and i1.status == sv.OK
+        assert abs(infos[k].iters - i1.iters) <= 1
+        assert rel(xs[k], x1) < TOL_X
 
 
 def test_multi_rhs_per_component_diagonal(cuda):
