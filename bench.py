@@ -47,6 +47,11 @@ def parse_args(argv=None):
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--profile", choices=["none", "spmv", "solve"], default="none",
                     help="short launch sequence for ncu (no JSON line)")
+    ap.add_argument("--engine", type=int, default=0,
+                    help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
+                         "loop (profiling)")
+    ap.add_argument("--spw", type=int, default=0, help="SELL slices per warp (0: default)")
+    ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
     return ap.parse_args(argv)
 
 
@@ -171,6 +176,7 @@ def run_ours(args):
     N, nnz = s.neq, s.nnz_full
     g = sv.GpuSystem(N, s.ia, s.ja, sv.CSRD, True, device=local)
     g.set_values(s.al, s.ad)
+    g.set_engine(args.engine, 0, args.spw)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     b = torch.tensor(s.b[0], device="cuda")
@@ -186,7 +192,8 @@ def run_ours(args):
             else:
                 for _ in range(args.warmup + args.steps):
                     g.solve_device(sv.PCG, b.data_ptr(), x.data_ptr(), tol=1e-10,
-                                   maxit=args.maxit, stream=sptr)
+                                   maxit=args.maxit, stream=sptr,
+                                   precision=sv.MIXED if args.mixed else sv.FP64)
         torch.cuda.synchronize()
         return None
 

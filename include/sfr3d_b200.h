@@ -113,6 +113,18 @@ int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
                         double tol, uint32_t maxit, int32_t newx,
                         int32_t precision, sfr_solve_info *info);
 
+/* Choose how solves run: engine 0 = automatic (by size), 1 = persistent
+ * (the whole solve in one cooperative launch: lowest latency, small
+ * systems), 2 = graph (one full-occupancy kernel per phase inside a CUDA
+ * graph whose iteration loop is a device-controlled conditional node: large
+ * systems), 3 = the graph engine's kernels launched from a host loop for
+ * exactly maxit iterations (for profilers, which cannot look inside graphs
+ * with conditional nodes; finished solves make the remaining launches
+ * no-ops).  threads (128 or 256) and slices_per_warp (1..64; a SELL slice is
+ * 32 rows) set the graph engine's launch shape; 0 keeps the current value. */
+int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
+                       int32_t slices_per_warp);
+
 int sfr_gpu_destroy(sfr_system *s);
 
 /* ---- kernels for measurement and tests (device pointers) ------------- */

@@ -81,6 +81,10 @@ int ensure_transpose(sfr_system *s) {
 
 }  // namespace
 
+namespace sfr {
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+}  // namespace sfr
+
 extern "C" {
 
 const char *sfr_status_string(int status) {
@@ -227,9 +231,20 @@ int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x, dou
   return sfr_gpu_solve_multi(s, solver, 1, nullptr, b, x, tol, maxit, newx, precision, info);
 }
 
+int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads, int32_t slices_per_warp) {
+  if (!s || engine < 0 || engine > 3) return SFR_BAD_INPUT;
+  if (threads != 0 && threads != 128 && threads != 256) return SFR_BAD_INPUT;
+  if (slices_per_warp < 0 || slices_per_warp > 64) return SFR_BAD_INPUT;
+  s->engine = engine;
+  if (threads) s->graph_threads = threads;
+  if (slices_per_warp) s->graph_spw = slices_per_warp;
+  return SFR_OK;
+}
+
 int sfr_gpu_destroy(sfr_system *s) {
   if (!s) return SFR_OK;
   cudaSetDevice(s->device);
+  sfr::release_stream_engine(s);
   io_release(s);
   sfr::free_sell(&s->A);
   sfr::free_sell(&s->At);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cuda/atomic>
 #include <cstdint>
+#include <type_traits>
 
 #include "sfr3d_b200.h"
 
@@ -22,6 +23,12 @@ template <typename T>
 __device__ __forceinline__ T ld_vec(const T *p) { return __ldcg(p); }
 template <typename T>
 __device__ __forceinline__ void st_vec(T *p, T v) { __stcg(p, v); }
+// Data no thread writes while the kernel runs: a plain (L1-cached, LSU) load.
+// Neighbouring rows of a warp share most of their gathers, and for divergent
+// gathers the LSU path sustains far more requests than the non-coherent
+// read-only path (ld.global.nc).
+template <typename T>
+__device__ __forceinline__ T ld_ro(const T *p) { return *p; }
 
 // ----------------------------------------------------------------------
 // Arithmetic that rounds exactly as the reference's host code does (one
@@ -174,6 +181,50 @@ __device__ __forceinline__ double row_spmv_exact(const SellView<V> &A, int s, in
   }
   return t;
 }
+
+// y_k[row] = diag*v(row) + sum_e val_e * v(col_e) for K vectors given by a
+// gather functor g(k, col): exact FP64 (the reference's rounding) or FP32
+// with FMA.  A row's column indices and values are loaded six at a time
+// before any gather, so all of them are in flight together.
+template <int K, bool kExact, typename V, typename G>
+__device__ __forceinline__ void row_product(const int *sptr, const int *colp, const V *valp,
+                                            const V *const *diagp, int s, int lane,
+                                            const int (&act)[K], G g,
+                                            typename std::conditional<kExact, double, float>::type (&y)[K]) {
+  using T = typename std::conditional<kExact, double, float>::type;
+  const int row = s * kWarp + lane;
+  const int base = __ldg(sptr + s);
+  const int w = (__ldg(sptr + s + 1) - base) >> 5;
+  const int *c = colp + base + lane;
+  const V *v = valp + base + lane;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (act[k]) {
+      const T dv = static_cast<T>(ld_vec(diagp[k] + row));
+      y[k] = kExact ? xmul(dv, g(k, row)) : dv * g(k, row);
+    }
+  for (int e0 = 0; e0 < w; e0 += 6) {
+    int jj[6];
+    T vv[6];
+#pragma unroll
+    for (int u = 0; u < 6; ++u)
+      if (e0 + u < w) {
+        jj[u] = ld_stream(c + (e0 + u) * kWarp);
+        vv[u] = static_cast<T>(ld_stream(v + (e0 + u) * kWarp));
+      }
+#pragma unroll
+    for (int u = 0; u < 6; ++u)
+      if (e0 + u < w) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (act[k]) {
+            const T gv = g(k, jj[u]);
+            y[k] = kExact ? xadd(y[k], xmul(vv[u], gv)) : fmaf(vv[u], gv, y[k]);
+          }
+      }
+  }
+}
+
 
 // Block-contiguous slice range of this block.
 __device__ __forceinline__ void block_slices(int nslices, int *first, int *last) {

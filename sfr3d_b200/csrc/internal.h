@@ -70,6 +70,11 @@ struct sfr_system {
   bool values_set = false;
   cudaStream_t stream = nullptr;
   sfr::Workspace ws;
+  // engine: 0 auto, 1 persistent (one cooperative launch), 2 graph,
+  // 3 the graph engine's kernels from a host loop (profiling)
+  int32_t engine = 0;
+  int32_t graph_threads = 256;   // graph engine launch shape
+  int32_t graph_spw = 4;         // SELL slices per warp
   int64_t bytes = 0;
 };
 
@@ -89,6 +94,13 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
 int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                 const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
                 cudaStream_t st, sfr_solve_info *info);
+// Graph engine (stream_solve.cu)
+int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
+                 const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
+                 int32_t precision, double delta, int threads, int spw, bool loop,
+                 cudaStream_t st, sfr_solve_info *info);
+void release_stream_engine(const sfr_system *s);
+double reliable_delta();
 int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag,
                 const double *d_x, double *d_y, double *d_dot, cudaStream_t st);
 int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
@@ -97,4 +109,6 @@ int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
 int dot_host(const double *d_a, const double *d_b, int32_t n, double *h_out,
              cudaStream_t st);
 int num_sms(int device);
+// Text for sfr_last_error() (capi.cpp)
+void set_last_error(const char *msg);
 }  // namespace sfr

@@ -524,11 +524,17 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) spmv_kernel(SellView<double> A, const double *x,
                                                    double *y) {
+  const int n = A.n;
   const int lane = threadIdx.x & 31;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += nw) {
-    const int row = s * kWarp + lane;
-    if (row < A.n) y[row] = row_spmv_exact(A, s, lane, x);
+  int s0, s1;
+  block_slices(A.nslices, &s0, &s1);
+  const double *diag[1] = {A.diag};
+  const int act[1] = {1};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double yv[1];
+    row_product<1, true, double>(A.sptr, A.col, A.val, diag, s_, lane, act,
+                                 [&](int, int c) { return x[c]; }, yv);
+    y[row_] = yv[0];
   }
 }
 
@@ -595,6 +601,8 @@ int num_sms(int device) {
 namespace {
 
 constexpr int kStatGrid = 4 * 148;  // standalone kernels: 4 blocks per SM
+// automatic engine choice: the graph engine from this many rows up
+constexpr int kGraphEngineRows = 100000;
 
 struct Scratch {  // per-device scratch for the standalone reductions
   double *part = nullptr;
@@ -642,7 +650,11 @@ int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag, const dou
   SellView<double> v{A.n, A.nslices, A.sptr, A.col, A.val, d_diag};
   const int grid = grid_for_slices(A.nslices, s->device);
   if (!d_dot) {
-    spmv_kernel<<<grid, 256, 0, st>>>(v, d_x, d_y);
+    // the graph engine's launch shape: 8 warps per block, graph_spw slices
+    // per warp, block-contiguous slice ranges
+    const int spw = std::max(1, s->graph_spw);
+    const int g2 = std::max(1, (A.nslices + 8 * spw - 1) / (8 * spw));
+    spmv_kernel<<<g2, 256, 0, st>>>(v, d_x, d_y);
   } else {
     Scratch *sc = nullptr;
     int rc = scratch_for(s->device, &sc);
@@ -777,6 +789,12 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
                  int32_t precision, cudaStream_t st, sfr_solve_info *info) {
   if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
+  int engine = s->engine;
+  if (engine == 0) engine = s->n >= kGraphEngineRows ? 2 : 1;
+  if (engine == 2 || engine == 3)
+    return solve_stream(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, precision,
+                        reliable_delta(), s->graph_threads, s->graph_spw, engine == 3, st,
+                        info);
   if (precision == SFR_MIXED)
     return solve_mixed(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);
   if (precision != SFR_FP64) return SFR_UNSUPPORTED;

@@ -749,6 +749,7 @@ int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k
 }
 
 void set_reliable_delta(double delta) { g_delta = delta; }
+double reliable_delta() { return g_delta; }
 
 }  // namespace sfr
 

@@ -1,0 +1,1445 @@
+// Graph engine: a Krylov solve as one CUDA graph whose iteration loop is a
+// device-controlled conditional WHILE node.
+//
+// Each phase of an iteration is its own full-occupancy kernel (one warp per
+// SELL slice, a thread per row), so every row's loads are in flight at once;
+// a phase's dot products end in the last block to finish, which sums the
+// block partials in a fixed order (deterministic), updates the Krylov scalars
+// in device memory and, from the last phase, sets the WHILE condition to 0
+// once every right-hand side has stopped.  The host launches the graph and
+// reads the result once: no per-iteration round trip.
+//
+// Loads: vectors are read with plain L1-cached loads (a warp's rows share
+// most of their gathers); the matrix streams with evict-first.
+// (The persistent engine cannot do this: other blocks rewrite its vectors
+// during the launch, so it reads them from L2.)
+//
+// The persistent engine (krylov.cu, mixed.cu) suits small systems where
+// launch latency dominates; this engine suits large ones.  Both follow the
+// same arithmetic: FP64 rows and updates bit-identical to the reference
+// (Cg.c, Bicgstab.c, HccaBlas.c), or FP32 inner iterations with FP64
+// reliable updates (the true residual and x in FP64; the update kernels sit in
+// a conditional IF node that runs only when a refinement is due).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+#include "persist.cuh"
+
+namespace sfr {
+
+namespace {
+
+constexpr int kCounters = 16;
+
+template <int K>
+struct SArgs {  // passed by value: every pointer is fixed for the graph's life
+  int n, nslices, npairs;
+  const int *sptr, *col;
+  const double *val64;
+  const float *val32;
+  // the graph's own padded workspace (rows padded to a multiple of 4)
+  double *diag64[K], *b[K], *x[K];
+  double *m[K], *r[K], *z[K], *q[K], *p0[K], *p1[K], *r0[K], *t[K];
+  float *d32[K], *m32[K], *fr[K], *fz[K], *fq[K], *fp0[K], *fp1[K], *fxs[K], *fr0[K], *ft[K];
+  double *part;
+  unsigned *counter;
+  cudaGraphConditionalHandle hwhile, hif, hif2;
+  int in_graph;  // 0: plain launch loop (profiling): no conditional handles
+};
+
+// Per-call scalars, copied into the state before each launch.
+struct SCall {
+  double tol, delta;
+  unsigned maxit;
+  int newx;
+};
+
+template <int K>
+struct SState {
+  SCall call;
+  double d[K], alpha[K], beta[K], omega[K], rr0[K], conv[K], bnorm[K], rmax[K];
+  int active[K], iters[K], status[K], refine[K], upd[K];
+  int any, any_upd;
+  unsigned j;
+  SolveOut out[K];
+};
+
+// Vector phases run over row pairs (r, r+1) with 16-byte (FP64) / 8-byte
+// (FP32) loads; every workspace vector is padded, so the pair is in bounds.
+#define SFR_FOR_PAIRS(i)                                                        \
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.npairs;             \
+       i += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ double2 ld2ro(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ float2 ld2ro(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
+__device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+
+// Totals of NV values over `G` block partials, fixed order, all threads of
+// the (last) block.  Result in sm[0..NV).
+template <int NV>
+__device__ __forceinline__ void block_totals(const double *part, int G, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double s[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    s[v] = 0.0;
+    for (int b = threadIdx.x; b < G; b += blockDim.x) s[v] += ld_vec(part + v * G + b);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = warp_sum(s[v]);
+    if (lane == 0) sm[32 + v * 32 + warp] = w;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double w = lane < nw ? sm[32 + v * 32 + lane] : 0.0;
+      w = warp_sum(w);
+      if (lane == 0) sm[v] = w;
+    }
+  }
+  __syncthreads();
+}
+
+// Block partials -> counter; true in the last block, with the totals in
+// sm[0..NV) for every thread of that block.  The counter is reset there.
+template <int NV>
+__device__ __forceinline__ bool last_block(const double (&acc)[NV], double *part,
+                                           unsigned *counter, double *sm) {
+  __shared__ bool s_last;
+  block_partials<NV>(acc, part, gridDim.x, sm + 32 + NV * 32);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  block_totals<NV>(part, gridDim.x, sm);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+#define SFR_SHARED_RED(NV) __shared__ double sm[32 + 2 * (NV) * 32]
+
+template <int K>
+__device__ __forceinline__ void load_active(const SState<K> *st, int (&act)[K]) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) act[k] = st->active[k];
+}
+
+// ============================= PCG =======================================
+
+// setup: m (and FP32 d/m), x0, (b, M^-1 b), (b, b)
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_setup(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  const int n = a.n;
+  const int newx = st->call.newx;
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const bool two = r + 1 < n;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double2 dk = ld2ro(a.diag64[k] + r);
+      const double2 mk = make_double2(1.0 / dk.x, 1.0 / dk.y);
+      if (kMixed) {
+        st2(a.d32[k] + r, make_float2(__double2float_rn(dk.x), __double2float_rn(dk.y)));
+        st2(a.m32[k] + r, make_float2(__double2float_rn(mk.x), __double2float_rn(mk.y)));
+      } else {
+        st2(a.m[k] + r, mk);
+      }
+      if (newx) st2(a.x[k] + r, make_double2(0.0, 0.0));
+      const double2 bk = ld2ro(a.b[k] + r);
+      acc[2 * k] += bk.x * xmul(bk.x, mk.x);
+      acc[2 * k + 1] += bk.x * bk.x;
+      if (two) {
+        acc[2 * k] += bk.y * xmul(bk.y, mk.y);
+        acc[2 * k + 1] += bk.y * bk.y;
+      }
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 0, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->conv[k] = st->call.tol * sqrt(fabs(sm[2 * k]));
+      st->bnorm[k] = sqrt(sm[2 * k + 1]);
+      st->active[k] = 1;
+      st->iters[k] = 0;
+      st->status[k] = SFR_OK;
+      st->refine[k] = 0;
+      st->upd[k] = 0;
+      st->beta[k] = 0.0;
+    }
+    st->j = 0;
+    st->any = 1;
+    st->any_upd = 0;
+  }
+}
+
+// PCG start: r = b - A x, z = M r, p = z, d = (r, z)  (FP64: Cg.c:84-102)
+// mixed: the same in FP64 for the true residual, then r, z, p in FP32.
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_pcg_start(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int all[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) all[k] = 1;
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[K];
+    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double rk = xsub(ld_ro(a.b[k] + row_), y[k]);
+      if (kMixed) {
+        const float rs = __double2float_rn(rk);
+        const float zs = ld_ro(a.m32[k] + row_) * rs;
+        st_vec(a.fr[k] + row_, rs);
+        st_vec(a.fz[k] + row_, zs);
+        st_vec(a.fp0[k] + row_, zs);
+        st_vec(a.fxs[k] + row_, 0.0f);
+        acc[2 * k] += rk * (rk / ld_ro(a.diag64[k] + row_));
+        acc[2 * k + 1] += static_cast<double>(rs) * static_cast<double>(zs);
+      } else {
+        const double zk = xmul(rk, ld_ro(a.m[k] + row_));
+        st_vec(a.r[k] + row_, rk);
+        st_vec(a.z[k] + row_, zk);
+        st_vec(a.p0[k] + row_, zk);
+        acc[2 * k + 1] += rk * zk;
+      }
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 1, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->d[k] = sm[2 * k + 1];
+      st->rmax[k] = sqrt(fabs(sm[2 * k]));
+    }
+  }
+}
+
+// phase A: q = A p, (q, p)  (Cg.c:105-109)
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(K);
+  if (!st->any) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int act[K];
+  load_active<K>(st, act);
+  const unsigned j = st->j;
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  if (!kMixed) {
+    SFR_FOR_OWN_ROWS(s0, s1) {
+      double y[K];
+      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.p0[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.q[k] + row_, y[k]);
+        acc[k] += y[k] * ld_ro(a.p0[k] + row_);
+      }
+    }
+  } else {
+    const float *const *d32 = a.d32;
+    SFR_FOR_OWN_ROWS(s0, s1) {
+      float y[K];
+      row_product<K, false, float>(a.sptr, a.col, a.val32, d32, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.fp0[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.fq[k] + row_, y[k]);
+        acc[k] += static_cast<double>(y[k]) * static_cast<double>(ld_ro(a.fp0[k] + row_));
+      }
+    }
+  }
+  if (!last_block<K>(acc, a.part, a.counter + 2, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      const double al = st->d[k] / sm[k];
+      st->alpha[k] = al;
+      if (!isfinite(al)) {
+        st->active[k] = 0;
+        st->status[k] = SFR_BREAKDOWN;
+        st->iters[k] = j + 1;
+      }
+    }
+  }
+}
+
+// phase B: x (or xs) += alpha p ; r -= alpha q ; z = M r ; (r, z) ; test
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_pcg_b(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(K);
+  if (!st->any) return;
+  const int n = a.n;
+  int act[K];
+  load_active<K>(st, act);
+  const unsigned j = st->j;
+  double acc[K], al[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    acc[k] = 0.0;
+    al[k] = st->alpha[k];
+  }
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const bool two = r + 1 < n;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      if (!kMixed) {
+        const double2 p = ld2ro(a.p0[k] + r), q = ld2ro(a.q[k] + r), m = ld2ro(a.m[k] + r);
+        double2 xv = ld2(a.x[k] + r), rv = ld2(a.r[k] + r), zv;
+        xv.x = xadd(xv.x, xmul(al[k], p.x));
+        xv.y = xadd(xv.y, xmul(al[k], p.y));
+        rv.x = xsub(rv.x, xmul(al[k], q.x));
+        rv.y = xsub(rv.y, xmul(al[k], q.y));
+        zv.x = xmul(rv.x, m.x);
+        zv.y = xmul(rv.y, m.y);
+        st2(a.x[k] + r, xv);
+        st2(a.r[k] + r, rv);
+        st2(a.z[k] + r, zv);
+        acc[k] += rv.x * zv.x;
+        if (two) acc[k] += rv.y * zv.y;
+      } else {
+        const float af = static_cast<float>(al[k]);
+        const float2 p = ld2ro(a.fp0[k] + r), q = ld2ro(a.fq[k] + r), m = ld2ro(a.m32[k] + r);
+        float2 xs = ld2(a.fxs[k] + r), rv = ld2(a.fr[k] + r), zv;
+        xs.x = fmaf(af, p.x, xs.x);
+        xs.y = fmaf(af, p.y, xs.y);
+        rv.x = fmaf(-af, q.x, rv.x);
+        rv.y = fmaf(-af, q.y, rv.y);
+        zv.x = m.x * rv.x;
+        zv.y = m.y * rv.y;
+        st2(a.fxs[k] + r, xs);
+        st2(a.fr[k] + r, rv);
+        st2(a.fz[k] + r, zv);
+        acc[k] += static_cast<double>(rv.x) * static_cast<double>(zv.x);
+        if (two) acc[k] += static_cast<double>(rv.y) * static_cast<double>(zv.y);
+      }
+    }
+  }
+  if (!last_block<K>(acc, a.part, a.counter + 3, sm)) return;
+  if (threadIdx.x == 0) {
+    int any = 0, any_upd = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->upd[k] = 0;
+      if (!act[k]) continue;
+      const double di = sm[k];
+      if (!kMixed) {
+        st->beta[k] = di / st->d[k];
+        st->d[k] = di;
+        if (sqrt(fabs(di)) < st->conv[k]) {
+          st->active[k] = 0;
+          st->iters[k] = j + 1;
+        } else if (!isfinite(st->beta[k])) {
+          st->active[k] = 0;
+          st->status[k] = SFR_BREAKDOWN;
+          st->iters[k] = j + 1;
+        }
+      } else {
+        const double est = sqrt(fabs(di));
+        if (!isfinite(di)) {
+          st->active[k] = 0;
+          st->status[k] = SFR_BREAKDOWN;
+          st->iters[k] = j + 1;
+        } else if (est < st->call.delta * st->rmax[k] || est < st->conv[k]) {
+          st->upd[k] = 1;
+          any_upd = 1;
+        } else {
+          st->beta[k] = di / st->d[k];
+          st->d[k] = di;
+        }
+      }
+      if (st->active[k] && !st->upd[k] && j + 1 >= st->call.maxit) {
+        st->active[k] = 0;
+        st->status[k] = SFR_MAXIT;
+        st->iters[k] = j + 2;
+      }
+      any |= st->active[k];
+    }
+    st->j = j + 1;
+    st->any = any;
+    st->any_upd = any_upd;
+    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif, any_upd ? 1u : 0u);
+    if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// phase C: p = z + beta p  (Cg.c:139-141), in place
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) {
+  if (!st->any) return;
+  int act[K];
+  load_active<K>(st, act);
+  double bv[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) bv[k] = st->beta[k];
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      if (!kMixed) {
+        const double2 zv = ld2ro(a.z[k] + r);
+        double2 p = ld2(a.p0[k] + r);
+        p.x = xadd(zv.x, xmul(bv[k], p.x));
+        p.y = xadd(zv.y, xmul(bv[k], p.y));
+        st2(a.p0[k] + r, p);
+      } else {
+        const float bf = static_cast<float>(bv[k]);
+        const float2 zv = ld2ro(a.fz[k] + r);
+        float2 p = ld2(a.fp0[k] + r);
+        p.x = fmaf(bf, p.x, zv.x);
+        p.y = fmaf(bf, p.y, zv.y);
+        st2(a.fp0[k] + r, p);
+      }
+    }
+  }
+}
+
+// reliable update, part 1: x += xs (FP64) for the flagged right-hand sides
+template <int K>
+__global__ void __launch_bounds__(256) k_fold(const SArgs<K> a, SState<K> *st, int all) {
+  if (!all && !st->any_upd) return;
+  int sel[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) sel[k] = all ? 1 : st->upd[k];
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!sel[k]) continue;
+      double2 xv = ld2(a.x[k] + r);
+      const float2 xs = ld2(a.fxs[k] + r);
+      xv.x += static_cast<double>(xs.x);
+      xv.y += static_cast<double>(xs.y);
+      st2(a.x[k] + r, xv);
+      if (all) st2(a.fxs[k] + r, make_float2(0.f, 0.f));
+    }
+  }
+}
+
+// reliable update, part 2 (PCG): r_true = b - A x in FP64, r = fl32(r_true),
+// z = M r, xs = 0; decide on the true residual.
+template <int K>
+__global__ void __launch_bounds__(256) k_pcg_refresh(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  if (!st->any_upd) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int sel[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) sel[k] = st->upd[k];
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[K];
+    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, sel,
+                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!sel[k]) continue;
+      const double rt = ld_ro(a.b[k] + row_) - y[k];
+      const float rs = __double2float_rn(rt);
+      const float zs = ld_ro(a.m32[k] + row_) * rs;
+      st_vec(a.fr[k] + row_, rs);
+      st_vec(a.fz[k] + row_, zs);
+      st_vec(a.fxs[k] + row_, 0.0f);
+      acc[2 * k] += rt * (rt / ld_ro(a.diag64[k] + row_));
+      acc[2 * k + 1] += static_cast<double>(rs) * static_cast<double>(zs);
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 4, sm)) return;
+  if (threadIdx.x == 0) {
+    const unsigned j = st->j;  // already advanced by phase B
+    int any = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (sel[k]) {
+        st->refine[k] += 1;
+        st->upd[k] = 0;
+        const double tr = sqrt(fabs(sm[2 * k]));
+        if (tr < st->conv[k]) {
+          st->active[k] = 0;
+          st->iters[k] = j;
+        } else {
+          st->beta[k] = sm[2 * k + 1] / st->d[k];
+          st->d[k] = sm[2 * k + 1];
+          st->rmax[k] = tr;
+          if (j >= st->call.maxit) {
+            st->active[k] = 0;
+            st->status[k] = SFR_MAXIT;
+            st->iters[k] = j + 1;
+          }
+        }
+      }
+      any |= st->active[k];
+    }
+    st->any = any;
+    st->any_upd = 0;
+    if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// post-processing: xKx, ||x||, ||b - Ax||_M, ||b - Ax|| (Cg.c:155-176)
+template <int K>
+__global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(4 * K);
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int all[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) all[k] = 1;
+  double acc[4 * K];
+#pragma unroll
+  for (int v = 0; v < 4 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[K];
+    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double xk = ld_ro(a.x[k] + row_);
+      const double rk = xsub(ld_ro(a.b[k] + row_), y[k]);
+      const double dk = ld_ro(a.diag64[k] + row_);
+      acc[4 * k + 0] += xk * y[k];
+      acc[4 * k + 1] += xk * xk;
+      acc[4 * k + 2] += rk * xmul(rk, 1.0 / dk);
+      acc[4 * k + 3] += rk * rk;
+    }
+  }
+  if (!last_block<4 * K>(acc, a.part, a.counter + 7, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      SolveOut o;
+      o.iters = st->iters[k];
+      o.status = st->status[k];
+      o.xKx = sm[4 * k];
+      o.norm_x = sqrt(sm[4 * k + 1]);
+      o.norm_r_m = sqrt(fabs(sm[4 * k + 2]));
+      o.norm_r = sqrt(sm[4 * k + 3]);
+      o.conv = st->conv[k];
+      o.bnorm = st->bnorm[k];
+      o.refinements = st->refine[k];
+      o.inner_iters = st->iters[k];
+      st->out[k] = o;
+    }
+  }
+}
+
+// =========================== BiCGSTAB ====================================
+// FP64: Bicgstab.c:50-245.  Vectors: r0 shadow, p (p0), z = M p or M s,
+// v (q), t.  Mixed: the same in FP32 with xs and reliable updates.
+
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int all[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) all[k] = 1;
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[K];
+    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double rk = xsub(ld_ro(a.b[k] + row_), y[k]);
+      if (kMixed) {
+        const float rs = __double2float_rn(rk);
+        st_vec(a.fr0[k] + row_, rs);
+        st_vec(a.fp0[k] + row_, rs);
+        st_vec(a.fr[k] + row_, rs);
+        st_vec(a.fz[k] + row_, ld_ro(a.m32[k] + row_) * rs);
+        st_vec(a.fxs[k] + row_, 0.0f);
+      } else {
+        st_vec(a.r0[k] + row_, rk);
+        st_vec(a.p0[k] + row_, rk);
+        st_vec(a.r[k] + row_, rk);
+        st_vec(a.z[k] + row_, xmul(rk, ld_ro(a.m[k] + row_)));
+      }
+      acc[2 * k] += rk * rk;
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 1, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->rmax[k] = sqrt(sm[2 * k]);
+      st->conv[k] = st->call.tol * st->bnorm[k];  // ||r|| < tol ||b|| (Bicgstab.c:72-80)
+    }
+  }
+}
+
+// A1: v = A z ; rr0 = (r, r0) ; alpha = rr0 / (v, r0)
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  if (!st->any) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int act[K];
+  load_active<K>(st, act);
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    if (!kMixed) {
+      double y[K];
+      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.q[k] + row_, y[k]);
+        const double r0k = ld_ro(a.r0[k] + row_);
+        acc[2 * k] += ld_ro(a.r[k] + row_) * r0k;
+        acc[2 * k + 1] += y[k] * r0k;
+      }
+    } else {
+      float y[K];
+      row_product<K, false, float>(a.sptr, a.col, a.val32, a.d32, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.fq[k] + row_, y[k]);
+        const double r0k = ld_ro(a.fr0[k] + row_);
+        acc[2 * k] += static_cast<double>(ld_ro(a.fr[k] + row_)) * r0k;
+        acc[2 * k + 1] += static_cast<double>(y[k]) * r0k;
+      }
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 2, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      st->rr0[k] = sm[2 * k];
+      st->alpha[k] = sm[2 * k] / sm[2 * k + 1];
+      if (!isfinite(st->alpha[k])) {
+        st->active[k] = 0;
+        st->status[k] = SFR_BREAKDOWN;
+        st->iters[k] = st->j + 1;
+      }
+    }
+  }
+}
+
+// B1: x += alpha z ; s = r -= alpha v ; z = M s ; (s, s) ; half-step test
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_b1(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(K);
+  if (!st->any) return;
+  const int n = a.n;
+  int act[K];
+  load_active<K>(st, act);
+  double acc[K], alv[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    acc[k] = 0.0;
+    alv[k] = st->alpha[k];
+  }
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const bool two = r + 1 < n;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      if (!kMixed) {
+        const double al = alv[k];
+        const double2 zv = ld2(a.z[k] + r), q = ld2ro(a.q[k] + r), m = ld2ro(a.m[k] + r);
+        double2 xv = ld2(a.x[k] + r), rv = ld2(a.r[k] + r);
+        xv.x = xadd(xv.x, xmul(al, zv.x));
+        xv.y = xadd(xv.y, xmul(al, zv.y));
+        rv.x = xsub(rv.x, xmul(al, q.x));
+        rv.y = xsub(rv.y, xmul(al, q.y));
+        st2(a.x[k] + r, xv);
+        st2(a.r[k] + r, rv);
+        st2(a.z[k] + r, make_double2(xmul(rv.x, m.x), xmul(rv.y, m.y)));
+        acc[k] += rv.x * rv.x;
+        if (two) acc[k] += rv.y * rv.y;
+      } else {
+        const float af = static_cast<float>(alv[k]);
+        const float2 zv = ld2(a.fz[k] + r), q = ld2ro(a.fq[k] + r), m = ld2ro(a.m32[k] + r);
+        float2 xs = ld2(a.fxs[k] + r), rv = ld2(a.fr[k] + r);
+        xs.x = fmaf(af, zv.x, xs.x);
+        xs.y = fmaf(af, zv.y, xs.y);
+        rv.x = fmaf(-af, q.x, rv.x);
+        rv.y = fmaf(-af, q.y, rv.y);
+        st2(a.fxs[k] + r, xs);
+        st2(a.fr[k] + r, rv);
+        st2(a.fz[k] + r, make_float2(m.x * rv.x, m.y * rv.y));
+        acc[k] += static_cast<double>(rv.x) * static_cast<double>(rv.x);
+        if (two) acc[k] += static_cast<double>(rv.y) * static_cast<double>(rv.y);
+      }
+    }
+  }
+  if (!last_block<K>(acc, a.part, a.counter + 3, sm)) return;
+  if (threadIdx.x == 0) {
+    int any = 0, any_upd = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->upd[k] = 0;
+      if (!act[k]) continue;
+      if (sqrt(sm[k]) < st->conv[k]) {
+        if (kMixed) {
+          st->upd[k] = 1;  // confirm on the FP64 true residual
+          any_upd = 1;
+        } else {
+          st->active[k] = 0;
+          st->iters[k] = st->j + 1;
+        }
+      }
+      any |= st->active[k];
+    }
+    st->any = any;
+    st->any_upd = any_upd;
+    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif, any_upd ? 1u : 0u);
+    if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// reliable update (BiCGSTAB): r_true = b - A x, r = fl32(r_true), z = M r,
+// xs = 0; ||r_true||; (r, r0).  `stage` 1 = after the half step, 2 = after
+// the full step (phase B2 already computed beta; it is recomputed with the
+// new (r, r0)).
+template <int K>
+__global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K> *st,
+                                                      int stage) {
+  SFR_SHARED_RED(2 * K);
+  if (!st->any_upd) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int sel[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) sel[k] = st->upd[k];
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[K];
+    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, sel,
+                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!sel[k]) continue;
+      const double rt = ld_ro(a.b[k] + row_) - y[k];
+      const float rs = __double2float_rn(rt);
+      st_vec(a.fr[k] + row_, rs);
+      st_vec(a.fz[k] + row_, ld_ro(a.m32[k] + row_) * rs);
+      st_vec(a.fxs[k] + row_, 0.0f);
+      acc[2 * k] += rt * rt;
+      acc[2 * k + 1] += static_cast<double>(rs) * static_cast<double>(ld_ro(a.fr0[k] + row_));
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 4, sm)) return;
+  if (threadIdx.x == 0) {
+    const unsigned j = st->j;
+    int any = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (sel[k]) {
+        st->refine[k] += 1;
+        st->upd[k] = 0;
+        const double tr = sqrt(sm[2 * k]);
+        if (tr < st->conv[k]) {
+          st->active[k] = 0;
+          st->iters[k] = stage == 1 ? j + 1 : j;
+        } else {
+          st->rmax[k] = tr;
+          if (stage == 2) {
+            st->beta[k] = (sm[2 * k + 1] / st->rr0[k]) * (st->alpha[k] / st->omega[k]);
+            if (j >= st->call.maxit) {
+              st->active[k] = 0;
+              st->status[k] = SFR_MAXIT;
+              st->iters[k] = j + 1;
+            }
+          }
+        }
+      }
+      any |= st->active[k];
+    }
+    st->any = any;
+    st->any_upd = 0;
+    if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// A2: t = A z ; w = (t, s) / (t, t)
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  if (!st->any) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  int act[K];
+  load_active<K>(st, act);
+  double acc[2 * K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    if (!kMixed) {
+      double y[K];
+      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.t[k] + row_, y[k]);
+        acc[2 * k] += y[k] * ld_ro(a.r[k] + row_);
+        acc[2 * k + 1] += y[k] * y[k];
+      }
+    } else {
+      float y[K];
+      row_product<K, false, float>(a.sptr, a.col, a.val32, a.d32, s_, lane, act,
+                                   [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (!act[k]) continue;
+        st_vec(a.ft[k] + row_, y[k]);
+        acc[2 * k] += static_cast<double>(y[k]) * static_cast<double>(ld_ro(a.fr[k] + row_));
+        acc[2 * k + 1] += static_cast<double>(y[k]) * static_cast<double>(y[k]);
+      }
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 5, sm)) return;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      st->omega[k] = sm[2 * k] / sm[2 * k + 1];
+      if (!isfinite(st->omega[k])) {
+        st->active[k] = 0;
+        st->status[k] = SFR_BREAKDOWN;
+        st->iters[k] = st->j + 1;
+      }
+    }
+  }
+}
+
+// B2: x += w z ; r -= w t ; (r, r), (r, r0) ; full-step test, beta
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_b2(const SArgs<K> a, SState<K> *st) {
+  SFR_SHARED_RED(2 * K);
+  if (!st->any) return;
+  const int n = a.n;
+  int act[K];
+  load_active<K>(st, act);
+  double acc[2 * K], omv[K];
+#pragma unroll
+  for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) omv[k] = st->omega[k];
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const bool two = r + 1 < n;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      if (!kMixed) {
+        const double w = omv[k];
+        const double2 zv = ld2ro(a.z[k] + r), tv = ld2ro(a.t[k] + r), r0 = ld2ro(a.r0[k] + r);
+        double2 xv = ld2(a.x[k] + r), rv = ld2(a.r[k] + r);
+        xv.x = xadd(xv.x, xmul(w, zv.x));
+        xv.y = xadd(xv.y, xmul(w, zv.y));
+        rv.x = xsub(rv.x, xmul(w, tv.x));
+        rv.y = xsub(rv.y, xmul(w, tv.y));
+        st2(a.x[k] + r, xv);
+        st2(a.r[k] + r, rv);
+        acc[2 * k] += rv.x * rv.x;
+        acc[2 * k + 1] += rv.x * r0.x;
+        if (two) {
+          acc[2 * k] += rv.y * rv.y;
+          acc[2 * k + 1] += rv.y * r0.y;
+        }
+      } else {
+        const float wf = static_cast<float>(omv[k]);
+        const float2 zv = ld2ro(a.fz[k] + r), tv = ld2ro(a.ft[k] + r), r0 = ld2ro(a.fr0[k] + r);
+        float2 xs = ld2(a.fxs[k] + r), rv = ld2(a.fr[k] + r);
+        xs.x = fmaf(wf, zv.x, xs.x);
+        xs.y = fmaf(wf, zv.y, xs.y);
+        rv.x = fmaf(-wf, tv.x, rv.x);
+        rv.y = fmaf(-wf, tv.y, rv.y);
+        st2(a.fxs[k] + r, xs);
+        st2(a.fr[k] + r, rv);
+        acc[2 * k] += static_cast<double>(rv.x) * static_cast<double>(rv.x);
+        acc[2 * k + 1] += static_cast<double>(rv.x) * static_cast<double>(r0.x);
+        if (two) {
+          acc[2 * k] += static_cast<double>(rv.y) * static_cast<double>(rv.y);
+          acc[2 * k + 1] += static_cast<double>(rv.y) * static_cast<double>(r0.y);
+        }
+      }
+    }
+  }
+  if (!last_block<2 * K>(acc, a.part, a.counter + 6, sm)) return;
+  if (threadIdx.x == 0) {
+    const unsigned j = st->j;
+    int any = 0, any_upd = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      st->upd[k] = 0;
+      if (!act[k]) continue;
+      const double est = sqrt(sm[2 * k]);
+      st->beta[k] = (sm[2 * k + 1] / st->rr0[k]) * (st->alpha[k] / st->omega[k]);
+      if (!kMixed) {
+        if (est < st->conv[k]) {
+          st->active[k] = 0;
+          st->iters[k] = j + 1;
+        }
+      } else if (est < st->conv[k] || est < st->call.delta * st->rmax[k]) {
+        st->upd[k] = 1;
+        any_upd = 1;
+      }
+      if (st->active[k] && !st->upd[k]) {
+        if (!isfinite(st->beta[k])) {
+          st->active[k] = 0;
+          st->status[k] = SFR_BREAKDOWN;
+          st->iters[k] = j + 1;
+        } else if (j + 1 >= st->call.maxit) {
+          st->active[k] = 0;
+          st->status[k] = SFR_MAXIT;
+          st->iters[k] = j + 2;
+        }
+      }
+      any |= st->active[k];
+    }
+    st->j = j + 1;
+    st->any = any;
+    st->any_upd = any_upd;
+    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif2, any_upd ? 1u : 0u);
+    if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// C: p = r + beta (p - w v) ; z = M p
+template <int K, bool kMixed>
+__global__ void __launch_bounds__(256) k_bicg_c(const SArgs<K> a, SState<K> *st) {
+  if (!st->any) return;
+  int act[K];
+  load_active<K>(st, act);
+  double bv[K], wv[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    bv[k] = st->beta[k];
+    wv[k] = st->omega[k];
+  }
+  SFR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!act[k]) continue;
+      if (!kMixed) {
+        const double2 rv = ld2ro(a.r[k] + r), q = ld2ro(a.q[k] + r), m = ld2ro(a.m[k] + r);
+        double2 p = ld2(a.p0[k] + r);
+        p.x = xadd(rv.x, xmul(bv[k], xsub(p.x, xmul(wv[k], q.x))));
+        p.y = xadd(rv.y, xmul(bv[k], xsub(p.y, xmul(wv[k], q.y))));
+        st2(a.p0[k] + r, p);
+        st2(a.z[k] + r, make_double2(xmul(p.x, m.x), xmul(p.y, m.y)));
+      } else {
+        const float bf = static_cast<float>(bv[k]);
+        const float wf = static_cast<float>(wv[k]);
+        const float2 rv = ld2ro(a.fr[k] + r), q = ld2ro(a.fq[k] + r), m = ld2ro(a.m32[k] + r);
+        float2 p = ld2(a.fp0[k] + r);
+        p.x = fmaf(bf, fmaf(-wf, q.x, p.x), rv.x);
+        p.y = fmaf(bf, fmaf(-wf, q.y, p.y), rv.y);
+        st2(a.fp0[k] + r, p);
+        st2(a.fz[k] + r, make_float2(m.x * p.x, m.y * p.y));
+      }
+    }
+  }
+}
+
+// ============================ host ======================================
+
+struct GraphKey {
+  int solver, k, precision, threads, spw;
+  bool operator<(const GraphKey &o) const {
+    return std::tie(solver, k, precision, threads, spw) <
+           std::tie(o.solver, o.k, o.precision, o.threads, o.spw);
+  }
+};
+
+// One instantiated graph with everything it touches: its own padded
+// workspace, partials, counters, state and the by-value kernel arguments.
+struct CachedGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void *d_state = nullptr;  // SState<K>
+  void *ws = nullptr;       // padded vectors
+  double *part = nullptr;
+  unsigned *counter = nullptr;
+  std::vector<char> args;   // SArgs<K> (host copy, also baked into the nodes)
+  cudaGraphConditionalHandle hwhile = 0, hif = 0, hif2 = 0;
+  int grid_s = 0, grid_v = 0, threads = 256;
+  uint64_t last_use = 0;
+  int64_t bytes = 0;
+};
+
+struct EngineCache {
+  std::map<GraphKey, std::unique_ptr<CachedGraph>> graphs;
+  uint64_t clock = 0;
+};
+std::map<const sfr_system *, EngineCache> g_engines;
+constexpr size_t kMaxGraphsPerSystem = 4;
+
+cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t *prev, void *func, int grid, int threads,
+                       void **params) {
+  cudaKernelNodeParams p{};
+  p.func = func;
+  p.gridDim = dim3(grid);
+  p.blockDim = dim3(threads);
+  p.sharedMemBytes = 0;
+  p.kernelParams = params;
+  cudaGraphNode_t node;
+  cudaError_t e = cudaGraphAddKernelNode(&node, g, *prev ? prev : nullptr, *prev ? 1 : 0, &p);
+  if (e == cudaSuccess) *prev = node;
+  return e;
+}
+
+cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t *prev, cudaGraphConditionalHandle h,
+                            cudaGraphConditionalNodeType type, cudaGraph_t *body) {
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  cudaError_t e = cudaGraphAddNode(&node, g, *prev ? prev : nullptr, *prev ? 1 : 0, &p);
+  if (e != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  *prev = node;
+  return cudaSuccess;
+}
+
+#define SFR_TRY(expr)                       \
+  do {                                      \
+    cudaError_t e_ = (expr);                \
+    if (e_ != cudaSuccess) return e_;       \
+  } while (0)
+
+constexpr int kVecs64Plain = 11;  // diag b x m r z q p0 p1 r0 t
+constexpr int kVecs64Mixed = 3;   // diag b x
+constexpr int kVecs32 = 10;       // d32 m32 r z q p0 p1 xs r0 t
+
+inline int64_t padded(int n) { return (static_cast<int64_t>(n) + 3) & ~static_cast<int64_t>(3); }
+
+// Allocate the graph's workspace and fill its by-value arguments.
+template <int K>
+cudaError_t prepare(sfr_system *s, int precision, int threads, int spw, CachedGraph *cg) {
+  const int n = s->n;
+  const int64_t np = padded(n);
+  const bool mixed = precision == SFR_MIXED;
+  const int warps = threads / kWarp;
+  cg->threads = threads;
+  cg->grid_s = std::max(1, (s->A.nslices + warps * spw - 1) / (warps * spw));
+  const int npairs = (n + 1) / 2;
+  const int wave = std::max(1, num_sms(s->device)) * (2048 / threads);
+  cg->grid_v = std::max(1, std::min(wave, (npairs + threads - 1) / threads));
+  const int gmax = std::max(cg->grid_s, cg->grid_v);
+  const int n64 = mixed ? kVecs64Mixed : kVecs64Plain;
+  const size_t bytes64 = sizeof(double) * static_cast<size_t>(np) * n64 * K;
+  const size_t bytes32 = mixed ? sizeof(float) * static_cast<size_t>(np) * kVecs32 * K : 0;
+  SFR_TRY(cudaMalloc(&cg->ws, bytes64 + bytes32));
+  SFR_TRY(cudaMemset(cg->ws, 0, bytes64 + bytes32));  // padding rows stay finite
+  SFR_TRY(cudaMalloc(&cg->d_state, sizeof(SState<K>)));
+  SFR_TRY(cudaMalloc(&cg->part, sizeof(double) * kMaxNV * static_cast<size_t>(gmax)));
+  SFR_TRY(cudaMalloc(&cg->counter, sizeof(unsigned) * kCounters));
+  SFR_TRY(cudaMemset(cg->counter, 0, sizeof(unsigned) * kCounters));
+  cg->bytes = static_cast<int64_t>(bytes64 + bytes32 + sizeof(double) * kMaxNV * gmax);
+
+  cg->args.assign(sizeof(SArgs<K>), 0);
+  SArgs<K> &a = *reinterpret_cast<SArgs<K> *>(cg->args.data());
+  a.n = n;
+  a.nslices = s->A.nslices;
+  a.npairs = npairs;
+  a.sptr = s->A.sptr;
+  a.col = s->A.col;
+  a.val64 = s->A.val;
+  a.val32 = s->A.val32;
+  double *v64 = static_cast<double *>(cg->ws);
+  float *v32 = reinterpret_cast<float *>(static_cast<char *>(cg->ws) + bytes64);
+  for (int k = 0; k < K; ++k) {
+    auto D = [&](int w) { return v64 + (static_cast<size_t>(w) * K + k) * np; };
+    auto F = [&](int w) { return v32 + (static_cast<size_t>(w) * K + k) * np; };
+    a.diag64[k] = D(0);
+    a.b[k] = D(1);
+    a.x[k] = D(2);
+    if (mixed) {
+      a.d32[k] = F(0);
+      a.m32[k] = F(1);
+      a.fr[k] = F(2);
+      a.fz[k] = F(3);
+      a.fq[k] = F(4);
+      a.fp0[k] = F(5);
+      a.fp1[k] = F(6);
+      a.fxs[k] = F(7);
+      a.fr0[k] = F(8);
+      a.ft[k] = F(9);
+    } else {
+      a.m[k] = D(3);
+      a.r[k] = D(4);
+      a.z[k] = D(5);
+      a.q[k] = D(6);
+      a.p0[k] = D(7);
+      a.p1[k] = D(8);
+      a.r0[k] = D(9);
+      a.t[k] = D(10);
+    }
+  }
+  a.part = cg->part;
+  a.counter = cg->counter;
+  return cudaSuccess;
+}
+
+// The graph for one (solver, K, precision, launch shape).
+template <int K>
+cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
+                        CachedGraph *cg) {
+  SFR_TRY(prepare<K>(s, precision, threads, spw, cg));
+  SFR_TRY(cudaGraphCreate(&cg->graph, 0));
+  cudaGraph_t g = cg->graph;
+  const bool mixed = precision == SFR_MIXED;
+  SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hwhile, g, 1, cudaGraphCondAssignDefault));
+  // one handle per conditional node
+  if (mixed) SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hif, g, 0, cudaGraphCondAssignDefault));
+  if (mixed && solver != SFR_PCG)
+    SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hif2, g, 0, cudaGraphCondAssignDefault));
+  SArgs<K> &a = *reinterpret_cast<SArgs<K> *>(cg->args.data());
+  a.hwhile = cg->hwhile;
+  a.hif = cg->hif;
+  a.hif2 = cg->hif2;
+  a.in_graph = 1;
+
+  // cudaGraphAddKernelNode copies the argument values these point to
+  void *ps = cg->d_state;
+  void *p2[2] = {&a, &ps};
+  int stage1 = 1, stage2 = 2, zero = 0, one = 1;
+  void *pf_sel[3] = {&a, &ps, &zero};
+  void *pf_all[3] = {&a, &ps, &one};
+  void *pr1[3] = {&a, &ps, &stage1};
+  void *pr2[3] = {&a, &ps, &stage2};
+  const int gs = cg->grid_s, gv = cg->grid_v;
+
+  cudaGraphNode_t prev = nullptr;
+  {
+    cudaMemsetParams mp{};
+    mp.dst = cg->counter;
+    mp.value = 0;
+    mp.elementSize = sizeof(unsigned);
+    mp.width = kCounters;
+    mp.height = 1;
+    mp.pitch = 0;
+    SFR_TRY(cudaGraphAddMemsetNode(&prev, g, nullptr, 0, &mp));
+  }
+  cudaGraph_t body = nullptr, ifbody = nullptr;
+  if (solver == SFR_PCG) {
+    if (mixed) {
+      SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, true>, gs, threads, p2));
+      SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
+      cudaGraphNode_t bp = nullptr;
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, true>, gv, threads, p2));
+      SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
+      cudaGraphNode_t ip = nullptr;
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, true>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
+    } else {
+      SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false>, gs, threads, p2));
+      SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
+      cudaGraphNode_t bp = nullptr;
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, false>, gv, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, false>, gv, threads, p2));
+    }
+  } else {
+    if (mixed) {
+      SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, true>, gs, threads, p2));
+      SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
+      cudaGraphNode_t bp = nullptr;
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, true>, gv, threads, p2));
+      SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
+      cudaGraphNode_t ip = nullptr;
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K>, gs, threads, pr1));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, true>, gv, threads, p2));
+      cudaGraph_t ifbody2 = nullptr;
+      SFR_TRY(add_conditional(body, &bp, cg->hif2, cudaGraphCondTypeIf, &ifbody2));
+      cudaGraphNode_t ip2 = nullptr;
+      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K>, gs, threads, pr2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, true>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
+    } else {
+      SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, false>, gs, threads, p2));
+      SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
+      cudaGraphNode_t bp = nullptr;
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, false>, gv, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, false>, gv, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, false>, gv, threads, p2));
+    }
+  }
+  SFR_TRY(add_kernel(g, &prev, (void *)k_post<K>, gs, threads, p2));
+  SFR_TRY(cudaGraphInstantiate(&cg->exec, g, 0));
+  return cudaSuccess;
+}
+
+void free_graph(CachedGraph *cg) {
+  if (cg->exec) cudaGraphExecDestroy(cg->exec);
+  if (cg->graph) cudaGraphDestroy(cg->graph);
+  cudaFree(cg->d_state);
+  cudaFree(cg->ws);
+  cudaFree(cg->part);
+  cudaFree(cg->counter);
+  *cg = CachedGraph{};
+}
+
+// The same kernels launched from a host loop for `maxit` iterations (kernels
+// of finished solves return at once).  For profilers, which cannot look into
+// graphs with conditional nodes; never the production path.
+template <int K>
+cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
+                        cudaStream_t st) {
+  SArgs<K> a = *reinterpret_cast<const SArgs<K> *>(cg->args.data());
+  a.in_graph = 0;
+  auto *ps = static_cast<SState<K> *>(cg->d_state);
+  const int gs = cg->grid_s, gv = cg->grid_v, t = cg->threads;
+  SFR_TRY(cudaMemsetAsync(cg->counter, 0, sizeof(unsigned) * kCounters, st));
+  if (solver == SFR_PCG) {
+    if (mixed) {
+      k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
+      k_pcg_start<K, true><<<gs, t, 0, st>>>(a, ps);
+      for (uint32_t it = 0; it < maxit; ++it) {
+        k_pcg_a<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_b<K, true><<<gv, t, 0, st>>>(a, ps);
+        k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
+        k_pcg_refresh<K><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_c<K, true><<<gv, t, 0, st>>>(a, ps);
+      }
+      k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
+    } else {
+      k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
+      k_pcg_start<K, false><<<gs, t, 0, st>>>(a, ps);
+      for (uint32_t it = 0; it < maxit; ++it) {
+        k_pcg_a<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_b<K, false><<<gv, t, 0, st>>>(a, ps);
+        k_pcg_c<K, false><<<gv, t, 0, st>>>(a, ps);
+      }
+    }
+  } else {
+    if (mixed) {
+      k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
+      k_bicg_start<K, true><<<gs, t, 0, st>>>(a, ps);
+      for (uint32_t it = 0; it < maxit; ++it) {
+        k_bicg_a1<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_b1<K, true><<<gv, t, 0, st>>>(a, ps);
+        k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
+        k_bicg_refresh<K><<<gs, t, 0, st>>>(a, ps, 1);
+        k_bicg_a2<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_b2<K, true><<<gv, t, 0, st>>>(a, ps);
+        k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
+        k_bicg_refresh<K><<<gs, t, 0, st>>>(a, ps, 2);
+        k_bicg_c<K, true><<<gv, t, 0, st>>>(a, ps);
+      }
+      k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
+    } else {
+      k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
+      k_bicg_start<K, false><<<gs, t, 0, st>>>(a, ps);
+      for (uint32_t it = 0; it < maxit; ++it) {
+        k_bicg_a1<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_b1<K, false><<<gv, t, 0, st>>>(a, ps);
+        k_bicg_a2<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_b2<K, false><<<gv, t, 0, st>>>(a, ps);
+        k_bicg_c<K, false><<<gv, t, 0, st>>>(a, ps);
+      }
+    }
+  }
+  k_post<K><<<gs, t, 0, st>>>(a, ps);
+  return cudaGetLastError();
+}
+
+template <int K>
+int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, double *d_x,
+        double tol, uint32_t maxit, int newx, int precision, double delta, int threads, int spw,
+        bool loop, cudaStream_t st, SolveOut *out, float *ms) {
+  const int n = s->n;
+  if (maxit == 0) return SFR_BAD_INPUT;
+  EngineCache &ec = g_engines[s];
+  GraphKey key{solver, K, precision, threads, spw};
+  auto it = ec.graphs.find(key);
+  if (it == ec.graphs.end()) {
+    if (ec.graphs.size() >= kMaxGraphsPerSystem) {  // drop the least recently used
+      auto lru = ec.graphs.begin();
+      for (auto g = ec.graphs.begin(); g != ec.graphs.end(); ++g)
+        if (g->second->last_use < lru->second->last_use) lru = g;
+      free_graph(lru->second.get());
+      ec.graphs.erase(lru);
+    }
+    auto cg = std::make_unique<CachedGraph>();
+    const cudaError_t be = build_graph<K>(s, solver, precision, threads, spw, cg.get());
+    if (be != cudaSuccess) {
+      set_last_error(cudaGetErrorString(be));
+      free_graph(cg.get());
+      return SFR_CUDA_ERROR;
+    }
+    it = ec.graphs.emplace(key, std::move(cg)).first;
+  }
+  CachedGraph *cg = it->second.get();
+  cg->last_use = ++ec.clock;
+  const SArgs<K> &a = *reinterpret_cast<const SArgs<K> *>(cg->args.data());
+  const bool mixed = precision == SFR_MIXED;
+  SCall call{tol, delta, maxit, newx};
+
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  cudaError_t err = cudaSuccess;
+  const size_t vb = sizeof(double) * static_cast<size_t>(n);
+  for (int k = 0; k < K && err == cudaSuccess; ++k) {
+    const double *dg = d_diag_k ? d_diag_k + static_cast<size_t>(k) * n : s->d_diag;
+    err = cudaMemcpyAsync(a.diag64[k], dg, vb, cudaMemcpyDeviceToDevice, st);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(a.b[k], d_b + static_cast<size_t>(k) * n, vb,
+                            cudaMemcpyDeviceToDevice, st);
+    if (err == cudaSuccess && !newx)
+      err = cudaMemcpyAsync(a.x[k], d_x + static_cast<size_t>(k) * n, vb,
+                            cudaMemcpyDeviceToDevice, st);
+  }
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(cg->d_state, &call, sizeof(call), cudaMemcpyHostToDevice, st);
+  if (err == cudaSuccess)
+    err = loop ? launch_loop<K>(cg, solver, mixed, maxit, st) : cudaGraphLaunch(cg->exec, st);
+  for (int k = 0; k < K && err == cudaSuccess; ++k)
+    err = cudaMemcpyAsync(d_x + static_cast<size_t>(k) * n, a.x[k], vb, cudaMemcpyDeviceToDevice,
+                          st);
+  cudaEventRecord(e1, st);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(out, static_cast<SState<K> *>(cg->d_state)->out, sizeof(SolveOut) * K,
+                          cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  if (err == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) {
+    set_last_error(cudaGetErrorString(err));
+    return SFR_CUDA_ERROR;
+  }
+  return SFR_OK;
+}
+
+}  // namespace
+
+int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
+                 const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
+                 int32_t precision, double delta, int threads, int spw, bool loop,
+                 cudaStream_t st, sfr_solve_info *info) {
+  if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
+  if (threads != 128 && threads != 256) return SFR_BAD_INPUT;
+  if (spw < 1 || spw > 64) return SFR_BAD_INPUT;
+  SolveOut out[kMaxK];
+  float ms = 0.f;
+  int rc;
+  switch (k) {
+    case 1: rc = run<1>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
+    case 2: rc = run<2>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
+    case 3: rc = run<3>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
+    default: rc = run<4>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
+  }
+  if (rc != SFR_OK) return rc;
+  int worst = SFR_OK;
+  for (int i = 0; i < k; ++i) {
+    if (info) {
+      sfr_solve_info &f = info[i];
+      std::memset(&f, 0, sizeof(f));
+      f.iters = out[i].iters;
+      f.status = out[i].status;
+      f.xKx = out[i].xKx;
+      f.norm_x = out[i].norm_x;
+      f.norm_r = out[i].norm_r;
+      f.norm_r_m = out[i].norm_r_m;
+      f.conv = out[i].conv;
+      f.seconds = ms * 1e-3;
+      f.refinements = out[i].refinements;
+      f.inner_iters = out[i].inner_iters;
+      f.relres = out[i].bnorm > 0 ? out[i].norm_r / out[i].bnorm : 0.0;
+    }
+    if (out[i].status != SFR_OK && worst == SFR_OK) worst = out[i].status;
+  }
+  return worst;
+}
+
+void release_stream_engine(const sfr_system *s) {
+  auto it = g_engines.find(s);
+  if (it == g_engines.end()) return;
+  for (auto &kv : it->second.graphs) free_graph(kv.second.get());
+  g_engines.erase(it);
+}
+
+}  // namespace sfr

@@ -21,6 +21,7 @@ CSRD, CSRC, ELLPACK = 2, 3, 4
 OK, MAXIT, BREAKDOWN = 0, 1, 2
 BAD_INPUT, CUDA_ERROR, TIMEOUT, UNSUPPORTED = -1, -2, -3, -4
 FP64, MIXED = 0, 1
+ENGINE_AUTO, ENGINE_PERSISTENT, ENGINE_GRAPH = 0, 1, 2
 
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -79,6 +80,7 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_double, ctypes.c_uint32, _I32,
                                       _I32, _P]
     L.sfr_gpu_destroy.argtypes = [_P]
+    L.sfr_gpu_set_engine.argtypes = [_P, _I32, _I32, _I32]
     L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_transpose.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_dot.argtypes = [_P, _P, _P, _P, _P]
@@ -158,6 +160,12 @@ class GpuSystem:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_engine(self, engine: int, threads: int = 0, slices_per_warp: int = 0):
+        """0 automatic, 1 persistent (one cooperative launch), 2 graph."""
+        rc = lib().sfr_gpu_set_engine(self.h, engine, threads, slices_per_warp)
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_engine")
 
     def set_values(self, al, ad, au=None):
         al, ad, au = _f64(al), _f64(ad), _f64(au)

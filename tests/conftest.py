@@ -52,3 +52,9 @@ def rel(a, b):
     b = np.asarray(b, dtype=np.float64)
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+@pytest.fixture(params=[1, 2], ids=["persistent", "graph"])
+def engine(request):
+    """Both solve engines: 1 = one cooperative launch, 2 = CUDA graph."""
+    return request.param

@@ -29,11 +29,12 @@ def true_residual(s, st, un, ia, ja, al, x, b, ad=None):
 
 
 @pytest.mark.parametrize("kind", ["uniform", "jittered"])
-def test_mixed_pcg_meets_reference_criterion(cuda, kind):
+def test_mixed_pcg_meets_reference_criterion(cuda, engine, kind):
     s = S.poisson_uniform(32, seed=1) if kind == "uniform" else S.poisson_jittered(40, seed=2)
     st, un, ia, ja, al, _ = layouts(s)["csrd_full"]
     g = sv.GpuSystem(s.neq, ia, ja, st, un)
     g.set_values(al, s.ad)
+    g.set_engine(engine)
     x, info = g.solve(sv.PCG, s.b[0], tol=TOL, precision=sv.MIXED)
     assert info.status == sv.OK, info
     r, rm, bm = true_residual(s, st, un, ia, ja, al, x, s.b[0])
@@ -49,12 +50,13 @@ def test_mixed_pcg_meets_reference_criterion(cuda, kind):
 
 
 @pytest.mark.parametrize("dt", [1e-2, 1.0])
-def test_mixed_bicgstab_meets_reference_criterion(cuda, dt):
+def test_mixed_bicgstab_meets_reference_criterion(cuda, engine, dt):
     s = S.build(S.params(kind=S.SFR_SYS_CONVDIFF, n=24, lengths=(np.pi,) * 3,
                          dirichlet=S.ALL_FACES, nrhs=1, rhs_normal=True,
                          peclet=50.0, nu=1e-3, dt=dt, seed=41))
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     g.set_values(s.al, s.ad)
+    g.set_engine(engine)
     x, info = g.solve(sv.PBICGSTAB, s.b[0], tol=TOL, precision=sv.MIXED)
     assert info.status == sv.OK, info
     r = s.b[0] - O.matvec(O.CSRD, True, s.ia, s.ja, s.al, s.ad, x)
@@ -63,11 +65,12 @@ def test_mixed_bicgstab_meets_reference_criterion(cuda, dt):
     assert rel(x, ref.x) < 1e-7
 
 
-def test_mixed_multi_rhs_per_component_diagonal(cuda):
+def test_mixed_multi_rhs_per_component_diagonal(cuda, engine):
     s = S.momentum(20, seed=53, nrhs=3)
     ad_k = np.stack([s.ad, 1.1 * s.ad, 0.95 * s.ad])
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     g.set_values(s.al, s.ad)
+    g.set_engine(engine)
     xs, infos = g.solve_multi(sv.PBICGSTAB, s.b, ad_k=ad_k, tol=TOL, precision=sv.MIXED)
     for k in range(3):
         assert infos[k].status == sv.OK
@@ -79,10 +82,11 @@ def test_mixed_multi_rhs_per_component_diagonal(cuda):
     assert rel(x1, xs[0]) < 1e-8
 
 
-def test_mixed_iteration_cap_folds_correction(cuda):
+def test_mixed_iteration_cap_folds_correction(cuda, engine):
     s = S.poisson_jittered(24, seed=9)
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     g.set_values(s.al, s.ad)
+    g.set_engine(engine)
     x, info = g.solve(sv.PCG, s.b[0], tol=TOL, maxit=40, precision=sv.MIXED)
     assert info.status == sv.MAXIT
     # x holds the FP64 solution after the last correction: the residual the

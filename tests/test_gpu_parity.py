@@ -25,10 +25,11 @@ TOL_X = 1e-12  # relative 2-norm error in x, FP64 path vs reference
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_solves.npz"))
 
 
-def gpu_system(sysx, lname):
+def gpu_system(sysx, lname, engine=0):
     st, un, ia, ja, al, au = layouts(sysx)[lname]
     g = sv.GpuSystem(sysx.neq, ia, ja, st, un)
     g.set_values(al, sysx.ad, au)
+    g.set_engine(engine)
     return g, (st, un, ia, ja, al)
 
 
@@ -70,13 +71,14 @@ def test_dot_deterministic(cuda):
 
 
 @pytest.mark.parametrize("name", [str(c) for c in GOLD["cases"]])
-def test_solver_against_reference_fixture(cuda, name):
+def test_solver_against_reference_fixture(cuda, engine, name):
     g = {k.split("/", 1)[1]: GOLD[k] for k in GOLD.files if k.startswith(name + "/")}
     solver, st, un, maxit, newx = (int(v) for v in g["meta"])
     iters, status = (int(v) for v in g["res"])
     n = len(g["ad"])
     sysg = sv.GpuSystem(n, g["ia"], g["ja"], st, bool(un))
     sysg.set_values(g["al"], g["ad"])
+    sysg.set_engine(engine)
     x, info = sysg.solve(solver, g["b"], x0=g["x0"], tol=float(g["tol"][0]),
                          maxit=maxit, newx=bool(newx))
     if status == 0:
@@ -90,9 +92,9 @@ def test_solver_against_reference_fixture(cuda, name):
 
 
 @pytest.mark.parametrize("lname", ["csrd_full", "csrd_sym", "csrc_sym", "ellpack"])
-def test_pcg_uniform_32(cuda, lname):
+def test_pcg_uniform_32(cuda, engine, lname):
     s = S.poisson_uniform(32, seed=1)
-    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    g, (st, un, ia, ja, al) = gpu_system(s, lname, engine)
     x, info = g.solve(sv.PCG, s.b[0], tol=1e-10)
     ref = reference(O.PCG, st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
     assert info.status == sv.OK and ref.status == 0
@@ -101,9 +103,9 @@ def test_pcg_uniform_32(cuda, lname):
     assert abs(info.xKx - ref.xKx) <= 1e-11 * abs(ref.xKx)
 
 
-def test_pcg_jittered_contrast(cuda):
+def test_pcg_jittered_contrast(cuda, engine):
     s = S.poisson_jittered(40, seed=2)
-    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full")
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full", engine)
     x, info = g.solve(sv.PCG, s.b[0], tol=1e-10)
     ref = O.pcg(st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
     assert info.status == sv.OK
@@ -119,10 +121,10 @@ def steady_system(n=24, seed=41):
 
 
 @pytest.mark.parametrize("lname", ["csrd_full", "csrc_unsym", "ellpack"])
-def test_bicgstab_momentum(cuda, lname):
+def test_bicgstab_momentum(cuda, engine, lname):
     # the momentum system as the SIMPLE loop sees it (dt = 1e-2)
     s = S.momentum(24, seed=41, nrhs=1)
-    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    g, (st, un, ia, ja, al) = gpu_system(s, lname, engine)
     x, info = g.solve(sv.PBICGSTAB, s.b[0], tol=1e-10)
     ref = reference(O.PBICGSTAB, st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
     assert info.status == sv.OK and ref.status == 0
@@ -145,13 +147,13 @@ def reference_spread(solver, s, b):
 
 @pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("lname", ["csrd_full", "csrc_unsym", "ellpack"])
-def test_bicgstab_steady_within_reference_spread(cuda, lname):
+def test_bicgstab_steady_within_reference_spread(cuda, engine, lname):
     # Convection-dominated and nearly steady: the BiCGSTAB residual history
     # is irregular near the threshold, so any change of summation order moves
     # the iteration count by a few and x by up to ~1e-9 -- the reference's
     # own OpenMP path does.  Bar: stay inside that spread (+1 iteration, x 4x).
     s = steady_system()
-    g, (st, un, ia, ja, al) = gpu_system(s, lname)
+    g, (st, un, ia, ja, al) = gpu_system(s, lname, engine)
     x, info = g.solve(sv.PBICGSTAB, s.b[0], tol=1e-10)
     ser, lo, hi, err = reference_spread(O.PBICGSTAB, s, s.b[0])
     assert info.status == sv.OK
@@ -160,7 +162,7 @@ def test_bicgstab_steady_within_reference_spread(cuda, lname):
 
 
 @pytest.mark.parametrize("solver", [sv.PCG, sv.PBICGSTAB])
-def test_multi_rhs_matches_single(cuda, solver):
+def test_multi_rhs_matches_single(cuda, engine, solver):
     # K right-hand sides in one launch against K single solves.  The K-RHS
     # kernel may run a different grid (occupancy), i.e. another reduction
     # order, so the bar is the parity bar, not bit equality.
@@ -168,7 +170,7 @@ def test_multi_rhs_matches_single(cuda, solver):
          else S.momentum(24, seed=52, nrhs=3))
     b = np.stack([s.b[0], -0.5 * s.b[0] + 0.1, np.cos(np.arange(s.neq))]) \
         if solver == sv.PCG else s.b
-    g, _ = gpu_system(s, "csrd_full")
+    g, _ = gpu_system(s, "csrd_full", engine)
     xs, infos = g.solve_multi(solver, b, tol=1e-10)
     for k in range(3):
         x1, i1 = g.solve(solver, b[k], tol=1e-10)
@@ -177,11 +179,11 @@ def test_multi_rhs_matches_single(cuda, solver):
         assert rel(xs[k], x1) < TOL_X
 
 
-def test_multi_rhs_per_component_diagonal(cuda):
+def test_multi_rhs_per_component_diagonal(cuda, engine):
     # u, v, w share al/au and differ in ad (Simple.c:2736-2750)
     s = S.momentum(14, seed=53, nrhs=3)
     ad_k = np.stack([s.ad, 1.1 * s.ad, 0.95 * s.ad])
-    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full")
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full", engine)
     xs, infos = g.solve_multi(sv.PBICGSTAB, s.b, ad_k=ad_k, tol=1e-10)
     for k in range(3):
         ref = O.pbicgstab(st, un, ia, ja, al, ad_k[k], s.b[k], tol=1e-10)
@@ -189,9 +191,9 @@ def test_multi_rhs_per_component_diagonal(cuda):
         assert rel(xs[k], ref.x) < TOL_X
 
 
-def test_warm_start_and_repeatability(cuda):
+def test_warm_start_and_repeatability(cuda, engine):
     s = S.poisson_uniform(20, seed=61)
-    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_sym")
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_sym", engine)
     x0 = np.linspace(-1, 1, s.neq)
     x1, i1 = g.solve(sv.PCG, s.b[0], x0=x0, newx=False, tol=1e-9)
     x2, i2 = g.solve(sv.PCG, s.b[0], x0=x0, newx=False, tol=1e-9)
@@ -201,9 +203,9 @@ def test_warm_start_and_repeatability(cuda):
     assert rel(x1, ref.x) < TOL_X
 
 
-def test_breakdown_and_maxit_are_statuses_not_hangs(cuda):
+def test_breakdown_and_maxit_are_statuses_not_hangs(cuda, engine):
     s = S.poisson_uniform(10, seed=71)
-    g, _ = gpu_system(s, "csrd_full")
+    g, _ = gpu_system(s, "csrd_full", engine)
     b = s.b[0].copy()
     b[5] = np.nan
     _, info = g.solve(sv.PCG, b, tol=1e-10, maxit=50)
