@@ -127,6 +127,39 @@ int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
 
 int sfr_gpu_destroy(sfr_system *s);
 
+/* ---- batches of independent systems ----------------------------------- */
+
+typedef struct sfr_batch sfr_batch; /* many systems solved in one launch */
+
+/* Upload nsys patterns of one storage kind (arrays of per-system pointers,
+ * each system as sfr_gpu_create takes it).  The systems are concatenated
+ * block-diagonally; one persistent cooperative launch (replayed from a CUDA
+ * graph) solves them all, each system by its own team of thread blocks with
+ * its own barrier, so each stops at its own convergence.  No counterpart in
+ * the reference, which solves systems one solverC call at a time. */
+int sfr_gpu_batch_create(int32_t nsys, const int32_t *neq, const int32_t *nad,
+                         const int32_t *const *ia, const int32_t *const *ja,
+                         int32_t storage, int32_t unsym, int32_t device,
+                         sfr_batch **out);
+int sfr_gpu_batch_set_values(sfr_batch *b, const double *const *al,
+                             const double *const *ad,
+                             const double *const *au);
+/* Solve every system (b[s], x[s] host arrays of its neq); info has nsys
+ * entries.  Returns the first non-OK per-system status, or an error. */
+int sfr_gpu_batch_solve(sfr_batch *b, int32_t solver, const double *const *bv,
+                        double *const *x, double tol, uint32_t maxit,
+                        int32_t newx, int32_t precision, sfr_solve_info *info);
+/* Work weights of the systems (blocks are shared out in proportion). */
+int sfr_gpu_batch_set_weights(sfr_batch *b, const double *w);
+/* Measure per-system iterations on bv, weight teams by slices x iterations,
+ * keep whichever plan solves faster; *ms_out = its solve time. */
+int sfr_gpu_batch_autotune(sfr_batch *b, int32_t solver,
+                           const double *const *bv, double tol,
+                           uint32_t maxit, int32_t precision, double *ms_out);
+int sfr_gpu_batch_stats(const sfr_batch *b, int32_t *grid, int64_t *rows,
+                        int64_t *bytes);
+int sfr_gpu_batch_destroy(sfr_batch *b);
+
 /* ---- kernels for measurement and tests (device pointers) ------------- */
 
 /* y = A x on the device (the matVec* family, HccaBlas.c:2620-4755). */

@@ -94,6 +94,20 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
 int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                 const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
                 cudaStream_t st, sfr_solve_info *info);
+// Batched (team) persistent launches, K = 1 (krylov.cu, mixed.cu)
+struct TeamTable;
+struct SolveOut;
+size_t team_ws_bytes_fp64(int n, int grid);
+size_t team_ws_bytes_mixed(int n, int grid);
+int team_max_grid_fp64(int32_t solver, int device);
+int team_max_grid_mixed(int32_t solver, int device);
+int enqueue_team_fp64(sfr_system *s, int32_t solver, const double *d_b, double *d_x, double tol,
+                      uint32_t maxit, int32_t newx, const TeamTable &team, int grid, void *ws,
+                      SolveOut *d_out, unsigned *ctl, cudaStream_t st);
+int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double *d_x, double tol,
+                       uint32_t maxit, int32_t newx, const TeamTable &team, int grid, void *ws,
+                       SolveOut *d_out, unsigned *ctl, cudaStream_t st);
+
 // Graph engine (stream_solve.cu)
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,

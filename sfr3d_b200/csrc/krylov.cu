@@ -39,6 +39,7 @@ struct KrylovArgs {
   double *r0[kMaxK];  // BiCGSTAB shadow residual
   double *part;       // 2 slots x kMaxNV x gridDim
   GridSync gs;
+  TeamTable team;     // block -> system map of a batched launch (null: one system)
   SolveOut *out;
   double tol;
   unsigned maxit;
@@ -47,9 +48,9 @@ struct KrylovArgs {
 
 // Reduce NV values of a FP64 solve: partials, barrier, totals.
 template <int NV>
-__device__ __forceinline__ bool reduce_all(const KrylovArgs &a, int &slot, double (&acc)[NV],
-                                           double (&tot)[NV], double *sm) {
-  return reduce_step<NV>(a.part, a.gs, slot, acc, tot, sm);
+__device__ __forceinline__ bool reduce_all(const KrylovArgs &a, const Team &t, int &slot,
+                                           double (&acc)[NV], double (&tot)[NV], double *sm) {
+  return reduce_team<NV>(a.part, t, slot, acc, tot, sm);
 }
 
 // y_k[row] for K right-hand sides from a gather functor g(k, col).
@@ -81,10 +82,10 @@ __device__ __forceinline__ void row_spmv_k(const SellView<double> &A, const doub
 template <int K>
 __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
   __shared__ double sm[kMaxNV * 32];
-  const int n = a.n;
+  const Team team = make_team(a.team, a.gs, a.A.nslices, a.n);
+  const int n = team.row_end;
   const int lane = threadIdx.x & 31;
-  int s0, s1;
-  block_slices(a.A.nslices, &s0, &s1);
+  const int s0 = team.s0, s1 = team.s1;
   int slot = 0;
   bool act[K];
   double d[K], conv[K], alpha[K], beta[K];
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         acc[k] += bk * xmul(bk, mk);
       }
     }
-    if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+    if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) conv[k] = a.tol * sqrt(fabs(tot[k]));
   }
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         acc[k] += rk * zk;
       }
     }
-    if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+    if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) d[k] = tot[k];
   }
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
           acc[k] += y[k] * pk;
         }
       }
-      if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -198,7 +199,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
           acc[k] += rk * zk;
         }
       }
-      if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
       bool any = false;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -249,8 +250,8 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         acc[4 * k + 3] += rk * rk;
       }
     }
-    if (!reduce_all<4 * K>(a, slot, acc, tot, sm)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!reduce_all<4 * K>(a, team, slot, acc, tot, sm)) return;
+    if (blockIdx.x == team.b0 && threadIdx.x == 0) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         SolveOut o;
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         o.bnorm = 0.0;
         o.refinements = 0;
         o.inner_iters = iters[k];
-        a.out[k] = o;
+        a.out[team.sys * K + k] = o;
       }
     }
   }
@@ -277,10 +278,10 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
 template <int K>
 __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
   __shared__ double sm[kMaxNV * 32];
-  const int n = a.n;
+  const Team team = make_team(a.team, a.gs, a.A.nslices, a.n);
+  const int n = team.row_end;
   const int lane = threadIdx.x & 31;
-  int s0, s1;
-  block_slices(a.A.nslices, &s0, &s1);
+  const int s0 = team.s0, s1 = team.s1;
   int slot = 0;
   bool act[K];
   double conv[K], alpha[K], w[K], rr0[K], beta[K];
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         acc[k] += bk * bk;
       }
     }
-    if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+    if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) conv[k] = a.tol * sqrt(tot[k]);
   }
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         st_vec(a.z[k] + row_, xmul(rk, ld_vec(a.m[k] + row_)));
       }
     }
-    if (!grid_sync(a.gs)) return;
+    if (!grid_sync(team.gs)) return;
   }
   unsigned j = 0;
   bool any = true;
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
           acc[2 * k + 1] += y[k] * r0k;
         }
       }
-      if (!reduce_all<2 * K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<2 * K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
           acc[k] += rk * rk;
         }
       }
-      if (!reduce_all<K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -404,7 +405,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
           acc[2 * k + 1] += y[k] * y[k];
         }
       }
-      if (!reduce_all<2 * K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<2 * K>(a, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
           acc[2 * k + 1] += rk * ld_vec(a.r0[k] + row_);
         }
       }
-      if (!reduce_all<2 * K>(a, slot, acc, tot, sm)) return;
+      if (!reduce_all<2 * K>(a, team, slot, acc, tot, sm)) return;
       any = false;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -467,7 +468,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
           st_vec(a.z[k] + row_, xmul(pk, ld_vec(a.m[k] + row_)));
         }
       }
-      if (!grid_sync(a.gs)) return;
+      if (!grid_sync(team.gs)) return;
     }
   }
 #pragma unroll
@@ -497,8 +498,8 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         acc[3 * k + 2] += rk * rk;
       }
     }
-    if (!reduce_all<3 * K>(a, slot, acc, tot, sm)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!reduce_all<3 * K>(a, team, slot, acc, tot, sm)) return;
+    if (blockIdx.x == team.b0 && threadIdx.x == 0) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         SolveOut o;
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         o.bnorm = 0.0;
         o.refinements = 0;
         o.inner_iters = iters[k];
-        a.out[k] = o;
+        a.out[team.sys * K + k] = o;
       }
     }
   }
@@ -783,6 +784,62 @@ int launch_krylov(sfr_system *s, int32_t solver, const double *d_diag_k, const d
 }
 
 }  // namespace
+
+// ---- batched (team) launches: K = 1, no host synchronisation, so the
+// launch can be captured in a CUDA graph.
+size_t team_ws_bytes_fp64(int n, int grid) {
+  auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  return align(sizeof(double) * static_cast<size_t>(n) * kVecs) +
+         align(sizeof(double) * 2 * kMaxNV * static_cast<size_t>(grid));
+}
+
+int team_max_grid_fp64(int32_t solver, int device) {
+  void (*kern)(KrylovArgs) = solver == SFR_PCG ? pcg_fp64_kernel<1> : bicgstab_fp64_kernel<1>;
+  int bps = 0;
+  return occupancy_grid(kern, kThreads, device, &bps);
+}
+
+int enqueue_team_fp64(sfr_system *s, int32_t solver, const double *d_b, double *d_x, double tol,
+                      uint32_t maxit, int32_t newx, const TeamTable &team, int grid, void *ws,
+                      SolveOut *d_out, unsigned *ctl, cudaStream_t st) {
+  const int n = s->n;
+  auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  double *vec = static_cast<double *>(ws);
+  auto V = [&](int which) { return vec + static_cast<size_t>(which) * n; };
+  KrylovArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.A = SellView<double>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val, s->d_diag};
+  a.n = n;
+  a.diag[0] = s->d_diag;
+  a.b[0] = d_b;
+  a.x[0] = d_x;
+  a.m[0] = V(0);
+  a.r[0] = V(1);
+  a.z[0] = V(2);
+  a.q[0] = V(3);
+  a.p0[0] = V(4);
+  a.p1[0] = V(5);
+  a.r0[0] = V(6);
+  a.part = reinterpret_cast<double *>(static_cast<char *>(ws) +
+                                      align(sizeof(double) * static_cast<size_t>(n) * kVecs));
+  a.gs.count = ctl;
+  a.gs.gen = ctl + 1;
+  a.gs.err = reinterpret_cast<int *>(ctl + 2);
+  a.gs.nblocks = grid;
+  a.gs.spin_limit = 1u << 22;
+  a.team = team;
+  a.out = d_out;
+  a.tol = tol;
+  a.maxit = maxit;
+  a.newx = newx;
+  if (cudaMemsetAsync(ctl, 0, 64, st) != cudaSuccess) return SFR_CUDA_ERROR;
+  void (*kern)(KrylovArgs) = solver == SFR_PCG ? pcg_fp64_kernel<1> : bicgstab_fp64_kernel<1>;
+  void *params[] = {&a};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), dim3(grid), dim3(kThreads),
+                                     params, 0, st) == cudaSuccess
+             ? SFR_OK
+             : SFR_CUDA_ERROR;
+}
 
 int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,

@@ -45,6 +45,7 @@ struct MixedArgs {
   float *t[kMaxK];    // BiCGSTAB t = A z
   double *part;
   GridSync gs;
+  TeamTable team;  // block -> system map of a batched launch (null: one system)
   SolveOut *out;
   double tol;
   double delta;
@@ -96,9 +97,10 @@ __device__ __forceinline__ double row_spmv64(const MixedArgs &a, int k, int s, i
 // With `first`, x is not updated and the PCG direction / BiCGSTAB shadow
 // residual and direction are initialised from r.
 template <int K, bool kPcg>
-__device__ bool reliable_update(const MixedArgs &a, int s0, int s1, const bool (&sel)[K],
+__device__ bool reliable_update(const MixedArgs &a, const Team &t, const bool (&sel)[K],
                                 bool first, int &slot, double *sm, double (&tot)[2 * K]) {
-  const int n = a.n;
+  const int n = t.row_end;
+  const int s0 = t.s0, s1 = t.s1;
   const int lane = threadIdx.x & 31;
   if (!first) {
     SFR_FOR_OWN_ROWS(s0, s1) {
@@ -109,7 +111,7 @@ __device__ bool reliable_update(const MixedArgs &a, int s0, int s1, const bool (
         st_vec(a.x[k] + row_, xk);
       }
     }
-    if (!grid_sync(a.gs)) return false;
+    if (!grid_sync(t.gs)) return false;
   }
   double acc[2 * K];
 #pragma unroll
@@ -140,14 +142,15 @@ __device__ bool reliable_update(const MixedArgs &a, int s0, int s1, const bool (
   }
   // BiCGSTAB: r0 was written above only on the first call; the (r, r0) read
   // uses the value this thread just stored, so no barrier is needed before it.
-  return reduce_step<2 * K>(a.part, a.gs, slot, acc, tot, sm);
+  return reduce_team<2 * K>(a.part, t, slot, acc, tot, sm);
 }
 
 template <int K, bool kPcg>
-__device__ void finish(const MixedArgs &a, int s0, int s1, const int (&iters)[K],
+__device__ void finish(const MixedArgs &a, const Team &t, const int (&iters)[K],
                        const int (&status)[K], const int (&refine)[K], const double (&conv)[K],
                        const double (&bnorm)[K], int &slot, double *sm) {
-  const int n = a.n;
+  const int n = t.row_end;
+  const int s0 = t.s0, s1 = t.s1;
   const int lane = threadIdx.x & 31;
   double acc[4 * K], tot[4 * K];
 #pragma unroll
@@ -164,8 +167,8 @@ __device__ void finish(const MixedArgs &a, int s0, int s1, const int (&iters)[K]
       acc[4 * k + 3] += rk * rk;
     }
   }
-  if (!reduce_step<4 * K>(a.part, a.gs, slot, acc, tot, sm)) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (!reduce_team<4 * K>(a.part, t, slot, acc, tot, sm)) return;
+  if (blockIdx.x == t.b0 && threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       SolveOut o;
@@ -179,7 +182,7 @@ __device__ void finish(const MixedArgs &a, int s0, int s1, const int (&iters)[K]
       o.bnorm = bnorm[k];
       o.refinements = refine[k];
       o.inner_iters = iters[k];
-      a.out[k] = o;
+      a.out[t.sys * K + k] = o;
     }
   }
 }
@@ -187,9 +190,10 @@ __device__ void finish(const MixedArgs &a, int s0, int s1, const int (&iters)[K]
 // Setup shared by both solvers: FP32 diagonal and Jacobi, x0, and the two
 // norms of b ((b, M^-1 b) and (b, b)).
 template <int K>
-__device__ bool setup(const MixedArgs &a, int s0, int s1, int &slot, double *sm,
+__device__ bool setup(const MixedArgs &a, const Team &t, int &slot, double *sm,
                       double (&bm)[K], double (&bb)[K]) {
-  const int n = a.n;
+  const int n = t.row_end;
+  const int s0 = t.s0, s1 = t.s1;
   double acc[2 * K], tot[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
@@ -205,7 +209,7 @@ __device__ bool setup(const MixedArgs &a, int s0, int s1, int &slot, double *sm,
       acc[2 * k + 1] += bk * bk;
     }
   }
-  if (!reduce_step<2 * K>(a.part, a.gs, slot, acc, tot, sm)) return false;
+  if (!reduce_team<2 * K>(a.part, t, slot, acc, tot, sm)) return false;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     bm[k] = tot[2 * k];
@@ -220,17 +224,17 @@ __device__ bool setup(const MixedArgs &a, int s0, int s1, int &slot, double *sm,
 template <int K>
 __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
   __shared__ double sm[kMaxNV * 32];
-  const int n = a.n;
+  const Team team = make_team(a.team, a.gs, a.A32.nslices, a.n);
+  const int n = team.row_end;
   const int lane = threadIdx.x & 31;
-  int s0, s1;
-  block_slices(a.A32.nslices, &s0, &s1);
+  const int s0 = team.s0, s1 = team.s1;
   int slot = 0;
   bool act[K];
   double d[K], conv[K], bnorm[K], alpha[K], beta[K], rmax[K];
   int iters[K], status[K], refine[K];
   {
     double bm[K], bb[K];
-    if (!setup<K>(a, s0, s1, slot, sm, bm, bb)) return;
+    if (!setup<K>(a, team, slot, sm, bm, bb)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       conv[k] = a.tol * sqrt(fabs(bm[k]));
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
   }
   {
     double tot[2 * K];
-    if (!reliable_update<K, true>(a, s0, s1, act, true, slot, sm, tot)) return;
+    if (!reliable_update<K, true>(a, team, act, true, slot, sm, tot)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       rmax[k] = sqrt(fabs(tot[2 * k]));
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
           acc[k] += static_cast<double>(y[k]) * static_cast<double>(pk);
         }
       }
-      if (!reduce_step<K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<K>(a.part, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
           acc[k] += static_cast<double>(rk) * static_cast<double>(zk);
         }
       }
-      if (!reduce_step<K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<K>(a.part, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         upd[k] = false;
@@ -343,7 +347,7 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
     }
     if (any_upd) {
       double tot[2 * K];
-      if (!reliable_update<K, true>(a, s0, s1, upd, false, slot, sm, tot)) return;
+      if (!reliable_update<K, true>(a, team, upd, false, slot, sm, tot)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!upd[k]) continue;
@@ -382,9 +386,9 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
         if (left[k])
           st_vec(a.x[k] + row_, ld_vec(a.x[k] + row_) + static_cast<double>(ld_vec(a.xs[k] + row_)));
     }
-    if (!grid_sync(a.gs)) return;
+    if (!grid_sync(team.gs)) return;
   }
-  finish<K, true>(a, s0, s1, iters, status, refine, conv, bnorm, slot, sm);
+  finish<K, true>(a, team, iters, status, refine, conv, bnorm, slot, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -393,17 +397,17 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
 template <int K>
 __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
   __shared__ double sm[kMaxNV * 32];
-  const int n = a.n;
+  const Team team = make_team(a.team, a.gs, a.A32.nslices, a.n);
+  const int n = team.row_end;
   const int lane = threadIdx.x & 31;
-  int s0, s1;
-  block_slices(a.A32.nslices, &s0, &s1);
+  const int s0 = team.s0, s1 = team.s1;
   int slot = 0;
   bool act[K];
   double conv[K], bnorm[K], alpha[K], w[K], rr0[K], beta[K], rmax[K];
   int iters[K], status[K], refine[K];
   {
     double bm[K], bb[K];
-    if (!setup<K>(a, s0, s1, slot, sm, bm, bb)) return;
+    if (!setup<K>(a, team, slot, sm, bm, bb)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       bnorm[k] = sqrt(bb[k]);
@@ -416,7 +420,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
   }
   {
     double tot[2 * K];
-    if (!reliable_update<K, false>(a, s0, s1, act, true, slot, sm, tot)) return;
+    if (!reliable_update<K, false>(a, team, act, true, slot, sm, tot)) return;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       rmax[k] = sqrt(tot[2 * k]);
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
           acc[2 * k + 1] += static_cast<double>(y[k]) * r0k;
         }
       }
-      if (!reduce_step<2 * K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<2 * K>(a.part, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
           acc[k] += static_cast<double>(rk) * static_cast<double>(rk);
         }
       }
-      if (!reduce_step<K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<K>(a.part, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         upd[k] = act[k] && sqrt(tot[k]) < conv[k];
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
     }
     if (any_upd) {  // half-step convergence claimed: check the true residual
       double tot[2 * K];
-      if (!reliable_update<K, false>(a, s0, s1, upd, false, slot, sm, tot)) return;
+      if (!reliable_update<K, false>(a, team, upd, false, slot, sm, tot)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!upd[k]) continue;
@@ -516,7 +520,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
           acc[2 * k + 1] += static_cast<double>(y[k]) * static_cast<double>(y[k]);
         }
       }
-      if (!reduce_step<2 * K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<2 * K>(a.part, team, slot, acc, tot, sm)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -545,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
           acc[2 * k + 1] += static_cast<double>(rk) * static_cast<double>(ld_vec(a.r0[k] + row_));
         }
       }
-      if (!reduce_step<2 * K>(a.part, a.gs, slot, acc, tot, sm)) return;
+      if (!reduce_team<2 * K>(a.part, team, slot, acc, tot, sm)) return;
       any_upd = false;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -561,7 +565,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
     }
     if (any_upd) {
       double tot[2 * K];
-      if (!reliable_update<K, false>(a, s0, s1, upd, false, slot, sm, tot)) return;
+      if (!reliable_update<K, false>(a, team, upd, false, slot, sm, tot)) return;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!upd[k]) continue;
@@ -600,7 +604,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
         st_vec(a.z[k] + row_, ld_vec(a.m32[k] + row_) * pk);
       }
     }
-    if (!grid_sync(a.gs)) return;
+    if (!grid_sync(team.gs)) return;
   }
   bool left[K];
   bool any_left = false;
@@ -620,9 +624,9 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
         if (left[k])
           st_vec(a.x[k] + row_, ld_vec(a.x[k] + row_) + static_cast<double>(ld_vec(a.xs[k] + row_)));
     }
-    if (!grid_sync(a.gs)) return;
+    if (!grid_sync(team.gs)) return;
   }
-  finish<K, false>(a, s0, s1, iters, status, refine, conv, bnorm, slot, sm);
+  finish<K, false>(a, team, iters, status, refine, conv, bnorm, slot, sm);
 }
 
 // --------------------------------------------------------------- host ---
@@ -711,6 +715,68 @@ int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const do
 }
 
 }  // namespace
+
+// ---- batched (team) launch, K = 1, capturable (no host synchronisation).
+size_t team_ws_bytes_mixed(int n, int grid) {
+  auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  return align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs) +
+         align(sizeof(double) * 2 * kMaxNV * static_cast<size_t>(grid));
+}
+
+int team_max_grid_mixed(int32_t solver, int device) {
+  void (*kern)(MixedArgs) = solver == SFR_PCG ? pcg_mixed_kernel<1> : bicgstab_mixed_kernel<1>;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0) != cudaSuccess)
+    return 0;
+  return occ * num_sms(device);
+}
+
+int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double *d_x, double tol,
+                       uint32_t maxit, int32_t newx, const TeamTable &team, int grid, void *ws,
+                       SolveOut *d_out, unsigned *ctl, cudaStream_t st) {
+  const int n = s->n;
+  auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  float *vec = static_cast<float *>(ws);
+  auto V = [&](int which) { return vec + static_cast<size_t>(which) * n; };
+  MixedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.A64 = SellView<double>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val, nullptr};
+  a.A32 = SellView<float>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val32, nullptr};
+  a.n = n;
+  a.diag64[0] = s->d_diag;
+  a.b[0] = d_b;
+  a.x[0] = d_x;
+  a.d32[0] = V(0);
+  a.m32[0] = V(1);
+  a.r[0] = V(2);
+  a.z[0] = V(3);
+  a.p0[0] = V(4);
+  a.p1[0] = V(5);
+  a.q[0] = V(6);
+  a.xs[0] = V(7);
+  a.r0[0] = V(8);
+  a.t[0] = V(9);
+  a.part = reinterpret_cast<double *>(static_cast<char *>(ws) +
+                                      align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs));
+  a.gs.count = ctl;
+  a.gs.gen = ctl + 1;
+  a.gs.err = reinterpret_cast<int *>(ctl + 2);
+  a.gs.nblocks = grid;
+  a.gs.spin_limit = 1u << 22;
+  a.team = team;
+  a.out = d_out;
+  a.tol = tol;
+  a.delta = g_delta;
+  a.maxit = maxit;
+  a.newx = newx;
+  if (cudaMemsetAsync(ctl, 0, 64, st) != cudaSuccess) return SFR_CUDA_ERROR;
+  void (*kern)(MixedArgs) = solver == SFR_PCG ? pcg_mixed_kernel<1> : bicgstab_mixed_kernel<1>;
+  void *params[] = {&a};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), dim3(grid), dim3(kThreads),
+                                     params, 0, st) == cudaSuccess
+             ? SFR_OK
+             : SFR_CUDA_ERROR;
+}
 
 int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                 const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,

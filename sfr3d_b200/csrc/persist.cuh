@@ -27,6 +27,64 @@ struct SolveOut {
     for (int row_ = s_ * kWarp + (threadIdx.x & 31), once_ = 1; once_; once_ = 0) \
       if (row_ < n)
 
+// A team is the set of blocks that solve one system together.  A launch for
+// one system is a single team of every block; a batched launch gives each
+// system its own team, with its own slice range, reductions over its own
+// blocks and its own barrier, so the systems run independently.
+struct TeamTable {
+  const int4 *block;   // per block {first slice, end slice, first block, end block}
+  const int2 *sys;     // per block {system, end row}
+  unsigned int *bar;   // per system {barrier count, generation}
+};
+
+struct Team {
+  int s0, s1;   // this block's slices
+  int b0, b1;   // the team's blocks
+  int sys;      // system index (0 for a single system)
+  int row_end;  // rows of the system end here (global row numbering)
+  GridSync gs;  // the team's barrier
+};
+
+__device__ __forceinline__ Team make_team(const TeamTable &tt, const GridSync &global,
+                                          int nslices, int n) {
+  Team t;
+  t.gs = global;
+  if (!tt.block) {
+    block_slices(nslices, &t.s0, &t.s1);
+    t.b0 = 0;
+    t.b1 = gridDim.x;
+    t.sys = 0;
+    t.row_end = n;
+  } else {
+    const int4 e = tt.block[blockIdx.x];
+    const int2 y = tt.sys[blockIdx.x];
+    t.s0 = e.x;
+    t.s1 = e.y;
+    t.b0 = e.z;
+    t.b1 = e.w;
+    t.sys = y.x;
+    t.row_end = y.y;
+    t.gs.count = tt.bar + 2 * t.sys;
+    t.gs.gen = tt.bar + 2 * t.sys + 1;
+    t.gs.nblocks = static_cast<unsigned>(t.b1 - t.b0);
+  }
+  return t;
+}
+
+// NV block partials -> the team's barrier -> totals over the team's blocks
+// in a fixed order.  False when the barrier failed.
+template <int NV>
+__device__ __forceinline__ bool reduce_team(double *part, const Team &t, int &slot,
+                                            double (&acc)[NV], double (&tot)[NV], double *sm) {
+  const int G = gridDim.x;
+  double *base = part + static_cast<size_t>(slot) * kMaxNV * G;
+  block_partials<NV>(acc, base, G, sm);
+  if (!grid_sync(t.gs)) return false;
+  grid_totals<NV>(base + t.b0, G, t.b1 - t.b0, tot, sm);
+  slot ^= 1;
+  return true;
+}
+
 // Write NV block partials into the next slot, wait at the grid barrier, and
 // total them (same order in every block).  False when the barrier failed.
 template <int NV>

@@ -90,6 +90,16 @@ def lib() -> ctypes.CDLL:
                               _P, _P, _P, _P, ctypes.c_double, ctypes.c_uint32,
                               ctypes.c_int16, ctypes.c_int16, _P, ctypes.c_bool,
                               ctypes.c_bool, ctypes.c_bool, ctypes.c_char_p]
+    L.sfr_gpu_batch_create.argtypes = [_I32, _P, _P, _P, _P, _I32, _I32, _I32,
+                                       ctypes.POINTER(_P)]
+    L.sfr_gpu_batch_set_values.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_batch_solve.argtypes = [_P, _I32, _P, _P, ctypes.c_double,
+                                      ctypes.c_uint32, _I32, _I32, _P]
+    L.sfr_gpu_batch_set_weights.argtypes = [_P, _P]
+    L.sfr_gpu_batch_autotune.argtypes = [_P, _I32, _P, ctypes.c_double,
+                                         ctypes.c_uint32, _I32, _P]
+    L.sfr_gpu_batch_stats.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_batch_destroy.argtypes = [_P]
     L.sfr_set_exit_on_failure.argtypes = [_I32]
     L.sfr_set_exit_on_failure.restype = None
     L.sfr_set_precision.argtypes = [_I32]
@@ -242,6 +252,88 @@ class GpuSystem:
         lib().sfr_gpu_stats(self.h, ctypes.byref(b), ctypes.byref(s),
                             ctypes.byref(w))
         return {"device_bytes": b.value, "slots": s.value, "bandwidth": w.value}
+
+
+def _ptr_array(arrays):
+    arr = (_P * len(arrays))()
+    for i, a in enumerate(arrays):
+        arr[i] = None if a is None else a.ctypes.data
+    return arr
+
+
+class GpuBatch:
+    """Many independent systems solved in one persistent launch
+    (sfr_gpu_batch_*).  `systems` is a list of (neq, ia, ja) in one storage."""
+
+    def __init__(self, systems, storage: int, unsym: bool, device: int = 0):
+        self.nsys = len(systems)
+        self._keep = []
+        neq = np.array([s[0] for s in systems], np.int32)
+        ias = [_i32(s[1]) for s in systems]
+        jas = [_i32(s[2]) for s in systems]
+        nad = np.array([len(j) for j in jas], np.int32)
+        self._keep += [neq, nad, ias, jas]
+        self.neq = neq
+        h = _P()
+        rc = lib().sfr_gpu_batch_create(self.nsys, _ptr(neq), _ptr(nad),
+                                        _ptr_array(ias), _ptr_array(jas),
+                                        storage, int(unsym), device,
+                                        ctypes.byref(h))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sfr_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_values(self, als, ads, aus=None):
+        als = [_f64(a) for a in als]
+        ads = [_f64(a) for a in ads]
+        aus = None if aus is None else [_f64(a) for a in aus]
+        rc = lib().sfr_gpu_batch_set_values(self.h, _ptr_array(als), _ptr_array(ads),
+                                            None if aus is None else _ptr_array(aus))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_batch_set_values")
+
+    def solve(self, solver, bs, x0s=None, tol=1e-10, maxit=100000, newx=True,
+              precision=FP64, raise_on_error=True):
+        bs = [_f64(b) for b in bs]
+        xs = ([np.zeros(int(n)) for n in self.neq] if x0s is None
+              else [np.array(x, dtype=np.float64) for x in x0s])
+        infos = (SolveInfoC * self.nsys)()
+        rc = lib().sfr_gpu_batch_solve(self.h, solver, _ptr_array(bs), _ptr_array(xs),
+                                       tol, maxit, int(newx), precision, infos)
+        if rc < 0 and raise_on_error:
+            raise SolverError(rc, "sfr_gpu_batch_solve")
+        return xs, [SolveInfo.from_c(infos[i]) for i in range(self.nsys)]
+
+    def set_weights(self, w):
+        w = _f64(w)
+        rc = lib().sfr_gpu_batch_set_weights(self.h, _ptr(w))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_batch_set_weights")
+
+    def autotune(self, solver, bs, tol=1e-10, maxit=100000, precision=FP64) -> float:
+        bs = [_f64(b) for b in bs]
+        ms = ctypes.c_double()
+        rc = lib().sfr_gpu_batch_autotune(self.h, solver, _ptr_array(bs), tol, maxit,
+                                          precision, ctypes.byref(ms))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_batch_autotune")
+        return ms.value
+
+    def stats(self):
+        g, r, b = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        lib().sfr_gpu_batch_stats(self.h, ctypes.byref(g), ctypes.byref(r), ctypes.byref(b))
+        return {"grid": g.value, "rows": r.value, "device_bytes": b.value}
 
 
 def dot(d_a: int, d_b: int, n: int, stream: int = 0) -> float:

@@ -73,3 +73,12 @@ def test_solverC_rejects_unsupported_solver_without_exiting():
     rc = sv.solverC(2, 2, 1, 0, ia, ja, np.ones(1), np.ones(2), None,
                     np.ones(2), x, 1e-10, 10, sv.CSRD, 4, exit_on_failure=False)
     assert rc == sv.UNSUPPORTED
+
+
+def test_batch_create_validates_every_system():
+    good = (2, np.array([0, 0, 1], np.int32), np.array([0], np.int32))
+    bad = (2, np.array([0, 1, 0], np.int32), np.array([0], np.int32))
+    with pytest.raises(sv.SolverError) as e:
+        sv.GpuBatch([good, bad], sv.CSRD, False)
+    assert e.value.status == sv.BAD_INPUT
+    assert "system 1" in sv.last_error()
