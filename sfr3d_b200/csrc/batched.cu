@@ -320,6 +320,8 @@ int sfr_gpu_batch_set_values(sfr_batch *b, const double *const *al, const double
   }
   int rc = sfr::gather_values(&c, &c.A, c.stream);
   if (rc != SFR_OK) return rc;
+  rc = sfr::row_compensation(&c, c.A, c.stream);
+  if (rc != SFR_OK) return rc;
   if (sfr::convert_diag32(c.d_diag, c.d_diag32, c.n, c.stream) != cudaSuccess ||
       cudaStreamSynchronize(c.stream) != cudaSuccess)
     return SFR_CUDA_ERROR;
@@ -439,6 +441,7 @@ int sfr_gpu_batch_destroy(sfr_batch *b) {
   cudaFree(b->cat.d_stage);
   cudaFree(b->cat.d_diag);
   cudaFree(b->cat.d_diag32);
+  cudaFree(b->cat.d_comp);
   if (b->cat.stream) cudaStreamDestroy(b->cat.stream);
   cudaFree(b->d_block);
   cudaFree(b->d_sys);

@@ -166,6 +166,8 @@ int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const 
   SFR_CU(cudaMemcpyAsync(s->d_diag, ad, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
   int rc = sfr::gather_values(s, &s->A, s->stream);
   if (rc != SFR_OK) return rc;
+  rc = sfr::row_compensation(s, s->A, s->stream);
+  if (rc != SFR_OK) return rc;
   if (s->at_ready) {
     rc = sfr::gather_values(s, &s->At, s->stream);
     if (rc != SFR_OK) return rc;
@@ -251,6 +253,7 @@ int sfr_gpu_destroy(sfr_system *s) {
   cudaFree(s->d_stage);
   cudaFree(s->d_diag);
   cudaFree(s->d_diag32);
+  cudaFree(s->d_comp);
   cudaFree(s->ws.base);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;

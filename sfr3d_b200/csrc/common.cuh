@@ -183,15 +183,15 @@ __device__ __forceinline__ double row_spmv_exact(const SellView<V> &A, int s, in
 }
 
 // y_k[row] = diag*v(row) + sum_e val_e * v(col_e) for K vectors given by a
-// gather functor g(k, col): exact FP64 (the reference's rounding) or FP32
-// with FMA.  A row's column indices and values are loaded six at a time
-// before any gather, so all of them are in flight together.
-template <int K, bool kExact, typename V, typename G>
-__device__ __forceinline__ void row_product(const int *sptr, const int *colp, const V *valp,
-                                            const V *const *diagp, int s, int lane,
-                                            const int (&act)[K], G g,
-                                            typename std::conditional<kExact, double, float>::type (&y)[K]) {
-  using T = typename std::conditional<kExact, double, float>::type;
+// gather functor g(k, col), accumulated in Acc: exact FP64 (kExact: the
+// reference's rounding, one rounding per product and per sum), or with FMA.
+// Values may be FP32 with FP64 accumulation (the mixed path).  A row's column
+// indices and values are loaded six at a time before any gather, so all of
+// them are in flight together.
+template <int K, typename Acc, bool kExact, typename V, typename DV, typename G>
+__device__ __forceinline__ void row_product_t(const int *sptr, const int *colp, const V *valp,
+                                              const DV *const *diagp, int s, int lane,
+                                              const int (&act)[K], G g, Acc (&y)[K]) {
   const int row = s * kWarp + lane;
   const int base = __ldg(sptr + s);
   const int w = (__ldg(sptr + s + 1) - base) >> 5;
@@ -200,17 +200,18 @@ __device__ __forceinline__ void row_product(const int *sptr, const int *colp, co
 #pragma unroll
   for (int k = 0; k < K; ++k)
     if (act[k]) {
-      const T dv = static_cast<T>(ld_vec(diagp[k] + row));
-      y[k] = kExact ? xmul(dv, g(k, row)) : dv * g(k, row);
+      const Acc dv = static_cast<Acc>(ld_vec(diagp[k] + row));
+      const Acc gv = static_cast<Acc>(g(k, row));
+      y[k] = kExact ? xmul(dv, gv) : dv * gv;
     }
   for (int e0 = 0; e0 < w; e0 += 6) {
     int jj[6];
-    T vv[6];
+    Acc vv[6];
 #pragma unroll
     for (int u = 0; u < 6; ++u)
       if (e0 + u < w) {
         jj[u] = ld_stream(c + (e0 + u) * kWarp);
-        vv[u] = static_cast<T>(ld_stream(v + (e0 + u) * kWarp));
+        vv[u] = static_cast<Acc>(ld_stream(v + (e0 + u) * kWarp));
       }
 #pragma unroll
     for (int u = 0; u < 6; ++u)
@@ -218,13 +219,21 @@ __device__ __forceinline__ void row_product(const int *sptr, const int *colp, co
 #pragma unroll
         for (int k = 0; k < K; ++k)
           if (act[k]) {
-            const T gv = g(k, jj[u]);
-            y[k] = kExact ? xadd(y[k], xmul(vv[u], gv)) : fmaf(vv[u], gv, y[k]);
+            const Acc gv = static_cast<Acc>(g(k, jj[u]));
+            y[k] = kExact ? xadd(y[k], xmul(vv[u], gv)) : fma(vv[u], gv, y[k]);
           }
       }
   }
 }
 
+template <int K, bool kExact, typename V, typename G>
+__device__ __forceinline__ void row_product(const int *sptr, const int *colp, const V *valp,
+                                            const V *const *diagp, int s, int lane,
+                                            const int (&act)[K], G g,
+                                            typename std::conditional<kExact, double, float>::type (&y)[K]) {
+  using T = typename std::conditional<kExact, double, float>::type;
+  row_product_t<K, T, kExact, V, V>(sptr, colp, valp, diagp, s, lane, act, g, y);
+}
 
 // Block-contiguous slice range of this block.
 __device__ __forceinline__ void block_slices(int nslices, int *first, int *last) {

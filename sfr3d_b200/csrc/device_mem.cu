@@ -38,7 +38,39 @@ __global__ void to_float_kernel(const double *src, float *dst, int n) {
     dst[i] = __double2float_rn(src[i]);
 }
 
+// comp[row] = -sum_e (fl32(val_e) - val_e) over the row's slots: the FP32
+// operator with diagonal (ad + comp) has the same row sums as the FP64 one,
+// so rounding the couplings does not disturb the near-null (smooth) modes
+// of a diffusion operator.
+__global__ void compensation_kernel(const int *sptr, const double *val, int n, int nslices,
+                                    double *comp) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nslices * 32; t += stride) {
+    const int s = t >> 5, lane = t & 31, row = t;
+    if (row >= n) continue;
+    const int base = sptr[s];
+    const int w = (sptr[s + 1] - base) >> 5;
+    double acc = 0.0;
+    for (int k = 0; k < w; ++k) {
+      const double v = val[base + k * 32 + lane];
+      acc += static_cast<double>(__double2float_rn(v)) - v;
+    }
+    comp[row] = -acc;
+  }
+}
+
 }  // namespace
+
+int row_compensation(sfr_system *s, const DevSell &d, cudaStream_t st) {
+  if (!s->d_comp) {
+    if (cudaMalloc(&s->d_comp, sizeof(double) * std::max(s->n, 1)) != cudaSuccess)
+      return SFR_CUDA_ERROR;
+    s->bytes += static_cast<int64_t>(sizeof(double)) * s->n;
+  }
+  const int grid = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(d.nslices) * 32 + 255) / 256, 4096));
+  compensation_kernel<<<std::max(grid, 1), 256, 0, st>>>(d.sptr, d.val, s->n, d.nslices, s->d_comp);
+  return cudaGetLastError() == cudaSuccess ? SFR_OK : SFR_CUDA_ERROR;
+}
 
 int upload_sell(const HostSell &h, DevSell *d, int64_t *bytes) {
   d->n = h.n;

@@ -66,6 +66,9 @@ struct sfr_system {
   bool at_ready = false;
   double *d_stage = nullptr;   // raw al|au
   double *d_diag = nullptr;    // ad
+  // -sum over each row of (fl32(a_ij) - a_ij): added to the diagonal of the
+  // FP32 operator so that it keeps the FP64 row sums (mixed precision)
+  double *d_comp = nullptr;
   float *d_diag32 = nullptr;
   bool values_set = false;
   cudaStream_t stream = nullptr;
@@ -84,6 +87,8 @@ void free_sell(DevSell *d);
 int ensure_workspace(sfr_system *s, size_t bytes);
 int gather_values(sfr_system *s, DevSell *d, cudaStream_t st);
 cudaError_t convert_diag32(const double *src, float *dst, int n, cudaStream_t st);
+// d_comp from the FP64 and FP32 values of d (allocates d_comp on first use)
+int row_compensation(sfr_system *s, const DevSell &d, cudaStream_t st);
 
 // kernels / solvers (krylov.cu)
 int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,

@@ -33,7 +33,8 @@ struct MixedArgs {
   const double *diag64[kMaxK];
   const double *b[kMaxK];
   double *x[kMaxK];
-  float *d32[kMaxK];  // FP32 diagonal
+  double *dc[kMaxK];  // diagonal of the FP32 operator: ad + row compensation (FP64)
+  const double *comp; // -sum_row (fl32(a_ij) - a_ij)
   float *m32[kMaxK];  // FP32 Jacobi 1/diag
   float *r[kMaxK];    // inner residual
   float *z[kMaxK];    // PCG: M r ; BiCGSTAB: M p
@@ -53,26 +54,22 @@ struct MixedArgs {
   int newx;
 };
 
-// y_k = (A32 v_k)[row], FP32 with FMA.
+// y_k = (A32 v_k)[row]: FP32 couplings and FP32 vectors, accumulated in FP64
+// around the compensated FP64 diagonal (so the FP32 operator keeps the FP64
+// row sums), rounded to FP32 once.
 template <int K, typename Gather>
 __device__ __forceinline__ void row_spmv32(const MixedArgs &a, int s, int lane, const bool (&act)[K],
                                            Gather g, float (&y)[K]) {
-  const int row = s * kWarp + lane;
-  const int base = __ldg(a.A32.sptr + s);
-  const int w = (__ldg(a.A32.sptr + s + 1) - base) >> 5;
+  int ia[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) ia[k] = act[k];
+  double yd[K];
+  const double *const *dc = a.dc;
+  row_product_t<K, double, false, float, double>(a.A32.sptr, a.A32.col, a.A32.val, dc, s, lane,
+                                                 ia, g, yd);
 #pragma unroll
   for (int k = 0; k < K; ++k)
-    if (act[k]) y[k] = ld_vec(a.d32[k] + row) * g(k, row);
-  const int *c = a.A32.col + base + lane;
-  const float *v = a.A32.val + base + lane;
-#pragma unroll 2
-  for (int e = 0; e < w; ++e) {
-    const int j = ld_stream(c + e * kWarp);
-    const float av = ld_stream(v + e * kWarp);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-      if (act[k]) y[k] = fmaf(av, g(k, j), y[k]);
-  }
+    if (act[k]) y[k] = __double2float_rn(yd[k]);
 }
 
 // (A64 x_k)[row] in FP64 (FMA allowed: this is the refinement residual).
@@ -201,7 +198,7 @@ __device__ bool setup(const MixedArgs &a, const Team &t, int &slot, double *sm,
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const double dk = ld_vec(a.diag64[k] + row_);
-      st_vec(a.d32[k] + row_, __double2float_rn(dk));
+      st_vec(a.dc[k] + row_, dk + ld_vec(a.comp + row_));
       st_vec(a.m32[k] + row_, __double2float_rn(1.0 / dk));
       if (a.newx) st_vec(a.x[k] + row_, 0.0);
       const double bk = ld_vec(a.b[k] + row_);
@@ -630,7 +627,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
 }
 
 // --------------------------------------------------------------- host ---
-constexpr int kFloatVecs = 10;  // d32 m32 r z p0 p1 q xs r0 t
+constexpr int kFloatVecs = 10;  // (unused) m32 r z p0 p1 q xs r0 t
 
 double g_delta = 0.1;
 
@@ -648,14 +645,16 @@ int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const do
   const int warps = kThreads / kWarp;
   const int grid = std::max(1, std::min(max_grid, (s->A.nslices + warps - 1) / warps));
   auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
-  const size_t vec_bytes = align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs * K);
+  const size_t dc_bytes = align(sizeof(double) * static_cast<size_t>(n) * K);
+  const size_t vec_bytes = dc_bytes + align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs * K);
   const size_t part_bytes = align(sizeof(double) * 2 * kMaxNV * static_cast<size_t>(grid));
   const size_t ctl_bytes = 256;
   const size_t out_bytes = align(sizeof(SolveOut) * kMaxK);
   int rc = ensure_workspace(s, vec_bytes + part_bytes + ctl_bytes + out_bytes);
   if (rc != SFR_OK) return rc;
   char *base = static_cast<char *>(s->ws.base);
-  float *vec = reinterpret_cast<float *>(base);
+  double *dcv = reinterpret_cast<double *>(base);
+  float *vec = reinterpret_cast<float *>(base + dc_bytes);
   auto V = [&](int which, int k) { return vec + (static_cast<size_t>(which) * K + k) * n; };
 
   MixedArgs a;
@@ -663,11 +662,12 @@ int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const do
   a.A64 = SellView<double>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val, nullptr};
   a.A32 = SellView<float>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val32, nullptr};
   a.n = n;
+  a.comp = s->d_comp;
   for (int k = 0; k < K; ++k) {
     a.diag64[k] = d_diag_k ? d_diag_k + static_cast<size_t>(k) * n : s->d_diag;
     a.b[k] = d_b + static_cast<size_t>(k) * n;
     a.x[k] = d_x + static_cast<size_t>(k) * n;
-    a.d32[k] = V(0, k);
+    a.dc[k] = dcv + static_cast<size_t>(k) * n;
     a.m32[k] = V(1, k);
     a.r[k] = V(2, k);
     a.z[k] = V(3, k);
@@ -719,7 +719,8 @@ int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const do
 // ---- batched (team) launch, K = 1, capturable (no host synchronisation).
 size_t team_ws_bytes_mixed(int n, int grid) {
   auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
-  return align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs) +
+  return align(sizeof(double) * static_cast<size_t>(n)) +
+         align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs) +
          align(sizeof(double) * 2 * kMaxNV * static_cast<size_t>(grid));
 }
 
@@ -736,7 +737,9 @@ int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double 
                        SolveOut *d_out, unsigned *ctl, cudaStream_t st) {
   const int n = s->n;
   auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
-  float *vec = static_cast<float *>(ws);
+  const size_t dc_bytes = align(sizeof(double) * static_cast<size_t>(n));
+  double *dcv = static_cast<double *>(ws);
+  float *vec = reinterpret_cast<float *>(static_cast<char *>(ws) + dc_bytes);
   auto V = [&](int which) { return vec + static_cast<size_t>(which) * n; };
   MixedArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -744,9 +747,10 @@ int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double 
   a.A32 = SellView<float>{s->A.n, s->A.nslices, s->A.sptr, s->A.col, s->A.val32, nullptr};
   a.n = n;
   a.diag64[0] = s->d_diag;
+  a.comp = s->d_comp;
   a.b[0] = d_b;
   a.x[0] = d_x;
-  a.d32[0] = V(0);
+  a.dc[0] = dcv;
   a.m32[0] = V(1);
   a.r[0] = V(2);
   a.z[0] = V(3);
@@ -756,7 +760,7 @@ int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double 
   a.xs[0] = V(7);
   a.r0[0] = V(8);
   a.t[0] = V(9);
-  a.part = reinterpret_cast<double *>(static_cast<char *>(ws) +
+  a.part = reinterpret_cast<double *>(static_cast<char *>(ws) + dc_bytes +
                                       align(sizeof(float) * static_cast<size_t>(n) * kFloatVecs));
   a.gs.count = ctl;
   a.gs.gen = ctl + 1;

@@ -48,8 +48,10 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   const float *val32;
   // the graph's own padded workspace (rows padded to a multiple of 4)
   double *diag64[K], *b[K], *x[K];
+  double *dc[K];        // mixed: diagonal of the FP32 operator, ad + compensation
+  const double *comp;   // mixed: -sum_row (fl32(a_ij) - a_ij)
   double *m[K], *r[K], *z[K], *q[K], *p0[K], *p1[K], *r0[K], *t[K];
-  float *d32[K], *m32[K], *fr[K], *fz[K], *fq[K], *fp0[K], *fp1[K], *fxs[K], *fr0[K], *ft[K];
+  float *m32[K], *fr[K], *fz[K], *fq[K], *fp0[K], *fp1[K], *fxs[K], *fr0[K], *ft[K];
   double *part;
   unsigned *counter;
   cudaGraphConditionalHandle hwhile, hif, hif2;
@@ -161,7 +163,8 @@ __global__ void __launch_bounds__(256) k_setup(const SArgs<K> a, SState<K> *st) 
       const double2 dk = ld2ro(a.diag64[k] + r);
       const double2 mk = make_double2(1.0 / dk.x, 1.0 / dk.y);
       if (kMixed) {
-        st2(a.d32[k] + r, make_float2(__double2float_rn(dk.x), __double2float_rn(dk.y)));
+        const double2 ck = ld2ro(a.comp + r);
+        st2(a.dc[k] + r, make_double2(dk.x + ck.x, dk.y + ck.y));
         st2(a.m32[k] + r, make_float2(__double2float_rn(mk.x), __double2float_rn(mk.y)));
       } else {
         st2(a.m[k] + r, mk);
@@ -273,16 +276,18 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
       }
     }
   } else {
-    const float *const *d32 = a.d32;
+    const double *const *dc = a.dc;
     SFR_FOR_OWN_ROWS(s0, s1) {
-      float y[K];
-      row_product<K, false, float>(a.sptr, a.col, a.val32, d32, s_, lane, act,
-                                   [&](int k, int c) { return ld_ro(a.fp0[k] + c); }, y);
+      double y[K];
+      row_product_t<K, double, false, float, double>(
+          a.sptr, a.col, a.val32, dc, s_, lane, act,
+          [&](int k, int c) { return ld_ro(a.fp0[k] + c); }, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
-        st_vec(a.fq[k] + row_, y[k]);
-        acc[k] += static_cast<double>(y[k]) * static_cast<double>(ld_ro(a.fp0[k] + row_));
+        const float yf = __double2float_rn(y[k]);
+        st_vec(a.fq[k] + row_, yf);
+        acc[k] += static_cast<double>(yf) * static_cast<double>(ld_ro(a.fp0[k] + row_));
       }
     }
   }
@@ -650,8 +655,15 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
       }
     } else {
       float y[K];
-      row_product<K, false, float>(a.sptr, a.col, a.val32, a.d32, s_, lane, act,
-                                   [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
+      {
+        double yd[K];
+        const double *const *dc = a.dc;
+        row_product_t<K, double, false, float, double>(
+            a.sptr, a.col, a.val32, dc, s_, lane, act,
+            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
+#pragma unroll
+        for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
+      }
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -848,8 +860,15 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
       }
     } else {
       float y[K];
-      row_product<K, false, float>(a.sptr, a.col, a.val32, a.d32, s_, lane, act,
-                                   [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
+      {
+        double yd[K];
+        const double *const *dc = a.dc;
+        row_product_t<K, double, false, float, double>(
+            a.sptr, a.col, a.val32, dc, s_, lane, act,
+            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
+#pragma unroll
+        for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
+      }
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -1075,8 +1094,8 @@ cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t *prev, cudaGraphCondi
   } while (0)
 
 constexpr int kVecs64Plain = 11;  // diag b x m r z q p0 p1 r0 t
-constexpr int kVecs64Mixed = 3;   // diag b x
-constexpr int kVecs32 = 10;       // d32 m32 r z q p0 p1 xs r0 t
+constexpr int kVecs64Mixed = 4;   // diag b x dc
+constexpr int kVecs32 = 10;       // (unused) m32 r z q p0 p1 xs r0 t
 
 inline int64_t padded(int n) { return (static_cast<int64_t>(n) + 3) & ~static_cast<int64_t>(3); }
 
@@ -1113,6 +1132,7 @@ cudaError_t prepare(sfr_system *s, int precision, int threads, int spw, CachedGr
   a.col = s->A.col;
   a.val64 = s->A.val;
   a.val32 = s->A.val32;
+  a.comp = s->d_comp;
   double *v64 = static_cast<double *>(cg->ws);
   float *v32 = reinterpret_cast<float *>(static_cast<char *>(cg->ws) + bytes64);
   for (int k = 0; k < K; ++k) {
@@ -1122,7 +1142,7 @@ cudaError_t prepare(sfr_system *s, int precision, int threads, int spw, CachedGr
     a.b[k] = D(1);
     a.x[k] = D(2);
     if (mixed) {
-      a.d32[k] = F(0);
+      a.dc[k] = D(3);
       a.m32[k] = F(1);
       a.fr[k] = F(2);
       a.fz[k] = F(3);
