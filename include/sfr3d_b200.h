@@ -125,6 +125,25 @@ int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
                        int32_t slices_per_warp);
 
+/* Solve A^T x = b (host arrays) with the same Krylov path.  The reference
+ * has no transpose solve; this serves the adjoint below. */
+int sfr_gpu_solve_transpose(sfr_system *s, int32_t solver, const double *b,
+                            double *x, double tol, uint32_t maxit,
+                            int32_t newx, int32_t precision,
+                            sfr_solve_info *info);
+
+/* Adjoint of x = A^-1 b for a scalar J with g = dJ/dx (host arrays):
+ * solves A^T lam = g and returns dJ/db = lam (n) and dJ/dA_ij = -lam_i x_j
+ * on the stored pattern, in the layout sfr_gpu_set_values takes: g_al like
+ * al, g_ad like ad, g_au like au (CSRC unsym).  An entry stored once for two
+ * mirrored positions (strict-lower storage of a symmetric matrix) gets both
+ * terms.  Any gradient pointer may be NULL.  No counterpart in the
+ * reference. */
+int sfr_gpu_adjoint(sfr_system *s, int32_t solver, const double *x,
+                    const double *g, double *lam, double *g_al, double *g_ad,
+                    double *g_au, double tol, uint32_t maxit,
+                    int32_t precision, sfr_solve_info *info);
+
 int sfr_gpu_destroy(sfr_system *s);
 
 /* ---- batches of independent systems ----------------------------------- */

@@ -2,6 +2,7 @@
 // include/sfr3d_b200.h) and the solverC drop-in.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
@@ -175,6 +176,7 @@ int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const 
   SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
   SFR_CU(cudaStreamSynchronize(s->stream));
   s->values_set = true;
+  if (s->tview) s->tview->comp_stale = true;
   return SFR_OK;
 }
 
@@ -246,18 +248,126 @@ int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads, int32_t s
 int sfr_gpu_destroy(sfr_system *s) {
   if (!s) return SFR_OK;
   cudaSetDevice(s->device);
+  if (s->tview) sfr_gpu_destroy(s->tview);
   sfr::release_stream_engine(s);
   io_release(s);
-  sfr::free_sell(&s->A);
-  sfr::free_sell(&s->At);
-  cudaFree(s->d_stage);
-  cudaFree(s->d_diag);
-  cudaFree(s->d_diag32);
+  if (!s->borrowed) {
+    sfr::free_sell(&s->A);
+    sfr::free_sell(&s->At);
+    cudaFree(s->d_stage);
+    cudaFree(s->d_diag);
+    cudaFree(s->d_diag32);
+  }
   cudaFree(s->d_comp);
   cudaFree(s->ws.base);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return SFR_OK;
+}
+
+namespace {
+
+// The transposed system: shares A^T (uploaded on first use), the diagonal
+// and the value staging of `s`; owns its workspace and compensation.
+int transpose_view(sfr_system *s, sfr_system **out) {
+  int rc = ensure_transpose(s);
+  if (rc != SFR_OK) return rc;
+  if (!s->tview) {
+    auto *t = new sfr_system;
+    t->borrowed = true;
+    t->device = s->device;
+    t->n = s->n;
+    t->storage = s->storage;
+    t->unsym = s->unsym;
+    t->nad = s->nad;
+    t->nsrc = s->nsrc;
+    t->bandwidth = s->bandwidth;
+    t->A = s->At;
+    t->d_stage = s->d_stage;
+    t->d_diag = s->d_diag;
+    t->d_diag32 = s->d_diag32;
+    if (cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete t;
+      return SFR_CUDA_ERROR;
+    }
+    s->tview = t;
+  }
+  sfr_system *t = s->tview;
+  t->values_set = s->values_set;
+  t->engine = s->engine;
+  t->graph_threads = s->graph_threads;
+  t->graph_spw = s->graph_spw;
+  if (t->comp_stale && s->values_set) {
+    rc = sfr::row_compensation(t, t->A, t->stream);
+    if (rc != SFR_OK) return rc;
+    if (cudaStreamSynchronize(t->stream) != cudaSuccess) return SFR_CUDA_ERROR;
+    t->comp_stale = false;
+  }
+  *out = t;
+  return SFR_OK;
+}
+
+}  // namespace
+
+int sfr_gpu_solve_transpose(sfr_system *s, int32_t solver, const double *b, double *x, double tol,
+                            uint32_t maxit, int32_t newx, int32_t precision,
+                            sfr_solve_info *info) {
+  if (!s || !b || !x) return SFR_BAD_INPUT;
+  if (!s->values_set) return SFR_BAD_INPUT;
+  SFR_CU(cudaSetDevice(s->device));
+  sfr_system *t = nullptr;
+  int rc = transpose_view(s, &t);
+  if (rc != SFR_OK) return rc;
+  return sfr_gpu_solve_multi(t, solver, 1, nullptr, b, x, tol, maxit, newx, precision, info);
+}
+
+int sfr_gpu_adjoint(sfr_system *s, int32_t solver, const double *x, const double *g,
+                    double *lam, double *g_al, double *g_ad, double *g_au, double tol,
+                    uint32_t maxit, int32_t precision, sfr_solve_info *info) {
+  if (!s || !x || !g || !lam) return SFR_BAD_INPUT;
+  const bool split = s->storage == SFR_CSRC && s->unsym;
+  if (std::all_of(g, g + s->n, [](double v) { return v == 0.0; })) {
+    // J does not depend on x: lam = 0 and every gradient is 0 (a Krylov
+    // solve of a zero right-hand side would report a breakdown)
+    std::fill(lam, lam + s->n, 0.0);
+    const size_t nl = split ? static_cast<size_t>(s->nsrc) / 2 : static_cast<size_t>(s->nsrc);
+    if (g_al) std::fill(g_al, g_al + nl, 0.0);
+    if (g_au && split) std::fill(g_au, g_au + nl, 0.0);
+    if (g_ad) std::fill(g_ad, g_ad + s->n, 0.0);
+    if (info) *info = sfr_solve_info{};
+    return SFR_OK;
+  }
+  int rc = sfr_gpu_solve_transpose(s, solver, g, lam, tol, maxit, 1, precision, info);
+  if (rc != SFR_OK) return rc;
+  if (!g_al && !g_ad && !g_au) return SFR_OK;
+  IoBuffers *io = nullptr;
+  rc = io_for(s, std::max<size_t>(static_cast<size_t>(s->n), static_cast<size_t>(s->nsrc)), &io);
+  if (rc != SFR_OK) return rc;
+  // io->b = lam, io->x = x, io->diag = gradient of the value source
+  double *d_gad = nullptr;
+  SFR_CU(cudaMalloc(&d_gad, sizeof(double) * s->n));
+  cudaError_t e = cudaMemcpyAsync(io->b, lam, sizeof(double) * s->n, cudaMemcpyHostToDevice,
+                                  s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(io->x, x, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) {
+    cudaFree(d_gad);
+    return cuda_fail(e);
+  }
+  rc = sfr::adjoint_gradients(s, io->b, io->x, io->diag, d_gad, s->stream);
+  if (rc == SFR_OK) {
+    const size_t nl = split ? static_cast<size_t>(s->nsrc) / 2 : static_cast<size_t>(s->nsrc);
+    if (g_al) e = cudaMemcpyAsync(g_al, io->diag, sizeof(double) * nl, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && split && g_au)
+      e = cudaMemcpyAsync(g_au, io->diag + nl, sizeof(double) * nl, cudaMemcpyDeviceToHost,
+                          s->stream);
+    if (e == cudaSuccess && g_ad)
+      e = cudaMemcpyAsync(g_ad, d_gad, sizeof(double) * s->n, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) rc = cuda_fail(e);
+  }
+  cudaFree(d_gad);
+  return rc;
 }
 
 int sfr_gpu_spmv(sfr_system *s, const double *d_x, double *d_y, void *stream) {

@@ -73,6 +73,10 @@ struct sfr_system {
   bool values_set = false;
   cudaStream_t stream = nullptr;
   sfr::Workspace ws;
+  // the transposed view used by the adjoint (shares A^T, diagonal, values)
+  sfr_system *tview = nullptr;
+  bool borrowed = false;     // a view: its matrix buffers belong to another handle
+  bool comp_stale = true;    // compensation not yet computed for the current values
   // engine: 0 auto, 1 persistent (one cooperative launch), 2 graph,
   // 3 the graph engine's kernels from a host loop (profiling)
   int32_t engine = 0;
@@ -128,6 +132,9 @@ int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
 int dot_host(const double *d_a, const double *d_b, int32_t n, double *h_out,
              cudaStream_t st);
 int num_sms(int device);
+// adjoint.cu: dJ/d(value source) and dJ/d(ad) from lam and x (device arrays)
+int adjoint_gradients(sfr_system *s, const double *d_lam, const double *d_x, double *d_gsrc,
+                      double *d_gad, cudaStream_t st);
 // Text for sfr_last_error() (capi.cpp)
 void set_last_error(const char *msg);
 }  // namespace sfr

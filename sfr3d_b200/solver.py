@@ -79,6 +79,10 @@ def lib() -> ctypes.CDLL:
     L.sfr_gpu_solve_multi.argtypes = [_P, _I32, _I32, _P, _P, _P,
                                       ctypes.c_double, ctypes.c_uint32, _I32,
                                       _I32, _P]
+    L.sfr_gpu_solve_transpose.argtypes = [_P, _I32, _P, _P, ctypes.c_double,
+                                          ctypes.c_uint32, _I32, _I32, _P]
+    L.sfr_gpu_adjoint.argtypes = [_P, _I32, _P, _P, _P, _P, _P, _P,
+                                  ctypes.c_double, ctypes.c_uint32, _I32, _P]
     L.sfr_gpu_destroy.argtypes = [_P]
     L.sfr_gpu_set_engine.argtypes = [_P, _I32, _I32, _I32]
     L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
@@ -147,6 +151,7 @@ class GpuSystem:
             nad = (int(self._ia[1]) if storage == ELLPACK
                    else int(self._ia[neq] - self._ia[0]))
         self.neq, self.nad, self.storage, self.unsym = neq, nad, storage, unsym
+        self.values_version = 0  # bumped by every set_values / set_diagonal
         h = _P()
         rc = lib().sfr_gpu_create(neq, nad, _ptr(self._ia), _ptr(self._ja),
                                   storage, int(unsym), device, ctypes.byref(h))
@@ -182,12 +187,14 @@ class GpuSystem:
         rc = lib().sfr_gpu_set_values(self.h, _ptr(al), _ptr(ad), _ptr(au))
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_values")
+        self.values_version += 1
 
     def set_diagonal(self, ad):
         ad = _f64(ad)
         rc = lib().sfr_gpu_set_diagonal(self.h, _ptr(ad))
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_diagonal")
+        self.values_version += 1
 
     def solve(self, solver: int, b, x0=None, tol: float = 1e-10,
               maxit: int = 100000, newx: bool = True, precision: int = FP64,
@@ -217,6 +224,51 @@ class GpuSystem:
         if rc < 0 and raise_on_error:
             raise SolverError(rc, "sfr_gpu_solve_multi")
         return x, [SolveInfo.from_c(infos[i]) for i in range(k)]
+
+    def solve_transpose(self, solver: int, b, x0=None, tol: float = 1e-10,
+                        maxit: int = 100000, newx: bool = True,
+                        precision: int = FP64, raise_on_error: bool = True):
+        """Solve A^T x = b (sfr_gpu_solve_transpose).  Returns (x, SolveInfo)."""
+        b = _f64(b)
+        x = np.zeros(self.neq) if x0 is None else np.array(x0, dtype=np.float64)
+        info = SolveInfoC()
+        rc = lib().sfr_gpu_solve_transpose(self.h, solver, _ptr(b), _ptr(x), tol,
+                                           maxit, int(newx), precision,
+                                           ctypes.byref(info))
+        if rc < 0 and raise_on_error:
+            raise SolverError(rc, "sfr_gpu_solve_transpose")
+        return x, SolveInfo.from_c(info)
+
+    def adjoint(self, solver: int, x, g, tol: float = 1e-12,
+                maxit: int = 100000, precision: int = FP64,
+                raise_on_error: bool = True):
+        """Adjoint of x = A^-1 b for dJ/dx = g (sfr_gpu_adjoint).
+
+        Returns (lam, g_al, g_ad, g_au, SolveInfo): dJ/db = lam and
+        dJ/dA_ij = -lam_i x_j in the value layout of set_values (g_au is
+        None unless the storage keeps a separate upper array).
+        """
+        x, g = _f64(x), _f64(g)
+        lam = np.zeros(self.neq)
+        split = self.storage == CSRC and self.unsym
+        nsrc = self._nsrc()
+        g_al = np.zeros(nsrc // 2 if split else nsrc)
+        g_ad = np.zeros(self.neq)
+        g_au = np.zeros(nsrc // 2) if split else None
+        info = SolveInfoC()
+        rc = lib().sfr_gpu_adjoint(self.h, solver, _ptr(x), _ptr(g), _ptr(lam),
+                                   _ptr(g_al), _ptr(g_ad), _ptr(g_au), tol,
+                                   maxit, precision, ctypes.byref(info))
+        if rc < 0 and raise_on_error:
+            raise SolverError(rc, "sfr_gpu_adjoint")
+        return lam, g_al, g_ad, g_au, SolveInfo.from_c(info)
+
+    def _nsrc(self) -> int:
+        """Number of stored off-diagonal values (al, plus au when split)."""
+        if self.storage == ELLPACK:
+            return int(self._ia[1])
+        n = int(self._ia[self.neq] - self._ia[0])
+        return 2 * n if (self.storage == CSRC and self.unsym) else n
 
     # device-pointer entry points (pointers are plain integers)
     def solve_device(self, solver, d_b: int, d_x: int, tol=1e-10,

@@ -27,3 +27,23 @@ def layouts(sys_):
         out["csrd_sym"] = (O.CSRD, False, il, jl, alo, None)
         out["csrc_sym"] = (O.CSRC, False, ia, ja, a[: len(ja)], None)
     return out
+
+
+def transpose_csrd(neq, ia, ja, al):
+    """Explicit transpose of a full CSRD matrix (off-diagonals only, the
+    diagonal is shared): rows of A^T with ascending column indices, the
+    order a transposed CSRD built by sorting takes."""
+    ia = np.asarray(ia, dtype=np.int64)
+    ja = np.asarray(ja, dtype=np.int64)
+    al = np.asarray(al, dtype=np.float64)
+    base = int(ia[0])
+    rows = np.repeat(np.arange(neq), np.diff(ia))
+    cols = ja[base:base + len(rows)]
+    order = np.lexsort((rows, cols))  # by new row (= col), then new col (= row)
+    t_rows = cols[order]
+    t_cols = rows[order]
+    t_val = al[: len(rows)][order]
+    t_ia = np.zeros(neq + 1, dtype=np.int32)
+    np.add.at(t_ia, t_rows + 1, 1)
+    t_ia = np.cumsum(t_ia).astype(np.int32)
+    return t_ia, t_cols.astype(np.int32), t_val
