@@ -2,22 +2,29 @@
 """Benchmark: Krylov solve time to 1e-10 on the 128^3 pressure-correction
 system (seeded jittered hex mesh, per-cell diffusivity 10^U(-2,2), harmonic
 faces, random permutation + RCM), Jacobi-PCG in FP64 on one B200, with the
-standalone SpMV's HBM roofline and the mixed-precision path beside it.
+SpMV's HBM roofline and the mixed-precision path beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 A step is one complete solve (x = 0 to relative M-norm residual 1e-10, the
-reference's own stopping test, Cg.c:145) of the system resident in HBM.
-Between timed steps L2 is flushed by writing a 256 MiB buffer (outside the
-timed events).  Under torchrun (N > 1) every rank solves its own seeded
-system of the same size (weak scaling, no collective on the data path);
-times are the max over ranks.
+reference's own stopping test, Cg.c:145) of the system resident in HBM: one
+CUDA-graph launch.  Between timed steps L2 is flushed by writing a 256 MiB
+buffer (outside the timed events).  Under torchrun (N > 1) every rank solves
+its own seeded system of the same size (weak scaling, no collective on the
+data path); times are the max over ranks.
+
+Beside the headline (N = 1 only): the mixed-precision solve of the same
+system and its error against the FP64 solution; the 128^3 momentum system
+(Peclet 50, three right-hand sides) solved one right-hand side at a time in
+FP64 and as one K = 3 mixed launch; 64 uneven Poisson systems in one batched
+launch; the adjoint of the 96^3 Peclet-20 momentum system with its
+central-difference check; the end-to-end drop-in call (host buffers); and
+the reference's own OpenMP solver on this host.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import re
 import statistics
@@ -45,11 +52,14 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--profile", choices=["none", "spmv", "solve"], default="none",
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the momentum, batched and adjoint legs")
+    ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab"], default="none",
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
                     help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
                          "loop (profiling)")
+    ap.add_argument("--threads", type=int, default=0, help="graph-engine block size (0: default)")
     ap.add_argument("--spw", type=int, default=0, help="SELL slices per warp (0: default)")
     ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
     return ap.parse_args(argv)
@@ -63,9 +73,9 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def committed_traffic(kernel: str):
-    """Per-unit DRAM traffic from a committed ncu summary: a line
-    `bench-traffic <kernel> <bytes> <unit>` in profiles/*.md."""
+def committed_traffic(name: str):
+    """DRAM traffic from a committed ncu summary: a line
+    `bench-traffic <name> <bytes> <unit>` in profiles/*.md."""
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
@@ -74,7 +84,7 @@ def committed_traffic(kernel: str):
             continue
         for line in open(os.path.join(pdir, fn)):
             m = re.match(r"\s*bench-traffic\s+(\S+)\s+([0-9.eE+]+)\s+(\S+)", line)
-            if m and m.group(1) == kernel:
+            if m and m.group(1) == name:
                 return float(m.group(2)), m.group(3)
     return None
 
@@ -131,7 +141,7 @@ class ClockSampler:
 
 def spmv_alg_bytes(n, nnz_off):
     # CSRD FP64: values + indices of the off-diagonals, row pointers, diagonal,
-    # x and y once each (the SpMV figure of the path's scope table)
+    # x and y once each
     return 12 * nnz_off + 4 * (n + 1) + 24 * n
 
 
@@ -139,6 +149,11 @@ def pcg_alg_bytes(n, nnz_off, iters):
     # setup and post-processing: two SpMVs; each iteration one SpMV plus the
     # 88 N bytes of its vector updates
     return (iters + 2) * spmv_alg_bytes(n, nnz_off) + iters * 88 * n
+
+
+def pcg_kernel_launches(iters):
+    # setup, start, three kernels per iteration, post-processing
+    return 3 * iters + 3
 
 
 # --------------------------------------------------------------- ours ----
@@ -176,7 +191,7 @@ def run_ours(args):
     N, nnz = s.neq, s.nnz_full
     g = sv.GpuSystem(N, s.ia, s.ja, sv.CSRD, True, device=local)
     g.set_values(s.al, s.ad)
-    g.set_engine(args.engine, 0, args.spw)
+    g.set_engine(args.engine, args.threads, args.spw)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     b = torch.tensor(s.b[0], device="cuda")
@@ -189,6 +204,17 @@ def run_ours(args):
                 y = torch.empty_like(b)
                 for _ in range(args.warmup + args.steps):
                     g.spmv(b.data_ptr(), y.data_ptr(), sptr)
+            elif args.profile == "bicgstab":
+                m = S.momentum(n, nrhs=1, seed=3)
+                gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=local)
+                gm.set_values(m.al, m.ad)
+                gm.set_engine(args.engine, args.threads, args.spw)
+                bm = torch.tensor(m.b[0], device="cuda")
+                xm = torch.zeros_like(bm)
+                for _ in range(args.warmup + args.steps):
+                    gm.solve_device(sv.PBICGSTAB, bm.data_ptr(), xm.data_ptr(), tol=1e-10,
+                                    maxit=args.maxit, stream=sptr,
+                                    precision=sv.MIXED if args.mixed else sv.FP64)
             else:
                 for _ in range(args.warmup + args.steps):
                     g.solve_device(sv.PCG, b.data_ptr(), x.data_ptr(), tol=1e-10,
@@ -197,67 +223,74 @@ def run_ours(args):
         torch.cuda.synchronize()
         return None
 
-    def timed_solves(precision, steps, warm):
+    def timed_solves(precision, steps, warm, xbuf):
         for _ in range(warm):
-            g.solve_device(sv.PCG, b.data_ptr(), x.data_ptr(), tol=1e-10,
+            g.solve_device(sv.PCG, b.data_ptr(), xbuf.data_ptr(), tol=1e-10,
                            maxit=args.maxit, precision=precision, stream=sptr)
         barrier()
-        times, infos = [], []
+        infos = []
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
         for i in range(steps):
             with torch.cuda.stream(stream):
                 flush.fill_(i & 0xFF)
             ev[i][0].record(stream)
-            info = g.solve_device(sv.PCG, b.data_ptr(), x.data_ptr(), tol=1e-10,
+            info = g.solve_device(sv.PCG, b.data_ptr(), xbuf.data_ptr(), tol=1e-10,
                                   maxit=args.maxit, precision=precision, stream=sptr)
             ev[i][1].record(stream)
             infos.append(info)
         barrier()
-        times = [a.elapsed_time(c) for a, c in ev]
-        return times, infos
+        return [a.elapsed_time(c) for a, c in ev], infos
 
     gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
     clocks = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     clocks.start()
     t_wall0 = time.perf_counter()
-    times, infos = timed_solves(sv.FP64, args.steps, args.warmup)
+    times, infos = timed_solves(sv.FP64, args.steps, args.warmup, x)
     t_wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
     ms_step = max_over_ranks(statistics.mean(times))
     iters = infos[-1].iters
-    status = infos[-1].status
-    if status != sv.OK:
-        raise RuntimeError(f"solve did not converge: {sv.status_string(status)}")
+    if infos[-1].status != sv.OK:
+        raise RuntimeError(f"solve did not converge: {sv.status_string(infos[-1].status)}")
 
-    # mixed precision beside it
+    extras = rank == 0 and world == 1
+    peak, peak_kind = peak_hbm()
+
+    # mixed precision on the same system, and its error against FP64
     mixed = None
     if not args.no_mixed:
+        xm = torch.zeros_like(b)
         try:
-            mt, mi = timed_solves(sv.MIXED, max(2, args.steps // 2), 1)
+            mt, mi = timed_solves(sv.MIXED, args.steps, 1, xm)
+            x64 = x.cpu().numpy()
+            x32 = xm.cpu().numpy()
             mixed = {"ms": max_over_ranks(statistics.mean(mt)),
                      "inner_iters": mi[-1].inner_iters,
                      "refinements": mi[-1].refinements,
-                     "relres": mi[-1].relres, "status": mi[-1].status}
+                     "status": mi[-1].status,
+                     "true_relres_2norm": mi[-1].relres,
+                     "err_vs_fp64_x": float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64)),
+                     "speedup_vs_fp64": ms_step / max(statistics.mean(mt), 1e-9)}
         except sv.SolverError as e:
             mixed = {"unavailable": str(e)}
 
-    # standalone SpMV roofline (CUDA events on the launching stream)
-    y = torch.empty_like(b)
-    for _ in range(3):
-        g.spmv(b.data_ptr(), y.data_ptr(), sptr)
-    reps = 30
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(reps):
-        g.spmv(b.data_ptr(), y.data_ptr(), sptr)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    spmv_ms = e0.elapsed_time(e1) / reps
-    peak, peak_kind = peak_hbm()
+    spmv_ms = spmv_time(torch, g, b, stream)
     sb = spmv_alg_bytes(N, nnz)
     spmv_gbs = sb / (spmv_ms * 1e-3) / 1e9
+    sp_tr = committed_traffic("spmv_kernel")
+
+    momentum = batch = adjoint = target = None
+    if extras and not args.no_extras:
+        momentum = momentum_leg(np, torch, sv, S, n, local)
+        batch = batch_leg(sv, S)
+        adjoint = adjoint_leg(np, sv, S)
+        if mixed and "ms" in mixed and momentum:
+            plain = ms_step + momentum["fp64_sequential_ms"]
+            fast = mixed["ms"] + momentum["mixed_k3_ms"]
+            target = {"what": "128^3 pressure PCG + 128^3 momentum BiCGSTAB (3 RHS) to 1e-10",
+                      "plain_fp64_ms": plain, "mixed_batched_ms": fast,
+                      "speedup": plain / fast, "goal": 2.0}
 
     # end to end through the reference-facing drop-in (sfr_solverC) with
     # pinned host buffers: al/ad/b uploaded and x read back every step
@@ -278,26 +311,25 @@ def run_ours(args):
                                  h_al.data_ptr(), h_ad.data_ptr(), None, h_b.data_ptr(),
                                  h_x.data_ptr(), None, None, 1e-10, args.maxit, sv.CSRD,
                                  sv.PCG, None, False, True, False, b"pressure")
-        for _ in range(max(1, args.warmup // 2)):
+        for _ in range(args.warmup):
             assert call() == sv.OK
         barrier()
         t0 = time.perf_counter()
-        e2e_steps = max(2, args.steps // 2)
-        for _ in range(e2e_steps):
+        for _ in range(args.steps):
             rc = call()
             if rc != sv.OK:
                 raise RuntimeError(f"drop-in solve failed: {sv.status_string(rc)}")
         barrier()
-        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps)
+        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
         e2e = {"value": e2e_ms, "unit": "ms",
                "h2d_bytes_per_step": int(h_al.numel() * 8 + h_ad.numel() * 8 + h_b.numel() * 8),
                "d2h_bytes_per_step": int(h_x.numel() * 8),
-               "api": "sfr_solverC (solverC drop-in), CSRD symmetric storage"}
+               "api": "sfr_solverC (solverC drop-in), CSRD symmetric storage, FP64"}
         sv.release_cache()
 
     # CPU baseline: the reference's own pcgOmp on this host (rank 0, N = 1)
     cpu = None
-    if not args.no_cpu and rank == 0 and world == 1:
+    if not args.no_cpu and extras:
         cpu = cpu_baseline(s, iters)
 
     if rank != 0:
@@ -307,10 +339,10 @@ def run_ours(args):
 
     alg = pcg_alg_bytes(N, nnz, iters)
     achieved = alg / (ms_step * 1e-3) / 1e9
-    tr = committed_traffic("pcg_fp64_kernel")
+    tr = committed_traffic("pcg_fp64_iteration")
     traffic = None
-    if tr is not None:
-        traffic = tr[0] * (iters if tr[1] == "per_iteration" else 1)
+    if tr is not None and tr[1] == "per_iteration_128":
+        traffic = tr[0] * (N / 128 ** 3) * iters
     line = {
         "metric": METRIC,
         "value": ms_step,
@@ -328,22 +360,30 @@ def run_ours(args):
                                f"nodes +-20%, diffusivity 10^U(-2,2), harmonic faces, "
                                f"permuted + RCM; Jacobi-PCG FP64 to 1e-10 (M-norm)",
                    "rows": N, "nnz_offdiag": nnz, "iterations": iters,
-                   "format": "SELL-32 (from CSRD)", "l2": "flushed between steps (256 MiB write)",
+                   "format": "SELL-32 (from CSRD)",
+                   "engine": "CUDA graph, device-side WHILE loop (3 kernels per iteration)",
+                   "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
         "iterations": iters,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "pcg_fp64_kernel (persistent, one launch per solve)",
+                     "kernel": "PCG solve graph (one launch per solve: k_pcg_a SpMV+dot, "
+                               "k_pcg_b update+dot, k_pcg_c direction per iteration)",
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "alg_bytes_per_launch": alg},
+                     "alg_bytes_per_launch": alg,
+                     "alg_bytes_rule": "(iters+2)*(12 nnz_off + 4(N+1) + 24N) + iters*88N"},
         "spmv": {"kernel": "spmv_kernel", "ms": spmv_ms, "alg_bytes": sb, "GB/s": spmv_gbs,
-                 "frac_of_peak": spmv_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs"},
+                 "frac": spmv_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                 "traffic": None if sp_tr is None else sp_tr[0] * (N / 128 ** 3),
+                 "timing": "graph of 20 x [256 MiB read, SpMV] minus graph of 20 x [256 MiB read]"},
         "mixed": mixed,
-        "fp64_plain_ms": ms_step,
-        "mixed_speedup": (ms_step / mixed["ms"]) if mixed and "ms" in mixed else None,
+        "momentum": momentum,
+        "batched": batch,
+        "adjoint": adjoint,
+        "target_mixed_batched_vs_fp64": target,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * pcg_kernel_launches(iters),
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }
@@ -353,10 +393,132 @@ def run_ours(args):
     return line
 
 
-def cpu_baseline(s, iters_full, sample_iters=None):
+def spmv_time(torch, g, x, stream, reps=20):
+    """Device time of one SpMV launch with a cold L2: CUDA events around a
+    graph of `reps` x [read 256 MiB, SpMV] minus a graph of `reps` x
+    [read 256 MiB] (a read leaves L2 clean, so the SpMV pays no write-backs
+    of the flush), divided by reps.  Best of three replays each."""
+    y = torch.empty_like(x)
+    fl = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    sink = torch.empty((), dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            torch.sum(fl, dim=0, out=sink)
+            g.spmv(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    with_spmv, flush_only = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(with_spmv, stream=stream):
+        for _ in range(reps):
+            torch.sum(fl, dim=0, out=sink)
+            g.spmv(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    with torch.cuda.graph(flush_only, stream=stream):
+        for _ in range(reps):
+            torch.sum(fl, dim=0, out=sink)
+    best = {}
+    for name, gr in (("a", with_spmv), ("b", flush_only)) * 3:
+        gr.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            gr.replay()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        best[name] = min(best.get(name, t), t)
+    return (best["a"] - best["b"]) / reps
+
+
+def momentum_leg(np, torch, sv, S, n, device):
+    """128^3 momentum (Peclet 50, nu 1e-3, dt 1e-2), three right-hand sides:
+    FP64 one right-hand side at a time vs one K = 3 mixed launch."""
+    m = S.momentum(n, nrhs=3, seed=3)
+    g = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=device)
+    g.set_values(m.al, m.ad)
+    out = {"workload": f"momentum {n}^3 Peclet 50, 3 RHS, Jacobi-BiCGSTAB to 1e-10"}
+    for _ in range(2):  # warm-up: graphs built, clocks up
+        for k in range(3):
+            g.solve(sv.PBICGSTAB, m.b[k], tol=1e-10)
+        g.solve_multi(sv.PBICGSTAB, m.b, tol=1e-10, precision=sv.MIXED)
+        g.solve_multi(sv.PBICGSTAB, m.b, tol=1e-10)
+    seq, its = 0.0, []
+    x64 = []
+    for k in range(3):
+        xk, info = g.solve(sv.PBICGSTAB, m.b[k], tol=1e-10)
+        seq += info.seconds * 1e3
+        its.append(info.iters)
+        x64.append(xk)
+    xs, infos = g.solve_multi(sv.PBICGSTAB, m.b, tol=1e-10, precision=sv.MIXED)
+    _, infos64 = g.solve_multi(sv.PBICGSTAB, m.b, tol=1e-10)
+    out.update({
+        "fp64_sequential_ms": seq, "fp64_iters": its,
+        "fp64_k3_ms": infos64[0].seconds * 1e3,
+        "mixed_k3_ms": infos[0].seconds * 1e3,
+        "mixed_iters": [i.iters for i in infos],
+        "mixed_status": [i.status for i in infos],
+        "mixed_err_vs_fp64_x": [float(np.linalg.norm(xs[k] - x64[k]) / np.linalg.norm(x64[k]))
+                                for k in range(3)],
+        "mixed_true_relres": [i.relres for i in infos],
+    })
+    g.close()
+    return out
+
+
+def batch_leg(sv, S):
+    """64 uneven Poisson systems (8..96 cells per axis) in one batched launch,
+    block shares autotuned from measured iterations."""
+    systems = S.poisson_batch(64, 8, 96, seed=4)
+    g = sv.GpuBatch([(s.neq, s.ia, s.ja) for s in systems], sv.CSRD, True)
+    g.set_values([s.al for s in systems], [s.ad for s in systems])
+    bs = [s.b[0] for s in systems]
+    out = {"workload": f"64 Poisson boxes, {sum(s.neq for s in systems)} rows total, PCG to 1e-10"}
+    for name, prec in (("fp64", sv.FP64), ("mixed", sv.MIXED)):
+        g.solve(sv.PCG, bs, tol=1e-10, precision=prec)
+        ms = g.autotune(sv.PCG, bs, tol=1e-10, precision=prec)
+        _, infos = g.solve(sv.PCG, bs, tol=1e-10, precision=prec)
+        out[name] = {"ms": infos[0].seconds * 1e3, "autotune_best_ms": ms,
+                     "max_iters": max(i.iters for i in infos),
+                     "all_converged": all(i.status == sv.OK for i in infos)}
+    out["grid_blocks"] = g.stats()["grid"]
+    g.close()
+    return out
+
+
+def adjoint_leg(np, sv, S):
+    """Adjoint of the 96^3 Peclet-20 momentum system, J = w.x: transpose
+    solve time (FP64 and mixed) and the largest relative difference to
+    central differences on 32 coefficients + 32 right-hand-side entries."""
+    from sfr3d_b200 import adjoint as A
+    m = S.momentum(96, peclet=20.0, nrhs=1, seed=5)
+    g = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
+    g.set_values(m.al, m.ad)
+    w = np.random.default_rng(5).standard_normal(m.neq)
+    x, _ = g.solve(sv.PBICGSTAB, m.b[0], tol=1e-14, maxit=5000, raise_on_error=False)
+    rng = np.random.default_rng(5)
+    nz = np.flatnonzero(m.al != 0.0)
+    ent = [A.Entry("al", int(k), A.value_positions(g, m.ia, m.ja, "al", int(k)))
+           for k in rng.choice(nz, 24, replace=False)]
+    ent += [A.Entry("ad", int(i), [(int(i), int(i))]) for i in rng.choice(m.neq, 8, replace=False)]
+    ent += [A.Entry("b", int(i), []) for i in rng.choice(m.neq, 32, replace=False)]
+    fd = A.central_differences(g, sv.PBICGSTAB, m.al, m.ad, None, m.b[0], x, w, ent,
+                               rel_step=1e-6, tol=1e-13, maxit=5000)
+    out = {"workload": "momentum 96^3 Peclet 20, J = w.x, w ~ N(0,1)"}
+    for name, prec, tol in (("fp64", sv.FP64, 1e-12), ("mixed", sv.MIXED, 1e-10)):
+        g.adjoint(sv.PBICGSTAB, x, w, tol=tol, precision=prec)
+        lam, g_al, g_ad, _, info = g.adjoint(sv.PBICGSTAB, x, w, tol=tol, precision=prec)
+        arrays = {"al": g_al, "ad": g_ad, "b": lam}
+        adj = np.array([arrays[e.array][e.index] for e in ent])
+        out[name] = {"transpose_solve_ms": info.seconds * 1e3, "iters": info.iters,
+                     "tol": tol,
+                     "max_rel_err_vs_central_diff": float(np.max(np.abs(adj - fd) / np.abs(fd)))}
+    g.close()
+    return out
+
+
+def cpu_baseline(s, iters_full):
     """The reference's own pcgOmp (Cg.c:490) with all host threads on the
-    same system in CSRC symmetric storage (the reference's default), run to a
-    bounded iteration count and scaled to the full solve."""
+    same system in CSRC symmetric storage (the reference's default): a full
+    solve when one takes under 30 s, else a bounded sample scaled to the
+    full iteration count."""
     try:
         from oracle import oracle as O
     except Exception as e:  # pragma: no cover
@@ -365,15 +527,24 @@ def cpu_baseline(s, iters_full, sample_iters=None):
         return {"unavailable": "oracle/_ref/libsfr3d_ref.so not built"}
     threads = os.cpu_count() or 1
     il, jl, al = s.csrd_lower()
-    if sample_iters is None:
-        sample_iters = min(iters_full, 300)
+    probe = O.ref_solve(O.PCG, O.CSRC, False, il, jl, al, s.ad, s.b[0], tol=1e-10,
+                        maxit=100, nthreads=threads)
+    per_it = probe.seconds / 100
+    if per_it * iters_full < 30:
+        r = O.ref_solve(O.PCG, O.CSRC, False, il, jl, al, s.ad, s.b[0], tol=1e-10,
+                        maxit=100000, nthreads=threads)
+        return {"value": r.seconds * 1e3, "unit": "ms", "cores": threads, "kind": "reference",
+                "sample": f"one full pcgOmp solve (CSRC symmetric, {threads} threads), "
+                          f"{r.iters} iterations",
+                "ms_per_iteration": r.seconds / r.iters * 1e3}
+    n_it = max(100, int(30 / per_it))
     r = O.ref_solve(O.PCG, O.CSRC, False, il, jl, al, s.ad, s.b[0], tol=1e-10,
-                    maxit=sample_iters, nthreads=threads)
-    per_it = r.seconds / sample_iters if r.status != 0 else r.seconds / max(r.iters, 1)
+                    maxit=n_it, nthreads=threads)
+    per_it = r.seconds / n_it
     return {"value": per_it * iters_full * 1e3, "unit": "ms", "cores": threads,
             "kind": "reference",
-            "sample": f"{sample_iters} pcgOmp iterations (CSRC symmetric, {threads} threads) "
-                      f"of the same system, scaled to the full solve's {iters_full} iterations",
+            "sample": f"{n_it} pcgOmp iterations (CSRC symmetric, {threads} threads), "
+                      f"scaled to the full solve's {iters_full} iterations",
             "ms_per_iteration": per_it * 1e3}
 
 
