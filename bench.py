@@ -416,9 +416,10 @@ def spmv_time(torch, g, x, stream, reps=20):
             torch.sum(fl, dim=0, out=sink)
     best = {}
     for name, gr in (("a", with_spmv), ("b", flush_only)) * 3:
-        gr.replay()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
+            gr.replay()  # warm
+            torch.cuda.synchronize()
             e0.record(stream)
             gr.replay()
             e1.record(stream)

@@ -121,7 +121,9 @@ int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
  * exactly maxit iterations (for profilers, which cannot look inside graphs
  * with conditional nodes; finished solves make the remaining launches
  * no-ops).  threads (128 or 256) and slices_per_warp (1..64; a SELL slice is
- * 32 rows) set the graph engine's launch shape; 0 keeps the current value. */
+ * 32 rows) set the graph engine's launch shape; 0 keeps the current value;
+ * slices_per_warp = -1 (the default) sizes the SpMV phases to one wave of
+ * the blocks resident on the GPU at once. */
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
                        int32_t slices_per_warp);
 

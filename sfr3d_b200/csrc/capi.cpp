@@ -238,10 +238,11 @@ int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x, dou
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads, int32_t slices_per_warp) {
   if (!s || engine < 0 || engine > 3) return SFR_BAD_INPUT;
   if (threads != 0 && threads != 128 && threads != 256) return SFR_BAD_INPUT;
-  if (slices_per_warp < 0 || slices_per_warp > 64) return SFR_BAD_INPUT;
+  if (slices_per_warp < -1 || slices_per_warp > 64) return SFR_BAD_INPUT;
   s->engine = engine;
   if (threads) s->graph_threads = threads;
-  if (slices_per_warp) s->graph_spw = slices_per_warp;
+  if (slices_per_warp > 0) s->graph_spw = slices_per_warp;
+  if (slices_per_warp == -1) s->graph_spw = 0;  // one wave of resident blocks
   return SFR_OK;
 }
 

@@ -81,7 +81,7 @@ struct sfr_system {
   // 3 the graph engine's kernels from a host loop (profiling)
   int32_t engine = 0;
   int32_t graph_threads = 256;   // graph engine launch shape
-  int32_t graph_spw = 4;         // SELL slices per warp
+  int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
   int64_t bytes = 0;
 };
 

@@ -651,10 +651,21 @@ int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag, const dou
   SellView<double> v{A.n, A.nslices, A.sptr, A.col, A.val, d_diag};
   const int grid = grid_for_slices(A.nslices, s->device);
   if (!d_dot) {
-    // the graph engine's launch shape: 8 warps per block, graph_spw slices
-    // per warp, block-contiguous slice ranges
-    const int spw = std::max(1, s->graph_spw);
-    const int g2 = std::max(1, (A.nslices + 8 * spw - 1) / (8 * spw));
+    // the graph engine's launch shape: 8 warps per block, block-contiguous
+    // slice ranges; graph_spw slices per warp, or (0) one wave of resident
+    // blocks
+    int g2 = 0;
+    if (s->graph_spw > 0) {
+      g2 = std::max(1, (A.nslices + 8 * s->graph_spw - 1) / (8 * s->graph_spw));
+    } else {
+      static int occ[64] = {};
+      const int d = s->device & 63;
+      if (!occ[d] && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[d], spmv_kernel, 256, 0) !=
+                          cudaSuccess ||
+                      occ[d] < 1))
+        occ[d] = 1;
+      g2 = std::max(1, std::min((A.nslices + 7) / 8, occ[d] * num_sms(s->device)));
+    }
     spmv_kernel<<<g2, 256, 0, st>>>(v, d_x, d_y);
   } else {
     Scratch *sc = nullptr;

@@ -1100,14 +1100,36 @@ constexpr int kVecs32 = 10;       // (unused) m32 r z q p0 p1 xs r0 t
 inline int64_t padded(int n) { return (static_cast<int64_t>(n) + 3) & ~static_cast<int64_t>(3); }
 
 // Allocate the graph's workspace and fill its by-value arguments.
+// Blocks of the iteration's SpMV kernel that fit on the GPU at once.
 template <int K>
-cudaError_t prepare(sfr_system *s, int precision, int threads, int spw, CachedGraph *cg) {
+int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
+  const void *kern =
+      solver == SFR_PCG
+          ? (mixed ? (const void *)k_pcg_a<K, true> : (const void *)k_pcg_a<K, false>)
+          : (mixed ? (const void *)k_bicg_a1<K, true> : (const void *)k_bicg_a1<K, false>);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  return occ * std::max(1, num_sms(s->device));
+}
+
+// spw > 0: `spw` slices per warp.  spw == 0: one wave, as many blocks as are
+// resident at once (fewer for small systems), so no partial last wave leaves
+// SMs idle while the phase's last blocks finish.
+template <int K>
+cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int spw,
+                    CachedGraph *cg) {
   const int n = s->n;
   const int64_t np = padded(n);
   const bool mixed = precision == SFR_MIXED;
   const int warps = threads / kWarp;
   cg->threads = threads;
-  cg->grid_s = std::max(1, (s->A.nslices + warps * spw - 1) / (warps * spw));
+  if (spw > 0)
+    cg->grid_s = std::max(1, (s->A.nslices + warps * spw - 1) / (warps * spw));
+  else
+    cg->grid_s = std::max(1, std::min((s->A.nslices + warps - 1) / warps,
+                                      resident_blocks<K>(s, solver, mixed, threads)));
   const int npairs = (n + 1) / 2;
   const int wave = std::max(1, num_sms(s->device)) * (2048 / threads);
   cg->grid_v = std::max(1, std::min(wave, (npairs + threads - 1) / threads));
@@ -1172,7 +1194,7 @@ cudaError_t prepare(sfr_system *s, int precision, int threads, int spw, CachedGr
 template <int K>
 cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
                         CachedGraph *cg) {
-  SFR_TRY(prepare<K>(s, precision, threads, spw, cg));
+  SFR_TRY(prepare<K>(s, solver, precision, threads, spw, cg));
   SFR_TRY(cudaGraphCreate(&cg->graph, 0));
   cudaGraph_t g = cg->graph;
   const bool mixed = precision == SFR_MIXED;
@@ -1422,7 +1444,7 @@ int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
                  cudaStream_t st, sfr_solve_info *info) {
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
   if (threads != 128 && threads != 256) return SFR_BAD_INPUT;
-  if (spw < 1 || spw > 64) return SFR_BAD_INPUT;
+  if (spw < 0 || spw > 64) return SFR_BAD_INPUT;
   SolveOut out[kMaxK];
   float ms = 0.f;
   int rc;
