@@ -14,13 +14,20 @@ constexpr int kWarp = 32;
 
 // ----------------------------------------------------------------------
 // Loads.  The matrix is read once per sweep: streaming (evict-first) loads
-// keep it from pushing the Krylov vectors out of L2.  Vectors written inside
-// a persistent launch are read with .cg (L2, never a stale L1 line).
+// keep it from pushing the Krylov vectors out of L2.
+// Vectors that other blocks of the same launch write (persistent kernels,
+// block partials) are read with plain (weak, L1-cached) loads, only after a
+// synchronisation that orders the writes before them: the grid barrier (the
+// writer's bar.sync + device-scope release, the reader's device-scope
+// acquire + bar.sync) or the last-block fence/atomic/fence pattern.  Under
+// the PTX memory model those reads observe the writes; the device-scope
+// acquire is what discards stale L1 lines.  Never ld.global.nc for them: the
+// non-coherent path is outside that guarantee.
 // ----------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
 template <typename T>
-__device__ __forceinline__ T ld_vec(const T *p) { return __ldcg(p); }
+__device__ __forceinline__ T ld_vec(const T *p) { return *p; }
 template <typename T>
 __device__ __forceinline__ void st_vec(T *p, T v) { __stcg(p, v); }
 // Data no thread writes while the kernel runs: a plain (L1-cached, LSU) load.

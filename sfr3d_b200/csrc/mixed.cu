@@ -219,7 +219,7 @@ __device__ bool setup(const MixedArgs &a, const Team &t, int &slot, double *sm,
 // Mixed PCG.
 // ---------------------------------------------------------------------------
 template <int K>
-__global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
+__global__ void __launch_bounds__(kThreads, K == 1 ? 2 : 1) pcg_mixed_kernel(MixedArgs a) {
   __shared__ double sm[kMaxNV * 32];
   const Team team = make_team(a.team, a.gs, a.A32.nslices, a.n);
   const int n = team.row_end;
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(MixedArgs a) {
 // Mixed BiCGSTAB (right-preconditioned, Bicgstab.c:50-245).
 // ---------------------------------------------------------------------------
 template <int K>
-__global__ void __launch_bounds__(kThreads) bicgstab_mixed_kernel(MixedArgs a) {
+__global__ void __launch_bounds__(kThreads, K == 1 ? 2 : 1) bicgstab_mixed_kernel(MixedArgs a) {
   __shared__ double sm[kMaxNV * 32];
   const Team team = make_team(a.team, a.gs, a.A32.nslices, a.n);
   const int n = team.row_end;

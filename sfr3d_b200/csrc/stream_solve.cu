@@ -11,8 +11,6 @@
 //
 // Loads: vectors are read with plain L1-cached loads (a warp's rows share
 // most of their gathers); the matrix streams with evict-first.
-// (The persistent engine cannot do this: other blocks rewrite its vectors
-// during the launch, so it reads them from L2.)
 //
 // The persistent engine (krylov.cu, mixed.cu) suits small systems where
 // launch latency dominates; this engine suits large ones.  Both follow the
