@@ -484,6 +484,18 @@ def batch_leg(sv, S):
                      "all_converged": all(i.status == sv.OK for i in infos)}
     out["grid_blocks"] = g.stats()["grid"]
     g.close()
+    # the plain path: the same systems one at a time, FP64 (device time of
+    # each solve, second of two)
+    seq = 0.0
+    for sy in systems:
+        one = sv.GpuSystem(sy.neq, sy.ia, sy.ja, sv.CSRD, True)
+        one.set_values(sy.al, sy.ad)
+        one.solve(sv.PCG, sy.b[0], tol=1e-10)
+        _, info = one.solve(sv.PCG, sy.b[0], tol=1e-10)
+        seq += info.seconds * 1e3
+        one.close()
+    out["fp64_one_at_a_time_ms"] = seq
+    out["speedup_mixed_batched_vs_fp64_one_at_a_time"] = seq / out["mixed"]["ms"]
     return out
 
 

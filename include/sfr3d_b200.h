@@ -241,9 +241,12 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
                 bool unSym, const char *name);
 void sfr_set_exit_on_failure(int32_t flag);
 /* SFR_MIXED: the inner FP32 residual must fall by this factor (0 < delta
- * < 1, default 0.1) before the FP64 solution is refreshed and the true
- * residual recomputed. */
+ * < 1) before the FP64 solution is refreshed and the true residual
+ * recomputed.  Sets the factor of both solvers (defaults: PCG 0.1,
+ * BiCGSTAB 1e-4). */
 void sfr_set_reliable_delta(double delta);
+/* The same for one solver (SFR_PCG or SFR_PBICGSTAB). */
+int sfr_set_solver_reliable_delta(int32_t solver, double delta);
 /* Precision used by sfr_solverC (SFR_FP64 default). */
 void sfr_set_precision(int32_t precision);
 /* Release every pattern sfr_solverC cached. */

@@ -861,7 +861,7 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   if (engine == 0) engine = s->n >= kGraphEngineRows ? 2 : 1;
   if (engine == 2 || engine == 3)
     return solve_stream(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, precision,
-                        reliable_delta(), s->graph_threads, s->graph_spw, engine == 3, st,
+                        reliable_delta(solver), s->graph_threads, s->graph_spw, engine == 3, st,
                         info);
   if (precision == SFR_MIXED)
     return solve_mixed(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);

@@ -629,7 +629,13 @@ __global__ void __launch_bounds__(kThreads, K == 1 ? 2 : 1) bicgstab_mixed_kerne
 // --------------------------------------------------------------- host ---
 constexpr int kFloatVecs = 10;  // (unused) m32 r z p0 p1 q xs r0 t
 
-double g_delta = 0.1;
+// Refresh factor per solver.  PCG on the ill-conditioned pressure systems
+// needs frequent refreshes (a smaller factor lets the FP32 recurrence drift
+// and multiplies the iterations); BiCGSTAB on the diagonally dominant
+// momentum systems converges in a few iterations, where each refresh (an
+// FP64 SpMV) is a large share of the work.
+double g_delta_pcg = 0.1;
+double g_delta_bicg = 1e-4;
 
 template <int K>
 int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const double *d_b,
@@ -687,7 +693,7 @@ int launch_mixed(sfr_system *s, int32_t solver, const double *d_diag_k, const do
   a.gs.spin_limit = 1u << 22;
   a.out = reinterpret_cast<SolveOut *>(base + vec_bytes + part_bytes + ctl_bytes);
   a.tol = tol;
-  a.delta = g_delta;
+  a.delta = reliable_delta(solver);
   a.maxit = maxit;
   a.newx = newx;
 
@@ -770,7 +776,7 @@ int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double 
   a.team = team;
   a.out = d_out;
   a.tol = tol;
-  a.delta = g_delta;
+  a.delta = reliable_delta(solver);
   a.maxit = maxit;
   a.newx = newx;
   if (cudaMemsetAsync(ctl, 0, 64, st) != cudaSuccess) return SFR_CUDA_ERROR;
@@ -818,11 +824,23 @@ int solve_mixed(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k
   return worst;
 }
 
-void set_reliable_delta(double delta) { g_delta = delta; }
-double reliable_delta() { return g_delta; }
+double reliable_delta(int32_t solver) {
+  return solver == SFR_PCG ? g_delta_pcg : g_delta_bicg;
+}
 
 }  // namespace sfr
 
 extern "C" void sfr_set_reliable_delta(double delta) {
-  if (delta > 0.0 && delta < 1.0) sfr::set_reliable_delta(delta);
+  if (delta > 0.0 && delta < 1.0) sfr::g_delta_pcg = sfr::g_delta_bicg = delta;
+}
+
+extern "C" int sfr_set_solver_reliable_delta(int32_t solver, double delta) {
+  if (!(delta > 0.0 && delta < 1.0)) return SFR_BAD_INPUT;
+  if (solver == SFR_PCG)
+    sfr::g_delta_pcg = delta;
+  else if (solver == SFR_PBICGSTAB)
+    sfr::g_delta_bicg = delta;
+  else
+    return SFR_BAD_INPUT;
+  return SFR_OK;
 }

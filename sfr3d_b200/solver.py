@@ -107,6 +107,9 @@ def lib() -> ctypes.CDLL:
     L.sfr_set_exit_on_failure.argtypes = [_I32]
     L.sfr_set_exit_on_failure.restype = None
     L.sfr_set_precision.argtypes = [_I32]
+    L.sfr_set_reliable_delta.argtypes = [ctypes.c_double]
+    L.sfr_set_reliable_delta.restype = None
+    L.sfr_set_solver_reliable_delta.argtypes = [_I32, ctypes.c_double]
     L.sfr_set_precision.restype = None
     L.sfr_solverC_release.restype = None
     L.sfr_solverC_release.argtypes = []
@@ -417,6 +420,17 @@ def solverC(nEq, nEqNov, nAd, nAdR, ia, ja, al, ad, au, b, x, tol, maxIt,
 
 def set_precision(precision: int) -> None:
     lib().sfr_set_precision(precision)
+
+
+def set_reliable_delta(delta: float, solver: int | None = None) -> None:
+    """Mixed precision: the factor the FP32 residual must fall by before an
+    FP64 refresh, for one solver or (solver=None) both."""
+    if solver is None:
+        lib().sfr_set_reliable_delta(delta)
+        return
+    rc = lib().sfr_set_solver_reliable_delta(solver, delta)
+    if rc != OK:
+        raise SolverError(rc, "sfr_set_solver_reliable_delta")
 
 
 def release_cache() -> None:

@@ -82,3 +82,12 @@ def test_batch_create_validates_every_system():
         sv.GpuBatch([good, bad], sv.CSRD, False)
     assert e.value.status == sv.BAD_INPUT
     assert "system 1" in sv.last_error()
+
+
+def test_reliable_delta_validation():
+    from sfr3d_b200 import solver as sv
+    assert sv.lib().sfr_set_solver_reliable_delta(sv.PCG, 0.0) == sv.BAD_INPUT
+    assert sv.lib().sfr_set_solver_reliable_delta(sv.PCG, 1.0) == sv.BAD_INPUT
+    assert sv.lib().sfr_set_solver_reliable_delta(7, 0.1) == sv.BAD_INPUT
+    sv.set_reliable_delta(0.1, sv.PCG)
+    sv.set_reliable_delta(1e-4, sv.PBICGSTAB)
