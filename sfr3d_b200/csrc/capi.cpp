@@ -176,6 +176,7 @@ int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const 
   SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
   SFR_CU(cudaStreamSynchronize(s->stream));
   s->values_set = true;
+  ++s->values_epoch;
   if (s->tview) s->tview->comp_stale = true;
   return SFR_OK;
 }
@@ -186,6 +187,7 @@ int sfr_gpu_set_diagonal(sfr_system *s, const double *ad) {
   SFR_CU(cudaMemcpyAsync(s->d_diag, ad, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
   SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
   SFR_CU(cudaStreamSynchronize(s->stream));
+  ++s->values_epoch;
   return SFR_OK;
 }
 
@@ -236,7 +238,7 @@ int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x, dou
 }
 
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads, int32_t slices_per_warp) {
-  if (!s || engine < 0 || engine > 3) return SFR_BAD_INPUT;
+  if (!s || engine < 0 || engine > 4) return SFR_BAD_INPUT;
   if (threads != 0 && threads != 128 && threads != 256) return SFR_BAD_INPUT;
   if (slices_per_warp < -1 || slices_per_warp > 64) return SFR_BAD_INPUT;
   s->engine = engine;
@@ -260,6 +262,10 @@ int sfr_gpu_destroy(sfr_system *s) {
     cudaFree(s->d_diag32);
   }
   cudaFree(s->d_comp);
+  cudaFree(s->d_rval);
+  cudaFree(s->d_roff);
+  cudaFree(s->d_rdelta);
+  cudaFree(s->d_rbad);
   cudaFree(s->ws.base);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -295,6 +301,7 @@ int transpose_view(sfr_system *s, sfr_system **out) {
   }
   sfr_system *t = s->tview;
   t->values_set = s->values_set;
+  t->values_epoch = s->values_epoch;
   t->engine = s->engine;
   t->graph_threads = s->graph_threads;
   t->graph_spw = s->graph_spw;

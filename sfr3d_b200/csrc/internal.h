@@ -77,8 +77,18 @@ struct sfr_system {
   sfr_system *tview = nullptr;
   bool borrowed = false;     // a view: its matrix buffers belong to another handle
   bool comp_stale = true;    // compensation not yet computed for the current values
+  // resident engine (resident.cu): the symmetrically scaled FP32 operator,
+  // rebuilt when the values or the diagonal change
+  float *d_rval = nullptr;      // fl32(a_ij / sqrt(ad_i ad_j)) per SELL slot
+  int16_t *d_roff = nullptr;    // col - row per SELL slot
+  float *d_rdelta = nullptr;    // per row: correction of the unit diagonal
+  int *d_rbad = nullptr;        // set when a diagonal entry is not positive
+  uint64_t values_epoch = 0;    // bumped by every value / diagonal upload
+  uint64_t resident_epoch = ~0ull;  // epoch the scaled operator was built for
+  bool resident_ok = false;     // the diagonal was positive at that epoch
   // engine: 0 auto, 1 persistent (one cooperative launch), 2 graph,
-  // 3 the graph engine's kernels from a host loop (profiling)
+  // 3 the graph engine's kernels from a host loop (profiling),
+  // 4 resident (mixed PCG with the inner iteration on chip)
   int32_t engine = 0;
   int32_t graph_threads = 256;   // graph engine launch shape
   int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
@@ -116,6 +126,13 @@ int enqueue_team_fp64(sfr_system *s, int32_t solver, const double *d_b, double *
 int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double *d_x, double tol,
                        uint32_t maxit, int32_t newx, const TeamTable &team, int grid, void *ws,
                        SolveOut *d_out, unsigned *ctl, cudaStream_t st);
+
+// Resident engine (resident.cu): mixed PCG, one right-hand side, the
+// system's own diagonal.  resident_fits: the pattern and size allow it;
+// solve_resident returns SFR_UNSUPPORTED when the diagonal is not positive.
+bool resident_fits(sfr_system *s);
+int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, uint32_t maxit,
+                   int32_t newx, cudaStream_t st, sfr_solve_info *info);
 
 // Graph engine (stream_solve.cu)
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,

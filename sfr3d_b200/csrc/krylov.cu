@@ -858,7 +858,14 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
   int engine = s->engine;
-  if (engine == 0) engine = s->n >= kGraphEngineRows ? 2 : 1;
+  const bool resident_case = precision == SFR_MIXED && solver == SFR_PCG && k == 1 && !d_diag_k;
+  if (engine == 4 || (engine == 0 && resident_case && s->n >= kGraphEngineRows && resident_fits(s))) {
+    if (!resident_case) return SFR_UNSUPPORTED;
+    const int rc = solve_resident(s, d_b, d_x, tol, maxit, newx, st, info);
+    // automatic choice: a diagonal that is not positive has no Jacobi scaling
+    if (rc != SFR_UNSUPPORTED || engine == 4) return rc;
+  }
+  if (engine == 0 || engine == 4) engine = s->n >= kGraphEngineRows ? 2 : 1;
   if (engine == 2 || engine == 3)
     return solve_stream(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, precision,
                         reliable_delta(solver), s->graph_threads, s->graph_spw, engine == 3, st,

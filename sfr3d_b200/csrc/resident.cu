@@ -1,0 +1,664 @@
+// Resident engine: mixed-precision Jacobi-PCG for large systems, with the
+// FP32 inner iteration held on chip.
+//
+// B200 has a 126 MB L2 and up to 227 KB of shared memory per block.  The
+// inner operator of a 128^3 pressure system, stored as SELL-32 with FP32
+// couplings and 16-bit column offsets, is 75 MB and stays in L2 from one
+// iteration to the next; the FP64 operator (150 MB) cannot.  One cooperative
+// launch runs the whole solve with one block per SM.  Each block owns a
+// contiguous range of SELL slices and keeps, for its rows, the inner
+// residual, the FP32 solution increment, A p and the diagonal correction in
+// shared memory (14 bytes a row).  The only global traffic of an inner
+// iteration is the operator (from L2), the gathers of p and the update of p.
+//
+// Arithmetic.  PCG with the Jacobi preconditioner M = diag(1/ad) (Cg.c:47-209,
+// PreCond.c:18-26) is CG on the symmetrically scaled system
+//     (S A S) y = S b,   x = S y,   S = diag(1/sqrt(ad)),
+// whose operator has a unit diagonal, so the inner iteration carries no
+// preconditioner vector.  Its couplings are rounded to FP32 once; a per-row
+// correction delta_i of the unit diagonal keeps the action of the rounded
+// operator on S^-1 1 (the constant vector of the unscaled space, the
+// near-null mode of a diffusion operator) equal to the FP64 one.  The 2-norm
+// of a scaled residual is the reference's M-norm, ||S r||_2 = sqrt(r^T M r)
+// (Cg.c:145).  Inner dot products accumulate in FP64.
+//
+// Reliable updates (Sleijpen & van der Vorst), as in mixed.cu: when the inner
+// estimate has fallen by `delta` since the last refresh, or claims
+// convergence, x += S xs in FP64, r = b - A x is recomputed with the FP64
+// operator, the reference's criterion sqrt|(r, M r)| < tol sqrt|(b, M b)|
+// (Cg.c:70-74, 145) is tested on it, and the inner residual restarts from
+// fl32(S r) with the search direction kept.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "internal.h"
+#include "persist.cuh"
+
+namespace sfr {
+
+namespace {
+
+constexpr int kResNV = 2;          // values of the setup and refresh exchanges
+constexpr int kResChunk = 6;       // slots of a row loaded before their gathers
+
+// Block-to-block exchange without atomics.  Each block owns a 64-byte slot
+// in each of three rotating buffers.  At epoch e a block empties its slot of
+// buffer (e+1) % 3, then (release fence) writes its partial sums into its slot
+// of buffer e % 3; thread b of every block polls block b's slot with relaxed
+// loads until every value has left the "empty" pattern, takes an acquire
+// fence, and the block sums the partials in block order -- the same order in
+// every block, so all blocks hold bit-identical totals.  Buffer (e+1) % 3 last
+// held epoch e-2, which every block finished reading before it published
+// e-1, so emptying it at e is safe; the fence orders the emptying before the
+// publication, so a block that has seen epoch e also sees the empty slots of
+// e+1.  Every wait is bounded: after spin_limit polls a block records
+// SFR_TIMEOUT in *err; a block that sees *err set stops waiting.
+constexpr unsigned long long kEmpty = 0x7ff4deadbeef0001ull;  // a NaN no arithmetic produces
+
+struct alignas(64) ExSlot {
+  unsigned long long v[8];
+};
+
+struct ExSync {
+  ExSlot *slots;  // 3 * nblocks, every word kEmpty at launch
+  int *err;
+  int nblocks;
+  unsigned spin_limit;
+};
+
+// Publishes NV block totals of acc and returns the totals over all blocks in
+// tot (every thread).  The writes of every thread of the block before the
+// call are visible to every thread of every block after it.  `sm` holds
+// 32 * (NV + 1) doubles; the block has at least nblocks threads.
+template <int NV>
+__device__ __forceinline__ bool exchange(const ExSync &f, unsigned &epoch, const double (&acc)[NV],
+                                         double (&tot)[NV], double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = warp_sum(acc[v]);
+    if (lane == 0) sm[v * 32 + warp] = w;
+  }
+  // orders the block's writes of this phase before thread 0's release fence
+  __syncthreads();
+  ++epoch;
+  ExSlot *cur = f.slots + static_cast<size_t>(epoch % 3u) * f.nblocks;
+  ExSlot *nxt = f.slots + static_cast<size_t>((epoch + 1u) % 3u) * f.nblocks;
+  if (warp == 0) {
+    double t[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) t[v] = warp_sum(lane < nw ? sm[v * 32 + lane] : 0.0);
+    if (lane == 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(nxt[blockIdx.x].v[v])
+            .store(kEmpty, cuda::memory_order_relaxed);
+      cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device);
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(cur[blockIdx.x].v[v])
+            .store(static_cast<unsigned long long>(__double_as_longlong(t[v])),
+                   cuda::memory_order_relaxed);
+    }
+  }
+  // thread b watches block b
+  const bool watcher = static_cast<int>(threadIdx.x) < f.nblocks;
+  double val[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) val[v] = 0.0;
+  int seen = !watcher;
+  int ok = 1;
+  cuda::atomic_ref<int, cuda::thread_scope_device> err(*f.err);
+  for (unsigned spins = 0;; ++spins) {
+    if (!seen) {
+      int all = 1;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const unsigned long long u =
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(cur[threadIdx.x].v[v])
+                .load(cuda::memory_order_relaxed);
+        val[v] = __longlong_as_double(static_cast<long long>(u));
+        all &= u != kEmpty;
+      }
+      seen = all;
+    }
+    if (__syncthreads_and(seen)) break;
+    // every exit below is taken by the whole block together
+    if ((spins & 63u) == 63u &&
+        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
+      ok = 0;
+      break;
+    }
+    if (spins > f.spin_limit) {
+      if (threadIdx.x == 0) {
+        int expected = 0;
+        err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+      }
+      ok = 0;
+      break;
+    }
+  }
+  if (watcher) cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+  // totals in block order: lanes within a warp, then warps in order
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = warp_sum(val[v]);
+    if (lane == 0) sm[v * 32 + warp] = w;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double w = warp_sum(lane < nw ? sm[v * 32 + lane] : 0.0);
+      if (lane == 0) sm[NV * 32 + v] = w;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < NV; ++v) tot[v] = sm[NV * 32 + v];
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool exchange_barrier(const ExSync &f, unsigned &epoch, double *sm) {
+  const double z[1] = {0.0};
+  double t[1];
+  return exchange<1>(f, epoch, z, t, sm);
+}
+
+// every word of the exchange buffers to kEmpty
+__global__ void empty_slots_kernel(unsigned long long *w, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    w[i] = kEmpty;
+}
+
+struct ResArgs {
+  int n, nslices;
+  const int *sptr;
+  // inner operator: FP32 scaled couplings and col - row offsets per slot
+  const float *val;
+  const int16_t *off;
+  const float *delta;  // per row: the unit diagonal is 1 + delta
+  // FP64 operator (refreshes and the final residuals)
+  const int *col64;
+  const double *val64;
+  const double *diag;
+  const double *b;
+  double *x;
+  float *p;  // search direction, nslices*32 entries (padding rows stay 0)
+  ExSync xs;
+  SolveOut *out;
+  double tol, rdelta;
+  unsigned maxit;
+  int newx;
+};
+
+// (A x)[row] with the FP64 operator; the matrix streams (evict-first) so the
+// FP32 operator keeps its place in L2.
+__device__ __forceinline__ double row_fp64(const ResArgs &a, int s, int lane, int row) {
+  const int base = __ldg(a.sptr + s);
+  const int w = (__ldg(a.sptr + s + 1) - base) >> 5;
+  double y = ld_vec(a.diag + row) * ld_vec(a.x + row);
+  const int *c = a.col64 + base + lane;
+  const double *v = a.val64 + base + lane;
+#pragma unroll 2
+  for (int e = 0; e < w; ++e) y = fma(ld_stream(v + e * kWarp), ld_vec(a.x + ld_stream(c + e * kWarp)), y);
+  return y;
+}
+
+// (A_s p)[row] of the scaled FP32 operator, accumulated in FP64 from the unit
+// diagonal: p_row (1 + delta_row) + sum_e val_e p_(row + off_e).
+__device__ __forceinline__ double row_scaled(const ResArgs &a, int s, int lane, int row,
+                                             float p_row, float dlt) {
+  const int base = __ldg(a.sptr + s);
+  const int w = (__ldg(a.sptr + s + 1) - base) >> 5;
+  double y = static_cast<double>(p_row) + static_cast<double>(dlt) * static_cast<double>(p_row);
+  const float *v = a.val + base + lane;
+  const int16_t *o = a.off + base + lane;
+  for (int e0 = 0; e0 < w; e0 += kResChunk) {
+    int jj[kResChunk];
+    float vv[kResChunk];
+#pragma unroll
+    for (int u = 0; u < kResChunk; ++u)
+      if (e0 + u < w) {
+        jj[u] = row + static_cast<int>(__ldcg(o + (e0 + u) * kWarp));
+        vv[u] = __ldcg(v + (e0 + u) * kWarp);
+      }
+#pragma unroll
+    for (int u = 0; u < kResChunk; ++u)
+      if (e0 + u < w)
+        y = fma(static_cast<double>(vv[u]), static_cast<double>(ld_vec(a.p + jj[u])), y);
+  }
+  return y;
+}
+
+// This block's rows, slice by slice: warp w takes slices s0 + w, s0 + w + NW,
+// ...; defines s (slice), row and lr (row within the block's shared state).
+#define SFR_RES_FOR(s, row, lr)                                             \
+  for (int s = s0 + warp; s < s1; s += NW)                                  \
+    for (int row = s * kWarp + lane, lr = row - r0, once_ = 1; once_; once_ = 0)
+
+// Refresh: r = b - A x in FP64 for this block's rows, r_s = fl32(S r) into
+// shared memory (and p = r_s on the first call), xs = 0.
+// tot[0] = (r, M r) = sum r^2 / ad, tot[1] = (r_s, r_s).
+template <int kT>
+__device__ __forceinline__ bool refresh(const ResArgs &a, int s0, int s1, int r0, float *sm_r,
+                                        float *sm_xs, bool first, unsigned &epoch, double *red,
+                                        double (&tot)[kResNV]) {
+  constexpr int NW = kT / kWarp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double acc[kResNV] = {0.0, 0.0};
+  SFR_RES_FOR(s, row, lr) {
+    float rs = 0.0f;
+    if (row < a.n) {
+      const double d = ld_vec(a.diag + row);
+      const double r = ld_vec(a.b + row) - row_fp64(a, s, lane, row);
+      rs = __double2float_rn(r / sqrt(d));
+      acc[0] += r * (r / d);
+      acc[1] += static_cast<double>(rs) * static_cast<double>(rs);
+    }
+    sm_r[lr] = rs;
+    sm_xs[lr] = 0.0f;
+    if (first) st_vec(a.p + row, rs);
+  }
+  return exchange<kResNV>(a.xs, epoch, acc, tot, red);
+}
+
+// x += S (xs + a_pend p) in FP64 for this block's rows; xs = 0.  a_pend is
+// the step of the current direction not yet added to xs.
+template <int kT>
+__device__ __forceinline__ void fold(const ResArgs &a, int s0, int s1, int r0, float *sm_xs,
+                                     float a_pend) {
+  constexpr int NW = kT / kWarp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  SFR_RES_FOR(s, row, lr) {
+    if (row < a.n) {
+      const float xs = fmaf(a_pend, ld_vec(a.p + row), sm_xs[lr]);
+      st_vec(a.x + row, ld_vec(a.x + row) + static_cast<double>(xs) / sqrt(ld_vec(a.diag + row)));
+    }
+    sm_xs[lr] = 0.0f;
+  }
+}
+
+// Iteration j (one exchange of partial sums and one barrier):
+//   q = A_s p ; (p, q), (r, q), (q, q), (r, r)                 [exchange]
+//   alpha = (r, r) / (p, q)
+//   (r', r') = (r, r) - 2 alpha (r, q) + alpha^2 (q, q)   for r' = r - alpha q
+//   (refresh when due)
+//   r = r - alpha q ; xs += alpha p ; p = r + beta p            [barrier]
+// The norm of the next residual follows from dot products the SpMV phase
+// already forms, so the residual update needs no exchange of its own; it is
+// accumulated in FP64 and only decides beta and when to refresh.  The next
+// SpMV phase recomputes (r, r) from the stored residual, so the recurrence's
+// alpha always uses the norm of the r it holds.
+template <int kT>
+__global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
+  constexpr int NW = kT / kWarp;
+  extern __shared__ float sm_dyn[];
+  __shared__ double red[32 * 5];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int r0 = s0 * kWarp;
+  const int rows = (s1 - s0) * kWarp;
+  float *sm_r = sm_dyn;           // inner residual (scaled)
+  float *sm_xs = sm_r + rows;     // FP32 solution increment (scaled)
+  float *sm_q = sm_xs + rows;     // A_s p
+  // diagonal correction, bf16: it is ~1e-7 of the unit diagonal, so 8 bits
+  // of it leave the operator's row sums exact to ~1e-9 relative
+  __nv_bfloat16 *sm_d = reinterpret_cast<__nv_bfloat16 *>(sm_q + rows);
+  unsigned epoch = 0;
+
+  // setup: delta into shared memory, x0, (b, M b), (b, b)
+  double bm = 0.0, bnorm = 0.0;
+  {
+    double acc[kResNV] = {0.0, 0.0}, tot[kResNV];
+    for (int lr = threadIdx.x; lr < rows; lr += kT) {
+      const int row = r0 + lr;
+      sm_d[lr] = __float2bfloat16_rn(row < a.n ? ld_vec(a.delta + row) : 0.0f);
+      if (row < a.n) {
+        if (a.newx) st_vec(a.x + row, 0.0);
+        const double bk = ld_vec(a.b + row);
+        acc[0] += bk * (bk / ld_vec(a.diag + row));
+        acc[1] += bk * bk;
+      }
+    }
+    if (!exchange<kResNV>(a.xs, epoch, acc, tot, red)) return;
+    bm = tot[0];
+    bnorm = sqrt(tot[1]);
+  }
+  const double conv = a.tol * sqrt(fabs(bm));
+  double d = 0.0, rmax;  // d: (r, r) of the residual the last direction was built from
+  bool act = true;
+  int status = SFR_OK, refine = 0;
+  unsigned iters = 0;
+  {
+    double tot[kResNV];
+    if (!refresh<kT>(a, s0, s1, r0, sm_r, sm_xs, true, epoch, red, tot)) return;
+    rmax = sqrt(fabs(tot[0]));
+    if (rmax < conv) act = false;
+  }
+  float a_pend = 0.0f;  // alpha of the current direction, not yet in xs
+  unsigned j = 0;
+  for (; j < a.maxit && act; ++j) {
+    // q = A_s p and the four dot products
+    double alpha, di;
+    {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0}, tot[4];
+      SFR_RES_FOR(s, row, lr) {
+        const float pr = ld_vec(a.p + row);
+        const float qi = __double2float_rn(
+            row_scaled(a, s, lane, row, pr, __bfloat162float(sm_d[lr])));
+        const float ri = sm_r[lr];
+        sm_q[lr] = qi;
+        acc[0] += static_cast<double>(qi) * static_cast<double>(pr);
+        acc[1] += static_cast<double>(qi) * static_cast<double>(ri);
+        acc[2] += static_cast<double>(qi) * static_cast<double>(qi);
+        acc[3] += static_cast<double>(ri) * static_cast<double>(ri);
+      }
+      if (!exchange<4>(a.xs, epoch, acc, tot, red)) return;
+      d = tot[3];
+      alpha = d / tot[0];
+      di = d - 2.0 * alpha * tot[1] + alpha * alpha * tot[2];
+      if (!isfinite(alpha) || !isfinite(di)) {
+        act = false;
+        status = SFR_BREAKDOWN;
+        iters = j + 1;
+        break;
+      }
+      a_pend = static_cast<float>(alpha);
+    }
+    const double est = sqrt(fabs(di));
+    double beta;
+    bool step = true;  // r -= alpha q still to do
+    if (est < a.rdelta * rmax || est < conv) {
+      // reliable update: x += S (xs + alpha p), r = fl32(S (b - A x))
+      fold<kT>(a, s0, s1, r0, sm_xs, a_pend);
+      a_pend = 0.0f;
+      step = false;
+      if (!exchange_barrier(a.xs, epoch, red)) return;
+      double tot[kResNV];
+      if (!refresh<kT>(a, s0, s1, r0, sm_r, sm_xs, false, epoch, red, tot)) return;
+      ++refine;
+      const double tr = sqrt(fabs(tot[0]));
+      if (tr < conv) {
+        act = false;
+        iters = j + 1;
+        break;
+      }
+      beta = tot[1] / d;
+      rmax = tr;
+    } else {
+      beta = di / d;
+    }
+    // r -= alpha q ; xs += alpha p ; p = r + beta p
+    {
+      const float bf = static_cast<float>(beta);
+      SFR_RES_FOR(s, row, lr) {
+        const float pr = ld_vec(a.p + row);
+        const float ri = step ? fmaf(-a_pend, sm_q[lr], sm_r[lr]) : sm_r[lr];
+        sm_r[lr] = ri;
+        sm_xs[lr] = fmaf(a_pend, pr, sm_xs[lr]);
+        st_vec(a.p + row, fmaf(bf, pr, ri));
+      }
+      a_pend = 0.0f;
+      if (!exchange_barrier(a.xs, epoch, red)) return;
+    }
+  }
+  if (act) {  // iteration cap
+    status = SFR_MAXIT;
+    iters = j + 1;
+  }
+  if (status != SFR_OK) {  // fold the last increment (a converged solve has folded it)
+    fold<kT>(a, s0, s1, r0, sm_xs, a_pend);
+    if (!exchange_barrier(a.xs, epoch, red)) return;
+  }
+  // xKx, ||x||, ||b - Ax||_M, ||b - Ax|| (Cg.c:155-176)
+  double acc[4] = {0.0, 0.0, 0.0, 0.0}, tot[4];
+  SFR_RES_FOR(s, row, lr) {
+    (void)lr;
+    if (row < a.n) {
+      const double y = row_fp64(a, s, lane, row);
+      const double xk = ld_vec(a.x + row);
+      const double rk = ld_vec(a.b + row) - y;
+      acc[0] += xk * y;
+      acc[1] += xk * xk;
+      acc[2] += rk * (rk / ld_vec(a.diag + row));
+      acc[3] += rk * rk;
+    }
+  }
+  if (!exchange<4>(a.xs, epoch, acc, tot, red)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    SolveOut o;
+    o.iters = static_cast<int>(iters);
+    o.status = status;
+    o.xKx = tot[0];
+    o.norm_x = sqrt(tot[1]);
+    o.norm_r_m = sqrt(fabs(tot[2]));
+    o.norm_r = sqrt(tot[3]);
+    o.conv = conv;
+    o.bnorm = bnorm;
+    o.refinements = refine;
+    o.inner_iters = static_cast<int>(iters);
+    *a.out = o;
+  }
+}
+
+#undef SFR_RES_FOR
+
+// Scaled FP32 operator from the FP64 SELL values and the diagonal:
+//   val_e = fl32(a_e / sqrt(ad_row ad_col)),  off_e = col_e - row,
+//   delta_row = -sum_e (val_e - a_e / sqrt(ad_row ad_col)) sqrt(ad_col / ad_row).
+// *bad is set when a diagonal entry is not positive and finite.
+__global__ void scaled_operator_kernel(const int *sptr, const int *col, const double *val,
+                                       const double *diag, int n, int nslices, float *sval,
+                                       int16_t *off, float *delta, int *bad) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nslices * kWarp; t += stride) {
+    const int s = t >> 5, lane = t & 31, row = t;
+    const int base = sptr[s];
+    const int w = (sptr[s + 1] - base) >> 5;
+    if (row >= n) {
+      for (int k = 0; k < w; ++k) {
+        sval[base + k * kWarp + lane] = 0.0f;
+        off[base + k * kWarp + lane] = 0;
+      }
+      continue;
+    }
+    const double di = diag[row];
+    if (!(di > 0.0) || !isfinite(di)) {
+      atomicExch(bad, 1);
+      continue;
+    }
+    const double si = 1.0 / sqrt(di);
+    double acc = 0.0;
+    for (int k = 0; k < w; ++k) {
+      const int e = base + k * kWarp + lane;
+      const int c = col[e];
+      const double dc = diag[c];
+      const double sc = dc > 0.0 ? sqrt(dc) : 0.0;
+      const double exact = sc > 0.0 ? val[e] * si / sc : 0.0;
+      const float f = __double2float_rn(exact);
+      sval[e] = f;
+      off[e] = static_cast<int16_t>(c - row);
+      acc += (static_cast<double>(f) - exact) * sc;
+    }
+    delta[row] = __double2float_rn(-acc * si);
+  }
+}
+
+int ensure_scaled_operator(sfr_system *s, cudaStream_t st) {
+  const int64_t nslots = s->A.nslots;
+  if (!s->d_rval) {
+    const size_t ns = static_cast<size_t>(std::max<int64_t>(nslots, 1));
+    if (cudaMalloc(&s->d_rval, sizeof(float) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
+    if (cudaMalloc(&s->d_roff, sizeof(int16_t) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
+    if (cudaMalloc(&s->d_rdelta, sizeof(float) * std::max(s->n, 1)) != cudaSuccess)
+      return SFR_CUDA_ERROR;
+    if (cudaMalloc(&s->d_rbad, sizeof(int)) != cudaSuccess) return SFR_CUDA_ERROR;
+    s->bytes += static_cast<int64_t>((sizeof(float) + sizeof(int16_t)) * ns +
+                                     sizeof(float) * s->n + sizeof(int));
+  }
+  if (s->resident_epoch == s->values_epoch) return SFR_OK;
+  if (cudaMemsetAsync(s->d_rbad, 0, sizeof(int), st) != cudaSuccess) return SFR_CUDA_ERROR;
+  const int grid = static_cast<int>(
+      std::min<int64_t>((static_cast<int64_t>(s->A.nslices) * kWarp + 255) / 256, 8192));
+  scaled_operator_kernel<<<std::max(grid, 1), 256, 0, st>>>(
+      s->A.sptr, s->A.col, s->A.val, s->d_diag, s->n, s->A.nslices, s->d_rval, s->d_roff,
+      s->d_rdelta, s->d_rbad);
+  if (cudaGetLastError() != cudaSuccess) return SFR_CUDA_ERROR;
+  int bad = 0;
+  if (cudaMemcpyAsync(&bad, s->d_rbad, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SFR_CUDA_ERROR;
+  s->resident_epoch = s->values_epoch;
+  s->resident_ok = bad == 0;
+  return SFR_OK;
+}
+
+// Launch shape: one block of 1024 threads per SM, 14 bytes of shared state
+// per row.
+constexpr int kResThreads = 1024;
+
+int max_smem_optin(int device) {
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+    return 0;
+  return v;
+}
+
+// Dynamic shared memory of a block, or 0 when a block's rows do not fit.
+size_t block_smem(int nslices, int grid, int device) {
+  const int per_block = (nslices + grid - 1) / grid;
+  const size_t bytes = static_cast<size_t>(per_block) * kWarp * (3 * sizeof(float) + 2);
+  // static shared memory of the kernel (reductions) comes on top
+  if (bytes + 4096 > static_cast<size_t>(max_smem_optin(device))) return 0;
+  return std::max<size_t>(bytes, 16);
+}
+
+}  // namespace
+
+bool resident_fits(sfr_system *s) {
+  if (s->bandwidth > 32767) return false;
+  return block_smem(s->A.nslices, std::max(1, num_sms(s->device)), s->device) != 0;
+}
+
+int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, uint32_t maxit,
+                   int32_t newx, cudaStream_t st, sfr_solve_info *info) {
+  if (maxit == 0) return SFR_BAD_INPUT;
+  if (!resident_fits(s)) return SFR_UNSUPPORTED;
+  int rc = ensure_scaled_operator(s, st);
+  if (rc != SFR_OK) return rc;
+  if (!s->resident_ok) return SFR_UNSUPPORTED;  // Jacobi scaling needs ad > 0
+  // a block per SM, fewer for small systems (a slice per warp at least):
+  // the cost of an exchange grows with the blocks taking part
+  const int grid = std::max(1, std::min(num_sms(s->device),
+                                        (s->A.nslices + kResThreads / kWarp - 1) /
+                                            (kResThreads / kWarp)));
+  const size_t smem = block_smem(s->A.nslices, grid, s->device);
+  if (!smem) return SFR_UNSUPPORTED;
+  void (*kern)(ResArgs) = pcg_resident_kernel<kResThreads>;
+  if (cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return SFR_CUDA_ERROR;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kResThreads, smem) !=
+          cudaSuccess ||
+      occ < 1)
+    return SFR_UNSUPPORTED;
+
+  auto align = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+  const size_t p_bytes = align(sizeof(float) * static_cast<size_t>(s->A.nslices) * kWarp);
+  const size_t part_bytes = align(sizeof(ExSlot) * 3 * static_cast<size_t>(grid));
+  const size_t ctl_bytes = 256;
+  const size_t out_bytes = align(sizeof(SolveOut));
+  rc = ensure_workspace(s, p_bytes + part_bytes + ctl_bytes + out_bytes);
+  if (rc != SFR_OK) return rc;
+  char *base = static_cast<char *>(s->ws.base);
+
+  ResArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = s->n;
+  a.nslices = s->A.nslices;
+  a.sptr = s->A.sptr;
+  a.val = s->d_rval;
+  a.off = s->d_roff;
+  a.delta = s->d_rdelta;
+  a.col64 = s->A.col;
+  a.val64 = s->A.val;
+  a.diag = s->d_diag;
+  a.b = d_b;
+  a.x = d_x;
+  a.p = reinterpret_cast<float *>(base);
+  a.xs.slots = reinterpret_cast<ExSlot *>(base + p_bytes);
+  unsigned *ctl = reinterpret_cast<unsigned *>(base + p_bytes + part_bytes);
+  a.xs.err = reinterpret_cast<int *>(ctl);
+  a.xs.nblocks = grid;
+  a.xs.spin_limit = 1u << 22;
+  a.out = reinterpret_cast<SolveOut *>(base + p_bytes + part_bytes + ctl_bytes);
+  a.tol = tol;
+  a.rdelta = reliable_delta(SFR_PCG);
+  a.maxit = maxit;
+  a.newx = newx;
+
+  // padding rows of p must read as 0
+  if (cudaMemsetAsync(a.p, 0, p_bytes, st) != cudaSuccess) return SFR_CUDA_ERROR;
+  // epochs restart at 0 in every launch, with every slot empty
+  if (cudaMemsetAsync(ctl, 0, ctl_bytes, st) != cudaSuccess) return SFR_CUDA_ERROR;
+  {
+    const int words = static_cast<int>(part_bytes / sizeof(unsigned long long));
+    empty_slots_kernel<<<std::min((words + 255) / 256, 64), 256, 0, st>>>(
+        reinterpret_cast<unsigned long long *>(a.xs.slots), words);
+    if (cudaGetLastError() != cudaSuccess) return SFR_CUDA_ERROR;
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return SFR_CUDA_ERROR;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return SFR_CUDA_ERROR;
+  }
+  void *params[] = {&a};
+  cudaEventRecord(e0, st);
+  const cudaError_t le = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), dim3(grid),
+                                                     dim3(kResThreads), params, smem, st);
+  cudaEventRecord(e1, st);
+  SolveOut out{};
+  int err = 0;
+  cudaError_t ce = le;
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(&out, a.out, sizeof(SolveOut), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess)
+    ce = cudaMemcpyAsync(&err, a.xs.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  float ms = 0.f;
+  if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ce != cudaSuccess) {
+    set_last_error(cudaGetErrorString(ce));
+    return SFR_CUDA_ERROR;
+  }
+  if (err != 0) return err;
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iters = out.iters;
+    info->status = out.status;
+    info->xKx = out.xKx;
+    info->norm_x = out.norm_x;
+    info->norm_r = out.norm_r;
+    info->norm_r_m = out.norm_r_m;
+    info->conv = out.conv;
+    info->seconds = ms * 1e-3;
+    info->refinements = out.refinements;
+    info->inner_iters = out.inner_iters;
+    info->relres = out.bnorm > 0 ? out.norm_r / out.bnorm : 0.0;
+  }
+  return out.status;
+}
+
+}  // namespace sfr

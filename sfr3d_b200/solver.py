@@ -21,7 +21,7 @@ CSRD, CSRC, ELLPACK = 2, 3, 4
 OK, MAXIT, BREAKDOWN = 0, 1, 2
 BAD_INPUT, CUDA_ERROR, TIMEOUT, UNSUPPORTED = -1, -2, -3, -4
 FP64, MIXED = 0, 1
-ENGINE_AUTO, ENGINE_PERSISTENT, ENGINE_GRAPH = 0, 1, 2
+ENGINE_AUTO, ENGINE_PERSISTENT, ENGINE_GRAPH, ENGINE_LOOP, ENGINE_RESIDENT = 0, 1, 2, 3, 4
 
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -180,7 +180,9 @@ class GpuSystem:
         self.close()
 
     def set_engine(self, engine: int, threads: int = 0, slices_per_warp: int = 0):
-        """0 automatic, 1 persistent (one cooperative launch), 2 graph."""
+        """0 automatic, 1 persistent (one cooperative launch), 2 graph,
+        3 graph kernels from a host loop (profilers), 4 resident (mixed
+        PCG, one right-hand side, inner iteration held on chip)."""
         rc = lib().sfr_gpu_set_engine(self.h, engine, threads, slices_per_warp)
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_engine")
