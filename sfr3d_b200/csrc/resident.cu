@@ -7,9 +7,11 @@
 // iteration to the next; the FP64 operator (150 MB) cannot.  One cooperative
 // launch runs the whole solve with one block per SM.  Each block owns a
 // contiguous range of SELL slices and keeps, for its rows, the inner
-// residual, the FP32 solution increment, A p and the diagonal correction in
-// shared memory (14 bytes a row).  The only global traffic of an inner
-// iteration is the operator (from L2), the gathers of p and the update of p.
+// residual, the FP32 solution increment, A p and (when it fits) the
+// diagonal correction in shared memory (16 bytes a row).  The global traffic
+// of an inner iteration is the operator (from L2), the gathers of p and the
+// update of p; one exchange of partial sums and one barrier separate its two
+// phases.
 //
 // Arithmetic.  PCG with the Jacobi preconditioner M = diag(1/ad) (Cg.c:47-209,
 // PreCond.c:18-26) is CG on the symmetrically scaled system
@@ -28,7 +30,6 @@
 // operator, the reference's criterion sqrt|(r, M r)| < tol sqrt|(b, M b)|
 // (Cg.c:70-74, 145) is tested on it, and the inner residual restarts from
 // fl32(S r) with the search direction kept.
-#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,66 +45,71 @@ namespace sfr {
 namespace {
 
 constexpr int kResNV = 2;          // values of the setup and refresh exchanges
-constexpr int kResChunk = 6;       // slots of a row loaded before their gathers
+constexpr int kResChunk = 6;       // slots of a row loaded before their gathers (a hex cell's faces)
 
 // Block-to-block exchange without atomics.  Each block owns a 64-byte slot
-// in each of three rotating buffers.  At epoch e a block empties its slot of
-// buffer (e+1) % 3, then (release fence) writes its partial sums into its slot
-// of buffer e % 3; thread b of every block polls block b's slot with relaxed
-// loads until every value has left the "empty" pattern, takes an acquire
-// fence, and the block sums the partials in block order -- the same order in
-// every block, so all blocks hold bit-identical totals.  Buffer (e+1) % 3 last
-// held epoch e-2, which every block finished reading before it published
-// e-1, so emptying it at e is safe; the fence orders the emptying before the
-// publication, so a block that has seen epoch e also sees the empty slots of
-// e+1.  Every wait is bounded: after spin_limit polls a block records
+// (eight 64-bit words) in each of three rotating buffers; epoch e uses buffer
+// e % 3.  A block publishes its partial sums by storing every word of its slot
+// with the two lowest bits of the FP64 pattern replaced by e & 3 (a change of
+// at most 3 units in the last place, the same in every block); thread b of
+// every block polls block b's words with relaxed loads until they carry the
+// tag, and the block sums the partials in block order -- the same order in
+// every block, so all blocks hold bit-identical totals.  Every word of buffer
+// e % 3 was last written at epoch e - 3, whose tag differs from e's, and every
+// block finished reading it before it published e - 2, so nothing needs
+// emptying between uses.  The values travel
+// inside the polled words: an exchange is one L2 round trip.
+// kFence additionally makes every global write of every block before the
+// call visible to every block after it (release fence before publishing,
+// acquire fence after the poll); exchanges that only carry partial sums skip
+// both.  Every wait is bounded: after spin_limit polls a block records
 // SFR_TIMEOUT in *err; a block that sees *err set stops waiting.
-constexpr unsigned long long kEmpty = 0x7ff4deadbeef0001ull;  // a NaN no arithmetic produces
-
 struct alignas(64) ExSlot {
   unsigned long long v[8];
 };
 
 struct ExSync {
-  ExSlot *slots;  // 3 * nblocks, every word kEmpty at launch
+  ExSlot *slots;  // 3 * nblocks, zero at launch
   int *err;
   int nblocks;
   unsigned spin_limit;
 };
 
+__device__ __forceinline__ unsigned long long tagged(double v, unsigned tag) {
+  return (static_cast<unsigned long long>(__double_as_longlong(v)) & ~3ull) | tag;
+}
+
 // Publishes NV block totals of acc and returns the totals over all blocks in
-// tot (every thread).  The writes of every thread of the block before the
-// call are visible to every thread of every block after it.  `sm` holds
-// 32 * (NV + 1) doubles; the block has at least nblocks threads.
-template <int NV>
+// tot (every thread).  `sm` holds 32 * (NV + 1) doubles; the block has at
+// least nblocks threads.
+template <int NV, bool kFence>
 __device__ __forceinline__ bool exchange(const ExSync &f, unsigned &epoch, const double (&acc)[NV],
                                          double (&tot)[NV], double *sm) {
+  static_assert(NV >= 1 && NV <= 8, "eight words a slot");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     const double w = warp_sum(acc[v]);
     if (lane == 0) sm[v * 32 + warp] = w;
   }
-  // orders the block's writes of this phase before thread 0's release fence
+  // with kFence, also orders the block's global writes before the release
   __syncthreads();
   ++epoch;
+  const unsigned tag = epoch & 3u;
   ExSlot *cur = f.slots + static_cast<size_t>(epoch % 3u) * f.nblocks;
-  ExSlot *nxt = f.slots + static_cast<size_t>((epoch + 1u) % 3u) * f.nblocks;
   if (warp == 0) {
     double t[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) t[v] = warp_sum(lane < nw ? sm[v * 32 + lane] : 0.0);
     if (lane == 0) {
+      if (kFence) cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device);
+      // every word of the slot takes the new tag, also those this exchange
+      // does not use: a word left untouched could carry a matching tag from
+      // twelve epochs back when a later exchange polls it
 #pragma unroll
-      for (int v = 0; v < NV; ++v)
-        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(nxt[blockIdx.x].v[v])
-            .store(kEmpty, cuda::memory_order_relaxed);
-      cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device);
-#pragma unroll
-      for (int v = 0; v < NV; ++v)
+      for (int v = 0; v < 8; ++v)
         cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(cur[blockIdx.x].v[v])
-            .store(static_cast<unsigned long long>(__double_as_longlong(t[v])),
-                   cuda::memory_order_relaxed);
+            .store(tagged(v < NV ? t[v < NV ? v : 0] : 0.0, tag), cuda::memory_order_relaxed);
     }
   }
   // thread b watches block b
@@ -123,7 +129,7 @@ __device__ __forceinline__ bool exchange(const ExSync &f, unsigned &epoch, const
             cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(cur[threadIdx.x].v[v])
                 .load(cuda::memory_order_relaxed);
         val[v] = __longlong_as_double(static_cast<long long>(u));
-        all &= u != kEmpty;
+        all &= (u & 3ull) == tag;
       }
       seen = all;
     }
@@ -143,7 +149,8 @@ __device__ __forceinline__ bool exchange(const ExSync &f, unsigned &epoch, const
       break;
     }
   }
-  if (watcher) cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+  if (kFence && watcher)
+    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
   // totals in block order: lanes within a warp, then warps in order
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
@@ -164,33 +171,29 @@ __device__ __forceinline__ bool exchange(const ExSync &f, unsigned &epoch, const
   return ok != 0;
 }
 
+// A barrier that also publishes the global writes before it.
 __device__ __forceinline__ bool exchange_barrier(const ExSync &f, unsigned &epoch, double *sm) {
   const double z[1] = {0.0};
   double t[1];
-  return exchange<1>(f, epoch, z, t, sm);
-}
-
-// every word of the exchange buffers to kEmpty
-__global__ void empty_slots_kernel(unsigned long long *w, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    w[i] = kEmpty;
+  return exchange<1, true>(f, epoch, z, t, sm);
 }
 
 struct ResArgs {
   int n, nslices;
   const int *sptr;
-  // inner operator: FP32 scaled couplings and col - row offsets per slot
+  // inner operator: FP32 scaled couplings and col - row offsets per slot,
+  // per row the correction of the unit diagonal (nslices * 32 entries)
   const float *val;
   const int16_t *off;
-  const float *delta;  // per row: the unit diagonal is 1 + delta
+  const float *delta;
   // FP64 operator (refreshes and the final residuals)
   const int *col64;
   const double *val64;
   const double *diag;
   const double *b;
   double *x;
-  float *p;  // search direction, nslices*32 entries (padding rows stay 0)
-  ExSync xs;
+  float *p;  // search direction, nslices * 32 entries (padding rows stay 0)
+  ExSync ex;
   SolveOut *out;
   double tol, rdelta;
   unsigned maxit;
@@ -210,13 +213,14 @@ __device__ __forceinline__ double row_fp64(const ResArgs &a, int s, int lane, in
   return y;
 }
 
-// (A_s p)[row] of the scaled FP32 operator, accumulated in FP64 from the unit
-// diagonal: p_row (1 + delta_row) + sum_e val_e p_(row + off_e).
-__device__ __forceinline__ double row_scaled(const ResArgs &a, int s, int lane, int row,
-                                             float p_row, float dlt) {
-  const int base = __ldg(a.sptr + s);
-  const int w = (__ldg(a.sptr + s + 1) - base) >> 5;
-  double y = static_cast<double>(p_row) + static_cast<double>(dlt) * static_cast<double>(p_row);
+// (A_s p)[row] for one slice of the block (base and width from the block's
+// slice pointers in shared memory), accumulated in FP64 from the unit
+// diagonal: p_row (1 + delta_row) + sum_e val_e p_(row + off_e).  A chunk of
+// slots -- offsets, couplings -- is loaded before its gathers, so a slice
+// costs two dependent L2 round trips.
+__device__ __forceinline__ double row_scaled(const ResArgs &a, int base, int w, int lane,
+                                             int row, float p_row, float dl) {
+  double y = fma(static_cast<double>(dl), static_cast<double>(p_row), static_cast<double>(p_row));
   const float *v = a.val + base + lane;
   const int16_t *o = a.off + base + lane;
   for (int e0 = 0; e0 < w; e0 += kResChunk) {
@@ -244,7 +248,8 @@ __device__ __forceinline__ double row_scaled(const ResArgs &a, int s, int lane, 
 
 // Refresh: r = b - A x in FP64 for this block's rows, r_s = fl32(S r) into
 // shared memory (and p = r_s on the first call), xs = 0.
-// tot[0] = (r, M r) = sum r^2 / ad, tot[1] = (r_s, r_s).
+// tot[0] = (r, M r) = sum r^2 / ad, tot[1] = (r_s, r_s).  The first call
+// publishes p (and x) to every block.
 template <int kT>
 __device__ __forceinline__ bool refresh(const ResArgs &a, int s0, int s1, int r0, float *sm_r,
                                         float *sm_xs, bool first, unsigned &epoch, double *red,
@@ -265,7 +270,8 @@ __device__ __forceinline__ bool refresh(const ResArgs &a, int s0, int s1, int r0
     sm_xs[lr] = 0.0f;
     if (first) st_vec(a.p + row, rs);
   }
-  return exchange<kResNV>(a.xs, epoch, acc, tot, red);
+  return first ? exchange<kResNV, true>(a.ex, epoch, acc, tot, red)
+               : exchange<kResNV, false>(a.ex, epoch, acc, tot, red);
 }
 
 // x += S (xs + a_pend p) in FP64 for this block's rows; xs = 0.  a_pend is
@@ -284,7 +290,7 @@ __device__ __forceinline__ void fold(const ResArgs &a, int s0, int s1, int r0, f
   }
 }
 
-// Iteration j (one exchange of partial sums and one barrier):
+// Iteration j (one exchange of partial sums, one barrier):
 //   q = A_s p ; (p, q), (r, q), (q, q), (r, r)                 [exchange]
 //   alpha = (r, r) / (p, q)
 //   (r', r') = (r, r) - 2 alpha (r, q) + alpha^2 (q, q)   for r' = r - alpha q
@@ -295,7 +301,7 @@ __device__ __forceinline__ void fold(const ResArgs &a, int s0, int s1, int r0, f
 // accumulated in FP64 and only decides beta and when to refresh.  The next
 // SpMV phase recomputes (r, r) from the stored residual, so the recurrence's
 // alpha always uses the norm of the r it holds.
-template <int kT>
+template <int kT, bool kDeltaShared>
 __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
   constexpr int NW = kT / kWarp;
   extern __shared__ float sm_dyn[];
@@ -305,21 +311,22 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
   block_slices(a.nslices, &s0, &s1);
   const int r0 = s0 * kWarp;
   const int rows = (s1 - s0) * kWarp;
-  float *sm_r = sm_dyn;           // inner residual (scaled)
-  float *sm_xs = sm_r + rows;     // FP32 solution increment (scaled)
-  float *sm_q = sm_xs + rows;     // A_s p
-  // diagonal correction, bf16: it is ~1e-7 of the unit diagonal, so 8 bits
-  // of it leave the operator's row sums exact to ~1e-9 relative
-  __nv_bfloat16 *sm_d = reinterpret_cast<__nv_bfloat16 *>(sm_q + rows);
+  float *sm_r = sm_dyn;          // inner residual (scaled)
+  float *sm_xs = sm_r + rows;    // FP32 solution increment (scaled)
+  float *sm_q = sm_xs + rows;    // A_s p
+  float *sm_d = sm_q + rows;     // diagonal correction (kDeltaShared)
+  int *sm_sp = reinterpret_cast<int *>(sm_q + (kDeltaShared ? 2 : 1) * rows);  // slice pointers
   unsigned epoch = 0;
+  for (int i = threadIdx.x; i <= s1 - s0; i += kT) sm_sp[i] = __ldg(a.sptr + s0 + i);
+  if (kDeltaShared)
+    for (int lr = threadIdx.x; lr < rows; lr += kT) sm_d[lr] = __ldcg(a.delta + r0 + lr);
 
-  // setup: delta into shared memory, x0, (b, M b), (b, b)
+  // setup: x0, (b, M b), (b, b)
   double bm = 0.0, bnorm = 0.0;
   {
     double acc[kResNV] = {0.0, 0.0}, tot[kResNV];
     for (int lr = threadIdx.x; lr < rows; lr += kT) {
       const int row = r0 + lr;
-      sm_d[lr] = __float2bfloat16_rn(row < a.n ? ld_vec(a.delta + row) : 0.0f);
       if (row < a.n) {
         if (a.newx) st_vec(a.x + row, 0.0);
         const double bk = ld_vec(a.b + row);
@@ -327,7 +334,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
         acc[1] += bk * bk;
       }
     }
-    if (!exchange<kResNV>(a.xs, epoch, acc, tot, red)) return;
+    if (!exchange<kResNV, true>(a.ex, epoch, acc, tot, red)) return;
     bm = tot[0];
     bnorm = sqrt(tot[1]);
   }
@@ -349,18 +356,22 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
     double alpha, di;
     {
       double acc[4] = {0.0, 0.0, 0.0, 0.0}, tot[4];
-      SFR_RES_FOR(s, row, lr) {
-        const float pr = ld_vec(a.p + row);
-        const float qi = __double2float_rn(
-            row_scaled(a, s, lane, row, pr, __bfloat162float(sm_d[lr])));
+      auto dots = [&](int lr, float qi, float pr) {
         const float ri = sm_r[lr];
         sm_q[lr] = qi;
         acc[0] += static_cast<double>(qi) * static_cast<double>(pr);
         acc[1] += static_cast<double>(qi) * static_cast<double>(ri);
         acc[2] += static_cast<double>(qi) * static_cast<double>(qi);
         acc[3] += static_cast<double>(ri) * static_cast<double>(ri);
+      };
+      SFR_RES_FOR(s, row, lr) {
+        const int base = sm_sp[s - s0];
+        const int w = (sm_sp[s - s0 + 1] - base) >> 5;
+        const float pr = ld_vec(a.p + row);
+        const float dl = kDeltaShared ? sm_d[lr] : __ldcg(a.delta + row);
+        dots(lr, __double2float_rn(row_scaled(a, base, w, lane, row, pr, dl)), pr);
       }
-      if (!exchange<4>(a.xs, epoch, acc, tot, red)) return;
+      if (!exchange<4, false>(a.ex, epoch, acc, tot, red)) return;
       d = tot[3];
       alpha = d / tot[0];
       di = d - 2.0 * alpha * tot[1] + alpha * alpha * tot[2];
@@ -380,7 +391,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
       fold<kT>(a, s0, s1, r0, sm_xs, a_pend);
       a_pend = 0.0f;
       step = false;
-      if (!exchange_barrier(a.xs, epoch, red)) return;
+      if (!exchange_barrier(a.ex, epoch, red)) return;
       double tot[kResNV];
       if (!refresh<kT>(a, s0, s1, r0, sm_r, sm_xs, false, epoch, red, tot)) return;
       ++refine;
@@ -406,7 +417,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
         st_vec(a.p + row, fmaf(bf, pr, ri));
       }
       a_pend = 0.0f;
-      if (!exchange_barrier(a.xs, epoch, red)) return;
+      if (!exchange_barrier(a.ex, epoch, red)) return;
     }
   }
   if (act) {  // iteration cap
@@ -415,7 +426,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
   }
   if (status != SFR_OK) {  // fold the last increment (a converged solve has folded it)
     fold<kT>(a, s0, s1, r0, sm_xs, a_pend);
-    if (!exchange_barrier(a.xs, epoch, red)) return;
+    if (!exchange_barrier(a.ex, epoch, red)) return;
   }
   // xKx, ||x||, ||b - Ax||_M, ||b - Ax|| (Cg.c:155-176)
   double acc[4] = {0.0, 0.0, 0.0, 0.0}, tot[4];
@@ -431,7 +442,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
       acc[3] += rk * rk;
     }
   }
-  if (!exchange<4>(a.xs, epoch, acc, tot, red)) return;
+  if (!exchange<4, false>(a.ex, epoch, acc, tot, red)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     SolveOut o;
     o.iters = static_cast<int>(iters);
@@ -467,6 +478,7 @@ __global__ void scaled_operator_kernel(const int *sptr, const int *col, const do
         sval[base + k * kWarp + lane] = 0.0f;
         off[base + k * kWarp + lane] = 0;
       }
+      delta[row] = 0.0f;
       continue;
     }
     const double di = diag[row];
@@ -497,11 +509,11 @@ int ensure_scaled_operator(sfr_system *s, cudaStream_t st) {
     const size_t ns = static_cast<size_t>(std::max<int64_t>(nslots, 1));
     if (cudaMalloc(&s->d_rval, sizeof(float) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
     if (cudaMalloc(&s->d_roff, sizeof(int16_t) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
-    if (cudaMalloc(&s->d_rdelta, sizeof(float) * std::max(s->n, 1)) != cudaSuccess)
-      return SFR_CUDA_ERROR;
+    const size_t rows = static_cast<size_t>(std::max(s->A.nslices, 1)) * kWarp;
+    if (cudaMalloc(&s->d_rdelta, sizeof(float) * rows) != cudaSuccess) return SFR_CUDA_ERROR;
     if (cudaMalloc(&s->d_rbad, sizeof(int)) != cudaSuccess) return SFR_CUDA_ERROR;
     s->bytes += static_cast<int64_t>((sizeof(float) + sizeof(int16_t)) * ns +
-                                     sizeof(float) * s->n + sizeof(int));
+                                     sizeof(float) * rows + sizeof(int));
   }
   if (s->resident_epoch == s->values_epoch) return SFR_OK;
   if (cudaMemsetAsync(s->d_rbad, 0, sizeof(int), st) != cudaSuccess) return SFR_CUDA_ERROR;
@@ -520,8 +532,9 @@ int ensure_scaled_operator(sfr_system *s, cudaStream_t st) {
   return SFR_OK;
 }
 
-// Launch shape: one block of 1024 threads per SM, 14 bytes of shared state
-// per row.
+// Launch shape: one block of 1024 threads per SM.  Shared state: 12 bytes per
+// row (inner residual, FP32 solution increment, A p), 16 when the diagonal
+// correction fits there too, and the block's slice pointers.
 constexpr int kResThreads = 1024;
 
 int max_smem_optin(int device) {
@@ -531,10 +544,12 @@ int max_smem_optin(int device) {
   return v;
 }
 
-// Dynamic shared memory of a block, or 0 when a block's rows do not fit.
-size_t block_smem(int nslices, int grid, int device) {
+// Dynamic shared memory of a block with `per_row` bytes of state a row, or 0
+// when a block's rows do not fit.
+size_t block_smem(int nslices, int grid, int device, int per_row) {
   const int per_block = (nslices + grid - 1) / grid;
-  const size_t bytes = static_cast<size_t>(per_block) * kWarp * (3 * sizeof(float) + 2);
+  const size_t bytes = static_cast<size_t>(per_block) * kWarp * per_row +
+                       sizeof(int) * (static_cast<size_t>(per_block) + 2);
   // static shared memory of the kernel (reductions) comes on top
   if (bytes + 4096 > static_cast<size_t>(max_smem_optin(device))) return 0;
   return std::max<size_t>(bytes, 16);
@@ -544,7 +559,7 @@ size_t block_smem(int nslices, int grid, int device) {
 
 bool resident_fits(sfr_system *s) {
   if (s->bandwidth > 32767) return false;
-  return block_smem(s->A.nslices, std::max(1, num_sms(s->device)), s->device) != 0;
+  return block_smem(s->A.nslices, std::max(1, num_sms(s->device)), s->device, 12) != 0;
 }
 
 int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, uint32_t maxit,
@@ -556,12 +571,16 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   if (!s->resident_ok) return SFR_UNSUPPORTED;  // Jacobi scaling needs ad > 0
   // a block per SM, fewer for small systems (a slice per warp at least):
   // the cost of an exchange grows with the blocks taking part
-  const int grid = std::max(1, std::min(num_sms(s->device),
-                                        (s->A.nslices + kResThreads / kWarp - 1) /
-                                            (kResThreads / kWarp)));
-  const size_t smem = block_smem(s->A.nslices, grid, s->device);
+  const int warps = kResThreads / kWarp;
+  const int grid = std::max(1, std::min(num_sms(s->device), (s->A.nslices + warps - 1) / warps));
+  // the diagonal correction in shared memory when it fits (the FP32 operator
+  // then keeps more of L2 to itself), else read with the couplings
+  size_t smem = block_smem(s->A.nslices, grid, s->device, 16);
+  const bool dshared = smem != 0;
+  if (!dshared) smem = block_smem(s->A.nslices, grid, s->device, 12);
   if (!smem) return SFR_UNSUPPORTED;
-  void (*kern)(ResArgs) = pcg_resident_kernel<kResThreads>;
+  void (*kern)(ResArgs) = dshared ? pcg_resident_kernel<kResThreads, true>
+                                  : pcg_resident_kernel<kResThreads, false>;
   if (cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
@@ -595,27 +614,23 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   a.b = d_b;
   a.x = d_x;
   a.p = reinterpret_cast<float *>(base);
-  a.xs.slots = reinterpret_cast<ExSlot *>(base + p_bytes);
-  unsigned *ctl = reinterpret_cast<unsigned *>(base + p_bytes + part_bytes);
-  a.xs.err = reinterpret_cast<int *>(ctl);
-  a.xs.nblocks = grid;
-  a.xs.spin_limit = 1u << 22;
-  a.out = reinterpret_cast<SolveOut *>(base + p_bytes + part_bytes + ctl_bytes);
+  base += p_bytes;
+  a.ex.slots = reinterpret_cast<ExSlot *>(base);
+  unsigned *ctl = reinterpret_cast<unsigned *>(base + part_bytes);
+  a.ex.err = reinterpret_cast<int *>(ctl);
+  a.ex.nblocks = grid;
+  a.ex.spin_limit = 1u << 22;
+  a.out = reinterpret_cast<SolveOut *>(base + part_bytes + ctl_bytes);
   a.tol = tol;
   a.rdelta = reliable_delta(SFR_PCG);
   a.maxit = maxit;
   a.newx = newx;
 
-  // padding rows of p must read as 0
+  // padding rows of p must read as 0; epochs restart at 0 in every launch,
+  // with every exchange word untagged
   if (cudaMemsetAsync(a.p, 0, p_bytes, st) != cudaSuccess) return SFR_CUDA_ERROR;
-  // epochs restart at 0 in every launch, with every slot empty
-  if (cudaMemsetAsync(ctl, 0, ctl_bytes, st) != cudaSuccess) return SFR_CUDA_ERROR;
-  {
-    const int words = static_cast<int>(part_bytes / sizeof(unsigned long long));
-    empty_slots_kernel<<<std::min((words + 255) / 256, 64), 256, 0, st>>>(
-        reinterpret_cast<unsigned long long *>(a.xs.slots), words);
-    if (cudaGetLastError() != cudaSuccess) return SFR_CUDA_ERROR;
-  }
+  if (cudaMemsetAsync(a.ex.slots, 0, part_bytes + ctl_bytes, st) != cudaSuccess)
+    return SFR_CUDA_ERROR;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return SFR_CUDA_ERROR;
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -633,7 +648,7 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(&out, a.out, sizeof(SolveOut), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess)
-    ce = cudaMemcpyAsync(&err, a.xs.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    ce = cudaMemcpyAsync(&err, a.ex.err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
   float ms = 0.f;
   if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
