@@ -113,14 +113,21 @@ int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
                         double tol, uint32_t maxit, int32_t newx,
                         int32_t precision, sfr_solve_info *info);
 
-/* Choose how solves run: engine 0 = automatic (by size), 1 = persistent
+/* Choose how solves run: engine 0 = automatic (by size and solve), 1 = persistent
  * (the whole solve in one cooperative launch: lowest latency, small
  * systems), 2 = graph (one full-occupancy kernel per phase inside a CUDA
  * graph whose iteration loop is a device-controlled conditional node: large
  * systems), 3 = the graph engine's kernels launched from a host loop for
  * exactly maxit iterations (for profilers, which cannot look inside graphs
  * with conditional nodes; finished solves make the remaining launches
- * no-ops).  threads (128 or 256) and slices_per_warp (1..64; a SELL slice is
+ * no-ops), 4 = resident (mixed-precision PCG with one right-hand side: one
+ * cooperative launch with a block per SM, the symmetrically scaled FP32
+ * operator with 16-bit column offsets held in L2 and the inner vectors in
+ * shared memory; SFR_UNSUPPORTED for other solves, for a diagonal that is
+ * not positive, a matrix bandwidth above 32767 or rows that do not fit the
+ * blocks' shared memory -- about 2.8 million on a B200).  The automatic
+ * choice takes the resident engine for mixed PCG from 100,000 rows when it
+ * applies.  threads (128 or 256) and slices_per_warp (1..64; a SELL slice is
  * 32 rows) set the graph engine's launch shape; 0 keeps the current value;
  * slices_per_warp = -1 (the default) sizes the SpMV phases to one wave of
  * the blocks resident on the GPU at once. */
@@ -242,8 +249,8 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
 void sfr_set_exit_on_failure(int32_t flag);
 /* SFR_MIXED: the inner FP32 residual must fall by this factor (0 < delta
  * < 1) before the FP64 solution is refreshed and the true residual
- * recomputed.  Sets the factor of both solvers (defaults: PCG 0.1,
- * BiCGSTAB 1e-4). */
+ * recomputed.  Sets the factor of both solvers on every engine (defaults:
+ * PCG 0.1, 0.02 on the resident engine; BiCGSTAB 1e-4). */
 void sfr_set_reliable_delta(double delta);
 /* The same for one solver (SFR_PCG or SFR_PBICGSTAB). */
 int sfr_set_solver_reliable_delta(int32_t solver, double delta);

@@ -141,6 +141,7 @@ int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
                  cudaStream_t st, sfr_solve_info *info);
 void release_stream_engine(const sfr_system *s);
 double reliable_delta(int32_t solver);
+double reliable_delta_resident();  // the resident engine's PCG factor
 int spmv_device(sfr_system *s, const DevSell &A, const double *d_diag,
                 const double *d_x, double *d_y, double *d_dot, cudaStream_t st);
 int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,

@@ -550,8 +550,8 @@ size_t block_smem(int nslices, int grid, int device, int per_row) {
   const int per_block = (nslices + grid - 1) / grid;
   const size_t bytes = static_cast<size_t>(per_block) * kWarp * per_row +
                        sizeof(int) * (static_cast<size_t>(per_block) + 2);
-  // static shared memory of the kernel (reductions) comes on top
-  if (bytes + 4096 > static_cast<size_t>(max_smem_optin(device))) return 0;
+  // the kernel's static shared memory (reductions, 1,280 bytes) comes on top
+  if (bytes + 1536 > static_cast<size_t>(max_smem_optin(device))) return 0;
   return std::max<size_t>(bytes, 16);
 }
 
@@ -622,7 +622,7 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   a.ex.spin_limit = 1u << 22;
   a.out = reinterpret_cast<SolveOut *>(base + part_bytes + ctl_bytes);
   a.tol = tol;
-  a.rdelta = reliable_delta(SFR_PCG);
+  a.rdelta = reliable_delta_resident();
   a.maxit = maxit;
   a.newx = newx;
 
