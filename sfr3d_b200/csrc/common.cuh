@@ -189,20 +189,36 @@ __device__ __forceinline__ double row_spmv_exact(const SellView<V> &A, int s, in
   return t;
 }
 
+// Column of a slot: an absolute index (int), or a 16-bit offset from the
+// row (int16_t: patterns whose bandwidth is below 32768, 2 bytes a slot
+// instead of 4).
+__device__ __forceinline__ int slot_col(const int *c, int k, int) { return ld_stream(c + k); }
+__device__ __forceinline__ int slot_col(const int16_t *c, int k, int row) {
+  return row + static_cast<int>(ld_stream(c + k));
+}
+
+// The columns of a SELL matrix's slots: offsets when the pattern has them,
+// else absolute indices.
+struct SlotCols {
+  const int *col;
+  const int16_t *off;  // null when the bandwidth does not fit 16 bits
+};
+
 // y_k[row] = diag*v(row) + sum_e val_e * v(col_e) for K vectors given by a
 // gather functor g(k, col), accumulated in Acc: exact FP64 (kExact: the
 // reference's rounding, one rounding per product and per sum), or with FMA.
 // Values may be FP32 with FP64 accumulation (the mixed path).  A row's column
 // indices and values are loaded six at a time before any gather, so all of
 // them are in flight together.
-template <int K, typename Acc, bool kExact, typename V, typename DV, typename G>
-__device__ __forceinline__ void row_product_t(const int *sptr, const int *colp, const V *valp,
+template <int K, typename Acc, bool kExact, typename V, typename DV, typename G,
+          typename I = int>
+__device__ __forceinline__ void row_product_t(const int *sptr, const I *colp, const V *valp,
                                               const DV *const *diagp, int s, int lane,
                                               const int (&act)[K], G g, Acc (&y)[K]) {
   const int row = s * kWarp + lane;
   const int base = __ldg(sptr + s);
   const int w = (__ldg(sptr + s + 1) - base) >> 5;
-  const int *c = colp + base + lane;
+  const I *c = colp + base + lane;
   const V *v = valp + base + lane;
 #pragma unroll
   for (int k = 0; k < K; ++k)
@@ -217,7 +233,7 @@ __device__ __forceinline__ void row_product_t(const int *sptr, const int *colp, 
 #pragma unroll
     for (int u = 0; u < 6; ++u)
       if (e0 + u < w) {
-        jj[u] = ld_stream(c + (e0 + u) * kWarp);
+        jj[u] = slot_col(c, (e0 + u) * kWarp, row);
         vv[u] = static_cast<Acc>(ld_stream(v + (e0 + u) * kWarp));
       }
 #pragma unroll
@@ -233,13 +249,35 @@ __device__ __forceinline__ void row_product_t(const int *sptr, const int *colp, 
   }
 }
 
-template <int K, bool kExact, typename V, typename G>
-__device__ __forceinline__ void row_product(const int *sptr, const int *colp, const V *valp,
+template <int K, bool kExact, typename V, typename G, typename I = int>
+__device__ __forceinline__ void row_product(const int *sptr, const I *colp, const V *valp,
                                             const V *const *diagp, int s, int lane,
                                             const int (&act)[K], G g,
                                             typename std::conditional<kExact, double, float>::type (&y)[K]) {
   using T = typename std::conditional<kExact, double, float>::type;
-  row_product_t<K, T, kExact, V, V>(sptr, colp, valp, diagp, s, lane, act, g, y);
+  row_product_t<K, T, kExact, V, V, G, I>(sptr, colp, valp, diagp, s, lane, act, g, y);
+}
+
+// The same over SlotCols: the offset form when the pattern has it.
+template <int K, bool kExact, typename V, typename G>
+__device__ __forceinline__ void row_product(const int *sptr, const SlotCols &cols, const V *valp,
+                                            const V *const *diagp, int s, int lane,
+                                            const int (&act)[K], G g,
+                                            typename std::conditional<kExact, double, float>::type (&y)[K]) {
+  if (cols.off)
+    row_product<K, kExact, V, G, int16_t>(sptr, cols.off, valp, diagp, s, lane, act, g, y);
+  else
+    row_product<K, kExact, V, G, int>(sptr, cols.col, valp, diagp, s, lane, act, g, y);
+}
+template <int K, typename Acc, bool kExact, typename V, typename DV, typename G>
+__device__ __forceinline__ void row_product_t(const int *sptr, const SlotCols &cols,
+                                              const V *valp, const DV *const *diagp, int s,
+                                              int lane, const int (&act)[K], G g, Acc (&y)[K]) {
+  if (cols.off)
+    row_product_t<K, Acc, kExact, V, DV, G, int16_t>(sptr, cols.off, valp, diagp, s, lane, act,
+                                                     g, y);
+  else
+    row_product_t<K, Acc, kExact, V, DV, G, int>(sptr, cols.col, valp, diagp, s, lane, act, g, y);
 }
 
 // Block-contiguous slice range of this block.

@@ -79,6 +79,15 @@ int upload_sell(const HostSell &h, DevSell *d, int64_t *bytes) {
   if (upload(&d->sptr, h.sptr, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
   if (upload(&d->col, h.col, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
   if (upload(&d->src, h.src, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
+  if (h.bandwidth <= 32767) {  // 16-bit column offsets: 2 bytes a slot instead of 4
+    std::vector<int16_t> off(h.col.size(), 0);
+    for (int32_t s = 0; s < h.nslices; ++s)
+      for (int32_t e = h.sptr[s]; e < h.sptr[s + 1]; ++e) {
+        const int32_t row = s * kWarpHost + (e - h.sptr[s]) % kWarpHost;
+        if (row < h.n) off[e] = static_cast<int16_t>(h.col[e] - row);
+      }
+    if (upload(&d->off, off, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
+  }
   const size_t ns = static_cast<size_t>(std::max<int64_t>(d->nslots, 1));
   if (cudaMalloc(&d->val, sizeof(double) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
   if (cudaMalloc(&d->val32, sizeof(float) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
@@ -90,6 +99,7 @@ void free_sell(DevSell *d) {
   cudaFree(d->sptr);
   cudaFree(d->col);
   cudaFree(d->src);
+  cudaFree(d->off);
   cudaFree(d->val);
   cudaFree(d->val32);
   *d = DevSell{};

@@ -39,6 +39,8 @@ struct DevSell {
   int32_t n = 0, nslices = 0;
   int64_t nslots = 0;
   int32_t *sptr = nullptr, *col = nullptr, *src = nullptr;
+  int16_t *off = nullptr;  // col - row per slot (0 in padding rows); null when the
+                           // bandwidth exceeds 32767
   double *val = nullptr;  // FP64 values
   float *val32 = nullptr; // FP32 copy (mixed precision)
 };
@@ -80,7 +82,6 @@ struct sfr_system {
   // resident engine (resident.cu): the symmetrically scaled FP32 operator,
   // rebuilt when the values or the diagonal change
   float *d_rval = nullptr;      // fl32(a_ij / sqrt(ad_i ad_j)) per SELL slot
-  int16_t *d_roff = nullptr;    // col - row per SELL slot
   float *d_rdelta = nullptr;    // per row: correction of the unit diagonal
   int *d_rbad = nullptr;        // set when a diagonal entry is not positive
   uint64_t values_epoch = 0;    // bumped by every value / diagonal upload

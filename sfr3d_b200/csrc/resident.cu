@@ -462,22 +462,19 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
 #undef SFR_RES_FOR
 
 // Scaled FP32 operator from the FP64 SELL values and the diagonal:
-//   val_e = fl32(a_e / sqrt(ad_row ad_col)),  off_e = col_e - row,
+//   val_e = fl32(a_e / sqrt(ad_row ad_col)),
 //   delta_row = -sum_e (val_e - a_e / sqrt(ad_row ad_col)) sqrt(ad_col / ad_row).
 // *bad is set when a diagonal entry is not positive and finite.
 __global__ void scaled_operator_kernel(const int *sptr, const int *col, const double *val,
                                        const double *diag, int n, int nslices, float *sval,
-                                       int16_t *off, float *delta, int *bad) {
+                                       float *delta, int *bad) {
   const int stride = gridDim.x * blockDim.x;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nslices * kWarp; t += stride) {
     const int s = t >> 5, lane = t & 31, row = t;
     const int base = sptr[s];
     const int w = (sptr[s + 1] - base) >> 5;
     if (row >= n) {
-      for (int k = 0; k < w; ++k) {
-        sval[base + k * kWarp + lane] = 0.0f;
-        off[base + k * kWarp + lane] = 0;
-      }
+      for (int k = 0; k < w; ++k) sval[base + k * kWarp + lane] = 0.0f;
       delta[row] = 0.0f;
       continue;
     }
@@ -496,7 +493,6 @@ __global__ void scaled_operator_kernel(const int *sptr, const int *col, const do
       const double exact = sc > 0.0 ? val[e] * si / sc : 0.0;
       const float f = __double2float_rn(exact);
       sval[e] = f;
-      off[e] = static_cast<int16_t>(c - row);
       acc += (static_cast<double>(f) - exact) * sc;
     }
     delta[row] = __double2float_rn(-acc * si);
@@ -508,11 +504,10 @@ int ensure_scaled_operator(sfr_system *s, cudaStream_t st) {
   if (!s->d_rval) {
     const size_t ns = static_cast<size_t>(std::max<int64_t>(nslots, 1));
     if (cudaMalloc(&s->d_rval, sizeof(float) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
-    if (cudaMalloc(&s->d_roff, sizeof(int16_t) * ns) != cudaSuccess) return SFR_CUDA_ERROR;
     const size_t rows = static_cast<size_t>(std::max(s->A.nslices, 1)) * kWarp;
     if (cudaMalloc(&s->d_rdelta, sizeof(float) * rows) != cudaSuccess) return SFR_CUDA_ERROR;
     if (cudaMalloc(&s->d_rbad, sizeof(int)) != cudaSuccess) return SFR_CUDA_ERROR;
-    s->bytes += static_cast<int64_t>((sizeof(float) + sizeof(int16_t)) * ns +
+    s->bytes += static_cast<int64_t>(sizeof(float) * ns +
                                      sizeof(float) * rows + sizeof(int));
   }
   if (s->resident_epoch == s->values_epoch) return SFR_OK;
@@ -520,8 +515,8 @@ int ensure_scaled_operator(sfr_system *s, cudaStream_t st) {
   const int grid = static_cast<int>(
       std::min<int64_t>((static_cast<int64_t>(s->A.nslices) * kWarp + 255) / 256, 8192));
   scaled_operator_kernel<<<std::max(grid, 1), 256, 0, st>>>(
-      s->A.sptr, s->A.col, s->A.val, s->d_diag, s->n, s->A.nslices, s->d_rval, s->d_roff,
-      s->d_rdelta, s->d_rbad);
+      s->A.sptr, s->A.col, s->A.val, s->d_diag, s->n, s->A.nslices, s->d_rval, s->d_rdelta,
+      s->d_rbad);
   if (cudaGetLastError() != cudaSuccess) return SFR_CUDA_ERROR;
   int bad = 0;
   if (cudaMemcpyAsync(&bad, s->d_rbad, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -558,7 +553,7 @@ size_t block_smem(int nslices, int grid, int device, int per_row) {
 }  // namespace
 
 bool resident_fits(sfr_system *s) {
-  if (s->bandwidth > 32767) return false;
+  if (!s->A.off) return false;  // bandwidth above 32767: no 16-bit column offsets
   return block_smem(s->A.nslices, std::max(1, num_sms(s->device)), s->device, 12) != 0;
 }
 
@@ -606,7 +601,7 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   a.nslices = s->A.nslices;
   a.sptr = s->A.sptr;
   a.val = s->d_rval;
-  a.off = s->d_roff;
+  a.off = s->A.off;
   a.delta = s->d_rdelta;
   a.col64 = s->A.col;
   a.val64 = s->A.val;

@@ -41,7 +41,8 @@ constexpr int kCounters = 16;
 template <int K>
 struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   int n, nslices, npairs;
-  const int *sptr, *col;
+  const int *sptr;
+  SlotCols cols;  // slot columns (16-bit offsets when the bandwidth allows)
   const double *val64;
   const float *val32;
   // the graph's own padded workspace (rows padded to a multiple of 4)
@@ -55,6 +56,16 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   cudaGraphConditionalHandle hwhile, hif, hif2;
   int in_graph;  // 0: plain launch loop (profiling): no conditional handles
 };
+
+// The slot columns a kernel instantiation reads: 16-bit offsets (I =
+// int16_t) or absolute indices (I = int).  Separate instantiations keep each
+// SpMV phase at the register count of one index form.
+template <typename I>
+__device__ __forceinline__ const I *cols_of(const SlotCols &c);
+template <>
+__device__ __forceinline__ const int *cols_of<int>(const SlotCols &c) { return c.col; }
+template <>
+__device__ __forceinline__ const int16_t *cols_of<int16_t>(const SlotCols &c) { return c.off; }
 
 // Per-call scalars, copied into the state before each launch.
 struct SCall {
@@ -198,7 +209,7 @@ __global__ void __launch_bounds__(256) k_setup(const SArgs<K> a, SState<K> *st) 
 
 // PCG start: r = b - A x, z = M r, p = z, d = (r, z)  (FP64: Cg.c:84-102)
 // mixed: the same in FP64 for the true residual, then r, z, p in FP32.
-template <int K, bool kMixed>
+template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_pcg_start(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   const int n = a.n;
@@ -213,7 +224,7 @@ __global__ void __launch_bounds__(256) k_pcg_start(const SArgs<K> a, SState<K> *
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     double y[K];
-    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
                                  [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -247,7 +258,7 @@ __global__ void __launch_bounds__(256) k_pcg_start(const SArgs<K> a, SState<K> *
 }
 
 // phase A: q = A p, (q, p)  (Cg.c:105-109)
-template <int K, bool kMixed>
+template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(K);
   if (!st->any) return;
@@ -264,7 +275,7 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
   if (!kMixed) {
     SFR_FOR_OWN_ROWS(s0, s1) {
       double y[K];
-      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+      row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.p0[k] + c); }, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -278,7 +289,7 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
     SFR_FOR_OWN_ROWS(s0, s1) {
       double y[K];
       row_product_t<K, double, false, float, double>(
-          a.sptr, a.col, a.val32, dc, s_, lane, act,
+          a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
           [&](int k, int c) { return ld_ro(a.fp0[k] + c); }, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -462,7 +473,7 @@ __global__ void __launch_bounds__(256) k_fold(const SArgs<K> a, SState<K> *st, i
 
 // reliable update, part 2 (PCG): r_true = b - A x in FP64, r = fl32(r_true),
 // z = M r, xs = 0; decide on the true residual.
-template <int K>
+template <int K, typename I>
 __global__ void __launch_bounds__(256) k_pcg_refresh(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any_upd) return;
@@ -478,7 +489,7 @@ __global__ void __launch_bounds__(256) k_pcg_refresh(const SArgs<K> a, SState<K>
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     double y[K];
-    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, sel,
+    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, sel,
                                  [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -526,7 +537,7 @@ __global__ void __launch_bounds__(256) k_pcg_refresh(const SArgs<K> a, SState<K>
 }
 
 // post-processing: xKx, ||x||, ||b - Ax||_M, ||b - Ax|| (Cg.c:155-176)
-template <int K>
+template <int K, typename I>
 __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(4 * K);
   const int n = a.n;
@@ -541,7 +552,7 @@ __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
   for (int v = 0; v < 4 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     double y[K];
-    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
                                  [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -578,7 +589,7 @@ __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
 // FP64: Bicgstab.c:50-245.  Vectors: r0 shadow, p (p0), z = M p or M s,
 // v (q), t.  Mixed: the same in FP32 with xs and reliable updates.
 
-template <int K, bool kMixed>
+template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   const int n = a.n;
@@ -593,7 +604,7 @@ __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> 
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     double y[K];
-    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, all,
+    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
                                  [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -625,7 +636,7 @@ __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> 
 }
 
 // A1: v = A z ; rr0 = (r, r0) ; alpha = rr0 / (v, r0)
-template <int K, bool kMixed>
+template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
@@ -641,7 +652,7 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
   SFR_FOR_OWN_ROWS(s0, s1) {
     if (!kMixed) {
       double y[K];
-      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+      row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -657,7 +668,7 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
         double yd[K];
         const double *const *dc = a.dc;
         row_product_t<K, double, false, float, double>(
-            a.sptr, a.col, a.val32, dc, s_, lane, act,
+            a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
             [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
 #pragma unroll
         for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
@@ -766,7 +777,7 @@ __global__ void __launch_bounds__(256) k_bicg_b1(const SArgs<K> a, SState<K> *st
 // xs = 0; ||r_true||; (r, r0).  `stage` 1 = after the half step, 2 = after
 // the full step (phase B2 already computed beta; it is recomputed with the
 // new (r, r0)).
-template <int K>
+template <int K, typename I>
 __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K> *st,
                                                       int stage) {
   SFR_SHARED_RED(2 * K);
@@ -783,7 +794,7 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     double y[K];
-    row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, sel,
+    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, sel,
                                  [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -831,7 +842,7 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
 }
 
 // A2: t = A z ; w = (t, s) / (t, t)
-template <int K, bool kMixed>
+template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
@@ -847,7 +858,7 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
   SFR_FOR_OWN_ROWS(s0, s1) {
     if (!kMixed) {
       double y[K];
-      row_product<K, true, double>(a.sptr, a.col, a.val64, a.diag64, s_, lane, act,
+      row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -862,7 +873,7 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
         double yd[K];
         const double *const *dc = a.dc;
         row_product_t<K, double, false, float, double>(
-            a.sptr, a.col, a.val32, dc, s_, lane, act,
+            a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
             [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
 #pragma unroll
         for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
@@ -1099,12 +1110,12 @@ inline int64_t padded(int n) { return (static_cast<int64_t>(n) + 3) & ~static_ca
 
 // Allocate the graph's workspace and fill its by-value arguments.
 // Blocks of the iteration's SpMV kernel that fit on the GPU at once.
-template <int K>
+template <int K, typename I>
 int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
   const void *kern =
       solver == SFR_PCG
-          ? (mixed ? (const void *)k_pcg_a<K, true> : (const void *)k_pcg_a<K, false>)
-          : (mixed ? (const void *)k_bicg_a1<K, true> : (const void *)k_bicg_a1<K, false>);
+          ? (mixed ? (const void *)k_pcg_a<K, true, I> : (const void *)k_pcg_a<K, false, I>)
+          : (mixed ? (const void *)k_bicg_a1<K, true, I> : (const void *)k_bicg_a1<K, false, I>);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess ||
       occ < 1)
@@ -1115,7 +1126,7 @@ int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
 // spw > 0: `spw` slices per warp.  spw == 0: one wave, as many blocks as are
 // resident at once (fewer for small systems), so no partial last wave leaves
 // SMs idle while the phase's last blocks finish.
-template <int K>
+template <int K, typename I>
 cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int spw,
                     CachedGraph *cg) {
   const int n = s->n;
@@ -1127,7 +1138,7 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
     cg->grid_s = std::max(1, (s->A.nslices + warps * spw - 1) / (warps * spw));
   else
     cg->grid_s = std::max(1, std::min((s->A.nslices + warps - 1) / warps,
-                                      resident_blocks<K>(s, solver, mixed, threads)));
+                                      resident_blocks<K, I>(s, solver, mixed, threads)));
   const int npairs = (n + 1) / 2;
   const int wave = std::max(1, num_sms(s->device)) * (2048 / threads);
   cg->grid_v = std::max(1, std::min(wave, (npairs + threads - 1) / threads));
@@ -1149,7 +1160,7 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
   a.nslices = s->A.nslices;
   a.npairs = npairs;
   a.sptr = s->A.sptr;
-  a.col = s->A.col;
+  a.cols = SlotCols{s->A.col, s->A.off};
   a.val64 = s->A.val;
   a.val32 = s->A.val32;
   a.comp = s->d_comp;
@@ -1189,10 +1200,10 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
 }
 
 // The graph for one (solver, K, precision, launch shape).
-template <int K>
+template <int K, typename I>
 cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
                         CachedGraph *cg) {
-  SFR_TRY(prepare<K>(s, solver, precision, threads, spw, cg));
+  SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, cg)));
   SFR_TRY(cudaGraphCreate(&cg->graph, 0));
   cudaGraph_t g = cg->graph;
   const bool mixed = precision == SFR_MIXED;
@@ -1232,60 +1243,60 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   if (solver == SFR_PCG) {
     if (mixed) {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, true, I>, gs, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, true, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, true>, gv, threads, p2));
       SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
       cudaGraphNode_t ip = nullptr;
       SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K>, gs, threads, p2));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false, I>, gs, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, false, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, false>, gv, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, false>, gv, threads, p2));
     }
   } else {
     if (mixed) {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, true, I>, gs, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, true, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, true>, gv, threads, p2));
       SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
       cudaGraphNode_t ip = nullptr;
       SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K>, gs, threads, pr1));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, true>, gs, threads, p2));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K, I>, gs, threads, pr1));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, true, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, true>, gv, threads, p2));
       cudaGraph_t ifbody2 = nullptr;
       SFR_TRY(add_conditional(body, &bp, cg->hif2, cudaGraphCondTypeIf, &ifbody2));
       cudaGraphNode_t ip2 = nullptr;
       SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K>, gs, threads, pr2));
+      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K, I>, gs, threads, pr2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, false, I>, gs, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, false, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, false>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, false, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, false>, gv, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, false>, gv, threads, p2));
     }
   }
-  SFR_TRY(add_kernel(g, &prev, (void *)k_post<K>, gs, threads, p2));
+  SFR_TRY(add_kernel(g, &prev, (void *)k_post<K, I>, gs, threads, p2));
   SFR_TRY(cudaGraphInstantiate(&cg->exec, g, 0));
   return cudaSuccess;
 }
@@ -1303,7 +1314,7 @@ void free_graph(CachedGraph *cg) {
 // The same kernels launched from a host loop for `maxit` iterations (kernels
 // of finished solves return at once).  For profilers, which cannot look into
 // graphs with conditional nodes; never the production path.
-template <int K>
+template <int K, typename I>
 cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
                         cudaStream_t st) {
   SArgs<K> a = *reinterpret_cast<const SArgs<K> *>(cg->args.data());
@@ -1314,20 +1325,20 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
   if (solver == SFR_PCG) {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
-      k_pcg_start<K, true><<<gs, t, 0, st>>>(a, ps);
+      k_pcg_start<K, true, I><<<gs, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_pcg_a<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_a<K, true, I><<<gs, t, 0, st>>>(a, ps);
         k_pcg_b<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_pcg_refresh<K><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_refresh<K, I><<<gs, t, 0, st>>>(a, ps);
         k_pcg_c<K, true><<<gv, t, 0, st>>>(a, ps);
       }
       k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
     } else {
       k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
-      k_pcg_start<K, false><<<gs, t, 0, st>>>(a, ps);
+      k_pcg_start<K, false, I><<<gs, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_pcg_a<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_a<K, false, I><<<gs, t, 0, st>>>(a, ps);
         k_pcg_b<K, false><<<gv, t, 0, st>>>(a, ps);
         k_pcg_c<K, false><<<gv, t, 0, st>>>(a, ps);
       }
@@ -1335,32 +1346,32 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
   } else {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
-      k_bicg_start<K, true><<<gs, t, 0, st>>>(a, ps);
+      k_bicg_start<K, true, I><<<gs, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_bicg_a1<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_a1<K, true, I><<<gs, t, 0, st>>>(a, ps);
         k_bicg_b1<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_bicg_refresh<K><<<gs, t, 0, st>>>(a, ps, 1);
-        k_bicg_a2<K, true><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_refresh<K, I><<<gs, t, 0, st>>>(a, ps, 1);
+        k_bicg_a2<K, true, I><<<gs, t, 0, st>>>(a, ps);
         k_bicg_b2<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_bicg_refresh<K><<<gs, t, 0, st>>>(a, ps, 2);
+        k_bicg_refresh<K, I><<<gs, t, 0, st>>>(a, ps, 2);
         k_bicg_c<K, true><<<gv, t, 0, st>>>(a, ps);
       }
       k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
     } else {
       k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
-      k_bicg_start<K, false><<<gs, t, 0, st>>>(a, ps);
+      k_bicg_start<K, false, I><<<gs, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_bicg_a1<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_a1<K, false, I><<<gs, t, 0, st>>>(a, ps);
         k_bicg_b1<K, false><<<gv, t, 0, st>>>(a, ps);
-        k_bicg_a2<K, false><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_a2<K, false, I><<<gs, t, 0, st>>>(a, ps);
         k_bicg_b2<K, false><<<gv, t, 0, st>>>(a, ps);
         k_bicg_c<K, false><<<gv, t, 0, st>>>(a, ps);
       }
     }
   }
-  k_post<K><<<gs, t, 0, st>>>(a, ps);
+  k_post<K, I><<<gs, t, 0, st>>>(a, ps);
   return cudaGetLastError();
 }
 
@@ -1382,7 +1393,9 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
       ec.graphs.erase(lru);
     }
     auto cg = std::make_unique<CachedGraph>();
-    const cudaError_t be = build_graph<K>(s, solver, precision, threads, spw, cg.get());
+    const cudaError_t be =
+        s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, cg.get())
+                 : build_graph<K, int>(s, solver, precision, threads, spw, cg.get());
     if (be != cudaSuccess) {
       set_last_error(cudaGetErrorString(be));
       free_graph(cg.get());
@@ -1415,7 +1428,9 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(cg->d_state, &call, sizeof(call), cudaMemcpyHostToDevice, st);
   if (err == cudaSuccess)
-    err = loop ? launch_loop<K>(cg, solver, mixed, maxit, st) : cudaGraphLaunch(cg->exec, st);
+    err = !loop     ? cudaGraphLaunch(cg->exec, st)
+          : s->A.off ? launch_loop<K, int16_t>(cg, solver, mixed, maxit, st)
+                     : launch_loop<K, int>(cg, solver, mixed, maxit, st);
   for (int k = 0; k < K && err == cudaSuccess; ++k)
     err = cudaMemcpyAsync(d_x + static_cast<size_t>(k) * n, a.x[k], vb, cudaMemcpyDeviceToDevice,
                           st);
