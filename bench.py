@@ -59,7 +59,7 @@ def parse_args(argv=None):
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
                     help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
-                         "loop (profiling)")
+                         "loop (profiling), 4 resident (mixed PCG)")
     ap.add_argument("--threads", type=int, default=0, help="graph-engine block size (0: default)")
     ap.add_argument("--spw", type=int, default=0, help="SELL slices per warp (0: default)")
     ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
@@ -266,13 +266,24 @@ def run_ours(args):
             mt, mi = timed_solves(sv.MIXED, args.steps, 1, xm)
             x64 = x.cpu().numpy()
             x32 = xm.cpu().numpy()
-            mixed = {"ms": max_over_ranks(statistics.mean(mt)),
+            m_ms = max_over_ranks(statistics.mean(mt))
+            inner = max(mi[-1].inner_iters, 1)
+            # per inner iteration: FP32 coupling + 16-bit offset per slot, the
+            # gather of p and the read and write of p (12 B a row)
+            inner_bytes = g.stats()["slots"] * 6 + 12 * N
+            mixed = {"ms": m_ms,
+                     "engine": ("resident: one cooperative launch, scaled FP32 operator held "
+                                "in L2, inner vectors in shared memory" if args.engine in (0, 4)
+                                else f"engine {args.engine}"),
                      "inner_iters": mi[-1].inner_iters,
                      "refinements": mi[-1].refinements,
                      "status": mi[-1].status,
                      "true_relres_2norm": mi[-1].relres,
                      "err_vs_fp64_x": float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64)),
-                     "speedup_vs_fp64": ms_step / max(statistics.mean(mt), 1e-9)}
+                     "speedup_vs_fp64": ms_step / max(m_ms, 1e-9),
+                     "us_per_inner_iteration": m_ms * 1e3 / inner,
+                     "alg_bytes_per_inner_iteration": inner_bytes,
+                     "inner_GB/s_from_L2": inner_bytes / (m_ms * 1e-3 / inner) / 1e9}
         except sv.SolverError as e:
             mixed = {"unavailable": str(e)}
 
@@ -363,7 +374,7 @@ def run_ours(args):
                                f"nodes +-20%, diffusivity 10^U(-2,2), harmonic faces, "
                                f"permuted + RCM; Jacobi-PCG FP64 to 1e-10 (M-norm)",
                    "rows": N, "nnz_offdiag": nnz, "iterations": iters,
-                   "format": "SELL-32 (from CSRD)",
+                   "format": "SELL-32 from CSRD: FP64 values, 16-bit column offsets",
                    "engine": "CUDA graph, device-side WHILE loop (3 kernels per iteration)",
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
@@ -374,7 +385,9 @@ def run_ours(args):
                                "k_pcg_b update+dot, k_pcg_c direction per iteration)",
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": alg,
-                     "alg_bytes_rule": "(iters+2)*(12 nnz_off + 4(N+1) + 24N) + iters*88N"},
+                     "alg_bytes_rule": "(iters+2)*(12 nnz_off + 4(N+1) + 24N) + iters*88N",
+                     "alg_bytes_note": "32-bit column indices, as the CSRD formula counts them; "
+                                       "the SpMV phases read 16-bit offsets (2 B a slot less)"},
         "spmv": {"kernel": "spmv_kernel", "ms": spmv_ms, "alg_bytes": sb, "GB/s": spmv_gbs,
                  "frac": spmv_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
                  "traffic": None if sp_tr is None else sp_tr[0] * (N / 128 ** 3),
