@@ -55,6 +55,9 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   unsigned *counter;
   cudaGraphConditionalHandle hwhile, hif, hif2;
   int in_graph;  // 0: plain launch loop (profiling): no conditional handles
+  // the right-hand sides share one diagonal: diag64, m, dc and m32 of every
+  // k point at k = 0's arrays, which k_setup fills once
+  int shared_diag;
 };
 
 // The slot columns a kernel instantiation reads: 16-bit offsets (I =
@@ -171,12 +174,14 @@ __global__ void __launch_bounds__(256) k_setup(const SArgs<K> a, SState<K> *st) 
     for (int k = 0; k < K; ++k) {
       const double2 dk = ld2ro(a.diag64[k] + r);
       const double2 mk = make_double2(1.0 / dk.x, 1.0 / dk.y);
-      if (kMixed) {
-        const double2 ck = ld2ro(a.comp + r);
-        st2(a.dc[k] + r, make_double2(dk.x + ck.x, dk.y + ck.y));
-        st2(a.m32[k] + r, make_float2(__double2float_rn(mk.x), __double2float_rn(mk.y)));
-      } else {
-        st2(a.m[k] + r, mk);
+      if (k == 0 || !a.shared_diag) {  // shared: k = 0's arrays serve every k
+        if (kMixed) {
+          const double2 ck = ld2ro(a.comp + r);
+          st2(a.dc[k] + r, make_double2(dk.x + ck.x, dk.y + ck.y));
+          st2(a.m32[k] + r, make_float2(__double2float_rn(mk.x), __double2float_rn(mk.y)));
+        } else {
+          st2(a.m[k] + r, mk);
+        }
       }
       if (newx) st2(a.x[k] + r, make_double2(0.0, 0.0));
       const double2 bk = ld2ro(a.b[k] + r);
@@ -663,15 +668,16 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
         acc[2 * k + 1] += y[k] * r0k;
       }
     } else {
+      // FP32 accumulation: the momentum systems BiCGSTAB serves are
+      // diagonally dominant, and FP64 accumulation of K right-hand sides
+      // costs two FP32 -> FP64 conversions a slot and right-hand side (the
+      // SpMV phase then ran slower than the FP64 one)
       float y[K];
       {
-        double yd[K];
         const double *const *dc = a.dc;
-        row_product_t<K, double, false, float, double>(
+        row_product_t<K, float, false, float, double>(
             a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
-            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
-#pragma unroll
-        for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
+            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
       }
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -868,15 +874,16 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
         acc[2 * k + 1] += y[k] * y[k];
       }
     } else {
+      // FP32 accumulation: the momentum systems BiCGSTAB serves are
+      // diagonally dominant, and FP64 accumulation of K right-hand sides
+      // costs two FP32 -> FP64 conversions a slot and right-hand side (the
+      // SpMV phase then ran slower than the FP64 one)
       float y[K];
       {
-        double yd[K];
         const double *const *dc = a.dc;
-        row_product_t<K, double, false, float, double>(
+        row_product_t<K, float, false, float, double>(
             a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
-            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, yd);
-#pragma unroll
-        for (int k = 0; k < K; ++k) y[k] = __double2float_rn(yd[k]);
+            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
       }
 #pragma unroll
       for (int k = 0; k < K; ++k) {
@@ -1038,9 +1045,10 @@ __global__ void __launch_bounds__(256) k_bicg_c(const SArgs<K> a, SState<K> *st)
 
 struct GraphKey {
   int solver, k, precision, threads, spw;
+  int shared_diag;  // the K right-hand sides share one diagonal
   bool operator<(const GraphKey &o) const {
-    return std::tie(solver, k, precision, threads, spw) <
-           std::tie(o.solver, o.k, o.precision, o.threads, o.spw);
+    return std::tie(solver, k, precision, threads, spw, shared_diag) <
+           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag);
   }
 };
 
@@ -1128,7 +1136,7 @@ int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
 // SMs idle while the phase's last blocks finish.
 template <int K, typename I>
 cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int spw,
-                    CachedGraph *cg) {
+                    int shared_diag, CachedGraph *cg) {
   const int n = s->n;
   const int64_t np = padded(n);
   const bool mixed = precision == SFR_MIXED;
@@ -1194,6 +1202,18 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
       a.t[k] = D(10);
     }
   }
+  if (shared_diag) {
+    for (int k = 1; k < K; ++k) {
+      a.diag64[k] = a.diag64[0];
+      if (mixed) {
+        a.dc[k] = a.dc[0];
+        a.m32[k] = a.m32[0];
+      } else {
+        a.m[k] = a.m[0];
+      }
+    }
+  }
+  a.shared_diag = shared_diag;
   a.part = cg->part;
   a.counter = cg->counter;
   return cudaSuccess;
@@ -1202,8 +1222,8 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
 // The graph for one (solver, K, precision, launch shape).
 template <int K, typename I>
 cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
-                        CachedGraph *cg) {
-  SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, cg)));
+                        int shared_diag, CachedGraph *cg) {
+  SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, shared_diag, cg)));
   SFR_TRY(cudaGraphCreate(&cg->graph, 0));
   cudaGraph_t g = cg->graph;
   const bool mixed = precision == SFR_MIXED;
@@ -1382,7 +1402,8 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
   const int n = s->n;
   if (maxit == 0) return SFR_BAD_INPUT;
   EngineCache &ec = g_engines[s];
-  GraphKey key{solver, K, precision, threads, spw};
+  const int shared_diag = K > 1 && !d_diag_k ? 1 : 0;
+  GraphKey key{solver, K, precision, threads, spw, shared_diag};
   auto it = ec.graphs.find(key);
   if (it == ec.graphs.end()) {
     if (ec.graphs.size() >= kMaxGraphsPerSystem) {  // drop the least recently used
@@ -1394,8 +1415,8 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
     }
     auto cg = std::make_unique<CachedGraph>();
     const cudaError_t be =
-        s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, cg.get())
-                 : build_graph<K, int>(s, solver, precision, threads, spw, cg.get());
+        s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, cg.get())
+                 : build_graph<K, int>(s, solver, precision, threads, spw, shared_diag, cg.get());
     if (be != cudaSuccess) {
       set_last_error(cudaGetErrorString(be));
       free_graph(cg.get());
@@ -1417,7 +1438,8 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
   const size_t vb = sizeof(double) * static_cast<size_t>(n);
   for (int k = 0; k < K && err == cudaSuccess; ++k) {
     const double *dg = d_diag_k ? d_diag_k + static_cast<size_t>(k) * n : s->d_diag;
-    err = cudaMemcpyAsync(a.diag64[k], dg, vb, cudaMemcpyDeviceToDevice, st);
+    if (k == 0 || !shared_diag)
+      err = cudaMemcpyAsync(a.diag64[k], dg, vb, cudaMemcpyDeviceToDevice, st);
     if (err == cudaSuccess)
       err = cudaMemcpyAsync(a.b[k], d_b + static_cast<size_t>(k) * n, vb,
                             cudaMemcpyDeviceToDevice, st);

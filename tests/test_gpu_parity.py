@@ -242,3 +242,27 @@ def test_solverC_dropin_log_line(cuda):
                       x2, 1e-10, 1000, sv.CSRD, sv.PCG) == sv.OK
     assert np.array_equal(x, x2)
     sv.release_cache()
+
+
+@pytest.mark.parametrize("eng", [2, 4])
+def test_wide_bandwidth_uses_32bit_columns(cuda, eng):
+    """Without RCM the bandwidth of a 40^3 system exceeds what 16-bit column
+    offsets hold: the graph engine reads 32-bit indices (same FP64 parity
+    bar), and the resident engine, which needs offsets, declines the solve."""
+    s = S.build(S.params(n=(40, 40, 40), jitter=0.2, log10k=(-2.0, 2.0), permute=True,
+                         rcm=False, seed=21))
+    g, (st, un, ia, ja, al) = gpu_system(s, "csrd_full", eng)
+    assert g.stats()["bandwidth"] > 32767
+    if eng == 4:
+        with pytest.raises(sv.SolverError) as e:
+            g.solve(sv.PCG, s.b[0], tol=1e-10, precision=sv.MIXED)
+        assert e.value.status == sv.UNSUPPORTED
+        g.set_engine(0)  # the automatic choice falls back to another engine
+        x, info = g.solve(sv.PCG, s.b[0], tol=1e-10, precision=sv.MIXED)
+        assert info.status == sv.OK
+        return
+    x, info = g.solve(sv.PCG, s.b[0], tol=1e-10)
+    ref = O.pcg(st, un, ia, ja, al, s.ad, s.b[0], tol=1e-10)
+    assert info.status == sv.OK
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(x, ref.x) < TOL_X
