@@ -1,6 +1,7 @@
 """ctypes wrappers of the parity oracle (test infrastructure only).
 
-``pcg`` / ``pbicgstab`` / ``matvec`` run the C restatement (sfr3d_oracle.c);
+``pcg`` / ``pbicgstab`` / ``pbicgstabl2`` / ``gmres`` / ``minres`` /
+``matvec`` run the C restatement (sfr3d_oracle.c);
 ``ref_solve`` runs the reference's own compiled solverC (Solv.c:64) through
 ref_harness.c, serial (nthreads=0) or OpenMP (nthreads>=1).
 """
@@ -17,7 +18,8 @@ LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libsfr3d_ref.so")
 
 CSRD, CSRC, ELLPACK = 2, 3, 4
-PCG, PBICGSTAB = 1, 2
+PCG, PBICGSTAB, PBICGSTABL2, GMRES, MINRES = 1, 2, 3, 4, 5  # Define.h:392-396
+NKRYLOV = 15  # solverC's GMRES restart length (Solv.c:82)
 
 _P = ctypes.c_void_p
 
@@ -62,11 +64,15 @@ def oracle_lib():
         lib.orc_matvec.restype = None
         lib.orc_matvec.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    _P, _P, _P, _P, _P, _P]
-        for f in (lib.orc_pcg, lib.orc_pbicgstab):
+        for f in (lib.orc_pcg, lib.orc_pbicgstab, lib.orc_minres, lib.orc_pbicgstabl2):
             f.restype = ctypes.c_int
             f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P,
                           _P, _P, _P, ctypes.c_double, ctypes.c_uint,
                           ctypes.c_int, ctypes.POINTER(_Stats)]
+        lib.orc_gmres.restype = ctypes.c_int
+        lib.orc_gmres.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P,
+                                  _P, _P, _P, ctypes.c_double, ctypes.c_uint,
+                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Stats)]
         lib._typed = True
     return lib
 
@@ -111,13 +117,13 @@ def matvec(storage, unsym, ia, ja, al, ad, x) -> np.ndarray:
     return y
 
 
-def _solve(fn, storage, unsym, ia, ja, al, ad, b, x0, tol, maxit, newx):
+def _solve(fn, storage, unsym, ia, ja, al, ad, b, x0, tol, maxit, newx, *extra):
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
     al, ad, b = _c(al, np.float64), _c(ad, np.float64), _c(b, np.float64)
     x = np.zeros(len(ad)) if x0 is None else np.array(x0, dtype=np.float64)
     st = _Stats()
     fn(storage, int(unsym), len(ad), _p(ia), _p(ja), _p(al), _p(ad), _p(b),
-       _p(x), tol, maxit, int(newx), ctypes.byref(st))
+       _p(x), tol, maxit, int(newx), *extra, ctypes.byref(st))
     return SolveResult(x=x, iters=st.iters, status=st.status, xKx=st.xKx,
                        norm_x=st.norm_x, norm_r=st.norm_r,
                        norm_r_m=st.norm_r_m, conv=st.conv)
@@ -135,6 +141,31 @@ def pbicgstab(storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,
     """Restatement of pbicgstab (Bicgstab.c:50-245)."""
     return _solve(oracle_lib().orc_pbicgstab, storage, unsym, ia, ja, al, ad,
                   b, x0, tol, maxit, newx)
+
+
+def minres(storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,
+           maxit=100000, newx=True) -> SolveResult:
+    """Restatement of pminres (Iters.c:309-558)."""
+    return _solve(oracle_lib().orc_minres, storage, unsym, ia, ja, al, ad, b, x0,
+                  tol, maxit, newx)
+
+
+def pbicgstabl2(storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,
+                maxit=100000, newx=True) -> SolveResult:
+    """Restatement of pbicgstabl2 (Bicgstab.c:1172-1460)."""
+    return _solve(oracle_lib().orc_pbicgstabl2, storage, unsym, ia, ja, al, ad,
+                  b, x0, tol, maxit, newx)
+
+
+def gmres(storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,
+          maxit=100000, newx=True, nk=NKRYLOV) -> SolveResult:
+    """Restatement of gmres (Iters.c:587-800); maxit counts cycles."""
+    return _solve(oracle_lib().orc_gmres, storage, unsym, ia, ja, al, ad, b, x0,
+                  tol, maxit, newx, int(nk))
+
+
+SOLVERS = {PCG: pcg, PBICGSTAB: pbicgstab, PBICGSTABL2: pbicgstabl2, GMRES: gmres,
+           MINRES: minres}
 
 
 def ref_solve(solver, storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,

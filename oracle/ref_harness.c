@@ -59,7 +59,8 @@ static void parse_log(const char *buf, int *iters, double *xKx, double *normx)
 
 /*
  * Solve one system with the reference's solverC.
- *   solver : PCG=1 | PBICGSTAB=2 (Define.h:392-393)
+ *   solver : PCG=1 | PBICGSTAB=2 | PBICGSTABL2=3 | GMRES=4 | MINRES=5
+ *            (Define.h:392-396)
  *   storage: CSRD=2 | CSRC=3 | ELLPACK=4 (Define.h:407-410)
  *   nthreads: 0 -> serial pcg/pbicgstab, >=1 -> pcgOmp/pbicgstabOmp
  * Returns 0 when the solver converged, otherwise the code it passed to
@@ -87,8 +88,9 @@ int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
   ompVar.fSolver = nthreads > 0;
   ompVar.nThreadsSolver = (unsigned short)(nthreads > 0 ? nthreads : 1);
 
-  /* workspace: pc + 6 Krylov vectors at most, plus the arena's alignment */
-  nvec = 8;
+  /* workspace: pc + the Krylov vectors (GMRES(15): 16 basis vectors; the
+   * others: 10 at most), plus the arena's alignment */
+  nvec = solver == 4 ? 20 : 12;
   nmax = (iptx)nvec * (iptx)(neq + 64) * (iptx)sizeof(double) + 65536;
   initMem(&mem, nmax, false);
   /* dalloc (Memoria.c:280) refuses to release the only vector of an arena;

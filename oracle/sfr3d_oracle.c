@@ -197,3 +197,318 @@ int orc_pbicgstab(int storage, int unsym, int neq, const int *ia,
   free(m);
   return st->status;
 }
+
+/* Iters.c:1171-1211 (symOrtho): Givens rotation for (a, b), with the
+ * reference's branch tests as written (the third compares |b| with a, not
+ * |a|; when no branch applies c, s and r keep their values). */
+static void orc_sym_ortho(double a, double b, double *c, double *s, double *r)
+{
+  const double ma = fabs(a), mb = fabs(b);
+  const double sa = a > 0.0 ? 1.0 : -1.0, sb = b > 0.0 ? 1.0 : -1.0;
+  if (b == 0.0) {
+    *s = 0.0;
+    *r = ma;
+    *c = a == 0.0 ? 1.0 : sa;
+  } else if (a == 0.0) {
+    *c = 0.0;
+    *s = sb;
+    *r = mb;
+  } else if (mb > a) {
+    const double t = a / b;
+    *s = sb / sqrt(1.0 + t * t);
+    *c = *s * t;
+    *r = b / *s;
+  } else if (ma > mb) {
+    const double t = b / a;
+    *c = sa / sqrt(1.0 + t * t);
+    *s = *c * t;
+    *r = a / *c;
+  }
+}
+
+/* Iters.c:309-558 (pminres): MINRES on the Jacobi-preconditioned system
+ * D^-1/2 A D^-1/2, with the Lanczos vectors kept in the unscaled space.
+ * The reference only warns when maxIt is reached; status 1 reports it. */
+int orc_minres(int storage, int unsym, int neq, const int *ia, const int *ja,
+               const double *al, const double *ad, const double *b, double *x,
+               double tol, unsigned maxit, int newx, orc_stats *st)
+{
+  double *m = malloc(sizeof(double) * (size_t)neq * 10);
+  double *v0 = m + neq, *v = v0 + neq, *w = v + neq, *w0 = w + neq,
+         *w00 = w0 + neq, *z = w00 + neq, *z0 = z + neq, *p = z0 + neq, *tmp;
+  double t1, t2, t3, t4, conv, beta, beta_old, neta, c, c_old, s, s_old,
+         ro1 = 1.0, ro2, ro3, alpha, delta, norm_r;
+  unsigned j;
+  int i;
+  if (!m) return -1;
+  for (i = 0; i < neq; i++) m[i] = 1.0 / ad[i];
+  if (newx)
+    for (i = 0; i < neq; i++) x[i] = 0.0;
+  for (i = 0; i < neq; i++) z[i] = b[i] * sqrt(m[i]);
+  conv = tol * sqrt(orc_dot(z, z, neq));
+  orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, z);
+  for (i = 0; i < neq; i++) {
+    v[i] = b[i] - z[i];
+    v0[i] = w0[i] = w00[i] = 0.0;
+    z0[i] = v[i] * m[i];
+  }
+  beta = sqrt(fabs(orc_dot(v, z0, neq)));
+  norm_r = beta;
+  neta = beta;
+  beta_old = beta;
+  c_old = c = 1.0;
+  s_old = s = 0.0;
+  for (j = 0; j < maxit; j++) {
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, z0, p);
+    t1 = 1.0 / (beta * beta);
+    alpha = orc_dot(z0, p, neq) * t1;
+    t1 = 1.0 / beta;
+    t2 = -alpha / beta;
+    t3 = -beta / beta_old;
+    for (i = 0; i < neq; i++) {
+      p[i] = t1 * p[i] + t2 * v[i] + t3 * v0[i];
+      z[i] = p[i] * m[i];
+    }
+    beta_old = beta;
+    beta = sqrt(orc_dot(z, p, neq));
+    delta = c * alpha - c_old * s * beta_old;
+    ro2 = s * alpha + c_old * c * beta_old;
+    ro3 = s_old * beta_old;
+    c_old = c;
+    s_old = s;
+    orc_sym_ortho(delta, beta, &c, &s, &ro1);
+    t1 = 1.0 / (beta_old * ro1);
+    t2 = -ro2 / ro1;
+    t3 = -ro3 / ro1;
+    t4 = c * neta;
+    for (i = 0; i < neq; i++) {
+      w[i] = t1 * z0[i] + t2 * w0[i] + t3 * w00[i];
+      x[i] += t4 * w[i];
+    }
+    /* v0 <- v, v <- p, z0 <- z, w00 <- w0, w0 <- w (by rotation) */
+    tmp = v0; v0 = v; v = p; p = tmp;
+    tmp = z0; z0 = z; z = tmp;
+    tmp = w00; w00 = w0; w0 = w; w = tmp;
+    norm_r = fabs(s) * norm_r;
+    if (norm_r < conv) break;
+    neta = -s * neta;
+  }
+  /* post-processing, Iters.c:481-497 */
+  orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, z);
+  st->xKx = orc_dot(x, z, neq);
+  st->norm_x = sqrt(orc_dot(x, x, neq));
+  for (i = 0; i < neq; i++) {
+    v[i] = b[i] - z[i];
+    z[i] = v[i] * sqrt(fabs(m[i]));
+  }
+  st->norm_r = sqrt(orc_dot(v, v, neq));
+  st->norm_r_m = sqrt(orc_dot(z, z, neq));
+  st->conv = conv;
+  st->iters = (int)j + 1;
+  st->status = j == maxit ? 1 : 0;
+  free(m);
+  return st->status;
+}
+
+/* Bicgstab.c:1172-1460 (pbicgstabl2): BiCGSTAB(2), right-preconditioned. */
+int orc_pbicgstabl2(int storage, int unsym, int neq, const int *ia,
+                    const int *ja, const double *al, const double *ad,
+                    const double *b, double *x, double tol, unsigned maxit,
+                    int newx, orc_stats *st)
+{
+  double *m = malloc(sizeof(double) * (size_t)neq * 12);
+  double *t = m + neq, *v = t + neq, *r = v + neq, *u = r + neq,
+         *r0 = u + neq, *w = r0 + neq, *s = w + neq, *p = s + neq,
+         *h = p + neq, *z = h + neq;
+  double alpha, beta, d, conv, rr0, rr1, omega1, omega2, gamma, mi, ni, tau;
+  unsigned j;
+  int i;
+  if (!m) return -1;
+  for (i = 0; i < neq; i++) m[i] = 1.0 / ad[i];
+  if (newx)
+    for (i = 0; i < neq; i++) x[i] = 0.0;
+  d = orc_dot(b, b, neq);
+  conv = tol * sqrt(d);
+  orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, t);
+  for (i = 0; i < neq; i++) {
+    r0[i] = b[i] - t[i];
+    r[i] = r0[i];
+    u[i] = 0.0;
+  }
+  rr0 = 1.0;
+  alpha = 0.0;
+  omega2 = 1.0;
+  for (j = 0; j < maxit; j++) {
+    rr0 = -omega2 * rr0;
+    /* even BiCG step */
+    rr1 = orc_dot(r, r0, neq);
+    beta = alpha * rr1 / rr0;
+    rr0 = rr1;
+    for (i = 0; i < neq; i++) {
+      u[i] = r[i] - beta * u[i];
+      z[i] = u[i] * m[i];
+    }
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, z, v);
+    gamma = orc_dot(v, r0, neq);
+    alpha = rr0 / gamma;
+    for (i = 0; i < neq; i++) {
+      r[i] -= alpha * v[i];
+      p[i] = r[i] * m[i];
+    }
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, p, s);
+    for (i = 0; i < neq; i++) x[i] += alpha * z[i];
+    /* odd BiCG step */
+    rr1 = orc_dot(s, r0, neq);
+    beta = alpha * rr1 / rr0;
+    rr0 = rr1;
+    for (i = 0; i < neq; i++) {
+      v[i] = s[i] - beta * v[i];
+      p[i] = v[i] * m[i];
+    }
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, p, w);
+    gamma = orc_dot(w, r0, neq);
+    alpha = rr0 / gamma;
+    for (i = 0; i < neq; i++) {
+      u[i] = r[i] - beta * u[i];
+      r[i] -= alpha * v[i];
+      s[i] -= alpha * w[i];
+      p[i] = s[i] * m[i];
+      z[i] = u[i] * m[i];
+      h[i] = r[i] * m[i];
+    }
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, p, t);
+    /* GCR(2) part */
+    omega1 = orc_dot(r, s, neq);
+    mi = orc_dot(s, s, neq);
+    ni = orc_dot(s, t, neq);
+    tau = orc_dot(t, t, neq);
+    omega2 = orc_dot(r, t, neq);
+    tau = tau - ni * ni / mi;
+    omega2 = (omega2 - ni * omega1 / mi) / tau;
+    omega1 = (omega1 - ni * omega2) / mi;
+    for (i = 0; i < neq; i++) {
+      x[i] += omega1 * h[i] + omega2 * p[i] + alpha * z[i];
+      r[i] -= (omega1 * s[i] + omega2 * t[i]);
+    }
+    d = orc_dot(r, r, neq);
+    if (sqrt(d) < conv) break;
+    for (i = 0; i < neq; i++) u[i] -= (omega1 * v[i] + omega2 * w[i]);
+  }
+  /* post-processing, Bicgstab.c:1395-1410 */
+  orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, z);
+  st->xKx = orc_dot(x, z, neq);
+  st->norm_x = sqrt(orc_dot(x, x, neq));
+  for (i = 0; i < neq; i++) r[i] = b[i] - z[i];
+  st->norm_r = sqrt(orc_dot(r, r, neq));
+  st->norm_r_m = 0.0;
+  st->conv = conv;
+  st->iters = (int)j + 1;
+  st->status = j == maxit ? 1 : 0;
+  free(m);
+  return st->status;
+}
+
+/* Iters.c:587-800 (gmres): restarted GMRES(nk) with the Jacobi
+ * preconditioner on the left, modified Gram-Schmidt and Givens rotations.
+ * As in the reference, a cycle always runs all nk Arnoldi steps, and the
+ * update uses the first nk-1 of them (the back substitution and the sum
+ * x += V y stop before the last column); convergence is tested on |e[nk]|
+ * after each cycle, and maxit counts cycles.  iters = nk * cycles + 1. */
+int orc_gmres(int storage, int unsym, int neq, const int *ia, const int *ja,
+              const double *al, const double *ad, const double *b, double *x,
+              double tol, unsigned maxit, int newx, int nk, orc_stats *st)
+{
+  double *m = malloc(sizeof(double) * (size_t)neq * (size_t)(nk + 2));
+  double *g = m + neq, *g1, *g2;
+  double *hh = malloc(sizeof(double) * (size_t)(nk + 1) * (size_t)nk);
+  double *y = malloc(sizeof(double) * (size_t)nk * 3 + sizeof(double) * (nk + 1));
+  double *c = y + nk, *s = c + nk, *e = s + nk;
+  double tmp, norm, eConv, beta, h1, h2, aux1, aux2, r;
+  unsigned l;
+  int i, j, ni = 0, nIt = 0;
+  long k;
+#define HH(row, col) hh[(long)(row) * nk + (col)]
+  if (!m || !hh || !y) {
+    free(m); free(hh); free(y);
+    return -1;
+  }
+  for (k = 0; k < (long)(nk + 1) * nk; k++) hh[k] = 0.0;
+  for (k = 0; k < 3L * nk + nk + 1; k++) y[k] = 0.0;
+  for (i = 0; i < neq; i++) m[i] = 1.0 / ad[i];
+  if (newx)
+    for (i = 0; i < neq; i++) x[i] = 0.0;
+  for (i = 0; i < neq; i++) g[i] = b[i] * m[i];
+  norm = sqrt(orc_dot(g, g, neq));
+  eConv = tol * norm;
+  for (l = 0; l < maxit; l++) {
+    orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, g);
+    for (i = 0; i < neq; i++) g[i] = (b[i] - g[i]) * m[i];
+    e[0] = sqrt(orc_dot(g, g, neq));
+    tmp = 1.0 / e[0];
+    for (i = 0; i < neq; i++) g[i] *= tmp;
+    for (ni = 0; ni < nk; ni++, nIt++) {
+      g1 = g + (long)ni * neq;
+      g2 = g + (long)(ni + 1) * neq;
+      orc_matvec(storage, unsym, neq, ia, ja, al, ad, g1, g2);
+      for (i = 0; i < neq; i++) g2[i] *= m[i];
+      for (j = 0; j <= ni; j++) {
+        g1 = g + (long)j * neq;
+        beta = orc_dot(g2, g1, neq);
+        for (i = 0; i < neq; i++) g2[i] -= beta * g1[i];
+        HH(j, ni) = beta;
+      }
+      norm = sqrt(orc_dot(g2, g2, neq));
+      HH(ni + 1, ni) = norm;
+      tmp = 1.0 / norm;
+      for (i = 0; i < neq; i++) g2[i] *= tmp;
+      for (j = 0; j < ni; j++) {
+        h1 = HH(j, ni);
+        h2 = HH(j + 1, ni);
+        aux1 = c[j] * h1 + s[j] * h2;
+        aux2 = -s[j] * h1 + c[j] * h2;
+        HH(j, ni) = aux1;
+        HH(j + 1, ni) = aux2;
+      }
+      h1 = HH(ni, ni);
+      h2 = HH(ni + 1, ni);
+      r = sqrt(h1 * h1 + h2 * h2);
+      tmp = 1.0 / r;
+      c[ni] = h1 * tmp;
+      s[ni] = h2 * tmp;
+      HH(ni, ni) = r;
+      HH(ni + 1, ni) = 0.0;
+      e[ni + 1] = -s[ni] * e[ni];
+      e[ni] = c[ni] * e[ni];
+    }
+    if (ni == nk) ni--;
+    y[ni] = e[ni] / HH(ni, ni);
+    for (i = ni - 1; i >= 0; i--) {
+      y[i] = 0.0;
+      for (j = i + 1; j < ni; j++) y[i] -= HH(i, j) * y[j];
+      y[i] = (y[i] + e[i]) / HH(i, i);
+    }
+    for (j = 0; j < ni; j++) {
+      tmp = y[j];
+      g1 = g + (long)j * neq;
+      for (i = 0; i < neq; i++) x[i] += g1[i] * tmp;
+    }
+    if (fabs(e[ni + 1]) < eConv) break;
+  }
+#undef HH
+  /* post-processing, Iters.c:746-760 */
+  g1 = g;
+  g2 = g + neq;
+  orc_matvec(storage, unsym, neq, ia, ja, al, ad, x, g1);
+  st->xKx = orc_dot(x, g1, neq);
+  st->norm_x = sqrt(orc_dot(x, x, neq));
+  for (i = 0; i < neq; i++) g2[i] = b[i] - g1[i];
+  st->norm_r = sqrt(orc_dot(g2, g2, neq));
+  st->norm_r_m = 0.0;
+  st->conv = eConv;
+  st->iters = nIt + 1;
+  st->status = l == maxit ? 1 : 0;
+  free(m);
+  free(hh);
+  free(y);
+  return st->status;
+}

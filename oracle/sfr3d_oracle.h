@@ -1,6 +1,7 @@
 /*
  * Test infrastructure, not product code: a plain-C restatement of SFR3D's
- * linear-solve path used as the parity oracle.  Only tests/, the smoke check
+ * linear-solve path (PCG, BiCGSTAB, and the other Krylov methods behind
+ * solverC: BiCGSTAB(2), GMRES, MINRES) used as the parity oracle.  Only tests/, the smoke check
  * and bench.py's CPU-baseline leg load it.  Every function cites the
  * reference lines it restates; the arithmetic is done in the same order as
  * the reference so that results are bit-identical to the reference's own
@@ -40,5 +41,22 @@ int orc_pbicgstab(int storage, int unsym, int neq, const int *ia,
                   const int *ja, const double *al, const double *ad,
                   const double *b, double *x, double tol, unsigned maxit,
                   int newx, orc_stats *st);
+
+/* Iters.c:309-558 (pminres) */
+int orc_minres(int storage, int unsym, int neq, const int *ia, const int *ja,
+               const double *al, const double *ad, const double *b, double *x,
+               double tol, unsigned maxit, int newx, orc_stats *st);
+
+/* Bicgstab.c:1172-1460 (pbicgstabl2) */
+int orc_pbicgstabl2(int storage, int unsym, int neq, const int *ia,
+                    const int *ja, const double *al, const double *ad,
+                    const double *b, double *x, double tol, unsigned maxit,
+                    int newx, orc_stats *st);
+
+/* Iters.c:587-800 (gmres), nk Krylov vectors a cycle (solverC: 15),
+ * maxit cycles */
+int orc_gmres(int storage, int unsym, int neq, const int *ia, const int *ja,
+              const double *al, const double *ad, const double *b, double *x,
+              double tol, unsigned maxit, int newx, int nk, orc_stats *st);
 
 #endif

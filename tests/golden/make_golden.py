@@ -47,6 +47,28 @@ def cases():
            mom.ad, mom.b[1], None, 1e-14, 1, True)
     yield ("mom8_rhs1", O.PBICGSTAB, O.CSRD, True, mom.ia, mom.ja, mom.al,
            mom.ad, mom.b[1], None, 1e-10, 100000, True)
+    # the other Krylov methods behind solverC: BiCGSTAB(2), GMRES(15)
+    # (maxit counts restart cycles), MINRES (symmetric systems only)
+    others = (("jit10", jit, (O.PBICGSTABL2, O.GMRES, O.MINRES)),
+              ("mom8", mom, (O.PBICGSTABL2, O.GMRES)),
+              ("steady8", steady, (O.PBICGSTABL2, O.GMRES)))
+    tags = {O.PBICGSTABL2: "bicgl2", O.GMRES: "gmres", O.MINRES: "minres"}
+    for name, sysx, solvers in others:
+        for solver in solvers:
+            for lname, (st, un, ia, ja, al, au) in layouts(sysx).items():
+                yield (f"{name}_{tags[solver]}_{lname}", solver, st, un, ia, ja, al,
+                       sysx.ad, sysx.b[0], None, 1e-10, 100000, True)
+    st, un, ia, ja, al, _ = layouts(jit)["csrd_sym"]
+    yield ("jit10_minres_warm", O.MINRES, st, un, ia, ja, al, jit.ad, jit.b[0],
+           0.5 * np.ones(jit.neq), 1e-8, 100000, False)
+    # iteration caps: GMRES and BiCGSTAB(2) exit with EXIT_FAILURE; MINRES
+    # only warns and reports maxIt + 1 iterations
+    yield ("jit10_gmres_maxit", O.GMRES, st, un, ia, ja, al, jit.ad, jit.b[0], None,
+           1e-10, 2, True)
+    yield ("jit10_minres_maxit", O.MINRES, st, un, ia, ja, al, jit.ad, jit.b[0], None,
+           1e-10, 7, True)
+    yield ("mom8_bicgl2_maxit", O.PBICGSTABL2, O.CSRD, True, mom.ia, mom.ja, mom.al,
+           mom.ad, mom.b[1], None, 1e-14, 1, True)
 
 
 def main():

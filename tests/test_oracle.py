@@ -31,10 +31,14 @@ def case(name):
 @pytest.mark.parametrize("name", CASES)
 def test_restatement_reproduces_reference_fixture(name):
     g, solver, st, un, maxit, newx, tol = case(name)
-    fn = O.pcg if solver == O.PCG else O.pbicgstab
+    fn = O.SOLVERS[solver]
     r = fn(st, un, g["ia"], g["ja"], g["al"], g["ad"], g["b"], x0=g["x0"],
            tol=tol, maxit=maxit, newx=newx)
     iters, status = (int(v) for v in g["res"])
+    if solver == O.MINRES and r.status == 1:
+        # the reference's MINRES only warns at maxIt (Iters.c:525-529)
+        assert status == 0 and iters == maxit + 1 == r.iters
+        status = 1
     assert (r.status == 0) == (status == 0)
     if status == 0:
         assert r.iters == iters
@@ -45,9 +49,13 @@ def test_restatement_reproduces_reference_fixture(name):
 
 
 def test_reference_exit_codes_recorded():
-    # PCG exits with EXIT_FAILURE (1), serial BiCGSTAB with EXIT_SOLVER (-2)
+    # PCG exits with EXIT_FAILURE (1), serial BiCGSTAB with EXIT_SOLVER (-2),
+    # GMRES and BiCGSTAB(2) with EXIT_FAILURE; MINRES does not exit
     assert int(GOLD["uni8_maxit/res"][1]) == 1
     assert int(GOLD["mom8_maxit/res"][1]) == -2
+    assert int(GOLD["jit10_gmres_maxit/res"][1]) == 1
+    assert int(GOLD["mom8_bicgl2_maxit/res"][1]) == 1
+    assert int(GOLD["jit10_minres_maxit/res"][1]) == 0
 
 
 def test_restatement_status_on_iteration_cap():
@@ -73,11 +81,29 @@ def test_restatement_bit_identical_to_compiled_reference(kind):
                              dirichlet=S.ALL_FACES, rhs_normal=True, peclet=50.0,
                              nu=1e-3, dt=1e3, seed=24))
         solver = O.PBICGSTAB
-    fn = O.pcg if solver == O.PCG else O.pbicgstab
+    fn = O.SOLVERS[solver]
     for lname, (st, un, ia, ja, al, au) in layouts(s).items():
         ref = O.ref_solve(solver, st, un, ia, ja, al, s.ad, s.b[0])
         mine = fn(st, un, ia, ja, al, s.ad, s.b[0])
         assert ref.status == 0, lname
+        assert mine.iters == ref.iters, lname
+        assert np.array_equal(mine.x, ref.x), lname
+
+
+@needs_ref
+@pytest.mark.parametrize("solver", [O.PBICGSTABL2, O.GMRES, O.MINRES])
+@pytest.mark.parametrize("kind", ["jittered", "momentum"])
+def test_other_krylov_restatements_bit_identical_to_compiled_reference(kind, solver):
+    """BiCGSTAB(2), GMRES(15) and MINRES: the restatement and the
+    reference's own solverC agree bit for bit on every layout."""
+    if kind == "momentum" and solver == O.MINRES:
+        pytest.skip("MINRES needs a symmetric matrix")
+    s = (S.poisson_jittered(11, seed=27) if kind == "jittered"
+         else S.momentum(11, seed=28, nrhs=1))
+    for lname, (st, un, ia, ja, al, au) in layouts(s).items():
+        ref = O.ref_solve(solver, st, un, ia, ja, al, s.ad, s.b[0])
+        mine = O.SOLVERS[solver](st, un, ia, ja, al, s.ad, s.b[0])
+        assert ref.status == 0 and mine.status == 0, lname
         assert mine.iters == ref.iters, lname
         assert np.array_equal(mine.x, ref.x), lname
 
