@@ -32,9 +32,12 @@
 extern "C" {
 #endif
 
-/* solver codes, Define.h:392-393 */
+/* solver codes, Define.h:392-396 */
 #define SFR_PCG 1
 #define SFR_PBICGSTAB 2
+#define SFR_PBICGSTABL2 3 /* BiCGSTAB(2), Bicgstab.c:1172 */
+#define SFR_GMRES 4       /* GMRES(15), Iters.c:587; maxit counts restart cycles */
+#define SFR_MINRES 5      /* MINRES, Iters.c:309 (symmetric matrices) */
 /* storage codes, Define.h:407-410 */
 #define SFR_CSRD 2
 #define SFR_CSRC 3
@@ -92,7 +95,12 @@ int sfr_gpu_set_diagonal(sfr_system *s, const double *ad);
 
 /* Solve A x = b with host b and x (copies inside).  Same semantics as
  * callCg (Solv.c:936) / callBicgStab (Solv.c:1052): newX zeroes x, tol is
- * the reference's relative tolerance.  info may be NULL. */
+ * the reference's relative tolerance.  info may be NULL.  SFR_PBICGSTABL2,
+ * SFR_GMRES and SFR_MINRES (callBicgStabl2 Solv.c:1173, callGmres
+ * Solv.c:1263, callMinRes Solv.c:1331) run in FP64 with one right-hand side
+ * (SFR_UNSUPPORTED with SFR_MIXED); GMRES's maxit counts restart cycles of
+ * 15 iterations and its iteration count is 15 x cycles + 1, as the
+ * reference reports it. */
 int sfr_gpu_solve(sfr_system *s, int32_t solver, const double *b, double *x,
                   double tol, uint32_t maxit, int32_t newx, int32_t precision,
                   sfr_solve_info *info);
@@ -237,9 +245,11 @@ int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor);
  * pattern is cached per (ia, ja, storage) so a repeated call uploads only
  * al/ad/au/b.  Writes the reference's log line to fSolvLog when fLog is
  * set.  On non-convergence prints the reference's message and calls
- * exit(EXIT_FAILURE) for PCG and exit(-2) for BiCGSTAB (Cg.c:195-200,
- * Bicgstab.c:225-231) unless sfr_set_exit_on_failure(0) was called, in which
- * case it returns the status. */
+ * exit(EXIT_FAILURE) for PCG, GMRES and BiCGSTAB(2) and exit(-2) for
+ * BiCGSTAB (Cg.c:195-200, Bicgstab.c:225-231, Iters.c:773-777,
+ * Bicgstab.c:1428-1432) unless sfr_set_exit_on_failure(0) was called, in
+ * which case it returns the status; MINRES only prints its warning, as the
+ * reference does (Iters.c:525-529). */
 int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
                 int32_t nAdR, int32_t *ia, int32_t *ja, double *al,
                 double *ad, double *au, double *b, double *x, void *iNeq,

@@ -69,12 +69,34 @@ def oracle_lib():
             f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P,
                           _P, _P, _P, ctypes.c_double, ctypes.c_uint,
                           ctypes.c_int, ctypes.POINTER(_Stats)]
+        lib.orc_set_dot_order.restype = None
+        lib.orc_set_dot_order.argtypes = [ctypes.c_int]
         lib.orc_gmres.restype = ctypes.c_int
         lib.orc_gmres.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P,
                                   _P, _P, _P, ctypes.c_double, ctypes.c_uint,
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Stats)]
         lib._typed = True
     return lib
+
+
+def order_spread(solver, storage, unsym, ia, ja, al, ad, b, **kw):
+    """How far the reference's own algorithm moves when only the summation
+    order of its dot products changes (right to left, pairwise): the largest
+    change in the iteration count and the largest relative change in x,
+    against the reference order."""
+    lib = oracle_lib()
+    fn = SOLVERS[solver]
+    base = fn(storage, unsym, ia, ja, al, ad, b, **kw)
+    d_it, d_x = 0, 0.0
+    try:
+        for order in (1, 2):
+            lib.orc_set_dot_order(order)
+            r = fn(storage, unsym, ia, ja, al, ad, b, **kw)
+            d_it = max(d_it, abs(r.iters - base.iters))
+            d_x = max(d_x, float(np.linalg.norm(r.x - base.x) / np.linalg.norm(base.x)))
+    finally:
+        lib.orc_set_dot_order(0)
+    return d_it, d_x
 
 
 def ref_available() -> bool:

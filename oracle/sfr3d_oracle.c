@@ -9,10 +9,34 @@
 #include <math.h>
 #include <stdlib.h>
 
+/* Summation order of orc_dot: 0 is the reference's; 1 (right to left) and
+ * 2 (pairwise over blocks of 64) exist only to measure how far the
+ * reference's own algorithms move when nothing but the order of a sum
+ * changes. */
+static int g_dot_order = 0;
+
+void orc_set_dot_order(int order) { g_dot_order = order; }
+
+static double dot_pairwise(const double *a, const double *b, int n)
+{
+  if (n <= 64) {
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+  }
+  const int h = n / 2;
+  return dot_pairwise(a, b, h) + dot_pairwise(a + h, b + h, n - h);
+}
+
 /* HccaBlas.c:393-437 (dot): one accumulator, left to right. */
 double orc_dot(const double *a, const double *b, int n)
 {
   double s = 0.0;
+  if (g_dot_order == 1) {
+    for (int i = n - 1; i >= 0; i--) s += a[i] * b[i];
+    return s;
+  }
+  if (g_dot_order == 2) return dot_pairwise(a, b, n);
   for (int i = 0; i < n; i++) s += a[i] * b[i];
   return s;
 }

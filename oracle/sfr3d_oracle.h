@@ -33,6 +33,11 @@ void orc_matvec(int storage, int unsym, int neq, const int *ia, const int *ja,
 
 double orc_dot(const double *a, const double *b, int n);
 
+/* 0: the reference's left-to-right dot (default); 1: right to left;
+ * 2: pairwise.  Only for measuring the reference's sensitivity to the
+ * summation order. */
+void orc_set_dot_order(int order);
+
 int orc_pcg(int storage, int unsym, int neq, const int *ia, const int *ja,
             const double *al, const double *ad, const double *b, double *x,
             double tol, unsigned maxit, int newx, orc_stats *st);

@@ -521,7 +521,9 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR,
   (void)bOmp;
   std::lock_guard<std::mutex> lk(g_shim_mu);
   int rc = SFR_OK;
-  if ((solver != SFR_PCG && solver != SFR_PBICGSTAB) || nEqNov != nEq) {
+  const bool known = solver == SFR_PCG || solver == SFR_PBICGSTAB || solver == SFR_PBICGSTABL2 ||
+                     solver == SFR_GMRES || solver == SFR_MINRES;
+  if (!known || nEqNov != nEq) {
     // the reference's ERRO_OP (Erro.h:17-20) for an option this path lacks
     fprintf(stderr, "Opcao %d e invalida!!\n", solver);
     fprintf(stderr, "Arquivo:%s\nFonte:  %s\n", __FILE__, "sfr_solverC");
@@ -558,33 +560,64 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR,
   if (rc == SFR_OK)
     rc = sfr_gpu_solve(s, solver, b, x, tol, maxIt, newX ? 1 : 0, g_precision, &info);
   if (rc == SFR_MAXIT) {
-    // Cg.c:195-200 / Bicgstab.c:225-231
-    printf("name : %s\n", name ? name : "");
-    if (solver == SFR_PCG)
-      printf("PCG: *** WARNING: no convergende reached !\n");
-    else
-      printf(" PBICGSTAB *** WARNING: no convergende reached !\n");
+    // Cg.c:195-200, Bicgstab.c:225-231, Bicgstab.c:1428-1432,
+    // Iters.c:773-777; MINRES only warns (Iters.c:525-529)
+    if (solver == SFR_PCG || solver == SFR_PBICGSTAB) printf("name : %s\n", name ? name : "");
+    switch (solver) {
+      case SFR_PCG: printf("PCG: *** WARNING: no convergende reached !\n"); break;
+      case SFR_PBICGSTAB: printf(" PBICGSTAB *** WARNING: no convergende reached !\n"); break;
+      case SFR_PBICGSTABL2:
+        printf(" PBICGSTAB(2) *** WARNING: no convergende reached !\n");
+        break;
+      case SFR_GMRES: printf(" GMRES *** WARNING: no convergende reached !\n"); break;
+      default: printf("PMINRES: *** WARNING: no convergende reached !\n"); break;
+    }
     printf("MAXIT = %d \n", maxIt);
-    if (g_exit_on_failure) exit(solver == SFR_PCG ? EXIT_FAILURE : -2);
-    return rc;
+    if (solver != SFR_MINRES) {
+      if (g_exit_on_failure) exit(solver == SFR_PBICGSTAB ? -2 : EXIT_FAILURE);
+      return rc;
+    }
   }
-  if (rc != SFR_OK) {
+  if (rc != SFR_OK && rc != SFR_MAXIT) {
     fprintf(stderr, "sfr_solverC: %s (%s)\n", sfr_status_string(rc), g_last_error.c_str());
-    if (g_exit_on_failure) exit(solver == SFR_PCG ? EXIT_FAILURE : -2);
+    if (g_exit_on_failure) exit(solver == SFR_PBICGSTAB ? -2 : EXIT_FAILURE);
     return rc;
   }
   if (fLog && fSolvLog) {
-    // Cg.c:201-208 / Bicgstab.c:235-242
-    if (solver == SFR_PCG)
-      fprintf(fSolvLog,
-              "PCG: tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e time %20.5lf\n", tol,
-              info.iters, info.xKx, info.norm_x, info.seconds);
-    else
-      fprintf(fSolvLog,
-              "PBICGSTAB: tol %20.2e iteration %d xKx %20.12e ||x*x|| %20.12e time %20.5lf\n",
-              tol, info.iters, info.xKx, info.norm_x, info.seconds);
+    // Cg.c:201-208, Bicgstab.c:235-242, Bicgstab.c:1436-1443,
+    // Iters.c:779-788, Iters.c:531-538
+    switch (solver) {
+      case SFR_PCG:
+        fprintf(fSolvLog,
+                "PCG: tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e time %20.5lf\n",
+                tol, info.iters, info.xKx, info.norm_x, info.seconds);
+        break;
+      case SFR_PBICGSTAB:
+        fprintf(fSolvLog,
+                "PBICGSTAB: tol %20.2e iteration %d xKx %20.12e ||x*x|| %20.12e time %20.5lf\n",
+                tol, info.iters, info.xKx, info.norm_x, info.seconds);
+        break;
+      case SFR_PBICGSTABL2:
+        fprintf(fSolvLog,
+                "PBICGSTAB(2): tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e "
+                "time %20.5lf\n",
+                tol, info.iters, info.xKx, info.norm_x, info.seconds);
+        break;
+      case SFR_GMRES:
+        fprintf(fSolvLog,
+                "GMRES: tol %20.2e  Cycles %d iteration %d  nKrylov %d  xKx %20.12e  "
+                "norma(x*x) %20.12e  time %20.5lf\n",
+                tol, (info.iters - 1) / 15, info.iters, 15, info.xKx, info.norm_x,
+                info.seconds);
+        break;
+      default:
+        fprintf(fSolvLog,
+                "PMINRES: tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e time %20.5lf\n",
+                tol, info.iters, info.xKx, info.norm_x, info.seconds);
+        break;
+    }
   }
-  return SFR_OK;
+  return rc;
 }
 
 }  // extern "C"

@@ -135,6 +135,11 @@ bool resident_fits(sfr_system *s);
 int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, uint32_t maxit,
                    int32_t newx, cudaStream_t st, sfr_solve_info *info);
 
+// BiCGSTAB(2), GMRES(15), MINRES (krylov_ext.cu): one right-hand side, FP64;
+// d_diag null means the system's own diagonal
+int solve_ext(sfr_system *s, int32_t solver, const double *d_diag, const double *d_b, double *d_x,
+              double tol, uint32_t maxit, int32_t newx, cudaStream_t st, sfr_solve_info *info);
+
 // Graph engine (stream_solve.cu)
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,

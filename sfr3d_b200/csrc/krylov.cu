@@ -855,8 +855,13 @@ int enqueue_team_fp64(sfr_system *s, int32_t solver, const double *d_b, double *
 int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
                  int32_t precision, cudaStream_t st, sfr_solve_info *info) {
-  if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
+  if (solver == SFR_PBICGSTABL2 || solver == SFR_GMRES || solver == SFR_MINRES) {
+    // one right-hand side, FP64, on every engine setting
+    if (k != 1 || precision != SFR_FP64) return SFR_UNSUPPORTED;
+    return solve_ext(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);
+  }
+  if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   int engine = s->engine;
   const bool resident_case = precision == SFR_MIXED && solver == SFR_PCG && k == 1 && !d_diag_k;
   if (engine == 4 || (engine == 0 && resident_case && s->n >= kGraphEngineRows && resident_fits(s))) {

@@ -16,7 +16,7 @@ import numpy as np
 from . import _native
 
 # solver / storage / status codes (include/sfr3d_b200.h; Define.h:392-412)
-PCG, PBICGSTAB = 1, 2
+PCG, PBICGSTAB, PBICGSTABL2, GMRES, MINRES = 1, 2, 3, 4, 5
 CSRD, CSRC, ELLPACK = 2, 3, 4
 OK, MAXIT, BREAKDOWN = 0, 1, 2
 BAD_INPUT, CUDA_ERROR, TIMEOUT, UNSUPPORTED = -1, -2, -3, -4

@@ -70,8 +70,9 @@ def test_solverC_rejects_unsupported_solver_without_exiting():
     ia = np.array([0, 0, 1], np.int32)
     ja = np.array([0], np.int32)
     x = np.zeros(2)
+    # 6 = PARDISO (Define.h:397): MKL's direct solver, not on this path
     rc = sv.solverC(2, 2, 1, 0, ia, ja, np.ones(1), np.ones(2), None,
-                    np.ones(2), x, 1e-10, 10, sv.CSRD, 4, exit_on_failure=False)
+                    np.ones(2), x, 1e-10, 10, sv.CSRD, 6, exit_on_failure=False)
     assert rc == sv.UNSUPPORTED
 
 

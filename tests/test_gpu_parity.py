@@ -80,14 +80,28 @@ def test_solver_against_reference_fixture(cuda, engine, name):
     sysg.set_values(g["al"], g["ad"])
     sysg.set_engine(engine)
     x, info = sysg.solve(solver, g["b"], x0=g["x0"], tol=float(g["tol"][0]),
-                         maxit=maxit, newx=bool(newx))
+                         maxit=maxit, newx=bool(newx), raise_on_error=False)
+    # GMRES counts iterations in restart cycles of 15 (Iters.c:651)
+    slack, x_bar = (15 if solver == sv.GMRES else 1), TOL_X
+    if solver in (sv.PBICGSTABL2, sv.GMRES) and status == 0:
+        # sensitive to the dot products' summation order: the bar is the
+        # spread the reference's own algorithm shows when only that changes
+        d_it, d_x = O.order_spread(solver, st, bool(un), g["ia"], g["ja"], g["al"], g["ad"],
+                                   g["b"], x0=g["x0"], tol=float(g["tol"][0]),
+                                   maxit=maxit, newx=bool(newx))
+        slack, x_bar = max(slack, 2 * d_it), max(x_bar, 20 * d_x)
+    if solver == sv.MINRES and iters == maxit + 1:
+        status = 1  # the reference's MINRES only warns at maxIt (Iters.c:525-529)
     if status == 0:
         assert info.status == sv.OK
-        assert abs(info.iters - iters) <= 1
-        assert rel(x, g["x"]) < TOL_X
+        assert abs(info.iters - iters) <= slack
+        assert rel(x, g["x"]) < x_bar
     else:
         assert info.status == sv.MAXIT
-        assert info.iters == iters + 1 or info.iters == maxit + 1
+        if solver == sv.GMRES:
+            assert info.iters == 15 * maxit + 1
+        else:
+            assert info.iters == iters + 1 or info.iters == maxit + 1
         assert rel(x, g["x"]) < 1e-10
 
 
