@@ -295,7 +295,9 @@ def run_ours(args):
     momentum = batch = adjoint = target = None
     if world > 1 and not args.no_extras:
         batch = batch_leg_sharded(sv, S, rank, world, max_over_ranks)
+    other = None
     if extras and not args.no_extras:
+        other = other_krylov_leg(sv, S, s, n)
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -344,7 +346,7 @@ def run_ours(args):
     # CPU baseline: the reference's own pcgOmp on this host (rank 0, N = 1)
     cpu = None
     if not args.no_cpu and extras:
-        cpu = cpu_baseline(s, iters)
+        cpu = cpu_baseline(s, iters, n)
 
     if rank != 0:
         if world > 1:
@@ -396,6 +398,7 @@ def run_ours(args):
         "momentum": momentum,
         "batched": batch,
         "adjoint": adjoint,
+        "other_krylov": other,
         "target_mixed_batched_vs_fp64": target,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -540,6 +543,30 @@ def batch_leg_sharded(sv, S, rank, world, max_over_ranks):
             "fp64_ms_max_over_ranks": ms["fp64"], "mixed_ms_max_over_ranks": ms["mixed"]}
 
 
+def other_krylov_leg(sv, S, s, n):
+    """The other Krylov methods behind solverC at 128^3, FP64, one
+    right-hand side: MINRES on the pressure system (symmetric), BiCGSTAB(2)
+    and GMRES(15) on the momentum system.  Device time of the second of two
+    solves; the reference's times are in cpu_baseline.other_krylov."""
+    m = S.momentum(n, nrhs=1, seed=3)
+    gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
+    gm.set_values(m.al, m.ad)
+    gp = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    gp.set_values(s.al, s.ad)
+    out = {}
+    for name, g, sysx, solver in (("minres_pressure", gp, s, sv.MINRES),
+                                  ("bicgstabl2_momentum", gm, m, sv.PBICGSTABL2),
+                                  ("gmres15_momentum", gm, m, sv.GMRES)):
+        for _ in range(2):
+            _, info = g.solve(solver, sysx.b[0], tol=1e-10, maxit=100000)
+        out[name] = {"ms": info.seconds * 1e3, "iters": info.iters, "status": info.status,
+                     "us_per_iteration": info.seconds * 1e6 / max(info.iters, 1),
+                     "true_relres_2norm": info.norm_r / float((sysx.b[0] ** 2).sum() ** 0.5)}
+    gm.close()
+    gp.close()
+    return out
+
+
 def adjoint_leg(np, sv, S):
     """Adjoint of the 96^3 Peclet-20 momentum system, J = w.x: transpose
     solve time (FP64 and mixed) and the largest relative difference to
@@ -571,7 +598,40 @@ def adjoint_leg(np, sv, S):
     return out
 
 
-def cpu_baseline(s, iters_full):
+def cpu_other_krylov(O, s, n, threads):
+    """The reference's own BiCGSTAB(2), GMRES(15) (OpenMP variants) and MINRES
+    (serial: its OpenMP branch is commented out in callMinRes) on the
+    other_krylov workloads: per-iteration time from a bounded sample."""
+    from sfr3d_b200 import systems as S
+    m = S.momentum(n, nrhs=1, seed=3)
+    il, jl, al = s.csrd_lower()
+    out = {}
+    for name, args, solver, maxit, nth in (
+            ("minres_pressure", (O.CSRC, False, il, jl, al, s.ad, s.b[0]), O.MINRES, 100, 0),
+            ("bicgstabl2_momentum", (O.CSRD, True, m.ia, m.ja, m.al, m.ad, m.b[0]),
+             O.PBICGSTABL2, 100000, threads),
+            ("gmres15_momentum", (O.CSRD, True, m.ia, m.ja, m.al, m.ad, m.b[0]),
+             O.GMRES, 100000, threads)):
+        r = O.ref_solve(solver, *args, tol=1e-10, maxit=maxit, nthreads=nth)
+        # MINRES only warns at maxIt and reports maxIt + 1 iterations
+        it = maxit if (solver == O.MINRES and r.iters > maxit) else r.iters
+        out[name] = {"ms_per_iteration": r.seconds / max(it, 1) * 1e3, "threads": max(nth, 1),
+                     "sample": ("full solve" if r.iters <= maxit else f"{maxit} iterations"),
+                     "iters": r.iters}
+    return out
+
+
+def cpu_baseline(s, iters_full, n):
+    """The reference's pcgOmp on the bench system (cpu_pcg_baseline), plus
+    its other Krylov methods on the other_krylov workloads."""
+    res = cpu_pcg_baseline(s, iters_full)
+    if "unavailable" not in res:
+        from oracle import oracle as O
+        res["other_krylov"] = cpu_other_krylov(O, s, n, res["cores"])
+    return res
+
+
+def cpu_pcg_baseline(s, iters_full):
     """The reference's own pcgOmp (Cg.c:490) with all host threads on the
     same system in CSRC symmetric storage (the reference's default): a full
     solve when one takes under 30 s, else a bounded sample scaled to the
