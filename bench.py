@@ -292,12 +292,13 @@ def run_ours(args):
     spmv_gbs = sb / (spmv_ms * 1e-3) / 1e9
     sp_tr = committed_traffic("spmv_kernel")
 
-    momentum = batch = adjoint = target = None
+    momentum = batch = adjoint = target = assembly = None
     if world > 1 and not args.no_extras:
         batch = batch_leg_sharded(sv, S, rank, world, max_over_ranks)
     other = None
     if extras and not args.no_extras:
         other = other_krylov_leg(sv, S, s, n)
+        assembly = assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -399,6 +400,7 @@ def run_ours(args):
         "batched": batch,
         "adjoint": adjoint,
         "other_krylov": other,
+        "assembly": assembly,
         "target_mixed_batched_vs_fp64": target,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -567,6 +569,106 @@ def other_krylov_leg(sv, S, s, n):
     return out
 
 
+# algorithmic bytes per row of the ORTHOGONAL diffusion assembly kernel on a
+# hexahedral mesh (6 faces): plan row header (cell 4 + face count 2), per
+# face the neighbour/destination words (8) and 3 geometry doubles (24), the
+# cell's own diffusivity and u0 (16); writes 6 off-diagonals, ad, b, rCell
+# (72).  Neighbour gathers are counted once (they are other rows' own reads).
+ASSEMBLY_ALG_BYTES_PER_ROW = 6 + 6 * 32 + 16 + 72
+
+
+def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
+    """systFormDif on the device for the 128^3 pressure mesh (ORTHOGONAL,
+    Dirichlet on x = 0, Neumann elsewhere, residual form): one call writes
+    A (CSRD) and b where the next solve reads them.  Beside it: the per-call
+    upload of A and b the host-assembled path needs, and the host-array
+    entry point (fields in, b and rCell out)."""
+    from sfr3d_b200 import assembly as A
+    m = s.mesh()
+    rng = np.random.default_rng(9)
+    facer = m.face_r([1, 0, 0, 0, 0, 0])
+    loads = [A.Load(A.DIRICHLET, (0.0,))]
+    t0 = time.perf_counter()
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    plan = A.DifPlan(g, m, facer, icod=A.ORTHOGONAL)
+    torch.cuda.synchronize()
+    plan_s = time.perf_counter() - t0
+    u0 = rng.standard_normal(m.numel)
+    dev = lambda a: torch.tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+    d_u0, d_k = dev(u0), dev(m.cdiff)
+    d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
+    d_r = torch.empty(m.numel, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def call():
+        plan.assemble_device(loads, d_u0.data_ptr(), d_k.data_ptr(), d_b=d_b.data_ptr(),
+                             d_rcell=d_r.data_ptr(), stream=st.cuda_stream)
+    reps = 10
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            call()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+        for i in range(reps):
+            flush.fill_(i & 0xFF)
+            ev[2 * i].record(st)
+            call()
+            ev[2 * i + 1].record(st)
+    st.synchronize()
+    dev_ms = sorted(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps))[reps // 2]
+    alg = ASSEMBLY_ALG_BYTES_PER_ROW * s.neq
+    # the host-assembled path: A (al, ad) and b uploaded every call
+    h_al = torch.from_numpy(s.al).pin_memory()
+    h_ad = torch.from_numpy(s.ad).pin_memory()
+    h_b = torch.from_numpy(s.b[0]).pin_memory()
+    d_al = torch.empty_like(h_al, device="cuda")
+    d_ad = torch.empty_like(h_ad, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        d_al.copy_(h_al, non_blocking=True)
+        d_ad.copy_(h_ad, non_blocking=True)
+        d_b.copy_(h_b, non_blocking=True)
+    torch.cuda.synchronize()
+    upload_ms = (time.perf_counter() - t0) * 1e3 / reps
+    # the host-array entry point: u0 and the diffusivity in, b and rCell out
+    plan.assemble(loads, u0, m.cdiff)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        plan.assemble(loads, u0, m.cdiff)
+    host_ms = (time.perf_counter() - t0) * 1e3 / 3
+    plan.close()
+    g.close()
+    gbs = alg / (dev_ms * 1e-3) / 1e9
+    return {"workload": f"systFormDif, diffusion {n}^3 = {s.neq} cells (the pressure mesh), "
+                        "ORTHOGONAL, Dirichlet x=0, residual form, CSRD",
+            "device_ms": dev_ms, "plan_create_s": plan_s,
+            "alg_bytes_per_call": alg, "alg_bytes_per_row": ASSEMBLY_ALG_BYTES_PER_ROW,
+            "GB/s": gbs, "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "timing": "CUDA events around one call (assembly kernel + the value refresh "
+                      "into the solver's SELL copy), 256 MiB L2 flush between calls, median "
+                      "of 10",
+            "upload_A_b_pinned_ms": upload_ms,
+            "host_api_ms": host_ms,
+            "host_api": "sfr_gpu_dif_assemble: u0 + diffusivity H2D, b + rCell D2H "
+                        "(pageable numpy)"}
+
+
+def cpu_assembly(O, s):
+    """The reference's own systFormDif (serial, as the reference runs it) on
+    the assembly leg's workload."""
+    import numpy as np
+    m = s.mesh()
+    rng = np.random.default_rng(9)
+    case = O.DifCase(mesh=m, facer=m.face_r([1, 0, 0, 0, 0, 0]),
+                     loads=[O.Load(O.DIRICHLET, (0.0,))], density=np.ones(m.numel),
+                     cdiff=m.cdiff, u0=rng.standard_normal(m.numel),
+                     gradu0=np.zeros((m.numel, 3)), icod=O.ORTHOGONAL)
+    rc, *_, sec = O.ref_dif_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    return {"ms": sec * 1e3, "threads": 1, "status": rc,
+            "sample": "one full systFormDif call (the reference's loop is serial)"}
+
+
 def adjoint_leg(np, sv, S):
     """Adjoint of the 96^3 Peclet-20 momentum system, J = w.x: transpose
     solve time (FP64 and mixed) and the largest relative difference to
@@ -628,6 +730,7 @@ def cpu_baseline(s, iters_full, n):
     if "unavailable" not in res:
         from oracle import oracle as O
         res["other_krylov"] = cpu_other_krylov(O, s, n, res["cores"])
+        res["assembly"] = cpu_assembly(O, s)
     return res
 
 

@@ -230,6 +230,109 @@ int sfr_gpu_dot_noalloc(const double *d_a, const double *d_b, int32_t n,
 int sfr_gpu_stats(const sfr_system *s, int64_t *bytes, int64_t *slots,
                   int32_t *bandwidth);
 
+/* ---- device assembly of the diffusion system ------------------------- */
+/* systFormDif (CellLoop.c:285-455) -> cellDif3D (CellDif.c:312-537) run on
+ * the GPU and write the system's values where solverC reads them: the raw
+ * al (| au) / ELLPACK slots the reference's csr()/ellPack() fill
+ * (Csr.c:549-1022, EllPack.c:113-149), the diagonal and the force vector,
+ * with the same rounding as the reference (ndf = 1, ndm = 3, one process).
+ * The matrix never crosses PCIe: the next sfr_gpu_solve_device uses it. */
+
+/* The mesh arrays systFormDif reads, as the reference stores them (1-based
+ * indices; MAT2D/MAT3D row-major).  Arrays systFormDif passes through but
+ * cellDif3D does not read (node incidence, eta, face centres, |vSkew|,
+ * geometry types) are not needed. */
+typedef struct {
+  int32_t numel;           /* cells (mesh->numelNov) */
+  int32_t maxviz;          /* face slots per cell (mesh->maxViz), 1..8 */
+  int64_t nfaces;          /* length of the per-face arrays */
+  int32_t nmat;            /* length of caltype */
+  int32_t pad;
+  const int32_t *nelcon;   /* numel*maxviz: neighbour + 1, -1 boundary (elm.adj.nelcon) */
+  const int16_t *nviz;     /* numel: faces of the cell (elm.adj.nViz) */
+  const int32_t *cellface; /* numel*maxviz: face + 1 (elm.cellFace) */
+  const int32_t *owner;    /* nfaces*2: owner cell + 1 first (face.owner) */
+  const double *volume;    /* numel (elm.geom.volume) */
+  const double *dcca;      /* numel*maxviz (elm.geom.dcca) */
+  const double *xmcc;      /* numel*maxviz*3 (elm.geom.xmcc) */
+  const double *mksi;      /* nfaces (face.mksi) */
+  const double *ksi;       /* nfaces*3 (face.ksi) */
+  const double *area;      /* nfaces (face.area) */
+  const double *normal;    /* nfaces*3 (face.normal) */
+  const double *vskew;     /* nfaces*3 (face.vSkew) */
+  const int16_t *caltype;  /* nmat: cell library of the material (1 = diffusion) */
+  const int16_t *mat;      /* numel: material + 1 (elm.mat) */
+  const int32_t *id;       /* numel: equation + 1 (sistEqD->id) */
+  const int16_t *facer;    /* numel*(maxviz+1): load + 1 per face, then the cell's own entry */
+} sfr_dif_mesh;
+
+/* One entry of the load table (Loads, StructDefine.h:356-366). */
+typedef struct {
+  int32_t type;   /* DIRICHLETBC 1, NEUMANNBC 2, ROBINBC 3, INLET 6 (Define.h:317-323) */
+  int32_t var;    /* nTypeVar: 0 constant (1 = function: SFR_UNSUPPORTED) */
+  int32_t np;     /* parameters given */
+  int32_t pad;
+  double par[20]; /* MAXLOADPARAMETER */
+} sfr_load;
+
+/* The rest of what systFormDif reads (Diffusion.iCod, DiffModel.fRes,
+ * Temporal). */
+typedef struct {
+  int32_t icod;      /* 1 ORTHOGONAL 2 MINIMAL 3 ORTHOGONALC 4 OVERRELAXED (Define.h:304-307) */
+  int32_t fres;      /* b = the cell residual (1) or the force (0) */
+  int32_t time_flag; /* Temporal.flag: implicit time term */
+  int32_t time_type; /* 0 EULER, 1 BACKWARD */
+  double dt, dt0;    /* Temporal.dt[0], dt[1] */
+} sfr_dif_opts;
+
+typedef struct sfr_dif_plan sfr_dif_plan;
+
+/* Bind a mesh to a system (whose pattern is the one dataStruct built for
+ * that mesh) and precompute on the GPU, once, what cellDif3D derives from
+ * the geometry alone for scheme `icod`: the face weights, |E| and the
+ * non-orthogonal split.  SFR_BAD_INPUT for a mesh the reference cannot
+ * assemble (a cell library other than diffusion, an equation number out of
+ * range or used twice, a neighbour index that is neither a cell nor -1, a
+ * row holding a column twice), with the reason in sfr_last_error(). */
+int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
+                            sfr_dif_plan **out);
+
+/* One systFormDif call with device arrays on `stream`: density, cdiff, u0
+ * (numel) and gradu0 (numel*3, unused for ORTHOGONAL) in; b (neq) and rcell
+ * (numel) out when forces / calrcell are set; the matrix into the system
+ * when matrix is set.  b0 (neq, may be NULL) is added to b and to the cell
+ * residuals as Diffusion.c:107-118 does after the call.  loads: nloads <= 32
+ * host entries; a face may only name a load below nloads.  SINBC loads and
+ * loads given as functions are SFR_UNSUPPORTED, OUTLET (which reads a
+ * velocity the diffusion cell has not) SFR_BAD_INPUT. */
+int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
+                                const sfr_dif_opts *o, const double *d_density,
+                                const double *d_cdiff, const double *d_u0,
+                                const double *d_gradu0, const double *d_b0, double *d_b,
+                                double *d_rcell, int32_t forces, int32_t matrix,
+                                int32_t calrcell, void *stream);
+
+/* The same with host arrays: the fields are copied in, b and rcell copied
+ * back (either may be NULL); the matrix stays on the device. */
+int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
+                         const sfr_dif_opts *o, const double *density, const double *cdiff,
+                         const double *u0, const double *gradu0, const double *b0, double *b,
+                         double *rcell, int32_t forces, int32_t matrix, int32_t calrcell);
+
+int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
+
+/* Copy the system's values back in the reference's layout: al (nad, or the
+ * neq*width ELLPACK slots), ad (neq) and, for unsym CSRC, au (nad).  Any
+ * pointer may be NULL. */
+int sfr_gpu_get_values(sfr_system *s, double *al, double *ad, double *au);
+
+/* x -> u as updateCellValue does after the solve (CellLoop.c:4023-4057,
+ * ndf = 1): u[cell] = x[id[cell] - 1] (add = 0) or += (add = 1) for every
+ * cell with id > 0, on device arrays. */
+int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, int32_t add,
+                             void *stream);
+
+
 const char *sfr_status_string(int status);
 /* Text of the last failure on the calling thread (validation or CUDA). */
 const char *sfr_last_error(void);

@@ -101,6 +101,43 @@ int sfr_sys_rhs(const void *h, double *b);
 /* new equation number of each natural cell id (i + nx*(j + ny*k)). */
 int sfr_sys_numbering(const void *h, int32_t *eq_of_cell);
 
+/* The box as the reference's mesh arrays: the geometry inputs of systFormDif
+ * (CellLoop.c:285-311) with maxViz = 6 face slots per cell in the order
+ * x-, x+, y-, y+, z-, z+ (the ELLPACK slot order above).  Cell arrays are
+ * indexed by natural cell id; every index is 1-based as the reference stores
+ * it.  Faces are oriented out of their owner (fOwner[2f], the minus-side
+ * cell; the plus-side cell on a minus boundary).  Geometry:
+ *   cell centre = mean of the 8 vertices; volume by 6 tetrahedra;
+ *   face centre xm = mean of the 4 vertices; area vector
+ *   0.5 (v2 - v0) x (v3 - v1); normal its unit vector;
+ *   ksi = unit vector from the owner's centre to the neighbour's (to xm on
+ *   the boundary), mksi its length; vSkew = (point where the centre line
+ *   crosses the face plane) - xm, zero on the boundary; eta = unit first
+ *   edge of the face; per cell slot xmcc = xm - centre and
+ *   dcca = |xmcc . normal|. */
+typedef struct {
+  int32_t *nelcon;   /* numel*6: neighbour cell + 1, -1 on the boundary */
+  int16_t *nviz;     /* numel: faces of the cell (6) */
+  int32_t *cellface; /* numel*6: face id + 1 */
+  double *volume;    /* numel */
+  double *dcca;      /* numel*6 */
+  double *xmcc;      /* numel*6*3 */
+  double *cdiff;     /* numel: the cell diffusivity of the system */
+  int32_t *id;       /* numel: equation + 1 */
+  int32_t *owner;    /* nface*2: owner cell + 1, neighbour cell + 1 or -1 */
+  double *mksi;      /* nface */
+  double *ksi;       /* nface*3 */
+  double *eta;       /* nface*3 */
+  double *area;      /* nface */
+  double *normal;    /* nface*3 */
+  double *xm;        /* nface*3 */
+  double *mvskew;    /* nface */
+  double *vskew;     /* nface*3 */
+} sfr_sys_mesh_t;
+
+int sfr_sys_mesh_sizes(const void *h, int32_t *numel, int64_t *nface);
+int sfr_sys_mesh(const void *h, const sfr_sys_mesh_t *m);
+
 /* Reverse Cuthill-McKee of a symmetric graph given as CSR adjacency
  * (xadj[n+1], adj[]): perm[new] = old.  Returns 0 on success. */
 int sfr_rcm(int32_t n, const int32_t *xadj, const int32_t *adj, int32_t *perm);

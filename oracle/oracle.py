@@ -215,3 +215,171 @@ def ell_ia(neq: int, width: int) -> np.ndarray:
     """The ifEllPack header solverC receives as ia for ELLPACK
     (EllPack.c:35-36): [width, neq*width]."""
     return np.array([width, neq * width], dtype=np.int32)
+
+
+# ------------------------------------------------ diffusion assembly --
+# systFormDif (CellLoop.c:285-455) -> cellDif3D (CellDif.c:312-537)
+MAXLOADPAR = 20                                   # Define.h:336
+DIRICHLET, NEUMANN, ROBIN, SINBC, INLET, OUTLET = 1, 2, 3, 4, 6, 7  # Define.h:317-323
+ORTHOGONAL, MINIMAL, ORTHOGONALC, OVERRELAXED = 1, 2, 3, 4        # Define.h:304-307
+EULER, BACKWARD = 0, 1                                             # Define.h:191-192
+
+
+@dataclass
+class Load:
+    """One entry of the reference's load table (Loads, StructDefine.h:356):
+    type, parameters, nTypeVar (0 constant, 1 function)."""
+    type: int
+    par: tuple = ()
+    var: int = 0
+    np: int | None = None
+
+    def arrays(self):
+        par = np.zeros(MAXLOADPAR)
+        par[:len(self.par)] = self.par
+        return self.type, self.var, len(self.par) if self.np is None else self.np, par
+
+
+@dataclass
+class DifCase:
+    """Everything one systFormDif call reads besides the pattern: the mesh
+    arrays (any object with the attributes of sfr3d_b200.systems.FvMesh),
+    the per-cell fields and the options."""
+    mesh: object
+    facer: np.ndarray            # (numel, maxviz + 1) short
+    loads: list
+    density: np.ndarray
+    cdiff: np.ndarray
+    u0: np.ndarray
+    gradu0: np.ndarray           # (numel, 3)
+    icod: int = ORTHOGONAL
+    fres: bool = True
+    time_flag: bool = False
+    time_type: int = EULER
+    dt: float = 1.0
+    dt0: float = 1.0
+    caltype: np.ndarray | None = None
+    mat: np.ndarray | None = None
+
+    def material(self):
+        mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
+               else _c(self.mat, np.int16))
+        cal = np.ones(1, np.int16) if self.caltype is None else _c(self.caltype, np.int16)
+        return cal, mat
+
+    def load_arrays(self):
+        n = max(len(self.loads), 1)
+        t = np.zeros(n, np.int32)
+        v = np.zeros(n, np.int32)
+        npar = np.zeros(n, np.int32)
+        par = np.zeros((n, MAXLOADPAR))
+        for i, ld in enumerate(self.loads):
+            t[i], v[i], npar[i], par[i] = ld.arrays()
+        return t, v, npar, par
+
+
+def dif_size(storage, unsym, neq, ia, ja) -> int:
+    """Length of the value array the assembly writes (al, al|au, ELL slots)."""
+    if storage == ELLPACK:
+        return int(ia[1])
+    return 2 * len(ja) if (storage == CSRC and unsym) else len(ja)
+
+
+class _DifMesh(ctypes.Structure):
+    _fields_ = [("numel", ctypes.c_int), ("maxviz", ctypes.c_int)] + [
+        (n, _P) for n in ("nelcon", "nface", "cellface", "owner", "volume",
+                          "dcca", "xmcc", "mksi", "ksi", "area", "normal",
+                          "vskew", "caltype", "mat", "id", "facer")]
+
+
+class _DifLoad(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("var", ctypes.c_int), ("np", ctypes.c_int),
+                ("par", ctypes.c_double * MAXLOADPAR)]
+
+
+class _DifOpts(ctypes.Structure):
+    _fields_ = [("icod", ctypes.c_int), ("fres", ctypes.c_int),
+                ("time_flag", ctypes.c_int), ("time_type", ctypes.c_int),
+                ("dt", ctypes.c_double), ("dt0", ctypes.c_double)]
+
+
+def _dif_out(storage, unsym, neq, ia, ja, numel, fill):
+    a = np.full(dif_size(storage, unsym, neq, ia, ja), fill)
+    return a, np.full(neq, fill), np.full(neq, fill), np.full(numel, fill)
+
+
+def dif_assemble(case: DifCase, storage, unsym, ia, ja, neq, forces=True,
+                 matrix=True, calrcell=True, fill=0.0):
+    """The C restatement of systFormDif: (rc, a, ad, b, rcell)."""
+    m = case.mesh
+    lib = oracle_lib()
+    if not getattr(lib, "_dif_typed", False):
+        lib.orc_dif_assemble.restype = ctypes.c_int
+        lib.orc_dif_assemble.argtypes = (
+            [ctypes.POINTER(_DifMesh), ctypes.POINTER(_DifLoad), ctypes.c_int,
+             ctypes.POINTER(_DifOpts)] + [_P] * 4 + [ctypes.c_int] * 4 + [_P] * 6
+            + [ctypes.c_int] * 3)
+        lib._dif_typed = True
+    cal, mat = case.material()
+    keep = dict(
+        nelcon=_c(m.nelcon, np.int32), nface=_c(m.nviz, np.int16),
+        cellface=_c(m.cellface, np.int32), owner=_c(m.owner, np.int32),
+        volume=_c(m.volume, np.float64), dcca=_c(m.dcca, np.float64),
+        xmcc=_c(m.xmcc, np.float64), mksi=_c(m.mksi, np.float64),
+        ksi=_c(m.ksi, np.float64), area=_c(m.area, np.float64),
+        normal=_c(m.normal, np.float64), vskew=_c(m.vskew, np.float64),
+        caltype=cal, mat=mat, id=_c(m.id, np.int32), facer=_c(case.facer, np.int16))
+    dm = _DifMesh(numel=m.numel, maxviz=m.nelcon.shape[1],
+                  **{k: _p(v) for k, v in keep.items()})
+    t, v, npar, par = case.load_arrays()
+    loads = (_DifLoad * len(t))()
+    for i in range(len(t)):
+        loads[i].type, loads[i].var, loads[i].np = int(t[i]), int(v[i]), int(npar[i])
+        loads[i].par[:] = list(par[i])
+    o = _DifOpts(icod=case.icod, fres=int(case.fres), time_flag=int(case.time_flag),
+                 time_type=case.time_type, dt=case.dt, dt0=case.dt0)
+    ia, ja = _c(ia, np.int32), _c(ja, np.int32)
+    a, ad, b, rc_ = _dif_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    fields = [_c(case.density, np.float64), _c(case.cdiff, np.float64),
+              _c(case.u0, np.float64), _c(case.gradu0, np.float64)]
+    nad = len(ja) if storage != ELLPACK else 0
+    rc = lib.orc_dif_assemble(ctypes.byref(dm), loads, len(case.loads), ctypes.byref(o),
+                              *[_p(f) for f in fields], storage, int(unsym), neq, nad,
+                              _p(ia), _p(ja), _p(a), _p(ad), _p(b), _p(rc_),
+                              int(forces), int(matrix), int(calrcell))
+    return rc, a, ad, b, rc_
+
+
+def ref_dif_assemble(case: DifCase, storage, unsym, ia, ja, neq, forces=True,
+                     matrix=True, calrcell=True, fill=0.0):
+    """The reference's own systFormDif: (rc, a, ad, b, rcell, seconds)."""
+    m = case.mesh
+    lib = ref_lib()
+    if not getattr(lib, "_dif_typed", False):
+        lib.sfr_ref_syst_form_dif.restype = ctypes.c_int
+        lib.sfr_ref_syst_form_dif.argtypes = (
+            [ctypes.c_int, ctypes.c_int] + [_P] * 29 + [ctypes.c_int] + [_P] * 4
+            + [ctypes.c_int] * 4 + [ctypes.c_double] * 2 + [ctypes.c_int] * 7 + [_P])
+        lib._dif_typed = True
+    cal, mat = case.material()
+    cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
+    ia, ja = cp(ia, np.int32), cp(ja, np.int32)
+    a, ad, b, rcell = _dif_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    t, v, npar, par = case.load_arrays()
+    sec = ctypes.c_double()
+    arrs = [cp(m.nelcon, np.int32), cp(m.nviz, np.int16), cp(m.cellface, np.int32),
+            cp(m.owner, np.int32), cp(m.volume, np.float64), cp(m.dcca, np.float64),
+            cp(m.xmcc, np.float64), cp(m.mksi, np.float64), cp(m.ksi, np.float64),
+            cp(m.eta, np.float64), cp(m.area, np.float64), cp(m.normal, np.float64),
+            cp(m.xm, np.float64), cp(m.mvskew, np.float64), cp(m.vskew, np.float64),
+            cal.copy(), mat.copy(), cp(case.density, np.float64),
+            cp(case.cdiff, np.float64), ia, ja, a, ad, b, cp(m.id, np.int32),
+            cp(case.facer, np.int16), cp(case.u0, np.float64),
+            cp(case.gradu0, np.float64), rcell]
+    nad = len(ja) if storage != ELLPACK else int(ia[1])
+    rc = lib.sfr_ref_syst_form_dif(
+        m.numel, m.nelcon.shape[1], *[_p(x) for x in arrs], len(case.loads),
+        _p(t), _p(v), _p(npar), _p(par), case.icod, int(case.fres),
+        int(case.time_flag), case.time_type, case.dt, case.dt0, neq, nad, storage,
+        int(forces), int(matrix), int(calrcell), int(unsym), ctypes.byref(sec))
+    return rc, a, ad, b, rcell, sec.value

@@ -22,6 +22,7 @@
 #include <omp.h>
 
 #include <Solv.h>
+#include <CellLoop.h>
 
 extern Omp ompVar;
 extern Mpi mpiVar;
@@ -150,3 +151,81 @@ int sfr_ref_solve(int neq, int nad, int *ia, int *ja, double *al, double *ad,
 double sfr_ref_smachn(void) { return smachn(); }
 
 int sfr_ref_max_threads(void) { return omp_get_max_threads(); }
+
+/*
+ * Assemble the diffusion system with the reference's own systFormDif
+ * (CellLoop.c:285-455) as diffusion() calls it (Diffusion.c:80-106), ndf = 1,
+ * ndm = 3, one process.  Loads are given as parallel arrays (type, nTypeVar,
+ * np, par[20] each); the scheme, residual form and time term as scalars.
+ * Arrays the assembly does not read (the node incidence, node counts,
+ * geometry types, face centres, eta, |vSkew|) are still passed through.
+ * Returns the exit code when the reference exits (an unknown scheme).
+ */
+int sfr_ref_syst_form_dif(int numel, int maxviz, int *nelcon, short *nface,
+                          int *cellface, int *owner, double *volume,
+                          double *dcca, double *xmcc, double *mksi,
+                          double *ksi, double *eta, double *area,
+                          double *normal, double *xm, double *mvskew,
+                          double *vskew, short *caltype, short *mat,
+                          double *density, double *cdiff, int *ia, int *ja,
+                          double *a, double *ad, double *b, int *id,
+                          short *facer, double *u0, double *gradu0,
+                          double *rcell, int nloads, const int *ltype,
+                          const int *lvar, const int *lnp, const double *lpar,
+                          int icod, int fres, int time_flag, int time_type,
+                          double dt, double dt0, int neq, int nad, int storage,
+                          int forces, int matrix, int calrcell, int unsym,
+                          double *seconds)
+{
+  Loads *loads = calloc(nloads > 0 ? nloads : 1, sizeof(Loads));
+  INT *el = calloc((size_t)numel * 8, sizeof(INT));
+  short *nen = malloc((size_t)numel * sizeof(short));
+  short *gtype = calloc((size_t)numel, sizeof(short));
+  Diffusion diff;
+  DiffModel dmodel;
+  Temporal ddt;
+  int i, j, rc = 0;
+  double t0;
+
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  mpiVar.nPrcs = 1;
+  mpiVar.myId = 0;
+  for (i = 0; i < numel; i++) nen[i] = 8;
+  for (i = 0; i < nloads; i++) {
+    loads[i].fUse = true;
+    loads[i].type = (short)ltype[i];
+    loads[i].nTypeVar = (short)lvar[i];
+    loads[i].np = (short)lnp[i];
+    for (j = 0; j < MAXLOADPARAMETER; j++) loads[i].par[j] = lpar[i * MAXLOADPARAMETER + j];
+  }
+  memset(&diff, 0, sizeof(diff));
+  memset(&dmodel, 0, sizeof(dmodel));
+  memset(&ddt, 0, sizeof(ddt));
+  diff.iCod = (short)icod;
+  dmodel.fRes = fres != 0;
+  ddt.flag = time_flag != 0;
+  ddt.type = (short)time_type;
+  ddt.dt[0] = dt;
+  ddt.dt[1] = dt0;
+  *seconds = 0.0;
+  if (setjmp(g_jump) == 0) {
+    g_armed = 1;
+    t0 = omp_get_wtime();
+    systFormDif(loads, &diff, &dmodel, el, nelcon, nen, nface, cellface, owner,
+                volume, dcca, xmcc, mksi, ksi, eta, area, normal, xm, mvskew,
+                vskew, gtype, caltype, mat, density, cdiff, ia, ja, a, ad, b,
+                id, facer, u0, gradu0, rcell, &ddt, neq, neq, nad, 0,
+                8, (short)maxviz, 3, numel, 1, (short)storage, forces != 0,
+                matrix != 0, calrcell != 0, unsym != 0);
+    *seconds = omp_get_wtime() - t0;
+    g_armed = 0;
+  } else {
+    rc = g_exit_code == 0 ? -1000 : g_exit_code;
+  }
+  free(loads);
+  free(el);
+  free(nen);
+  free(gtype);
+  return rc;
+}

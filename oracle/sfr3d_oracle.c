@@ -536,3 +536,217 @@ int orc_gmres(int storage, int unsym, int neq, const int *ia, const int *ja,
   free(y);
   return st->status;
 }
+
+/* ======================================================================
+ * Diffusion system assembly: systFormDif (CellLoop.c:285-455) calling
+ * cellDif3D (CellDif.c:312-537) per cell, then csr()/ellPack() (Csr.c:549,
+ * EllPack.c:113).  Every floating-point expression keeps the reference's
+ * operand order (C evaluates a + b + c as (a + b) + c).
+ * ====================================================================== */
+
+/* difusionSchemeNew, ndm = 3 (CellLib.c:5824-6000): split of the area
+ * vector s into the implicit part e along ksi and the explicit rest t. */
+static int dif_scheme(const double s[3], const double k[3], double e[3], double t[3], int icod)
+{
+  double ss, nk, tmp;
+  int j;
+  switch (icod) {
+  case 1: /* ORTHOGONAL */
+    ss = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (j = 0; j < 3; j++) { e[j] = ss * k[j]; t[j] = 0.0; }
+    return 0;
+  case 2: /* MINIMAL */
+    nk = s[0] * k[0] + s[1] * k[1] + s[2] * k[2];
+    tmp = nk;
+    for (j = 0; j < 3; j++) e[j] = tmp * k[j];
+    for (j = 0; j < 3; j++) t[j] = s[j] - e[j];
+    return 0;
+  case 3: /* ORTHOGONALC */
+    ss = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (j = 0; j < 3; j++) e[j] = ss * k[j];
+    for (j = 0; j < 3; j++) t[j] = s[j] - e[j];
+    return 0;
+  case 4: /* OVERRELAXED */
+    ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    nk = s[0] * k[0] + s[1] * k[1] + s[2] * k[2];
+    tmp = ss / nk;
+    for (j = 0; j < 3; j++) e[j] = tmp * k[j];
+    for (j = 0; j < 3; j++) t[j] = s[j] - e[j];
+    return 0;
+  }
+  return -1;
+}
+
+/* pLoad for constant loads (Loads.c:881-990, getLoads Loads.c:122-169):
+ * adds the boundary face's share to the diagonal sP and the force p. */
+static int dif_load(const orc_load *ld, double *sP, double *p, const double n[3], double kc,
+                    double area, double dcca)
+{
+  double aP, h, tA, wfn, rhoEnv;
+  switch (ld->type) {
+  case 1: /* DIRICHLETBC */
+    if (ld->var != 0) return -2;
+    if (ld->np < 1) return -1;
+    tA = ld->par[0];
+    aP = kc * area / dcca;
+    *sP += aP;
+    *p += aP * tA;
+    return 0;
+  case 3: /* ROBINBC: par[0] = h, par[1] = the far value */
+    h = ld->par[0];
+    tA = ld->par[1];
+    aP = ((kc * h) / (kc + h * dcca)) * area;
+    *sP += aP;
+    *p += aP * tA;
+    return 0;
+  case 2: /* NEUMANNBC */
+    if (ld->np < 1) return -1;
+    tA = ld->par[0];
+    *p += area * tA;
+    return 0;
+  case 4: /* SINBC: sin products of the face centre */
+    return -2;
+  case 6: /* INLET: par[0] value, par[1..3] velocity, par[4] density */
+    if (ld->var != 0) return -2;
+    if (ld->np < 5) return -1;
+    tA = ld->par[0];
+    rhoEnv = ld->par[4];
+    wfn = ld->par[1] * n[0] + ld->par[2] * n[1];
+    wfn += ld->par[3] * n[2];
+    *p -= wfn * rhoEnv * area * tA;
+    aP = kc * area / dcca;
+    *sP += aP;
+    *p += aP * tA;
+    return 0;
+  case 7: /* OUTLET reads the cell velocity, which the diffusion cell has not */
+    return -1;
+  }
+  return 0; /* other codes add nothing (pLoad's chain of tests falls through) */
+}
+
+/* the slot of column c in row r of a CSR pattern; writes every match as the
+ * reference's search loop does */
+static void dif_put(const int *ia, const int *ja, int r, int c, double *dst, double v)
+{
+  int k;
+  for (k = ia[r]; k < ia[r + 1]; k++)
+    if (ja[k] == c) dst[k] = v;
+}
+
+int orc_dif_assemble(const orc_dif_mesh *m, const orc_load *loads, int nloads,
+                     const orc_dif_opts *o, const double *density,
+                     const double *cdiff, const double *u0,
+                     const double *gradu0, int storage, int unsym, int neq,
+                     int nad, const int *ia, const int *ja, double *a,
+                     double *ad, double *b, double *rcell, int forces,
+                     int matrix, int calrcell)
+{
+  enum { MAXF = 32 };
+  const int mv = m->maxviz;
+  int nel, f, j, rc;
+  (void)neq;
+  if (mv < 1 || mv > MAXF - 1) return -1;
+  for (nel = 0; nel < m->numel; nel++) {
+    double lA[MAXF], ksi[3], nrm[3], s[3], e[3], t[3], gf[3], gc[3], v[3];
+    int viz[MAXF], lid[MAXF];
+    const int nf = m->nface[nel];
+    const short *fr = m->facer + (long)nel * (mv + 1);
+    double p = 0.0, sP = 0.0, r = 0.0, kc, rho, vol, lB;
+    int row;
+    if (calrcell) rcell[nel] = 0.0;
+    if (nf < 1 || nf > mv) return -1;
+    if (fr[nf] >= 1) continue; /* no equation in this cell */
+    if (m->caltype[m->mat[nel] - 1] != 1) return -1;
+    row = m->id[nel] - 1;
+    kc = cdiff[nel];
+    rho = density[nel];
+    vol = m->volume[nel];
+    for (f = 0; f < nf; f++) {
+      const long q = (long)nel * mv + f;
+      const int face = m->cellface[q] - 1;
+      const double ch = (m->owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+      const double mk = m->mksi[face], area = m->area[face];
+      const double *xmcc = m->xmcc + 3 * q;
+      viz[f] = m->nelcon[q] - 1;
+      lid[f] = viz[f] != -2 ? m->id[viz[f]] - 1 : -1;
+      for (j = 0; j < 3; j++) {
+        ksi[j] = ch * m->ksi[3 * face + j];
+        nrm[j] = ch * m->normal[3 * face + j];
+      }
+      if (viz[f] > -1) {
+        const int nb = viz[f];
+        double duDksi, alpha, am1, coef, modE, dfd, gfk, du;
+        duDksi = (u0[nb] - u0[nel]) / mk;
+        for (j = 0; j < 3; j++) s[j] = area * nrm[j];
+        if (dif_scheme(s, ksi, e, t, o->icod)) return -1;
+        /* interpolFace, INTPOLFACELINEAR (CellLib.c:7174-7200) */
+        for (j = 0; j < 3; j++) v[j] = m->vskew[3 * face + j] + xmcc[j];
+        alpha = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / mk;
+        am1 = 1.0 - alpha;
+        coef = alpha / kc + am1 / cdiff[nb];
+        coef = 1.0 / coef;
+        modE = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        dfd = coef * modE / mk;
+        for (j = 0; j < 3; j++) gf[j] = am1 * gradu0[3 * nel + j] + alpha * gradu0[3 * nb + j];
+        gfk = gf[0] * ksi[0] + gf[1] * ksi[1] + gf[2] * ksi[2];
+        du = duDksi - gfk;
+        for (j = 0; j < 3; j++) gc[j] = gf[j] + du * ksi[j];
+        gfk = gc[0] * t[0] + gc[1] * t[1] + gc[2] * t[2];
+        lA[f] = dfd;
+        p += coef * gfk;
+      } else {
+        lA[f] = 0.0;
+        if (fr[f]) {
+          const int l = fr[f] - 1;
+          if (l < 0 || l >= nloads) return -1;
+          rc = dif_load(&loads[l], &sP, &p, nrm, kc, area, m->dcca[q]);
+          if (rc) return rc;
+        }
+      }
+    }
+    /* implicit time term, CellDif.c:485-497 */
+    if (o->time_flag) {
+      if (o->time_type == 0)
+        sP += rho * vol / o->dt;
+      else if (o->time_type == 1) {
+        const double tmp = 1.e0 / o->dt + 1.e0 / (o->dt + o->dt0);
+        sP += tmp * rho * vol;
+      }
+    }
+    lA[nf] = sP;
+    for (f = 0; f < nf; f++) lA[nf] += lA[f];
+    for (f = 0; f < nf; f++)
+      if (viz[f] > -1) {
+        if (lid[f] == -2)
+          p += lA[f] * u0[viz[f]];
+        else
+          r += lA[f] * u0[viz[f]];
+      }
+    r += p - lA[nf] * u0[nel];
+    for (f = 0; f < nf; f++) lA[f] *= -1.e0;
+    lB = o->fres ? r : p;
+    if (calrcell) rcell[nel] = r;
+    /* csr() / ellPack(), ndf = 1 */
+    if (forces) b[row] = lB;
+    if (!matrix) continue;
+    ad[row] = lA[nf];
+    if (storage == ORC_ELLPACK) {
+      const int w = ia[0];
+      for (f = 0; f < nf; f++) a[(long)row * w + f] = lA[f];
+      continue;
+    }
+    for (f = 0; f < nf; f++) {
+      const int c = lid[f];
+      if (c <= -1) continue;
+      if (storage == ORC_CSRC && unsym) {
+        if (c < row)
+          dif_put(ia, ja, row, c, a, lA[f]);
+        else if (c > row)
+          dif_put(ia, ja, c, row, a + nad, lA[f]);
+      } else {
+        dif_put(ia, ja, row, c, a, lA[f]);
+      }
+    }
+  }
+  return 0;
+}

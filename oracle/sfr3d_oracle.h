@@ -64,4 +64,58 @@ int orc_gmres(int storage, int unsym, int neq, const int *ia, const int *ja,
               const double *al, const double *ad, const double *b, double *x,
               double tol, unsigned maxit, int newx, int nk, orc_stats *st);
 
+/* ---- diffusion system assembly (systFormDif, CellLoop.c:285-455) ------ */
+
+#define ORC_MAXLOADPAR 20 /* MAXLOADPARAMETER, Define.h:336 */
+
+/* The mesh arrays systFormDif reads (1-based indices as the reference
+ * stores them; MAT2D/MAT3D row-major). */
+typedef struct {
+  int numel, maxviz;
+  const int *nelcon;      /* numel*maxviz: neighbour + 1, -1 boundary */
+  const short *nface;     /* numel */
+  const int *cellface;    /* numel*maxviz: face + 1 */
+  const int *owner;       /* nface*2 */
+  const double *volume;   /* numel */
+  const double *dcca;     /* numel*maxviz */
+  const double *xmcc;     /* numel*maxviz*3 */
+  const double *mksi;     /* per face */
+  const double *ksi;      /* per face *3 */
+  const double *area;     /* per face */
+  const double *normal;   /* per face *3 */
+  const double *vskew;    /* per face *3 */
+  const short *caltype;   /* per material */
+  const short *mat;       /* numel, 1-based material */
+  const int *id;          /* numel: equation + 1 (0: none) */
+  const short *facer;     /* numel*(maxviz+1): load + 1 per face, then the cell */
+} orc_dif_mesh;
+
+/* The fields of Loads (StructDefine.h:356-366) that pLoad reads. */
+typedef struct {
+  int type, var, np;
+  double par[ORC_MAXLOADPAR];
+} orc_load;
+
+typedef struct {
+  int icod;              /* Diffusion.iCod: 1 orthogonal .. 4 over-relaxed */
+  int fres;              /* DiffModel.fRes */
+  int time_flag;         /* Temporal.flag */
+  int time_type;         /* 0 EULER, 1 BACKWARD */
+  double dt, dt0;        /* Temporal.dt[0], dt[1] */
+} orc_dif_opts;
+
+/* systFormDif with ndf = 1 and ndm = 3 on one process: writes a (al, or al
+ * then au for unsym CSRC; the neq x width slots for ELLPACK), ad, b and rcell
+ * as csr()/ellPack() (Csr.c:549-1022, EllPack.c:113-149) would.  Returns 0,
+ * -1 for input the reference cannot take (a material whose cell library is
+ * not diffusion, an unknown non-orthogonal scheme, an OUTLET load, a load
+ * with too few parameters), -2 for loads given as functions or SINBC. */
+int orc_dif_assemble(const orc_dif_mesh *m, const orc_load *loads, int nloads,
+                     const orc_dif_opts *o, const double *density,
+                     const double *cdiff, const double *u0,
+                     const double *gradu0, int storage, int unsym, int neq,
+                     int nad, const int *ia, const int *ja, double *a,
+                     double *ad, double *b, double *rcell, int forces,
+                     int matrix, int calrcell);
+
 #endif

@@ -1,0 +1,207 @@
+"""Device assembly of the diffusion system (host side of assembly.cu).
+
+The reference builds A and b on the host with systFormDif (CellLoop.c:285)
+-> cellDif3D (CellDif.c:312) and hands them to solverC.  Here a plan binds a
+mesh (the arrays systFormDif reads) to a resident ``GpuSystem`` once; each
+``assemble`` then writes the system's values on the GPU, where the next
+``solve_device`` reads them, and returns b and the cell residuals.  Results
+are bit-identical to the reference's systFormDif on the same inputs.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import solver as _sv
+
+# load types (Define.h:317-323), non-orthogonal schemes (Define.h:304-307),
+# time schemes (Define.h:191-192)
+DIRICHLET, NEUMANN, ROBIN, SINBC, INLET, OUTLET = 1, 2, 3, 4, 6, 7
+ORTHOGONAL, MINIMAL, ORTHOGONALC, OVERRELAXED = 1, 2, 3, 4
+EULER, BACKWARD = 0, 1
+MAXLOADPAR = 20   # MAXLOADPARAMETER, Define.h:336
+MAX_LOADS = 32
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+
+
+class DifMeshC(ctypes.Structure):
+    _fields_ = [("numel", _I32), ("maxviz", _I32), ("nfaces", ctypes.c_int64),
+                ("nmat", _I32), ("pad", _I32)] + [
+        (n, _P) for n in ("nelcon", "nviz", "cellface", "owner", "volume",
+                          "dcca", "xmcc", "mksi", "ksi", "area", "normal",
+                          "vskew", "caltype", "mat", "id", "facer")]
+
+
+class LoadC(ctypes.Structure):
+    _fields_ = [("type", _I32), ("var", _I32), ("np", _I32), ("pad", _I32),
+                ("par", ctypes.c_double * MAXLOADPAR)]
+
+
+class DifOptsC(ctypes.Structure):
+    _fields_ = [("icod", _I32), ("fres", _I32), ("time_flag", _I32),
+                ("time_type", _I32), ("dt", ctypes.c_double),
+                ("dt0", ctypes.c_double)]
+
+
+def _lib():
+    L = _sv.lib()
+    if not getattr(L, "_dif_typed", False):
+        L.sfr_gpu_dif_plan_create.argtypes = [_P, ctypes.POINTER(DifMeshC), _I32,
+                                              ctypes.POINTER(_P)]
+        L.sfr_gpu_dif_assemble.argtypes = ([_P, _P, _I32, ctypes.POINTER(DifOptsC)]
+                                           + [_P] * 7 + [_I32] * 3)
+        L.sfr_gpu_dif_assemble_device.argtypes = (
+            [_P, _P, _I32, ctypes.POINTER(DifOptsC)] + [_P] * 7 + [_I32] * 3 + [_P])
+        L.sfr_gpu_dif_update_cells.argtypes = [_P, _P, _P, _I32, _P]
+        L.sfr_gpu_dif_plan_destroy.argtypes = [_P]
+        L.sfr_gpu_get_values.argtypes = [_P, _P, _P, _P]
+        L._dif_typed = True
+    return L
+
+
+@dataclass
+class Load:
+    """One load (Loads, StructDefine.h:356): type, parameters, nTypeVar."""
+    type: int
+    par: tuple = ()
+    var: int = 0
+    np: int | None = None
+
+
+def _loads_c(loads):
+    if len(loads) > MAX_LOADS:
+        raise ValueError(f"at most {MAX_LOADS} loads")
+    arr = (LoadC * max(len(loads), 1))()
+    for i, ld in enumerate(loads):
+        arr[i].type = ld.type
+        arr[i].var = ld.var
+        arr[i].np = len(ld.par) if ld.np is None else ld.np
+        for j, v in enumerate(ld.par):
+            arr[i].par[j] = v
+    return arr
+
+
+def _c(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class DifPlan:
+    """A mesh bound to a resident system for device-side systFormDif.
+
+    ``mesh`` is any object with the attributes of
+    ``sfr3d_b200.systems.FvMesh`` (numel, nface, nelcon, nviz, cellface,
+    owner, volume, dcca, xmcc, mksi, ksi, area, normal, vskew, id).
+    ``facer`` is the reference's faceR, (numel, maxviz + 1) shorts.
+    ``caltype``/``mat`` default to one diffusion material.
+    """
+
+    def __init__(self, system: "_sv.GpuSystem", mesh, facer, icod: int = ORTHOGONAL,
+                 caltype=None, mat=None):
+        self.system = system
+        self.numel = int(mesh.numel)
+        self.neq = system.neq
+        self.icod = icod
+        cal = np.ones(1, np.int16) if caltype is None else _c(caltype, np.int16)
+        mt = np.ones(self.numel, np.int16) if mat is None else _c(mat, np.int16)
+        keep = dict(
+            nelcon=_c(mesh.nelcon, np.int32), nviz=_c(mesh.nviz, np.int16),
+            cellface=_c(mesh.cellface, np.int32), owner=_c(mesh.owner, np.int32),
+            volume=_c(mesh.volume, np.float64), dcca=_c(mesh.dcca, np.float64),
+            xmcc=_c(mesh.xmcc, np.float64), mksi=_c(mesh.mksi, np.float64),
+            ksi=_c(mesh.ksi, np.float64), area=_c(mesh.area, np.float64),
+            normal=_c(mesh.normal, np.float64), vskew=_c(mesh.vskew, np.float64),
+            caltype=cal, mat=mt, id=_c(mesh.id, np.int32), facer=_c(facer, np.int16))
+        m = DifMeshC(numel=self.numel, maxviz=int(keep["nelcon"].size // self.numel),
+                     nfaces=int(mesh.mksi.shape[0]), nmat=int(cal.size),
+                     **{k: _ptr(v) for k, v in keep.items()})
+        h = _P()
+        rc = _lib().sfr_gpu_dif_plan_create(system.h, ctypes.byref(m), icod,
+                                            ctypes.byref(h))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_dif_plan_create: " + _sv.last_error())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().sfr_gpu_dif_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _opts(self, fres, time):
+        o = DifOptsC(icod=self.icod, fres=int(fres))
+        if time is not None:
+            o.time_flag = 1
+            o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
+        return o
+
+    def assemble(self, loads, u0, cdiff, density=None, gradu0=None, b0=None,
+                 fres=True, time=None, forces=True, matrix=True, calrcell=True):
+        """One systFormDif call with host arrays: the matrix goes into the
+        system (marked as new values); returns (b, rcell) as numpy arrays
+        (None where not requested).  time = (type, dt, dt0) or None."""
+        u0, cdiff = _c(u0, np.float64), _c(cdiff, np.float64)
+        density, gradu0, b0 = (_c(density, np.float64), _c(gradu0, np.float64),
+                               _c(b0, np.float64))
+        b = np.empty(self.neq) if forces else None
+        rcell = np.empty(self.numel) if calrcell else None
+        loads_c = _loads_c(loads)
+        o = self._opts(fres, time)
+        rc = _lib().sfr_gpu_dif_assemble(
+            self.h, loads_c, len(loads), ctypes.byref(o), _ptr(density), _ptr(cdiff),
+            _ptr(u0), _ptr(gradu0), _ptr(b0), _ptr(b), _ptr(rcell), int(forces),
+            int(matrix), int(calrcell))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_dif_assemble: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
+        return b, rcell
+
+    def assemble_device(self, loads, d_u0: int, d_cdiff: int, d_density: int = 0,
+                        d_gradu0: int = 0, d_b0: int = 0, d_b: int = 0, d_rcell: int = 0,
+                        fres=True, time=None, forces=True, matrix=True, calrcell=True,
+                        stream: int = 0):
+        """The same on device pointers (plain integers), asynchronous on
+        `stream` (0: the system's stream)."""
+        loads_c = _loads_c(loads)
+        o = self._opts(fres, time)
+        rc = _lib().sfr_gpu_dif_assemble_device(
+            self.h, loads_c, len(loads), ctypes.byref(o), d_density or None, d_cdiff,
+            d_u0, d_gradu0 or None, d_b0 or None, d_b or None, d_rcell or None,
+            int(forces), int(matrix), int(calrcell), stream or None)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_dif_assemble_device: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
+
+    def update_cells(self, d_x: int, d_u: int, add: bool, stream: int = 0):
+        """u <- x (or u += x) over the cells, updateCellValue on the device."""
+        rc = _lib().sfr_gpu_dif_update_cells(self.h, d_x, d_u, int(add), stream or None)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_dif_update_cells")
+
+
+def get_values(system: "_sv.GpuSystem"):
+    """(al, ad, au) of the system in the reference's layout, copied back
+    (au is None unless the storage is unsym CSRC)."""
+    nsrc = system._nsrc()
+    split = system.storage == _sv.CSRC and system.unsym
+    al = np.empty(nsrc // 2 if split else nsrc)
+    au = np.empty(nsrc // 2) if split else None
+    ad = np.empty(system.neq)
+    rc = _lib().sfr_gpu_get_values(system.h, _ptr(al), _ptr(ad), _ptr(au))
+    if rc != _sv.OK:
+        raise _sv.SolverError(rc, "sfr_gpu_get_values: " + _sv.last_error())
+    return al, ad, au

@@ -28,7 +28,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["krylov.cu", "mixed.cu", "stream_solve.cu", "batched.cu", "device_mem.cu",
-                "noalloc.cu", "adjoint.cu", "resident.cu", "krylov_ext.cu"]
+                "noalloc.cu", "adjoint.cu", "resident.cu", "krylov_ext.cu",
+                "assembly.cu"]
 HOST_SOURCES = ["capi.cpp", "sell_build.cpp"]
 SYSTEM_SOURCES = ["systems.cpp"]
 

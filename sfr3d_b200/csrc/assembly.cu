@@ -1,0 +1,691 @@
+// Device assembly of the diffusion system: systFormDif (CellLoop.c:285-455)
+// -> cellDif3D (CellDif.c:312-537) -> csr()/ellPack() (Csr.c:549-1022,
+// EllPack.c:113-149), ndf = 1, ndm = 3, one process.
+//
+// Every cell writes exactly one row (its own), so the assembly is one thread
+// per equation with no atomics.  A plan binds the mesh to a system once:
+//   - cells are put in equation order, so that the per-call reads of the
+//     plan are coalesced and row r's outputs land at r;
+//   - what cellDif3D derives from the geometry alone (the owner-signed ksi
+//     and normal, the interpolation weight alpha of interpolFace, |E| of
+//     difusionSchemeNew and the explicit part t) is computed once, on the
+//     GPU, by the same IEEE operations in the same order, so that the
+//     per-call arithmetic starts from bit-identical values;
+//   - the destination of each coefficient in the reference's raw value array
+//     (al, al|au, or the ELLPACK slots) is resolved once from the system's
+//     own pattern.
+// A call then reads the plan (face-major, row-contiguous) and the per-cell
+// fields, and writes al|au, ad and b where solverC reads them; the system's
+// usual value refresh (the gather into its SELL copy) follows on the stream.
+// All products and sums use explicitly rounded intrinsics (no contraction),
+// in the reference's C evaluation order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace sfr {
+namespace {
+
+constexpr int kMaxViz = 8;        // face slots per cell handled
+constexpr int kGeo = 9;           // geometry fields per (face, row)
+constexpr int kMaxLoads = 32;     // entries of the load table
+constexpr int32_t kFlagP = 0x40000000;  // neighbour whose equation id is -1
+
+// plan-time error codes (first one wins)
+enum PlanError : int {
+  kErrNone = 0,
+  kErrNface = 1,
+  kErrLibrary = 2,
+  kErrId = 3,
+  kErrIdTwice = 4,
+  kErrFace = 5,
+  kErrNeighbour = 6,
+  kErrColumnTwice = 7,
+  kErrLoad = 8,
+  kErrWidth = 9,
+};
+
+const char *plan_error_text(int e) {
+  switch (e) {
+    case kErrNface: return "a cell's face count is outside 1..maxviz";
+    case kErrLibrary: return "a cell's material does not use the diffusion cell library (calType 1)";
+    case kErrId: return "an equation number is outside 1..neq";
+    case kErrIdTwice: return "two cells carry the same equation number";
+    case kErrFace: return "a cellFace entry or its owner is out of range";
+    case kErrNeighbour: return "a neighbour index is neither a cell nor -1 (boundary)";
+    case kErrColumnTwice: return "a row of the pattern holds the same column twice";
+    case kErrLoad: return "a boundary face names a load outside 1..32";
+    case kErrWidth: return "a cell has more faces than the ELLPACK row has slots";
+  }
+  return "unknown plan error";
+}
+
+struct MeshDev {
+  int32_t numel, maxviz, nmat;
+  int64_t nfaces;
+  const int32_t *nelcon, *cellface, *owner, *id;
+  const int16_t *nviz, *caltype, *mat, *facer;
+  const double *volume, *dcca, *xmcc, *mksi, *ksi, *area, *normal, *vskew;
+};
+
+struct PatternDev {
+  const int32_t *sptr, *col, *src;
+  int32_t n, storage, unsym, width;  // width: ELLPACK slots per row
+};
+
+struct PlanDev {
+  int32_t n, maxviz;
+  size_t fstride;       // maxviz * n: distance between geometry fields
+  int32_t *cell;        // [n] cell assembling row r, -1 none
+  int16_t *nface;       // [n]
+  int32_t *nb;          // [maxviz][n] neighbour cell (| kFlagP), -1 bare boundary, -(load+2)
+  int32_t *dst;         // [maxviz][n] raw value index, -1 none
+  double *geo;          // [kGeo][maxviz][n]
+  double *vol;          // [n]
+};
+
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return xadd(xadd(xmul(a[0], b[0]), xmul(a[1], b[1])), xmul(a[2], b[2]));
+}
+
+__device__ __forceinline__ void flag_error(int *err, int code) { atomicCAS(err, 0, code); }
+
+// difusionSchemeNew, ndm = 3 (CellLib.c:5824-6000)
+__device__ void dif_scheme(int icod, const double s[3], const double k[3], double e[3],
+                           double t[3]) {
+  if (icod == 1) {  // ORTHOGONAL
+    const double ss = xsqrt(dot3(s, s));
+    for (int j = 0; j < 3; ++j) {
+      e[j] = xmul(ss, k[j]);
+      t[j] = 0.0;
+    }
+    return;
+  }
+  double tmp;
+  if (icod == 2) {  // MINIMAL
+    tmp = dot3(s, k);
+  } else if (icod == 3) {  // ORTHOGONALC
+    tmp = xsqrt(dot3(s, s));
+  } else {  // OVERRELAXED
+    tmp = xdiv(dot3(s, s), dot3(s, k));
+  }
+  for (int j = 0; j < 3; ++j) e[j] = xmul(tmp, k[j]);
+  for (int j = 0; j < 3; ++j) t[j] = xsub(s[j], e[j]);
+}
+
+// column c of row r in the system's SELL copy -> index in the raw values;
+// -1 absent, -3 present twice
+__device__ int raw_index(const PatternDev &P, int r, int c) {
+  const int slice = r >> 5, lane = r & 31;
+  const int beg = P.sptr[slice];
+  const int w = (P.sptr[slice + 1] - beg) >> 5;
+  int found = -1, hits = 0;
+  for (int j = 0; j < w; ++j) {
+    const int e = beg + j * 32 + lane;
+    if (P.col[e] == c && P.src[e] >= 0) {
+      found = P.src[e];
+      ++hits;
+    }
+  }
+  return hits > 1 ? -3 : found;
+}
+
+__global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *err,
+                            unsigned *used_loads, int *free_cells) {
+  const int nel = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nel >= m.numel) return;
+  const int mv = m.maxviz;
+  const int nf = m.nviz[nel];
+  if (nf < 1 || nf > mv) return flag_error(err, kErrNface);
+  const int16_t *fr = m.facer + static_cast<size_t>(nel) * (mv + 1);
+  if (fr[nf] >= 1) {  // the cell's value is prescribed: no equation
+    atomicAdd(free_cells, 1);
+    return;
+  }
+  const int lm = m.mat[nel] - 1;
+  if (lm < 0 || lm >= m.nmat || m.caltype[lm] != 1) return flag_error(err, kErrLibrary);
+  const int row = m.id[nel] - 1;
+  if (row < 0 || row >= P.n) return flag_error(err, kErrId);
+  if (P.storage == SFR_ELLPACK && nf > P.width) return flag_error(err, kErrWidth);
+  if (atomicCAS(p.cell + row, -1, nel) != -1) return flag_error(err, kErrIdTwice);
+  p.nface[row] = static_cast<int16_t>(nf);
+  p.vol[row] = m.volume[nel];
+  const bool sym_lower = !P.unsym && P.storage != SFR_ELLPACK;
+  for (int f = 0; f < nf; ++f) {
+    const size_t q = static_cast<size_t>(nel) * mv + f;
+    const size_t o = static_cast<size_t>(f) * P.n + row;
+    const int64_t face = static_cast<int64_t>(m.cellface[q]) - 1;
+    if (face < 0 || face >= m.nfaces) return flag_error(err, kErrFace);
+    const double ch = (m.owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+    double ksi[3], nrm[3], g[kGeo];
+    for (int j = 0; j < 3; ++j) {
+      ksi[j] = xmul(ch, m.ksi[3 * face + j]);
+      nrm[j] = xmul(ch, m.normal[3 * face + j]);
+    }
+    const int viz = m.nelcon[q] - 1;
+    int32_t nbv, dst = -1;
+    if (viz > -1) {
+      if (viz >= m.numel) return flag_error(err, kErrNeighbour);
+      const double area = m.area[face], mk = m.mksi[face];
+      double s[3], e[3], t[3], v[3];
+      for (int j = 0; j < 3; ++j) s[j] = xmul(area, nrm[j]);
+      dif_scheme(icod, s, ksi, e, t);
+      // interpolFace, INTPOLFACELINEAR (CellLib.c:7174-7200)
+      for (int j = 0; j < 3; ++j) v[j] = xadd(m.vskew[3 * face + j], m.xmcc[3 * q + j]);
+      g[0] = xdiv(xsqrt(dot3(v, v)), mk);  // alpha
+      g[1] = xsqrt(dot3(e, e));             // |E|
+      g[2] = mk;
+      for (int j = 0; j < 3; ++j) {
+        g[3 + j] = ksi[j];
+        g[6 + j] = t[j];
+      }
+      const int lid = m.id[viz] - 1;
+      nbv = viz | (lid == -2 ? kFlagP : 0);
+      if (P.storage == SFR_ELLPACK) {
+        dst = row * P.width + f;
+      } else if (lid > -1 && !(sym_lower && lid > row)) {
+        dst = raw_index(P, row, lid);
+        if (dst == -3) return flag_error(err, kErrColumnTwice);
+      }
+    } else {
+      if (viz != -2) return flag_error(err, kErrNeighbour);
+      const int ld = fr[f];
+      if (ld < 0 || ld > kMaxLoads) return flag_error(err, kErrLoad);
+      if (ld > 0) atomicOr(used_loads, 1u << (ld - 1));
+      nbv = ld > 0 ? -(ld - 1) - 2 : -1;
+      g[0] = m.area[face];
+      g[1] = m.dcca[q];
+      g[2] = 0.0;
+      for (int j = 0; j < 3; ++j) {
+        g[3 + j] = nrm[j];
+        g[6 + j] = 0.0;
+      }
+      if (P.storage == SFR_ELLPACK) dst = row * P.width + f;
+    }
+    p.nb[o] = nbv;
+    p.dst[o] = dst;
+    for (int k = 0; k < kGeo; ++k) p.geo[k * p.fstride + o] = g[k];
+  }
+}
+
+struct DevLoad {
+  int32_t type;
+  int32_t pad;
+  double par[5];
+};
+
+struct CallOpts {
+  int fres, time_flag, time_type, forces, matrix, calrcell;
+  double dt, dt0;
+};
+
+// pLoad for constant loads (Loads.c:881-990)
+__device__ __forceinline__ void apply_load(const DevLoad &L, double kc, double area, double dcca,
+                                           const double n[3], double &sP, double &pp) {
+  switch (L.type) {
+    case 1: {  // DIRICHLETBC
+      const double aP = xdiv(xmul(kc, area), dcca);
+      sP = xadd(sP, aP);
+      pp = xadd(pp, xmul(aP, L.par[0]));
+      break;
+    }
+    case 3: {  // ROBINBC
+      const double h = L.par[0];
+      const double aP = xmul(xdiv(xmul(kc, h), xadd(kc, xmul(h, dcca))), area);
+      sP = xadd(sP, aP);
+      pp = xadd(pp, xmul(aP, L.par[1]));
+      break;
+    }
+    case 2:  // NEUMANNBC
+      pp = xadd(pp, xmul(area, L.par[0]));
+      break;
+    case 6: {  // INLET
+      const double tA = L.par[0];
+      double wfn = xadd(xmul(L.par[1], n[0]), xmul(L.par[2], n[1]));
+      wfn = xadd(wfn, xmul(L.par[3], n[2]));
+      pp = xsub(pp, xmul(xmul(xmul(wfn, L.par[4]), area), tA));
+      const double aP = xdiv(xmul(kc, area), dcca);
+      sP = xadd(sP, aP);
+      pp = xadd(pp, xmul(aP, tA));
+      break;
+    }
+    default:
+      break;  // codes pLoad does not test add nothing
+  }
+}
+
+// One row of cellDif3D.  kOrth: ORTHOGONAL scheme, whose explicit part t is
+// zero, so the non-orthogonal correction adds coef * (+-0) to a force that
+// can never be -0: it changes nothing for finite fields and is skipped
+// (gradu0 is not read).
+template <bool kOrth>
+__global__ void __launch_bounds__(256)
+    dif_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, CallOpts o,
+                        const double *__restrict__ density, const double *__restrict__ cdiff,
+                        const double *__restrict__ u0, const double *__restrict__ gradu0,
+                        const double *__restrict__ b0, double *__restrict__ stage,
+                        double *__restrict__ diag, double *__restrict__ b,
+                        double *__restrict__ rcell) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n) return;
+  const int cell = p.cell[r];
+  if (cell < 0) return;
+  const int nf = p.nface[r];
+  const double kc = cdiff[cell], uc = u0[cell];
+  double gp[3] = {0.0, 0.0, 0.0};
+  if (!kOrth)
+    for (int j = 0; j < 3; ++j) gp[j] = gradu0[3 * static_cast<size_t>(cell) + j];
+  double la[kMaxViz], un[kMaxViz];
+  int32_t nbs[kMaxViz];
+  double pp = 0.0, sP = 0.0;
+  const size_t fs = p.fstride;
+#pragma unroll
+  for (int f = 0; f < kMaxViz; ++f) {
+    la[f] = 0.0;
+    un[f] = 0.0;
+    nbs[f] = -1;
+    if (f < nf) {
+      const size_t q = static_cast<size_t>(f) * p.n + r;
+      const int32_t nb = __ldcs(p.nb + q);
+      nbs[f] = nb;
+      const double *g = p.geo + q;
+      if (nb >= 0) {
+        const int c = nb & (kFlagP - 1);
+        const double alpha = __ldcs(g), modE = __ldcs(g + fs), mk = __ldcs(g + 2 * fs);
+        const double am1 = xsub(1.0, alpha);
+        un[f] = u0[c];
+        double coef = xadd(xdiv(alpha, kc), xdiv(am1, cdiff[c]));
+        coef = xdiv(1.0, coef);
+        la[f] = xdiv(xmul(coef, modE), mk);
+        if (!kOrth) {
+          const double duDksi = xdiv(xsub(un[f], uc), mk);
+          double k[3], t[3], gf[3], gc[3];
+          for (int j = 0; j < 3; ++j) {
+            k[j] = __ldcs(g + (3 + j) * fs);
+            t[j] = __ldcs(g + (6 + j) * fs);
+            gf[j] = xadd(xmul(am1, gp[j]),
+                         xmul(alpha, gradu0[3 * static_cast<size_t>(c) + j]));
+          }
+          const double du = xsub(duDksi, dot3(gf, k));
+          for (int j = 0; j < 3; ++j) gc[j] = xadd(gf[j], xmul(du, k[j]));
+          pp = xadd(pp, xmul(coef, dot3(gc, t)));
+        }
+      } else if (nb <= -2) {
+        const double n[3] = {__ldcs(g + 3 * fs), __ldcs(g + 4 * fs), __ldcs(g + 5 * fs)};
+        apply_load(loads[-nb - 2], kc, __ldcs(g), __ldcs(g + fs), n, sP, pp);
+      }
+    }
+  }
+  // implicit time term, CellDif.c:485-497
+  if (o.time_flag) {
+    const double rho = density[cell], vol = p.vol[r];
+    if (o.time_type == 0) {
+      sP = xadd(sP, xdiv(xmul(rho, vol), o.dt));
+    } else if (o.time_type == 1) {
+      const double tmp = xadd(xdiv(1.0, o.dt), xdiv(1.0, xadd(o.dt, o.dt0)));
+      sP = xadd(sP, xmul(xmul(tmp, rho), vol));
+    }
+  }
+  double d = sP;
+#pragma unroll
+  for (int f = 0; f < kMaxViz; ++f)
+    if (f < nf) d = xadd(d, la[f]);
+  double rr = 0.0;
+#pragma unroll
+  for (int f = 0; f < kMaxViz; ++f)
+    if (f < nf && nbs[f] >= 0) {
+      if (nbs[f] & kFlagP)
+        pp = xadd(pp, xmul(la[f], un[f]));
+      else
+        rr = xadd(rr, xmul(la[f], un[f]));
+    }
+  rr = xadd(rr, xsub(pp, xmul(d, uc)));
+  const double bb = b0 ? b0[r] : 0.0;
+  if (o.forces) {
+    const double lb = o.fres ? rr : pp;
+    b[r] = b0 ? xadd(lb, bb) : lb;
+  }
+  if (o.calrcell) rcell[cell] = b0 ? xadd(rr, bb) : rr;
+  if (!o.matrix) return;
+  diag[r] = d;
+#pragma unroll
+  for (int f = 0; f < kMaxViz; ++f)
+    if (f < nf) {
+      const int32_t t = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+      if (t >= 0) stage[t] = xmul(la[f], -1.0);
+    }
+}
+
+__global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
+                                    double *u, int add) {
+  const int nel = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nel >= numel) return;
+  const int row = id[nel] - 1;
+  if (row > -1 && row < n) u[nel] = add ? xadd(u[nel], x[row]) : x[row];
+}
+
+template <typename T>
+cudaError_t upload(T **dst, const T *src, size_t count) {
+  *dst = nullptr;
+  if (count == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(dst, sizeof(T) * count);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+}  // namespace sfr
+
+struct sfr_dif_plan {
+  sfr_system *s = nullptr;
+  int32_t numel = 0, maxviz = 0, icod = 0;
+  int free_cells = 0;            // cells without an equation (their rcell is zeroed)
+  unsigned used_loads = 0;       // bit l: some boundary face names load l
+  sfr::PlanDev d{};
+  int32_t *d_id = nullptr;       // per cell: equation + 1 (updateCellValue)
+  sfr::DevLoad *d_loads = nullptr;
+  std::vector<sfr::DevLoad> loads_host;  // what d_loads holds
+  // host-array calls: device copies of the fields and results
+  double *h_fields = nullptr;    // density | cdiff | u0 | gradu0 (numel * 6)
+  double *h_b0 = nullptr, *h_b = nullptr, *h_rcell = nullptr;
+};
+
+namespace {
+
+#define SFR_CUA(expr)                                     \
+  do {                                                    \
+    cudaError_t e_ = (expr);                              \
+    if (e_ != cudaSuccess) {                              \
+      sfr::set_last_error(cudaGetErrorString(e_));        \
+      return SFR_CUDA_ERROR;                              \
+    }                                                     \
+  } while (0)
+
+int bad(const char *why) {
+  sfr::set_last_error(why);
+  return SFR_BAD_INPUT;
+}
+
+void free_plan_buffers(sfr_dif_plan *p) {
+  cudaFree(p->d.cell);
+  cudaFree(p->d.nface);
+  cudaFree(p->d.nb);
+  cudaFree(p->d.dst);
+  cudaFree(p->d.geo);
+  cudaFree(p->d.vol);
+  cudaFree(p->d_id);
+  cudaFree(p->d_loads);
+  cudaFree(p->h_fields);
+  cudaFree(p->h_b0);
+  cudaFree(p->h_b);
+  cudaFree(p->h_rcell);
+}
+
+// Check the loads the mesh uses against what pLoad accepts (Loads.c:881-990,
+// getLoads Loads.c:122-169) and stage them on the device.
+int stage_loads(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads, cudaStream_t st) {
+  if (nloads < 0 || nloads > sfr::kMaxLoads || (nloads > 0 && !loads))
+    return bad("nloads must be 0..32");
+  for (int l = 0; l < sfr::kMaxLoads; ++l) {
+    if (!(p->used_loads & (1u << l))) continue;
+    if (l >= nloads) return bad("a boundary face names a load beyond nloads");
+    const sfr_load &L = loads[l];
+    const bool needs_value = L.type == 1 || L.type == 2 || L.type == 6;
+    if ((L.type == 1 || L.type == 6) && L.var != 0) {
+      sfr::set_last_error("loads given as functions (nTypeVar 1) are not assembled on the device");
+      return SFR_UNSUPPORTED;
+    }
+    if (L.type == 4) {
+      sfr::set_last_error("SINBC loads are not assembled on the device");
+      return SFR_UNSUPPORTED;
+    }
+    if (L.type == 7) return bad("an OUTLET load reads a cell velocity the diffusion cell has not");
+    if (needs_value && L.np < 1) return bad("a load has no parameters");
+    if (L.type == 6 && L.np < 5) return bad("an INLET load needs 5 parameters");
+  }
+  std::vector<sfr::DevLoad> h(sfr::kMaxLoads);
+  for (int l = 0; l < nloads; ++l) {
+    h[l].type = loads[l].type;
+    for (int j = 0; j < 5; ++j) h[l].par[j] = loads[l].par[j];
+  }
+  if (std::memcmp(h.data(), p->loads_host.data(), sizeof(sfr::DevLoad) * h.size()) != 0) {
+    SFR_CUA(cudaMemcpyAsync(p->d_loads, h.data(), sizeof(sfr::DevLoad) * h.size(),
+                            cudaMemcpyHostToDevice, st));
+    SFR_CUA(cudaStreamSynchronize(st));  // h is a local
+    p->loads_host = h;
+  }
+  return SFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
+                            sfr_dif_plan **out) {
+  if (!s || !mesh || !out) return bad("NULL argument");
+  *out = nullptr;
+  const sfr_dif_mesh &m = *mesh;
+  if (icod < 1 || icod > 4) return bad("icod must be 1..4 (Define.h:304-307)");
+  if (m.numel < 1 || m.maxviz < 1 || m.maxviz > sfr::kMaxViz || m.nfaces < 1 || m.nmat < 1)
+    return bad("mesh sizes out of range (maxviz 1..8)");
+  const void *need[] = {m.nelcon, m.nviz, m.cellface, m.owner, m.volume, m.dcca, m.xmcc,
+                        m.mksi, m.ksi, m.area, m.normal, m.vskew, m.caltype, m.mat,
+                        m.id, m.facer};
+  for (const void *q : need)
+    if (!q) return bad("a mesh array is NULL");
+  if (static_cast<int64_t>(s->n) * m.maxviz > INT32_MAX) return bad("system too large");
+  for (int64_t f = 0; f < m.nfaces; ++f)
+    if (m.owner[2 * f] < 1 || m.owner[2 * f] > m.numel) return bad("a face owner is out of range");
+  SFR_CUA(cudaSetDevice(s->device));
+  auto *p = new sfr_dif_plan;
+  p->s = s;
+  p->numel = m.numel;
+  p->maxviz = m.maxviz;
+  p->icod = icod;
+  p->loads_host.assign(sfr::kMaxLoads, sfr::DevLoad{});
+  const int n = s->n;
+  const size_t slots = static_cast<size_t>(m.maxviz) * n;
+  sfr::MeshDev md{};
+  md.numel = m.numel;
+  md.maxviz = m.maxviz;
+  md.nmat = m.nmat;
+  md.nfaces = m.nfaces;
+  const size_t ne = m.numel, nv = ne * m.maxviz, nf = m.nfaces;
+  int rc = SFR_OK;
+  int *d_err = nullptr;
+  auto release_mesh = [&]() {
+    cudaFree(const_cast<int32_t *>(md.nelcon));
+    cudaFree(const_cast<int32_t *>(md.cellface));
+    cudaFree(const_cast<int32_t *>(md.owner));
+    cudaFree(const_cast<int32_t *>(md.id));
+    cudaFree(const_cast<int16_t *>(md.nviz));
+    cudaFree(const_cast<int16_t *>(md.caltype));
+    cudaFree(const_cast<int16_t *>(md.mat));
+    cudaFree(const_cast<int16_t *>(md.facer));
+    cudaFree(const_cast<double *>(md.volume));
+    cudaFree(const_cast<double *>(md.dcca));
+    cudaFree(const_cast<double *>(md.xmcc));
+    cudaFree(const_cast<double *>(md.mksi));
+    cudaFree(const_cast<double *>(md.ksi));
+    cudaFree(const_cast<double *>(md.area));
+    cudaFree(const_cast<double *>(md.normal));
+    cudaFree(const_cast<double *>(md.vskew));
+    cudaFree(d_err);
+  };
+  auto up = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == SFR_OK) {
+      sfr::set_last_error(cudaGetErrorString(e));
+      rc = SFR_CUDA_ERROR;
+    }
+  };
+  {
+    int32_t *t32;
+    int16_t *t16;
+    double *t64;
+    up(sfr::upload(&t32, m.nelcon, nv)); md.nelcon = t32;
+    up(sfr::upload(&t32, m.cellface, nv)); md.cellface = t32;
+    up(sfr::upload(&t32, m.owner, 2 * nf)); md.owner = t32;
+    up(sfr::upload(&t32, m.id, ne)); md.id = t32;
+    p->d_id = t32;  // kept by the plan for updateCellValue
+    up(sfr::upload(&t16, m.nviz, ne)); md.nviz = t16;
+    up(sfr::upload(&t16, m.caltype, static_cast<size_t>(m.nmat))); md.caltype = t16;
+    up(sfr::upload(&t16, m.mat, ne)); md.mat = t16;
+    up(sfr::upload(&t16, m.facer, ne * (m.maxviz + 1))); md.facer = t16;
+    up(sfr::upload(&t64, m.volume, ne)); md.volume = t64;
+    up(sfr::upload(&t64, m.dcca, nv)); md.dcca = t64;
+    up(sfr::upload(&t64, m.xmcc, 3 * nv)); md.xmcc = t64;
+    up(sfr::upload(&t64, m.mksi, nf)); md.mksi = t64;
+    up(sfr::upload(&t64, m.ksi, 3 * nf)); md.ksi = t64;
+    up(sfr::upload(&t64, m.area, nf)); md.area = t64;
+    up(sfr::upload(&t64, m.normal, 3 * nf)); md.normal = t64;
+    up(sfr::upload(&t64, m.vskew, 3 * nf)); md.vskew = t64;
+  }
+  sfr::PlanDev &d = p->d;
+  d.n = n;
+  d.maxviz = m.maxviz;
+  d.fstride = slots;
+  up(cudaMalloc(&d.cell, sizeof(int32_t) * n));
+  up(cudaMalloc(&d.nface, sizeof(int16_t) * n));
+  up(cudaMalloc(&d.nb, sizeof(int32_t) * slots));
+  up(cudaMalloc(&d.dst, sizeof(int32_t) * slots));
+  up(cudaMalloc(&d.geo, sizeof(double) * slots * sfr::kGeo));
+  up(cudaMalloc(&d.vol, sizeof(double) * n));
+  up(cudaMalloc(&p->d_loads, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
+  up(cudaMalloc(&d_err, sizeof(int) * 3));
+  if (rc == SFR_OK) {
+    up(cudaMemset(d.cell, 0xFF, sizeof(int32_t) * n));
+    up(cudaMemset(d.nface, 0, sizeof(int16_t) * n));
+    up(cudaMemset(d.nb, 0xFF, sizeof(int32_t) * slots));
+    up(cudaMemset(d.dst, 0xFF, sizeof(int32_t) * slots));
+    up(cudaMemset(p->d_loads, 0, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
+    up(cudaMemset(d_err, 0, sizeof(int) * 3));
+  }
+  if (rc == SFR_OK) {
+    sfr::PatternDev P{s->A.sptr, s->A.col, s->A.src, n, s->storage, s->unsym,
+                      s->storage == SFR_ELLPACK ? s->nsrc / std::max(n, 1) : 0};
+    const int blocks = (m.numel + 255) / 256;
+    sfr::plan_kernel<<<blocks, 256>>>(md, P, d, icod, d_err,
+                                      reinterpret_cast<unsigned *>(d_err + 1), d_err + 2);
+    up(cudaGetLastError());
+    int h[3] = {0, 0, 0};
+    up(cudaMemcpy(h, d_err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (rc == SFR_OK && h[0] != sfr::kErrNone) rc = bad(sfr::plan_error_text(h[0]));
+    p->used_loads = static_cast<unsigned>(h[1]);
+    p->free_cells = h[2];
+  }
+  md.id = nullptr;  // the plan's (freed with it)
+  release_mesh();
+  if (rc != SFR_OK) {
+    free_plan_buffers(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return SFR_OK;
+}
+
+int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
+                                const sfr_dif_opts *o, const double *d_density,
+                                const double *d_cdiff, const double *d_u0,
+                                const double *d_gradu0, const double *d_b0, double *d_b,
+                                double *d_rcell, int32_t forces, int32_t matrix,
+                                int32_t calrcell, void *stream) {
+  if (!p || !o) return bad("NULL argument");
+  if (o->icod != p->icod) return bad("opts.icod differs from the scheme the plan was built for");
+  if (!d_cdiff || !d_u0) return bad("cdiff and u0 are required");
+  if (o->icod != 1 && !d_gradu0) return bad("gradu0 is required by non-orthogonal schemes");
+  if (o->time_flag && !d_density) return bad("density is required by the time term");
+  if (forces && !d_b) return bad("forces set without b");
+  if (calrcell && !d_rcell) return bad("calrcell set without rcell");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  int rc = stage_loads(p, loads, nloads, st);
+  if (rc != SFR_OK) return rc;
+  if (calrcell && p->free_cells > 0)
+    SFR_CUA(cudaMemsetAsync(d_rcell, 0, sizeof(double) * p->numel, st));
+  sfr::CallOpts co{o->fres != 0, o->time_flag != 0, o->time_type, forces != 0, matrix != 0,
+                   calrcell != 0, o->dt, o->dt0};
+  const int blocks = (s->n + 255) / 256;
+  if (p->icod == 1)
+    sfr::dif_assemble_kernel<true><<<blocks, 256, 0, st>>>(
+        p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0, d_b0, s->d_stage,
+        s->d_diag, d_b, d_rcell);
+  else
+    sfr::dif_assemble_kernel<false><<<blocks, 256, 0, st>>>(
+        p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0, d_b0, s->d_stage,
+        s->d_diag, d_b, d_rcell);
+  SFR_CUA(cudaGetLastError());
+  if (matrix) return sfr::values_refreshed(s, st);
+  return SFR_OK;
+}
+
+int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
+                         const sfr_dif_opts *o, const double *density, const double *cdiff,
+                         const double *u0, const double *gradu0, const double *b0, double *b,
+                         double *rcell, int32_t forces, int32_t matrix, int32_t calrcell) {
+  if (!p || !o) return bad("NULL argument");
+  if (!cdiff || !u0) return bad("cdiff and u0 are required");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  const size_t ne = p->numel;
+  if (!p->h_fields) {
+    SFR_CUA(cudaMalloc(&p->h_fields, sizeof(double) * ne * 6));
+    SFR_CUA(cudaMalloc(&p->h_b0, sizeof(double) * s->n));
+    SFR_CUA(cudaMalloc(&p->h_b, sizeof(double) * s->n));
+    SFR_CUA(cudaMalloc(&p->h_rcell, sizeof(double) * ne));
+  }
+  cudaStream_t st = s->stream;
+  double *fd = p->h_fields;
+  double *d_density = fd, *d_cdiff = fd + ne, *d_u0 = fd + 2 * ne, *d_grad = fd + 3 * ne;
+  if (density)
+    SFR_CUA(cudaMemcpyAsync(d_density, density, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  SFR_CUA(cudaMemcpyAsync(d_cdiff, cdiff, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  SFR_CUA(cudaMemcpyAsync(d_u0, u0, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  if (gradu0)
+    SFR_CUA(cudaMemcpyAsync(d_grad, gradu0, sizeof(double) * ne * 3, cudaMemcpyHostToDevice, st));
+  if (b0)
+    SFR_CUA(cudaMemcpyAsync(p->h_b0, b0, sizeof(double) * s->n, cudaMemcpyHostToDevice, st));
+  int rc = sfr_gpu_dif_assemble_device(p, loads, nloads, o, density ? d_density : nullptr,
+                                       d_cdiff, d_u0, gradu0 ? d_grad : nullptr,
+                                       b0 ? p->h_b0 : nullptr, p->h_b, p->h_rcell, forces,
+                                       matrix, calrcell, st);
+  if (rc != SFR_OK) return rc;
+  if (forces && b)
+    SFR_CUA(cudaMemcpyAsync(b, p->h_b, sizeof(double) * s->n, cudaMemcpyDeviceToHost, st));
+  if (calrcell && rcell)
+    SFR_CUA(cudaMemcpyAsync(rcell, p->h_rcell, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
+  SFR_CUA(cudaStreamSynchronize(st));
+  return SFR_OK;
+}
+
+int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, int32_t add,
+                             void *stream) {
+  if (!p || !d_x || !d_u) return bad("NULL argument");
+  SFR_CUA(cudaSetDevice(p->s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : p->s->stream;
+  sfr::update_cells_kernel<<<(p->numel + 255) / 256, 256, 0, st>>>(p->d_id, p->numel, p->s->n,
+                                                                     d_x, d_u, add != 0);
+  SFR_CUA(cudaGetLastError());
+  return SFR_OK;
+}
+
+int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p) {
+  if (!p) return SFR_OK;
+  cudaSetDevice(p->s->device);
+  free_plan_buffers(p);
+  delete p;
+  return SFR_OK;
+}
+
+}  // extern "C"

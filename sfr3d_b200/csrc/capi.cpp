@@ -152,6 +152,31 @@ int sfr_gpu_create(int32_t neq, int32_t nad, const int32_t *ia, const int32_t *j
   return SFR_OK;
 }
 
+extern "C++" {
+namespace sfr {
+
+// After new raw values (d_stage) and diagonal (d_diag) are in place on `st`:
+// the SELL copies, the FP32 compensation and diagonal, and the epoch the
+// derived operators are keyed on.
+int values_refreshed(sfr_system *s, cudaStream_t st) {
+  int rc = gather_values(s, &s->A, st);
+  if (rc != SFR_OK) return rc;
+  rc = row_compensation(s, s->A, st);
+  if (rc != SFR_OK) return rc;
+  if (s->at_ready) {
+    rc = gather_values(s, &s->At, st);
+    if (rc != SFR_OK) return rc;
+  }
+  SFR_CU(convert_diag32(s->d_diag, s->d_diag32, s->n, st));
+  s->values_set = true;
+  ++s->values_epoch;
+  if (s->tview) s->tview->comp_stale = true;
+  return SFR_OK;
+}
+
+}  // namespace sfr
+}  // extern "C++"
+
 int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const double *au) {
   if (!s || !ad || (!al && s->nsrc > 0)) return SFR_BAD_INPUT;
   SFR_CU(cudaSetDevice(s->device));
@@ -166,19 +191,31 @@ int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const 
                            s->stream));
   }
   SFR_CU(cudaMemcpyAsync(s->d_diag, ad, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
-  int rc = sfr::gather_values(s, &s->A, s->stream);
+  const int rc = sfr::values_refreshed(s, s->stream);
   if (rc != SFR_OK) return rc;
-  rc = sfr::row_compensation(s, s->A, s->stream);
-  if (rc != SFR_OK) return rc;
-  if (s->at_ready) {
-    rc = sfr::gather_values(s, &s->At, s->stream);
-    if (rc != SFR_OK) return rc;
-  }
-  SFR_CU(sfr::convert_diag32(s->d_diag, s->d_diag32, s->n, s->stream));
   SFR_CU(cudaStreamSynchronize(s->stream));
-  s->values_set = true;
-  ++s->values_epoch;
-  if (s->tview) s->tview->comp_stale = true;
+  return SFR_OK;
+}
+
+int sfr_gpu_get_values(sfr_system *s, double *al, double *ad, double *au) {
+  if (!s) return SFR_BAD_INPUT;
+  if (!s->values_set) {
+    g_last_error = "no values were set or assembled";
+    return SFR_BAD_INPUT;
+  }
+  SFR_CU(cudaSetDevice(s->device));
+  const bool split = s->storage == SFR_CSRC && s->unsym;
+  const size_t first = split ? static_cast<size_t>(s->nsrc) / 2 : static_cast<size_t>(s->nsrc);
+  if (al && first > 0)
+    SFR_CU(cudaMemcpyAsync(al, s->d_stage, sizeof(double) * first, cudaMemcpyDeviceToHost,
+                           s->stream));
+  if (au && split)
+    SFR_CU(cudaMemcpyAsync(au, s->d_stage + first, sizeof(double) * first,
+                           cudaMemcpyDeviceToHost, s->stream));
+  if (ad)
+    SFR_CU(cudaMemcpyAsync(ad, s->d_diag, sizeof(double) * s->n, cudaMemcpyDeviceToHost,
+                           s->stream));
+  SFR_CU(cudaStreamSynchronize(s->stream));
   return SFR_OK;
 }
 

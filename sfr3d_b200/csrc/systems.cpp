@@ -90,6 +90,9 @@ struct System {
   std::vector<double> rhs;    // nrhs * neq
   std::vector<int32_t> eq_of_cell;
   int32_t nnz_full = 0, nnz_lower = 0, bandwidth = 0;
+  // the mesh itself, kept for the export in the reference's mesh arrays
+  std::vector<Vec3> node, centre;  // vertices; cell centres (natural cell id)
+  std::vector<double> volume, kappa;
 };
 
 // ---------------------------------------------------------------- RCM ----
@@ -199,6 +202,45 @@ inline int64_t node_id(int i, int j, int k, int nx, int ny) {
              (static_cast<int64_t>(j) + static_cast<int64_t>(ny + 1) * k);
 }
 
+// The four vertices of the face at node-plane `pl` of axis `ax` spanning the
+// cell (u, w) of the two other axes, ordered so that
+// 0.5 (v2 - v0) x (v3 - v1) points along +axis.
+void face_vertices(const std::vector<Vec3> &node, int nx, int ny, int ax, int pl, int u, int w,
+                   Vec3 v[4]) {
+  if (ax == 0) {  // x-face: i = pl, j = u, k = w
+    v[0] = node[node_id(pl, u, w, nx, ny)];
+    v[1] = node[node_id(pl, u + 1, w, nx, ny)];
+    v[2] = node[node_id(pl, u + 1, w + 1, nx, ny)];
+    v[3] = node[node_id(pl, u, w + 1, nx, ny)];
+  } else if (ax == 1) {  // y-face: j = pl, k = u, i = w
+    v[0] = node[node_id(w, pl, u, nx, ny)];
+    v[1] = node[node_id(w, pl, u + 1, nx, ny)];
+    v[2] = node[node_id(w + 1, pl, u + 1, nx, ny)];
+    v[3] = node[node_id(w + 1, pl, u, nx, ny)];
+  } else {  // z-face: k = pl, i = u, j = w
+    v[0] = node[node_id(u, w, pl, nx, ny)];
+    v[1] = node[node_id(u + 1, w, pl, nx, ny)];
+    v[2] = node[node_id(u + 1, w + 1, pl, nx, ny)];
+    v[3] = node[node_id(u, w + 1, pl, nx, ny)];
+  }
+}
+
+// the cell on the + side of node-plane pl (index pl along ax)
+inline int32_t plus_cell(int nx, int ny, int ax, int pl, int u, int w) {
+  int i, j, k;
+  if (ax == 0) { i = pl; j = u; k = w; }
+  else if (ax == 1) { j = pl; k = u; i = w; }
+  else { k = pl; i = u; j = w; }
+  return i + nx * (j + ny * k);
+}
+
+// extents (u, w) of the faces of axis ax
+inline void face_span(int nx, int ny, int nz, int ax, int *nu, int *nw) {
+  if (ax == 0) { *nu = ny; *nw = nz; }
+  else if (ax == 1) { *nu = nz; *nw = nx; }
+  else { *nu = nx; *nw = ny; }
+}
+
 bool valid(const sfr_sys_params &p) {
   if (p.kind != SFR_SYS_DIFFUSION && p.kind != SFR_SYS_CONVDIFF) return false;
   if (p.nx < 1 || p.ny < 1 || p.nz < 1) return false;
@@ -281,25 +323,10 @@ System *build(const sfr_sys_params &p) {
   // face geometry of the face at node-plane `pl` of axis `ax` spanning the
   // cell (u, w) of the two other axes; area vector points along +axis
   auto face = [&](int ax, int pl, int u, int w, Vec3 *S, Vec3 *xf) {
-    Vec3 n0, n1, n2, n3;
-    if (ax == 0) {  // x-face: i = pl, j = u, k = w
-      n0 = node[node_id(pl, u, w, nx, ny)];
-      n1 = node[node_id(pl, u + 1, w, nx, ny)];
-      n2 = node[node_id(pl, u + 1, w + 1, nx, ny)];
-      n3 = node[node_id(pl, u, w + 1, nx, ny)];
-    } else if (ax == 1) {  // y-face: j = pl, k = u, i = w
-      n0 = node[node_id(w, pl, u, nx, ny)];
-      n1 = node[node_id(w, pl, u + 1, nx, ny)];
-      n2 = node[node_id(w + 1, pl, u + 1, nx, ny)];
-      n3 = node[node_id(w + 1, pl, u, nx, ny)];
-    } else {  // z-face: k = pl, i = u, j = w
-      n0 = node[node_id(u, w, pl, nx, ny)];
-      n1 = node[node_id(u + 1, w, pl, nx, ny)];
-      n2 = node[node_id(u + 1, w + 1, pl, nx, ny)];
-      n3 = node[node_id(u, w + 1, pl, nx, ny)];
-    }
-    *S = 0.5 * cross(n2 - n0, n3 - n1);
-    *xf = 0.25 * (n0 + n1 + n2 + n3);
+    Vec3 v[4];
+    face_vertices(node, nx, ny, ax, pl, u, w, v);
+    *S = 0.5 * cross(v[2] - v[0], v[3] - v[1]);
+    *xf = 0.25 * (v[0] + v[1] + v[2] + v[3]);
   };
 
   // convective face flux in +axis direction for unit velocity scale, from the
@@ -320,18 +347,9 @@ System *build(const sfr_sys_params &p) {
 
   const int dims[3] = {nx, ny, nz};
   auto cell_of = [&](int ax, int pl, int u, int w) -> int32_t {
-    // the cell on the + side of node-plane pl (index pl along ax)
-    int i, j, k;
-    if (ax == 0) { i = pl; j = u; k = w; }
-    else if (ax == 1) { j = pl; k = u; i = w; }
-    else { k = pl; i = u; j = w; }
-    return i + nx * (j + ny * k);
+    return plus_cell(nx, ny, ax, pl, u, w);
   };
-  auto span = [&](int ax, int *nu, int *nw) {
-    if (ax == 0) { *nu = ny; *nw = nz; }
-    else if (ax == 1) { *nu = nz; *nw = nx; }
-    else { *nu = nx; *nw = ny; }
-  };
+  auto span = [&](int ax, int *nu, int *nw) { face_span(nx, ny, nz, ax, nu, nw); };
 
   // Peclet scaling: U = peclet / max_f(|F_unit| / D_f) over interior faces
   double U = 0.0;
@@ -473,7 +491,95 @@ System *build(const sfr_sys_params &p) {
   s->rhs.resize(static_cast<size_t>(p.nrhs) * ncell);
   Rng rng_b(p.seed ^ 0xA54FF53A5F1D36F1ULL);
   for (auto &v : s->rhs) v = p.rhs_normal ? rng_b.normal() : rng_b.uniform(-1.0, 1.0);
+  s->node = std::move(node);
+  s->centre = std::move(centre);
+  s->volume = std::move(volume);
+  s->kappa = std::move(kappa);
   return s;
+}
+
+int64_t face_count(const sfr_sys_params &p) {
+  return static_cast<int64_t>(p.nx + 1) * p.ny * p.nz + static_cast<int64_t>(p.ny + 1) * p.nz * p.nx +
+         static_cast<int64_t>(p.nz + 1) * p.nx * p.ny;
+}
+
+inline Vec3 unit(Vec3 a) { return (1.0 / norm(a)) * a; }
+
+// The box as the reference's mesh arrays (the inputs of systFormDif,
+// CellLoop.c:285-311).  Faces are numbered axis by axis, node-plane by
+// node-plane, in the order build() visits them.  The owner of a face is its
+// minus-side cell (the plus-side cell for a face on a minus boundary); the
+// face vectors point out of the owner, and a cell that is not the owner takes
+// them negated (OWNER, CellLoop.c:376-388).
+void export_mesh(const System &s, const sfr_sys_mesh_t &m) {
+  const int nx = s.p.nx, ny = s.p.ny, nz = s.p.nz;
+  const int32_t ncell = nx * ny * nz;
+  const int dims[3] = {nx, ny, nz};
+  for (int32_t c = 0; c < ncell; ++c) {
+    m.nviz[c] = kFaces;
+    m.volume[c] = s.volume[c];
+    m.cdiff[c] = s.kappa[c];
+    m.id[c] = s.eq_of_cell[c] + 1;
+  }
+  int64_t f = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    int nu, nw;
+    face_span(nx, ny, nz, ax, &nu, &nw);
+    for (int pl = 0; pl <= dims[ax]; ++pl)
+      for (int w = 0; w < nw; ++w)
+        for (int u = 0; u < nu; ++u, ++f) {
+          Vec3 v[4];
+          face_vertices(s.node, nx, ny, ax, pl, u, w, v);
+          const Vec3 S = 0.5 * cross(v[2] - v[0], v[3] - v[1]);
+          const Vec3 xm = 0.25 * (v[0] + v[1] + v[2] + v[3]);
+          const bool has_minus = pl > 0, has_plus = pl < dims[ax];
+          const int32_t cm = has_minus ? plus_cell(nx, ny, ax, pl - 1, u, w) : -1;
+          const int32_t cp = has_plus ? plus_cell(nx, ny, ax, pl, u, w) : -1;
+          const int32_t own = has_minus ? cm : cp;
+          const int32_t nbr = has_minus && has_plus ? cp : -1;
+          const double area = norm(S);
+          const Vec3 n = (has_minus ? 1.0 / area : -1.0 / area) * S;  // out of the owner
+          const Vec3 cP = s.centre[own];
+          const Vec3 d = nbr >= 0 ? s.centre[nbr] - cP : xm - cP;
+          const double mksi = norm(d);
+          const Vec3 ksi = (1.0 / mksi) * d;
+          Vec3 skew{0, 0, 0};
+          if (nbr >= 0) {
+            // where the line of the centres crosses the plane of the face
+            const double lam = dot(xm - cP, n) / dot(ksi, n);
+            skew = (cP + lam * ksi) - xm;
+          }
+          const Vec3 eta = unit(v[1] - v[0]);
+          m.owner[2 * f] = own + 1;
+          m.owner[2 * f + 1] = nbr >= 0 ? nbr + 1 : -1;
+          m.mksi[f] = mksi;
+          m.area[f] = area;
+          m.mvskew[f] = norm(skew);
+          const Vec3 *vec[5] = {&ksi, &eta, &n, &xm, &skew};
+          double *dst[5] = {m.ksi, m.eta, m.normal, m.xm, m.vskew};
+          for (int q = 0; q < 5; ++q) {
+            dst[q][3 * f] = vec[q]->x;
+            dst[q][3 * f + 1] = vec[q]->y;
+            dst[q][3 * f + 2] = vec[q]->z;
+          }
+          // the face in its cells' face slots: 2*ax + 1 in the minus cell, 2*ax in the plus cell
+          const int32_t cells[2] = {cm, cp};
+          const int slots[2] = {2 * ax + 1, 2 * ax};
+          for (int q = 0; q < 2; ++q) {
+            const int32_t c = cells[q];
+            if (c < 0) continue;
+            const size_t e = static_cast<size_t>(c) * kFaces + slots[q];
+            const int32_t other = cells[q ^ 1];
+            m.nelcon[e] = other >= 0 ? other + 1 : -1;
+            m.cellface[e] = static_cast<int32_t>(f + 1);
+            const Vec3 xmcc = xm - s.centre[c];
+            m.xmcc[3 * e] = xmcc.x;
+            m.xmcc[3 * e + 1] = xmcc.y;
+            m.xmcc[3 * e + 2] = xmcc.z;
+            m.dcca[e] = std::fabs(dot(xmcc, n));
+          }
+        }
+  }
 }
 
 // sorted (col, face) pairs of one row
@@ -600,6 +706,29 @@ int sfr_sys_numbering(const void *h, int32_t *eq_of_cell) {
   if (!h || !eq_of_cell) return -1;
   const auto &s = *static_cast<const System *>(h);
   std::copy(s.eq_of_cell.begin(), s.eq_of_cell.end(), eq_of_cell);
+  return 0;
+}
+
+int sfr_sys_mesh_sizes(const void *h, int32_t *numel, int64_t *nface) {
+  if (!h || !numel || !nface) return -1;
+  const auto &s = *static_cast<const System *>(h);
+  *numel = s.neq;
+  *nface = face_count(s.p);
+  return 0;
+}
+
+int sfr_sys_mesh(const void *h, const sfr_sys_mesh_t *m) {
+  if (!h || !m) return -1;
+  const void *need[] = {m->nelcon, m->nviz, m->cellface, m->volume, m->dcca, m->xmcc,
+                        m->cdiff, m->id, m->owner, m->mksi, m->ksi, m->eta, m->area,
+                        m->normal, m->xm, m->mvskew, m->vskew};
+  for (const void *q : need)
+    if (!q) return -1;
+  try {
+    export_mesh(*static_cast<const System *>(h), *m);
+  } catch (...) {
+    return -1;
+  }
   return 0;
 }
 

@@ -63,6 +63,13 @@ class SysInfo(ctypes.Structure):
     ]
 
 
+class SysMesh(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in (
+        "nelcon", "nviz", "cellface", "volume", "dcca", "xmcc", "cdiff", "id",
+        "owner", "mksi", "ksi", "eta", "area", "normal", "xm", "mvskew",
+        "vskew")]
+
+
 _P = ctypes.c_void_p
 
 
@@ -79,6 +86,8 @@ def _lib():
                         ("sfr_sys_rhs", 1), ("sfr_sys_numbering", 1)):
             getattr(lib, name).argtypes = [_P] + [_P] * n
             getattr(lib, name).restype = ctypes.c_int
+        lib.sfr_sys_mesh_sizes.argtypes = [_P, _P, _P]
+        lib.sfr_sys_mesh.argtypes = [_P, ctypes.POINTER(SysMesh)]
         lib.sfr_rcm.argtypes = [ctypes.c_int32, _P, _P, _P]
         lib.sfr_sys_batch_params.argtypes = [
             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64,
@@ -89,6 +98,46 @@ def _lib():
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+MAX_VIZ = 6  # face slots per hexahedral cell: x-, x+, y-, y+, z-, z+
+
+
+@dataclass
+class FvMesh:
+    """The box in the reference's mesh arrays (the geometry inputs of
+    systFormDif, CellLoop.c:285-311): 1-based indices, cell arrays by natural
+    cell id, maxViz = 6.  Shapes: nelcon/cellface/dcca (numel, 6),
+    xmcc (numel, 6, 3), owner (nface, 2), the face vectors (nface, 3)."""
+    numel: int
+    nface: int
+    nelcon: np.ndarray
+    nviz: np.ndarray
+    cellface: np.ndarray
+    volume: np.ndarray
+    dcca: np.ndarray
+    xmcc: np.ndarray
+    cdiff: np.ndarray
+    id: np.ndarray
+    owner: np.ndarray
+    mksi: np.ndarray
+    ksi: np.ndarray
+    eta: np.ndarray
+    area: np.ndarray
+    normal: np.ndarray
+    xm: np.ndarray
+    mvskew: np.ndarray
+    vskew: np.ndarray
+
+    def face_r(self, side_load) -> np.ndarray:
+        """faceR (numel, maxViz + 1), short: load number + 1 (0 = none) of
+        each boundary face from a per-side table (x-, x+, y-, y+, z-, z+),
+        and 0 in the cell's own entry (every cell carries an equation)."""
+        side = np.asarray(side_load, np.int16)
+        fr = np.zeros((self.numel, MAX_VIZ + 1), np.int16)
+        bnd = self.nelcon == -1
+        fr[:, :MAX_VIZ] = np.where(bnd, side[None, :], 0)
+        return fr
 
 
 @dataclass
@@ -158,6 +207,31 @@ class FvSystem:
         e = np.empty(self.neq, np.int32)
         _check(_lib().sfr_sys_numbering(self._need(), _ptr(e)))
         return e
+
+    def mesh(self) -> FvMesh:
+        """The mesh the system was built on, in the reference's arrays."""
+        if "mesh" not in self._cache:
+            numel = ctypes.c_int32()
+            nface = ctypes.c_int64()
+            lib = _lib()
+            _check(lib.sfr_sys_mesh_sizes(self._need(), ctypes.byref(numel),
+                                          ctypes.byref(nface)))
+            ne, nf = numel.value, nface.value
+            m = FvMesh(
+                numel=ne, nface=nf,
+                nelcon=np.empty((ne, MAX_VIZ), np.int32),
+                nviz=np.empty(ne, np.int16),
+                cellface=np.empty((ne, MAX_VIZ), np.int32),
+                volume=np.empty(ne), dcca=np.empty((ne, MAX_VIZ)),
+                xmcc=np.empty((ne, MAX_VIZ, 3)), cdiff=np.empty(ne),
+                id=np.empty(ne, np.int32), owner=np.empty((nf, 2), np.int32),
+                mksi=np.empty(nf), ksi=np.empty((nf, 3)), eta=np.empty((nf, 3)),
+                area=np.empty(nf), normal=np.empty((nf, 3)), xm=np.empty((nf, 3)),
+                mvskew=np.empty(nf), vskew=np.empty((nf, 3)))
+            st = SysMesh(**{name: _ptr(getattr(m, name)) for name, _ in SysMesh._fields_})
+            _check(lib.sfr_sys_mesh(self._need(), ctypes.byref(st)))
+            self._cache["mesh"] = m
+        return self._cache["mesh"]
 
     def release(self):
         """Free the native copy (the CSRD arrays stay)."""

@@ -47,3 +47,63 @@ def transpose_csrd(neq, ia, ja, al):
     np.add.at(t_ia, t_rows + 1, 1)
     t_ia = np.cumsum(t_ia).astype(np.int32)
     return t_ia, t_cols.astype(np.int32), t_val
+
+
+class _Bag:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def dif_fixture():
+    """tests/golden/dif_assembly.npz as (mesh, fields, loads, layouts, cases):
+    mesh an object with the FvMesh attributes, fields a dict of the per-cell
+    arrays, loads a list of oracle.Load, layouts {name: (storage, unsym, ia,
+    ja, neq)}, cases a list of dicts (name, layout, icod, fres, time, forces,
+    matrix, calrcell, a, ad, b, rcell)."""
+    import os
+    from oracle import oracle as O
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "dif_assembly.npz")
+    z = np.load(path)
+    mk = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith("mesh/")}
+    facer = mk.pop("facer")
+    numel = len(mk["nviz"])
+    mesh = _Bag(numel=numel, nface=len(mk["mksi"]), **mk)
+    fields = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith("field/")}
+    loads = []
+    for i in range(len(z["loads/type"])):
+        loads.append(O.Load(int(z["loads/type"][i]), tuple(z["loads/par"][i][:int(z["loads/np"][i])]),
+                            var=int(z["loads/var"][i]), np=int(z["loads/np"][i])))
+    lays = {}
+    for k in z.files:
+        if k.startswith("layout/") and k.endswith("/meta"):
+            name = k.split("/")[1]
+            st, un, neq = (int(v) for v in z[k])
+            lays[name] = (st, bool(un), z[f"layout/{name}/ia"], z[f"layout/{name}/ja"], neq)
+    cases = []
+    for name in z["cases"]:
+        name = str(name)
+        icod, fres, tf, tt, forces, matrix, calr = (int(v) for v in z[f"{name}/meta"])
+        dt, dt0 = (float(v) for v in z[f"{name}/time"])
+        cases.append(dict(name=name, layout=str(z[f"{name}/layout"]), icod=icod,
+                          fres=bool(fres), time=(tt, dt, dt0) if tf else None,
+                          forces=bool(forces), matrix=bool(matrix), calrcell=bool(calr),
+                          a=z[f"{name}/a"], ad=z[f"{name}/ad"], b=z[f"{name}/b"],
+                          rcell=z[f"{name}/rcell"]))
+    return mesh, facer, fields, loads, lays, cases
+
+
+def dif_case(mesh, facer, fields, loads, c):
+    """An oracle.DifCase for one fixture case dict (or any dict with icod,
+    fres and time)."""
+    from oracle import oracle as O
+    t = c["time"]
+    return O.DifCase(mesh=mesh, facer=facer, loads=loads, icod=c["icod"], fres=c["fres"],
+                     time_flag=t is not None, time_type=t[0] if t else 0,
+                     dt=t[1] if t else 1.0, dt0=t[2] if t else 1.0, **fields)
+
+
+def bits_equal(a, b) -> bool:
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))

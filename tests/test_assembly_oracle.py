@@ -1,0 +1,110 @@
+"""The diffusion assembly oracle (systFormDif restated in C) against the
+reference's own compiled systFormDif: the committed fixture always, and
+live when oracle/_ref is built.  No GPU."""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sfr3d_b200 import systems as S
+from helpers import bits_equal, dif_case, dif_fixture, layouts
+
+
+def test_oracle_matches_reference_fixture():
+    mesh, facer, fields, loads, lays, cases = dif_fixture()
+    assert len(cases) >= 20
+    for c in cases:
+        st, un, ia, ja, neq = lays[c["layout"]]
+        rc, a, ad, b, rcell = O.dif_assemble(dif_case(mesh, facer, fields, loads, c), st, un,
+                                             ia, ja, neq, c["forces"], c["matrix"],
+                                             c["calrcell"], fill=0.0)
+        assert rc == 0, c["name"]
+        for got, want, what in ((a, c["a"], "a"), (ad, c["ad"], "ad"), (b, c["b"], "b"),
+                                (rcell, c["rcell"], "rcell")):
+            assert bits_equal(got, want), (c["name"], what)
+
+
+def _random_case(m, rng, icod, fres, time):
+    return O.DifCase(
+        mesh=m, facer=m.face_r([1, 4, 2, 6, 3, 0]),
+        loads=[O.Load(O.DIRICHLET, (0.5,)), O.Load(O.NEUMANN, (0.25,)),
+               O.Load(O.ROBIN, (2.0, 1.5)), O.Load(9, (1.0,)), O.Load(0, ()),
+               O.Load(O.INLET, (1.0, 0.3, -0.2, 0.1, 1.2))],
+        density=rng.uniform(0.5, 2, m.numel), cdiff=m.cdiff * rng.uniform(0.5, 2, m.numel),
+        u0=rng.standard_normal(m.numel), gradu0=rng.standard_normal((m.numel, 3)),
+        icod=icod, fres=fres, time_flag=time is not None,
+        time_type=time[0] if time else 0, dt=0.1, dt0=0.05)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_oracle_matches_reference_live():
+    s = S.poisson_jittered(5, seed=4)
+    m = s.mesh()
+    rng = np.random.default_rng(2)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    n = 0
+    for icod, time, fres, flags in itertools.product(
+            (1, 2, 3, 4), (None, (O.EULER,), (O.BACKWARD,)), (False, True),
+            ((1, 1, 1), (1, 0, 0), (0, 1, 1))):
+        case = _random_case(m, rng, icod, fres, time)
+        for name, (st, un, ia, ja, _al, _au) in lay.items():
+            r1 = O.dif_assemble(case, st, un, ia, ja, s.neq, *flags, fill=7.0)
+            r2 = O.ref_dif_assemble(case, st, un, ia, ja, s.neq, *flags, fill=7.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:5]):
+                assert bits_equal(x, y), (icod, time, fres, flags, name)
+            n += 1
+    assert n == 4 * 3 * 2 * 3 * len(lay)
+
+
+def test_oracle_error_paths():
+    s = S.poisson_uniform(4, seed=1)
+    m = s.mesh()
+    base = dict(mesh=m, facer=m.face_r([1, 0, 0, 0, 0, 0]), density=np.ones(m.numel),
+                cdiff=m.cdiff, u0=np.zeros(m.numel), gradu0=np.zeros((m.numel, 3)))
+    run = lambda **kw: O.dif_assemble(O.DifCase(**{**base, **kw}), O.CSRD, True,  # noqa: E731
+                                      s.ia, s.ja, s.neq)[0]
+    assert run(loads=[O.Load(O.DIRICHLET, (1.0,))]) == 0
+    assert run(loads=[O.Load(O.SINBC, (1.0,) * 9)]) == -2       # sin of the face centre
+    assert run(loads=[O.Load(O.DIRICHLET, (1.0,), var=1)]) == -2  # a function
+    assert run(loads=[O.Load(O.OUTLET, ())]) == -1              # needs a velocity
+    assert run(loads=[O.Load(O.DIRICHLET, (1.0,))], icod=5) == -1  # the reference exits
+    assert run(loads=[O.Load(O.DIRICHLET, (1.0,))], caltype=np.array([2], np.int16)) == -1
+
+
+def test_mesh_export_geometry():
+    s = S.poisson_jittered(6, seed=3)
+    m = s.mesh()
+    assert m.nface == 3 * 6 * 6 * 7
+    # outward area vectors of every cell close
+    fid = m.cellface - 1
+    ch = np.where(m.owner[fid, 0] - 1 == np.arange(m.numel)[:, None], 1.0, -1.0)
+    tot = (ch[..., None] * m.area[fid][..., None] * m.normal[fid]).sum(axis=1)
+    assert abs(tot).max() < 1e-14
+    # face neighbours = the system's pattern, in equation numbers
+    eq = m.id - 1
+    for c in range(m.numel):
+        r = eq[c]
+        nb = m.nelcon[c][m.nelcon[c] > 0] - 1
+        assert sorted(eq[nb]) == sorted(s.ja[s.ia[r]:s.ia[r + 1]])
+    # ksi is a unit vector pointing from the owner towards the neighbour
+    assert np.allclose(np.linalg.norm(m.ksi, axis=1), 1.0)
+    assert (np.einsum("ij,ij->i", m.ksi, m.normal) > 0).all()
+    # the ELLPACK layout of the system is in the same face order
+    ja, _ = s.ell()
+    ja = ja.reshape(s.neq, s.width)
+    for c in range(0, m.numel, 7):
+        for f in range(6):
+            want = eq[m.nelcon[c, f] - 1] if m.nelcon[c, f] > 0 else eq[c]
+            assert ja[eq[c], f] == want
+
+
+def test_dif_plan_rejects_too_many_loads():
+    from sfr3d_b200 import assembly as A
+    with pytest.raises(ValueError):
+        A._loads_c([A.Load(A.NEUMANN, (0.0,))] * 33)

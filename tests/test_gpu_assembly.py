@@ -1,0 +1,231 @@
+"""Device assembly of the diffusion system against the reference's
+systFormDif: the committed fixture (made by the reference's own compiled
+code) and the oracle restatement, bit for bit, then the assembled system
+solved on the device."""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sfr3d_b200 import assembly as A
+from sfr3d_b200 import solver as sv
+from sfr3d_b200 import systems as S
+from helpers import bits_equal, dif_case, dif_fixture, layouts, rel
+
+pytestmark = pytest.mark.gpu
+
+LOADS = [O.Load(O.DIRICHLET, (0.5,)), O.Load(O.NEUMANN, (0.25,)), O.Load(O.ROBIN, (2.0, 1.5)),
+         O.Load(9, (1.0,)), O.Load(0, ()), O.Load(O.INLET, (1.0, 0.3, -0.2, 0.1, 1.2))]
+SIDES = [1, 4, 2, 6, 3, 0]
+
+
+def _loads(loads):
+    return [A.Load(ld.type, tuple(ld.par), var=ld.var, np=ld.np) for ld in loads]
+
+
+def _time(case):
+    return (case.time_type, case.dt, case.dt0) if case.time_flag else None
+
+
+def _device_assemble(gs, plan, case, flags, fill=0.0):
+    """Assemble on the device with host arrays; read back (a, ad, b, rcell)
+    in the reference's layout.  The values start from `fill` so that
+    entries the reference leaves alone are compared too."""
+    forces, matrix, calr = flags
+    if matrix or not gs.values_version:
+        n = gs._nsrc()
+        split = gs.storage == sv.CSRC and gs.unsym
+        gs.set_values(np.full(n // 2 if split else n, fill), np.full(gs.neq, fill),
+                      np.full(n // 2, fill) if split else None)
+    b, rcell = plan.assemble(_loads(case.loads), case.u0, case.cdiff, density=case.density,
+                             gradu0=case.gradu0, fres=case.fres, time=_time(case),
+                             forces=forces, matrix=matrix, calrcell=calr)
+    al, ad, au = A.get_values(gs)
+    a = al if au is None else np.concatenate([al, au])
+    return a, ad, b, rcell
+
+
+def test_fixture_replay(cuda):
+    mesh, facer, fields, loads, lays, cases = dif_fixture()
+    for lname, (st, un, ia, ja, neq) in lays.items():
+        gs = sv.GpuSystem(neq, ia, ja, st, un)
+        plans = {}
+        for c in (c for c in cases if c["layout"] == lname):
+            plan = plans.get(c["icod"])
+            if plan is None:
+                plan = plans[c["icod"]] = A.DifPlan(gs, mesh, facer, icod=c["icod"])
+            case = dif_case(mesh, facer, fields, loads, c)
+            flags = (c["forces"], c["matrix"], c["calrcell"])
+            a, ad, b, rcell = _device_assemble(gs, plan, case, flags)
+            if c["matrix"]:
+                assert bits_equal(a, c["a"]), c["name"]
+                assert bits_equal(ad, c["ad"]), c["name"]
+            if c["forces"]:
+                assert bits_equal(b, c["b"]), c["name"]
+            if c["calrcell"]:
+                assert bits_equal(rcell, c["rcell"]), c["name"]
+
+
+@pytest.fixture(scope="module")
+def box():
+    s = S.poisson_jittered(7, seed=5)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    return s, s.mesh(), lay
+
+
+@pytest.mark.parametrize("icod", [1, 2, 3, 4])
+def test_every_layout_and_option_matches_oracle(cuda, box, icod):
+    s, m, lay = box
+    rng = np.random.default_rng(icod)
+    for name, (st, un, ia, ja, _al, _au) in lay.items():
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.DifPlan(gs, m, m.face_r(SIDES), icod=icod)
+        for time, fres, flags in itertools.product((None, O.EULER, O.BACKWARD), (False, True),
+                                                   ((1, 1, 1), (1, 0, 0), (0, 1, 1))):
+            case = O.DifCase(mesh=m, facer=m.face_r(SIDES), loads=LOADS,
+                             density=rng.uniform(0.5, 2, m.numel),
+                             cdiff=m.cdiff * rng.uniform(0.5, 2, m.numel),
+                             u0=rng.standard_normal(m.numel),
+                             gradu0=rng.standard_normal((m.numel, 3)), icod=icod, fres=fres,
+                             time_flag=time is not None, time_type=time or 0, dt=0.1, dt0=0.05)
+            want = O.dif_assemble(case, st, un, ia, ja, s.neq, *flags, fill=3.0)
+            assert want[0] == 0
+            got = _device_assemble(gs, plan, case, flags, fill=3.0)
+            forces, matrix, calr = flags
+            if matrix:
+                assert bits_equal(got[0], want[1]), (name, time, fres, flags)
+                assert bits_equal(got[1], want[2]), (name, time, fres, flags)
+            if forces:
+                assert bits_equal(got[2], want[3]), (name, time, fres, flags)
+            if calr:
+                assert bits_equal(got[3], want[4]), (name, time, fres, flags)
+        plan.close()
+        gs.close()
+
+
+@pytest.mark.parametrize("icod", [1, 4])
+def test_64cubed_matches_oracle(cuda, icod):
+    s = S.poisson_jittered(64, seed=6)
+    m = s.mesh()
+    rng = np.random.default_rng(7)
+    case = O.DifCase(mesh=m, facer=m.face_r([1, 0, 2, 0, 0, 3]), loads=LOADS[:3],
+                     density=np.ones(m.numel), cdiff=m.cdiff, u0=rng.standard_normal(m.numel),
+                     gradu0=rng.standard_normal((m.numel, 3)), icod=icod, fres=True,
+                     time_flag=True, time_type=O.EULER, dt=1e-2)
+    want = O.dif_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    gs = sv.GpuSystem(s.neq, s.ia, s.ja, O.CSRD, True)
+    plan = A.DifPlan(gs, m, case.facer, icod=icod)
+    got = _device_assemble(gs, plan, case, (1, 1, 1))
+    for g, w in zip(got, want[1:]):
+        assert bits_equal(g, w)
+
+
+def test_b0_and_update_cells(cuda, box):
+    torch = cuda
+    s, m, lay = box
+    st, un, ia, ja, _al, _au = lay["csrd_full"]
+    rng = np.random.default_rng(11)
+    case = O.DifCase(mesh=m, facer=m.face_r(SIDES), loads=LOADS, density=np.ones(m.numel),
+                     cdiff=m.cdiff, u0=rng.standard_normal(m.numel),
+                     gradu0=rng.standard_normal((m.numel, 3)), icod=O.MINIMAL)
+    want = O.dif_assemble(case, st, un, ia, ja, s.neq)
+    b0 = rng.standard_normal(s.neq)
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    plan = A.DifPlan(gs, m, case.facer, icod=O.MINIMAL)
+    dev = lambda a: torch.tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+    d_u0, d_k, d_g, d_b0 = dev(case.u0), dev(case.cdiff), dev(case.gradu0), dev(b0)
+    d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
+    d_r = torch.empty(m.numel, dtype=torch.float64, device="cuda")
+    plan.assemble_device(_loads(LOADS), d_u0.data_ptr(), d_k.data_ptr(),
+                         d_gradu0=d_g.data_ptr(), d_b0=d_b0.data_ptr(), d_b=d_b.data_ptr(),
+                         d_rcell=d_r.data_ptr())
+    torch.cuda.synchronize()
+    # addVector (b + b0) and updateCellValue (rCell + b0[id - 1]), Diffusion.c:107-118
+    assert bits_equal(d_b.cpu().numpy(), want[3] + b0)
+    assert bits_equal(d_r.cpu().numpy(), want[4] + b0[m.id - 1])
+    x = rng.standard_normal(s.neq)
+    d_x = dev(x)
+    d_u = d_u0.clone()
+    plan.update_cells(d_x.data_ptr(), d_u.data_ptr(), add=True)
+    torch.cuda.synchronize()
+    assert bits_equal(d_u.cpu().numpy(), case.u0 + x[m.id - 1])
+    plan.update_cells(d_x.data_ptr(), d_u.data_ptr(), add=False)
+    torch.cuda.synchronize()
+    assert bits_equal(d_u.cpu().numpy(), x[m.id - 1])
+
+
+def test_assembled_system_solves_like_reference(cuda, box):
+    """Assemble on the device, solve on the device: the solution of the
+    system the oracle assembles, solved by the oracle's PCG."""
+    torch = cuda
+    s, m, lay = box
+    st, un, ia, ja, _al, _au = lay["csrc_sym"]
+    rng = np.random.default_rng(12)
+    case = O.DifCase(mesh=m, facer=m.face_r([1, 0, 2, 0, 0, 0]), loads=LOADS[:2],
+                     density=np.ones(m.numel), cdiff=m.cdiff, u0=rng.standard_normal(m.numel),
+                     gradu0=np.zeros((m.numel, 3)), icod=O.ORTHOGONAL)
+    rc, a, ad, b, _ = O.dif_assemble(case, st, un, ia, ja, s.neq)
+    ref = O.pcg(st, un, ia, ja, a, ad, b, tol=1e-10)
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    plan = A.DifPlan(gs, m, case.facer, icod=O.ORTHOGONAL)
+    dev = lambda v: torch.tensor(np.ascontiguousarray(v), device="cuda")  # noqa: E731
+    d_u0, d_k = dev(case.u0), dev(case.cdiff)
+    d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
+    d_x = torch.zeros(s.neq, dtype=torch.float64, device="cuda")
+    plan.assemble_device(_loads(LOADS[:2]), d_u0.data_ptr(), d_k.data_ptr(),
+                         d_b=d_b.data_ptr(), calrcell=False)
+    info = gs.solve_device(sv.PCG, d_b.data_ptr(), d_x.data_ptr(), tol=1e-10)
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(d_x.cpu().numpy(), ref.x) < 1e-12
+    # new coefficients reach every engine: the resident mixed path re-derives
+    # its scaled operator from the new values
+    case2 = O.DifCase(**{**case.__dict__, "cdiff": case.cdiff * 3.0})
+    rc, a2, ad2, b2, _ = O.dif_assemble(case2, st, un, ia, ja, s.neq)
+    ref2 = O.pcg(st, un, ia, ja, a2, ad2, b2, tol=1e-10)
+    plan.assemble_device(_loads(LOADS[:2]), d_u0.data_ptr(), dev(case2.cdiff).data_ptr(),
+                         d_b=d_b.data_ptr(), calrcell=False)
+    d_x.zero_()
+    info = gs.solve_device(sv.PCG, d_b.data_ptr(), d_x.data_ptr(), tol=1e-10,
+                           precision=sv.MIXED)
+    assert info.relres < 1e-10
+    # the residual of the new system (assembled by the oracle) at the GPU's x
+    x2 = d_x.cpu().numpy()
+    r2 = b2 - O.matvec(st, un, ia, ja, a2, ad2, x2)
+    assert np.linalg.norm(r2) / np.linalg.norm(b2) < 2e-10
+    assert rel(x2, ref2.x) < 1e-6
+
+
+def test_plan_and_call_validation(cuda, box):
+    s, m, lay = box
+    st, un, ia, ja, _al, _au = lay["csrd_full"]
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    bad = S.FvMesh(**{**m.__dict__, "id": m.id.copy()})
+    bad.id[3] = bad.id[4]
+    with pytest.raises(sv.SolverError) as e:
+        A.DifPlan(gs, bad, m.face_r(SIDES))
+    assert e.value.status == sv.BAD_INPUT and "same equation" in sv.last_error()
+    with pytest.raises(sv.SolverError) as e:
+        A.DifPlan(gs, m, m.face_r(SIDES), caltype=np.array([3], np.int16))
+    assert e.value.status == sv.BAD_INPUT
+    plan = A.DifPlan(gs, m, m.face_r(SIDES))
+    u0 = np.zeros(m.numel)
+    with pytest.raises(sv.SolverError) as e:   # a face names load 6 of 2
+        plan.assemble(_loads(LOADS[:2]), u0, m.cdiff)
+    assert e.value.status == sv.BAD_INPUT
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.SINBC, (1.0,) * 9)] + _loads(LOADS[1:]), u0, m.cdiff)
+    assert e.value.status == sv.UNSUPPORTED
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.DIRICHLET, (1.0,), var=1)] + _loads(LOADS[1:]), u0, m.cdiff)
+    assert e.value.status == sv.UNSUPPORTED
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.OUTLET, ())] + _loads(LOADS[1:]), u0, m.cdiff)
+    assert e.value.status == sv.BAD_INPUT
+    # a load no face names is not checked, as in the reference
+    assert 4 not in [v - 1 for v in SIDES if v]
+    plan.assemble(_loads(LOADS[:4]) + [A.Load(A.OUTLET, ())] + _loads(LOADS[5:]), u0, m.cdiff)
