@@ -319,6 +319,8 @@ int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
                          const double *u0, const double *gradu0, const double *b0, double *b,
                          double *rcell, int32_t forces, int32_t matrix, int32_t calrcell);
 
+/* Frees the plan; safe after the system is destroyed (the plan's calls are
+ * not). */
 int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
 
 /* Copy the system's values back in the reference's layout: al (nad, or the

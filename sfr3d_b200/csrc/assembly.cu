@@ -266,8 +266,10 @@ __device__ __forceinline__ void apply_load(const DevLoad &L, double kc, double a
 // One row of cellDif3D.  kOrth: ORTHOGONAL scheme, whose explicit part t is
 // zero, so the non-orthogonal correction adds coef * (+-0) to a force that
 // can never be -0: it changes nothing for finite fields and is skipped
-// (gradu0 is not read).
-template <bool kOrth>
+// (gradu0 is not read).  kMV: face slots of the plan (maxviz rounded up to
+// 6 or 8); every slot is read, unused ones hold a bare-boundary marker, so
+// that all of a row's loads are issued before the first is used.
+template <bool kOrth, int kMV>
 __global__ void __launch_bounds__(256)
     dif_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, CallOpts o,
                         const double *__restrict__ density, const double *__restrict__ cdiff,
@@ -277,52 +279,69 @@ __global__ void __launch_bounds__(256)
                         double *__restrict__ rcell) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.n) return;
-  const int cell = p.cell[r];
+  const int cell = __ldcs(p.cell + r);
   if (cell < 0) return;
-  const int nf = p.nface[r];
+  const int nf = __ldcs(p.nface + r);
+  const size_t fs = p.fstride;
+  int32_t nbs[kMV], dsts[kMV];
+  double alpha[kMV], modE[kMV], mk[kMV], kn[kMV], un[kMV];
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    const size_t q = static_cast<size_t>(f) * p.n + r;
+    nbs[f] = __ldcs(p.nb + q);
+    alpha[f] = __ldcs(p.geo + q);
+    modE[f] = __ldcs(p.geo + fs + q);
+    mk[f] = __ldcs(p.geo + 2 * fs + q);
+  }
   const double kc = cdiff[cell], uc = u0[cell];
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    const int c = nbs[f] >= 0 ? (nbs[f] & (kFlagP - 1)) : cell;
+    kn[f] = cdiff[c];
+    un[f] = u0[c];
+  }
+  if (o.matrix) {
+#pragma unroll
+    for (int f = 0; f < kMV; ++f) dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+  }
   double gp[3] = {0.0, 0.0, 0.0};
   if (!kOrth)
     for (int j = 0; j < 3; ++j) gp[j] = gradu0[3 * static_cast<size_t>(cell) + j];
-  double la[kMaxViz], un[kMaxViz];
-  int32_t nbs[kMaxViz];
+  double la[kMV];
   double pp = 0.0, sP = 0.0;
-  const size_t fs = p.fstride;
 #pragma unroll
-  for (int f = 0; f < kMaxViz; ++f) {
+  for (int f = 0; f < kMV; ++f) {
     la[f] = 0.0;
-    un[f] = 0.0;
-    nbs[f] = -1;
-    if (f < nf) {
-      const size_t q = static_cast<size_t>(f) * p.n + r;
-      const int32_t nb = __ldcs(p.nb + q);
-      nbs[f] = nb;
-      const double *g = p.geo + q;
-      if (nb >= 0) {
+    if (f >= nf) continue;
+    const int32_t nb = nbs[f];
+    if (nb >= 0) {
+      const double am1 = xsub(1.0, alpha[f]);
+      double coef = xadd(xdiv(alpha[f], kc), xdiv(am1, kn[f]));
+      coef = xdiv(1.0, coef);
+      la[f] = xdiv(xmul(coef, modE[f]), mk[f]);
+      if (!kOrth) {
+        const size_t q = static_cast<size_t>(f) * p.n + r;
         const int c = nb & (kFlagP - 1);
-        const double alpha = __ldcs(g), modE = __ldcs(g + fs), mk = __ldcs(g + 2 * fs);
-        const double am1 = xsub(1.0, alpha);
-        un[f] = u0[c];
-        double coef = xadd(xdiv(alpha, kc), xdiv(am1, cdiff[c]));
-        coef = xdiv(1.0, coef);
-        la[f] = xdiv(xmul(coef, modE), mk);
-        if (!kOrth) {
-          const double duDksi = xdiv(xsub(un[f], uc), mk);
-          double k[3], t[3], gf[3], gc[3];
-          for (int j = 0; j < 3; ++j) {
-            k[j] = __ldcs(g + (3 + j) * fs);
-            t[j] = __ldcs(g + (6 + j) * fs);
-            gf[j] = xadd(xmul(am1, gp[j]),
-                         xmul(alpha, gradu0[3 * static_cast<size_t>(c) + j]));
-          }
-          const double du = xsub(duDksi, dot3(gf, k));
-          for (int j = 0; j < 3; ++j) gc[j] = xadd(gf[j], xmul(du, k[j]));
-          pp = xadd(pp, xmul(coef, dot3(gc, t)));
+        const double duDksi = xdiv(xsub(un[f], uc), mk[f]);
+        double k[3], t[3], gf[3], gc[3];
+        for (int j = 0; j < 3; ++j) {
+          k[j] = __ldcs(p.geo + (3 + j) * fs + q);
+          t[j] = __ldcs(p.geo + (6 + j) * fs + q);
+          gf[j] = xadd(xmul(am1, gp[j]),
+                       xmul(alpha[f], gradu0[3 * static_cast<size_t>(c) + j]));
         }
-      } else if (nb <= -2) {
-        const double n[3] = {__ldcs(g + 3 * fs), __ldcs(g + 4 * fs), __ldcs(g + 5 * fs)};
-        apply_load(loads[-nb - 2], kc, __ldcs(g), __ldcs(g + fs), n, sP, pp);
+        const double du = xsub(duDksi, dot3(gf, k));
+        for (int j = 0; j < 3; ++j) gc[j] = xadd(gf[j], xmul(du, k[j]));
+        pp = xadd(pp, xmul(coef, dot3(gc, t)));
       }
+    } else if (nb <= -2) {
+      // boundary slot: alpha holds the area, modE the centre-face distance
+      const size_t q = static_cast<size_t>(f) * p.n + r;
+      double n[3] = {0.0, 0.0, 0.0};
+      const DevLoad &L = loads[-nb - 2];
+      if (L.type == 6)
+        for (int j = 0; j < 3; ++j) n[j] = __ldcs(p.geo + (3 + j) * fs + q);
+      apply_load(L, kc, alpha[f], modE[f], n, sP, pp);
     }
   }
   // implicit time term, CellDif.c:485-497
@@ -337,11 +356,11 @@ __global__ void __launch_bounds__(256)
   }
   double d = sP;
 #pragma unroll
-  for (int f = 0; f < kMaxViz; ++f)
+  for (int f = 0; f < kMV; ++f)
     if (f < nf) d = xadd(d, la[f]);
   double rr = 0.0;
 #pragma unroll
-  for (int f = 0; f < kMaxViz; ++f)
+  for (int f = 0; f < kMV; ++f)
     if (f < nf && nbs[f] >= 0) {
       if (nbs[f] & kFlagP)
         pp = xadd(pp, xmul(la[f], un[f]));
@@ -358,11 +377,8 @@ __global__ void __launch_bounds__(256)
   if (!o.matrix) return;
   diag[r] = d;
 #pragma unroll
-  for (int f = 0; f < kMaxViz; ++f)
-    if (f < nf) {
-      const int32_t t = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
-      if (t >= 0) stage[t] = xmul(la[f], -1.0);
-    }
+  for (int f = 0; f < kMV; ++f)
+    if (f < nf && dsts[f] >= 0) stage[dsts[f]] = xmul(la[f], -1.0);
 }
 
 __global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
@@ -386,7 +402,8 @@ cudaError_t upload(T **dst, const T *src, size_t count) {
 }  // namespace sfr
 
 struct sfr_dif_plan {
-  sfr_system *s = nullptr;
+  sfr_system *s = nullptr;       // the system written; must outlive the plan's calls
+  int32_t device = 0;            // destroy needs no live system
   int32_t numel = 0, maxviz = 0, icod = 0;
   int free_cells = 0;            // cells without an equation (their rcell is zeroed)
   unsigned used_loads = 0;       // bit l: some boundary face names load l
@@ -489,12 +506,14 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   SFR_CUA(cudaSetDevice(s->device));
   auto *p = new sfr_dif_plan;
   p->s = s;
+  p->device = s->device;
   p->numel = m.numel;
   p->maxviz = m.maxviz;
   p->icod = icod;
   p->loads_host.assign(sfr::kMaxLoads, sfr::DevLoad{});
   const int n = s->n;
-  const size_t slots = static_cast<size_t>(m.maxviz) * n;
+  const int mvpad = m.maxviz <= 6 ? 6 : sfr::kMaxViz;  // slots the assembly kernel reads
+  const size_t slots = static_cast<size_t>(mvpad) * n;
   sfr::MeshDev md{};
   md.numel = m.numel;
   md.maxviz = m.maxviz;
@@ -552,7 +571,7 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   }
   sfr::PlanDev &d = p->d;
   d.n = n;
-  d.maxviz = m.maxviz;
+  d.maxviz = mvpad;
   d.fstride = slots;
   up(cudaMalloc(&d.cell, sizeof(int32_t) * n));
   up(cudaMalloc(&d.nface, sizeof(int16_t) * n));
@@ -567,6 +586,7 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
     up(cudaMemset(d.nface, 0, sizeof(int16_t) * n));
     up(cudaMemset(d.nb, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.dst, 0xFF, sizeof(int32_t) * slots));
+    up(cudaMemset(d.geo, 0, sizeof(double) * slots * sfr::kGeo));
     up(cudaMemset(p->d_loads, 0, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
     up(cudaMemset(d_err, 0, sizeof(int) * 3));
   }
@@ -617,14 +637,16 @@ int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t 
   sfr::CallOpts co{o->fres != 0, o->time_flag != 0, o->time_type, forces != 0, matrix != 0,
                    calrcell != 0, o->dt, o->dt0};
   const int blocks = (s->n + 255) / 256;
-  if (p->icod == 1)
-    sfr::dif_assemble_kernel<true><<<blocks, 256, 0, st>>>(
-        p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0, d_b0, s->d_stage,
-        s->d_diag, d_b, d_rcell);
+  auto launch = [&](auto kernel) {
+    kernel<<<blocks, 256, 0, st>>>(p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0,
+                                   d_b0, s->d_stage, s->d_diag, d_b, d_rcell);
+  };
+  if (p->d.maxviz == 6)
+    p->icod == 1 ? launch(sfr::dif_assemble_kernel<true, 6>)
+                 : launch(sfr::dif_assemble_kernel<false, 6>);
   else
-    sfr::dif_assemble_kernel<false><<<blocks, 256, 0, st>>>(
-        p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0, d_b0, s->d_stage,
-        s->d_diag, d_b, d_rcell);
+    p->icod == 1 ? launch(sfr::dif_assemble_kernel<true, sfr::kMaxViz>)
+                 : launch(sfr::dif_assemble_kernel<false, sfr::kMaxViz>);
   SFR_CUA(cudaGetLastError());
   if (matrix) return sfr::values_refreshed(s, st);
   return SFR_OK;
@@ -682,7 +704,7 @@ int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, in
 
 int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p) {
   if (!p) return SFR_OK;
-  cudaSetDevice(p->s->device);
+  cudaSetDevice(p->device);
   free_plan_buffers(p);
   delete p;
   return SFR_OK;

@@ -229,3 +229,19 @@ def test_plan_and_call_validation(cuda, box):
     # a load no face names is not checked, as in the reference
     assert 4 not in [v - 1 for v in SIDES if v]
     plan.assemble(_loads(LOADS[:4]) + [A.Load(A.OUTLET, ())] + _loads(LOADS[5:]), u0, m.cdiff)
+
+
+def test_plan_outliving_its_system_leaves_no_error(cuda, box):
+    """Garbage collection may free a system before its plan: destroying the
+    plan then must not touch the system (a stale CUDA error would fail the
+    next launch check of any handle)."""
+    s, m, lay = box
+    st, un, ia, ja, al, _au = lay["csrd_full"]
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    plan = A.DifPlan(gs, m, m.face_r(SIDES))
+    gs.close()
+    plan.close()
+    g2 = sv.GpuSystem(s.neq, ia, ja, st, un)
+    g2.set_values(al, s.ad)
+    x, info = g2.solve(sv.PCG, s.b[0], tol=1e-10)
+    assert info.status == sv.OK
