@@ -570,11 +570,13 @@ def other_krylov_leg(sv, S, s, n):
 
 
 # algorithmic bytes per row of the ORTHOGONAL diffusion assembly kernel on a
-# hexahedral mesh (6 faces): plan row header (cell 4 + face count 2), per
-# face the neighbour/destination words (8) and 3 geometry doubles (24), the
-# cell's own diffusivity and u0 (16); writes 6 off-diagonals, ad, b, rCell
-# (72).  Neighbour gathers are counted once (they are other rows' own reads).
-ASSEMBLY_ALG_BYTES_PER_ROW = 6 + 6 * 32 + 16 + 72
+# hexahedral mesh (6 faces), CSRD full: plan row header (cell 4 + face count
+# 2), per face the neighbour, raw-destination and SELL-slot words (12) and 3
+# geometry doubles (24), the cell's own diffusivity and u0 (16); writes the
+# 6 off-diagonals in the reference's layout and in the solver's copy (FP64 +
+# FP32: 6 * 20), ad, its FP32 copy, the row compensation, b and rCell (36).
+# Neighbour gathers are counted once (they are other rows' own reads).
+ASSEMBLY_ALG_BYTES_PER_ROW = 6 + 6 * 36 + 16 + 6 * 20 + 36
 
 
 def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
@@ -645,8 +647,9 @@ def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
             "device_ms": dev_ms, "plan_create_s": plan_s,
             "alg_bytes_per_call": alg, "alg_bytes_per_row": ASSEMBLY_ALG_BYTES_PER_ROW,
             "GB/s": gbs, "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
-            "timing": "CUDA events around one call (assembly kernel + the value refresh "
-                      "into the solver's SELL copy), 256 MiB L2 flush between calls, median "
+            "kernel": "dif_assemble_kernel<orthogonal, 6 faces, fused> (one launch: also "
+                      "writes the solver's SELL copy, its FP32 copy and compensation)",
+            "timing": "CUDA events around one call, 256 MiB L2 flush between calls, median "
                       "of 10",
             "upload_A_b_pinned_ms": upload_ms,
             "host_api_ms": host_ms,

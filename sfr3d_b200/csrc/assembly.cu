@@ -87,8 +87,21 @@ struct PlanDev {
   int16_t *nface;       // [n]
   int32_t *nb;          // [maxviz][n] neighbour cell (| kFlagP), -1 bare boundary, -(load+2)
   int32_t *dst;         // [maxviz][n] raw value index, -1 none
+  int32_t *sslot;       // [maxviz][n] slot of the value in row r of the SELL copy, -1 none
   double *geo;          // [kGeo][maxviz][n]
   double *vol;          // [n]
+};
+
+// The system's SELL copy, written directly when every stored value of a row
+// comes from that row's own cell (full-row layouts): the assembly then also
+// does what the value refresh would (the FP32 copy, the row compensation and
+// the FP32 diagonal), in the same slot order.
+struct FuseDev {
+  double *val;
+  float *val32;
+  const int32_t *sptr;
+  double *comp;
+  float *diag32;
 };
 
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
@@ -122,25 +135,37 @@ __device__ void dif_scheme(int icod, const double s[3], const double k[3], doubl
   for (int j = 0; j < 3; ++j) t[j] = xsub(s[j], e[j]);
 }
 
-// column c of row r in the system's SELL copy -> index in the raw values;
-// -1 absent, -3 present twice
-__device__ int raw_index(const PatternDev &P, int r, int c) {
+// column c of row r in the system's SELL copy -> index in the raw values
+// (and the slot, in *slot); -1 absent, -3 present twice
+__device__ int raw_index(const PatternDev &P, int r, int c, int *slot) {
   const int slice = r >> 5, lane = r & 31;
   const int beg = P.sptr[slice];
   const int w = (P.sptr[slice + 1] - beg) >> 5;
   int found = -1, hits = 0;
+  *slot = -1;
   for (int j = 0; j < w; ++j) {
     const int e = beg + j * 32 + lane;
     if (P.col[e] == c && P.src[e] >= 0) {
       found = P.src[e];
+      *slot = e;
       ++hits;
     }
   }
   return hits > 1 ? -3 : found;
 }
 
+// stored (non-padding) slots of row r
+__device__ int real_slots(const PatternDev &P, int r) {
+  const int slice = r >> 5, lane = r & 31;
+  const int beg = P.sptr[slice];
+  const int w = (P.sptr[slice + 1] - beg) >> 5;
+  int k = 0;
+  for (int j = 0; j < w; ++j) k += P.src[beg + j * 32 + lane] >= 0;
+  return k;
+}
+
 __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *err,
-                            unsigned *used_loads, int *free_cells) {
+                            unsigned *used_loads, int *free_cells, int *partial_rows) {
   const int nel = blockIdx.x * blockDim.x + threadIdx.x;
   if (nel >= m.numel) return;
   const int mv = m.maxviz;
@@ -160,6 +185,7 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
   p.nface[row] = static_cast<int16_t>(nf);
   p.vol[row] = m.volume[nel];
   const bool sym_lower = !P.unsym && P.storage != SFR_ELLPACK;
+  int written = 0;  // SELL slots of row r this cell writes
   for (int f = 0; f < nf; ++f) {
     const size_t q = static_cast<size_t>(nel) * mv + f;
     const size_t o = static_cast<size_t>(f) * P.n + row;
@@ -173,6 +199,7 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
     }
     const int viz = m.nelcon[q] - 1;
     int32_t nbv, dst = -1;
+    int slot = -1;
     if (viz > -1) {
       if (viz >= m.numel) return flag_error(err, kErrNeighbour);
       const double area = m.area[face], mk = m.mksi[face];
@@ -192,8 +219,9 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
       nbv = viz | (lid == -2 ? kFlagP : 0);
       if (P.storage == SFR_ELLPACK) {
         dst = row * P.width + f;
+        slot = P.sptr[row >> 5] + f * 32 + (row & 31);
       } else if (lid > -1 && !(sym_lower && lid > row)) {
-        dst = raw_index(P, row, lid);
+        dst = raw_index(P, row, lid, &slot);
         if (dst == -3) return flag_error(err, kErrColumnTwice);
       }
     } else {
@@ -209,12 +237,19 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
         g[3 + j] = nrm[j];
         g[6 + j] = 0.0;
       }
-      if (P.storage == SFR_ELLPACK) dst = row * P.width + f;
+      if (P.storage == SFR_ELLPACK) {
+        dst = row * P.width + f;
+        slot = P.sptr[row >> 5] + f * 32 + (row & 31);
+      }
     }
+    if (sym_lower) slot = -1;  // the row's mirrored slots come from other cells
+    written += slot >= 0;
     p.nb[o] = nbv;
     p.dst[o] = dst;
+    p.sslot[o] = slot;
     for (int k = 0; k < kGeo; ++k) p.geo[k * p.fstride + o] = g[k];
   }
+  if (sym_lower || written != real_slots(P, row)) atomicAdd(partial_rows, 1);
 }
 
 struct DevLoad {
@@ -269,9 +304,9 @@ __device__ __forceinline__ void apply_load(const DevLoad &L, double kc, double a
 // (gradu0 is not read).  kMV: face slots of the plan (maxviz rounded up to
 // 6 or 8); every slot is read, unused ones hold a bare-boundary marker, so
 // that all of a row's loads are issued before the first is used.
-template <bool kOrth, int kMV>
+template <bool kOrth, int kMV, bool kFused>
 __global__ void __launch_bounds__(256)
-    dif_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, CallOpts o,
+    dif_assemble_kernel(PlanDev p, FuseDev fu, const DevLoad *__restrict__ loads, CallOpts o,
                         const double *__restrict__ density, const double *__restrict__ cdiff,
                         const double *__restrict__ u0, const double *__restrict__ gradu0,
                         const double *__restrict__ b0, double *__restrict__ stage,
@@ -300,9 +335,13 @@ __global__ void __launch_bounds__(256)
     kn[f] = cdiff[c];
     un[f] = u0[c];
   }
+  int32_t slots[kMV];
   if (o.matrix) {
 #pragma unroll
-    for (int f = 0; f < kMV; ++f) dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+    for (int f = 0; f < kMV; ++f) {
+      dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+      slots[f] = kFused ? __ldcs(p.sslot + static_cast<size_t>(f) * p.n + r) : -1;
+    }
   }
   double gp[3] = {0.0, 0.0, 0.0};
   if (!kOrth)
@@ -379,6 +418,25 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int f = 0; f < kMV; ++f)
     if (f < nf && dsts[f] >= 0) stage[dsts[f]] = xmul(la[f], -1.0);
+  if (kFused) {
+    // the value refresh for this row: SELL values, their FP32 copy, and the
+    // compensation summed in slot order as the refresh sums it
+    fu.diag32[r] = __double2float_rn(d);
+    const int base = fu.sptr[r >> 5] + (r & 31);
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMV; ++k)
+#pragma unroll
+      for (int f = 0; f < kMV; ++f)
+        if (f < nf && slots[f] == base + 32 * k) {
+          const double v = xmul(la[f], -1.0);
+          const float v32 = __double2float_rn(v);
+          fu.val[slots[f]] = v;
+          fu.val32[slots[f]] = v32;
+          acc = xadd(acc, xsub(static_cast<double>(v32), v));
+        }
+    fu.comp[r] = -acc;
+  }
 }
 
 __global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
@@ -408,6 +466,7 @@ struct sfr_dif_plan {
   int free_cells = 0;            // cells without an equation (their rcell is zeroed)
   unsigned used_loads = 0;       // bit l: some boundary face names load l
   sfr::PlanDev d{};
+  bool fused = false;            // the assembly also refreshes the SELL copy
   int32_t *d_id = nullptr;       // per cell: equation + 1 (updateCellValue)
   sfr::DevLoad *d_loads = nullptr;
   std::vector<sfr::DevLoad> loads_host;  // what d_loads holds
@@ -437,6 +496,7 @@ void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->d.nface);
   cudaFree(p->d.nb);
   cudaFree(p->d.dst);
+  cudaFree(p->d.sslot);
   cudaFree(p->d.geo);
   cudaFree(p->d.vol);
   cudaFree(p->d_id);
@@ -577,31 +637,46 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   up(cudaMalloc(&d.nface, sizeof(int16_t) * n));
   up(cudaMalloc(&d.nb, sizeof(int32_t) * slots));
   up(cudaMalloc(&d.dst, sizeof(int32_t) * slots));
+  up(cudaMalloc(&d.sslot, sizeof(int32_t) * slots));
   up(cudaMalloc(&d.geo, sizeof(double) * slots * sfr::kGeo));
   up(cudaMalloc(&d.vol, sizeof(double) * n));
   up(cudaMalloc(&p->d_loads, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
-  up(cudaMalloc(&d_err, sizeof(int) * 3));
+  up(cudaMalloc(&d_err, sizeof(int) * 4));
   if (rc == SFR_OK) {
     up(cudaMemset(d.cell, 0xFF, sizeof(int32_t) * n));
     up(cudaMemset(d.nface, 0, sizeof(int16_t) * n));
     up(cudaMemset(d.nb, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.dst, 0xFF, sizeof(int32_t) * slots));
+    up(cudaMemset(d.sslot, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.geo, 0, sizeof(double) * slots * sfr::kGeo));
     up(cudaMemset(p->d_loads, 0, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
-    up(cudaMemset(d_err, 0, sizeof(int) * 3));
+    up(cudaMemset(d_err, 0, sizeof(int) * 4));
   }
   if (rc == SFR_OK) {
     sfr::PatternDev P{s->A.sptr, s->A.col, s->A.src, n, s->storage, s->unsym,
                       s->storage == SFR_ELLPACK ? s->nsrc / std::max(n, 1) : 0};
     const int blocks = (m.numel + 255) / 256;
     sfr::plan_kernel<<<blocks, 256>>>(md, P, d, icod, d_err,
-                                      reinterpret_cast<unsigned *>(d_err + 1), d_err + 2);
+                                      reinterpret_cast<unsigned *>(d_err + 1), d_err + 2,
+                                      d_err + 3);
     up(cudaGetLastError());
-    int h[3] = {0, 0, 0};
+    int h[4] = {0, 0, 0, 0};
     up(cudaMemcpy(h, d_err, sizeof(h), cudaMemcpyDeviceToHost));
     if (rc == SFR_OK && h[0] != sfr::kErrNone) rc = bad(sfr::plan_error_text(h[0]));
     p->used_loads = static_cast<unsigned>(h[1]);
     p->free_cells = h[2];
+    // every stored value of every row written by the row's own cell
+    p->fused = h[3] == 0 && s->A.val32 != nullptr;
+  }
+  if (rc == SFR_OK && p->fused) {
+    if (!s->d_comp) {
+      up(cudaMalloc(&s->d_comp, sizeof(double) * std::max(n, 1)));
+      if (rc == SFR_OK) s->bytes += static_cast<int64_t>(sizeof(double)) * n;
+    }
+    if (!s->values_set) {  // padding slots hold zeros, as the refresh leaves them
+      up(cudaMemset(s->A.val, 0, sizeof(double) * std::max<int64_t>(s->A.nslots, 1)));
+      up(cudaMemset(s->A.val32, 0, sizeof(float) * std::max<int64_t>(s->A.nslots, 1)));
+    }
   }
   md.id = nullptr;  // the plan's (freed with it)
   release_mesh();
@@ -637,18 +712,31 @@ int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t 
   sfr::CallOpts co{o->fres != 0, o->time_flag != 0, o->time_type, forces != 0, matrix != 0,
                    calrcell != 0, o->dt, o->dt0};
   const int blocks = (s->n + 255) / 256;
+  const bool fuse = p->fused && matrix;
+  sfr::FuseDev fu{s->A.val, s->A.val32, s->A.sptr, s->d_comp, s->d_diag32};
   auto launch = [&](auto kernel) {
-    kernel<<<blocks, 256, 0, st>>>(p->d, p->d_loads, co, d_density, d_cdiff, d_u0, d_gradu0,
-                                   d_b0, s->d_stage, s->d_diag, d_b, d_rcell);
+    kernel<<<blocks, 256, 0, st>>>(p->d, fu, p->d_loads, co, d_density, d_cdiff, d_u0,
+                                   d_gradu0, d_b0, s->d_stage, s->d_diag, d_b, d_rcell);
   };
-  if (p->d.maxviz == 6)
-    p->icod == 1 ? launch(sfr::dif_assemble_kernel<true, 6>)
-                 : launch(sfr::dif_assemble_kernel<false, 6>);
-  else
-    p->icod == 1 ? launch(sfr::dif_assemble_kernel<true, sfr::kMaxViz>)
-                 : launch(sfr::dif_assemble_kernel<false, sfr::kMaxViz>);
+  const bool orth = p->icod == 1, six = p->d.maxviz == 6;
+  constexpr int k8 = sfr::kMaxViz;
+  if (fuse) {
+    if (six)
+      orth ? launch(sfr::dif_assemble_kernel<true, 6, true>)
+           : launch(sfr::dif_assemble_kernel<false, 6, true>);
+    else
+      orth ? launch(sfr::dif_assemble_kernel<true, k8, true>)
+           : launch(sfr::dif_assemble_kernel<false, k8, true>);
+  } else {
+    if (six)
+      orth ? launch(sfr::dif_assemble_kernel<true, 6, false>)
+           : launch(sfr::dif_assemble_kernel<false, 6, false>);
+    else
+      orth ? launch(sfr::dif_assemble_kernel<true, k8, false>)
+           : launch(sfr::dif_assemble_kernel<false, k8, false>);
+  }
   SFR_CUA(cudaGetLastError());
-  if (matrix) return sfr::values_refreshed(s, st);
+  if (matrix) return sfr::values_refreshed(s, st, fuse);
   return SFR_OK;
 }
 

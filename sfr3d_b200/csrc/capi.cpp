@@ -157,17 +157,21 @@ namespace sfr {
 
 // After new raw values (d_stage) and diagonal (d_diag) are in place on `st`:
 // the SELL copies, the FP32 compensation and diagonal, and the epoch the
-// derived operators are keyed on.
-int values_refreshed(sfr_system *s, cudaStream_t st) {
-  int rc = gather_values(s, &s->A, st);
-  if (rc != SFR_OK) return rc;
-  rc = row_compensation(s, s->A, st);
-  if (rc != SFR_OK) return rc;
+// derived operators are keyed on.  a_done: the SELL copy of A, its
+// compensation and the FP32 diagonal were written with the values.
+int values_refreshed(sfr_system *s, cudaStream_t st, bool a_done) {
+  int rc = SFR_OK;
+  if (!a_done) {
+    rc = gather_values(s, &s->A, st);
+    if (rc != SFR_OK) return rc;
+    rc = row_compensation(s, s->A, st);
+    if (rc != SFR_OK) return rc;
+    SFR_CU(convert_diag32(s->d_diag, s->d_diag32, s->n, st));
+  }
   if (s->at_ready) {
     rc = gather_values(s, &s->At, st);
     if (rc != SFR_OK) return rc;
   }
-  SFR_CU(convert_diag32(s->d_diag, s->d_diag32, s->n, st));
   s->values_set = true;
   ++s->values_epoch;
   if (s->tview) s->tview->comp_stale = true;

@@ -102,7 +102,7 @@ void free_sell(DevSell *d);
 int ensure_workspace(sfr_system *s, size_t bytes);
 int gather_values(sfr_system *s, DevSell *d, cudaStream_t st);
 // the derived copies and epoch after new raw values and diagonal (capi.cpp)
-int values_refreshed(sfr_system *s, cudaStream_t st);
+int values_refreshed(sfr_system *s, cudaStream_t st, bool a_done = false);
 cudaError_t convert_diag32(const double *src, float *dst, int n, cudaStream_t st);
 // d_comp from the FP64 and FP32 values of d (allocates d_comp on first use)
 int row_compensation(sfr_system *s, const DevSell &d, cudaStream_t st);
