@@ -55,7 +55,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the momentum, batched and adjoint legs")
-    ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab"], default="none",
+    ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab", "assembly",
+                                          "pressure"], default="none",
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
                     help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
@@ -205,6 +206,12 @@ def run_ours(args):
                 y = torch.empty_like(b)
                 for _ in range(args.warmup + args.steps):
                     g.spmv(b.data_ptr(), y.data_ptr(), sptr)
+            elif args.profile in ("assembly", "pressure"):
+                setup = dif_call_setup if args.profile == "assembly" else pres_call_setup
+                call, close = setup(np, torch, sv, s, sptr)
+                for _ in range(args.warmup + args.steps):
+                    call()
+                close()
             elif args.profile == "bicgstab":
                 m = S.momentum(n, nrhs=1, seed=3)
                 gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=local)
@@ -299,6 +306,7 @@ def run_ours(args):
     if extras and not args.no_extras:
         other = other_krylov_leg(sv, S, s, n)
         assembly = assembly_leg(np, torch, sv, s, n, peak, peak_kind)
+        assembly["pressure"] = pressure_leg(np, torch, sv, s, n, peak, peak_kind)
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -579,34 +587,75 @@ def other_krylov_leg(sv, S, s, n):
 ASSEMBLY_ALG_BYTES_PER_ROW = 6 + 6 * 36 + 16 + 6 * 20 + 36
 
 
-def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
-    """systFormDif on the device for the 128^3 pressure mesh (ORTHOGONAL,
-    Dirichlet on x = 0, Neumann elsewhere, residual form): one call writes
-    A (CSRD) and b where the next solve reads them.  Beside it: the per-call
-    upload of A and b the host-assembled path needs, and the host-array
-    entry point (fields in, b and rCell out)."""
+def dif_call_setup(np, torch, sv, s, stream):
+    """A device systFormDif call on the system's mesh (ORTHOGONAL, Dirichlet
+    on x = 0, Neumann elsewhere, residual form, CSRD): (call, close)."""
     from sfr3d_b200 import assembly as A
     m = s.mesh()
     rng = np.random.default_rng(9)
-    facer = m.face_r([1, 0, 0, 0, 0, 0])
-    loads = [A.Load(A.DIRICHLET, (0.0,))]
-    t0 = time.perf_counter()
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
-    plan = A.DifPlan(g, m, facer, icod=A.ORTHOGONAL)
-    torch.cuda.synchronize()
-    plan_s = time.perf_counter() - t0
-    u0 = rng.standard_normal(m.numel)
+    plan = A.DifPlan(g, m, m.face_r([1, 0, 0, 0, 0, 0]), icod=A.ORTHOGONAL)
+    loads = [A.Load(A.DIRICHLET, (0.0,))]
     dev = lambda a: torch.tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
-    d_u0, d_k = dev(u0), dev(m.cdiff)
+    d_u0, d_k = dev(rng.standard_normal(m.numel)), dev(m.cdiff)
     d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
     d_r = torch.empty(m.numel, dtype=torch.float64, device="cuda")
-    st = torch.cuda.Stream()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def call():
         plan.assemble_device(loads, d_u0.data_ptr(), d_k.data_ptr(), d_b=d_b.data_ptr(),
-                             d_rcell=d_r.data_ptr(), stream=st.cuda_stream)
-    reps = 10
+                             d_rcell=d_r.data_ptr(), stream=stream)
+
+    def close():
+        plan.close()
+        g.close()
+    return call, close
+
+
+# the SIMPLE pressure correction on the same mesh: a lid-driven cavity's
+# loads (static walls, the z-max lid moving) with the pressure fixed on x = 0
+PRES_SIDES_VEL = [2, 2, 2, 2, 2, 1]
+PRES_SIDES_PRES = [1, 0, 0, 0, 0, 0]
+
+
+def pres_inputs(np, s):
+    m = s.mesh()
+    rng = np.random.default_rng(10)
+    prop = np.zeros((1, 10))
+    prop[0, 1] = 1.0
+    return m, prop, dict(pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         dfield=rng.uniform(0.5, 1.0, (m.numel, 3)))
+
+
+def pres_call_setup(np, torch, sv, s, stream):
+    """A device systFormSimplePres call on the system's mesh: (call, close)."""
+    from sfr3d_b200 import assembly as A
+    m, prop, f = pres_inputs(np, s)
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    plan = A.PresPlan(g, m, m.face_r(PRES_SIDES_PRES), m.face_r(PRES_SIDES_VEL),
+                      icod=A.ORTHOGONAL)
+    lvel = [A.Load(A.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), A.Load(A.STATICWALL, ())]
+    lpres = [A.Load(A.DIRICHLET, (0.0,))]
+    dev = {k: torch.tensor(np.ascontiguousarray(v), device="cuda") for k, v in f.items()}
+    d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
+    d_r = torch.empty(m.numel, dtype=torch.float64, device="cuda")
+
+    def call():
+        plan.assemble_device(lvel, lpres, prop, dev["pres"].data_ptr(),
+                             dev["gradpres"].data_ptr(), dev["vel"].data_ptr(),
+                             dev["dfield"].data_ptr(), d_b=d_b.data_ptr(),
+                             d_rcell=d_r.data_ptr(), stream=stream)
+
+    def close():
+        plan.close()
+        g.close()
+    return call, close
+
+
+def time_calls(torch, call, st, reps=10):
+    """Median device time of `call` (CUDA events on st, L2 flushed between)."""
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     with torch.cuda.stream(st):
         for _ in range(3):
             call()
@@ -617,14 +666,32 @@ def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
             call()
             ev[2 * i + 1].record(st)
     st.synchronize()
-    dev_ms = sorted(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps))[reps // 2]
+    return sorted(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps))[reps // 2]
+
+
+def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
+    """systFormDif on the device for the 128^3 pressure mesh (ORTHOGONAL,
+    Dirichlet on x = 0, Neumann elsewhere, residual form): one call writes
+    A (CSRD) and b where the next solve reads them.  Beside it: the per-call
+    upload of A and b the host-assembled path needs, and the host-array
+    entry point (fields in, b and rCell out)."""
+    from sfr3d_b200 import assembly as A
+    st = torch.cuda.Stream()
+    t0 = time.perf_counter()
+    call, close = dif_call_setup(np, torch, sv, s, st.cuda_stream)
+    torch.cuda.synchronize()
+    plan_s = time.perf_counter() - t0
+    dev_ms = time_calls(torch, call, st)
+    close()
     alg = ASSEMBLY_ALG_BYTES_PER_ROW * s.neq
+    reps = 10
     # the host-assembled path: A (al, ad) and b uploaded every call
     h_al = torch.from_numpy(s.al).pin_memory()
     h_ad = torch.from_numpy(s.ad).pin_memory()
     h_b = torch.from_numpy(s.b[0]).pin_memory()
     d_al = torch.empty_like(h_al, device="cuda")
     d_ad = torch.empty_like(h_ad, device="cuda")
+    d_b = torch.empty_like(h_b, device="cuda")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(reps):
@@ -634,6 +701,11 @@ def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
     torch.cuda.synchronize()
     upload_ms = (time.perf_counter() - t0) * 1e3 / reps
     # the host-array entry point: u0 and the diffusivity in, b and rCell out
+    m = s.mesh()
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    plan = A.DifPlan(g, m, m.face_r([1, 0, 0, 0, 0, 0]), icod=A.ORTHOGONAL)
+    u0 = np.random.default_rng(9).standard_normal(m.numel)
+    loads = [A.Load(A.DIRICHLET, (0.0,))]
     plan.assemble(loads, u0, m.cdiff)
     t0 = time.perf_counter()
     for _ in range(3):
@@ -657,6 +729,29 @@ def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
                         "(pageable numpy)"}
 
 
+# algorithmic bytes per row of the ORTHOGONAL pressure-correction kernel
+# (6 faces, CSRD full): row header 6, per face the plan words (12) and 9
+# geometry doubles (72), the cell's own pres, gradpres, vel, dfield and
+# material (10 doubles + 2), the writes of the diffusion kernel (156).
+PRES_ALG_BYTES_PER_ROW = 6 + 6 * (12 + 72) + 82 + 6 * 20 + 36
+
+
+def pressure_leg(np, torch, sv, s, n, peak, peak_kind):
+    """systFormSimplePres on the device for the same mesh (lid-driven cavity
+    loads, pressure fixed on x = 0, ORTHOGONAL, CSRD)."""
+    st = torch.cuda.Stream()
+    call, close = pres_call_setup(np, torch, sv, s, st.cuda_stream)
+    dev_ms = time_calls(torch, call, st)
+    close()
+    alg = PRES_ALG_BYTES_PER_ROW * s.neq
+    gbs = alg / (dev_ms * 1e-3) / 1e9
+    return {"workload": f"systFormSimplePres, {n}^3 = {s.neq} cells, cavity loads (static "
+                        "walls, moving lid), pressure fixed on x=0, ORTHOGONAL, CSRD",
+            "device_ms": dev_ms, "alg_bytes_per_row": PRES_ALG_BYTES_PER_ROW,
+            "GB/s": gbs, "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "kernel": "pres_assemble_kernel<orthogonal, 6 faces, fused>"}
+
+
 def cpu_assembly(O, s):
     """The reference's own systFormDif (serial, as the reference runs it) on
     the assembly leg's workload."""
@@ -668,8 +763,20 @@ def cpu_assembly(O, s):
                      cdiff=m.cdiff, u0=rng.standard_normal(m.numel),
                      gradu0=np.zeros((m.numel, 3)), icod=O.ORTHOGONAL)
     rc, *_, sec = O.ref_dif_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    m, prop, f = pres_inputs(np, s)
+    pcase = O.PresCase(mesh=m, facevelr=m.face_r(PRES_SIDES_VEL),
+                       facepresr=m.face_r(PRES_SIDES_PRES),
+                       lvel=[O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0)),
+                             O.Load(O.STATICWALL, ())],
+                       lpres=[O.Load(O.DIRICHLET, (0.0,))], prop=prop, **f)
+    threads = os.cpu_count() or 1
+    prc, *_, psec = O.ref_pres_assemble(pcase, O.CSRD, True, s.ia, s.ja, s.neq,
+                                        nthreads=threads)
     return {"ms": sec * 1e3, "threads": 1, "status": rc,
-            "sample": "one full systFormDif call (the reference's loop is serial)"}
+            "sample": "one full systFormDif call (the reference's loop is serial)",
+            "pressure": {"ms": psec * 1e3, "threads": threads, "status": prc,
+                         "sample": "one full systFormSimplePres call with its OpenMP cell "
+                                   "loop on all host threads"}}
 
 
 def adjoint_leg(np, sv, S):

@@ -268,11 +268,14 @@ typedef struct {
 
 /* One entry of the load table (Loads, StructDefine.h:356-366). */
 typedef struct {
-  int32_t type;   /* DIRICHLETBC 1, NEUMANNBC 2, ROBINBC 3, INLET 6 (Define.h:317-323) */
+  int32_t type;   /* DIRICHLETBC 1, NEUMANNBC 2, ROBINBC 3, INLET 6, OUTLET 7,
+                   * MOVEWALL 8, INLETSTAICTPRES 9, OPEN 10, INLETTOTALPRES 13,
+                   * STATICWALL 14, FLUXPRES 15 (Define.h:317-332) */
   int32_t var;    /* nTypeVar: 0 constant (1 = function: SFR_UNSUPPORTED) */
   int32_t np;     /* parameters given */
   int32_t pad;
   double par[20]; /* MAXLOADPARAMETER */
+  double density; /* Loads.density (an OPEN velocity load's inflow density) */
 } sfr_load;
 
 /* The rest of what systFormDif reads (Diffusion.iCod, DiffModel.fRes,
@@ -319,8 +322,39 @@ int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
                          const double *u0, const double *gradu0, const double *b0, double *b,
                          double *rcell, int32_t forces, int32_t matrix, int32_t calrcell);
 
-/* Frees the plan; safe after the system is destroyed (the plan's calls are
- * not). */
+/* ---- device assembly of the SIMPLE pressure correction ---------------- */
+/* systFormSimplePres (CellLoopInc.c:471-700) -> cellSimplePres3D
+ * (CellPres.c:903-1218): face coefficients rho_f |E_f| / |ksi| from the
+ * momentum D field, the Rhie-Chow face mass fluxes as the force, pressure
+ * loads (pLoadSimplePres) and velocity loads (pLoadSimple, pressure part),
+ * serial and without a wall model, as velPresCoupling builds it.  mesh->facer
+ * is facePresR; facevelr (numel*(maxviz+1)) is faceVelR.  icod is the
+ * pressure scheme: 1 ORTHOGONAL or 4 OVERRELAXED (the reference's split sets
+ * nothing for the other two). */
+int sfr_gpu_pres_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr,
+                             int32_t icod, sfr_dif_plan **out);
+
+/* One systFormSimplePres call on device arrays: pres (numel), gradpres, vel
+ * and dfield (numel*3) in; b and rcell (the cell mass residual) out.  prop
+ * is the host material table, nmat x MAXPROP (10) doubles, density in
+ * column 1.  lvel / lpres: at most 32 entries each.  INLET velocity loads
+ * given as functions are SFR_UNSUPPORTED. */
+int sfr_gpu_pres_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                                 const sfr_load *lpres, int32_t nlpres, const double *prop,
+                                 const double *d_pres, const double *d_gradpres,
+                                 const double *d_vel, const double *d_dfield, double *d_b,
+                                 double *d_rcell, int32_t forces, int32_t matrix,
+                                 int32_t calrcell, void *stream);
+
+/* The same with host arrays (b and rcell copied back when not NULL). */
+int sfr_gpu_pres_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                          const sfr_load *lpres, int32_t nlpres, const double *prop,
+                          const double *pres, const double *gradpres, const double *vel,
+                          const double *dfield, double *b, double *rcell, int32_t forces,
+                          int32_t matrix, int32_t calrcell);
+
+/* Frees a plan (either kind); safe after the system is destroyed (the
+ * plan's calls are not). */
 int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
 
 /* Copy the system's values back in the reference's layout: al (nad, or the

@@ -221,6 +221,8 @@ def ell_ia(neq: int, width: int) -> np.ndarray:
 # systFormDif (CellLoop.c:285-455) -> cellDif3D (CellDif.c:312-537)
 MAXLOADPAR = 20                                   # Define.h:336
 DIRICHLET, NEUMANN, ROBIN, SINBC, INLET, OUTLET = 1, 2, 3, 4, 6, 7  # Define.h:317-323
+MOVEWALL, INLETSTAICTPRES, OPEN, INLETTOTALPRES, STATICWALL, FLUXPRES = 8, 9, 10, 13, 14, 15
+MAXPROP, DENSITY = 10, 1                                           # Define.h:349, 203
 ORTHOGONAL, MINIMAL, ORTHOGONALC, OVERRELAXED = 1, 2, 3, 4        # Define.h:304-307
 EULER, BACKWARD = 0, 1                                             # Define.h:191-192
 
@@ -233,6 +235,7 @@ class Load:
     par: tuple = ()
     var: int = 0
     np: int | None = None
+    density: float = 0.0
 
     def arrays(self):
         par = np.zeros(MAXLOADPAR)
@@ -294,7 +297,27 @@ class _DifMesh(ctypes.Structure):
 
 class _DifLoad(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int), ("var", ctypes.c_int), ("np", ctypes.c_int),
-                ("par", ctypes.c_double * MAXLOADPAR)]
+                ("par", ctypes.c_double * MAXLOADPAR), ("density", ctypes.c_double)]
+
+
+def _load_table(loads):
+    arr = (_DifLoad * max(len(loads), 1))()
+    for i, ld in enumerate(loads):
+        t, v, npar, par = ld.arrays()
+        arr[i].type, arr[i].var, arr[i].np = int(t), int(v), int(npar)
+        arr[i].par[:] = list(par)
+        arr[i].density = ld.density
+    return arr
+
+
+def _load_arrays(loads):
+    n = max(len(loads), 1)
+    t, v, npar = (np.zeros(n, np.int32) for _ in range(3))
+    par, dens = np.zeros((n, MAXLOADPAR)), np.zeros(n)
+    for i, ld in enumerate(loads):
+        t[i], v[i], npar[i], par[i] = ld.arrays()
+        dens[i] = ld.density
+    return t, v, npar, par, dens
 
 
 class _DifOpts(ctypes.Structure):
@@ -331,11 +354,7 @@ def dif_assemble(case: DifCase, storage, unsym, ia, ja, neq, forces=True,
         caltype=cal, mat=mat, id=_c(m.id, np.int32), facer=_c(case.facer, np.int16))
     dm = _DifMesh(numel=m.numel, maxviz=m.nelcon.shape[1],
                   **{k: _p(v) for k, v in keep.items()})
-    t, v, npar, par = case.load_arrays()
-    loads = (_DifLoad * len(t))()
-    for i in range(len(t)):
-        loads[i].type, loads[i].var, loads[i].np = int(t[i]), int(v[i]), int(npar[i])
-        loads[i].par[:] = list(par[i])
+    loads = _load_table(case.loads)
     o = _DifOpts(icod=case.icod, fres=int(case.fres), time_flag=int(case.time_flag),
                  time_type=case.time_type, dt=case.dt, dt0=case.dt0)
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
@@ -382,4 +401,107 @@ def ref_dif_assemble(case: DifCase, storage, unsym, ia, ja, neq, forces=True,
         _p(t), _p(v), _p(npar), _p(par), case.icod, int(case.fres),
         int(case.time_flag), case.time_type, case.dt, case.dt0, neq, nad, storage,
         int(forces), int(matrix), int(calrcell), int(unsym), ctypes.byref(sec))
+    return rc, a, ad, b, rcell, sec.value
+
+
+# ------------------------------------------ pressure-correction assembly --
+# systFormSimplePres (CellLoopInc.c:471-700) -> cellSimplePres3D (CellPres.c:903)
+@dataclass
+class PresCase:
+    """Everything one systFormSimplePres call reads besides the pattern: the
+    mesh arrays, faceVelR / facePresR, the two load tables, the material
+    table prop (nmat x MAXPROP, density in column DENSITY), and the cell
+    fields pres, gradPres, vel and dField (the momentum D, 3 per cell)."""
+    mesh: object
+    facevelr: np.ndarray
+    facepresr: np.ndarray
+    lvel: list
+    lpres: list
+    prop: np.ndarray
+    pres: np.ndarray
+    gradpres: np.ndarray
+    vel: np.ndarray
+    dfield: np.ndarray
+    icod: int = ORTHOGONAL
+    mat: np.ndarray | None = None
+    caltype: np.ndarray | None = None
+
+    def material(self):
+        mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
+               else _c(self.mat, np.int16))
+        nmat = len(np.asarray(self.prop).reshape(-1, MAXPROP))
+        cal = np.ones(nmat, np.int16) if self.caltype is None else _c(self.caltype, np.int16)
+        return cal, mat
+
+
+def pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
+                  matrix=True, calrcell=True, fill=0.0):
+    """The C restatement of systFormSimplePres: (rc, a, ad, b, rcell)."""
+    m = case.mesh
+    lib = oracle_lib()
+    if not getattr(lib, "_pres_typed", False):
+        lib.orc_pres_assemble.restype = ctypes.c_int
+        lib.orc_pres_assemble.argtypes = (
+            [ctypes.POINTER(_DifMesh), _P, _P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int]
+            + [_P] * 5 + [ctypes.c_int] * 4 + [_P] * 6 + [ctypes.c_int] * 3)
+        lib._pres_typed = True
+    cal, mat = case.material()
+    keep = dict(
+        nelcon=_c(m.nelcon, np.int32), nface=_c(m.nviz, np.int16),
+        cellface=_c(m.cellface, np.int32), owner=_c(m.owner, np.int32),
+        volume=_c(m.volume, np.float64), dcca=_c(m.dcca, np.float64),
+        xmcc=_c(m.xmcc, np.float64), mksi=_c(m.mksi, np.float64),
+        ksi=_c(m.ksi, np.float64), area=_c(m.area, np.float64),
+        normal=_c(m.normal, np.float64), vskew=_c(m.vskew, np.float64),
+        caltype=cal, mat=mat, id=_c(m.id, np.int32), facer=_c(case.facepresr, np.int16))
+    dm = _DifMesh(numel=m.numel, maxviz=m.nelcon.shape[1],
+                  **{k: _p(v) for k, v in keep.items()})
+    fvr = _c(case.facevelr, np.int16)
+    lv, lp = _load_table(case.lvel), _load_table(case.lpres)
+    ia, ja = _c(ia, np.int32), _c(ja, np.int32)
+    a, ad, b, rc_ = _dif_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    fields = [_c(case.prop, np.float64), _c(case.pres, np.float64),
+              _c(case.gradpres, np.float64), _c(case.vel, np.float64),
+              _c(case.dfield, np.float64)]
+    nad = len(ja) if storage != ELLPACK else 0
+    rc = lib.orc_pres_assemble(ctypes.byref(dm), _p(fvr), lv, len(case.lvel), lp,
+                               len(case.lpres), case.icod, *[_p(f) for f in fields],
+                               storage, int(unsym), neq, nad, _p(ia), _p(ja), _p(a), _p(ad),
+                               _p(b), _p(rc_), int(forces), int(matrix), int(calrcell))
+    return rc, a, ad, b, rc_
+
+
+def ref_pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
+                      matrix=True, calrcell=True, fill=0.0, nthreads=0):
+    """The reference's own systFormSimplePres: (rc, a, ad, b, rcell, seconds)."""
+    m = case.mesh
+    lib = ref_lib()
+    if not getattr(lib, "_pres_typed", False):
+        lib.sfr_ref_syst_form_simple_pres.restype = ctypes.c_int
+        lib.sfr_ref_syst_form_simple_pres.argtypes = (
+            [ctypes.c_int, ctypes.c_int] + [_P] * 31 + [ctypes.c_int] + [_P] * 5
+            + [ctypes.c_int] + [_P] * 5 + [ctypes.c_int] * 9 + [_P])
+        lib._pres_typed = True
+    cal, mat = case.material()
+    cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
+    ia, ja = cp(ia, np.int32), cp(ja, np.int32)
+    a, ad, b, rcell = _dif_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    vt = _load_arrays(case.lvel)
+    pt = _load_arrays(case.lpres)
+    sec = ctypes.c_double()
+    arrs = [cp(m.nelcon, np.int32), cp(m.nviz, np.int16), cp(m.cellface, np.int32),
+            cp(m.owner, np.int32), cp(m.volume, np.float64), cp(m.dcca, np.float64),
+            cp(m.xmcc, np.float64), cp(m.mksi, np.float64), cp(m.ksi, np.float64),
+            cp(m.eta, np.float64), cp(m.area, np.float64), cp(m.normal, np.float64),
+            cp(m.xm, np.float64), cp(m.mvskew, np.float64), cp(m.vskew, np.float64),
+            cal.copy(), mat.copy(), cp(case.prop, np.float64), ia, ja, a, ad, b,
+            cp(m.id, np.int32), cp(case.facevelr, np.int16), cp(case.facepresr, np.int16),
+            cp(case.pres, np.float64), cp(case.gradpres, np.float64),
+            cp(case.vel, np.float64), cp(case.dfield, np.float64), rcell]
+    nad = len(ja) if storage != ELLPACK else int(ia[1])
+    rc = lib.sfr_ref_syst_form_simple_pres(
+        m.numel, m.nelcon.shape[1], *[_p(x) for x in arrs],
+        len(case.lvel), *[_p(x) for x in vt], len(case.lpres), *[_p(x) for x in pt],
+        case.icod, neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym),
+        nthreads, ctypes.byref(sec))
     return rc, a, ad, b, rcell, sec.value

@@ -229,3 +229,96 @@ int sfr_ref_syst_form_dif(int numel, int maxviz, int *nelcon, short *nface,
   free(gtype);
   return rc;
 }
+
+static void fill_loads(Loads *dst, int n, const int *type, const int *var, const int *np,
+                       const double *par, const double *density)
+{
+  int i, j;
+  for (i = 0; i < n; i++) {
+    memset(&dst[i], 0, sizeof(Loads));
+    dst[i].fUse = true;
+    dst[i].type = (short)type[i];
+    dst[i].nTypeVar = (short)var[i];
+    dst[i].np = (short)np[i];
+    dst[i].density = density[i];
+    for (j = 0; j < MAXLOADPARAMETER; j++) dst[i].par[j] = par[i * MAXLOADPARAMETER + j];
+  }
+}
+
+/*
+ * Assemble the SIMPLE pressure-correction system with the reference's own
+ * systFormSimplePres (CellLoopInc.c:471-700), no wall model, as
+ * velPresCoupling calls it; nthreads > 1 turns on its OpenMP cell loop.  cellSimplePres3D reads the velocity loads from
+ * the global loadsVel table (CellPres.c, pLoadSimple call), so they are
+ * copied there as well as passed.  Mesh arrays as for systFormDif; prop is
+ * the nmat x MAXPROP material table.
+ */
+int sfr_ref_syst_form_simple_pres(int numel, int maxviz, int *nelcon, short *nface,
+                                  int *cellface, int *owner, double *volume,
+                                  double *dcca, double *xmcc, double *mksi,
+                                  double *ksi, double *eta, double *area,
+                                  double *normal, double *xm, double *mvskew,
+                                  double *vskew, short *caltype, short *mat,
+                                  double *prop, int *ia, int *ja, double *a,
+                                  double *ad, double *b, int *id, short *facevelr,
+                                  short *facepresr, double *pres, double *gradpres,
+                                  double *vel, double *dfield, double *rcell,
+                                  int nlvel, const int *vtype, const int *vvar,
+                                  const int *vnp, const double *vpar,
+                                  const double *vdens, int nlpres,
+                                  const int *ptype, const int *pvar, const int *pnp,
+                                  const double *ppar, const double *pdens, int icod,
+                                  int neq, int nad, int storage, int forces,
+                                  int matrix, int calrcell, int unsym,
+                                  int nthreads, double *seconds)
+{
+  Loads *lp = calloc(nlpres > 0 ? nlpres : 1, sizeof(Loads));
+  INT *el = calloc((size_t)numel * 8, sizeof(INT));
+  short *nen = malloc((size_t)numel * sizeof(short));
+  short *gtype = calloc((size_t)numel, sizeof(short));
+  double *cc = calloc((size_t)numel * 3, sizeof(double));
+  double *wallpar = calloc((size_t)numel * NWALLPAR, sizeof(double));
+  Diffusion diff;
+  Turbulence tmodel;
+  Temporal ddt;
+  int i, rc = 0;
+  double t0;
+
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  mpiVar.nPrcs = 1;
+  mpiVar.myId = 0;
+  ompVar.fCell = nthreads > 1;
+  ompVar.nThreadsCell = (short)(nthreads > 1 ? nthreads : 1);
+  for (i = 0; i < numel; i++) nen[i] = 8;
+  fill_loads(loadsVel, nlvel, vtype, vvar, vnp, vpar, vdens);
+  fill_loads(lp, nlpres, ptype, pvar, pnp, ppar, pdens);
+  memset(&diff, 0, sizeof(diff));
+  memset(&tmodel, 0, sizeof(tmodel));
+  memset(&ddt, 0, sizeof(ddt));
+  diff.iCod = (short)icod;
+  tmodel.fWall = false;
+  *seconds = 0.0;
+  if (setjmp(g_jump) == 0) {
+    g_armed = 1;
+    t0 = omp_get_wtime();
+    systFormSimplePres(loadsVel, lp, &diff, &tmodel, el, nelcon, nen, nface, cellface,
+                       owner, volume, dcca, xmcc, cc, mksi, ksi, eta, area, normal, xm,
+                       mvskew, vskew, gtype, prop, caltype, mat, ia, ja, a, ad, b, id,
+                       facevelr, facepresr, pres, gradpres, vel, dfield, wallpar, rcell,
+                       &ddt, neq, neq, nad, 0, 8, (short)maxviz, 3, numel, 1,
+                       (short)storage, forces != 0, matrix != 0, calrcell != 0,
+                       unsym != 0);
+    *seconds = omp_get_wtime() - t0;
+    g_armed = 0;
+  } else {
+    rc = g_exit_code == 0 ? -1000 : g_exit_code;
+  }
+  free(lp);
+  free(el);
+  free(nen);
+  free(gtype);
+  free(cc);
+  free(wallpar);
+  return rc;
+}

@@ -750,3 +750,233 @@ int orc_dif_assemble(const orc_dif_mesh *m, const orc_load *loads, int nloads,
   }
   return 0;
 }
+
+/* ======================================================================
+ * Pressure-correction assembly: systFormSimplePres (CellLoopInc.c:471-700)
+ * calling cellSimplePres3D (CellPres.c:903-1218) per cell.
+ * ====================================================================== */
+
+/* difusionSchemeAnisotropic, ndm = 3 (CellLib.c:6054-6170): only ORTHOGONAL
+ * and OVERRELAXED set e and t */
+static int pres_scheme(const double s[3], const double k[3], double e[3], double t[3], int icod)
+{
+  double ss, nk, tmp;
+  int j;
+  if (icod == 1) {
+    ss = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (j = 0; j < 3; j++) { e[j] = ss * k[j]; t[j] = 0.0; }
+    return 0;
+  }
+  if (icod == 4) {
+    ss = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+    nk = s[0] * k[0] + s[1] * k[1] + s[2] * k[2];
+    tmp = ss / nk;
+    for (j = 0; j < 3; j++) e[j] = tmp * k[j];
+    for (j = 0; j < 3; j++) t[j] = s[j] - e[j];
+    return 0;
+  }
+  return -1;
+}
+
+static double dot3c(const double a[3], const double b[3])
+{
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+/* pLoadSimplePres with fCal, no buoyancy (Loads.c:728-845): the pressure
+ * load's share of the diagonal */
+static int pres_load(const orc_load *ld, double *sP, const double e[3], const double n[3],
+                     const double velC[3], double rhoC, double area, double dd)
+{
+  double tmp0, tmp1, modE, dc, m, modVel, rhoEnv;
+  tmp0 = e[0] * e[0] + e[1] * e[1];
+  tmp0 += e[2] * e[2];
+  modE = sqrt(tmp0);
+  switch (ld->type) {
+  case 1: /* DIRICHLETBC */
+    *sP += rhoC * modE / dd;
+    return 0;
+  case 13: /* INLETTOTALPRES: par = density, total pressure, direction
+            * (getLoads copies the first five whatever np says) */
+    rhoEnv = ld->par[0];
+    dc = modE / dd;
+    tmp0 = velC[0] * n[0] + velC[1] * n[1] + velC[2] * n[2];
+    tmp1 = (ld->par[2] * n[0] + ld->par[3] * n[1] + ld->par[4] * n[2]) * area;
+    m = rhoEnv * tmp0 * area;
+    modVel = m / (rhoEnv * tmp1);
+    tmp0 = rhoEnv * modVel;
+    tmp1 = m - dc * tmp0 * tmp0;
+    *sP += rhoEnv * m * dc / tmp1;
+    return 0;
+  case 10: /* OPEN: outflow only, added twice as the reference does */
+    tmp0 = velC[0] * n[0] + velC[1] * n[1];
+    tmp0 += velC[2] * n[2];
+    if (tmp0 > 0.e0) {
+      *sP += rhoC * modE / dd;
+      *sP += rhoC * modE / dd;
+    }
+    return 0;
+  }
+  return 0; /* FLUXPRES without buoyancy and the other codes add nothing */
+}
+
+/* pLoadSimple with fCalVel = false, fCalPres = true (Loads.c:265-720): the
+ * velocity load's mass flux in the pressure equation */
+static int vel_load(const orc_load *ld, double *p, const double n[3], const double velC[3],
+                    double rhoC, double area)
+{
+  double wfn, m, rho;
+  switch (ld->type) {
+  case 9:  /* INLETSTAICTPRES */
+  case 7:  /* OUTLET */
+    wfn = velC[0] * n[0] + velC[1] * n[1] + velC[2] * n[2];
+    if (ld->type == 7) {
+      wfn = velC[0] * n[0] + velC[1] * n[1];
+      wfn += velC[2] * n[2];
+    }
+    m = rhoC * wfn * area;
+    *p -= m;
+    return 0;
+  case 6: /* INLET: par[0..2] velocity, par[np-1] density (getLoads copies
+           * np parameters) */
+    if (ld->var != 0) return -2;
+    if (ld->np < 3) return -1;
+    wfn = ld->par[0] * n[0] + ld->par[1] * n[1];
+    wfn += ld->par[2] * n[2];
+    m = ld->par[ld->np - 1] * wfn * area;
+    *p -= m;
+    return 0;
+  case 10: /* OPEN */
+    wfn = velC[0] * n[0] + velC[1] * n[1];
+    wfn += velC[2] * n[2];
+    rho = wfn >= 0.e0 ? rhoC : ld->density;
+    m = rho * wfn * area;
+    *p -= m;
+    return 0;
+  case 13: /* INLETTOTALPRES */
+    wfn = velC[0] * n[0] + velC[1] * n[1] + velC[2] * n[2];
+    m = ld->par[0] * wfn * area;
+    *p -= m;
+    return 0;
+  }
+  return 0; /* MOVEWALL, STATICWALL, ...: nothing in the pressure equation */
+}
+
+int orc_pres_assemble(const orc_dif_mesh *m, const short *facevelr,
+                      const orc_load *lvel, int nlvel, const orc_load *lpres,
+                      int nlpres, int icod, const double *prop,
+                      const double *pres, const double *gradpres,
+                      const double *vel, const double *dfield, int storage,
+                      int unsym, int neq, int nad, const int *ia,
+                      const int *ja, double *a, double *ad, double *b,
+                      double *rcell, int forces, int matrix, int calrcell)
+{
+  enum { MAXF = 32 };
+  const int mv = m->maxviz;
+  int nel, f, j, rc;
+  (void)neq;
+  if (mv < 1 || mv > MAXF - 1) return -1;
+  if (icod != 1 && icod != 4) return -1;
+  for (nel = 0; nel < m->numel; nel++) {
+    double lA[MAXF], ksi[3], nrm[3], s[3], e[3], t[3], dF[3], wf[3], gf[3], v[3];
+    int viz[MAXF], lid[MAXF];
+    const int nf = m->nface[nel];
+    const short *fr = m->facer + (long)nel * (mv + 1);
+    const short *fv = facevelr + (long)nel * (mv + 1);
+    const double *velC = vel + 3 * (long)nel, *gpC = gradpres + 3 * (long)nel;
+    const double *dC = dfield + 3 * (long)nel;
+    double p = 0.0, sP = 0.0, rhoC, presC;
+    int row, lm;
+    if (calrcell) rcell[nel] = 0.0;
+    if (nf < 1 || nf > mv) return -1;
+    if (fr[nf] > 0) continue; /* prescribed pressure: no equation */
+    lm = m->mat[nel] - 1;
+    if (m->caltype[lm] != 1) return -1;
+    row = m->id[nel] - 1;
+    rhoC = prop[lm * ORC_MAXPROP + ORC_DENSITY];
+    presC = pres[nel];
+    for (f = 0; f < nf; f++) {
+      const long q = (long)nel * mv + f;
+      const int face = m->cellface[q] - 1;
+      const double ch = (m->owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+      const double mk = m->mksi[face], area = m->area[face];
+      const double *xmcc = m->xmcc + 3 * q;
+      viz[f] = m->nelcon[q] - 1;
+      lid[f] = viz[f] != -2 ? m->id[viz[f]] - 1 : -1;
+      for (j = 0; j < 3; j++) {
+        ksi[j] = ch * m->ksi[3 * face + j];
+        nrm[j] = ch * m->normal[3 * face + j];
+      }
+      if (viz[f] > -1) {
+        const int nb = viz[f];
+        const double *velV = vel + 3 * (long)nb, *gpV = gradpres + 3 * (long)nb;
+        const double *dV = dfield + 3 * (long)nb;
+        const double rhoV = prop[(m->mat[nb] - 1) * ORC_MAXPROP + ORC_DENSITY];
+        double alpha, am1, rho, modE, dfd, wfn, nk, g0, g1;
+        /* interpolFace, INTPOLFACELINEAR (CellLib.c:7174-7200) */
+        for (j = 0; j < 3; j++) v[j] = m->vskew[3 * face + j] + xmcc[j];
+        alpha = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / mk;
+        am1 = 1.0e0 - alpha;
+        rho = am1 * rhoC + alpha * rhoV;
+        for (j = 0; j < 3; j++) dF[j] = am1 * dC[j] + alpha * dV[j];
+        for (j = 0; j < 3; j++) s[j] = dF[j] * area * nrm[j];
+        if (pres_scheme(s, ksi, e, t, icod)) return -1;
+        modE = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        dfd = rho * modE / mk;
+        lA[f] = dfd;
+        /* interpolFaceVel, ndm = 3 (CellLib.c:6853-6960): Rhie-Chow face
+         * velocity */
+        for (j = 0; j < 3; j++) wf[j] = am1 * velC[j] + alpha * velV[j];
+        wfn = dot3c(wf, nrm);
+        for (j = 0; j < 3; j++) gf[j] = am1 * gpC[j] + alpha * gpV[j];
+        g0 = (pres[nb] - presC) / mk;
+        nk = dF[0] * ksi[0] * nrm[0] + dF[1] * ksi[1] * nrm[1] + dF[2] * ksi[2] * nrm[2];
+        g1 = dot3c(gf, ksi);
+        g1 = (g1 - g0) * nk;
+        wfn += g1;
+        p -= rho * wfn * area;
+      } else {
+        lA[f] = 0.0;
+        if (fr[f]) {
+          const int l = fr[f] - 1;
+          if (l < 0 || l >= nlpres) return -1;
+          for (j = 0; j < 3; j++) s[j] = dC[j] * area * nrm[j];
+          if (pres_scheme(s, ksi, e, t, icod)) return -1;
+          rc = pres_load(&lpres[l], &sP, e, nrm, velC, rhoC, area, m->dcca[q]);
+          if (rc) return rc;
+        }
+        if (fv[f]) {
+          const int l = fv[f] - 1;
+          if (l < 0 || l >= nlvel) return -1;
+          rc = vel_load(&lvel[l], &p, nrm, velC, rhoC, area);
+          if (rc) return rc;
+        }
+      }
+    }
+    lA[nf] = sP;
+    for (f = 0; f < nf; f++) lA[nf] += lA[f];
+    for (f = 0; f < nf; f++) lA[f] *= -1.e0;
+    if (calrcell) rcell[nel] = p;
+    if (forces) b[row] = p;
+    if (!matrix) continue;
+    ad[row] = lA[nf];
+    if (storage == ORC_ELLPACK) {
+      const int w = ia[0];
+      for (f = 0; f < nf; f++) a[(long)row * w + f] = lA[f];
+      continue;
+    }
+    for (f = 0; f < nf; f++) {
+      const int c = lid[f];
+      if (c <= -1) continue;
+      if (storage == ORC_CSRC && unsym) {
+        if (c < row)
+          dif_put(ia, ja, row, c, a, lA[f]);
+        else if (c > row)
+          dif_put(ia, ja, c, row, a + nad, lA[f]);
+      } else {
+        dif_put(ia, ja, row, c, a, lA[f]);
+      }
+    }
+  }
+  return 0;
+}

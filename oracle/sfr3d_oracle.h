@@ -94,6 +94,7 @@ typedef struct {
 typedef struct {
   int type, var, np;
   double par[ORC_MAXLOADPAR];
+  double density;        /* Loads.density (OPEN inflow) */
 } orc_load;
 
 typedef struct {
@@ -117,5 +118,26 @@ int orc_dif_assemble(const orc_dif_mesh *m, const orc_load *loads, int nloads,
                      int nad, const int *ia, const int *ja, double *a,
                      double *ad, double *b, double *rcell, int forces,
                      int matrix, int calrcell);
+
+/* ---- pressure-correction assembly (systFormSimplePres,
+ *      CellLoopInc.c:471-700 -> cellSimplePres3D, CellPres.c:903-1218) ---- */
+
+#define ORC_MAXPROP 10 /* Define.h:349 */
+#define ORC_DENSITY 1  /* Define.h:203 */
+
+/* m->facer is facePresR (pressure loads); facevelr the velocity loads
+ * (faceVelR), same shape.  prop: nmat x MAXPROP material table; pres
+ * (numel), gradpres, vel and dfield (numel x 3).  icod: 1 ORTHOGONAL or
+ * 4 OVERRELAXED (difusionSchemeAnisotropic leaves e and t unset for the
+ * other two).  Returns 0, -1 for input the reference cannot take, -2 for
+ * loads given as functions. */
+int orc_pres_assemble(const orc_dif_mesh *m, const short *facevelr,
+                      const orc_load *lvel, int nlvel, const orc_load *lpres,
+                      int nlpres, int icod, const double *prop,
+                      const double *pres, const double *gradpres,
+                      const double *vel, const double *dfield, int storage,
+                      int unsym, int neq, int nad, const int *ia,
+                      const int *ja, double *a, double *ad, double *b,
+                      double *rcell, int forces, int matrix, int calrcell);
 
 #endif

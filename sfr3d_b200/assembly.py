@@ -19,6 +19,8 @@ from . import solver as _sv
 # load types (Define.h:317-323), non-orthogonal schemes (Define.h:304-307),
 # time schemes (Define.h:191-192)
 DIRICHLET, NEUMANN, ROBIN, SINBC, INLET, OUTLET = 1, 2, 3, 4, 6, 7
+MOVEWALL, INLETSTAICTPRES, OPEN, INLETTOTALPRES, STATICWALL, FLUXPRES = 8, 9, 10, 13, 14, 15
+MAXPROP, DENSITY = 10, 1  # material table width and the density column (Define.h:349, 203)
 ORTHOGONAL, MINIMAL, ORTHOGONALC, OVERRELAXED = 1, 2, 3, 4
 EULER, BACKWARD = 0, 1
 MAXLOADPAR = 20   # MAXLOADPARAMETER, Define.h:336
@@ -38,7 +40,7 @@ class DifMeshC(ctypes.Structure):
 
 class LoadC(ctypes.Structure):
     _fields_ = [("type", _I32), ("var", _I32), ("np", _I32), ("pad", _I32),
-                ("par", ctypes.c_double * MAXLOADPAR)]
+                ("par", ctypes.c_double * MAXLOADPAR), ("density", ctypes.c_double)]
 
 
 class DifOptsC(ctypes.Structure):
@@ -57,6 +59,11 @@ def _lib():
         L.sfr_gpu_dif_assemble_device.argtypes = (
             [_P, _P, _I32, ctypes.POINTER(DifOptsC)] + [_P] * 7 + [_I32] * 3 + [_P])
         L.sfr_gpu_dif_update_cells.argtypes = [_P, _P, _P, _I32, _P]
+        L.sfr_gpu_pres_plan_create.argtypes = [_P, ctypes.POINTER(DifMeshC), _P, _I32,
+                                               ctypes.POINTER(_P)]
+        L.sfr_gpu_pres_assemble.argtypes = [_P, _P, _I32, _P, _I32] + [_P] * 7 + [_I32] * 3
+        L.sfr_gpu_pres_assemble_device.argtypes = ([_P, _P, _I32, _P, _I32] + [_P] * 7
+                                                   + [_I32] * 3 + [_P])
         L.sfr_gpu_dif_plan_destroy.argtypes = [_P]
         L.sfr_gpu_get_values.argtypes = [_P, _P, _P, _P]
         L._dif_typed = True
@@ -70,6 +77,7 @@ class Load:
     par: tuple = ()
     var: int = 0
     np: int | None = None
+    density: float = 0.0
 
 
 def _loads_c(loads):
@@ -82,6 +90,7 @@ def _loads_c(loads):
         arr[i].np = len(ld.par) if ld.np is None else ld.np
         for j, v in enumerate(ld.par):
             arr[i].par[j] = v
+        arr[i].density = ld.density
     return arr
 
 
@@ -91,6 +100,28 @@ def _c(a, dt):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(_P)
+
+
+def _mesh_c(mesh, facer, caltype, mat, nmat=None):
+    """The sfr_dif_mesh struct of a mesh object (and the arrays it points
+    to, which the caller keeps alive for the call)."""
+    numel = int(mesh.numel)
+    if caltype is None:
+        caltype = np.ones(nmat or 1, np.int16)
+    cal = _c(caltype, np.int16)
+    mt = np.ones(numel, np.int16) if mat is None else _c(mat, np.int16)
+    keep = dict(
+        nelcon=_c(mesh.nelcon, np.int32), nviz=_c(mesh.nviz, np.int16),
+        cellface=_c(mesh.cellface, np.int32), owner=_c(mesh.owner, np.int32),
+        volume=_c(mesh.volume, np.float64), dcca=_c(mesh.dcca, np.float64),
+        xmcc=_c(mesh.xmcc, np.float64), mksi=_c(mesh.mksi, np.float64),
+        ksi=_c(mesh.ksi, np.float64), area=_c(mesh.area, np.float64),
+        normal=_c(mesh.normal, np.float64), vskew=_c(mesh.vskew, np.float64),
+        caltype=cal, mat=mt, id=_c(mesh.id, np.int32), facer=_c(facer, np.int16))
+    m = DifMeshC(numel=numel, maxviz=int(keep["nelcon"].size // numel),
+                 nfaces=int(mesh.mksi.shape[0]), nmat=int(cal.size),
+                 **{k: _ptr(v) for k, v in keep.items()})
+    return m, keep
 
 
 class DifPlan:
@@ -109,19 +140,7 @@ class DifPlan:
         self.numel = int(mesh.numel)
         self.neq = system.neq
         self.icod = icod
-        cal = np.ones(1, np.int16) if caltype is None else _c(caltype, np.int16)
-        mt = np.ones(self.numel, np.int16) if mat is None else _c(mat, np.int16)
-        keep = dict(
-            nelcon=_c(mesh.nelcon, np.int32), nviz=_c(mesh.nviz, np.int16),
-            cellface=_c(mesh.cellface, np.int32), owner=_c(mesh.owner, np.int32),
-            volume=_c(mesh.volume, np.float64), dcca=_c(mesh.dcca, np.float64),
-            xmcc=_c(mesh.xmcc, np.float64), mksi=_c(mesh.mksi, np.float64),
-            ksi=_c(mesh.ksi, np.float64), area=_c(mesh.area, np.float64),
-            normal=_c(mesh.normal, np.float64), vskew=_c(mesh.vskew, np.float64),
-            caltype=cal, mat=mt, id=_c(mesh.id, np.int32), facer=_c(facer, np.int16))
-        m = DifMeshC(numel=self.numel, maxviz=int(keep["nelcon"].size // self.numel),
-                     nfaces=int(mesh.mksi.shape[0]), nmat=int(cal.size),
-                     **{k: _ptr(v) for k, v in keep.items()})
+        m, keep = _mesh_c(mesh, facer, caltype, mat)
         h = _P()
         rc = _lib().sfr_gpu_dif_plan_create(system.h, ctypes.byref(m), icod,
                                             ctypes.byref(h))
@@ -191,6 +210,68 @@ class DifPlan:
         rc = _lib().sfr_gpu_dif_update_cells(self.h, d_x, d_u, int(add), stream or None)
         if rc != _sv.OK:
             raise _sv.SolverError(rc, "sfr_gpu_dif_update_cells")
+
+
+class PresPlan(DifPlan):
+    """A mesh bound to a resident system for device-side systFormSimplePres
+    (the SIMPLE pressure correction, CellLoopInc.c:471).  facepresr /
+    facevelr are the reference's facePresR / faceVelR, (numel, maxviz + 1)
+    shorts; mat is the material of each cell (1-based) and nmat the number of
+    materials in the prop table.  icod: ORTHOGONAL or OVERRELAXED."""
+
+    def __init__(self, system: "_sv.GpuSystem", mesh, facepresr, facevelr,
+                 icod: int = ORTHOGONAL, mat=None, nmat: int = 1, caltype=None):
+        self.system = system
+        self.numel = int(mesh.numel)
+        self.neq = system.neq
+        self.icod = icod
+        self.nmat = nmat
+        m, keep = _mesh_c(mesh, facepresr, caltype, mat, nmat)
+        fv = _c(facevelr, np.int16)
+        h = _P()
+        rc = _lib().sfr_gpu_pres_plan_create(system.h, ctypes.byref(m), _ptr(fv), icod,
+                                             ctypes.byref(h))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_pres_plan_create: " + _sv.last_error())
+        self.h = h
+
+    def _prop(self, prop):
+        prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
+        if prop.shape[0] < self.nmat:
+            raise ValueError("prop has fewer rows than materials")
+        return prop
+
+    def assemble(self, lvel, lpres, prop, pres, gradpres, vel, dfield, forces=True,
+                 matrix=True, calrcell=True):
+        """One systFormSimplePres call with host arrays; returns (b, rcell)."""
+        prop = self._prop(prop)
+        arrs = [_c(a, np.float64) for a in (pres, gradpres, vel, dfield)]
+        b = np.empty(self.neq) if forces else None
+        rcell = np.empty(self.numel) if calrcell else None
+        lv, lp = _loads_c(lvel), _loads_c(lpres)
+        rc = _lib().sfr_gpu_pres_assemble(
+            self.h, lv, len(lvel), lp, len(lpres), _ptr(prop), *[_ptr(a) for a in arrs],
+            _ptr(b), _ptr(rcell), int(forces), int(matrix), int(calrcell))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_pres_assemble: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
+        return b, rcell
+
+    def assemble_device(self, lvel, lpres, prop, d_pres: int, d_gradpres: int, d_vel: int,
+                        d_dfield: int, d_b: int = 0, d_rcell: int = 0, forces=True,
+                        matrix=True, calrcell=True, stream: int = 0):
+        """The same on device pointers, asynchronous on `stream`."""
+        prop = self._prop(prop)
+        lv, lp = _loads_c(lvel), _loads_c(lpres)
+        rc = _lib().sfr_gpu_pres_assemble_device(
+            self.h, lv, len(lvel), lp, len(lpres), _ptr(prop), d_pres, d_gradpres, d_vel,
+            d_dfield, d_b or None, d_rcell or None, int(forces), int(matrix), int(calrcell),
+            stream or None)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_pres_assemble_device: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
 
 
 def get_values(system: "_sv.GpuSystem"):

@@ -72,6 +72,7 @@ struct MeshDev {
   int64_t nfaces;
   const int32_t *nelcon, *cellface, *owner, *id;
   const int16_t *nviz, *caltype, *mat, *facer;
+  const int16_t *facevelr;  // pressure plans: the velocity loads of each face
   const double *volume, *dcca, *xmcc, *mksi, *ksi, *area, *normal, *vskew;
 };
 
@@ -164,8 +165,14 @@ __device__ int real_slots(const PatternDev &P, int r) {
   return k;
 }
 
-__global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *err,
-                            unsigned *used_loads, int *free_cells, int *partial_rows) {
+// kind 0: diffusion (systFormDif) geometry [alpha, |E|, |ksi|, ksi, t];
+// kind 1: pressure correction (systFormSimplePres) [alpha, area, |ksi|, ksi,
+// normal], the anisotropic split being per call (it scales S by the face D).
+// Boundary slots: [area, dcca, 0, normal, 0] (kind 0), [area, dcca, 0, ksi,
+// normal] (kind 1).
+__global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int kind, int *err,
+                            unsigned *used_loads, int *free_cells, int *partial_rows,
+                            unsigned *used_vel_loads) {
   const int nel = blockIdx.x * blockDim.x + threadIdx.x;
   if (nel >= m.numel) return;
   const int mv = m.maxviz;
@@ -203,17 +210,26 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
     if (viz > -1) {
       if (viz >= m.numel) return flag_error(err, kErrNeighbour);
       const double area = m.area[face], mk = m.mksi[face];
-      double s[3], e[3], t[3], v[3];
-      for (int j = 0; j < 3; ++j) s[j] = xmul(area, nrm[j]);
-      dif_scheme(icod, s, ksi, e, t);
+      double v[3];
       // interpolFace, INTPOLFACELINEAR (CellLib.c:7174-7200)
       for (int j = 0; j < 3; ++j) v[j] = xadd(m.vskew[3 * face + j], m.xmcc[3 * q + j]);
       g[0] = xdiv(xsqrt(dot3(v, v)), mk);  // alpha
-      g[1] = xsqrt(dot3(e, e));             // |E|
       g[2] = mk;
-      for (int j = 0; j < 3; ++j) {
-        g[3 + j] = ksi[j];
-        g[6 + j] = t[j];
+      if (kind == 0) {
+        double s[3], e[3], t[3];
+        for (int j = 0; j < 3; ++j) s[j] = xmul(area, nrm[j]);
+        dif_scheme(icod, s, ksi, e, t);
+        g[1] = xsqrt(dot3(e, e));  // |E|
+        for (int j = 0; j < 3; ++j) {
+          g[3 + j] = ksi[j];
+          g[6 + j] = t[j];
+        }
+      } else {
+        g[1] = area;
+        for (int j = 0; j < 3; ++j) {
+          g[3 + j] = ksi[j];
+          g[6 + j] = nrm[j];
+        }
       }
       const int lid = m.id[viz] - 1;
       nbv = viz | (lid == -2 ? kFlagP : 0);
@@ -229,13 +245,24 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int *e
       const int ld = fr[f];
       if (ld < 0 || ld > kMaxLoads) return flag_error(err, kErrLoad);
       if (ld > 0) atomicOr(used_loads, 1u << (ld - 1));
-      nbv = ld > 0 ? -(ld - 1) - 2 : -1;
       g[0] = m.area[face];
       g[1] = m.dcca[q];
       g[2] = 0.0;
-      for (int j = 0; j < 3; ++j) {
-        g[3 + j] = nrm[j];
-        g[6 + j] = 0.0;
+      if (kind == 0) {
+        nbv = ld > 0 ? -(ld - 1) - 2 : -1;
+        for (int j = 0; j < 3; ++j) {
+          g[3 + j] = nrm[j];
+          g[6 + j] = 0.0;
+        }
+      } else {
+        const int lv = m.facevelr[static_cast<size_t>(nel) * (mv + 1) + f];
+        if (lv < 0 || lv > kMaxLoads) return flag_error(err, kErrLoad);
+        if (lv > 0) atomicOr(used_vel_loads, 1u << (lv - 1));
+        nbv = -2 - (ld | (lv << 6));  // both loads of the face, 0 = none
+        for (int j = 0; j < 3; ++j) {
+          g[3 + j] = ksi[j];
+          g[6 + j] = nrm[j];
+        }
       }
       if (P.storage == SFR_ELLPACK) {
         dst = row * P.width + f;
@@ -256,6 +283,8 @@ struct DevLoad {
   int32_t type;
   int32_t pad;
   double par[5];
+  double par_last;  // par[np - 1]
+  double density;   // Loads.density
 };
 
 struct CallOpts {
@@ -295,6 +324,38 @@ __device__ __forceinline__ void apply_load(const DevLoad &L, double kc, double a
     }
     default:
       break;  // codes pLoad does not test add nothing
+  }
+}
+
+// The row's coefficients (off-diagonals -la, diagonal d) where the reference's
+// csr()/ellPack() put them, and, fused, the value refresh for the row: SELL
+// values, their FP32 copy, the FP32 diagonal and the compensation summed in
+// slot order as the refresh sums it.
+template <int kMV, bool kFused>
+__device__ __forceinline__ void write_row(const FuseDev &fu, int r, int nf, const double (&la)[kMV],
+                                          double d, const int32_t (&dsts)[kMV],
+                                          const int32_t (&slots)[kMV], double *stage,
+                                          double *diag) {
+  diag[r] = d;
+#pragma unroll
+  for (int f = 0; f < kMV; ++f)
+    if (f < nf && dsts[f] >= 0) stage[dsts[f]] = xmul(la[f], -1.0);
+  if (kFused) {
+    fu.diag32[r] = __double2float_rn(d);
+    const int base = fu.sptr[r >> 5] + (r & 31);
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMV; ++k)
+#pragma unroll
+      for (int f = 0; f < kMV; ++f)
+        if (f < nf && slots[f] == base + 32 * k) {
+          const double v = xmul(la[f], -1.0);
+          const float v32 = __double2float_rn(v);
+          fu.val[slots[f]] = v;
+          fu.val32[slots[f]] = v32;
+          acc = xadd(acc, xsub(static_cast<double>(v32), v));
+        }
+    fu.comp[r] = -acc;
   }
 }
 
@@ -413,30 +474,180 @@ __global__ void __launch_bounds__(256)
     b[r] = b0 ? xadd(lb, bb) : lb;
   }
   if (o.calrcell) rcell[cell] = b0 ? xadd(rr, bb) : rr;
-  if (!o.matrix) return;
-  diag[r] = d;
+  if (o.matrix) write_row<kMV, kFused>(fu, r, nf, la, d, dsts, slots, stage, diag);
+}
+
+// difusionSchemeAnisotropic, ndm = 3 (CellLib.c:6054-6170): ORTHOGONAL or
+// OVERRELAXED (the only two that set e and t)
+template <bool kOver>
+__device__ __forceinline__ void pres_split(const double s[3], const double k[3], double e[3],
+                                           double t[3]) {
+  if (!kOver) {
+    const double ss = xsqrt(dot3(s, s));
+    for (int j = 0; j < 3; ++j) {
+      e[j] = xmul(ss, k[j]);
+      t[j] = 0.0;
+    }
+  } else {
+    const double tmp = xdiv(dot3(s, s), dot3(s, k));
+    for (int j = 0; j < 3; ++j) e[j] = xmul(tmp, k[j]);
+    for (int j = 0; j < 3; ++j) t[j] = xsub(s[j], e[j]);
+  }
+}
+
+// pLoadSimplePres with fCal and no buoyancy (Loads.c:728-845): a pressure
+// load's share of the diagonal
+__device__ __forceinline__ void pres_load(const DevLoad &L, const double e[3], const double n[3],
+                                          const double vc[3], double rhoC, double area,
+                                          double dd, double &sP) {
+  const double modE = xsqrt(dot3(e, e));
+  if (L.type == 1) {  // DIRICHLETBC
+    sP = xadd(sP, xdiv(xmul(rhoC, modE), dd));
+  } else if (L.type == 13) {  // INLETTOTALPRES
+    const double rhoEnv = L.par[0];
+    const double dc = xdiv(modE, dd);
+    const double ev[3] = {L.par[2], L.par[3], L.par[4]};
+    double tmp0 = dot3(vc, n);
+    double tmp1 = xmul(dot3(ev, n), area);
+    const double m = xmul(xmul(rhoEnv, tmp0), area);
+    const double modVel = xdiv(m, xmul(rhoEnv, tmp1));
+    tmp0 = xmul(rhoEnv, modVel);
+    tmp1 = xsub(m, xmul(xmul(dc, tmp0), tmp0));
+    sP = xadd(sP, xdiv(xmul(xmul(rhoEnv, m), dc), tmp1));
+  } else if (L.type == 10) {  // OPEN: outflow only, added twice as the reference does
+    if (dot3(vc, n) > 0.0) {
+      const double a = xdiv(xmul(rhoC, modE), dd);
+      sP = xadd(sP, a);
+      sP = xadd(sP, a);
+    }
+  }
+}
+
+// pLoadSimple with fCalVel = false, fCalPres = true (Loads.c:265-720): a
+// velocity load's mass flux in the pressure equation
+__device__ __forceinline__ void vel_load(const DevLoad &L, const double n[3], const double vc[3],
+                                         double rhoC, double area, double &pp) {
+  double m;
+  switch (L.type) {
+    case 7:   // OUTLET
+    case 9:   // INLETSTAICTPRES
+      m = xmul(xmul(rhoC, dot3(vc, n)), area);
+      break;
+    case 6: {  // INLET: prescribed velocity par[0..2], density par[np - 1]
+      const double t[3] = {L.par[0], L.par[1], L.par[2]};
+      m = xmul(xmul(L.par_last, dot3(t, n)), area);
+      break;
+    }
+    case 10: {  // OPEN
+      const double wfn = dot3(vc, n);
+      m = xmul(xmul(wfn >= 0.0 ? rhoC : L.density, wfn), area);
+      break;
+    }
+    case 13:  // INLETTOTALPRES
+      m = xmul(xmul(L.par[0], dot3(vc, n)), area);
+      break;
+    default:
+      return;  // walls and the rest: nothing in the pressure equation
+  }
+  pp = xsub(pp, m);
+}
+
+struct PresOpts {
+  int forces, matrix, calrcell;
+};
+
+// One row of cellSimplePres3D (CellPres.c:903-1218).  kOver: the
+// OVERRELAXED anisotropic split (else ORTHOGONAL).  loads: [0, 32) pressure
+// loads, [32, 64) velocity loads; dens: density of each material.
+template <bool kOver, int kMV, bool kFused>
+__global__ void __launch_bounds__(256)
+    pres_assemble_kernel(PlanDev p, FuseDev fu, const DevLoad *__restrict__ loads, PresOpts o,
+                         const int16_t *__restrict__ mat, const double *__restrict__ dens,
+                         const double *__restrict__ pres, const double *__restrict__ gradp,
+                         const double *__restrict__ vel, const double *__restrict__ dfield,
+                         double *__restrict__ stage, double *__restrict__ diag,
+                         double *__restrict__ b, double *__restrict__ rcell) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n) return;
+  const int cell = __ldcs(p.cell + r);
+  if (cell < 0) return;
+  const int nf = __ldcs(p.nface + r);
+  const size_t fs = p.fstride;
+  int32_t nbs[kMV], dsts[kMV], slots[kMV];
+  double alpha[kMV], area[kMV], mk[kMV];
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    const size_t q = static_cast<size_t>(f) * p.n + r;
+    nbs[f] = __ldcs(p.nb + q);
+    alpha[f] = __ldcs(p.geo + q);
+    area[f] = __ldcs(p.geo + fs + q);
+    mk[f] = __ldcs(p.geo + 2 * fs + q);
+  }
+  if (o.matrix) {
+#pragma unroll
+    for (int f = 0; f < kMV; ++f) {
+      dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+      slots[f] = kFused ? __ldcs(p.sslot + static_cast<size_t>(f) * p.n + r) : -1;
+    }
+  }
+  const size_t c3 = 3 * static_cast<size_t>(cell);
+  const double rhoC = dens[mat[cell] - 1], presC = pres[cell];
+  const double vc[3] = {vel[c3], vel[c3 + 1], vel[c3 + 2]};
+  const double gpc[3] = {gradp[c3], gradp[c3 + 1], gradp[c3 + 2]};
+  const double dc[3] = {dfield[c3], dfield[c3 + 1], dfield[c3 + 2]};
+  double la[kMV];
+  double pp = 0.0, sP = 0.0;
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    la[f] = 0.0;
+    if (f >= nf) continue;
+    const int32_t nb = nbs[f];
+    const size_t q = static_cast<size_t>(f) * p.n + r;
+    double k[3], n[3], s[3], e[3], t[3];
+    for (int j = 0; j < 3; ++j) {
+      k[j] = __ldcs(p.geo + (3 + j) * fs + q);
+      n[j] = __ldcs(p.geo + (6 + j) * fs + q);
+    }
+    if (nb >= 0) {
+      const size_t v3 = 3 * static_cast<size_t>(nb & (kFlagP - 1));
+      const int c = nb & (kFlagP - 1);
+      const double a = alpha[f], am1 = xsub(1.0, a);
+      const double rho = xadd(xmul(am1, rhoC), xmul(a, dens[mat[c] - 1]));
+      double dF[3], wf[3], gf[3];
+      for (int j = 0; j < 3; ++j) {
+        dF[j] = xadd(xmul(am1, dc[j]), xmul(a, dfield[v3 + j]));
+        s[j] = xmul(xmul(dF[j], area[f]), n[j]);
+        wf[j] = xadd(xmul(am1, vc[j]), xmul(a, vel[v3 + j]));
+        gf[j] = xadd(xmul(am1, gpc[j]), xmul(a, gradp[v3 + j]));
+      }
+      pres_split<kOver>(s, k, e, t);
+      la[f] = xdiv(xmul(rho, xsqrt(dot3(e, e))), mk[f]);
+      // interpolFaceVel, ndm = 3 (CellLib.c:6853-6960): Rhie-Chow face velocity
+      double wfn = dot3(wf, n);
+      const double g0 = xdiv(xsub(pres[c], presC), mk[f]);
+      const double nk = xadd(xadd(xmul(xmul(dF[0], k[0]), n[0]), xmul(xmul(dF[1], k[1]), n[1])),
+                             xmul(xmul(dF[2], k[2]), n[2]));
+      const double g1 = xmul(xsub(dot3(gf, k), g0), nk);
+      wfn = xadd(wfn, g1);
+      pp = xsub(pp, xmul(xmul(rho, wfn), area[f]));
+    } else {
+      const int code = -nb - 2;
+      const int lp = code & 63, lv = code >> 6;
+      if (lp) {
+        for (int j = 0; j < 3; ++j) s[j] = xmul(xmul(dc[j], alpha[f]), n[j]);
+        pres_split<kOver>(s, k, e, t);
+        pres_load(loads[lp - 1], e, n, vc, rhoC, alpha[f], area[f], sP);
+      }
+      if (lv) vel_load(loads[kMaxLoads + lv - 1], n, vc, rhoC, alpha[f], pp);
+    }
+  }
+  double d = sP;
 #pragma unroll
   for (int f = 0; f < kMV; ++f)
-    if (f < nf && dsts[f] >= 0) stage[dsts[f]] = xmul(la[f], -1.0);
-  if (kFused) {
-    // the value refresh for this row: SELL values, their FP32 copy, and the
-    // compensation summed in slot order as the refresh sums it
-    fu.diag32[r] = __double2float_rn(d);
-    const int base = fu.sptr[r >> 5] + (r & 31);
-    double acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < kMV; ++k)
-#pragma unroll
-      for (int f = 0; f < kMV; ++f)
-        if (f < nf && slots[f] == base + 32 * k) {
-          const double v = xmul(la[f], -1.0);
-          const float v32 = __double2float_rn(v);
-          fu.val[slots[f]] = v;
-          fu.val32[slots[f]] = v32;
-          acc = xadd(acc, xsub(static_cast<double>(v32), v));
-        }
-    fu.comp[r] = -acc;
-  }
+    if (f < nf) d = xadd(d, la[f]);
+  if (o.forces) b[r] = pp;
+  if (o.calrcell) rcell[cell] = pp;
+  if (o.matrix) write_row<kMV, kFused>(fu, r, nf, la, d, dsts, slots, stage, diag);
 }
 
 __global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
@@ -462,16 +673,22 @@ cudaError_t upload(T **dst, const T *src, size_t count) {
 struct sfr_dif_plan {
   sfr_system *s = nullptr;       // the system written; must outlive the plan's calls
   int32_t device = 0;            // destroy needs no live system
-  int32_t numel = 0, maxviz = 0, icod = 0;
+  int32_t kind = 0;              // 0 diffusion (systFormDif), 1 pressure (systFormSimplePres)
+  int32_t numel = 0, maxviz = 0, icod = 0, nmat = 0;
   int free_cells = 0;            // cells without an equation (their rcell is zeroed)
-  unsigned used_loads = 0;       // bit l: some boundary face names load l
+  unsigned used_loads = 0;       // bit l: some boundary face names load l (pressure loads)
+  unsigned used_vel_loads = 0;   // the same for the velocity loads (pressure plans)
   sfr::PlanDev d{};
   bool fused = false;            // the assembly also refreshes the SELL copy
   int32_t *d_id = nullptr;       // per cell: equation + 1 (updateCellValue)
-  sfr::DevLoad *d_loads = nullptr;
-  std::vector<sfr::DevLoad> loads_host;  // what d_loads holds
+  int16_t *d_mat = nullptr;      // per cell: material + 1 (pressure plans)
+  // the load tables ([0, 32) loads, [32, 64) velocity loads) then the density
+  // of each material (pressure plans)
+  unsigned char *d_table = nullptr;
+  std::vector<unsigned char> table_host;  // what d_table holds
   // host-array calls: device copies of the fields and results
-  double *h_fields = nullptr;    // density | cdiff | u0 | gradu0 (numel * 6)
+  double *h_fields = nullptr;    // diffusion: density | cdiff | u0 | gradu0; pressure:
+                                 // pres | gradpres | vel | dfield
   double *h_b0 = nullptr, *h_b = nullptr, *h_rcell = nullptr;
 };
 
@@ -491,6 +708,17 @@ int bad(const char *why) {
   return SFR_BAD_INPUT;
 }
 
+int unsupported(const char *why) {
+  sfr::set_last_error(why);
+  return SFR_UNSUPPORTED;
+}
+
+constexpr size_t kTableLoads = 2 * sfr::kMaxLoads;
+
+size_t table_bytes(const sfr_dif_plan *p) {
+  return sizeof(sfr::DevLoad) * kTableLoads + sizeof(double) * std::max(p->nmat, 1);
+}
+
 void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->d.cell);
   cudaFree(p->d.nface);
@@ -500,16 +728,34 @@ void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->d.geo);
   cudaFree(p->d.vol);
   cudaFree(p->d_id);
-  cudaFree(p->d_loads);
+  cudaFree(p->d_mat);
+  cudaFree(p->d_table);
   cudaFree(p->h_fields);
   cudaFree(p->h_b0);
   cudaFree(p->h_b);
   cudaFree(p->h_rcell);
 }
 
-// Check the loads the mesh uses against what pLoad accepts (Loads.c:881-990,
-// getLoads Loads.c:122-169) and stage them on the device.
-int stage_loads(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads, cudaStream_t st) {
+void fill_load(sfr::DevLoad *d, const sfr_load &L) {
+  d->type = L.type;
+  for (int j = 0; j < 5; ++j) d->par[j] = L.par[j];
+  d->par_last = L.np >= 1 && L.np <= 20 ? L.par[L.np - 1] : 0.0;
+  d->density = L.density;
+}
+
+// Copy the host table to the device when it changed since the last call.
+int stage_table(sfr_dif_plan *p, const std::vector<unsigned char> &h, cudaStream_t st) {
+  if (h != p->table_host) {
+    SFR_CUA(cudaMemcpyAsync(p->d_table, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+    SFR_CUA(cudaStreamSynchronize(st));  // h is the caller's local
+    p->table_host = h;
+  }
+  return SFR_OK;
+}
+
+// Diffusion: the loads the mesh uses against what pLoad accepts
+// (Loads.c:881-990, getLoads Loads.c:122-169).
+int stage_dif_loads(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads, cudaStream_t st) {
   if (nloads < 0 || nloads > sfr::kMaxLoads || (nloads > 0 && !loads))
     return bad("nloads must be 0..32");
   for (int l = 0; l < sfr::kMaxLoads; ++l) {
@@ -517,42 +763,59 @@ int stage_loads(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads, cudaStre
     if (l >= nloads) return bad("a boundary face names a load beyond nloads");
     const sfr_load &L = loads[l];
     const bool needs_value = L.type == 1 || L.type == 2 || L.type == 6;
-    if ((L.type == 1 || L.type == 6) && L.var != 0) {
-      sfr::set_last_error("loads given as functions (nTypeVar 1) are not assembled on the device");
-      return SFR_UNSUPPORTED;
-    }
-    if (L.type == 4) {
-      sfr::set_last_error("SINBC loads are not assembled on the device");
-      return SFR_UNSUPPORTED;
-    }
+    if ((L.type == 1 || L.type == 6) && L.var != 0)
+      return unsupported("loads given as functions (nTypeVar 1) are not assembled on the device");
+    if (L.type == 4) return unsupported("SINBC loads are not assembled on the device");
     if (L.type == 7) return bad("an OUTLET load reads a cell velocity the diffusion cell has not");
     if (needs_value && L.np < 1) return bad("a load has no parameters");
     if (L.type == 6 && L.np < 5) return bad("an INLET load needs 5 parameters");
   }
-  std::vector<sfr::DevLoad> h(sfr::kMaxLoads);
-  for (int l = 0; l < nloads; ++l) {
-    h[l].type = loads[l].type;
-    for (int j = 0; j < 5; ++j) h[l].par[j] = loads[l].par[j];
-  }
-  if (std::memcmp(h.data(), p->loads_host.data(), sizeof(sfr::DevLoad) * h.size()) != 0) {
-    SFR_CUA(cudaMemcpyAsync(p->d_loads, h.data(), sizeof(sfr::DevLoad) * h.size(),
-                            cudaMemcpyHostToDevice, st));
-    SFR_CUA(cudaStreamSynchronize(st));  // h is a local
-    p->loads_host = h;
-  }
-  return SFR_OK;
+  std::vector<unsigned char> h(table_bytes(p), 0);
+  auto *t = reinterpret_cast<sfr::DevLoad *>(h.data());
+  for (int l = 0; l < nloads; ++l) fill_load(t + l, loads[l]);
+  return stage_table(p, h, st);
 }
 
-}  // namespace
+// Pressure correction: pLoadSimplePres (Loads.c:728-845) reads pressure
+// loads' parameters directly; of the velocity loads (pLoadSimple,
+// Loads.c:265-720) only INLET reads a parameter list (getLoads copies np of
+// them, then par[0..2] and par[np - 1] are read).  prop: nmat x MAXPROP.
+int stage_pres_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                      const sfr_load *lpres, int32_t nlpres, const double *prop,
+                      cudaStream_t st) {
+  if (nlvel < 0 || nlvel > sfr::kMaxLoads || (nlvel > 0 && !lvel) || nlpres < 0 ||
+      nlpres > sfr::kMaxLoads || (nlpres > 0 && !lpres))
+    return bad("nlvel and nlpres must be 0..32");
+  if (!prop) return bad("prop is NULL");
+  for (int l = 0; l < sfr::kMaxLoads; ++l) {
+    if ((p->used_loads & (1u << l)) && l >= nlpres)
+      return bad("a boundary face names a pressure load beyond nlpres");
+    if (!(p->used_vel_loads & (1u << l))) continue;
+    if (l >= nlvel) return bad("a boundary face names a velocity load beyond nlvel");
+    const sfr_load &L = lvel[l];
+    if (L.type == 6 && L.var != 0)
+      return unsupported("loads given as functions (nTypeVar 1) are not assembled on the device");
+    if (L.type == 6 && (L.np < 3 || L.np > 20)) return bad("an INLET load needs 3..20 parameters");
+  }
+  std::vector<unsigned char> h(table_bytes(p), 0);
+  auto *t = reinterpret_cast<sfr::DevLoad *>(h.data());
+  for (int l = 0; l < nlpres; ++l) fill_load(t + l, lpres[l]);
+  for (int l = 0; l < nlvel; ++l) fill_load(t + sfr::kMaxLoads + l, lvel[l]);
+  auto *dens = reinterpret_cast<double *>(h.data() + sizeof(sfr::DevLoad) * kTableLoads);
+  for (int k = 0; k < p->nmat; ++k) dens[k] = prop[k * 10 + 1];  // MAXPROP 10, DENSITY 1
+  return stage_table(p, h, st);
+}
 
-extern "C" {
-
-int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
-                            sfr_dif_plan **out) {
+int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr, int32_t icod,
+                int32_t kind, sfr_dif_plan **out) {
   if (!s || !mesh || !out) return bad("NULL argument");
   *out = nullptr;
   const sfr_dif_mesh &m = *mesh;
-  if (icod < 1 || icod > 4) return bad("icod must be 1..4 (Define.h:304-307)");
+  if (kind == 0 && (icod < 1 || icod > 4)) return bad("icod must be 1..4 (Define.h:304-307)");
+  if (kind == 1 && icod != 1 && icod != 4)
+    return bad("the pressure split (difusionSchemeAnisotropic) sets e and t only for "
+               "ORTHOGONAL (1) and OVERRELAXED (4)");
+  if (kind == 1 && !facevelr) return bad("facevelr is NULL");
   if (m.numel < 1 || m.maxviz < 1 || m.maxviz > sfr::kMaxViz || m.nfaces < 1 || m.nmat < 1)
     return bad("mesh sizes out of range (maxviz 1..8)");
   const void *need[] = {m.nelcon, m.nviz, m.cellface, m.owner, m.volume, m.dcca, m.xmcc,
@@ -563,16 +826,21 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   if (static_cast<int64_t>(s->n) * m.maxviz > INT32_MAX) return bad("system too large");
   for (int64_t f = 0; f < m.nfaces; ++f)
     if (m.owner[2 * f] < 1 || m.owner[2 * f] > m.numel) return bad("a face owner is out of range");
+  if (kind == 1)
+    for (int32_t c = 0; c < m.numel; ++c)  // the density lookup of every cell
+      if (m.mat[c] < 1 || m.mat[c] > m.nmat) return bad("a cell's material is out of range");
   SFR_CUA(cudaSetDevice(s->device));
   auto *p = new sfr_dif_plan;
   p->s = s;
   p->device = s->device;
+  p->kind = kind;
   p->numel = m.numel;
   p->maxviz = m.maxviz;
   p->icod = icod;
-  p->loads_host.assign(sfr::kMaxLoads, sfr::DevLoad{});
+  p->nmat = m.nmat;
+  p->table_host.assign(table_bytes(p), 0);
   const int n = s->n;
-  const int mvpad = m.maxviz <= 6 ? 6 : sfr::kMaxViz;  // slots the assembly kernel reads
+  const int mvpad = m.maxviz <= 6 ? 6 : sfr::kMaxViz;  // slots the assembly kernels read
   const size_t slots = static_cast<size_t>(mvpad) * n;
   sfr::MeshDev md{};
   md.numel = m.numel;
@@ -586,11 +854,10 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
     cudaFree(const_cast<int32_t *>(md.nelcon));
     cudaFree(const_cast<int32_t *>(md.cellface));
     cudaFree(const_cast<int32_t *>(md.owner));
-    cudaFree(const_cast<int32_t *>(md.id));
     cudaFree(const_cast<int16_t *>(md.nviz));
     cudaFree(const_cast<int16_t *>(md.caltype));
-    cudaFree(const_cast<int16_t *>(md.mat));
     cudaFree(const_cast<int16_t *>(md.facer));
+    cudaFree(const_cast<int16_t *>(md.facevelr));
     cudaFree(const_cast<double *>(md.volume));
     cudaFree(const_cast<double *>(md.dcca));
     cudaFree(const_cast<double *>(md.xmcc));
@@ -619,7 +886,12 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
     up(sfr::upload(&t16, m.nviz, ne)); md.nviz = t16;
     up(sfr::upload(&t16, m.caltype, static_cast<size_t>(m.nmat))); md.caltype = t16;
     up(sfr::upload(&t16, m.mat, ne)); md.mat = t16;
+    p->d_mat = t16;  // kept by the plan for the density lookup
     up(sfr::upload(&t16, m.facer, ne * (m.maxviz + 1))); md.facer = t16;
+    if (kind == 1) {
+      up(sfr::upload(&t16, facevelr, ne * (m.maxviz + 1)));
+      md.facevelr = t16;
+    }
     up(sfr::upload(&t64, m.volume, ne)); md.volume = t64;
     up(sfr::upload(&t64, m.dcca, nv)); md.dcca = t64;
     up(sfr::upload(&t64, m.xmcc, 3 * nv)); md.xmcc = t64;
@@ -640,8 +912,8 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   up(cudaMalloc(&d.sslot, sizeof(int32_t) * slots));
   up(cudaMalloc(&d.geo, sizeof(double) * slots * sfr::kGeo));
   up(cudaMalloc(&d.vol, sizeof(double) * n));
-  up(cudaMalloc(&p->d_loads, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
-  up(cudaMalloc(&d_err, sizeof(int) * 4));
+  up(cudaMalloc(&p->d_table, table_bytes(p)));
+  up(cudaMalloc(&d_err, sizeof(int) * 5));
   if (rc == SFR_OK) {
     up(cudaMemset(d.cell, 0xFF, sizeof(int32_t) * n));
     up(cudaMemset(d.nface, 0, sizeof(int16_t) * n));
@@ -649,22 +921,23 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
     up(cudaMemset(d.dst, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.sslot, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.geo, 0, sizeof(double) * slots * sfr::kGeo));
-    up(cudaMemset(p->d_loads, 0, sizeof(sfr::DevLoad) * sfr::kMaxLoads));
-    up(cudaMemset(d_err, 0, sizeof(int) * 4));
+    up(cudaMemset(p->d_table, 0, table_bytes(p)));
+    up(cudaMemset(d_err, 0, sizeof(int) * 5));
   }
   if (rc == SFR_OK) {
     sfr::PatternDev P{s->A.sptr, s->A.col, s->A.src, n, s->storage, s->unsym,
                       s->storage == SFR_ELLPACK ? s->nsrc / std::max(n, 1) : 0};
     const int blocks = (m.numel + 255) / 256;
-    sfr::plan_kernel<<<blocks, 256>>>(md, P, d, icod, d_err,
+    sfr::plan_kernel<<<blocks, 256>>>(md, P, d, icod, kind, d_err,
                                       reinterpret_cast<unsigned *>(d_err + 1), d_err + 2,
-                                      d_err + 3);
+                                      d_err + 3, reinterpret_cast<unsigned *>(d_err + 4));
     up(cudaGetLastError());
-    int h[4] = {0, 0, 0, 0};
+    int h[5] = {0, 0, 0, 0, 0};
     up(cudaMemcpy(h, d_err, sizeof(h), cudaMemcpyDeviceToHost));
     if (rc == SFR_OK && h[0] != sfr::kErrNone) rc = bad(sfr::plan_error_text(h[0]));
     p->used_loads = static_cast<unsigned>(h[1]);
     p->free_cells = h[2];
+    p->used_vel_loads = static_cast<unsigned>(h[4]);
     // every stored value of every row written by the row's own cell
     p->fused = h[3] == 0 && s->A.val32 != nullptr;
   }
@@ -678,7 +951,8 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
       up(cudaMemset(s->A.val32, 0, sizeof(float) * std::max<int64_t>(s->A.nslots, 1)));
     }
   }
-  md.id = nullptr;  // the plan's (freed with it)
+  md.id = nullptr;   // the plan's (freed with it)
+  md.mat = nullptr;  // likewise
   release_mesh();
   if (rc != SFR_OK) {
     free_plan_buffers(p);
@@ -689,6 +963,41 @@ int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
   return SFR_OK;
 }
 
+int ensure_host_buffers(sfr_dif_plan *p) {
+  if (p->h_fields) return SFR_OK;
+  const size_t ne = p->numel;
+  SFR_CUA(cudaMalloc(&p->h_fields, sizeof(double) * ne * 10));
+  SFR_CUA(cudaMalloc(&p->h_b0, sizeof(double) * p->s->n));
+  SFR_CUA(cudaMalloc(&p->h_b, sizeof(double) * p->s->n));
+  SFR_CUA(cudaMalloc(&p->h_rcell, sizeof(double) * ne));
+  return SFR_OK;
+}
+
+int copy_back(sfr_dif_plan *p, double *b, double *rcell, int32_t forces, int32_t calrcell,
+              cudaStream_t st) {
+  if (forces && b)
+    SFR_CUA(cudaMemcpyAsync(b, p->h_b, sizeof(double) * p->s->n, cudaMemcpyDeviceToHost, st));
+  if (calrcell && rcell)
+    SFR_CUA(cudaMemcpyAsync(rcell, p->h_rcell, sizeof(double) * p->numel, cudaMemcpyDeviceToHost,
+                            st));
+  SFR_CUA(cudaStreamSynchronize(st));
+  return SFR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfr_gpu_dif_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
+                            sfr_dif_plan **out) {
+  return create_plan(s, mesh, nullptr, icod, 0, out);
+}
+
+int sfr_gpu_pres_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr,
+                             int32_t icod, sfr_dif_plan **out) {
+  return create_plan(s, mesh, facevelr, icod, 1, out);
+}
+
 int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
                                 const sfr_dif_opts *o, const double *d_density,
                                 const double *d_cdiff, const double *d_u0,
@@ -696,6 +1005,7 @@ int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t 
                                 double *d_rcell, int32_t forces, int32_t matrix,
                                 int32_t calrcell, void *stream) {
   if (!p || !o) return bad("NULL argument");
+  if (p->kind != 0) return bad("not a diffusion plan");
   if (o->icod != p->icod) return bad("opts.icod differs from the scheme the plan was built for");
   if (!d_cdiff || !d_u0) return bad("cdiff and u0 are required");
   if (o->icod != 1 && !d_gradu0) return bad("gradu0 is required by non-orthogonal schemes");
@@ -705,7 +1015,7 @@ int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t 
   sfr_system *s = p->s;
   SFR_CUA(cudaSetDevice(s->device));
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
-  int rc = stage_loads(p, loads, nloads, st);
+  int rc = stage_dif_loads(p, loads, nloads, st);
   if (rc != SFR_OK) return rc;
   if (calrcell && p->free_cells > 0)
     SFR_CUA(cudaMemsetAsync(d_rcell, 0, sizeof(double) * p->numel, st));
@@ -714,9 +1024,10 @@ int sfr_gpu_dif_assemble_device(sfr_dif_plan *p, const sfr_load *loads, int32_t 
   const int blocks = (s->n + 255) / 256;
   const bool fuse = p->fused && matrix;
   sfr::FuseDev fu{s->A.val, s->A.val32, s->A.sptr, s->d_comp, s->d_diag32};
+  const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   auto launch = [&](auto kernel) {
-    kernel<<<blocks, 256, 0, st>>>(p->d, fu, p->d_loads, co, d_density, d_cdiff, d_u0,
-                                   d_gradu0, d_b0, s->d_stage, s->d_diag, d_b, d_rcell);
+    kernel<<<blocks, 256, 0, st>>>(p->d, fu, loads_d, co, d_density, d_cdiff, d_u0, d_gradu0,
+                                   d_b0, s->d_stage, s->d_diag, d_b, d_rcell);
   };
   const bool orth = p->icod == 1, six = p->d.maxviz == 6;
   constexpr int k8 = sfr::kMaxViz;
@@ -748,13 +1059,9 @@ int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
   if (!cdiff || !u0) return bad("cdiff and u0 are required");
   sfr_system *s = p->s;
   SFR_CUA(cudaSetDevice(s->device));
+  int rc = ensure_host_buffers(p);
+  if (rc != SFR_OK) return rc;
   const size_t ne = p->numel;
-  if (!p->h_fields) {
-    SFR_CUA(cudaMalloc(&p->h_fields, sizeof(double) * ne * 6));
-    SFR_CUA(cudaMalloc(&p->h_b0, sizeof(double) * s->n));
-    SFR_CUA(cudaMalloc(&p->h_b, sizeof(double) * s->n));
-    SFR_CUA(cudaMalloc(&p->h_rcell, sizeof(double) * ne));
-  }
   cudaStream_t st = s->stream;
   double *fd = p->h_fields;
   double *d_density = fd, *d_cdiff = fd + ne, *d_u0 = fd + 2 * ne, *d_grad = fd + 3 * ne;
@@ -766,23 +1073,94 @@ int sfr_gpu_dif_assemble(sfr_dif_plan *p, const sfr_load *loads, int32_t nloads,
     SFR_CUA(cudaMemcpyAsync(d_grad, gradu0, sizeof(double) * ne * 3, cudaMemcpyHostToDevice, st));
   if (b0)
     SFR_CUA(cudaMemcpyAsync(p->h_b0, b0, sizeof(double) * s->n, cudaMemcpyHostToDevice, st));
-  int rc = sfr_gpu_dif_assemble_device(p, loads, nloads, o, density ? d_density : nullptr,
-                                       d_cdiff, d_u0, gradu0 ? d_grad : nullptr,
-                                       b0 ? p->h_b0 : nullptr, p->h_b, p->h_rcell, forces,
-                                       matrix, calrcell, st);
+  rc = sfr_gpu_dif_assemble_device(p, loads, nloads, o, density ? d_density : nullptr, d_cdiff,
+                                   d_u0, gradu0 ? d_grad : nullptr, b0 ? p->h_b0 : nullptr,
+                                   p->h_b, p->h_rcell, forces, matrix, calrcell, st);
   if (rc != SFR_OK) return rc;
-  if (forces && b)
-    SFR_CUA(cudaMemcpyAsync(b, p->h_b, sizeof(double) * s->n, cudaMemcpyDeviceToHost, st));
-  if (calrcell && rcell)
-    SFR_CUA(cudaMemcpyAsync(rcell, p->h_rcell, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
-  SFR_CUA(cudaStreamSynchronize(st));
+  return copy_back(p, b, rcell, forces, calrcell, st);
+}
+
+int sfr_gpu_pres_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                                 const sfr_load *lpres, int32_t nlpres, const double *prop,
+                                 const double *d_pres, const double *d_gradpres,
+                                 const double *d_vel, const double *d_dfield, double *d_b,
+                                 double *d_rcell, int32_t forces, int32_t matrix,
+                                 int32_t calrcell, void *stream) {
+  if (!p) return bad("NULL argument");
+  if (p->kind != 1) return bad("not a pressure-correction plan");
+  if (!d_pres || !d_gradpres || !d_vel || !d_dfield)
+    return bad("pres, gradpres, vel and dfield are required");
+  if (forces && !d_b) return bad("forces set without b");
+  if (calrcell && !d_rcell) return bad("calrcell set without rcell");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  int rc = stage_pres_tables(p, lvel, nlvel, lpres, nlpres, prop, st);
+  if (rc != SFR_OK) return rc;
+  if (calrcell && p->free_cells > 0)
+    SFR_CUA(cudaMemsetAsync(d_rcell, 0, sizeof(double) * p->numel, st));
+  sfr::PresOpts po{forces != 0, matrix != 0, calrcell != 0};
+  const int blocks = (s->n + 255) / 256;
+  const bool fuse = p->fused && matrix;
+  sfr::FuseDev fu{s->A.val, s->A.val32, s->A.sptr, s->d_comp, s->d_diag32};
+  const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
+  const auto *dens =
+      reinterpret_cast<const double *>(p->d_table + sizeof(sfr::DevLoad) * kTableLoads);
+  auto launch = [&](auto kernel) {
+    kernel<<<blocks, 256, 0, st>>>(p->d, fu, loads_d, po, p->d_mat, dens, d_pres, d_gradpres,
+                                   d_vel, d_dfield, s->d_stage, s->d_diag, d_b, d_rcell);
+  };
+  const bool over = p->icod == 4, six = p->d.maxviz == 6;
+  constexpr int k8 = sfr::kMaxViz;
+  if (fuse) {
+    if (six)
+      over ? launch(sfr::pres_assemble_kernel<true, 6, true>)
+           : launch(sfr::pres_assemble_kernel<false, 6, true>);
+    else
+      over ? launch(sfr::pres_assemble_kernel<true, k8, true>)
+           : launch(sfr::pres_assemble_kernel<false, k8, true>);
+  } else {
+    if (six)
+      over ? launch(sfr::pres_assemble_kernel<true, 6, false>)
+           : launch(sfr::pres_assemble_kernel<false, 6, false>);
+    else
+      over ? launch(sfr::pres_assemble_kernel<true, k8, false>)
+           : launch(sfr::pres_assemble_kernel<false, k8, false>);
+  }
+  SFR_CUA(cudaGetLastError());
+  if (matrix) return sfr::values_refreshed(s, st, fuse);
   return SFR_OK;
+}
+
+int sfr_gpu_pres_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                          const sfr_load *lpres, int32_t nlpres, const double *prop,
+                          const double *pres, const double *gradpres, const double *vel,
+                          const double *dfield, double *b, double *rcell, int32_t forces,
+                          int32_t matrix, int32_t calrcell) {
+  if (!p) return bad("NULL argument");
+  if (!pres || !gradpres || !vel || !dfield) return bad("pres, gradpres, vel and dfield are required");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  int rc = ensure_host_buffers(p);
+  if (rc != SFR_OK) return rc;
+  const size_t ne = p->numel;
+  cudaStream_t st = s->stream;
+  double *fd = p->h_fields;
+  double *d_pres = fd, *d_gp = fd + ne, *d_vel = fd + 4 * ne, *d_df = fd + 7 * ne;
+  SFR_CUA(cudaMemcpyAsync(d_pres, pres, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  SFR_CUA(cudaMemcpyAsync(d_gp, gradpres, sizeof(double) * ne * 3, cudaMemcpyHostToDevice, st));
+  SFR_CUA(cudaMemcpyAsync(d_vel, vel, sizeof(double) * ne * 3, cudaMemcpyHostToDevice, st));
+  SFR_CUA(cudaMemcpyAsync(d_df, dfield, sizeof(double) * ne * 3, cudaMemcpyHostToDevice, st));
+  rc = sfr_gpu_pres_assemble_device(p, lvel, nlvel, lpres, nlpres, prop, d_pres, d_gp, d_vel,
+                                    d_df, p->h_b, p->h_rcell, forces, matrix, calrcell, st);
+  if (rc != SFR_OK) return rc;
+  return copy_back(p, b, rcell, forces, calrcell, st);
 }
 
 int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, int32_t add,
                              void *stream) {
   if (!p || !d_x || !d_u) return bad("NULL argument");
-  SFR_CUA(cudaSetDevice(p->s->device));
+  SFR_CUA(cudaSetDevice(p->device));
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : p->s->stream;
   sfr::update_cells_kernel<<<(p->numel + 255) / 256, 256, 0, st>>>(p->d_id, p->numel, p->s->n,
                                                                      d_x, d_u, add != 0);

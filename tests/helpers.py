@@ -107,3 +107,46 @@ def bits_equal(a, b) -> bool:
     a = np.ascontiguousarray(a, np.float64)
     b = np.ascontiguousarray(b, np.float64)
     return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+def pres_fixture():
+    """tests/golden/pres_assembly.npz as (mesh, sides, fields, lvel, lpres,
+    layouts, cases); sides[k] = (facevelr, facepresr); cases are dicts
+    (name, layout, icod, sides, forces, matrix, calrcell, a, ad, b, rcell)."""
+    import os
+    from oracle import oracle as O
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "pres_assembly.npz")
+    z = np.load(path)
+    mk = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith("mesh/")}
+    mesh = _Bag(numel=len(mk["nviz"]), nface=len(mk["mksi"]), **mk)
+    fields = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith("field/")}
+    tables = {}
+    for tag in ("lvel", "lpres"):
+        loads = []
+        for i in range(len(z[f"{tag}/type"])):
+            npar = int(z[f"{tag}/np"][i])
+            loads.append(O.Load(int(z[f"{tag}/type"][i]), tuple(z[f"{tag}/par"][i][:npar]),
+                                var=int(z[f"{tag}/var"][i]), np=npar,
+                                density=float(z[f"{tag}/density"][i])))
+        tables[tag] = loads
+    sides = {}
+    k = 0
+    while f"sides/{k}/facevelr" in z.files:
+        sides[k] = (z[f"sides/{k}/facevelr"], z[f"sides/{k}/facepresr"])
+        k += 1
+    lays = {}
+    for key in z.files:
+        if key.startswith("layout/") and key.endswith("/meta"):
+            name = key.split("/")[1]
+            st, un, neq = (int(v) for v in z[key])
+            lays[name] = (st, bool(un), z[f"layout/{name}/ia"], z[f"layout/{name}/ja"], neq)
+    cases = []
+    for name in z["cases"]:
+        name = str(name)
+        icod, k, forces, matrix, calr = (int(v) for v in z[f"{name}/meta"])
+        cases.append(dict(name=name, layout=str(z[f"{name}/layout"]), icod=icod, sides=k,
+                          forces=bool(forces), matrix=bool(matrix), calrcell=bool(calr),
+                          a=z[f"{name}/a"], ad=z[f"{name}/ad"], b=z[f"{name}/b"],
+                          rcell=z[f"{name}/rcell"]))
+    return mesh, sides, fields, tables["lvel"], tables["lpres"], lays, cases

@@ -108,3 +108,69 @@ def test_dif_plan_rejects_too_many_loads():
     from sfr3d_b200 import assembly as A
     with pytest.raises(ValueError):
         A._loads_c([A.Load(A.NEUMANN, (0.0,))] * 33)
+
+
+# ------------------------------------------------ pressure correction --
+from helpers import pres_fixture  # noqa: E402
+
+
+def test_pres_oracle_matches_reference_fixture():
+    mesh, sides, f, lvel, lpres, lays, cases = pres_fixture()
+    assert len(cases) >= 20
+    for c in cases:
+        st, un, ia, ja, neq = lays[c["layout"]]
+        fv, fp = sides[c["sides"]]
+        case = O.PresCase(mesh=mesh, facevelr=fv, facepresr=fp, lvel=lvel, lpres=lpres,
+                          icod=c["icod"], **f)
+        rc, a, ad, b, rcell = O.pres_assemble(case, st, un, ia, ja, neq, c["forces"],
+                                              c["matrix"], c["calrcell"], fill=0.0)
+        assert rc == 0, c["name"]
+        for got, want, what in ((a, c["a"], "a"), (ad, c["ad"], "ad"), (b, c["b"], "b"),
+                                (rcell, c["rcell"], "rcell")):
+            assert bits_equal(got, want), (c["name"], what)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_pres_oracle_matches_reference_live():
+    s = S.poisson_jittered(5, seed=8)
+    m = s.mesh()
+    rng = np.random.default_rng(4)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    prop = np.zeros((3, O.MAXPROP))
+    prop[:, O.DENSITY] = (1.0, 0.8, 1.4)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.INLET, (0.5, 0.1, -0.2), np=3),
+            O.Load(O.OPEN, (), density=1.1), O.Load(O.OUTLET, ())]
+    lpres = [O.Load(O.DIRICHLET, (0.0,)), O.Load(O.OPEN, (0.0,))]
+    for icod in (O.ORTHOGONAL, O.OVERRELAXED):
+        case = O.PresCase(mesh=m, facevelr=m.face_r([1, 2, 3, 4, 1, 1]),
+                          facepresr=m.face_r([0, 1, 2, 0, 0, 0]), lvel=lvel, lpres=lpres,
+                          prop=prop, mat=rng.integers(1, 4, m.numel).astype(np.int16),
+                          pres=rng.standard_normal(m.numel),
+                          gradpres=rng.standard_normal((m.numel, 3)),
+                          vel=rng.standard_normal((m.numel, 3)),
+                          dfield=rng.uniform(0.1, 1.0, (m.numel, 3)), icod=icod)
+        for name, (st, un, ia, ja, _al, _au) in lay.items():
+            r1 = O.pres_assemble(case, st, un, ia, ja, s.neq, fill=2.0)
+            r2 = O.ref_pres_assemble(case, st, un, ia, ja, s.neq, fill=2.0)
+            r3 = O.ref_pres_assemble(case, st, un, ia, ja, s.neq, fill=2.0, nthreads=4)
+            assert r1[0] == r2[0] == r3[0] == 0
+            for x, y, z in zip(r1[1:], r2[1:5], r3[1:5]):
+                assert bits_equal(x, y) and bits_equal(x, z), (icod, name)
+
+
+def test_pres_oracle_rejects_what_the_reference_cannot_take():
+    s = S.poisson_uniform(4, seed=1)
+    m = s.mesh()
+    base = dict(mesh=m, facevelr=m.face_r([1, 0, 0, 0, 0, 0]), facepresr=m.face_r([0] * 6),
+                lpres=[], prop=np.array([[0.0, 1.0] + [0.0] * 8]),
+                pres=np.zeros(m.numel), gradpres=np.zeros((m.numel, 3)),
+                vel=np.zeros((m.numel, 3)), dfield=np.ones((m.numel, 3)))
+    run = lambda **kw: O.pres_assemble(O.PresCase(**{**base, **kw}), O.CSRD, True,  # noqa: E731
+                                       s.ia, s.ja, s.neq)[0]
+    assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0))]) == 0
+    assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
+    assert run(lvel=[O.Load(O.INLET, (1.0, 0.0))]) == -1
+    # MINIMAL / ORTHOGONALC leave the split unset in the reference
+    assert run(lvel=[O.Load(O.STATICWALL, ())], icod=O.MINIMAL) == -1

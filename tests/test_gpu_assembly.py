@@ -272,3 +272,152 @@ def test_solver_copy_matches_uploaded_values(cuda, box, name):
         assert ia_.iters == iu_.iters and ia_.status == iu_.status == sv.OK
         assert bits_equal(xa, xu), (name, prec)
     plan.close()
+
+
+# ------------------------------------------------ pressure correction --
+from helpers import pres_fixture  # noqa: E402
+
+PLVEL = [O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), O.Load(O.INLET, (0.5, 0.1, -0.2, 1.1)),
+         O.Load(O.OUTLET, ()), O.Load(O.OPEN, (0.0,), density=0.9),
+         O.Load(O.INLETSTAICTPRES, (1.0, 0.0, 0.0, 1.0)),
+         O.Load(O.INLETTOTALPRES, (1.2, 2.0, 1.0, 0.0, 0.0)), O.Load(O.STATICWALL, ())]
+PLPRES = [O.Load(O.DIRICHLET, (0.0,)), O.Load(O.OPEN, (0.0,)),
+          O.Load(O.INLETTOTALPRES, (1.2, 2.0, 1.0, 0.0, 0.0)), O.Load(O.FLUXPRES, ())]
+
+
+def _aloads(loads):
+    return [A.Load(ld.type, tuple(ld.par), var=ld.var, np=ld.np, density=ld.density)
+            for ld in loads]
+
+
+def _pres_device(gs, plan, case, flags, fill=0.0):
+    forces, matrix, calr = flags
+    if matrix or not gs.values_version:
+        n = gs._nsrc()
+        split = gs.storage == sv.CSRC and gs.unsym
+        gs.set_values(np.full(n // 2 if split else n, fill), np.full(gs.neq, fill),
+                      np.full(n // 2, fill) if split else None)
+    b, rcell = plan.assemble(_aloads(case.lvel), _aloads(case.lpres), case.prop, case.pres,
+                             case.gradpres, case.vel, case.dfield, forces=forces,
+                             matrix=matrix, calrcell=calr)
+    al, ad, au = A.get_values(gs)
+    return (al if au is None else np.concatenate([al, au])), ad, b, rcell
+
+
+def _pres_compare(got, want, flags, what):
+    forces, matrix, calr = flags
+    if matrix:
+        assert bits_equal(got[0], want[1]), what
+        assert bits_equal(got[1], want[2]), what
+    if forces:
+        assert bits_equal(got[2], want[3]), what
+    if calr:
+        assert bits_equal(got[3], want[4]), what
+
+
+def test_pres_fixture_replay(cuda):
+    mesh, sides, f, lvel, lpres, lays, cases = pres_fixture()
+    for lname, (st, un, ia, ja, neq) in lays.items():
+        gs = sv.GpuSystem(neq, ia, ja, st, un)
+        for c in (c for c in cases if c["layout"] == lname):
+            fv, fp = sides[c["sides"]]
+            plan = A.PresPlan(gs, mesh, fp, fv, icod=c["icod"], mat=f["mat"],
+                              nmat=len(f["prop"]))
+            case = O.PresCase(mesh=mesh, facevelr=fv, facepresr=fp, lvel=lvel, lpres=lpres,
+                              icod=c["icod"], **f)
+            flags = (c["forces"], c["matrix"], c["calrcell"])
+            got = _pres_device(gs, plan, case, flags)
+            _pres_compare(got, (0, c["a"], c["ad"], c["b"], c["rcell"]), flags, c["name"])
+            plan.close()
+        gs.close()
+
+
+@pytest.mark.parametrize("icod", [1, 4])
+def test_pres_every_layout_matches_oracle(cuda, box, icod):
+    s, m, lay = box
+    rng = np.random.default_rng(20 + icod)
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, O.DENSITY] = (1.2, 0.9)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    for name, (st, un, ia, ja, _al, _au) in lay.items():
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        for vs, ps in (((1, 2, 3, 4, 5, 6), (1, 0, 2, 0, 3, 4)),
+                       ((7, 3, 0, 4, 6, 2), (0, 0, 0, 0, 0, 1))):
+            fv, fp = m.face_r(vs), m.face_r(ps)
+            plan = A.PresPlan(gs, m, fp, fv, icod=icod, mat=mat, nmat=2)
+            for flags in ((1, 1, 1), (1, 0, 0), (0, 1, 1)):
+                case = O.PresCase(mesh=m, facevelr=fv, facepresr=fp, lvel=PLVEL, lpres=PLPRES,
+                                  prop=prop, mat=mat, pres=rng.standard_normal(m.numel),
+                                  gradpres=rng.standard_normal((m.numel, 3)),
+                                  vel=rng.standard_normal((m.numel, 3)),
+                                  dfield=rng.uniform(0.1, 1.0, (m.numel, 3)), icod=icod)
+                want = O.pres_assemble(case, st, un, ia, ja, s.neq, *flags, fill=4.0)
+                assert want[0] == 0
+                got = _pres_device(gs, plan, case, flags, fill=4.0)
+                _pres_compare(got, want, flags, (name, vs, flags))
+            plan.close()
+        gs.close()
+
+
+def test_pres_64cubed_matches_oracle_and_solves(cuda):
+    torch = cuda
+    s = S.poisson_jittered(64, seed=9)
+    m = s.mesh()
+    rng = np.random.default_rng(21)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, O.DENSITY] = 1.0
+    fv = m.face_r([7, 7, 7, 7, 7, 1])       # static walls, a moving lid
+    fp = m.face_r([1, 0, 0, 0, 0, 0])       # pressure fixed on x = 0
+    lvel = [O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0))] + [O.Load(O.STATICWALL, ())] * 6
+    lpres = [O.Load(O.DIRICHLET, (0.0,))]
+    case = O.PresCase(mesh=m, facevelr=fv, facepresr=fp, lvel=lvel, lpres=lpres, prop=prop,
+                      pres=rng.standard_normal(m.numel),
+                      gradpres=rng.standard_normal((m.numel, 3)),
+                      vel=rng.standard_normal((m.numel, 3)),
+                      dfield=rng.uniform(0.5, 1.0, (m.numel, 3)), icod=O.ORTHOGONAL)
+    rc, a, ad, b, rcell = O.pres_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    assert rc == 0
+    gs = sv.GpuSystem(s.neq, s.ia, s.ja, O.CSRD, True)
+    plan = A.PresPlan(gs, m, fp, fv, icod=O.ORTHOGONAL)
+    dev = lambda v: torch.tensor(np.ascontiguousarray(v), device="cuda")  # noqa: E731
+    d = [dev(x) for x in (case.pres, case.gradpres, case.vel, case.dfield)]
+    d_b = torch.empty(s.neq, dtype=torch.float64, device="cuda")
+    d_r = torch.empty(m.numel, dtype=torch.float64, device="cuda")
+    plan.assemble_device(_aloads(lvel), _aloads(lpres), prop, *[t.data_ptr() for t in d],
+                         d_b=d_b.data_ptr(), d_rcell=d_r.data_ptr())
+    torch.cuda.synchronize()
+    assert bits_equal(d_b.cpu().numpy(), b) and bits_equal(d_r.cpu().numpy(), rcell)
+    al, ad_g, _ = A.get_values(gs)
+    assert bits_equal(al, a) and bits_equal(ad_g, ad)
+    # the pressure correction solved where it was assembled
+    ref = O.pcg(O.CSRD, True, s.ia, s.ja, a, ad, b, tol=1e-10)
+    d_x = torch.zeros(s.neq, dtype=torch.float64, device="cuda")
+    info = gs.solve_device(sv.PCG, d_b.data_ptr(), d_x.data_ptr(), tol=1e-10)
+    assert abs(info.iters - ref.iters) <= 1
+    assert rel(d_x.cpu().numpy(), ref.x) < 1e-12
+
+
+def test_pres_validation(cuda, box):
+    s, m, lay = box
+    st, un, ia, ja, _al, _au = lay["csrd_full"]
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    fv, fp = m.face_r([1, 2, 0, 0, 0, 0]), m.face_r([0, 0, 1, 0, 0, 0])
+    with pytest.raises(sv.SolverError) as e:
+        A.PresPlan(gs, m, fp, fv, icod=O.MINIMAL)
+    assert e.value.status == sv.BAD_INPUT
+    plan = A.PresPlan(gs, m, fp, fv)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, O.DENSITY] = 1.0
+    z1, z3 = np.zeros(m.numel), np.zeros((m.numel, 3))
+    lp = [A.Load(A.DIRICHLET, (0.0,))]
+    with pytest.raises(sv.SolverError) as e:   # velocity load 2 named, one given
+        plan.assemble([A.Load(A.STATICWALL, ())], lp, prop, z1, z3, z3, z3)
+    assert e.value.status == sv.BAD_INPUT
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.STATICWALL, ()), A.Load(A.INLET, (1.0, 0.0, 0.0), var=1)], lp,
+                      prop, z1, z3, z3, z3)
+    assert e.value.status == sv.UNSUPPORTED
+    plan.assemble([A.Load(A.STATICWALL, ()), A.Load(A.INLET, (1.0, 0.0, 0.0))], lp, prop, z1,
+                  z3, z3, z3)
+    plan.close()
+    gs.close()
