@@ -714,9 +714,11 @@ def assembly_leg(np, torch, sv, s, n, peak, peak_kind):
     plan.close()
     g.close()
     gbs = alg / (dev_ms * 1e-3) / 1e9
+    tr = committed_traffic("dif_assemble_kernel")
     return {"workload": f"systFormDif, diffusion {n}^3 = {s.neq} cells (the pressure mesh), "
                         "ORTHOGONAL, Dirichlet x=0, residual form, CSRD",
             "device_ms": dev_ms, "plan_create_s": plan_s,
+            "traffic": None if tr is None else tr[0] * (s.neq / 128 ** 3),
             "alg_bytes_per_call": alg, "alg_bytes_per_row": ASSEMBLY_ALG_BYTES_PER_ROW,
             "GB/s": gbs, "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
             "kernel": "dif_assemble_kernel<orthogonal, 6 faces, fused> (one launch: also "
@@ -745,9 +747,11 @@ def pressure_leg(np, torch, sv, s, n, peak, peak_kind):
     close()
     alg = PRES_ALG_BYTES_PER_ROW * s.neq
     gbs = alg / (dev_ms * 1e-3) / 1e9
+    tr = committed_traffic("pres_assemble_kernel")
     return {"workload": f"systFormSimplePres, {n}^3 = {s.neq} cells, cavity loads (static "
                         "walls, moving lid), pressure fixed on x=0, ORTHOGONAL, CSRD",
             "device_ms": dev_ms, "alg_bytes_per_row": PRES_ALG_BYTES_PER_ROW,
+            "traffic": None if tr is None else tr[0] * (s.neq / 128 ** 3),
             "GB/s": gbs, "frac": gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
             "kernel": "pres_assemble_kernel<orthogonal, 6 faces, fused>"}
 

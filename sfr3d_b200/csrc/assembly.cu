@@ -560,7 +560,7 @@ struct PresOpts {
 // OVERRELAXED anisotropic split (else ORTHOGONAL).  loads: [0, 32) pressure
 // loads, [32, 64) velocity loads; dens: density of each material.
 template <bool kOver, int kMV, bool kFused>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     pres_assemble_kernel(PlanDev p, FuseDev fu, const DevLoad *__restrict__ loads, PresOpts o,
                          const int16_t *__restrict__ mat, const double *__restrict__ dens,
                          const double *__restrict__ pres, const double *__restrict__ gradp,
@@ -582,13 +582,6 @@ __global__ void __launch_bounds__(256)
     alpha[f] = __ldcs(p.geo + q);
     area[f] = __ldcs(p.geo + fs + q);
     mk[f] = __ldcs(p.geo + 2 * fs + q);
-  }
-  if (o.matrix) {
-#pragma unroll
-    for (int f = 0; f < kMV; ++f) {
-      dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
-      slots[f] = kFused ? __ldcs(p.sslot + static_cast<size_t>(f) * p.n + r) : -1;
-    }
   }
   const size_t c3 = 3 * static_cast<size_t>(cell);
   const double rhoC = dens[mat[cell] - 1], presC = pres[cell];
@@ -647,7 +640,13 @@ __global__ void __launch_bounds__(256)
     if (f < nf) d = xadd(d, la[f]);
   if (o.forces) b[r] = pp;
   if (o.calrcell) rcell[cell] = pp;
-  if (o.matrix) write_row<kMV, kFused>(fu, r, nf, la, d, dsts, slots, stage, diag);
+  if (!o.matrix) return;
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {  // loaded late: fewer live registers in the face loop
+    dsts[f] = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+    slots[f] = kFused ? __ldcs(p.sslot + static_cast<size_t>(f) * p.n + r) : -1;
+  }
+  write_row<kMV, kFused>(fu, r, nf, la, d, dsts, slots, stage, diag);
 }
 
 __global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
