@@ -150,3 +150,26 @@ def pres_fixture():
                           a=z[f"{name}/a"], ad=z[f"{name}/ad"], b=z[f"{name}/b"],
                           rcell=z[f"{name}/rcell"]))
     return mesh, sides, fields, tables["lvel"], tables["lpres"], lays, cases
+
+
+def cavity_systems():
+    """tests/golden/cavity_systems.npz: {tag: dict(storage, unsym, solver, ia,
+    ja, a, al, au, ad, b, x, tol, maxit, neq)} for the harvested pressure and
+    momentum systems of the reference's lid-driven cavity; `a` is what the
+    oracle takes (al, or al then au for unsym CSRC) and x the reference's own
+    solution."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "cavity_systems.npz")
+    z = np.load(path)
+    out = {}
+    for tag in ("pressure", "momentum"):
+        neq, nad, st, solver, unsym, newx, maxit = (int(v) for v in z[f"{tag}/meta"])
+        al = z[f"{tag}/al"]
+        au = z[f"{tag}/au"] if unsym else None
+        out[tag] = dict(storage=st, unsym=bool(unsym), solver=solver, ia=z[f"{tag}/ia"],
+                        ja=z[f"{tag}/ja"], al=al, au=au,
+                        a=np.concatenate([al, au]) if unsym else al, ad=z[f"{tag}/ad"],
+                        b=z[f"{tag}/b"], x=z[f"{tag}/x"], tol=float(z[f"{tag}/tol"][0]),
+                        maxit=maxit, neq=neq)
+    return out
