@@ -1,24 +1,26 @@
-// Device assembly of the diffusion system: systFormDif (CellLoop.c:285-455)
-// -> cellDif3D (CellDif.c:312-537) -> csr()/ellPack() (Csr.c:549-1022,
-// EllPack.c:113-149), ndf = 1, ndm = 3, one process.
+// Device assembly: systFormDif (CellLoop.c:285-455) -> cellDif3D
+// (CellDif.c:312-537) and systFormSimplePres (CellLoopInc.c:471-700) ->
+// cellSimplePres3D (CellPres.c:903-1218), placing values as csr()/ellPack()
+// do (Csr.c:549-1022, EllPack.c:113-149); ndf = 1, ndm = 3, one process.
 //
 // Every cell writes exactly one row (its own), so the assembly is one thread
-// per equation with no atomics.  A plan binds the mesh to a system once:
+// per equation with no atomics.  A plan binds the mesh to a system once, on
+// the device:
 //   - cells are put in equation order, so that the per-call reads of the
 //     plan are coalesced and row r's outputs land at r;
-//   - what cellDif3D derives from the geometry alone (the owner-signed ksi
-//     and normal, the interpolation weight alpha of interpolFace, |E| of
-//     difusionSchemeNew and the explicit part t) is computed once, on the
-//     GPU, by the same IEEE operations in the same order, so that the
-//     per-call arithmetic starts from bit-identical values;
+//   - what the cell routines derive from the geometry alone (the
+//     owner-signed ksi and normal, interpolFace's alpha, and for diffusion
+//     |E| and the explicit part t of difusionSchemeNew) is computed once by
+//     the same IEEE operations in the same order, so that the per-call
+//     arithmetic starts from bit-identical values;
 //   - the destination of each coefficient in the reference's raw value array
-//     (al, al|au, or the ELLPACK slots) is resolved once from the system's
-//     own pattern.
+//     (al, al|au, or the ELLPACK slots) and in the solver's SELL copy is
+//     resolved from the system's own pattern.
 // A call then reads the plan (face-major, row-contiguous) and the per-cell
-// fields, and writes al|au, ad and b where solverC reads them; the system's
-// usual value refresh (the gather into its SELL copy) follows on the stream.
-// All products and sums use explicitly rounded intrinsics (no contraction),
-// in the reference's C evaluation order.
+// fields, and writes al|au, ad and b where solverC reads them, plus the
+// solver's SELL copy on full-row layouts.  All products, sums, divisions and
+// square roots use explicitly rounded intrinsics (no contraction), in the
+// reference's C evaluation order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
