@@ -288,6 +288,9 @@ typedef struct {
   double dt, dt0;    /* Temporal.dt[0], dt[1] */
 } sfr_dif_opts;
 
+/* A plan is not re-entrant: calls on one plan must not overlap (they share
+ * its staged load table and, for the host-array calls, its device buffers).
+ * Different plans may be used from different threads. */
 typedef struct sfr_dif_plan sfr_dif_plan;
 
 /* Bind a mesh to a system (whose pattern is the one dataStruct built for

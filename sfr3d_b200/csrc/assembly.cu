@@ -964,13 +964,28 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
   return SFR_OK;
 }
 
+// device copies for the host-array calls, allocated together on first use
+// (all or none, so that a failed allocation leaves the plan as it was)
 int ensure_host_buffers(sfr_dif_plan *p) {
   if (p->h_fields) return SFR_OK;
-  const size_t ne = p->numel;
-  SFR_CUA(cudaMalloc(&p->h_fields, sizeof(double) * ne * 10));
-  SFR_CUA(cudaMalloc(&p->h_b0, sizeof(double) * p->s->n));
-  SFR_CUA(cudaMalloc(&p->h_b, sizeof(double) * p->s->n));
-  SFR_CUA(cudaMalloc(&p->h_rcell, sizeof(double) * ne));
+  const size_t ne = p->numel, n = p->s->n;
+  double *f = nullptr, *b0 = nullptr, *b = nullptr, *rc = nullptr;
+  cudaError_t e = cudaMalloc(&f, sizeof(double) * ne * 10);
+  if (e == cudaSuccess) e = cudaMalloc(&b0, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&rc, sizeof(double) * ne);
+  if (e != cudaSuccess) {
+    cudaFree(f);
+    cudaFree(b0);
+    cudaFree(b);
+    cudaFree(rc);
+    sfr::set_last_error(cudaGetErrorString(e));
+    return SFR_CUDA_ERROR;
+  }
+  p->h_fields = f;
+  p->h_b0 = b0;
+  p->h_b = b;
+  p->h_rcell = rc;
   return SFR_OK;
 }
 
