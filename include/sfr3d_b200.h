@@ -365,6 +365,18 @@ int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
  * pointer may be NULL. */
 int sfr_gpu_get_values(sfr_system *s, double *al, double *ad, double *au);
 
+/* Matrix Market dumps in the reference's own format (writeCoo and writeCooB,
+ * WriteMtx.c:26-179, as the "pcoo" macro writes the assembled system,
+ * Main.c:995-1020): CSRD only; bin writes 1.0 for every entry (the "pgraph"
+ * macro).  sfr_gpu_write_coo dumps a device system (its values as
+ * sfr_gpu_get_values reads them) with the host's pattern. */
+int sfr_write_coo(const char *path, int32_t neq, const int32_t *ia, const int32_t *ja,
+                  const double *au, const double *ad, const double *al, int32_t nad,
+                  int32_t storage, int32_t unsym, int32_t bin);
+int sfr_write_coo_b(const char *path, const double *b, int32_t neq);
+int sfr_gpu_write_coo(sfr_system *s, const char *path, const int32_t *ia, const int32_t *ja,
+                      int32_t bin);
+
 /* x -> u as updateCellValue does after the solve (CellLoop.c:4023-4057,
  * ndf = 1): u[cell] = x[id[cell] - 1] (add = 0) or += (add = 1) for every
  * cell with id > 0, on device arrays. */

@@ -23,6 +23,7 @@
 
 #include <Solv.h>
 #include <CellLoop.h>
+#include <Coo.h>
 
 extern Omp ompVar;
 extern Mpi mpiVar;
@@ -321,4 +322,48 @@ int sfr_ref_syst_form_simple_pres(int numel, int maxviz, int *nelcon, short *nfa
   free(cc);
   free(wallpar);
   return rc;
+}
+
+/*
+ * The reference's Matrix Market dumps (WriteMtx.c, built with -D_MMIO_):
+ * writeCoo (the "pcoo"/"pgraph" macros of Main.c:975-1010) for the matrix,
+ * writeCooB for the force vector.  Returns the exit code when the reference
+ * exits (a storage other than CSRD).
+ */
+int sfr_ref_write_coo(int neq, int nad, int *ia, int *ja, double *au, double *ad, double *al,
+                      int storage, int unsym, int bin, const char *name)
+{
+  Memoria mem;
+  char path[1024];
+  int rc = 0;
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  nmax = (iptx)3 * (iptx)(neq + nad + 64) * (iptx)sizeof(double) + 65536;
+  initMem(&mem, nmax, false);
+  {
+    DOUBLE *base = NULL;
+    HccaAlloc(DOUBLE, &mem, base, 8, "harness_base", false);
+    (void)base;
+  }
+  strncpy(path, name, sizeof(path) - 1);
+  path[sizeof(path) - 1] = 0;
+  if (setjmp(g_jump) == 0) {
+    g_armed = 1;
+    writeCoo(&mem, ia, ja, neq, au, ad, al, nad, (short)storage, unsym != 0, bin != 0, path);
+    fflush(NULL);
+    g_armed = 0;
+  } else {
+    rc = g_exit_code == 0 ? -1000 : g_exit_code;
+  }
+  finalizeMem(&mem, false);
+  return rc;
+}
+
+void sfr_ref_write_coo_b(double *b, int neq, const char *name)
+{
+  char path[1024];
+  strncpy(path, name, sizeof(path) - 1);
+  path[sizeof(path) - 1] = 0;
+  writeCooB(b, neq, path);
+  fflush(NULL);  /* writeCooB leaves its file open */
 }

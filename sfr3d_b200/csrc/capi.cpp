@@ -201,6 +201,90 @@ int sfr_gpu_set_values(sfr_system *s, const double *al, const double *ad, const 
   return SFR_OK;
 }
 
+// Matrix Market dumps as the reference writes them (WriteMtx.c:26-179 with
+// its vendored writer): the diagonal then the stored entries of each row,
+// 1-based, "%d %d %30.14e"; values al below the diagonal and, for unsym, au
+// above it (csrToCoo).  Only CSRD, as writeCoo.
+int sfr_write_coo(const char *path, int32_t neq, const int32_t *ia, const int32_t *ja,
+                  const double *au, const double *ad, const double *al, int32_t nad,
+                  int32_t storage, int32_t unsym, int32_t bin) {
+  if (!path || neq < 0 || nad < 0 || !ia || (nad > 0 && !ja)) {
+    g_last_error = "NULL argument or negative size";
+    return SFR_BAD_INPUT;
+  }
+  if (storage != SFR_CSRD) {
+    g_last_error = "writeCoo writes CSRD only";
+    return SFR_BAD_INPUT;
+  }
+  if (!bin && (!ad || (nad > 0 && (!al || (unsym && !au))))) {
+    g_last_error = "values are NULL";
+    return SFR_BAD_INPUT;
+  }
+  if (ia[neq] - ia[0] != nad) {
+    g_last_error = "ia[neq] - ia[0] != nad";
+    return SFR_BAD_INPUT;
+  }
+  std::unique_ptr<FILE, int (*)(FILE *)> f(std::fopen(path, "w"), &std::fclose);
+  if (!f) {
+    g_last_error = std::string("cannot open ") + path;
+    return SFR_BAD_INPUT;
+  }
+  std::fprintf(f.get(), "%%%%MatrixMarket matrix coordinate real %s\n",
+               unsym ? "general" : "symmetric");
+  std::fprintf(f.get(), "%d %d %d\n", neq, neq, neq + nad);
+  for (int32_t i = 0; i < neq; ++i) {
+    const int32_t row = i + 1;
+    std::fprintf(f.get(), "%d %d %30.14e\n", row, row, bin ? 1.0 : ad[i]);
+    for (int32_t k = ia[i]; k < ia[i + 1]; ++k) {
+      const int32_t col = ja[k] + 1;
+      double v = 0.0;
+      if (bin)
+        v = 1.0;
+      else if (col < row)
+        v = al[k];
+      else if (col > row && unsym)
+        v = au[k];
+      std::fprintf(f.get(), "%d %d %30.14e\n", row, col, v);
+    }
+  }
+  return std::ferror(f.get()) ? SFR_BAD_INPUT : SFR_OK;
+}
+
+int sfr_write_coo_b(const char *path, const double *b, int32_t neq) {
+  if (!path || !b || neq < 0) {
+    g_last_error = "NULL argument or negative size";
+    return SFR_BAD_INPUT;
+  }
+  std::unique_ptr<FILE, int (*)(FILE *)> f(std::fopen(path, "w"), &std::fclose);
+  if (!f) {
+    g_last_error = std::string("cannot open ") + path;
+    return SFR_BAD_INPUT;
+  }
+  // writeCooB's own banner (WriteMtx.c:171-176: one '%')
+  std::fprintf(f.get(), "%%MatrixMarket matrix array real general\n");
+  std::fprintf(f.get(), "%d %d\n", neq, 1);
+  for (int32_t i = 0; i < neq; ++i) std::fprintf(f.get(), "%.14e\n", b[i]);
+  return std::ferror(f.get()) ? SFR_BAD_INPUT : SFR_OK;
+}
+
+int sfr_gpu_write_coo(sfr_system *s, const char *path, const int32_t *ia, const int32_t *ja,
+                      int32_t bin) {
+  if (!s || !ia) {
+    g_last_error = "NULL argument";
+    return SFR_BAD_INPUT;
+  }
+  if (s->storage != SFR_CSRD) {
+    g_last_error = "writeCoo writes CSRD only";
+    return SFR_BAD_INPUT;
+  }
+  std::vector<double> al(static_cast<size_t>(std::max(s->nsrc, 1))), ad(s->n);
+  const int rc = sfr_gpu_get_values(s, al.data(), ad.data(), nullptr);
+  if (rc != SFR_OK) return rc;
+  // CSRD keeps every stored value in al: above the diagonal too
+  return sfr_write_coo(path, s->n, ia, ja, al.data(), ad.data(), al.data(), s->nsrc,
+                       s->storage, s->unsym, bin);
+}
+
 int sfr_gpu_get_values(sfr_system *s, double *al, double *ad, double *au) {
   if (!s) return SFR_BAD_INPUT;
   if (!s->values_set) {

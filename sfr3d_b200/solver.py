@@ -110,6 +110,10 @@ def lib() -> ctypes.CDLL:
     L.sfr_set_reliable_delta.argtypes = [ctypes.c_double]
     L.sfr_set_reliable_delta.restype = None
     L.sfr_set_solver_reliable_delta.argtypes = [_I32, ctypes.c_double]
+    L.sfr_write_coo.argtypes = [ctypes.c_char_p, _I32, _P, _P, _P, _P, _P, _I32, _I32, _I32,
+                                _I32]
+    L.sfr_write_coo_b.argtypes = [ctypes.c_char_p, _P, _I32]
+    L.sfr_gpu_write_coo.argtypes = [_P, ctypes.c_char_p, _P, _P, _I32]
     L.sfr_set_precision.restype = None
     L.sfr_solverC_release.restype = None
     L.sfr_solverC_release.argtypes = []
@@ -275,6 +279,14 @@ class GpuSystem:
         n = int(self._ia[self.neq] - self._ia[0])
         return 2 * n if (self.storage == CSRC and self.unsym) else n
 
+    def write_coo(self, path, binary=False):
+        """The system's current values as the reference's writeCoo dump
+        (CSRD only), e.g. right after a device assembly."""
+        rc = lib().sfr_gpu_write_coo(self.h, str(path).encode(), _ptr(self._ia),
+                                     _ptr(self._ja), int(binary))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_write_coo: " + last_error())
+
     # device-pointer entry points (pointers are plain integers)
     def solve_device(self, solver, d_b: int, d_x: int, tol=1e-10,
                      maxit=100000, newx=True, precision=FP64, stream: int = 0):
@@ -437,3 +449,43 @@ def set_reliable_delta(delta: float, solver: int | None = None) -> None:
 
 def release_cache() -> None:
     lib().sfr_solverC_release()
+
+
+# ------------------------------------------------------ Matrix Market --
+def write_coo(path, ia, ja, ad, al, au=None, storage=CSRD, unsym=True, binary=False):
+    """The reference's writeCoo (WriteMtx.c:26): the CSRD system as a Matrix
+    Market coordinate file, diagonal first in each row."""
+    ia, ja = _i32(ia), _i32(ja)
+    ad, al = _f64(ad), _f64(al)
+    au = al if au is None else _f64(au)
+    rc = lib().sfr_write_coo(str(path).encode(), len(ia) - 1, _ptr(ia), _ptr(ja), _ptr(au),
+                             _ptr(ad), _ptr(al), len(ja), storage, int(unsym), int(binary))
+    if rc != OK:
+        raise SolverError(rc, "sfr_write_coo: " + last_error())
+
+
+def write_coo_b(path, b):
+    """The reference's writeCooB (WriteMtx.c:163): a force vector."""
+    b = _f64(b)
+    rc = lib().sfr_write_coo_b(str(path).encode(), _ptr(b), len(b))
+    if rc != OK:
+        raise SolverError(rc, "sfr_write_coo_b: " + last_error())
+
+
+def read_mtx(path):
+    """A Matrix Market file as written by write_coo / write_coo_b (or any
+    real coordinate / array file): ("coordinate", rows, cols, (i, j, v)
+    0-based, symmetric flag) or ("array", rows, cols, values)."""
+    with open(path) as f:
+        banner = f.readline().split()
+        kind = banner[2]
+        line = f.readline()
+        while line.startswith("%"):
+            line = f.readline()
+        dims = [int(t) for t in line.split()]
+        if kind == "coordinate":
+            data = np.loadtxt(f, ndmin=2)
+            i = data[:, 0].astype(np.int64) - 1
+            j = data[:, 1].astype(np.int64) - 1
+            return "coordinate", dims[0], dims[1], (i, j, data[:, 2]), banner[4] == "symmetric"
+        return "array", dims[0], dims[1], np.loadtxt(f, ndmin=1)

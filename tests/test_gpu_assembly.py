@@ -421,3 +421,27 @@ def test_pres_validation(cuda, box):
                   z3, z3, z3)
     plan.close()
     gs.close()
+
+
+def test_device_system_dumped_as_the_reference_writes_it(cuda, box, tmp_path):
+    """The pcoo macro's dump (writeCoo) of a system assembled on the device:
+    byte for byte the dump of the oracle's assembly."""
+    s, m, lay = box
+    rng = np.random.default_rng(15)
+    for name in ("csrd_full", "csrd_sym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        case = O.DifCase(mesh=m, facer=m.face_r(SIDES), loads=LOADS[:3] + LOADS[3:],
+                         density=np.ones(m.numel), cdiff=m.cdiff,
+                         u0=rng.standard_normal(m.numel), gradu0=np.zeros((m.numel, 3)))
+        rc, a, ad, b, _ = O.dif_assemble(case, st, un, ia, ja, s.neq)
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.DifPlan(gs, m, case.facer)
+        bd, _ = plan.assemble(_loads(case.loads), case.u0, case.cdiff, calrcell=False)
+        gs.write_coo(tmp_path / "dev.mtx")
+        sv.write_coo(tmp_path / "ref.mtx", ia, ja, ad, a, unsym=un)
+        assert (tmp_path / "dev.mtx").read_bytes() == (tmp_path / "ref.mtx").read_bytes()
+        sv.write_coo_b(tmp_path / "bd.mtx", bd)
+        sv.write_coo_b(tmp_path / "br.mtx", b)
+        assert (tmp_path / "bd.mtx").read_bytes() == (tmp_path / "br.mtx").read_bytes()
+        plan.close()
+        gs.close()
