@@ -505,3 +505,140 @@ def ref_pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
         case.icod, neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym),
         nthreads, ctypes.byref(sec))
     return rc, a, ad, b, rcell, sec.value
+
+
+# ------------------------------------------------------ momentum assembly --
+# systFormSimpleVel (CellLoopInc.c:98-470) -> cellSimpleVel3D (CellSimple.c:106)
+SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
+
+
+@dataclass
+class VelCase:
+    """What one laminar, first-order-upwind systFormSimpleVel call reads:
+    the mesh arrays plus centroids cc (numel, 3) and face centres xm
+    (nface, 3), faceVelR / faceRpres, the velocity loads, the material
+    table (DYNAMICVISCOSITY column 0, DENSITY 1) and the cell fields (gradvel
+    (numel, 3, 3), row i = grad u_i; dfield is updated in place)."""
+    mesh: object
+    cc: np.ndarray
+    facevelr: np.ndarray
+    facepresr: np.ndarray
+    lvel: list
+    prop: np.ndarray
+    pres: np.ndarray
+    gradpres: np.ndarray
+    vel: np.ndarray
+    gradvel: np.ndarray
+    dfield: np.ndarray
+    icod: int = ORTHOGONAL
+    fso: bool = True
+    fvisc: bool = False
+    fres: bool = True
+    type_simple: int = SIMPLE
+    time_flag: bool = False
+    time_type: int = EULER
+    dt: float = 1.0
+    dt0: float = 1.0
+    under: float = 0.7
+    mat: np.ndarray | None = None
+    caltype: np.ndarray | None = None
+
+    def material(self):
+        mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
+               else _c(self.mat, np.int16))
+        nmat = len(np.asarray(self.prop).reshape(-1, MAXPROP))
+        cal = np.ones(nmat, np.int16) if self.caltype is None else _c(self.caltype, np.int16)
+        return cal, mat
+
+
+class _VelOpts(ctypes.Structure):
+    _fields_ = [("icod", ctypes.c_int), ("fso", ctypes.c_int), ("fvisc", ctypes.c_int),
+                ("fres", ctypes.c_int), ("type_simple", ctypes.c_int),
+                ("time_flag", ctypes.c_int), ("time_type", ctypes.c_int),
+                ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double)]
+
+
+def _vel_out(storage, unsym, neq, ia, ja, numel, fill):
+    a = np.full(dif_size(storage, unsym, neq, ia, ja), fill)
+    return a, np.full(3 * neq, fill), np.full(3 * neq, fill), np.full(3 * numel, fill)
+
+
+def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix=True,
+                 calrcell=True, fill=0.0):
+    """The C restatement: (rc, a, ad, b, rcell, dfield)."""
+    m = case.mesh
+    lib = oracle_lib()
+    if not getattr(lib, "_vel_typed", False):
+        lib.orc_vel_assemble.restype = ctypes.c_int
+        lib.orc_vel_assemble.argtypes = (
+            [ctypes.POINTER(_DifMesh), _P, _P, _P, _P, ctypes.c_int, ctypes.POINTER(_VelOpts)]
+            + [_P] * 6 + [ctypes.c_int] * 4 + [_P] * 6 + [ctypes.c_int] * 3)
+        lib._vel_typed = True
+    cal, mat = case.material()
+    keep = dict(
+        nelcon=_c(m.nelcon, np.int32), nface=_c(m.nviz, np.int16),
+        cellface=_c(m.cellface, np.int32), owner=_c(m.owner, np.int32),
+        volume=_c(m.volume, np.float64), dcca=_c(m.dcca, np.float64),
+        xmcc=_c(m.xmcc, np.float64), mksi=_c(m.mksi, np.float64),
+        ksi=_c(m.ksi, np.float64), area=_c(m.area, np.float64),
+        normal=_c(m.normal, np.float64), vskew=_c(m.vskew, np.float64),
+        caltype=cal, mat=mat, id=_c(m.id, np.int32), facer=_c(case.facevelr, np.int16))
+    dm = _DifMesh(numel=m.numel, maxviz=m.nelcon.shape[1],
+                  **{k: _p(v) for k, v in keep.items()})
+    o = _VelOpts(icod=case.icod, fso=int(case.fso), fvisc=int(case.fvisc),
+                 fres=int(case.fres), type_simple=case.type_simple,
+                 time_flag=int(case.time_flag), time_type=case.time_type, dt=case.dt,
+                 dt0=case.dt0, under=case.under)
+    ia, ja = _c(ia, np.int32), _c(ja, np.int32)
+    a, ad, b, rc_ = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    dfield = np.array(case.dfield, dtype=np.float64, copy=True, order="C")
+    fpr = _c(case.facepresr, np.int16)
+    cc, xm = _c(case.cc, np.float64), _c(m.xm, np.float64)
+    lv = _load_table(case.lvel)
+    fields = [_c(case.prop, np.float64), _c(case.pres, np.float64),
+              _c(case.gradpres, np.float64), _c(case.vel, np.float64),
+              _c(case.gradvel, np.float64), dfield]
+    nad = len(ja) if storage != ELLPACK else 0
+    rc = lib.orc_vel_assemble(ctypes.byref(dm), _p(fpr), _p(cc), _p(xm), lv, len(case.lvel),
+                              ctypes.byref(o), *[_p(f) for f in fields], storage, int(unsym),
+                              neq, nad, _p(ia), _p(ja), _p(a), _p(ad), _p(b), _p(rc_),
+                              int(forces), int(matrix), int(calrcell))
+    return rc, a, ad, b, rc_, dfield
+
+
+def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix=True,
+                     calrcell=True, fill=0.0):
+    """The reference's own systFormSimpleVel: (rc, a, ad, b, rcell, dfield, seconds)."""
+    m = case.mesh
+    lib = ref_lib()
+    if not getattr(lib, "_vel_typed", False):
+        lib.sfr_ref_syst_form_simple_vel.restype = ctypes.c_int
+        lib.sfr_ref_syst_form_simple_vel.argtypes = (
+            [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
+            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 7 + [_P])
+        lib._vel_typed = True
+    cal, mat = case.material()
+    cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
+    ia, ja = cp(ia, np.int32), cp(ja, np.int32)
+    a, ad, b, rcell = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
+    dfield = cp(case.dfield, np.float64)
+    vt = _load_arrays(case.lvel)
+    sec = ctypes.c_double()
+    arrs = [cp(m.nelcon, np.int32), cp(m.nviz, np.int16), cp(m.cellface, np.int32),
+            cp(m.owner, np.int32), cp(m.volume, np.float64), cp(m.dcca, np.float64),
+            cp(m.xmcc, np.float64), cp(case.cc, np.float64), cp(m.mksi, np.float64),
+            cp(m.ksi, np.float64), cp(m.eta, np.float64), cp(m.area, np.float64),
+            cp(m.normal, np.float64), cp(m.xm, np.float64), cp(m.mvskew, np.float64),
+            cp(m.vskew, np.float64), cal.copy(), mat.copy(), cp(case.prop, np.float64), ia, ja,
+            a, ad, b, cp(m.id, np.int32), cp(case.facevelr, np.int16),
+            cp(case.facepresr, np.int16), cp(case.pres, np.float64),
+            cp(case.gradpres, np.float64), cp(case.vel, np.float64),
+            cp(case.gradvel, np.float64), dfield, rcell]
+    nad = len(ja) if storage != ELLPACK else int(ia[1])
+    rc = lib.sfr_ref_syst_form_simple_vel(
+        m.numel, m.nelcon.shape[1], *[_p(x) for x in arrs], len(case.lvel),
+        *[_p(x) for x in vt], case.icod, int(case.fso), int(case.fvisc), int(case.fres),
+        case.type_simple, int(case.time_flag), case.time_type, case.dt, case.dt0, case.under,
+        neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym),
+        ctypes.byref(sec))
+    return rc, a, ad, b, rcell, dfield, sec.value

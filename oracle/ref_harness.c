@@ -367,3 +367,87 @@ void sfr_ref_write_coo_b(double *b, int neq, const char *name)
   writeCooB(b, neq, path);
   fflush(NULL);  /* writeCooB leaves its file open */
 }
+
+/*
+ * Assemble the SIMPLE momentum system with the reference's own
+ * systFormSimpleVel (CellLoopInc.c:98-470) as velPresCoupling calls it
+ * (Simple.c:2864-2898): ndf = 3, laminar (Turbulence all off), first-order
+ * upwind, without Rhie-Chow, serial.  dfield is updated in place.
+ */
+int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nface,
+                                 int *cellface, int *owner, double *volume, double *dcca,
+                                 double *xmcc, double *cc, double *mksi, double *ksi,
+                                 double *eta, double *area, double *normal, double *xm,
+                                 double *mvskew, double *vskew, short *caltype, short *mat,
+                                 double *prop, int *ia, int *ja, double *a, double *ad,
+                                 double *b, int *id, short *facevelr, short *facepresr,
+                                 double *pres, double *gradpres, double *vel, double *gradvel,
+                                 double *dfield, double *rcell, int nlvel, const int *vtype,
+                                 const int *vvar, const int *vnp, const double *vpar,
+                                 const double *vdens, int icod, int fso, int fvisc, int fres,
+                                 int type_simple, int time_flag, int time_type, double dt,
+                                 double dt0, double under, int neq, int nad, int storage,
+                                 int forces, int matrix, int calrcell, int unsym,
+                                 double *seconds)
+{
+  INT *el = calloc((size_t)numel * 8, sizeof(INT));
+  short *nen = malloc((size_t)numel * sizeof(short));
+  short *gtype = calloc((size_t)numel, sizeof(short));
+  double *stressr = calloc((size_t)numel * 6, sizeof(double));
+  double *eddy = calloc((size_t)numel, sizeof(double));
+  double *wallpar = calloc((size_t)numel * NWALLPAR, sizeof(double));
+  Advection adv;
+  Diffusion diff;
+  Turbulence tmodel;
+  MomentumModel mm;
+  Temporal ddt;
+  int i, rc = 0;
+  double t0;
+
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  mpiVar.nPrcs = 1;
+  mpiVar.myId = 0;
+  ompVar.fCell = false;
+  ompVar.nThreadsCell = 1;
+  for (i = 0; i < numel; i++) nen[i] = 8;
+  fill_loads(loadsVel, nlvel, vtype, vvar, vnp, vpar, vdens);
+  memset(&adv, 0, sizeof(adv));
+  memset(&diff, 0, sizeof(diff));
+  memset(&tmodel, 0, sizeof(tmodel));
+  memset(&mm, 0, sizeof(mm));
+  memset(&ddt, 0, sizeof(ddt));
+  adv.iCod1 = FOUP;
+  diff.iCod = (short)icod;
+  mm.fRes = fres != 0;
+  mm.fRhieChowInt = false;
+  mm.fViscosity = fvisc != 0;
+  mm.fSoPressure = fso != 0;
+  ddt.flag = time_flag != 0;
+  ddt.type = (short)time_type;
+  ddt.dt[0] = dt;
+  ddt.dt[1] = dt0;
+  *seconds = 0.0;
+  if (setjmp(g_jump) == 0) {
+    g_armed = 1;
+    t0 = omp_get_wtime();
+    systFormSimpleVel(loadsVel, loadsPres, &adv, &diff, &tmodel, &mm, NULL, (short)type_simple,
+                      el, nelcon, nen, nface, cellface, owner, volume, dcca, xmcc, cc, mksi,
+                      ksi, eta, area, normal, xm, mvskew, vskew, gtype, prop, caltype, mat,
+                      ia, ja, a, ad, b, id, facevelr, facepresr, pres, gradpres, vel, gradvel,
+                      dfield, under, rcell, stressr, eddy, wallpar, &ddt, neq, neq, nad, 0, 8,
+                      (short)maxviz, 3, numel, 3, 6, (short)storage, forces != 0,
+                      matrix != 0, calrcell != 0, unsym != 0);
+    *seconds = omp_get_wtime() - t0;
+    g_armed = 0;
+  } else {
+    rc = g_exit_code == 0 ? -1000 : g_exit_code;
+  }
+  free(el);
+  free(nen);
+  free(gtype);
+  free(stressr);
+  free(eddy);
+  free(wallpar);
+  return rc;
+}

@@ -980,3 +980,243 @@ int orc_pres_assemble(const orc_dif_mesh *m, const short *facevelr,
   }
   return 0;
 }
+
+/* ======================================================================
+ * Momentum assembly: systFormSimpleVel (CellLoopInc.c:98-470) calling
+ * cellSimpleVel3D (CellSimple.c:106-727) per cell, placed by csrSimple
+ * (Csr.c:1024-1200): laminar (no eddy viscosity, no structural stress, no
+ * wall model), first-order upwind (advectiveScheme FOUP, CellLib.c:6394:
+ * no deferred correction), face velocity without Rhie-Chow.
+ * ====================================================================== */
+
+/* moveWall, not Dirichlet (CellLib.c:7715-7770): the wall's tangential
+ * stress on the diagonals sPc and the force p */
+static void move_wall(const double vC[3], const double vB[3], const double n[3], double sPc[3],
+                      double p[3], double dcca, double visc, double area)
+{
+  const double aP = visc * area / dcca;
+  sPc[0] += aP * (1.e0 - n[0] * n[0]);
+  sPc[1] += aP * (1.e0 - n[1] * n[1]);
+  sPc[2] += aP * (1.e0 - n[2] * n[2]);
+  p[0] += aP * (vB[0] * (1.0 - n[0] * n[0]) + (vC[1] - vB[1]) * n[1] * n[0] +
+                (vC[2] - vB[2]) * n[2] * n[0]);
+  p[1] += aP * (vB[1] * (1.0 - n[1] * n[1]) + (vC[0] - vB[0]) * n[0] * n[1] +
+                (vC[2] - vB[2]) * n[2] * n[1]);
+  p[2] += aP * (vB[2] * (1.0 - n[2] * n[2]) + (vC[0] - vB[0]) * n[0] * n[2] +
+                (vC[1] - vB[1]) * n[1] * n[2]);
+}
+
+int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
+                     const double *xm, const orc_load *lvel, int nlvel,
+                     const orc_vel_opts *o, const double *prop, const double *pres,
+                     const double *gradpres, const double *vel, const double *gradvel,
+                     double *dfield, int storage, int unsym, int neq, int nad,
+                     const int *ia, const int *ja, double *a, double *ad, double *b,
+                     double *rcell, int forces, int matrix, int calrcell)
+{
+  enum { MAXF = 32 };
+  const int mv = m->maxviz, numel = m->numel;
+  int nel, f, i, j, k;
+  (void)facepresr;
+  if (mv < 1 || mv > MAXF - 1 || storage == ORC_ELLPACK) return -1;
+  /* any other typeSimple leaves D as the first neighbour's copy */
+  if (o->type_simple != 1 && o->type_simple != 2) return -1;
+  for (nel = 0; nel < numel; nel++) {
+    double lA[MAXF + 3], ksi[3], nrm[3], s[3], e[3], t[3];
+    double p[3] = {0.0, 0.0, 0.0}, pf[3] = {0.0, 0.0, 0.0}, sPc[3] = {0.0, 0.0, 0.0};
+    double rc[3], lB[3], gvC[3][3], velC[3], gpC[3], sP = 0.0, lAn, rhoC, muC, effC, presC;
+    int viz[MAXF], lid[MAXF], lm, row;
+    const int nf = m->nface[nel];
+    const short *fr = m->facer + (long)nel * (mv + 1);
+    if (calrcell) {
+      rcell[nel] = 0.e0;
+      rcell[numel + nel] = 0.e0;
+      rcell[2 * numel + nel] = 0.e0;
+    }
+    if (nf < 1 || nf > mv) return -1;
+    if (fr[nf] > 0) continue; /* prescribed velocity: no equation */
+    lm = m->mat[nel] - 1;
+    if (m->caltype[lm] != 1) return -1;
+    row = m->id[nel] - 1;
+    rhoC = prop[lm * ORC_MAXPROP + ORC_DENSITY];
+    muC = prop[lm * ORC_MAXPROP + 0];
+    effC = muC + 0.0e0; /* laminar: no eddy viscosity */
+    presC = pres[nel];
+    for (i = 0; i < 3; i++) {
+      for (j = 0; j < 3; j++) gvC[i][j] = gradvel[9 * (long)nel + 3 * i + j];
+      gpC[i] = gradpres[3 * (long)nel + i];
+      velC[i] = vel[3 * (long)nel + i];
+    }
+    for (f = 0; f < nf; f++) {
+      const long q = (long)nel * mv + f;
+      const int face = m->cellface[q] - 1;
+      const double ch = (m->owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+      const double mk = m->mksi[face], area = m->area[face];
+      const double *xmcc = m->xmcc + 3 * q;
+      viz[f] = m->nelcon[q] - 1;
+      lid[f] = viz[f] != -2 ? m->id[viz[f]] - 1 : -1;
+      for (j = 0; j < 3; j++) {
+        ksi[j] = ch * m->ksi[3 * face + j];
+        nrm[j] = ch * m->normal[3 * face + j];
+      }
+      if (viz[f] > -1) {
+        const int nb = viz[f];
+        const int lmv = m->mat[nb] - 1;
+        const double rhoV = prop[lmv * ORC_MAXPROP + ORC_DENSITY];
+        const double effV = prop[lmv * ORC_MAXPROP + 0] + 0.0e0;
+        const double presV = pres[nb];
+        double velV[3], gpV[3], duDksi[3], gvV[3][3], ccV[3], lXm[3], v[3];
+        double alpha, am1, visc, modE, dfd, density, wfn, cv, gf[3][3], wf[3], gvc[3][3];
+        double dfdc[3], gk, du, p1, p2, pFace, tmp;
+        for (i = 0; i < 3; i++) {
+          velV[i] = vel[3 * (long)nb + i];
+          gpV[i] = gradpres[3 * (long)nb + i];
+          duDksi[i] = (velV[i] - velC[i]) / mk;
+          for (j = 0; j < 3; j++) gvV[i][j] = gradvel[9 * (long)nb + 3 * i + j];
+          ccV[i] = cc[3 * (long)nb + i];
+          lXm[i] = xm[3 * (long)face + i];
+        }
+        for (j = 0; j < 3; j++) s[j] = area * nrm[j];
+        if (dif_scheme(s, ksi, e, t, o->icod)) return -1;
+        for (j = 0; j < 3; j++) v[j] = m->vskew[3 * face + j] + xmcc[j];
+        alpha = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / mk;
+        am1 = 1.0e0 - alpha;
+        /* mediaHarmonica (CellLib.c:7879) */
+        visc = (effC == 0.e0 || effV == 0.e0) ? 0.e0 : 1.e0 / (alpha / effC + am1 / effV);
+        modE = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        dfd = visc * modE / mk;
+        for (i = 0; i < 3; i++) {
+          for (j = 0; j < 3; j++) gf[i][j] = am1 * gvC[i][j] + alpha * gvV[i][j];
+          wf[i] = am1 * velC[i] + alpha * velV[i];
+        }
+        density = am1 * rhoC + alpha * rhoV;
+        wfn = wf[0] * nrm[0] + wf[1] * nrm[1] + wf[2] * nrm[2];
+        for (i = 0; i < 3; i++) {
+          gk = gf[i][0] * ksi[0] + gf[i][1] * ksi[1] + gf[i][2] * ksi[2];
+          du = duDksi[i] - gk;
+          for (j = 0; j < 3; j++) gvc[i][j] = gf[i][j] + du * ksi[j];
+          gk = gvc[i][0] * t[0] + gvc[i][1] * t[1] + gvc[i][2] * t[2];
+          dfdc[i] = visc * gk;
+        }
+        cv = density * wfn * area;
+        lA[f] = dfd - (cv < 0.0e0 ? cv : 0.0e0);
+        sP += cv;
+        for (i = 0; i < 3; i++) p[i] += dfdc[i] - cv * 0.e0; /* FoUp: cvc = 0 */
+        /* facePressure (CellLib.c:7499), interior */
+        if (o->fso) {
+          for (j = 0; j < 3; j++) v[j] = lXm[j] - ccV[j];
+          p1 = presC + gpC[0] * xmcc[0] + gpC[1] * xmcc[1] + gpC[2] * xmcc[2];
+          p2 = presV + gpV[0] * v[0] + gpV[1] * v[1] + gpV[2] * v[2];
+          pFace = 0.5e0 * (p1 + p2);
+        } else {
+          pFace = am1 * presC + alpha * presV;
+        }
+        tmp = pFace * area;
+        for (i = 0; i < 3; i++) pf[i] += tmp * nrm[i];
+        /* viscosityPartExp (CellLib.c:7439), fDiv false */
+        if (o->fvisc) {
+          const double aP = muC * area;
+          for (i = 0; i < 3; i++)
+            p[i] += aP * (gvc[0][i] * nrm[0] + gvc[1][i] * nrm[1] + gvc[2][i] * nrm[2]);
+        }
+      } else {
+        double tmp;
+        lA[f] = 0.0e0;
+        /* facePressure, boundary: the cell's own pressure on the face */
+        tmp = presC * area;
+        for (i = 0; i < 3; i++) pf[i] += tmp * nrm[i];
+        for (j = 0; j < 3; j++) s[j] = area * nrm[j];
+        if (dif_scheme(s, ksi, e, t, o->icod)) return -1;
+        if (fr[f]) {
+          const int l = fr[f] - 1;
+          const orc_load *ld;
+          double tA[3] = {0.0, 0.0, 0.0};
+          if (l < 0 || l >= nlvel) return -1;
+          ld = &lvel[l];
+          if (ld->type == 8 || ld->type == 14) { /* MOVEWALL, STATICWALL */
+            if (ld->type == 8)
+              for (j = 0; j < 3; j++) tA[j] = ld->par[j];
+            move_wall(velC, tA, nrm, sPc, p, m->dcca[q], effC, area);
+          } else if (ld->type == 6) { /* INLET */
+            double wfn, ss[6], tr, mflux;
+            if (ld->var != 0) return -2;
+            if (ld->np < 3) return -1;
+            for (j = 0; j < 3; j++) tA[j] = ld->par[j];
+            wfn = tA[0] * nrm[0] + tA[1] * nrm[1];
+            wfn += tA[2] * nrm[2];
+            mflux = ld->par[ld->np - 1] * wfn * area;
+            /* stress (CellLib.c:7013), lambda = 0 */
+            tr = gvC[0][0] + gvC[1][1] + gvC[2][2];
+            ss[0] = 2.e0 * muC * gvC[0][0] + 0.0 * tr;
+            ss[1] = 2.e0 * muC * gvC[1][1] + 0.0 * tr;
+            ss[2] = 2.e0 * muC * gvC[2][2] + 0.0 * tr;
+            ss[3] = muC * (gvC[1][0] + gvC[0][1]);
+            ss[4] = muC * (gvC[2][1] + gvC[1][2]);
+            ss[5] = muC * (gvC[2][0] + gvC[0][2]);
+            p[0] += ss[0] * s[0] + ss[3] * s[1] + ss[5] * s[2];
+            p[1] += ss[3] * s[0] + ss[1] * s[1] + ss[4] * s[2];
+            p[2] += ss[5] * s[0] + ss[4] * s[1] + ss[2] * s[2];
+            p[0] -= mflux * tA[0];
+            p[1] -= mflux * tA[1];
+            p[2] -= mflux * tA[2];
+          } else if (ld->type == 7 || ld->type == 9 || ld->type == 10 || ld->type == 13) {
+            return -2; /* OUTLET, INLETSTAICTPRES, OPEN, INLETTOTALPRES */
+          }
+        }
+      }
+    }
+    /* implicit time term, CellSimple.c:606-617 */
+    if (o->time_flag) {
+      if (o->time_type == 0)
+        sP += rhoC * m->volume[nel] / o->dt;
+      else if (o->time_type == 1) {
+        const double tmp = 1.e0 / o->dt + 1.e0 / (o->dt + o->dt0);
+        sP += tmp * rhoC * m->volume[nel];
+      }
+    }
+    lAn = 0.e0;
+    for (f = 0; f < nf; f++) lAn += lA[f];
+    for (k = 0; k < 3; k++) lA[nf + k] = sP + sPc[k] + lAn;
+    for (k = 0; k < 3; k++) lA[nf + k] = lA[nf + k] / o->under;
+    for (k = 0; k < 3; k++) p[k] += (1 - o->under) * lA[nf + k] * velC[k];
+    for (k = 0; k < 3; k++) p[k] -= pf[k];
+    for (k = 0; k < 3; k++) rc[k] = 0.0e0;
+    for (f = 0; f < nf; f++)
+      if (viz[f] > -1)
+        for (k = 0; k < 3; k++) {
+          if (lid[f] == -2)
+            p[k] += lA[f] * vel[3 * (long)viz[f] + k];
+          else
+            rc[k] += lA[f] * vel[3 * (long)viz[f] + k];
+        }
+    for (k = 0; k < 3; k++) rc[k] += p[k] - lA[nf + k] * velC[k];
+    /* the momentum D field, written back in place (CellLoopInc.c, after
+     * cellLibSimpleVel) */
+    for (k = 0; k < 3; k++)
+      dfield[3 * (long)nel + k] = o->type_simple == 2
+                                      ? m->volume[nel] / (lA[nf + k] - lAn)
+                                      : m->volume[nel] / lA[nf + k];
+    for (f = 0; f < nf; f++) lA[f] *= -1.e0;
+    for (k = 0; k < 3; k++) lB[k] = o->fres ? rc[k] : p[k];
+    if (calrcell)
+      for (k = 0; k < 3; k++) rcell[(long)k * numel + nel] = rc[k];
+    /* csrSimple (Csr.c:1024), ndf = 3 */
+    if (forces)
+      for (k = 0; k < 3; k++) b[(long)k * neq + row] = lB[k];
+    if (!matrix) continue;
+    for (k = 0; k < 3; k++) ad[(long)k * neq + row] = lA[nf + k];
+    for (f = 0; f < nf; f++) {
+      const int c = lid[f];
+      if (c <= -1) continue;
+      if (storage == ORC_CSRC && unsym) {
+        if (c < row)
+          dif_put(ia, ja, row, c, a, lA[f]);
+        else if (c > row)
+          dif_put(ia, ja, c, row, a + nad, lA[f]);
+      } else {
+        dif_put(ia, ja, row, c, a, lA[f]);
+      }
+    }
+  }
+  return 0;
+}

@@ -140,4 +140,35 @@ int orc_pres_assemble(const orc_dif_mesh *m, const short *facevelr,
                       const int *ja, double *a, double *ad, double *b,
                       double *rcell, int forces, int matrix, int calrcell);
 
+/* ---- momentum assembly (systFormSimpleVel, CellLoopInc.c:98-470 ->
+ *      cellSimpleVel3D, CellSimple.c:106-727), laminar, first-order upwind,
+ *      no Rhie-Chow face velocity, no wall model ----------------------- */
+typedef struct {
+  int icod;          /* Diffusion.iCod (difusionSchemeNew) */
+  int fso;           /* MomentumModel.fSoPressure: second-order face pressure */
+  int fvisc;         /* MomentumModel.fViscosity: explicit viscous part */
+  int fres;          /* MomentumModel.fRes */
+  int type_simple;   /* 1 SIMPLE, 2 SIMPLEC (Define.h:223-224) */
+  int time_flag, time_type;
+  double dt, dt0;
+  double under;      /* underU (alphaVel) */
+} orc_vel_opts;
+
+/* m->facer is faceVelR (velocity loads; a cell flagged there has no
+ * equation), facepresr faceRpres (read, without effect on the momentum
+ * system).  cc: cell centroids (numel*3); xm: face centres (nface*3); prop
+ * nmat x MAXPROP (DYNAMICVISCOSITY 0, DENSITY 1); vel, gradpres, dfield
+ * numel*3; gradvel numel*9 (row i = grad u_i).  dfield is updated in place
+ * cell by cell as the reference does.  a: al (al|au for unsym CSRC); ad and
+ * b: 3*neq (u, v, w blocks); rcell 3*numel.  Returns 0, -1 for input the
+ * reference cannot take, -2 for loads outside MOVEWALL, STATICWALL and
+ * constant INLET. */
+int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
+                     const double *xm, const orc_load *lvel, int nlvel,
+                     const orc_vel_opts *o, const double *prop, const double *pres,
+                     const double *gradpres, const double *vel, const double *gradvel,
+                     double *dfield, int storage, int unsym, int neq, int nad,
+                     const int *ia, const int *ja, double *a, double *ad, double *b,
+                     double *rcell, int forces, int matrix, int calrcell);
+
 #endif

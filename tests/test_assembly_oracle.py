@@ -174,3 +174,63 @@ def test_pres_oracle_rejects_what_the_reference_cannot_take():
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0))]) == -1
     # MINIMAL / ORTHOGONALC leave the split unset in the reference
     assert run(lvel=[O.Load(O.STATICWALL, ())], icod=O.MINIMAL) == -1
+
+
+# ------------------------------------------------------ momentum --
+def _cell_centres(m):
+    """Cell centroids consistent with the exported geometry (xm - xmcc)."""
+    return m.xm[m.cellface[:, 0] - 1] - m.xmcc[:, 0, :]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_vel_oracle_matches_reference_live():
+    s = S.poisson_jittered(5, seed=4)
+    m = s.mesh()
+    rng = np.random.default_rng(5)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]  # csrSimple's ELLPACK branch refuses ndf > 1
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+            O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1))]
+    for icod, fso, fvisc, fres, ts, time in itertools.product(
+            (1, 4), (0, 1), (0, 1), (0, 1), (O.SIMPLE, O.SIMPLEC), (None, O.EULER, O.BACKWARD)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop, mat=mat,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)),
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=icod, fso=bool(fso),
+                         fvisc=bool(fvisc), fres=bool(fres), type_simple=ts,
+                         time_flag=time is not None, time_type=time or 0, dt=0.05, dt0=0.04,
+                         under=0.7)
+        for name, (st, un, ia, ja, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (icod, fso, fvisc, fres, ts, time, name)
+
+
+def test_vel_oracle_rejects_what_it_does_not_restate():
+    s = S.poisson_uniform(4, seed=1)
+    m = s.mesh()
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    base = dict(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 0, 0, 0, 0, 0]),
+                facepresr=m.face_r([0] * 6), prop=prop, pres=np.zeros(m.numel),
+                gradpres=np.zeros((m.numel, 3)), vel=np.zeros((m.numel, 3)),
+                gradvel=np.zeros((m.numel, 3, 3)), dfield=np.ones((m.numel, 3)))
+    run = lambda **kw: O.vel_assemble(O.VelCase(**{**base, **kw}), O.CSRD, True,  # noqa: E731
+                                      s.ia, s.ja, s.neq)[0]
+    assert run(lvel=[O.Load(O.STATICWALL, ())]) == 0
+    assert run(lvel=[O.Load(O.OUTLET, ())]) == -2
+    assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
+    assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
+    assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
+                          O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1
