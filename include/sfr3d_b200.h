@@ -264,6 +264,8 @@ typedef struct {
   const int16_t *mat;      /* numel: material + 1 (elm.mat) */
   const int32_t *id;       /* numel: equation + 1 (sistEqD->id) */
   const int16_t *facer;    /* numel*(maxviz+1): load + 1 per face, then the cell's own entry */
+  const double *cc;        /* numel*3 cell centroids (elm.geom.cc): momentum plans only */
+  const double *xm;        /* nfaces*3 face centres (face.xm): momentum plans only */
 } sfr_dif_mesh;
 
 /* One entry of the load table (Loads, StructDefine.h:356-366). */
@@ -356,8 +358,55 @@ int sfr_gpu_pres_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
                           const double *dfield, double *b, double *rcell, int32_t forces,
                           int32_t matrix, int32_t calrcell);
 
-/* Frees a plan (either kind); safe after the system is destroyed (the
- * plan's calls are not). */
+/* ---- device assembly of the SIMPLE momentum system ------------------- */
+/* systFormSimpleVel (CellLoopInc.c:98-470) -> cellSimpleVel3D
+ * (CellSimple.c:106-727) placed by csrSimple (Csr.c:1024): the u, v, w
+ * systems share the off-diagonals and carry their own diagonals, forces and
+ * residuals; the momentum D field (V / a_P, or V / (a_P - sum a_N) for
+ * SIMPLEC) comes out for the pressure correction.  Restated for laminar flow
+ * (no eddy viscosity, structural stress or wall model), first-order upwind
+ * advection (FoUp: no deferred correction) and face velocities without
+ * Rhie-Chow (with it on, the reference's serial loop reads D fields it has
+ * already overwritten, so its result depends on the cell order); velocity
+ * loads MOVEWALL, STATICWALL and constant INLET (the others are
+ * SFR_UNSUPPORTED).  mesh->facer is faceVelR; mesh->cc and mesh->xm are
+ * required.  CSRD or CSRC. */
+typedef struct {
+  int32_t icod;        /* Diffusion.iCod: 1..4 */
+  int32_t fso;         /* MomentumModel.fSoPressure: second-order face pressure */
+  int32_t fvisc;       /* MomentumModel.fViscosity: explicit viscous part */
+  int32_t fres;        /* MomentumModel.fRes */
+  int32_t type_simple; /* 1 SIMPLE, 2 SIMPLEC */
+  int32_t time_flag, time_type, pad;
+  double dt, dt0;
+  double under;        /* under-relaxation of the velocity (alphaVel) */
+} sfr_vel_opts;
+
+int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
+                            sfr_dif_plan **out);
+
+/* One call on device arrays: pres (numel), gradpres, vel, dfield (numel*3),
+ * gradvel (numel*9, row i = grad u_i) in; dfield (the new D), ad3 and b3
+ * (3*neq: u, v, w blocks; ad3 may be NULL), rcell3 (3*numel) out; the shared
+ * off-diagonals and the u diagonal into the system.  prop: host material
+ * table nmat x 10 (viscosity column 0, density column 1). */
+int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                                const sfr_vel_opts *o, const double *prop, const double *d_pres,
+                                const double *d_gradpres, const double *d_vel,
+                                const double *d_gradvel, double *d_dfield, double *d_ad3,
+                                double *d_b3, double *d_rcell3, int32_t forces, int32_t matrix,
+                                int32_t calrcell, void *stream);
+
+/* The same with host arrays (dfield updated in place; ad3, b3, rcell3
+ * copied back when not NULL). */
+int sfr_gpu_vel_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                         const sfr_vel_opts *o, const double *prop, const double *pres,
+                         const double *gradpres, const double *vel, const double *gradvel,
+                         double *dfield, double *ad3, double *b3, double *rcell3, int32_t forces,
+                         int32_t matrix, int32_t calrcell);
+
+/* Frees a plan (any kind); safe after the system is destroyed (the plan's
+ * calls are not). */
 int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
 
 /* Copy the system's values back in the reference's layout: al (nad, or the

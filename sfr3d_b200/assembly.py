@@ -35,7 +35,14 @@ class DifMeshC(ctypes.Structure):
                 ("nmat", _I32), ("pad", _I32)] + [
         (n, _P) for n in ("nelcon", "nviz", "cellface", "owner", "volume",
                           "dcca", "xmcc", "mksi", "ksi", "area", "normal",
-                          "vskew", "caltype", "mat", "id", "facer")]
+                          "vskew", "caltype", "mat", "id", "facer", "cc", "xm")]
+
+
+class VelOptsC(ctypes.Structure):
+    _fields_ = [("icod", _I32), ("fso", _I32), ("fvisc", _I32), ("fres", _I32),
+                ("type_simple", _I32), ("time_flag", _I32), ("time_type", _I32),
+                ("pad", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
+                ("under", ctypes.c_double)]
 
 
 class LoadC(ctypes.Structure):
@@ -64,6 +71,12 @@ def _lib():
         L.sfr_gpu_pres_assemble.argtypes = [_P, _P, _I32, _P, _I32] + [_P] * 7 + [_I32] * 3
         L.sfr_gpu_pres_assemble_device.argtypes = ([_P, _P, _I32, _P, _I32] + [_P] * 7
                                                    + [_I32] * 3 + [_P])
+        L.sfr_gpu_vel_plan_create.argtypes = [_P, ctypes.POINTER(DifMeshC), _I32,
+                                              ctypes.POINTER(_P)]
+        L.sfr_gpu_vel_assemble.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)] + [_P] * 9
+                                           + [_I32] * 3)
+        L.sfr_gpu_vel_assemble_device.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)]
+                                                  + [_P] * 9 + [_I32] * 3 + [_P])
         L.sfr_gpu_dif_plan_destroy.argtypes = [_P]
         L.sfr_gpu_get_values.argtypes = [_P, _P, _P, _P]
         L._dif_typed = True
@@ -102,7 +115,7 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(_P)
 
 
-def _mesh_c(mesh, facer, caltype, mat, nmat=None):
+def _mesh_c(mesh, facer, caltype, mat, nmat=None, cc=None):
     """The sfr_dif_mesh struct of a mesh object (and the arrays it points
     to, which the caller keeps alive for the call)."""
     numel = int(mesh.numel)
@@ -118,6 +131,9 @@ def _mesh_c(mesh, facer, caltype, mat, nmat=None):
         ksi=_c(mesh.ksi, np.float64), area=_c(mesh.area, np.float64),
         normal=_c(mesh.normal, np.float64), vskew=_c(mesh.vskew, np.float64),
         caltype=cal, mat=mt, id=_c(mesh.id, np.int32), facer=_c(facer, np.int16))
+    if cc is not None:
+        keep["cc"] = _c(cc, np.float64)
+        keep["xm"] = _c(mesh.xm, np.float64)
     m = DifMeshC(numel=numel, maxviz=int(keep["nelcon"].size // numel),
                  nfaces=int(mesh.mksi.shape[0]), nmat=int(cal.size),
                  **{k: _ptr(v) for k, v in keep.items()})
@@ -270,6 +286,77 @@ class PresPlan(DifPlan):
             stream or None)
         if rc != _sv.OK:
             raise _sv.SolverError(rc, "sfr_gpu_pres_assemble_device: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
+
+
+SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
+
+
+class VelPlan(DifPlan):
+    """A mesh bound to a resident system for device-side systFormSimpleVel
+    (the SIMPLE momentum system: u, v, w share the off-diagonals), laminar,
+    first-order upwind, without Rhie-Chow.  facevelr is faceVelR; cc the
+    cell centroids (numel, 3); the mesh must carry face centres (xm)."""
+
+    def __init__(self, system: "_sv.GpuSystem", mesh, facevelr, cc, icod: int = ORTHOGONAL,
+                 mat=None, nmat: int = 1, caltype=None):
+        self.system = system
+        self.numel = int(mesh.numel)
+        self.neq = system.neq
+        self.icod = icod
+        self.nmat = nmat
+        m, keep = _mesh_c(mesh, facevelr, caltype, mat, nmat, cc=cc)
+        h = _P()
+        rc = _lib().sfr_gpu_vel_plan_create(system.h, ctypes.byref(m), icod, ctypes.byref(h))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_vel_plan_create: " + _sv.last_error())
+        self.h = h
+
+    def _vopts(self, fso, fvisc, fres, type_simple, time, under):
+        o = VelOptsC(icod=self.icod, fso=int(fso), fvisc=int(fvisc), fres=int(fres),
+                     type_simple=type_simple, under=under)
+        if time is not None:
+            o.time_flag = 1
+            o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
+        return o
+
+    def assemble(self, lvel, prop, pres, gradpres, vel, gradvel, dfield, fso=True,
+                 fvisc=False, fres=True, type_simple=SIMPLE, time=None, under=0.7,
+                 forces=True, matrix=True, calrcell=True):
+        """One call with host arrays: returns (ad3, b3, rcell3, dfield), each
+        component block after the other (u, v, w)."""
+        prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
+        arrs = [_c(a, np.float64) for a in (pres, gradpres, vel, gradvel)]
+        df = np.array(dfield, dtype=np.float64, copy=True, order="C")
+        ad3 = np.empty(3 * self.neq) if matrix else None
+        b3 = np.empty(3 * self.neq) if forces else None
+        rc3 = np.empty(3 * self.numel) if calrcell else None
+        lv = _loads_c(lvel)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under)
+        rc = _lib().sfr_gpu_vel_assemble(
+            self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), *[_ptr(a) for a in arrs],
+            _ptr(df), _ptr(ad3), _ptr(b3), _ptr(rc3), int(forces), int(matrix), int(calrcell))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_vel_assemble: " + _sv.last_error())
+        if matrix:
+            self.system.values_version += 1
+        return ad3, b3, rc3, df
+
+    def assemble_device(self, lvel, prop, d_pres: int, d_gradpres: int, d_vel: int,
+                        d_gradvel: int, d_dfield: int, d_ad3: int = 0, d_b3: int = 0,
+                        d_rcell3: int = 0, fso=True, fvisc=False, fres=True,
+                        type_simple=SIMPLE, time=None, under=0.7, forces=True, matrix=True,
+                        calrcell=True, stream: int = 0):
+        prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
+        lv = _loads_c(lvel)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under)
+        rc = _lib().sfr_gpu_vel_assemble_device(
+            self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), d_pres, d_gradpres, d_vel,
+            d_gradvel, d_dfield, d_ad3 or None, d_b3 or None, d_rcell3 or None, int(forces),
+            int(matrix), int(calrcell), stream or None)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_vel_assemble_device: " + _sv.last_error())
         if matrix:
             self.system.values_version += 1
 

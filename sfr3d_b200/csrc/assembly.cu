@@ -36,7 +36,8 @@ namespace sfr {
 namespace {
 
 constexpr int kMaxViz = 8;        // face slots per cell handled
-constexpr int kGeo = 9;           // geometry fields per (face, row)
+constexpr int kGeo = 9;           // geometry fields per (face, row): diffusion, pressure
+constexpr int kGeoVel = 19;       // momentum
 constexpr int kMaxLoads = 32;     // entries of the load table
 constexpr int32_t kFlagP = 0x40000000;  // neighbour whose equation id is -1
 
@@ -76,6 +77,7 @@ struct MeshDev {
   const int16_t *nviz, *caltype, *mat, *facer;
   const int16_t *facevelr;  // pressure plans: the velocity loads of each face
   const double *volume, *dcca, *xmcc, *mksi, *ksi, *area, *normal, *vskew;
+  const double *cc, *xm;    // momentum plans: cell centroids, face centres
 };
 
 struct PatternDev {
@@ -201,7 +203,9 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
     const int64_t face = static_cast<int64_t>(m.cellface[q]) - 1;
     if (face < 0 || face >= m.nfaces) return flag_error(err, kErrFace);
     const double ch = (m.owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
-    double ksi[3], nrm[3], g[kGeo];
+    double ksi[3], nrm[3], g[kGeoVel];
+    const int nfield = kind == 2 ? kGeoVel : kGeo;
+    for (int k = kGeo; k < kGeoVel; ++k) g[k] = 0.0;
     for (int j = 0; j < 3; ++j) {
       ksi[j] = xmul(ch, m.ksi[3 * face + j]);
       nrm[j] = xmul(ch, m.normal[3 * face + j]);
@@ -217,7 +221,7 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
       for (int j = 0; j < 3; ++j) v[j] = xadd(m.vskew[3 * face + j], m.xmcc[3 * q + j]);
       g[0] = xdiv(xsqrt(dot3(v, v)), mk);  // alpha
       g[2] = mk;
-      if (kind == 0) {
+      if (kind != 1) {
         double s[3], e[3], t[3];
         for (int j = 0; j < 3; ++j) s[j] = xmul(area, nrm[j]);
         dif_scheme(icod, s, ksi, e, t);
@@ -225,6 +229,14 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
         for (int j = 0; j < 3; ++j) {
           g[3 + j] = ksi[j];
           g[6 + j] = t[j];
+        }
+        if (kind == 2) {  // [9..11] normal, 12 area, [13..15] xmcc, [16..18] xm - c_V
+          for (int j = 0; j < 3; ++j) {
+            g[9 + j] = nrm[j];
+            g[13 + j] = m.xmcc[3 * q + j];
+            g[16 + j] = xsub(m.xm[3 * face + j], m.cc[3 * static_cast<size_t>(viz) + j]);
+          }
+          g[12] = area;
         }
       } else {
         g[1] = area;
@@ -256,6 +268,14 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
           g[3 + j] = nrm[j];
           g[6 + j] = 0.0;
         }
+      } else if (kind == 2) {  // faceVelR's load; [9..11] normal, 12 area
+        nbv = ld > 0 ? -(ld - 1) - 2 : -1;
+        for (int j = 0; j < 3; ++j) {
+          g[3 + j] = ksi[j];
+          g[6 + j] = 0.0;
+          g[9 + j] = nrm[j];
+        }
+        g[12] = m.area[face];
       } else {
         const int lv = m.facevelr[static_cast<size_t>(nel) * (mv + 1) + f];
         if (lv < 0 || lv > kMaxLoads) return flag_error(err, kErrLoad);
@@ -276,7 +296,7 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
     p.nb[o] = nbv;
     p.dst[o] = dst;
     p.sslot[o] = slot;
-    for (int k = 0; k < kGeo; ++k) p.geo[k * p.fstride + o] = g[k];
+    for (int k = 0; k < nfield; ++k) p.geo[k * p.fstride + o] = g[k];
   }
   if (sym_lower || written != real_slots(P, row)) atomicAdd(partial_rows, 1);
 }
@@ -651,6 +671,226 @@ __global__ void __launch_bounds__(256, 2)
   write_row<kMV, kFused>(fu, r, nf, la, d, dsts, slots, stage, diag);
 }
 
+struct VelOpts {
+  int fso, fvisc, fres, simplec, time_flag, time_type, forces, matrix, calrcell;
+  double dt, dt0, under;
+};
+
+// moveWall, not Dirichlet (CellLib.c:7715-7770)
+__device__ __forceinline__ void move_wall(const double vC[3], const double vB[3],
+                                          const double n[3], double sPc[3], double p[3],
+                                          double dcca, double visc, double area) {
+  const double aP = xdiv(xmul(visc, area), dcca);
+  double w[3];
+  for (int k = 0; k < 3; ++k) {
+    w[k] = xsub(1.0, xmul(n[k], n[k]));
+    sPc[k] = xadd(sPc[k], xmul(aP, w[k]));
+  }
+  // p_k += aP (vB_k (1 - n_k n_k) + (vC_a - vB_a) n_a n_k + (vC_b - vB_b) n_b n_k),
+  // a < b the two other components in increasing order
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int a = k == 0 ? 1 : 0, b = k == 2 ? 1 : 2;
+    const double t1 = xmul(vB[k], w[k]);
+    const double t2 = xmul(xmul(xsub(vC[a], vB[a]), n[a]), n[k]);
+    const double t3 = xmul(xmul(xsub(vC[b], vB[b]), n[b]), n[k]);
+    p[k] = xadd(p[k], xmul(aP, xadd(xadd(t1, t2), t3)));
+  }
+}
+
+// One row of cellSimpleVel3D (CellSimple.c:106-727), laminar, first-order
+// upwind, face velocity without Rhie-Chow; three diagonals and forces.
+// mtab: density then viscosity of each material.
+template <int kMV>
+__global__ void __launch_bounds__(256)
+    vel_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, VelOpts o,
+                        const int16_t *__restrict__ mat, const double *__restrict__ mtab, int nmat,
+                        const double *__restrict__ pres, const double *__restrict__ gradp,
+                        const double *__restrict__ vel, const double *__restrict__ gradvel,
+                        double *__restrict__ dfield, double *__restrict__ stage,
+                        double *__restrict__ diag, double *__restrict__ ad3,
+                        double *__restrict__ b3, double *__restrict__ rcell3, int numel) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n) return;
+  const int cell = __ldcs(p.cell + r);
+  if (cell < 0) return;
+  const int nf = __ldcs(p.nface + r);
+  const size_t fs = p.fstride;
+  const int mc = mat[cell] - 1;
+  const double rhoC = mtab[mc], muC = mtab[nmat + mc];
+  const double effC = xadd(muC, 0.0);  // laminar: no eddy viscosity
+  const size_t c3 = 3 * static_cast<size_t>(cell), c9 = 9 * static_cast<size_t>(cell);
+  const double presC = pres[cell];
+  double velC[3], gpC[3], gvC[9];
+  for (int k = 0; k < 3; ++k) {
+    velC[k] = vel[c3 + k];
+    gpC[k] = gradp[c3 + k];
+  }
+  for (int k = 0; k < 9; ++k) gvC[k] = gradvel[c9 + k];
+  double pp[3] = {0.0, 0.0, 0.0}, pf[3] = {0.0, 0.0, 0.0}, sPc[3] = {0.0, 0.0, 0.0};
+  double sP = 0.0, la[kMV];
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    la[f] = 0.0;
+    if (f >= nf) continue;
+    const size_t q = static_cast<size_t>(f) * p.n + r;
+    const int32_t nb = __ldcs(p.nb + q);
+    const double *g = p.geo + q;
+    double n[3];
+    for (int j = 0; j < 3; ++j) n[j] = __ldcs(g + (9 + j) * fs);
+    const double area = __ldcs(g + 12 * fs);
+    if (nb >= 0) {
+      const int c = nb & (kFlagP - 1);
+      const size_t v3 = 3 * static_cast<size_t>(c), v9 = 9 * static_cast<size_t>(c);
+      const int mv = mat[c] - 1;
+      const double rhoV = mtab[mv], effV = xadd(mtab[nmat + mv], 0.0);
+      const double alpha = __ldcs(g), modE = __ldcs(g + fs), mk = __ldcs(g + 2 * fs);
+      const double am1 = xsub(1.0, alpha);
+      double ksi[3], t[3], velV[3], wf[3];
+      for (int j = 0; j < 3; ++j) {
+        ksi[j] = __ldcs(g + (3 + j) * fs);
+        t[j] = __ldcs(g + (6 + j) * fs);
+        velV[j] = vel[v3 + j];
+        wf[j] = xadd(xmul(am1, velC[j]), xmul(alpha, velV[j]));
+      }
+      // mediaHarmonica (CellLib.c:7879)
+      const double visc = (effC == 0.0 || effV == 0.0)
+                              ? 0.0
+                              : xdiv(1.0, xadd(xdiv(alpha, effC), xdiv(am1, effV)));
+      const double dfd = xdiv(xmul(visc, modE), mk);
+      const double density = xadd(xmul(am1, rhoC), xmul(alpha, rhoV));
+      const double wfn = dot3(wf, n);
+      const double cv = xmul(xmul(density, wfn), area);
+      la[f] = xsub(dfd, cv < 0.0 ? cv : 0.0);
+      sP = xadd(sP, cv);
+      const double cvz = xmul(cv, 0.0);  // FoUp: no deferred correction, cvc = 0
+      double gvc[9];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        double gf[3];
+        for (int j = 0; j < 3; ++j)
+          gf[j] = xadd(xmul(am1, gvC[3 * i + j]), xmul(alpha, gradvel[v9 + 3 * i + j]));
+        const double du = xsub(xdiv(xsub(velV[i], velC[i]), mk), dot3(gf, ksi));
+        for (int j = 0; j < 3; ++j) gvc[3 * i + j] = xadd(gf[j], xmul(du, ksi[j]));
+        const double dfdc = xmul(visc, dot3(gvc + 3 * i, t));
+        pp[i] = xadd(pp[i], xsub(dfdc, cvz));  // p += dfdc - cv cvc
+      }
+      // facePressure (CellLib.c:7499), interior
+      double pFace;
+      if (o.fso) {
+        double xmcc[3], vv[3], gpV[3];
+        for (int j = 0; j < 3; ++j) {
+          xmcc[j] = __ldcs(g + (13 + j) * fs);
+          vv[j] = __ldcs(g + (16 + j) * fs);
+          gpV[j] = gradp[v3 + j];
+        }
+        double p1 = xadd(presC, xmul(gpC[0], xmcc[0]));
+        p1 = xadd(p1, xmul(gpC[1], xmcc[1]));
+        p1 = xadd(p1, xmul(gpC[2], xmcc[2]));
+        double p2 = xadd(pres[c], xmul(gpV[0], vv[0]));
+        p2 = xadd(p2, xmul(gpV[1], vv[1]));
+        p2 = xadd(p2, xmul(gpV[2], vv[2]));
+        pFace = xmul(0.5, xadd(p1, p2));
+      } else {
+        pFace = xadd(xmul(am1, presC), xmul(alpha, pres[c]));
+      }
+      const double tmp = xmul(pFace, area);
+      for (int j = 0; j < 3; ++j) pf[j] = xadd(pf[j], xmul(tmp, n[j]));
+      // viscosityPartExp (CellLib.c:7439), fDiv false
+      if (o.fvisc) {
+        const double aP = xmul(muC, area);
+        for (int i = 0; i < 3; ++i) {
+          const double col[3] = {gvc[i], gvc[3 + i], gvc[6 + i]};
+          pp[i] = xadd(pp[i], xmul(aP, dot3(col, n)));
+        }
+      }
+    } else {
+      const double dcca = __ldcs(g + fs);
+      const double tmp = xmul(presC, area);
+      for (int j = 0; j < 3; ++j) pf[j] = xadd(pf[j], xmul(tmp, n[j]));
+      if (nb <= -2) {
+        const DevLoad &L = loads[-nb - 2];
+        if (L.type == 8 || L.type == 14) {  // MOVEWALL, STATICWALL
+          const double vB[3] = {L.type == 8 ? L.par[0] : 0.0, L.type == 8 ? L.par[1] : 0.0,
+                                L.type == 8 ? L.par[2] : 0.0};
+          move_wall(velC, vB, n, sPc, pp, dcca, effC, area);
+        } else if (L.type == 6) {  // INLET
+          const double tA[3] = {L.par[0], L.par[1], L.par[2]};
+          double wfn = xadd(xmul(tA[0], n[0]), xmul(tA[1], n[1]));
+          wfn = xadd(wfn, xmul(tA[2], n[2]));
+          const double mflux = xmul(xmul(L.par_last, wfn), area);
+          // stress (CellLib.c:7013), lambda = 0
+          const double tr = xadd(xadd(gvC[0], gvC[4]), gvC[8]);
+          const double nu2 = xmul(2.0, muC), z = xmul(0.0, tr);
+          const double ss[6] = {xadd(xmul(nu2, gvC[0]), z), xadd(xmul(nu2, gvC[4]), z),
+                                xadd(xmul(nu2, gvC[8]), z), xmul(muC, xadd(gvC[3], gvC[1])),
+                                xmul(muC, xadd(gvC[7], gvC[5])), xmul(muC, xadd(gvC[6], gvC[2]))};
+          const double sa[3] = {xmul(area, n[0]), xmul(area, n[1]), xmul(area, n[2])};
+          const double r0[3] = {ss[0], ss[3], ss[5]}, r1[3] = {ss[3], ss[1], ss[4]},
+                       r2[3] = {ss[5], ss[4], ss[2]};
+          pp[0] = xadd(pp[0], dot3(r0, sa));
+          pp[1] = xadd(pp[1], dot3(r1, sa));
+          pp[2] = xadd(pp[2], dot3(r2, sa));
+          for (int k = 0; k < 3; ++k) pp[k] = xsub(pp[k], xmul(mflux, tA[k]));
+        }
+      }
+    }
+  }
+  // implicit time term, CellSimple.c:606-617
+  if (o.time_flag) {
+    const double vol = p.vol[r];
+    if (o.time_type == 0) {
+      sP = xadd(sP, xdiv(xmul(rhoC, vol), o.dt));
+    } else if (o.time_type == 1) {
+      const double tmp = xadd(xdiv(1.0, o.dt), xdiv(1.0, xadd(o.dt, o.dt0)));
+      sP = xadd(sP, xmul(xmul(tmp, rhoC), vol));
+    }
+  }
+  double lAn = 0.0;
+#pragma unroll
+  for (int f = 0; f < kMV; ++f)
+    if (f < nf) lAn = xadd(lAn, la[f]);
+  double dk[3], rc[3];
+  const double relax = xsub(1.0, o.under);
+  for (int k = 0; k < 3; ++k) {
+    dk[k] = xdiv(xadd(xadd(sP, sPc[k]), lAn), o.under);
+    pp[k] = xadd(pp[k], xmul(xmul(relax, dk[k]), velC[k]));
+    pp[k] = xsub(pp[k], pf[k]);
+    rc[k] = 0.0;
+  }
+#pragma unroll
+  for (int f = 0; f < kMV; ++f) {
+    if (f >= nf) continue;
+    const int32_t nb = __ldcs(p.nb + static_cast<size_t>(f) * p.n + r);
+    if (nb < 0) continue;
+    const size_t v3 = 3 * static_cast<size_t>(nb & (kFlagP - 1));
+    for (int k = 0; k < 3; ++k) {
+      const double t = xmul(la[f], vel[v3 + k]);
+      if (nb & kFlagP)
+        pp[k] = xadd(pp[k], t);
+      else
+        rc[k] = xadd(rc[k], t);
+    }
+  }
+  const double vol = p.vol[r];
+  for (int k = 0; k < 3; ++k) {
+    rc[k] = xadd(rc[k], xsub(pp[k], xmul(dk[k], velC[k])));
+    dfield[c3 + k] = o.simplec ? xdiv(vol, xsub(dk[k], lAn)) : xdiv(vol, dk[k]);
+    if (o.forces) b3[static_cast<size_t>(k) * p.n + r] = o.fres ? rc[k] : pp[k];
+    if (o.calrcell) rcell3[static_cast<size_t>(k) * numel + cell] = rc[k];
+  }
+  if (!o.matrix) return;
+  diag[r] = dk[0];
+  if (ad3)
+    for (int k = 0; k < 3; ++k) ad3[static_cast<size_t>(k) * p.n + r] = dk[k];
+#pragma unroll
+  for (int f = 0; f < kMV; ++f)
+    if (f < nf) {
+      const int32_t t = __ldcs(p.dst + static_cast<size_t>(f) * p.n + r);
+      if (t >= 0) stage[t] = xmul(la[f], -1.0);
+    }
+}
+
 __global__ void update_cells_kernel(const int32_t *id, int numel, int n, const double *x,
                                     double *u, int add) {
   const int nel = blockIdx.x * blockDim.x + threadIdx.x;
@@ -674,7 +914,8 @@ cudaError_t upload(T **dst, const T *src, size_t count) {
 struct sfr_dif_plan {
   sfr_system *s = nullptr;       // the system written; must outlive the plan's calls
   int32_t device = 0;            // destroy needs no live system
-  int32_t kind = 0;              // 0 diffusion (systFormDif), 1 pressure (systFormSimplePres)
+  int32_t kind = 0;              // 0 diffusion (systFormDif), 1 pressure (systFormSimplePres),
+                                 // 2 momentum (systFormSimpleVel)
   int32_t numel = 0, maxviz = 0, icod = 0, nmat = 0;
   int free_cells = 0;            // cells without an equation (their rcell is zeroed)
   unsigned used_loads = 0;       // bit l: some boundary face names load l (pressure loads)
@@ -716,8 +957,9 @@ int unsupported(const char *why) {
 
 constexpr size_t kTableLoads = 2 * sfr::kMaxLoads;
 
+// the load tables, then density and viscosity of each material
 size_t table_bytes(const sfr_dif_plan *p) {
-  return sizeof(sfr::DevLoad) * kTableLoads + sizeof(double) * std::max(p->nmat, 1);
+  return sizeof(sfr::DevLoad) * kTableLoads + 2 * sizeof(double) * std::max(p->nmat, 1);
 }
 
 void free_plan_buffers(sfr_dif_plan *p) {
@@ -807,12 +1049,46 @@ int stage_pres_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
   return stage_table(p, h, st);
 }
 
+// Momentum: pLoadSimple with fCalVel (Loads.c:265-720) for the loads this
+// kernel restates (MOVEWALL, STATICWALL, constant INLET); prop: nmat x
+// MAXPROP (DYNAMICVISCOSITY 0, DENSITY 1).
+int stage_vel_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel, const double *prop,
+                     cudaStream_t st) {
+  if (nlvel < 0 || nlvel > sfr::kMaxLoads || (nlvel > 0 && !lvel))
+    return bad("nlvel must be 0..32");
+  if (!prop) return bad("prop is NULL");
+  for (int l = 0; l < sfr::kMaxLoads; ++l) {
+    if (!(p->used_loads & (1u << l))) continue;
+    if (l >= nlvel) return bad("a boundary face names a velocity load beyond nlvel");
+    const sfr_load &L = lvel[l];
+    if (L.type == 7 || L.type == 9 || L.type == 10 || L.type == 13)
+      return unsupported("OUTLET, INLETSTAICTPRES, OPEN and INLETTOTALPRES velocity loads are "
+                         "not assembled on the device");
+    if (L.type == 6 && L.var != 0)
+      return unsupported("loads given as functions (nTypeVar 1) are not assembled on the device");
+    if (L.type == 6 && (L.np < 3 || L.np > 20)) return bad("an INLET load needs 3..20 parameters");
+  }
+  std::vector<unsigned char> h(table_bytes(p), 0);
+  auto *t = reinterpret_cast<sfr::DevLoad *>(h.data());
+  for (int l = 0; l < nlvel; ++l) fill_load(t + l, lvel[l]);
+  auto *mt = reinterpret_cast<double *>(h.data() + sizeof(sfr::DevLoad) * kTableLoads);
+  for (int k = 0; k < p->nmat; ++k) {
+    mt[k] = prop[k * 10 + 1];            // DENSITY
+    mt[p->nmat + k] = prop[k * 10 + 0];  // DYNAMICVISCOSITY
+  }
+  return stage_table(p, h, st);
+}
+
 int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr, int32_t icod,
                 int32_t kind, sfr_dif_plan **out) {
   if (!s || !mesh || !out) return bad("NULL argument");
   *out = nullptr;
   const sfr_dif_mesh &m = *mesh;
   if (kind == 0 && (icod < 1 || icod > 4)) return bad("icod must be 1..4 (Define.h:304-307)");
+  if (kind == 2 && (icod < 1 || icod > 4)) return bad("icod must be 1..4 (Define.h:304-307)");
+  if (kind == 2 && (!m.cc || !m.xm)) return bad("the momentum plan needs cc and xm");
+  if (kind == 2 && s->storage == SFR_ELLPACK)
+    return bad("csrSimple refuses ELLPACK for ndf > 1 (EllPack.c:143-147)");
   if (kind == 1 && icod != 1 && icod != 4)
     return bad("the pressure split (difusionSchemeAnisotropic) sets e and t only for "
                "ORTHOGONAL (1) and OVERRELAXED (4)");
@@ -827,7 +1103,7 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
   if (static_cast<int64_t>(s->n) * m.maxviz > INT32_MAX) return bad("system too large");
   for (int64_t f = 0; f < m.nfaces; ++f)
     if (m.owner[2 * f] < 1 || m.owner[2 * f] > m.numel) return bad("a face owner is out of range");
-  if (kind == 1)
+  if (kind != 0)
     for (int32_t c = 0; c < m.numel; ++c)  // the density lookup of every cell
       if (m.mat[c] < 1 || m.mat[c] > m.nmat) return bad("a cell's material is out of range");
   SFR_CUA(cudaSetDevice(s->device));
@@ -867,6 +1143,8 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
     cudaFree(const_cast<double *>(md.area));
     cudaFree(const_cast<double *>(md.normal));
     cudaFree(const_cast<double *>(md.vskew));
+    cudaFree(const_cast<double *>(md.cc));
+    cudaFree(const_cast<double *>(md.xm));
     cudaFree(d_err);
   };
   auto up = [&](cudaError_t e) {
@@ -901,6 +1179,10 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
     up(sfr::upload(&t64, m.area, nf)); md.area = t64;
     up(sfr::upload(&t64, m.normal, 3 * nf)); md.normal = t64;
     up(sfr::upload(&t64, m.vskew, 3 * nf)); md.vskew = t64;
+    if (kind == 2) {
+      up(sfr::upload(&t64, m.cc, 3 * ne)); md.cc = t64;
+      up(sfr::upload(&t64, m.xm, 3 * nf)); md.xm = t64;
+    }
   }
   sfr::PlanDev &d = p->d;
   d.n = n;
@@ -911,7 +1193,8 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
   up(cudaMalloc(&d.nb, sizeof(int32_t) * slots));
   up(cudaMalloc(&d.dst, sizeof(int32_t) * slots));
   up(cudaMalloc(&d.sslot, sizeof(int32_t) * slots));
-  up(cudaMalloc(&d.geo, sizeof(double) * slots * sfr::kGeo));
+  const int nfield = kind == 2 ? sfr::kGeoVel : sfr::kGeo;
+  up(cudaMalloc(&d.geo, sizeof(double) * slots * nfield));
   up(cudaMalloc(&d.vol, sizeof(double) * n));
   up(cudaMalloc(&p->d_table, table_bytes(p)));
   up(cudaMalloc(&d_err, sizeof(int) * 5));
@@ -921,7 +1204,7 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
     up(cudaMemset(d.nb, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.dst, 0xFF, sizeof(int32_t) * slots));
     up(cudaMemset(d.sslot, 0xFF, sizeof(int32_t) * slots));
-    up(cudaMemset(d.geo, 0, sizeof(double) * slots * sfr::kGeo));
+    up(cudaMemset(d.geo, 0, sizeof(double) * slots * nfield));
     up(cudaMemset(p->d_table, 0, table_bytes(p)));
     up(cudaMemset(d_err, 0, sizeof(int) * 5));
   }
@@ -939,8 +1222,9 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
     p->used_loads = static_cast<unsigned>(h[1]);
     p->free_cells = h[2];
     p->used_vel_loads = static_cast<unsigned>(h[4]);
-    // every stored value of every row written by the row's own cell
-    p->fused = h[3] == 0 && s->A.val32 != nullptr;
+    // every stored value of every row written by the row's own cell (the
+    // momentum kernel leaves the refresh to the usual gather)
+    p->fused = kind != 2 && h[3] == 0 && s->A.val32 != nullptr;
   }
   if (rc == SFR_OK && p->fused) {
     if (!s->d_comp) {
@@ -1171,6 +1455,103 @@ int sfr_gpu_pres_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
                                     d_df, p->h_b, p->h_rcell, forces, matrix, calrcell, st);
   if (rc != SFR_OK) return rc;
   return copy_back(p, b, rcell, forces, calrcell, st);
+}
+
+int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
+                            sfr_dif_plan **out) {
+  return create_plan(s, mesh, nullptr, icod, 2, out);
+}
+
+int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                                const sfr_vel_opts *o, const double *prop, const double *d_pres,
+                                const double *d_gradpres, const double *d_vel,
+                                const double *d_gradvel, double *d_dfield, double *d_ad3,
+                                double *d_b3, double *d_rcell3, int32_t forces, int32_t matrix,
+                                int32_t calrcell, void *stream) {
+  if (!p || !o) return bad("NULL argument");
+  if (p->kind != 2) return bad("not a momentum plan");
+  if (o->icod != p->icod) return bad("opts.icod differs from the scheme the plan was built for");
+  if (o->type_simple != 1 && o->type_simple != 2)
+    return bad("type_simple must be SIMPLE (1) or SIMPLEC (2)");
+  if (!d_pres || !d_gradpres || !d_vel || !d_gradvel || !d_dfield)
+    return bad("pres, gradpres, vel, gradvel and dfield are required");
+  if (forces && !d_b3) return bad("forces set without b");
+  if (calrcell && !d_rcell3) return bad("calrcell set without rcell");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  int rc = stage_vel_tables(p, lvel, nlvel, prop, st);
+  if (rc != SFR_OK) return rc;
+  if (calrcell && p->free_cells > 0)
+    SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
+  sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
+                  o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
+                  o->dt, o->dt0, o->under};
+  const int blocks = (s->n + 255) / 256;
+  const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
+  const auto *mtab =
+      reinterpret_cast<const double *>(p->d_table + sizeof(sfr::DevLoad) * kTableLoads);
+  auto launch = [&](auto kernel) {
+    kernel<<<blocks, 256, 0, st>>>(p->d, loads_d, vo, p->d_mat, mtab, p->nmat, d_pres,
+                                   d_gradpres, d_vel, d_gradvel, d_dfield, s->d_stage,
+                                   s->d_diag, d_ad3, d_b3, d_rcell3, p->numel);
+  };
+  if (p->d.maxviz == 6)
+    launch(sfr::vel_assemble_kernel<6>);
+  else
+    launch(sfr::vel_assemble_kernel<sfr::kMaxViz>);
+  SFR_CUA(cudaGetLastError());
+  if (matrix) return sfr::values_refreshed(s, st, false);
+  return SFR_OK;
+}
+
+int sfr_gpu_vel_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
+                         const sfr_vel_opts *o, const double *prop, const double *pres,
+                         const double *gradpres, const double *vel, const double *gradvel,
+                         double *dfield, double *ad3, double *b3, double *rcell3, int32_t forces,
+                         int32_t matrix, int32_t calrcell) {
+  if (!p || !o) return bad("NULL argument");
+  if (!pres || !gradpres || !vel || !gradvel || !dfield)
+    return bad("pres, gradpres, vel, gradvel and dfield are required");
+  sfr_system *s = p->s;
+  SFR_CUA(cudaSetDevice(s->device));
+  const size_t ne = p->numel, n = s->n;
+  // pres | gradpres | vel | gradvel | dfield | rcell3, and ad3 | b3
+  double *f = nullptr, *e = nullptr;
+  SFR_CUA(cudaMalloc(&f, sizeof(double) * ne * 22));
+  if (cudaMalloc(&e, sizeof(double) * n * 6) != cudaSuccess) {
+    cudaFree(f);
+    return bad("device memory for the host-array call");
+  }
+  cudaStream_t st = s->stream;
+  double *d_pres = f, *d_gp = f + ne, *d_vel = f + 4 * ne, *d_gv = f + 7 * ne,
+         *d_df = f + 16 * ne, *d_rc = f + 19 * ne, *d_ad3 = e, *d_b3 = e + 3 * n;
+  int rc = SFR_OK;
+  auto cp = [&](void *dst, const void *src, size_t bytes, cudaMemcpyKind k) {
+    if (rc == SFR_OK && cudaMemcpyAsync(dst, src, bytes, k, st) != cudaSuccess) {
+      sfr::set_last_error("a copy of the host-array call failed");
+      rc = SFR_CUDA_ERROR;
+    }
+  };
+  cp(d_pres, pres, sizeof(double) * ne, cudaMemcpyHostToDevice);
+  cp(d_gp, gradpres, sizeof(double) * ne * 3, cudaMemcpyHostToDevice);
+  cp(d_vel, vel, sizeof(double) * ne * 3, cudaMemcpyHostToDevice);
+  cp(d_gv, gradvel, sizeof(double) * ne * 9, cudaMemcpyHostToDevice);
+  cp(d_df, dfield, sizeof(double) * ne * 3, cudaMemcpyHostToDevice);
+  if (rc == SFR_OK)
+    rc = sfr_gpu_vel_assemble_device(p, lvel, nlvel, o, prop, d_pres, d_gp, d_vel, d_gv, d_df,
+                                     d_ad3, d_b3, d_rc, forces, matrix, calrcell, st);
+  if (rc == SFR_OK) {
+    cp(dfield, d_df, sizeof(double) * ne * 3, cudaMemcpyDeviceToHost);
+    if (matrix && ad3) cp(ad3, d_ad3, sizeof(double) * n * 3, cudaMemcpyDeviceToHost);
+    if (forces && b3) cp(b3, d_b3, sizeof(double) * n * 3, cudaMemcpyDeviceToHost);
+    if (calrcell && rcell3) cp(rcell3, d_rc, sizeof(double) * ne * 3, cudaMemcpyDeviceToHost);
+    if (rc == SFR_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = SFR_CUDA_ERROR;
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(f);
+  cudaFree(e);
+  return rc;
 }
 
 int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, int32_t add,

@@ -445,3 +445,125 @@ def test_device_system_dumped_as_the_reference_writes_it(cuda, box, tmp_path):
         assert (tmp_path / "bd.mtx").read_bytes() == (tmp_path / "br.mtx").read_bytes()
         plan.close()
         gs.close()
+
+
+# ------------------------------------------------------------ momentum --
+VLOADS = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+          O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1))]
+
+
+def _centres(m):
+    return m.xm[m.cellface[:, 0] - 1] - m.xmcc[:, 0, :]
+
+
+@pytest.mark.parametrize("icod", [1, 4])
+def test_vel_matches_oracle(cuda, box, icod):
+    s, m, lay = box
+    rng = np.random.default_rng(40 + icod)
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    cc = _centres(m)
+    fv = m.face_r([1, 1, 2, 1, 3, 1])
+    for name in ("csrd_full", "csrd_sym", "csrc_sym", "csrc_unsym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.VelPlan(gs, m, fv, cc, icod=icod, mat=mat, nmat=2)
+        for fso, fvisc, fres, ts, time in itertools.product(
+                (0, 1), (0, 1), (0, 1), (A.SIMPLE, A.SIMPLEC), (None, (O.EULER, 0.05, 0.04))):
+            case = O.VelCase(mesh=m, cc=cc, facevelr=fv, facepresr=m.face_r([0] * 6),
+                             lvel=VLOADS, prop=prop, mat=mat, pres=rng.standard_normal(m.numel),
+                             gradpres=rng.standard_normal((m.numel, 3)),
+                             vel=rng.standard_normal((m.numel, 3)),
+                             gradvel=rng.standard_normal((m.numel, 3, 3)),
+                             dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=icod,
+                             fso=bool(fso), fvisc=bool(fvisc), fres=bool(fres), type_simple=ts,
+                             time_flag=time is not None, time_type=time[0] if time else 0,
+                             dt=time[1] if time else 1.0, dt0=time[2] if time else 1.0,
+                             under=0.7)
+            want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
+            assert want[0] == 0
+            n = gs._nsrc()
+            split = st == sv.CSRC and un
+            gs.set_values(np.zeros(n // 2 if split else n), np.zeros(s.neq),
+                          np.zeros(n // 2) if split else None)
+            ad3, b3, rc3, df = plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres,
+                                             case.vel, case.gradvel, case.dfield, fso=fso,
+                                             fvisc=fvisc, fres=fres, type_simple=ts, time=time,
+                                             under=0.7)
+            al, ad, au = A.get_values(gs)
+            a = al if au is None else np.concatenate([al, au])
+            what = (name, fso, fvisc, fres, ts, time)
+            assert bits_equal(a, want[1]), what
+            assert bits_equal(ad3, want[2]) and bits_equal(ad, want[2][:s.neq]), what
+            assert bits_equal(b3, want[3]), what
+            assert bits_equal(rc3, want[4]), what
+            assert bits_equal(df, want[5]), what
+        plan.close()
+        gs.close()
+
+
+def test_vel_assembled_momentum_solves_like_reference(cuda):
+    """A lid-driven cavity's momentum system assembled and solved (u, v, w
+    with their own diagonals) on the device."""
+    torch = cuda
+    s = S.poisson_jittered(24, seed=9)
+    m = s.mesh()
+    rng = np.random.default_rng(41)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-2, 1.0)
+    fv = m.face_r([1, 1, 1, 1, 1, 2])   # static walls, the z-max lid moving
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0))]
+    case = O.VelCase(mesh=m, cc=_centres(m), facevelr=fv, facepresr=m.face_r([0] * 6), lvel=lvel,
+                     prop=prop, pres=rng.standard_normal(m.numel) * 1e-2,
+                     gradpres=rng.standard_normal((m.numel, 3)) * 1e-2,
+                     vel=rng.standard_normal((m.numel, 3)) * 0.1,
+                     gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.1,
+                     dfield=np.ones((m.numel, 3)), time_flag=True, dt=0.01, fres=False)
+    rc, a, ad3, b3, _, _ = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    refs = [O.pbicgstab(O.CSRD, True, s.ia, s.ja, a, ad3[k * s.neq:(k + 1) * s.neq],
+                        b3[k * s.neq:(k + 1) * s.neq], tol=1e-10) for k in range(3)]
+    gs = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    plan = A.VelPlan(gs, m, fv, case.cc)
+    dev = lambda v: torch.tensor(np.ascontiguousarray(v), device="cuda")  # noqa: E731
+    d = [dev(x) for x in (case.pres, case.gradpres, case.vel, case.gradvel, case.dfield)]
+    d_ad3 = torch.empty(3 * s.neq, dtype=torch.float64, device="cuda")
+    d_b3 = torch.empty(3 * s.neq, dtype=torch.float64, device="cuda")
+    plan.assemble_device(_aloads(lvel), prop, *[t.data_ptr() for t in d], d_ad3=d_ad3.data_ptr(),
+                         d_b3=d_b3.data_ptr(), fres=False, time=(O.EULER, 0.01, 0.01),
+                         calrcell=False)
+    torch.cuda.synchronize()
+    assert bits_equal(d_ad3.cpu().numpy(), ad3) and bits_equal(d_b3.cpu().numpy(), b3)
+    xs, infos = gs.solve_multi(sv.PBICGSTAB, d_b3.cpu().numpy().reshape(3, -1), tol=1e-10,
+                               ad_k=d_ad3.cpu().numpy().reshape(3, -1))
+    for k in range(3):
+        assert infos[k].status == sv.OK
+        assert abs(infos[k].iters - refs[k].iters) <= 1
+        assert rel(xs[k], refs[k].x) < 1e-12
+    plan.close()
+    gs.close()
+
+
+def test_vel_validation(cuda, box):
+    s, m, lay = box
+    st, un, ia, ja, _al, _au = lay["ellpack"]
+    cc = _centres(m)
+    ge = sv.GpuSystem(s.neq, ia, ja, st, un)
+    with pytest.raises(sv.SolverError) as e:
+        A.VelPlan(ge, m, m.face_r([1] * 6), cc)
+    assert e.value.status == sv.BAD_INPUT
+    st, un, ia, ja, _al, _au = lay["csrd_full"]
+    gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+    plan = A.VelPlan(gs, m, m.face_r([1] * 6), cc)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    z1, z3, z9 = np.zeros(m.numel), np.zeros((m.numel, 3)), np.zeros((m.numel, 9))
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.OUTLET, ())], prop, z1, z3, z3, z9, z3)
+    assert e.value.status == sv.UNSUPPORTED
+    with pytest.raises(sv.SolverError) as e:
+        plan.assemble([A.Load(A.STATICWALL, ())], prop, z1, z3, z3, z9, z3, type_simple=3)
+    assert e.value.status == sv.BAD_INPUT
+    plan.assemble([A.Load(A.STATICWALL, ())], prop, z1, z3, z3, z9, z3)
+    plan.close()
