@@ -56,7 +56,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the momentum, batched and adjoint legs")
     ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab", "assembly",
-                                          "pressure"], default="none",
+                                          "pressure", "momentum"], default="none",
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
                     help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
@@ -206,8 +206,9 @@ def run_ours(args):
                 y = torch.empty_like(b)
                 for _ in range(args.warmup + args.steps):
                     g.spmv(b.data_ptr(), y.data_ptr(), sptr)
-            elif args.profile in ("assembly", "pressure"):
-                setup = dif_call_setup if args.profile == "assembly" else pres_call_setup
+            elif args.profile in ("assembly", "pressure", "momentum"):
+                setup = {"assembly": dif_call_setup, "pressure": pres_call_setup,
+                         "momentum": vel_call_setup}[args.profile]
                 call, close = setup(np, torch, sv, s, sptr)
                 for _ in range(args.warmup + args.steps):
                     call()
@@ -307,6 +308,7 @@ def run_ours(args):
         other = other_krylov_leg(sv, S, s, n)
         assembly = assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["pressure"] = pressure_leg(np, torch, sv, s, n, peak, peak_kind)
+        assembly["momentum"] = momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -756,6 +758,71 @@ def pressure_leg(np, torch, sv, s, n, peak, peak_kind):
             "kernel": "pres_assemble_kernel<orthogonal, 6 faces, fused>"}
 
 
+def vel_inputs(np, s):
+    m = s.mesh()
+    rng = np.random.default_rng(11)
+    prop = np.zeros((1, 10))
+    prop[0, :2] = (1e-3, 1.0)
+    cc = m.xm[m.cellface[:, 0] - 1] - m.xmcc[:, 0, :]
+    return m, prop, cc, dict(pres=rng.standard_normal(m.numel) * 1e-2,
+                             gradpres=rng.standard_normal((m.numel, 3)) * 1e-2,
+                             vel=rng.standard_normal((m.numel, 3)) * 0.1,
+                             gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.1,
+                             dfield=np.ones((m.numel, 3)))
+
+
+def vel_call_setup(np, torch, sv, s, stream):
+    """A device systFormSimpleVel call on the system's mesh (lid-driven
+    cavity loads, second-order face pressure, SIMPLE, Euler dt = 1e-2,
+    under-relaxation 0.7, CSRD): (call, close)."""
+    from sfr3d_b200 import assembly as A
+    m, prop, cc, f = vel_inputs(np, s)
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    plan = A.VelPlan(g, m, m.face_r(PRES_SIDES_VEL), cc)
+    lvel = [A.Load(A.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), A.Load(A.STATICWALL, ())]
+    dev = {k: torch.tensor(np.ascontiguousarray(v), device="cuda") for k, v in f.items()}
+    d_ad3 = torch.empty(3 * s.neq, dtype=torch.float64, device="cuda")
+    d_b3 = torch.empty(3 * s.neq, dtype=torch.float64, device="cuda")
+    d_r3 = torch.empty(3 * m.numel, dtype=torch.float64, device="cuda")
+
+    def call():
+        plan.assemble_device(lvel, prop, dev["pres"].data_ptr(), dev["gradpres"].data_ptr(),
+                             dev["vel"].data_ptr(), dev["gradvel"].data_ptr(),
+                             dev["dfield"].data_ptr(), d_ad3=d_ad3.data_ptr(),
+                             d_b3=d_b3.data_ptr(), d_rcell3=d_r3.data_ptr(),
+                             time=(0, 1e-2, 1e-2), stream=stream)
+
+    def close():
+        plan.close()
+        g.close()
+    return call, close
+
+
+# algorithmic bytes per row of the momentum kernel (6 faces, CSRD full): row
+# header 6, per face the plan words (8) and 19 geometry doubles (152), the
+# cell's own pres, gradpres, vel, gradvel and material (16 doubles + 2), the
+# writes: 6 off-diagonals, the u diagonal, 3 diagonals, 3 forces, 3 cell
+# residuals and the D field (6 * 8 + 8 + 12 * 8).
+VEL_ALG_BYTES_PER_ROW = 6 + 6 * 160 + 130 + 48 + 8 + 96
+
+
+def momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind):
+    """systFormSimpleVel on the device for the same mesh (the kernel writes
+    the raw values; the solver-copy refresh follows as its own launches)."""
+    st = torch.cuda.Stream()
+    call, close = vel_call_setup(np, torch, sv, s, st.cuda_stream)
+    dev_ms = time_calls(torch, call, st)
+    close()
+    alg = VEL_ALG_BYTES_PER_ROW * s.neq
+    gbs = alg / (dev_ms * 1e-3) / 1e9
+    return {"workload": f"systFormSimpleVel, {n}^3 = {s.neq} cells, cavity loads, laminar, "
+                        "first-order upwind, second-order face pressure, SIMPLE, Euler, CSRD",
+            "device_ms": dev_ms, "alg_bytes_per_row": VEL_ALG_BYTES_PER_ROW,
+            "GB/s_incl_refresh": gbs, "frac_incl_refresh": gbs / peak,
+            "peak_source": f"{peak_kind} hbm_gbs",
+            "kernel": "vel_assemble_kernel<6 faces> + the gather/compensation refresh"}
+
+
 def cpu_assembly(O, s):
     """The reference's own systFormDif (serial, as the reference runs it) on
     the assembly leg's workload."""
@@ -776,10 +843,20 @@ def cpu_assembly(O, s):
     threads = os.cpu_count() or 1
     prc, *_, psec = O.ref_pres_assemble(pcase, O.CSRD, True, s.ia, s.ja, s.neq,
                                         nthreads=threads)
+    m, prop, cc, f = vel_inputs(np, s)
+    vcase = O.VelCase(mesh=m, cc=cc, facevelr=m.face_r(PRES_SIDES_VEL),
+                      facepresr=m.face_r([0] * 6),
+                      lvel=[O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), O.Load(O.STATICWALL, ())],
+                      prop=prop, time_flag=True, dt=1e-2, dt0=1e-2, **f)
+    vrc, *_, vsec = O.ref_vel_assemble(vcase, O.CSRD, True, s.ia, s.ja, s.neq,
+                                       nthreads=threads)
     return {"ms": sec * 1e3, "threads": 1, "status": rc,
             "sample": "one full systFormDif call (the reference's loop is serial)",
             "pressure": {"ms": psec * 1e3, "threads": threads, "status": prc,
                          "sample": "one full systFormSimplePres call with its OpenMP cell "
+                                   "loop on all host threads"},
+            "momentum": {"ms": vsec * 1e3, "threads": threads, "status": vrc,
+                         "sample": "one full systFormSimpleVel call with its OpenMP cell "
                                    "loop on all host threads"}}
 
 

@@ -607,7 +607,7 @@ def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix
 
 
 def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix=True,
-                     calrcell=True, fill=0.0):
+                     calrcell=True, fill=0.0, nthreads=0):
     """The reference's own systFormSimpleVel: (rc, a, ad, b, rcell, dfield, seconds)."""
     m = case.mesh
     lib = ref_lib()
@@ -615,7 +615,7 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         lib.sfr_ref_syst_form_simple_vel.restype = ctypes.c_int
         lib.sfr_ref_syst_form_simple_vel.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
-            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 7 + [_P])
+            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 8 + [_P])
         lib._vel_typed = True
     cal, mat = case.material()
     cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
@@ -639,6 +639,6 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         m.numel, m.nelcon.shape[1], *[_p(x) for x in arrs], len(case.lvel),
         *[_p(x) for x in vt], case.icod, int(case.fso), int(case.fvisc), int(case.fres),
         case.type_simple, int(case.time_flag), case.time_type, case.dt, case.dt0, case.under,
-        neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym),
+        neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym), nthreads,
         ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value

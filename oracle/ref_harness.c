@@ -372,7 +372,8 @@ void sfr_ref_write_coo_b(double *b, int neq, const char *name)
  * Assemble the SIMPLE momentum system with the reference's own
  * systFormSimpleVel (CellLoopInc.c:98-470) as velPresCoupling calls it
  * (Simple.c:2864-2898): ndf = 3, laminar (Turbulence all off), first-order
- * upwind, without Rhie-Chow, serial.  dfield is updated in place.
+ * upwind, without Rhie-Chow; nthreads > 1 turns on its OpenMP cell loop.
+ * dfield is updated in place.
  */
 int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nface,
                                  int *cellface, int *owner, double *volume, double *dcca,
@@ -388,7 +389,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int type_simple, int time_flag, int time_type, double dt,
                                  double dt0, double under, int neq, int nad, int storage,
                                  int forces, int matrix, int calrcell, int unsym,
-                                 double *seconds)
+                                 int nthreads, double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -408,8 +409,10 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   fileLogDebug = stderr;
   mpiVar.nPrcs = 1;
   mpiVar.myId = 0;
-  ompVar.fCell = false;
-  ompVar.nThreadsCell = 1;
+  /* its OpenMP cell loop only writes D here (Rhie-Chow is off), so threads
+   * change nothing but the time */
+  ompVar.fCell = nthreads > 1;
+  ompVar.nThreadsCell = (short)(nthreads > 1 ? nthreads : 1);
   for (i = 0; i < numel; i++) nen[i] = 8;
   fill_loads(loadsVel, nlvel, vtype, vvar, vnp, vpar, vdens);
   memset(&adv, 0, sizeof(adv));

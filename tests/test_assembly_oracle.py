@@ -215,6 +215,12 @@ def test_vel_oracle_matches_reference_live():
             assert r1[0] == r2[0] == 0
             for x, y in zip(r1[1:], r2[1:6]):
                 assert bits_equal(x, y), (icod, fso, fvisc, fres, ts, time, name)
+        # its OpenMP cell loop gives the same system (without Rhie-Chow it
+        # only writes the D field)
+        st, un, ia, ja, _al, _au = lay["csrd_full"]
+        r3 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0, nthreads=4)
+        for x, y in zip(r1[1:], r3[1:6]):
+            assert bits_equal(x, y)
 
 
 def test_vel_oracle_rejects_what_it_does_not_restate():
