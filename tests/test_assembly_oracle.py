@@ -218,6 +218,7 @@ def test_vel_oracle_matches_reference_live():
         # its OpenMP cell loop gives the same system (without Rhie-Chow it
         # only writes the D field)
         st, un, ia, ja, _al, _au = lay["csrd_full"]
+        r1 = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
         r3 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0, nthreads=4)
         for x, y in zip(r1[1:], r3[1:6]):
             assert bits_equal(x, y)
