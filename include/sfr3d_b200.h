@@ -121,6 +121,13 @@ int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k,
                         double tol, uint32_t maxit, int32_t newx,
                         int32_t precision, sfr_solve_info *info);
 
+/* The same with device arrays (d_ad_k may be NULL) on `stream`, e.g. the
+ * u, v, w systems a device momentum assembly left in d_ad3 / d_b3. */
+int sfr_gpu_solve_multi_device(sfr_system *s, int32_t solver, int32_t k, const double *d_ad_k,
+                               const double *d_b, double *d_x, double tol, uint32_t maxit,
+                               int32_t newx, int32_t precision, void *stream,
+                               sfr_solve_info *info);
+
 /* Choose how solves run: engine 0 = automatic (by size and solve), 1 = persistent
  * (the whole solve in one cooperative launch: lowest latency, small
  * systems), 2 = graph (one full-occupancy kernel per phase inside a CUDA

@@ -702,7 +702,7 @@ __device__ __forceinline__ void move_wall(const double vC[3], const double vB[3]
 // upwind, face velocity without Rhie-Chow; three diagonals and forces.
 // mtab: density then viscosity of each material.
 template <int kMV>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     vel_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, VelOpts o,
                         const int16_t *__restrict__ mat, const double *__restrict__ mtab, int nmat,
                         const double *__restrict__ pres, const double *__restrict__ gradp,

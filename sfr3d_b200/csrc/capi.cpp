@@ -330,6 +330,20 @@ int sfr_gpu_solve_device(sfr_system *s, int32_t solver, const double *d_b, doubl
   return sfr::solve_device(s, solver, 1, nullptr, d_b, d_x, tol, maxit, newx, precision, st, info);
 }
 
+int sfr_gpu_solve_multi_device(sfr_system *s, int32_t solver, int32_t k, const double *d_ad_k,
+                               const double *d_b, double *d_x, double tol, uint32_t maxit,
+                               int32_t newx, int32_t precision, void *stream,
+                               sfr_solve_info *info) {
+  if (!s || !d_b || !d_x || k < 1) return SFR_BAD_INPUT;
+  if (!s->values_set) {
+    g_last_error = "sfr_gpu_set_values was not called";
+    return SFR_BAD_INPUT;
+  }
+  SFR_CU(cudaSetDevice(s->device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  return sfr::solve_device(s, solver, k, d_ad_k, d_b, d_x, tol, maxit, newx, precision, st, info);
+}
+
 int sfr_gpu_solve_multi(sfr_system *s, int32_t solver, int32_t k, const double *ad_k,
                         const double *b, double *x, double tol, uint32_t maxit, int32_t newx,
                         int32_t precision, sfr_solve_info *info) {

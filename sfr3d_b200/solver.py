@@ -76,6 +76,8 @@ def lib() -> ctypes.CDLL:
                                 ctypes.c_uint32, _I32, _I32, _P]
     L.sfr_gpu_solve_device.argtypes = [_P, _I32, _P, _P, ctypes.c_double,
                                        ctypes.c_uint32, _I32, _I32, _P, _P]
+    L.sfr_gpu_solve_multi_device.argtypes = [_P, _I32, _I32, _P, _P, _P, ctypes.c_double,
+                                             ctypes.c_uint32, _I32, _I32, _P, _P]
     L.sfr_gpu_solve_multi.argtypes = [_P, _I32, _I32, _P, _P, _P,
                                       ctypes.c_double, ctypes.c_uint32, _I32,
                                       _I32, _P]
@@ -297,6 +299,19 @@ class GpuSystem:
         if rc < 0:
             raise SolverError(rc, "sfr_gpu_solve_device")
         return SolveInfo.from_c(info)
+
+    def solve_multi_device(self, solver, k: int, d_b: int, d_x: int, d_ad_k: int = 0,
+                           tol=1e-10, maxit=100000, newx=True, precision=FP64,
+                           stream: int = 0):
+        """k right-hand sides on device arrays (b and x k*neq, RHS r at
+        offset r*neq; d_ad_k 0 for the system's own diagonal)."""
+        infos = (SolveInfoC * k)()
+        rc = lib().sfr_gpu_solve_multi_device(self.h, solver, k, d_ad_k or None, d_b, d_x, tol,
+                                              maxit, int(newx), precision, stream or None,
+                                              infos)
+        if rc < 0:
+            raise SolverError(rc, "sfr_gpu_solve_multi_device")
+        return [SolveInfo.from_c(infos[i]) for i in range(k)]
 
     def spmv(self, d_x: int, d_y: int, stream: int = 0):
         rc = lib().sfr_gpu_spmv(self.h, d_x, d_y, stream or None)

@@ -535,8 +535,11 @@ def test_vel_assembled_momentum_solves_like_reference(cuda):
                          calrcell=False)
     torch.cuda.synchronize()
     assert bits_equal(d_ad3.cpu().numpy(), ad3) and bits_equal(d_b3.cpu().numpy(), b3)
-    xs, infos = gs.solve_multi(sv.PBICGSTAB, d_b3.cpu().numpy().reshape(3, -1), tol=1e-10,
-                               ad_k=d_ad3.cpu().numpy().reshape(3, -1))
+    # the three solves where the systems were assembled
+    d_x3 = torch.zeros(3 * s.neq, dtype=torch.float64, device="cuda")
+    infos = gs.solve_multi_device(sv.PBICGSTAB, 3, d_b3.data_ptr(), d_x3.data_ptr(),
+                                  d_ad_k=d_ad3.data_ptr(), tol=1e-10)
+    xs = d_x3.cpu().numpy().reshape(3, -1)
     for k in range(3):
         assert infos[k].status == sv.OK
         assert abs(infos[k].iters - refs[k].iters) <= 1
