@@ -309,6 +309,7 @@ def run_ours(args):
         assembly = assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["pressure"] = pressure_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["momentum"] = momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind)
+        assembly["simple_step"] = simple_step_leg(np, torch, sv, s, n)
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -823,6 +824,66 @@ def momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind):
             "kernel": "vel_assemble_kernel<6 faces> + the gather/compensation refresh"}
 
 
+def simple_step_leg(np, torch, sv, s, n):
+    """The linear-algebra half of one SIMPLE iteration kept on the device:
+    momentum assembly, the u, v, w BiCGSTAB solves in one batched launch,
+    the pressure-correction assembly from the new D field, and its PCG solve
+    (FP64 and mixed), with no host transfer between the steps."""
+    from sfr3d_b200 import assembly as A
+    m, prop, cc, f = vel_inputs(np, s)
+    gv = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    gp = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    vplan = A.VelPlan(gv, m, m.face_r(PRES_SIDES_VEL), cc)
+    pplan = A.PresPlan(gp, m, m.face_r(PRES_SIDES_PRES), m.face_r(PRES_SIDES_VEL))
+    lvel = [A.Load(A.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), A.Load(A.STATICWALL, ())]
+    lpres = [A.Load(A.DIRICHLET, (0.0,))]
+    dev = {k: torch.tensor(np.ascontiguousarray(v), device="cuda") for k, v in f.items()}
+    N = s.neq
+    z = lambda k: torch.zeros(k, dtype=torch.float64, device="cuda")  # noqa: E731
+    d_ad3, d_b3, d_x3, d_bp, d_xp = z(3 * N), z(3 * N), z(3 * N), z(N), z(N)
+    st = torch.cuda.Stream()
+    sp = st.cuda_stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    out = {"workload": f"{n}^3 cavity: systFormSimpleVel + 3 momentum BiCGSTAB (one batched "
+                       "launch) + systFormSimplePres from the new D + pressure PCG, to 1e-10, "
+                       "all on the device"}
+    for prec, tag in ((sv.FP64, "fp64"), (sv.MIXED, "mixed")):
+        for rep in range(2):  # the second pass is timed (graphs built, clocks up)
+            with torch.cuda.stream(st):
+                ev[0].record(st)
+                vplan.assemble_device(lvel, prop, dev["pres"].data_ptr(),
+                                      dev["gradpres"].data_ptr(), dev["vel"].data_ptr(),
+                                      dev["gradvel"].data_ptr(), dev["dfield"].data_ptr(),
+                                      d_ad3=d_ad3.data_ptr(), d_b3=d_b3.data_ptr(),
+                                      fres=False, time=(0, 1e-2, 1e-2), calrcell=False,
+                                      stream=sp)
+                ev[1].record(st)
+                iv = gv.solve_multi_device(sv.PBICGSTAB, 3, d_b3.data_ptr(), d_x3.data_ptr(),
+                                           d_ad_k=d_ad3.data_ptr(), tol=1e-10, precision=prec,
+                                           stream=sp)
+                ev[2].record(st)
+                pplan.assemble_device(lvel, lpres, np.array([[0.0, 1.0] + [0.0] * 8]),
+                                      dev["pres"].data_ptr(), dev["gradpres"].data_ptr(),
+                                      dev["vel"].data_ptr(), dev["dfield"].data_ptr(),
+                                      d_b=d_bp.data_ptr(), calrcell=False, stream=sp)
+                ev[3].record(st)
+                ip = gp.solve_device(sv.PCG, d_bp.data_ptr(), d_xp.data_ptr(), tol=1e-10,
+                                     precision=prec, stream=sp)
+                ev[4].record(st)
+            st.synchronize()
+        t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+        out[tag] = {"total_ms": sum(t), "momentum_assembly_ms": t[0],
+                    "momentum_solves_ms": t[1], "pressure_assembly_ms": t[2],
+                    "pressure_solve_ms": t[3], "momentum_iters": [i.iters for i in iv],
+                    "pressure_iters": ip.iters,
+                    "status": [i.status for i in iv] + [ip.status]}
+    vplan.close()
+    pplan.close()
+    gv.close()
+    gp.close()
+    return out
+
+
 def cpu_assembly(O, s):
     """The reference's own systFormDif (serial, as the reference runs it) on
     the assembly leg's workload."""
@@ -850,7 +911,27 @@ def cpu_assembly(O, s):
                       prop=prop, time_flag=True, dt=1e-2, dt0=1e-2, **f)
     vrc, *_, vsec = O.ref_vel_assemble(vcase, O.CSRD, True, s.ia, s.ja, s.neq,
                                        nthreads=threads)
+    # the same SIMPLE linear-algebra step on the host, the reference's way:
+    # its own assembly routines and its OpenMP solvers
+    t0 = time.perf_counter()
+    vr = O.ref_vel_assemble(O.VelCase(**{**vcase.__dict__, "fres": False}), O.CSRD, True,
+                            s.ia, s.ja, s.neq, nthreads=threads, calrcell=False)
+    N = s.neq
+    mom_iters = []
+    for k in range(3):
+        r = O.ref_solve(O.PBICGSTAB, O.CSRD, True, s.ia, s.ja, vr[1], vr[2][k * N:(k + 1) * N],
+                        vr[3][k * N:(k + 1) * N], tol=1e-10, nthreads=threads)
+        mom_iters.append(r.iters)
+    pc2 = O.PresCase(**{**pcase.__dict__, "dfield": vr[5]})
+    pr = O.ref_pres_assemble(pc2, O.CSRD, True, s.ia, s.ja, N, nthreads=threads, calrcell=False)
+    rp = O.ref_solve(O.PCG, O.CSRD, True, s.ia, s.ja, pr[1], pr[2], pr[3], tol=1e-10,
+                     nthreads=threads)
+    step_ms = (time.perf_counter() - t0) * 1e3
     return {"ms": sec * 1e3, "threads": 1, "status": rc,
+            "simple_step": {"ms": step_ms, "threads": threads, "momentum_iters": mom_iters,
+                            "pressure_iters": rp.iters, "status": [vr[0], pr[0], rp.status],
+                            "sample": "systFormSimpleVel + 3 pbicgstabOmp + systFormSimplePres "
+                                      "+ pcgOmp, the device step's inputs"},
             "sample": "one full systFormDif call (the reference's loop is serial)",
             "pressure": {"ms": psec * 1e3, "threads": threads, "status": prc,
                          "sample": "one full systFormSimplePres call with its OpenMP cell "
