@@ -1250,14 +1250,18 @@ int create_plan(sfr_system *s, const sfr_dif_mesh *mesh, const int16_t *facevelr
 
 // device copies for the host-array calls, allocated together on first use
 // (all or none, so that a failed allocation leaves the plan as it was)
+// fields a cell: diffusion density, cdiff, u0, gradu0 (6); pressure pres,
+// gradpres, vel, dfield (10); momentum pres, gradpres, vel, gradvel, dfield
+// (19).  Momentum calls keep their three-block ad and b in h_b0 and h_b.
 int ensure_host_buffers(sfr_dif_plan *p) {
   if (p->h_fields) return SFR_OK;
-  const size_t ne = p->numel, n = p->s->n;
+  const size_t ne = p->numel, n = p->s->n, k = p->kind == 2 ? 3 : 1;
+  const size_t per_cell = p->kind == 2 ? 19 : 10;
   double *f = nullptr, *b0 = nullptr, *b = nullptr, *rc = nullptr;
-  cudaError_t e = cudaMalloc(&f, sizeof(double) * ne * 10);
-  if (e == cudaSuccess) e = cudaMalloc(&b0, sizeof(double) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(double) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&rc, sizeof(double) * ne);
+  cudaError_t e = cudaMalloc(&f, sizeof(double) * ne * per_cell);
+  if (e == cudaSuccess) e = cudaMalloc(&b0, sizeof(double) * n * k);
+  if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(double) * n * k);
+  if (e == cudaSuccess) e = cudaMalloc(&rc, sizeof(double) * ne * k);
   if (e != cudaSuccess) {
     cudaFree(f);
     cudaFree(b0);
@@ -1513,20 +1517,16 @@ int sfr_gpu_vel_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
   if (!p || !o) return bad("NULL argument");
   if (!pres || !gradpres || !vel || !gradvel || !dfield)
     return bad("pres, gradpres, vel, gradvel and dfield are required");
+  if (p->kind != 2) return bad("not a momentum plan");
   sfr_system *s = p->s;
   SFR_CUA(cudaSetDevice(s->device));
+  int rc = ensure_host_buffers(p);
+  if (rc != SFR_OK) return rc;
   const size_t ne = p->numel, n = s->n;
-  // pres | gradpres | vel | gradvel | dfield | rcell3, and ad3 | b3
-  double *f = nullptr, *e = nullptr;
-  SFR_CUA(cudaMalloc(&f, sizeof(double) * ne * 22));
-  if (cudaMalloc(&e, sizeof(double) * n * 6) != cudaSuccess) {
-    cudaFree(f);
-    return bad("device memory for the host-array call");
-  }
   cudaStream_t st = s->stream;
+  double *f = p->h_fields;
   double *d_pres = f, *d_gp = f + ne, *d_vel = f + 4 * ne, *d_gv = f + 7 * ne,
-         *d_df = f + 16 * ne, *d_rc = f + 19 * ne, *d_ad3 = e, *d_b3 = e + 3 * n;
-  int rc = SFR_OK;
+         *d_df = f + 16 * ne, *d_rc = p->h_rcell, *d_ad3 = p->h_b0, *d_b3 = p->h_b;
   auto cp = [&](void *dst, const void *src, size_t bytes, cudaMemcpyKind k) {
     if (rc == SFR_OK && cudaMemcpyAsync(dst, src, bytes, k, st) != cudaSuccess) {
       sfr::set_last_error("a copy of the host-array call failed");
@@ -1549,8 +1549,6 @@ int sfr_gpu_vel_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
     if (rc == SFR_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = SFR_CUDA_ERROR;
   }
   cudaStreamSynchronize(st);
-  cudaFree(f);
-  cudaFree(e);
   return rc;
 }
 
