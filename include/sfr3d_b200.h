@@ -447,6 +447,100 @@ const char *sfr_last_error(void);
  * returns SFR_OK when the device can run it. */
 int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor);
 
+/* ---- row partition over several GPUs (the reference's MPI path) ------ */
+
+/* The reference's interface map (Interface, include/Mesh.h:212-222), with
+ * the same field order and types, so a pointer to the reference's struct can
+ * be passed as is.  Local equations 0..nEqNov-1 are this rank's rows, nEqNov..
+ * nEq-1 its ghosts.  xb[0..nRcvs) receives and xb[nRcvs..nRcvs+nSends) sends;
+ * neighbour n = vizPart[n] sends xb[iaRcvs[n]..iaRcvs[n+1]) to this rank and
+ * receives xb[iaSends[n]..iaSends[n+1]) from it; fMap[i] is the local
+ * equation of xb[i] (comunicateNeq, ParallelMpi.c:3346-3418).  xb is unused
+ * here (the device keeps its own buffers) and may be NULL. */
+typedef struct {
+  int32_t nRcvs;
+  int32_t nSends;
+  int32_t *iaSends;
+  int32_t *iaRcvs;
+  int32_t *fMap;
+  double *xb;
+  uint16_t nVizPart;
+  int16_t *vizPart;
+} sfr_interface;
+
+/* A row partition of one global CSRD system into the reference's per-rank
+ * layouts (the preprocessor's product that dataStruct turns into the MPI
+ * CSRD, Datastruct.c:129-190).  Built on the host. */
+typedef struct sfr_part sfr_part;
+
+/* Sizes of rank `rank`'s layout. */
+typedef struct {
+  int32_t nEq;      /* owned + ghost equations */
+  int32_t nEqNov;   /* owned equations */
+  int32_t nAd;      /* entries of the square part */
+  int32_t nAdR;     /* entries of the rectangular (ghost-column) part; 0 unsym */
+  int32_t nRcvs, nSends;
+  int32_t nVizPart;
+  int32_t ia_len;   /* nEqNov+1 (unsym) or 2*(nEqNov+1) (sym) */
+} sfr_part_sizes;
+
+/* Partition the rows of a global CSRD system (unsym = 1: full off-diagonal
+ * rows; 0: strict lower part, the symmetric storage).  part[i] is the rank
+ * of row i, or part = NULL for contiguous row blocks balanced by entries.
+ * Each rank numbers its rows in global order, then its ghosts by neighbour
+ * rank and, within a neighbour, by global number; rows are sorted by local
+ * column (sortGraphCsr, Graph.c:114).  unsym: ia[nEqNov+1], ja[nAd] full
+ * rows (mpiMatVecCsrD, HccaBlas.c:4096-4130).  sym: ia[0..nEqNov] the strict
+ * lower square part and ia[nEqNov+1..] the ghost columns of the full row,
+ * indexing ja + nAd (mpiMatVecCsrDSym, HccaBlas.c:2846-2895). */
+int sfr_part_create(int32_t neq, const int32_t *ia, const int32_t *ja, int32_t unsym,
+                    int32_t nparts, const int32_t *part, sfr_part **out);
+int sfr_part_sizes_of(const sfr_part *p, int32_t rank, sfr_part_sizes *sz);
+/* Fill rank `rank`'s arrays (sizes from sfr_part_sizes_of): ia, ja; src[k]
+ * = index in the global al of local entry k (nAd + nAdR entries); l2g[nEq]
+ * = global equation of each local one; the interface arrays iaSends and
+ * iaRcvs (nVizPart+1), fMap (nRcvs+nSends), vizPart (nVizPart).  Any
+ * output may be NULL. */
+int sfr_part_fill(const sfr_part *p, int32_t rank, int32_t *ia, int32_t *ja, int32_t *src,
+                  int32_t *l2g, int32_t *iaSends, int32_t *iaRcvs, int32_t *fMap,
+                  int16_t *vizPart);
+int sfr_part_destroy(sfr_part *p);
+
+/* A set of ranks that solve together.  A local group holds all nparts ranks
+ * in this process on one device (the halo is a device gather, the sums are
+ * taken in rank order); an NCCL group is one rank per process, the halo
+ * exchanged with ncclSend/ncclRecv and the sums with ncclAllReduce.  NCCL is
+ * loaded at run time (libnccl.so.2, or the file named by SFR_NCCL_LIBRARY). */
+typedef struct sfr_dist_group sfr_dist_group;
+/* One rank's partition resident on a device. */
+typedef struct sfr_dist sfr_dist;
+
+int sfr_dist_group_local(int32_t nparts, int32_t device, sfr_dist_group **out);
+/* 128-byte NCCL unique id, made on one rank and given to every rank. */
+int sfr_dist_nccl_id(uint8_t id[128]);
+int sfr_dist_group_nccl(int32_t nranks, int32_t rank, const uint8_t id[128], int32_t device,
+                        sfr_dist_group **out);
+int sfr_dist_group_destroy(sfr_dist_group *g);
+
+/* Upload rank `rank`'s layout (as sfr_part_fill writes it, or as the
+ * reference's dataStruct builds it under MPI) and interface.  Storage is
+ * CSRD.  In a local group every rank is created in this process before the
+ * first solve. */
+int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nEqNov,
+                        int32_t nAd, int32_t nAdR, const int32_t *ia, const int32_t *ja,
+                        int32_t unsym, const sfr_interface *iNeq, sfr_dist **out);
+/* al[nAd + nAdR], ad[nEqNov] (host). */
+int sfr_gpu_dist_set_values(sfr_dist *d, const double *al, const double *ad);
+/* mpiPcg (Cg.c:256-442) or mpiPbicgstab (Bicgstab.c:298-520) over every
+ * rank this process holds: parts[nlocal] in rank order (all ranks for a
+ * local group, the one rank for NCCL), b[r][nEqNov] and x[r][nEq] on the
+ * host (x's ghost entries are written too).  info (may be NULL) is
+ * identical on every rank. */
+int sfr_gpu_dist_solve(sfr_dist_group *g, int32_t nlocal, sfr_dist *const *parts,
+                       int32_t solver, const double *const *b, double *const *x,
+                       double tol, uint32_t maxIt, int32_t newX, sfr_solve_info *info);
+int sfr_gpu_dist_destroy(sfr_dist *d);
+
 /* ---- drop-in for the reference entry point --------------------------- */
 
 /* Same arguments and meaning as solverC (Solv.h:59-70, Solv.c:64-501).

@@ -186,6 +186,57 @@ def gmres(storage, unsym, ia, ja, al, ad, b, x0=None, tol=1e-10,
                   tol, maxit, newx, int(nk))
 
 
+
+class _Rank(ctypes.Structure):
+    _fields_ = [("nEq", ctypes.c_int), ("nEqNov", ctypes.c_int), ("nAd", ctypes.c_int),
+                ("nAdR", ctypes.c_int), ("unsym", ctypes.c_int), ("ia", _P), ("ja", _P),
+                ("al", _P), ("ad", _P), ("nRcvs", ctypes.c_int), ("nSends", ctypes.c_int),
+                ("nVizPart", ctypes.c_int), ("iaSends", _P), ("iaRcvs", _P), ("fMap", _P),
+                ("vizPart", _P)]
+
+
+def mpi_solve(solver, ranks, al, ad, b, x0=None, tol=1e-10, maxit=100000,
+              newx=True) -> tuple[list, SolveResult]:
+    """Restatement of mpiPcg (Cg.c:256-442) / mpiPbicgstab (Bicgstab.c:298-520)
+    with the ranks simulated in one process.  ranks[r] has the attributes
+    unsym, nEq, nEqNov, nAd, nAdR, ia, ja, iaSends, iaRcvs, fMap, vizPart (the
+    reference's MPI CSRD and Interface); al[r], ad[r], b[r] its values and
+    rows of b; x0[r] its nEq entries.  Returns ([x_r], SolveResult) with
+    SolveResult.x the concatenated rows."""
+    lib = oracle_lib()
+    if not getattr(lib, "_mpi_typed", False):
+        lib.orc_mpi_solve.restype = ctypes.c_int
+        lib.orc_mpi_solve.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_double,
+                                      ctypes.c_uint, ctypes.c_int, ctypes.POINTER(_Stats)]
+        lib._mpi_typed = True
+    n = len(ranks)
+    keep = []
+    arr = (_Rank * n)()
+    xs = []
+    for r, q in enumerate(ranks):
+        ia, ja = _c(q.ia, np.int32), _c(q.ja, np.int32)
+        a, d = _c(al[r], np.float64), _c(ad[r], np.float64)
+        ias, iar, fm = _c(q.iaSends, np.int32), _c(q.iaRcvs, np.int32), _c(q.fMap, np.int32)
+        vz = _c(q.vizPart, np.int16)
+        bb = _c(b[r], np.float64)
+        keep += [ia, ja, a, d, ias, iar, fm, vz, bb]
+        nrcv = q.nEq - q.nEqNov
+        arr[r] = _Rank(q.nEq, q.nEqNov, q.nAd, q.nAdR, int(bool(q.unsym)), _p(ia), _p(ja),
+                       _p(a), _p(d), nrcv, len(fm) - nrcv, len(vz), _p(ias), _p(iar),
+                       _p(fm), _p(vz))
+        xs.append(np.zeros(q.nEq) if x0 is None else np.array(x0[r], dtype=np.float64))
+    bp = (_P * n)(*[_p(keep[9 * r + 8]) for r in range(n)])
+    xp = (_P * n)(*[_p(x) for x in xs])
+    st = _Stats()
+    rc = lib.orc_mpi_solve(int(solver), n, ctypes.cast(arr, _P), bp, xp, tol, maxit,
+                           int(newx), ctypes.byref(st))
+    if rc < 0:
+        raise ValueError("orc_mpi_solve: bad interface")
+    x = np.concatenate([xs[r][:q.nEqNov] for r, q in enumerate(ranks)])
+    return xs, SolveResult(x=x, iters=st.iters, status=st.status, xKx=st.xKx,
+                           norm_x=st.norm_x, norm_r=st.norm_r, norm_r_m=st.norm_r_m,
+                           conv=st.conv)
+
 SOLVERS = {PCG: pcg, PBICGSTAB: pbicgstab, PBICGSTABL2: pbicgstabl2, GMRES: gmres,
            MINRES: minres}
 

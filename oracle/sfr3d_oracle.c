@@ -1220,3 +1220,254 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
   }
   return 0;
 }
+
+/* ---- the MPI path (test infrastructure) ------------------------------- */
+
+typedef struct {
+  int nranks;
+  const orc_rank *rk;
+  double **xb;   /* per rank: nRcvs + nSends */
+  int **peer;    /* per rank and neighbour n: the neighbour's index of this rank */
+} orc_comm;
+
+static int comm_init(orc_comm *c, int nranks, const orc_rank *rk)
+{
+  int r, n, m;
+  c->nranks = nranks;
+  c->rk = rk;
+  c->xb = calloc((size_t)nranks, sizeof(double *));
+  c->peer = calloc((size_t)nranks, sizeof(int *));
+  if (!c->xb || !c->peer) return -1;
+  for (r = 0; r < nranks; r++) {
+    const orc_rank *q = &rk[r];
+    c->xb[r] = malloc(sizeof(double) * (size_t)(q->nRcvs + q->nSends + 1));
+    c->peer[r] = malloc(sizeof(int) * (size_t)(q->nVizPart + 1));
+    if (!c->xb[r] || !c->peer[r]) return -1;
+    for (n = 0; n < q->nVizPart; n++) {
+      const int p = q->vizPart[n];
+      const orc_rank *o;
+      if (p < 0 || p >= nranks) return -1;
+      o = &rk[p];
+      c->peer[r][n] = -1;
+      for (m = 0; m < o->nVizPart; m++)
+        if (o->vizPart[m] == r) c->peer[r][n] = m;
+      if (c->peer[r][n] < 0) {
+        if (q->iaRcvs[n + 1] != q->iaRcvs[n]) return -1;
+      } else if (o->iaSends[c->peer[r][n] + 1] - o->iaSends[c->peer[r][n]] !=
+                 q->iaRcvs[n + 1] - q->iaRcvs[n]) {
+        return -1;
+      }
+    }
+  }
+  return 0;
+}
+
+static void comm_free(orc_comm *c)
+{
+  int r;
+  for (r = 0; r < c->nranks; r++) {
+    if (c->xb) free(c->xb[r]);
+    if (c->peer) free(c->peer[r]);
+  }
+  free(c->xb);
+  free(c->peer);
+}
+
+/* comunicateNeq (ParallelMpi.c:3346-3418) on every rank: makeBuffer, the
+ * sends and receives, getBuffer */
+static void comunicate(const orc_comm *c, double *const *v)
+{
+  int r, n, i;
+  for (r = 0; r < c->nranks; r++) {
+    const orc_rank *q = &c->rk[r];
+    for (i = 0; i < q->nSends; i++)
+      c->xb[r][q->nRcvs + i] = v[r][q->fMap[q->nRcvs + i]];
+  }
+  for (r = 0; r < c->nranks; r++) {
+    const orc_rank *q = &c->rk[r];
+    for (n = 0; n < q->nVizPart; n++) {
+      const int p = q->vizPart[n], m = c->peer[r][n];
+      if (m < 0) continue;
+      for (i = 0; i < q->iaRcvs[n + 1] - q->iaRcvs[n]; i++)
+        c->xb[r][q->iaRcvs[n] + i] = c->xb[p][c->rk[p].iaSends[m] + i];
+    }
+  }
+  for (r = 0; r < c->nranks; r++) {
+    const orc_rank *q = &c->rk[r];
+    for (i = 0; i < q->nRcvs; i++) v[r][q->fMap[i]] = c->xb[r][i];
+  }
+}
+
+/* mpiMatVecCsrD / mpiMatVecCsrDSym of every rank, after comunicateNeq */
+static void mpi_matvec(const orc_comm *c, double *const *x, double *const *y)
+{
+  int r, i, k;
+  comunicate(c, x);
+  for (r = 0; r < c->nranks; r++) {
+    const orc_rank *q = &c->rk[r];
+    const double *xr = x[r];
+    double *yr = y[r];
+    if (q->unsym) {
+      for (i = 0; i < q->nEqNov; i++) {
+        double tmp = q->ad[i] * xr[i];
+        for (k = q->ia[i]; k < q->ia[i + 1]; k++) tmp += q->al[k] * xr[q->ja[k]];
+        yr[i] = tmp;
+      }
+    } else {
+      const int *iar = q->ia + q->nEqNov + 1, *jar = q->ja + q->nAd;
+      const double *ar = q->al + q->nAd;
+      for (i = 0; i < q->nEqNov; i++) {
+        const double xi = xr[i];
+        double tmp = q->ad[i] * xi;
+        for (k = q->ia[i]; k < q->ia[i + 1]; k++) {
+          const int j = q->ja[k];
+          const double s = q->al[k];
+          tmp += s * xr[j];
+          yr[j] += s * xi;
+        }
+        for (k = iar[i]; k < iar[i + 1]; k++) tmp += ar[k] * xr[jar[k]];
+        yr[i] = tmp;
+      }
+    }
+  }
+}
+
+/* dot under MPI: each rank's sum, then the sum over the ranks in rank order */
+static double mpi_dot(const orc_comm *c, double *const *a, double *const *b)
+{
+  double t = 0.0;
+  int r;
+  for (r = 0; r < c->nranks; r++) {
+    const double l = orc_dot(a[r], b[r], c->rk[r].nEqNov);
+    t = r == 0 ? l : t + l;
+  }
+  return t;
+}
+
+int orc_mpi_solve(int solver, int nranks, const orc_rank *rk, const double *const *b,
+                  double *const *x, double tol, unsigned maxit, int newx, orc_stats *st)
+{
+  enum { NV = 8 };
+  orc_comm c = {0, 0, 0, 0};
+  double **w[NV];
+  double alpha, beta, d, di, conv, rr0, om;
+  unsigned j = 0;
+  int q, i, k, rc = 0;
+  if (nranks <= 0 || (solver != 1 && solver != 2)) return -1;
+  for (k = 0; k < NV; k++) {
+    w[k] = calloc((size_t)nranks, sizeof(double *));
+    if (!w[k]) return -1;
+  }
+  if (comm_init(&c, nranks, rk) != 0) { rc = -1; goto done; }
+  for (k = 0; k < NV; k++)
+    for (q = 0; q < nranks; q++) {
+      w[k][q] = calloc((size_t)rk[q].nEq + 1, sizeof(double));
+      if (!w[k][q]) { rc = -1; goto done; }
+    }
+  {
+    double **m = w[0], **z = w[1], **r = w[2], **p = w[3], **t = w[4], **v = w[5],
+           **r0 = w[6], **bb = w[7];
+    for (q = 0; q < nranks; q++) {
+      for (i = 0; i < rk[q].nEqNov; i++) {
+        m[q][i] = 1.0 / rk[q].ad[i];
+        bb[q][i] = b[q][i];
+      }
+      if (newx)
+        for (i = 0; i < rk[q].nEq; i++) x[q][i] = 0.0;
+    }
+    if (solver == 1) {
+      /* mpiPcg, Cg.c:283-366 */
+      for (q = 0; q < nranks; q++)
+        for (i = 0; i < rk[q].nEqNov; i++) z[q][i] = bb[q][i] * m[q][i];
+      d = mpi_dot(&c, bb, z);
+      conv = tol * sqrt(fabs(d));
+      mpi_matvec(&c, x, z);
+      for (q = 0; q < nranks; q++)
+        for (i = 0; i < rk[q].nEqNov; i++) {
+          r[q][i] = bb[q][i] - z[q][i];
+          z[q][i] = r[q][i] * m[q][i];
+          p[q][i] = z[q][i];
+        }
+      d = mpi_dot(&c, r, z);
+      for (j = 0; j < maxit; j++) {
+        mpi_matvec(&c, p, z);
+        alpha = d / mpi_dot(&c, z, p);
+        for (q = 0; q < nranks; q++)
+          for (i = 0; i < rk[q].nEqNov; i++) {
+            x[q][i] += alpha * p[q][i];
+            r[q][i] -= alpha * z[q][i];
+            z[q][i] = r[q][i] * m[q][i];
+          }
+        di = mpi_dot(&c, r, z);
+        beta = di / d;
+        for (q = 0; q < nranks; q++)
+          for (i = 0; i < rk[q].nEqNov; i++) p[q][i] = z[q][i] + beta * p[q][i];
+        d = di;
+        if (sqrt(fabs(d)) < conv) break;
+      }
+    } else {
+      /* mpiPbicgstab, Bicgstab.c:325-437 */
+      d = mpi_dot(&c, bb, bb);
+      conv = tol * sqrt(d);
+      mpi_matvec(&c, x, z);
+      for (q = 0; q < nranks; q++)
+        for (i = 0; i < rk[q].nEqNov; i++) {
+          r0[q][i] = bb[q][i] - z[q][i];
+          p[q][i] = r0[q][i];
+          r[q][i] = r0[q][i];
+          z[q][i] = p[q][i] * m[q][i];
+        }
+      for (j = 0; j < maxit; j++) {
+        mpi_matvec(&c, z, v);
+        rr0 = mpi_dot(&c, r, r0);
+        alpha = rr0 / mpi_dot(&c, v, r0);
+        for (q = 0; q < nranks; q++)
+          for (i = 0; i < rk[q].nEqNov; i++) {
+            x[q][i] += alpha * z[q][i];
+            r[q][i] -= alpha * v[q][i];
+            z[q][i] = r[q][i] * m[q][i];
+          }
+        d = mpi_dot(&c, r, r);
+        if (sqrt(d) < conv) break;
+        mpi_matvec(&c, z, t);
+        om = mpi_dot(&c, t, r) / mpi_dot(&c, t, t);
+        for (q = 0; q < nranks; q++)
+          for (i = 0; i < rk[q].nEqNov; i++) {
+            x[q][i] += om * z[q][i];
+            r[q][i] -= om * t[q][i];
+          }
+        d = mpi_dot(&c, r, r);
+        if (sqrt(fabs(d)) < conv) break;
+        beta = (mpi_dot(&c, r, r0) / rr0) * (alpha / om);
+        for (q = 0; q < nranks; q++)
+          for (i = 0; i < rk[q].nEqNov; i++) {
+            p[q][i] = r[q][i] + beta * (p[q][i] - om * v[q][i]);
+            z[q][i] = p[q][i] * m[q][i];
+          }
+      }
+    }
+    /* post-processing, Cg.c:376-396 / Bicgstab.c:440-455 */
+    mpi_matvec(&c, x, z);
+    st->xKx = mpi_dot(&c, x, z);
+    st->norm_x = sqrt(mpi_dot(&c, x, x));
+    for (q = 0; q < nranks; q++)
+      for (i = 0; i < rk[q].nEqNov; i++) {
+        r[q][i] = bb[q][i] - z[q][i];
+        z[q][i] = r[q][i] * m[q][i];
+      }
+    st->norm_r_m = solver == 1 ? sqrt(fabs(mpi_dot(&c, r, z))) : NAN;
+    st->norm_r = sqrt(mpi_dot(&c, r, r));
+    st->conv = conv;
+    st->iters = (int)j + 1;
+    st->status = j == maxit ? 1 : 0;
+    rc = st->status;
+  }
+done:
+  for (k = 0; k < NV; k++) {
+    if (w[k])
+      for (q = 0; q < nranks; q++) free(w[k][q]);
+    free(w[k]);
+  }
+  comm_free(&c);
+  return rc;
+}

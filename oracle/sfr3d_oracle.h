@@ -171,4 +171,27 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
                      const int *ia, const int *ja, double *a, double *ad, double *b,
                      double *rcell, int forces, int matrix, int calrcell);
 
+/* ---- the MPI path: row-partitioned PCG and BiCGSTAB ------------------- */
+
+/* One rank's layout and interface (Interface, Mesh.h:212-222; the MPI CSRD of
+ * Datastruct.c:129-190): rows 0..nEqNov-1 owned, nEqNov..nEq-1 ghosts. */
+typedef struct {
+  int nEq, nEqNov, nAd, nAdR, unsym;
+  const int *ia, *ja;
+  const double *al, *ad;
+  int nRcvs, nSends, nVizPart;
+  const int *iaSends, *iaRcvs, *fMap;
+  const short *vizPart;
+} orc_rank;
+
+/* mpiPcg (Cg.c:256-442, solver 1) or mpiPbicgstab (Bicgstab.c:298-520,
+ * solver 2) with nranks ranks simulated in this process: comunicateNeq
+ * (ParallelMpi.c:3346-3418) before every product, mpiMatVecCsrD
+ * (HccaBlas.c:4096-4130) or mpiMatVecCsrDSym (HccaBlas.c:2846-2895), and
+ * each dot a rank's left-to-right sum, summed over the ranks in rank order
+ * (the MPI_Allreduce of dot, HccaBlas.c:393-437).  b[r][nEqNov], x[r][nEq].
+ * Returns the status; -1 on a bad interface. */
+int orc_mpi_solve(int solver, int nranks, const orc_rank *rk, const double *const *b,
+                  double *const *x, double tol, unsigned maxit, int newx, orc_stats *st);
+
 #endif

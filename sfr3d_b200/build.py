@@ -27,14 +27,28 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["krylov.cu", "mixed.cu", "stream_solve.cu", "batched.cu", "device_mem.cu",
+CUDA_SOURCES = ["krylov.cu", "mixed.cu", "stream_solve.cu", "batched.cu", "device_mem.cu", "halo.cu",
                 "noalloc.cu", "adjoint.cu", "resident.cu", "krylov_ext.cu",
                 "assembly.cu"]
-HOST_SOURCES = ["capi.cpp", "sell_build.cpp"]
+HOST_SOURCES = ["capi.cpp", "sell_build.cpp", "partition.cpp"]
 SYSTEM_SOURCES = ["systems.cpp"]
 
 LIB = os.path.join(HERE, "libsfr3d_b200.so")
 SYSLIB = os.path.join(HERE, "libsfr3d_systems.so")
+
+
+def _nccl_include() -> list[str]:
+    # nccl.h of the NCCL that torch loads (the library itself is opened at
+    # run time); the system header otherwise
+    try:
+        import nvidia.nccl as _n  # noqa: PLC0415
+        for base in _n.__path__:
+            inc = os.path.join(base, "include")
+            if os.path.exists(os.path.join(inc, "nccl.h")):
+                return ["-I", inc]
+    except ImportError:
+        pass
+    return []
 
 
 def _host_cxx() -> str:
@@ -73,7 +87,7 @@ def _compile(src: str, ptxas: bool) -> str:
     cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17",
            "-ccbin", _host_cxx(), "-Xcompiler", "-fPIC,-O2",
            "--expt-relaxed-constexpr", "--extended-lambda",
-           "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+           "-I", INCLUDE, "-I", CSRC, *_nccl_include(), "-c", src, "-o", obj]
     if ptxas and src.endswith(".cu"):
         cmd.insert(1, "-Xptxas")
         cmd.insert(2, "-v")
@@ -89,7 +103,7 @@ def build_cuda(ptxas: bool = False) -> str:
         objs = list(ex.map(lambda s: _compile(s, ptxas), srcs))
     if _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-ccbin", _host_cxx(),
-              *objs, "-o", LIB + ".tmp"])
+              *objs, "-ldl", "-o", LIB + ".tmp"])
         os.replace(LIB + ".tmp", LIB)
     return LIB
 

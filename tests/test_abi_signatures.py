@@ -5,7 +5,7 @@ from __future__ import annotations
 import os
 import re
 
-from sfr3d_b200 import assembly, solver
+from sfr3d_b200 import assembly, halo, solver
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -24,6 +24,7 @@ def test_argtypes_match_the_header():
     arity = declared_arity("sfr3d_b200.h")
     lib = solver.lib()
     assembly._lib()
+    halo._lib()
     checked = 0
     for name, n in arity.items():
         fn = getattr(lib, name, None)
@@ -31,4 +32,4 @@ def test_argtypes_match_the_header():
             continue
         assert len(fn.argtypes) == n, (name, len(fn.argtypes), n)
         checked += 1
-    assert checked >= 40
+    assert checked >= 52

@@ -1,0 +1,146 @@
+"""The partitioned solve on the GPU (csrc/halo.cu through the C ABI) against
+the oracle's restatement of mpiPcg / mpiPbicgstab with the same ranks.
+
+A local group runs every rank on one device (the only form a single GPU
+can run); an NCCL group of one rank runs the NCCL transport's calls.  Bar:
+the matrix rows are the reference's (bit-identical products); each rank's
+partial dots are a fixed tree instead of the reference's left-to-right sum,
+so iterations agree within one and x to 1e-12 relative (PCG) / within the
+tolerance-level spread (BiCGSTAB)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sfr3d_b200 import halo as H
+from sfr3d_b200 import solver as SV
+from sfr3d_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _ranked(lays, al, ad, b):
+    return ([lay.values(al, ad)[0] for lay in lays], [lay.values(al, ad)[1] for lay in lays],
+            [lay.rows(b) for lay in lays])
+
+
+def _global(lays, xs, n):
+    x = np.zeros(n)
+    for lay, xr in zip(lays, xs):
+        x[lay.l2g[:lay.nEqNov]] = xr[:lay.nEqNov]
+    return x
+
+
+def _gpu(lays, al, ad, b, solver, **kw):
+    g = H.LocalGroup(len(lays), 0)
+    systems = [H.DistSystem(g, lay) for lay in lays]
+    a_r, d_r, b_r = _ranked(lays, al, ad, b)
+    for s, a, d in zip(systems, a_r, d_r):
+        s.set_values(a, d)
+    xs, info = H.solve(g, systems, solver, b_r, **kw)
+    g.close()
+    return xs, info
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("unsym", [True, False])
+@pytest.mark.parametrize("nparts", [1, 2, 4])
+def test_local_group_pcg_matches_the_oracle(unsym, nparts):
+    s = S.poisson_jittered(24, seed=7)
+    ia, ja, al = (s.ia, s.ja, s.al) if unsym else s.csrd_lower()
+    ad, b = s.ad, s.b[0]
+    lays = H.partition(s.neq, ia, ja, unsym, nparts)
+    xs_o, ref = O.mpi_solve(O.PCG, lays, *_ranked(lays, al, ad, b), tol=1e-10)
+    xs, info = _gpu(lays, al, ad, b, O.PCG, tol=1e-10)
+    assert info.status == 0
+    assert abs(info.iters - ref.iters) <= 1
+    x = _global(lays, xs, s.neq)
+    assert _rel(x, ref.x) < 1e-12
+    assert abs(info.xKx - ref.xKx) <= 1e-10 * abs(ref.xKx)
+    assert abs(info.norm_x - ref.norm_x) <= 1e-10 * ref.norm_x
+    assert info.norm_r_m < 3.16 * info.conv
+    # ghost entries: the owners' final values
+    for lay, xr in zip(lays, xs):
+        assert np.array_equal(xr[lay.nEqNov:], x[lay.l2g[lay.nEqNov:]])
+
+
+@pytest.mark.parametrize("nparts", [1, 3])
+def test_local_group_bicgstab_matches_the_oracle(nparts):
+    m = S.momentum(20, peclet=50.0, nrhs=1)
+    lays = H.partition(m.neq, m.ia, m.ja, True, nparts)
+    _, ref = O.mpi_solve(O.PBICGSTAB, lays, *_ranked(lays, m.al, m.ad, m.b[0]), tol=1e-10)
+    xs, info = _gpu(lays, m.al, m.ad, m.b[0], O.PBICGSTAB, tol=1e-10)
+    assert info.status == 0
+    assert abs(info.iters - ref.iters) <= 1
+    assert _rel(_global(lays, xs, m.neq), ref.x) < 1e-12
+
+
+def test_bicgstab_on_a_poisson_system_within_the_order_spread():
+    """BiCGSTAB on a symmetric system is sensitive to the summation order:
+    the bar is the spread of the oracle itself over partitionings."""
+    s = S.poisson_jittered(16, seed=9)
+    al, ad, b = s.al, s.ad, s.b[0]
+    its, xs_ref = [], []
+    for R in (1, 2, 3):
+        lays = H.partition(s.neq, s.ia, s.ja, True, R)
+        xs, r = O.mpi_solve(O.PBICGSTAB, lays, *_ranked(lays, al, ad, b), tol=1e-10)
+        its.append(r.iters)
+        xs_ref.append(_global(lays, xs, s.neq))
+    lays = H.partition(s.neq, s.ia, s.ja, True, 2)
+    xs, info = _gpu(lays, al, ad, b, O.PBICGSTAB, tol=1e-10)
+    x = _global(lays, xs, s.neq)
+    assert info.status == 0
+    assert min(its) - 1 <= info.iters <= max(its) + 1
+    spread = max(_rel(v, xs_ref[0]) for v in xs_ref[1:])
+    assert _rel(x, xs_ref[1]) <= max(10 * spread, 1e-12)
+
+
+def test_warm_start_and_maxit():
+    s = S.poisson_jittered(16, seed=4)
+    lays = H.partition(s.neq, s.ia, s.ja, True, 3)
+    rng = np.random.default_rng(2)
+    xg0 = rng.standard_normal(s.neq)
+    x0 = [xg0[lay.l2g] for lay in lays]
+    _, ref = O.mpi_solve(O.PCG, lays, *_ranked(lays, s.al, s.ad, s.b[0]), x0=x0,
+                         tol=1e-10, newx=False)
+    xs, info = _gpu(lays, s.al, s.ad, s.b[0], O.PCG, x0=x0, tol=1e-10, newx=False)
+    assert abs(info.iters - ref.iters) <= 1
+    assert _rel(_global(lays, xs, s.neq), ref.x) < 1e-12
+    _, ref = O.mpi_solve(O.PCG, lays, *_ranked(lays, s.al, s.ad, s.b[0]), tol=1e-10, maxit=7)
+    xs, info = _gpu(lays, s.al, s.ad, s.b[0], O.PCG, tol=1e-10, maxit=7)
+    assert info.status == 1 and info.iters == ref.iters == 8
+    assert _rel(_global(lays, xs, s.neq), ref.x) < 1e-12
+
+
+def test_nccl_group_of_one_rank_equals_the_local_group():
+    s = S.poisson_jittered(20, seed=6)
+    lays = H.partition(s.neq, s.ia, s.ja, True, 1)
+    xs_l, info_l = _gpu(lays, s.al, s.ad, s.b[0], O.PCG, tol=1e-10)
+    g = H.NcclGroup(1, 0, H.nccl_unique_id(), 0)
+    d = H.DistSystem(g, lays[0])
+    a, dd = lays[0].values(s.al, s.ad)
+    d.set_values(a, dd)
+    xs, info = H.solve(g, [d], O.PCG, [lays[0].rows(s.b[0])], tol=1e-10)
+    g.close()
+    assert info.iters == info_l.iters
+    assert np.array_equal(xs[0], xs_l[0])
+
+
+def test_interface_mismatch_is_an_error_before_any_solve():
+    s = S.poisson_jittered(10, seed=3)
+    lays = H.partition(s.neq, s.ia, s.ja, True, 2)
+    lay = lays[1]
+    lay.iaSends = lay.iaSends.copy()
+    lay.fMap = lay.fMap[:-1].copy()  # one value fewer sent to rank 0
+    lay.iaSends[-1] -= 1
+    g = H.LocalGroup(2, 0)
+    systems = [H.DistSystem(g, la) for la in lays]
+    for sy, la in zip(systems, lays):
+        sy.set_values(*la.values(s.al, s.ad))
+    with pytest.raises(SV.SolverError, match="interface mismatch"):
+        H.solve(g, systems, O.PCG, [la.rows(s.b[0]) for la in lays], tol=1e-10)
+    g.close()
