@@ -56,7 +56,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the momentum, batched and adjoint legs")
     ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab", "assembly",
-                                          "pressure", "momentum"], default="none",
+                                          "pressure", "momentum", "partitioned"],
+                    default="none",
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
                     help="0 auto, 1 persistent, 2 graph, 3 graph kernels from a host "
@@ -213,6 +214,17 @@ def run_ours(args):
                 for _ in range(args.warmup + args.steps):
                     call()
                 close()
+            elif args.profile == "partitioned":
+                from sfr3d_b200 import halo as H
+                lays = H.partition(N, s.ia, s.ja, True, 2)
+                hg = H.LocalGroup(2, local)
+                hs = [H.DistSystem(hg, lay) for lay in lays]
+                for sy, lay in zip(hs, lays):
+                    sy.set_values(*lay.values(s.al, s.ad))
+                b_r = [lay.rows(s.b[0]) for lay in lays]
+                for _ in range(args.warmup + args.steps):
+                    H.solve(hg, hs, sv.PCG, b_r, tol=1e-10, maxit=args.maxit)
+                hg.close()
             elif args.profile == "bicgstab":
                 m = S.momentum(n, nrhs=1, seed=3)
                 gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=local)
@@ -300,7 +312,7 @@ def run_ours(args):
     spmv_gbs = sb / (spmv_ms * 1e-3) / 1e9
     sp_tr = committed_traffic("spmv_kernel")
 
-    momentum = batch = adjoint = target = assembly = None
+    momentum = batch = adjoint = target = assembly = partitioned = None
     if world > 1 and not args.no_extras:
         batch = batch_leg_sharded(sv, S, rank, world, max_over_ranks)
     other = None
@@ -310,6 +322,7 @@ def run_ours(args):
         assembly["pressure"] = pressure_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["momentum"] = momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["simple_step"] = simple_step_leg(np, torch, sv, s, n)
+        partitioned = partitioned_leg(np, sv, s, n, ms_step, x.cpu().numpy())
         momentum = momentum_leg(np, torch, sv, S, n, local)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
@@ -408,6 +421,7 @@ def run_ours(args):
                  "timing": "graph of 20 x [256 MiB read, SpMV] minus graph of 20 x [256 MiB read]"},
         "mixed": mixed,
         "momentum": momentum,
+        "partitioned": partitioned,
         "batched": batch,
         "adjoint": adjoint,
         "other_krylov": other,
@@ -459,6 +473,44 @@ def spmv_time(torch, g, x, stream, reps=20):
         t = e0.elapsed_time(e1)
         best[name] = min(best.get(name, t), t)
     return (best["a"] - best["b"]) / reps
+
+
+def partitioned_leg(np, sv, s, n, fp64_ms, x64):
+    """The row-partitioned PCG (the reference's MPI path, mpiPcg) on the
+    headline system, its ranks held by one GPU: device time per solve at 1,
+    2 and 4 ranks against the unpartitioned solve."""
+    from sfr3d_b200 import halo as H
+    out = {"what": f"mpiPcg path, {n}^3 headline system, R ranks in one process on one GPU "
+                   "(halo = one device gather, sums in rank order inside the kernels, the "
+                   "iteration loop a CUDA graph of 32 iterations); FP64 to 1e-10",
+           "timing": "CUDA events inside sfr_gpu_dist_solve, mean of 2 after 1 warm-up"}
+    N, nnz = s.neq, s.nnz_full
+    for R in (1, 2, 4):
+        lays = H.partition(N, s.ia, s.ja, True, R)
+        g = H.LocalGroup(R, 0)
+        systems = [H.DistSystem(g, lay) for lay in lays]
+        for sy, lay in zip(systems, lays):
+            sy.set_values(*lay.values(s.al, s.ad))
+        b_r = [lay.rows(s.b[0]) for lay in lays]
+        H.solve(g, systems, sv.PCG, b_r, tol=1e-10)
+        ms = []
+        for _ in range(2):
+            xs, info = H.solve(g, systems, sv.PCG, b_r, tol=1e-10)
+            ms.append(info.seconds * 1e3)
+        x = np.zeros(N)
+        for lay, xr in zip(lays, xs):
+            x[lay.l2g[:lay.nEqNov]] = xr[:lay.nEqNov]
+        ghosts = sum(lay.nRcvs for lay in lays)
+        alg = pcg_alg_bytes(N, nnz, info.iters) + (info.iters + 2) * 16 * ghosts
+        t = statistics.mean(ms)
+        out[f"ranks_{R}"] = {"ms": t, "iterations": info.iters, "ghost_entries": ghosts,
+                             "vs_unpartitioned": t / fp64_ms,
+                             "alg_GB/s": alg / (t * 1e-3) / 1e9,
+                             "err_vs_unpartitioned_x": float(np.linalg.norm(x - x64)
+                                                             / np.linalg.norm(x64)),
+                             "launches_per_iteration": 3 * R + (1 if R > 1 else 0)}
+        g.close()
+    return out
 
 
 def momentum_leg(np, torch, sv, S, n, device):

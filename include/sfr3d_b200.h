@@ -521,6 +521,8 @@ int sfr_dist_nccl_id(uint8_t id[128]);
 int sfr_dist_group_nccl(int32_t nranks, int32_t rank, const uint8_t id[128], int32_t device,
                         sfr_dist_group **out);
 int sfr_dist_group_destroy(sfr_dist_group *g);
+/* kind (0 local, 1 NCCL), rank count and, for NCCL, this process's rank. */
+int sfr_dist_group_info(const sfr_dist_group *g, int32_t *kind, int32_t *nranks, int32_t *rank);
 
 /* Upload rank `rank`'s layout (as sfr_part_fill writes it, or as the
  * reference's dataStruct builds it under MPI) and interface.  Storage is
@@ -560,6 +562,16 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd,
                 void *bOmp, double tol, uint32_t maxIt, int16_t storage,
                 int16_t solver, FILE *fSolvLog, bool fLog, bool newX,
                 bool unSym, const char *name);
+/* The MPI branch of solverC (Solv.c:952-977, 1070-1093: mpiPcg and
+ * mpiPbicgstab when nPrcs > 1).  With an NCCL group set, every sfr_solverC
+ * call of this process is one rank's share: iNeq is the reference's
+ * Interface (sfr_interface has its layout), storage must be CSRD, al holds
+ * nAd + nAdR values, x holds nEq entries (ghosts are written too), and
+ * solver PCG or PBICGSTAB.  Rank 0 writes the MPIPCG / MPIPBICGSTAB log line
+ * and the non-convergence messages; failure exits with EXIT_SOLVER (-2) as
+ * the reference does (Cg.c:409-420, Bicgstab.c:478-488).  The partition is
+ * cached per (ia, ja); g = NULL returns to the single-GPU path. */
+int sfr_solverC_set_group(sfr_dist_group *g);
 void sfr_set_exit_on_failure(int32_t flag);
 /* SFR_MIXED: the inner FP32 residual must fall by this factor (0 < delta
  * < 1) before the FP64 solution is refreshed and the true residual

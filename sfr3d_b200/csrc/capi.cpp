@@ -643,10 +643,111 @@ uint64_t pattern_hash(const int32_t *ia, const int32_t *ja, int32_t n_ia, int64_
 void sfr_set_exit_on_failure(int32_t flag) { g_exit_on_failure = flag != 0; }
 void sfr_set_precision(int32_t precision) { g_precision = precision; }
 
+namespace {
+void release_dist_cache();
+}
+
 void sfr_solverC_release(void) {
   std::lock_guard<std::mutex> lk(g_shim_mu);
   for (auto &kv : g_cache) sfr_gpu_destroy(kv.second.sys);
   g_cache.clear();
+  release_dist_cache();
+}
+
+// The MPI branch: one rank's share of a row-partitioned system per call.
+namespace {
+sfr_dist_group *g_group = nullptr;
+struct DistCached {
+  sfr_dist *d = nullptr;
+  uint64_t hash = 0;
+};
+std::map<PatternKey, DistCached> g_dist_cache;
+
+void release_dist_cache() {
+  for (auto &kv : g_dist_cache)
+    if (kv.second.d) sfr_gpu_dist_destroy(kv.second.d);
+  g_dist_cache.clear();
+}
+
+int solverC_mpi(int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR, int32_t *ia,
+                int32_t *ja, double *al, double *ad, double *b, double *x, void *iNeq,
+                double tol, uint32_t maxIt, int16_t storage, int16_t solver, FILE *fSolvLog,
+                bool fLog, bool newX, bool unSym, const char *name) {
+  int32_t kind = 0, nranks = 0, rank = 0;
+  sfr_dist_group_info(g_group, &kind, &nranks, &rank);
+  if (storage != SFR_CSRD || (solver != SFR_PCG && solver != SFR_PBICGSTAB) || !iNeq ||
+      kind != 1) {
+    fprintf(stderr, "Opcao %d e invalida!!\n", storage != SFR_CSRD ? storage : solver);
+    fprintf(stderr, "Arquivo:%s\nFonte:  %s\n", __FILE__, "sfr_solverC (MPI)");
+    if (g_exit_on_failure) exit(EXIT_FAILURE);
+    return SFR_UNSUPPORTED;
+  }
+  const int32_t n_ia = unSym ? nEqNov + 1 : 2 * (nEqNov + 1);
+  const uint64_t h = pattern_hash(ia, ja, n_ia, static_cast<int64_t>(nAd) + nAdR) ^
+                     (static_cast<uint64_t>(nEq) << 32);
+  PatternKey key{ia, ja, nEqNov, storage, unSym ? 1 : 0};
+  DistCached &c = g_dist_cache[key];
+  int rc = SFR_OK;
+  if (!c.d || c.hash != h) {
+    if (c.d) sfr_gpu_dist_destroy(c.d);
+    c.d = nullptr;
+    rc = sfr_gpu_dist_create(g_group, rank, nEq, nEqNov, nAd, nAdR, ia, ja, unSym ? 1 : 0,
+                             static_cast<const sfr_interface *>(iNeq), &c.d);
+    if (rc != SFR_OK) g_dist_cache.erase(key);
+    else c.hash = h;
+  }
+  sfr_solve_info info;
+  std::memset(&info, 0, sizeof(info));
+  if (rc == SFR_OK) rc = sfr_gpu_dist_set_values(c.d, al, ad);
+  if (rc == SFR_OK) {
+    sfr_dist *parts[1] = {c.d};
+    const double *bs[1] = {b};
+    double *xs[1] = {x};
+    rc = sfr_gpu_dist_solve(g_group, 1, parts, solver, bs, xs, tol, maxIt, newX ? 1 : 0, &info);
+  }
+  const bool pcg = solver == SFR_PCG;
+  if (rc == SFR_MAXIT) {
+    if (rank == 0) {
+      printf("name : %s\n", name ? name : "");
+      printf(pcg ? " MPIPCG *** WARNING: no convergende reached !\n"
+                 : " MPIPBICGSTAB *** WARNING: no convergende reached !\n");
+      printf("MAXIT = %d \n", maxIt);
+    }
+    if (g_exit_on_failure) exit(-2);
+    return rc;
+  }
+  if (rc != SFR_OK) {
+    fprintf(stderr, "sfr_solverC: %s (%s)\n", sfr_status_string(rc), g_last_error.c_str());
+    if (g_exit_on_failure) exit(-2);
+    return rc;
+  }
+  if (rank == 0 && fLog && fSolvLog) {
+    if (pcg)
+      fprintf(fSolvLog,
+              "MPIPCG: tol %20.2e iteration %d xKx %20.12e norma(x*x) %20.12e time %20.5lf\n",
+              tol, info.iters, info.xKx, info.norm_x, info.seconds);
+    else
+      fprintf(fSolvLog,
+              "MPIPBICGSTAB: tol %20.2e iteration %d xKx %20.12e ||x*x|| %20.12e "
+              "time %20.5lf\n",
+              tol, info.iters, info.xKx, info.norm_x, info.seconds);
+  }
+  return rc;
+}
+}  // namespace
+
+int sfr_solverC_set_group(sfr_dist_group *g) {
+  std::lock_guard<std::mutex> lk(g_shim_mu);
+  if (g) {
+    int32_t kind = 0;
+    if (sfr_dist_group_info(g, &kind, nullptr, nullptr) != SFR_OK || kind != 1) {
+      g_last_error = "solverC takes an NCCL group (one rank per process)";
+      return SFR_BAD_INPUT;
+    }
+  }
+  release_dist_cache();
+  g_group = g;
+  return SFR_OK;
 }
 
 int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR, int32_t *ia,
@@ -655,10 +756,11 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR,
                 int16_t solver, FILE *fSolvLog, bool fLog, bool newX, bool unSym,
                 const char *name) {
   (void)m;
-  (void)nAdR;
-  (void)iNeq;
   (void)bOmp;
   std::lock_guard<std::mutex> lk(g_shim_mu);
+  if (g_group)
+    return solverC_mpi(nEq, nEqNov, nAd, nAdR, ia, ja, al, ad, b, x, iNeq, tol, maxIt, storage,
+                       solver, fSolvLog, fLog, newX, unSym, name);
   int rc = SFR_OK;
   const bool known = solver == SFR_PCG || solver == SFR_PBICGSTAB || solver == SFR_PBICGSTABL2 ||
                      solver == SFR_GMRES || solver == SFR_MINRES;

@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -55,6 +56,7 @@ using sfr::xsub;
 
 constexpr int kThreads = 256;
 constexpr int kSlots = 8;  // sums per phase, at most
+constexpr int kChunk = 32; // iterations per replay of the captured loop
 
 // ---------------------------------------------------------------- NCCL ----
 // Loaded at run time so that the library needs NCCL only when an NCCL group
@@ -128,7 +130,19 @@ struct Args {  // one rank's launch arguments
   double *part;
   unsigned *counter;
   DState *st;
+  // local group: every rank's state, so that a kernel sums the ranks'
+  // partials itself (in rank order); null for NCCL (the allreduce did it)
+  DState *const *sts;
+  int nranks;
 };
+
+// The sum over the ranks of partial s.
+__device__ __forceinline__ double total(const Args &a, int s) {
+  if (!a.sts) return a.st->glob[s];
+  double t = a.sts[0]->loc[s];
+  for (int r = 1; r < a.nranks; ++r) t = xadd(t, a.sts[r]->loc[s]);
+  return t;
+}
 
 // Block partials of NV values -> the last block sums them in block order and
 // returns true there, with the totals in tot (all its threads).
@@ -175,6 +189,13 @@ __device__ __forceinline__ double row_y(const Args &a, const double *xv, int row
 
 #define ROWS_OF(a) \
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < (a).n; row += gridDim.x * blockDim.x)
+// row pairs (2pr, 2pr+1) with 16-byte loads; every vector starts 16-byte
+// aligned, and a last odd row is handled alone
+#define PAIRS_OF(a) \
+  for (int pr = blockIdx.x * blockDim.x + threadIdx.x; 2 * pr < (a).n; pr += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
 
 __device__ __forceinline__ void stop(DState *st, int status, unsigned iters) {
   st->active = 0;
@@ -214,7 +235,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_start(Args a) {
   double tot[1];
   if (rank_sums<1>(acc, a, tot) && threadIdx.x == 0) {
     a.st->loc[1] = tot[0];
-    a.st->conv = xmul(a.st->tol, sqrt(fabs(a.st->glob[0])));
+    a.st->conv = xmul(a.st->tol, sqrt(fabs(total(a, 0))));
   }
 }
 
@@ -230,23 +251,39 @@ __global__ void __launch_bounds__(kThreads) k_pcg_a(Args a) {
   double tot[1];
   if (rank_sums<1>(acc, a, tot) && threadIdx.x == 0) {
     a.st->loc[2] = tot[0];
-    if (a.st->j == 0) a.st->d = a.st->glob[1];
+    if (a.st->j == 0) a.st->d = total(a, 1);
   }
 }
 
 // alpha = d / (z, p); x += alpha p; r -= alpha z; z = M r; sum (r, z)
 __global__ void __launch_bounds__(kThreads) k_pcg_b(Args a) {
   if (!a.st->active) return;
-  const double alpha = a.st->d / a.st->glob[2];
+  const double alpha = a.st->d / total(a, 2);
   double acc[1] = {0.0};
-  ROWS_OF(a) {
-    const double pi = a.p[row];
-    a.x[row] = xadd(a.x[row], xmul(alpha, pi));
-    const double ri = xsub(a.r[row], xmul(alpha, a.q[row]));
-    const double zi = xmul(ri, a.m[row]);
-    a.r[row] = ri;
-    a.z[row] = zi;
-    acc[0] = xadd(acc[0], xmul(ri, zi));
+  PAIRS_OF(a) {
+    const int row = 2 * pr;
+    if (row + 1 < a.n) {
+      const double2 pv = ld2(a.p + row), qv = ld2(a.q + row), mv = ld2(a.m + row);
+      double2 xv = ld2(a.x + row), rv = ld2(a.r + row), zv;
+      xv.x = xadd(xv.x, xmul(alpha, pv.x));
+      xv.y = xadd(xv.y, xmul(alpha, pv.y));
+      rv.x = xsub(rv.x, xmul(alpha, qv.x));
+      rv.y = xsub(rv.y, xmul(alpha, qv.y));
+      zv.x = xmul(rv.x, mv.x);
+      zv.y = xmul(rv.y, mv.y);
+      st2(a.x + row, xv);
+      st2(a.r + row, rv);
+      st2(a.z + row, zv);
+      acc[0] = xadd(acc[0], xmul(rv.x, zv.x));
+      acc[0] = xadd(acc[0], xmul(rv.y, zv.y));
+    } else {
+      a.x[row] = xadd(a.x[row], xmul(alpha, a.p[row]));
+      const double ri = xsub(a.r[row], xmul(alpha, a.q[row]));
+      const double zi = xmul(ri, a.m[row]);
+      a.r[row] = ri;
+      a.z[row] = zi;
+      acc[0] = xadd(acc[0], xmul(ri, zi));
+    }
   }
   double tot[1];
   if (rank_sums<1>(acc, a, tot) && threadIdx.x == 0) {
@@ -258,10 +295,21 @@ __global__ void __launch_bounds__(kThreads) k_pcg_b(Args a) {
 // beta = di / d; p = z + beta p; d = di; the stopping test sqrt|d| < conv
 __global__ void __launch_bounds__(kThreads) k_pcg_c(Args a) {
   if (!a.st->active) return;
-  const double di = a.st->glob[3];
+  const double di = total(a, 3);
   const double beta = di / a.st->d;
   const unsigned j = a.st->j;
-  ROWS_OF(a) { a.p[row] = xadd(a.z[row], xmul(beta, a.p[row])); }
+  PAIRS_OF(a) {
+    const int row = 2 * pr;
+    if (row + 1 < a.n) {
+      const double2 zv = ld2(a.z + row);
+      double2 pv = ld2(a.p + row);
+      pv.x = xadd(zv.x, xmul(beta, pv.x));
+      pv.y = xadd(zv.y, xmul(beta, pv.y));
+      st2(a.p + row, pv);
+    } else {
+      a.p[row] = xadd(a.z[row], xmul(beta, a.p[row]));
+    }
+  }
   double acc[1] = {0.0}, tot[1];
   if (rank_sums<1>(acc, a, tot) && threadIdx.x == 0) {
     DState *st = a.st;
@@ -319,7 +367,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_start(Args a) {
   }
   double acc[1] = {0.0}, tot[1];
   if (rank_sums<1>(acc, a, tot) && threadIdx.x == 0)
-    a.st->conv = xmul(a.st->tol, sqrt(a.st->glob[0]));
+    a.st->conv = xmul(a.st->tol, sqrt(total(a, 0)));
 }
 
 // v = A z; sums (r, r0), (v, r0)
@@ -343,8 +391,8 @@ __global__ void __launch_bounds__(kThreads) k_bicg_a1(Args a) {
 // alpha = rr0 / (v, r0); x += alpha z; r -= alpha v; z = M r; sum (r, r)
 __global__ void __launch_bounds__(kThreads) k_bicg_b1(Args a) {
   if (!a.st->active) return;
-  const double rr0 = a.st->glob[0];
-  const double alpha = rr0 / a.st->glob[1];
+  const double rr0 = total(a, 0);
+  const double alpha = rr0 / total(a, 1);
   double acc[1] = {0.0};
   ROWS_OF(a) {
     a.x[row] = xadd(a.x[row], xmul(alpha, a.z[row]));
@@ -364,7 +412,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_b1(Args a) {
 // the test sqrt(s, s) < conv; t = A z; sums (t, r), (t, t)
 __global__ void __launch_bounds__(kThreads) k_bicg_a2(Args a) {
   if (!a.st->active) return;
-  const double d = a.st->glob[2];
+  const double d = total(a, 2);
   const bool done = sqrt(d) < a.st->conv;
   double acc[2] = {0.0, 0.0};
   if (!done) {
@@ -389,7 +437,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_a2(Args a) {
 // w = (t, r) / (t, t); x += w z; r -= w t; sums (r, r), (r, r0)
 __global__ void __launch_bounds__(kThreads) k_bicg_b2(Args a) {
   if (!a.st->active) return;
-  const double w = a.st->glob[3] / a.st->glob[4];
+  const double w = total(a, 3) / total(a, 4);
   double acc[2] = {0.0, 0.0};
   ROWS_OF(a) {
     a.x[row] = xadd(a.x[row], xmul(w, a.z[row]));
@@ -411,10 +459,10 @@ __global__ void __launch_bounds__(kThreads) k_bicg_b2(Args a) {
 __global__ void __launch_bounds__(kThreads) k_bicg_c(Args a) {
   if (!a.st->active) return;
   const DState *cs = a.st;
-  const double d = cs->glob[5];
+  const double d = total(a, 5);
   const bool done = sqrt(fabs(d)) < cs->conv;
   const double w = cs->omega;
-  const double beta = xmul(cs->glob[6] / cs->rr0, cs->alpha / w);
+  const double beta = xmul(total(a, 6) / cs->rr0, cs->alpha / w);
   if (!done) {
     ROWS_OF(a) {
       const double pi = xadd(a.r[row], xmul(beta, xsub(a.p[row], xmul(w, a.v[row]))));
@@ -450,12 +498,13 @@ __global__ void k_unpack(double *v, const int *fmap_rcv, int nrcv, const double 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrcv; i += gridDim.x * blockDim.x)
     v[fmap_rcv[i]] = rbuf[i];
 }
-// local group: ghost i of this rank = vector `which` of rank src_rank[i] at src_idx[i]
-__global__ void k_gather(double *v, const int *dst, const int *src_rank, const int *src_idx,
-                         int nrcv, const double *const *tab, const DState *st, int always) {
+// local group: every rank's ghost entries of one vector, in one launch
+// (*dst[i] = *src[i], the pairs listed once per vector)
+__global__ void k_gather(double *const *dst, const double *const *src, int count,
+                         const DState *st, int always) {
   if (!always && !st->active) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrcv; i += gridDim.x * blockDim.x)
-    v[dst[i]] = tab[src_rank[i]][src_idx[i]];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    *dst[i] = *src[i];
 }
 // local group: glob[s] of every rank = sum over the ranks in rank order of loc[s]
 __global__ void k_rank_sum(DState *const *sts, int nranks, int first, int count, int always) {
@@ -485,10 +534,19 @@ struct sfr_dist_group {
   std::vector<sfr_dist *> members;  // local: by rank
   bool wired = false;               // local: ghost sources built
   ncclComm_t comm = nullptr;
-  // local: device tables of each rank's state and vectors (x, p, z)
+  // local: device table of each rank's state; per vector (x, p, z) the
+  // ghost entries of every rank and their owners' entries
   DState **d_sts = nullptr;
-  double **d_vtab = nullptr;  // 3 * nranks
-  int *h_flag = nullptr;      // pinned
+  double **d_gdst[3] = {nullptr, nullptr, nullptr};
+  double **d_gsrc[3] = {nullptr, nullptr, nullptr};
+  int nghost = 0;
+  int *h_flag = nullptr;      // pinned, two entries (read one chunk behind)
+  // the iteration loop as a CUDA graph of kChunk iterations, per solver
+  // (0 PCG, 1 BiCGSTAB), captured for the current set of ranks (epoch)
+  cudaGraphExec_t chunk[2] = {nullptr, nullptr};
+  uint64_t chunk_epoch[2] = {0, 0};
+  uint64_t epoch = 1;
+  cudaEvent_t flag_ev[2] = {nullptr, nullptr};
 };
 
 struct sfr_dist {
@@ -505,7 +563,6 @@ struct sfr_dist {
   bool rcv_contig = false;  // fMap[i] = nEqNov + i for the received values
   int *d_fmap = nullptr;    // nrcv + nsnd
   double *d_sbuf = nullptr, *d_rbuf = nullptr;
-  int *d_gdst = nullptr, *d_grank = nullptr, *d_gidx = nullptr;  // local group
   // vectors (ncols each) and reductions
   double *d_vec = nullptr;
   double *x = nullptr, *b = nullptr, *m = nullptr, *r = nullptr, *z = nullptr, *p = nullptr,
@@ -513,7 +570,7 @@ struct sfr_dist {
   double *d_part = nullptr;
   unsigned *d_counter = nullptr;
   DState *d_st = nullptr;
-  int grid = 1;
+  int max_blocks = 1;  // a resident wave of the widest kernel
 };
 
 namespace {
@@ -537,6 +594,30 @@ int cuda_fail(cudaError_t e, const char *where) {
       return fail(std::string(#call ": ") + nccl().GetErrorString(r_), SFR_CUDA_ERROR); \
   } while (0)
 
+// One resident wave of `kernel` (its occupancy at kThreads a block), or
+// fewer blocks when the rows do not need them.  A wave keeps the last-block
+// counter at one arrival per resident block and leaves no tail.
+template <typename K>
+int wave_grid(K kernel, const sfr_dist *d) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), d->device);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+      int occ = 0, sms = 148;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, 0);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device);
+      it = cache.emplace(key, std::max(1, occ) * sms).first;
+    }
+    per_sm = it->second;
+  }
+  const int need = std::max(1, (d->n + kThreads - 1) / kThreads);
+  return std::min({per_sm, need, d->max_blocks});
+}
+
 Args args_of(const sfr_dist *d) {
   Args a;
   a.n = d->n;
@@ -552,6 +633,8 @@ Args args_of(const sfr_dist *d) {
   a.part = d->d_part;
   a.counter = d->d_counter;
   a.st = d->d_st;
+  a.sts = d->g && d->g->kind == 0 ? d->g->d_sts : nullptr;
+  a.nranks = d->g ? d->g->nranks : 1;
   return a;
 }
 
@@ -564,9 +647,6 @@ void free_dist(sfr_dist *d) {
   cudaFree(d->d_fmap);
   cudaFree(d->d_sbuf);
   cudaFree(d->d_rbuf);
-  cudaFree(d->d_gdst);
-  cudaFree(d->d_grank);
-  cudaFree(d->d_gidx);
   cudaFree(d->d_vec);
   cudaFree(d->d_part);
   cudaFree(d->d_counter);
@@ -580,9 +660,9 @@ int wire_local(sfr_dist_group *g) {
   const int R = g->nranks;
   for (int r = 0; r < R; ++r)
     if (!g->members[r]) return fail("local group: rank " + std::to_string(r) + " not created");
+  std::vector<double *> dst[3], src[3];
   for (int r = 0; r < R; ++r) {
     sfr_dist *d = g->members[r];
-    std::vector<int> dst, srank, sidx;
     for (size_t n = 0; n < d->viz.size(); ++n) {
       const int p = d->viz[n];
       const sfr_dist *o = g->members[p];
@@ -600,36 +680,36 @@ int wire_local(sfr_dist_group *g) {
                     std::to_string(slen) + " values to rank " + std::to_string(r) +
                     ", which receives " + std::to_string(len));
       for (int i = 0; i < len; ++i) {
-        dst.push_back(d->fmap[d->ia_rcv[n] + i]);
-        srank.push_back(p);
-        sidx.push_back(o->fmap[o->ia_snd[mm] + i]);
+        const int di = d->fmap[d->ia_rcv[n] + i];
+        const int si = o->fmap[o->ia_snd[mm] + i];
+        double *const dv[3] = {d->x, d->p, d->z};
+        double *const sv[3] = {o->x, o->p, o->z};
+        for (int w = 0; w < 3; ++w) {
+          dst[w].push_back(dv[w] + di);
+          src[w].push_back(sv[w] + si);
+        }
       }
     }
-    cudaFree(d->d_gdst);
-    cudaFree(d->d_grank);
-    cudaFree(d->d_gidx);
-    d->d_gdst = d->d_grank = d->d_gidx = nullptr;
-    if (!dst.empty()) {
-      const size_t bytes = dst.size() * sizeof(int);
-      CK(cudaMalloc(&d->d_gdst, bytes));
-      CK(cudaMalloc(&d->d_grank, bytes));
-      CK(cudaMalloc(&d->d_gidx, bytes));
-      CK(cudaMemcpy(d->d_gdst, dst.data(), bytes, cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(d->d_grank, srank.data(), bytes, cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(d->d_gidx, sidx.data(), bytes, cudaMemcpyHostToDevice));
+  }
+  for (int w = 0; w < 3; ++w) {
+    cudaFree(g->d_gdst[w]);
+    cudaFree(g->d_gsrc[w]);
+    g->d_gdst[w] = g->d_gsrc[w] = nullptr;
+  }
+  g->nghost = static_cast<int>(dst[0].size());
+  if (g->nghost > 0)
+    for (int w = 0; w < 3; ++w) {
+      const size_t bytes = dst[w].size() * sizeof(double *);
+      CK(cudaMalloc(&g->d_gdst[w], bytes));
+      CK(cudaMalloc(&g->d_gsrc[w], bytes));
+      CK(cudaMemcpy(g->d_gdst[w], dst[w].data(), bytes, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(g->d_gsrc[w], src[w].data(), bytes, cudaMemcpyHostToDevice));
     }
-  }
   std::vector<DState *> sts(R);
-  std::vector<double *> vt(3 * R);
-  for (int r = 0; r < R; ++r) {
-    sts[r] = g->members[r]->d_st;
-    vt[r] = g->members[r]->x;
-    vt[R + r] = g->members[r]->p;
-    vt[2 * R + r] = g->members[r]->z;
-  }
+  for (int r = 0; r < R; ++r) sts[r] = g->members[r]->d_st;
   CK(cudaMemcpy(g->d_sts, sts.data(), R * sizeof(DState *), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(g->d_vtab, vt.data(), 3 * R * sizeof(double *), cudaMemcpyHostToDevice));
   g->wired = true;
+  ++g->epoch;
   return SFR_OK;
 }
 
@@ -638,14 +718,10 @@ int exchange(sfr_dist_group *g, sfr_dist *const *parts, int nlocal, int which, b
   const int aw = always ? 1 : 0;
   cudaStream_t st = g->stream;
   if (g->kind == 0) {
-    for (int k = 0; k < nlocal; ++k) {
-      sfr_dist *d = parts[k];
-      if (d->nrcv == 0) continue;
-      double *v = which == 0 ? d->x : which == 1 ? d->p : d->z;
-      const int blocks = std::min(1184, (d->nrcv + 255) / 256);
-      k_gather<<<blocks, 256, 0, st>>>(v, d->d_gdst, d->d_grank, d->d_gidx, d->nrcv,
-                                       g->d_vtab + which * g->nranks, d->d_st, aw);
-    }
+    if (g->nghost == 0) return SFR_OK;
+    const int blocks = std::min(1184, (g->nghost + 255) / 256);
+    k_gather<<<blocks, 256, 0, st>>>(g->d_gdst[which], g->d_gsrc[which], g->nghost,
+                                     parts[0]->d_st, aw);
     CK(cudaGetLastError());
     return SFR_OK;
   }
@@ -677,9 +753,12 @@ int exchange(sfr_dist_group *g, sfr_dist *const *parts, int nlocal, int which, b
   return SFR_OK;
 }
 
-// glob[first..first+count) = the sums over the ranks of loc[...]
+// glob[first..first+count) = the sums over the ranks of loc[...].  A local
+// group's kernels sum the ranks' partials themselves; it runs the kernel only
+// for the totals the host reads (`always`).
 int rank_sum(sfr_dist_group *g, sfr_dist *const *parts, int first, int count, bool always) {
   if (g->kind == 0) {
+    if (!always) return SFR_OK;
     k_rank_sum<<<1, 32, 0, g->stream>>>(g->d_sts, g->nranks, first, count, always ? 1 : 0);
     CK(cudaGetLastError());
     return SFR_OK;
@@ -706,8 +785,9 @@ int sfr_dist_group_local(int32_t nparts, int32_t device, sfr_dist_group **out) {
   g->members.assign(nparts, nullptr);
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&g->d_sts, nparts * sizeof(DState *));
-  if (e == cudaSuccess) e = cudaMalloc(&g->d_vtab, 3 * nparts * sizeof(double *));
-  if (e == cudaSuccess) e = cudaMallocHost(&g->h_flag, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&g->h_flag, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->flag_ev[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->flag_ev[1], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     sfr_dist_group_destroy(g);
     return cuda_fail(e, "local group allocation");
@@ -742,7 +822,9 @@ int sfr_dist_group_nccl(int32_t nranks, int32_t rank, const uint8_t id[128], int
   g->rank = rank;
   g->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMallocHost(&g->h_flag, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&g->h_flag, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->flag_ev[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->flag_ev[1], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     sfr_dist_group_destroy(g);
     return cuda_fail(e, "NCCL group allocation");
@@ -767,10 +849,25 @@ int sfr_dist_group_destroy(sfr_dist_group *g) {
   for (sfr_dist *d : g->members)
     if (d) d->g = nullptr;
   cudaFree(g->d_sts);
-  cudaFree(g->d_vtab);
+  for (int w = 0; w < 3; ++w) {
+    cudaFree(g->d_gdst[w]);
+    cudaFree(g->d_gsrc[w]);
+  }
   if (g->h_flag) cudaFreeHost(g->h_flag);
+  for (int k = 0; k < 2; ++k) {
+    if (g->chunk[k]) cudaGraphExecDestroy(g->chunk[k]);
+    if (g->flag_ev[k]) cudaEventDestroy(g->flag_ev[k]);
+  }
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
+  return SFR_OK;
+}
+
+int sfr_dist_group_info(const sfr_dist_group *g, int32_t *kind, int32_t *nranks, int32_t *rank) {
+  if (!g) return fail("group is NULL");
+  if (kind) *kind = g->kind;
+  if (nranks) *nranks = g->nranks;
+  if (rank) *rank = g->rank;
   return SFR_OK;
 }
 
@@ -938,11 +1035,16 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
   d->ia_snd = ias;
   d->fmap = fmap;
   d->rcv_contig = contig;
-  d->grid = std::max(1, std::min((nEqNov + kThreads - 1) / kThreads, 148 * 8));
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    d->max_blocks = sms * (2048 / kThreads);
+  }
   int64_t bytes = 0;
   int rc = sfr::upload_sell(h, &d->A, &bytes);
   cudaError_t e = rc == SFR_OK ? cudaSuccess : cudaErrorMemoryAllocation;
-  const size_t nv = static_cast<size_t>(ncols) + 1;
+  // vectors padded to an even length: each starts 16-byte aligned
+  const size_t nv = (static_cast<size_t>(ncols) + 2) & ~static_cast<size_t>(1);
   if (e == cudaSuccess) e = cudaMalloc(&d->A.val, std::max<int64_t>(total, 1) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&d->d_raw, std::max(d->nsrc, 1) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&d->d_ad, nEqNov * sizeof(double));
@@ -955,7 +1057,7 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
   if (e == cudaSuccess) e = cudaMalloc(&d->d_rbuf, std::max(nrcv, 1) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&d->d_vec, 10 * nv * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(d->d_vec, 0, 10 * nv * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d->d_part, static_cast<size_t>(d->grid) * kSlots * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d->d_part, static_cast<size_t>(d->max_blocks) * kSlots * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&d->d_counter, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(d->d_counter, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc(&d->d_st, sizeof(DState));
@@ -975,6 +1077,7 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
   } else {
     g->members.assign(1, d);
   }
+  ++g->epoch;
   *out = d;
   return SFR_OK;
 }
@@ -1050,7 +1153,7 @@ int sfr_gpu_dist_solve(sfr_dist_group *g, int32_t nlocal, sfr_dist *const *parts
   int rc = SFR_OK;
   auto launch = [&](auto kernel, auto... extra) -> int {
     for (int k = 0; k < nlocal; ++k)
-      kernel<<<parts[k]->grid, kThreads, 0, st>>>(args_of(parts[k]), extra...);
+      kernel<<<wave_grid(kernel, parts[k]), kThreads, 0, st>>>(args_of(parts[k]), extra...);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SFR_OK : cuda_fail(e, "kernel launch");
   };
@@ -1063,53 +1166,80 @@ int sfr_gpu_dist_solve(sfr_dist_group *g, int32_t nlocal, sfr_dist *const *parts
     } else {
       if ((r = launch(k_bicg_setup, newX ? 1 : 0)) != SFR_OK) return r;
     }
-    if ((r = rank_sum(g, parts, 0, 1, true)) != SFR_OK) return r;
+    if ((r = rank_sum(g, parts, 0, 1, false)) != SFR_OK) return r;
     if (!newX && (r = exchange(g, parts, nlocal, 0, true)) != SFR_OK) return r;
     if (pcg) {
       if ((r = launch(k_pcg_start)) != SFR_OK) return r;
-      if ((r = rank_sum(g, parts, 1, 1, true)) != SFR_OK) return r;
+      if ((r = rank_sum(g, parts, 1, 1, false)) != SFR_OK) return r;
     } else if ((r = launch(k_bicg_start)) != SFR_OK) {
       return r;
     }
-    // iterations, in chunks between reads of the stop flag
-    uint64_t issued = 0;
-    int chunk = 4;
-    DState *s0 = parts[0]->d_st;
-    while (issued < maxIt) {
-      const int nrun = static_cast<int>(std::min<uint64_t>(chunk, maxIt - issued));
-      for (int it = 0; it < nrun; ++it) {
-        if (pcg) {
-          if ((r = exchange(g, parts, nlocal, 1, false)) != SFR_OK) return r;
-          if ((r = launch(k_pcg_a)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 2, 1, false)) != SFR_OK) return r;
-          if ((r = launch(k_pcg_b)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 3, 1, false)) != SFR_OK) return r;
-          if ((r = launch(k_pcg_c)) != SFR_OK) return r;
-        } else {
-          if ((r = exchange(g, parts, nlocal, 2, false)) != SFR_OK) return r;
-          if ((r = launch(k_bicg_a1)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 0, 2, false)) != SFR_OK) return r;
-          if ((r = launch(k_bicg_b1)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 2, 1, false)) != SFR_OK) return r;
-          if ((r = exchange(g, parts, nlocal, 2, false)) != SFR_OK) return r;
-          if ((r = launch(k_bicg_a2)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 3, 2, false)) != SFR_OK) return r;
-          if ((r = launch(k_bicg_b2)) != SFR_OK) return r;
-          if ((r = rank_sum(g, parts, 5, 2, false)) != SFR_OK) return r;
-          if ((r = launch(k_bicg_c)) != SFR_OK) return r;
-        }
+    // one iteration's launches (Cg.c:322-366, Bicgstab.c:350-437)
+    auto iteration = [&]() -> int {
+      int q;
+      if (pcg) {
+        if ((q = exchange(g, parts, nlocal, 1, false)) != SFR_OK) return q;
+        if ((q = launch(k_pcg_a)) != SFR_OK) return q;
+        if ((q = rank_sum(g, parts, 2, 1, false)) != SFR_OK) return q;
+        if ((q = launch(k_pcg_b)) != SFR_OK) return q;
+        if ((q = rank_sum(g, parts, 3, 1, false)) != SFR_OK) return q;
+        return launch(k_pcg_c);
       }
-      issued += nrun;
-      // the stop flag, agreed over the ranks
+      if ((q = exchange(g, parts, nlocal, 2, false)) != SFR_OK) return q;
+      if ((q = launch(k_bicg_a1)) != SFR_OK) return q;
+      if ((q = rank_sum(g, parts, 0, 2, false)) != SFR_OK) return q;
+      if ((q = launch(k_bicg_b1)) != SFR_OK) return q;
+      if ((q = rank_sum(g, parts, 2, 1, false)) != SFR_OK) return q;
+      if ((q = exchange(g, parts, nlocal, 2, false)) != SFR_OK) return q;
+      if ((q = launch(k_bicg_a2)) != SFR_OK) return q;
+      if ((q = rank_sum(g, parts, 3, 2, false)) != SFR_OK) return q;
+      if ((q = launch(k_bicg_b2)) != SFR_OK) return q;
+      if ((q = rank_sum(g, parts, 5, 2, false)) != SFR_OK) return q;
+      return launch(k_bicg_c);
+    };
+    // the loop: a graph of kChunk iterations (captured once for this set of
+    // ranks), replayed until the ranks agree that the solve stopped; the
+    // kernels stop by themselves at maxIt, so a replay past the end is idle
+    const int which = pcg ? 0 : 1;
+    if (!g->chunk[which] || g->chunk_epoch[which] != g->epoch) {
+      if (g->chunk[which]) cudaGraphExecDestroy(g->chunk[which]);
+      g->chunk[which] = nullptr;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int q = SFR_OK;
+      for (int it = 0; it < kChunk && q == SFR_OK; ++it) q = iteration();
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+      if (q != SFR_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return q;
+      }
+      CK(ec);
+      const cudaError_t ei = cudaGraphInstantiate(&g->chunk[which], graph, 0);
+      cudaGraphDestroy(graph);
+      CK(ei);
+      g->chunk_epoch[which] = g->epoch;
+    }
+    DState *s0 = parts[0]->d_st;
+    const uint64_t nchunks = (static_cast<uint64_t>(maxIt) + kChunk - 1) / kChunk;
+    int prev = -1;
+    for (uint64_t c = 0; c < nchunks; ++c) {
+      const int slot = static_cast<int>(c & 1);
+      CK(cudaGraphLaunch(g->chunk[which], st));
+      // the stop flag, agreed over the ranks, read one chunk behind
       if (g->kind == 1 && g->nranks > 1) {
         NK(nccl().AllReduce(&s0->active, &s0->active_all, 1, ncclInt32, ncclMax, g->comm, st));
-        CK(cudaMemcpyAsync(g->h_flag, &s0->active_all, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(g->h_flag + slot, &s0->active_all, sizeof(int),
+                           cudaMemcpyDeviceToHost, st));
       } else {
-        CK(cudaMemcpyAsync(g->h_flag, &s0->active, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(g->h_flag + slot, &s0->active, sizeof(int), cudaMemcpyDeviceToHost,
+                           st));
       }
-      CK(cudaStreamSynchronize(st));
-      if (*g->h_flag == 0) break;
-      chunk = std::min(chunk * 2, 64);
+      CK(cudaEventRecord(g->flag_ev[slot], st));
+      if (prev >= 0) {
+        CK(cudaEventSynchronize(g->flag_ev[prev]));
+        if (g->h_flag[prev] == 0) break;
+      }
+      prev = slot;
     }
     // post-processing (Cg.c:376-396, Bicgstab.c:440-455)
     if ((r = exchange(g, parts, nlocal, 0, true)) != SFR_OK) return r;
@@ -1161,6 +1291,7 @@ int sfr_gpu_dist_destroy(sfr_dist *d) {
     } else {
       d->g->members.clear();
     }
+    ++d->g->epoch;
   }
   free_dist(d);
   delete d;

@@ -51,6 +51,7 @@ def _lib() -> ctypes.CDLL:
     L.sfr_dist_nccl_id.argtypes = [_P]
     L.sfr_dist_group_nccl.argtypes = [_I32, _I32, _P, _I32, ctypes.POINTER(_P)]
     L.sfr_dist_group_destroy.argtypes = [_P]
+    L.sfr_dist_group_info.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_dist_create.argtypes = [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32,
                                       ctypes.POINTER(InterfaceC), ctypes.POINTER(_P)]
     L.sfr_gpu_dist_set_values.argtypes = [_P, _P, _P]
@@ -307,6 +308,14 @@ class DistSystem:
             self.close()
         except Exception:
             pass
+
+
+def set_solverC_group(group: "NcclGroup | None") -> None:
+    """Route sfr_solverC through the MPI branch on this NCCL group (None:
+    back to the single-GPU path)."""
+    rc = _lib().sfr_solverC_set_group(None if group is None else group._h)
+    if rc != 0:
+        raise _sv.SolverError(rc, "sfr_solverC_set_group")
 
 
 def solve(group: _Group, systems: list[DistSystem], solver: int, b, x0=None, tol=1e-10,

@@ -117,6 +117,7 @@ def lib() -> ctypes.CDLL:
     L.sfr_write_coo_b.argtypes = [ctypes.c_char_p, _P, _I32]
     L.sfr_gpu_write_coo.argtypes = [_P, ctypes.c_char_p, _P, _P, _I32]
     L.sfr_set_precision.restype = None
+    L.sfr_solverC_set_group.argtypes = [_P]
     L.sfr_solverC_release.restype = None
     L.sfr_solverC_release.argtypes = []
     L._typed = True
@@ -430,7 +431,7 @@ def dot(d_a: int, d_b: int, n: int, stream: int = 0) -> float:
 
 def solverC(nEq, nEqNov, nAd, nAdR, ia, ja, al, ad, au, b, x, tol, maxIt,
             storage, solver, fSolvLog=None, fLog=False, newX=True,
-            unSym=False, name="system", exit_on_failure=False) -> int:
+            unSym=False, name="system", exit_on_failure=False, iNeq=None) -> int:
     """The reference's solverC (Solv.c:64) through sfr_solverC: x is updated
     in place, b is left unchanged.  fSolvLog is a C FILE* (integer) or None.
     Returns the status (the reference returns nothing and exits on failure;
@@ -441,8 +442,9 @@ def solverC(nEq, nEqNov, nAd, nAdR, ia, ja, al, ad, au, b, x, tol, maxIt,
     al, ad, au, b = _f64(al), _f64(ad), _f64(au), _f64(b)
     if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
         raise TypeError("x must be a C-contiguous float64 array (updated in place)")
+    ineq = None if iNeq is None else ctypes.cast(ctypes.pointer(iNeq), _P)
     return L.sfr_solverC(None, nEq, nEqNov, nAd, nAdR, _ptr(ia), _ptr(ja),
-                         _ptr(al), _ptr(ad), _ptr(au), _ptr(b), _ptr(x), None,
+                         _ptr(al), _ptr(ad), _ptr(au), _ptr(b), _ptr(x), ineq,
                          None, tol, maxIt, storage, solver, fSolvLog,
                          bool(fLog), bool(newX), bool(unSym), name.encode())
 

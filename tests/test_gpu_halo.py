@@ -144,3 +144,55 @@ def test_interface_mismatch_is_an_error_before_any_solve():
     with pytest.raises(SV.SolverError, match="interface mismatch"):
         H.solve(g, systems, O.PCG, [la.rows(s.b[0]) for la in lays], tol=1e-10)
     g.close()
+
+
+def _fopen(path):
+    import ctypes
+    libc = ctypes.CDLL(None)
+    libc.fopen.restype = ctypes.c_void_p
+    libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    libc.fclose.argtypes = [ctypes.c_void_p]
+    return libc, libc.fopen(path.encode(), b"w")
+
+
+@pytest.mark.parametrize("solver,head", [(O.PCG, "MPIPCG: tol"), (O.PBICGSTAB, "MPIPBICGSTAB: tol")])
+def test_solverC_mpi_branch_on_an_nccl_group(tmp_path, solver, head):
+    """solverC with nPrcs > 1 calls mpiPcg / mpiPbicgstab (Solv.c:952-977,
+    1070-1093): the drop-in's MPI branch on a one-rank NCCL group, with the
+    reference's Interface passed as iNeq and the symmetric MPI CSRD."""
+    # PCG on a pressure system (symmetric MPI CSRD), BiCGSTAB on a momentum
+    # system (unsymmetric); BiCGSTAB on a symmetric system moves by a few
+    # iterations with the summation order alone
+    unsym = solver == O.PBICGSTAB
+    s = S.momentum(14, peclet=50.0, nrhs=1) if unsym else S.poisson_jittered(14, seed=8)
+    il, jl, al = (s.ia, s.ja, s.al) if unsym else s.csrd_lower()
+    lay = H.partition(s.neq, il, jl, unsym, 1)[0]
+    a, d = lay.values(al, s.ad)
+    b = lay.rows(s.b[0])
+    _, ref = O.mpi_solve(solver, [lay], [a], [d], [b], tol=1e-10)
+    g = H.NcclGroup(1, 0, H.nccl_unique_id(), 0)
+    with pytest.raises(SV.SolverError):
+        H.set_solverC_group(H.LocalGroup(1, 0))
+    H.set_solverC_group(g)
+    try:
+        libc, f = _fopen(str(tmp_path / "solv.log"))
+        x = np.zeros(lay.nEq)
+        iface = lay.interface()
+        rc = SV.solverC(lay.nEq, lay.nEqNov, lay.nAd, lay.nAdR, lay.ia, lay.ja, a, d, None, b,
+                        x, 1e-10, 100000, SV.CSRD, solver, fSolvLog=f, fLog=True, newX=True,
+                        unSym=unsym, name="pres", iNeq=iface)
+        libc.fclose(f)
+        assert rc == 0
+        line = open(tmp_path / "solv.log").read()
+        assert line.startswith(head)
+        assert abs(int(line.split("iteration")[1].split()[0]) - ref.iters) <= 1
+        assert _rel(x[:lay.nEqNov], ref.x) < 1e-12
+        # a storage the MPI branch lacks is the reference's invalid option
+        rc = SV.solverC(lay.nEq, lay.nEqNov, lay.nAd, lay.nAdR, lay.ia, lay.ja, a, d, None, b,
+                        x, 1e-10, 100000, SV.CSRC, solver, newX=True, unSym=unsym,
+                        iNeq=iface)
+        assert rc == SV.UNSUPPORTED
+    finally:
+        H.set_solverC_group(None)
+        SV.release_cache()
+        g.close()
