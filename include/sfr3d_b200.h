@@ -384,7 +384,9 @@ typedef struct {
   int32_t fvisc;       /* MomentumModel.fViscosity: explicit viscous part */
   int32_t fres;        /* MomentumModel.fRes */
   int32_t type_simple; /* 1 SIMPLE, 2 SIMPLEC */
-  int32_t time_flag, time_type, pad;
+  int32_t time_flag, time_type;
+  int32_t adv;         /* Advection.iCod1 (advectiveScheme, CellLib.c:6394-6480): 0 or 1
+                          FoUp, 2 CD (deferred central), 3 SoUp (linear upwind) */
   double dt, dt0;
   double under;        /* under-relaxation of the velocity (alphaVel) */
 } sfr_vel_opts;

@@ -561,6 +561,7 @@ def ref_pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
 # ------------------------------------------------------ momentum assembly --
 # systFormSimpleVel (CellLoopInc.c:98-470) -> cellSimpleVel3D (CellSimple.c:106)
 SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
+FOUP, CD, SOUP = 1, 2, 3  # advection schemes, Define.h:267-269
 
 
 @dataclass
@@ -593,6 +594,7 @@ class VelCase:
     under: float = 0.7
     mat: np.ndarray | None = None
     caltype: np.ndarray | None = None
+    adv: int = FOUP
 
     def material(self):
         mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
@@ -606,6 +608,7 @@ class _VelOpts(ctypes.Structure):
     _fields_ = [("icod", ctypes.c_int), ("fso", ctypes.c_int), ("fvisc", ctypes.c_int),
                 ("fres", ctypes.c_int), ("type_simple", ctypes.c_int),
                 ("time_flag", ctypes.c_int), ("time_type", ctypes.c_int),
+                ("adv", ctypes.c_int),
                 ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double)]
 
 
@@ -638,8 +641,8 @@ def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix
                   **{k: _p(v) for k, v in keep.items()})
     o = _VelOpts(icod=case.icod, fso=int(case.fso), fvisc=int(case.fvisc),
                  fres=int(case.fres), type_simple=case.type_simple,
-                 time_flag=int(case.time_flag), time_type=case.time_type, dt=case.dt,
-                 dt0=case.dt0, under=case.under)
+                 time_flag=int(case.time_flag), time_type=case.time_type, adv=case.adv,
+                 dt=case.dt, dt0=case.dt0, under=case.under)
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
     a, ad, b, rc_ = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
     dfield = np.array(case.dfield, dtype=np.float64, copy=True, order="C")
@@ -666,7 +669,7 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         lib.sfr_ref_syst_form_simple_vel.restype = ctypes.c_int
         lib.sfr_ref_syst_form_simple_vel.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
-            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 8 + [_P])
+            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 9 + [_P])
         lib._vel_typed = True
     cal, mat = case.material()
     cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
@@ -691,5 +694,5 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         *[_p(x) for x in vt], case.icod, int(case.fso), int(case.fvisc), int(case.fres),
         case.type_simple, int(case.time_flag), case.time_type, case.dt, case.dt0, case.under,
         neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym), nthreads,
-        ctypes.byref(sec))
+        case.adv, ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value

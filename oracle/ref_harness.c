@@ -389,7 +389,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int type_simple, int time_flag, int time_type, double dt,
                                  double dt0, double under, int neq, int nad, int storage,
                                  int forces, int matrix, int calrcell, int unsym,
-                                 int nthreads, double *seconds)
+                                 int nthreads, int advcod, double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -420,7 +420,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   memset(&tmodel, 0, sizeof(tmodel));
   memset(&mm, 0, sizeof(mm));
   memset(&ddt, 0, sizeof(ddt));
-  adv.iCod1 = FOUP;
+  adv.iCod1 = (short)(advcod > 0 ? advcod : FOUP);
   diff.iCod = (short)icod;
   mm.fRes = fres != 0;
   mm.fRhieChowInt = false;

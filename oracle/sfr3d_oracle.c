@@ -1021,6 +1021,7 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
   if (mv < 1 || mv > MAXF - 1 || storage == ORC_ELLPACK) return -1;
   /* any other typeSimple leaves D as the first neighbour's copy */
   if (o->type_simple != 1 && o->type_simple != 2) return -1;
+  if (o->adv < 0 || o->adv > 3) return -1; /* TVD, NVD and LUST not restated */
   for (nel = 0; nel < numel; nel++) {
     double lA[MAXF + 3], ksi[3], nrm[3], s[3], e[3], t[3];
     double p[3] = {0.0, 0.0, 0.0}, pf[3] = {0.0, 0.0, 0.0}, sPc[3] = {0.0, 0.0, 0.0};
@@ -1101,7 +1102,23 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
         cv = density * wfn * area;
         lA[f] = dfd - (cv < 0.0e0 ? cv : 0.0e0);
         sP += cv;
-        for (i = 0; i < 3; i++) p[i] += dfdc[i] - cv * 0.e0; /* FoUp: cvc = 0 */
+        /* advectiveScheme (CellLib.c:6394-6480), cv in the place of wfn */
+        {
+          double cvc[3] = {0.e0, 0.e0, 0.e0}, rV[3];
+          for (j = 0; j < 3; j++) rV[j] = lXm[j] - ccV[j];
+          for (i = 0; i < 3; i++) {
+            if (o->adv == 2) { /* deferredCd, CellLib.c:5113-5127 */
+              const double cd = am1 * velC[i] + alpha * velV[i];
+              cvc[i] = cd - (cv < 0.e0 ? velV[i] : velC[i]);
+            } else if (o->adv == 3) { /* upwindLinearV1, CellLib.c:5072-5090 */
+              if (cv < 0.e0)
+                cvc[i] = gvV[i][0] * rV[0] + gvV[i][1] * rV[1] + gvV[i][2] * rV[2];
+              else
+                cvc[i] = gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1] + gvC[i][2] * xmcc[2];
+            }
+          }
+          for (i = 0; i < 3; i++) p[i] += dfdc[i] - cv * cvc[i];
+        }
         /* facePressure (CellLib.c:7499), interior */
         if (o->fso) {
           for (j = 0; j < 3; j++) v[j] = lXm[j] - ccV[j];

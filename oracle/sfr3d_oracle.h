@@ -141,8 +141,8 @@ int orc_pres_assemble(const orc_dif_mesh *m, const short *facevelr,
                       double *rcell, int forces, int matrix, int calrcell);
 
 /* ---- momentum assembly (systFormSimpleVel, CellLoopInc.c:98-470 ->
- *      cellSimpleVel3D, CellSimple.c:106-727), laminar, first-order upwind,
- *      no Rhie-Chow face velocity, no wall model ----------------------- */
+ *      cellSimpleVel3D, CellSimple.c:106-727), laminar, advection FoUp, CD
+ *      or SoUp, no Rhie-Chow face velocity, no wall model -------------- */
 typedef struct {
   int icod;          /* Diffusion.iCod (difusionSchemeNew) */
   int fso;           /* MomentumModel.fSoPressure: second-order face pressure */
@@ -150,6 +150,8 @@ typedef struct {
   int fres;          /* MomentumModel.fRes */
   int type_simple;   /* 1 SIMPLE, 2 SIMPLEC (Define.h:223-224) */
   int time_flag, time_type;
+  int adv;           /* Advection.iCod1: 0 or 1 FoUp, 2 CD, 3 SoUp
+                        (advectiveScheme, CellLib.c:6394-6480) */
   double dt, dt0;
   double under;      /* underU (alphaVel) */
 } orc_vel_opts;

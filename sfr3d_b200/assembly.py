@@ -41,7 +41,7 @@ class DifMeshC(ctypes.Structure):
 class VelOptsC(ctypes.Structure):
     _fields_ = [("icod", _I32), ("fso", _I32), ("fvisc", _I32), ("fres", _I32),
                 ("type_simple", _I32), ("time_flag", _I32), ("time_type", _I32),
-                ("pad", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
+                ("adv", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
                 ("under", ctypes.c_double)]
 
 
@@ -291,12 +291,13 @@ class PresPlan(DifPlan):
 
 
 SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
+FOUP, CD, SOUP = 1, 2, 3  # advection schemes (Advection.iCod1), Define.h:267-269
 
 
 class VelPlan(DifPlan):
     """A mesh bound to a resident system for device-side systFormSimpleVel
     (the SIMPLE momentum system: u, v, w share the off-diagonals), laminar,
-    first-order upwind, without Rhie-Chow.  facevelr is faceVelR; cc the
+    advection FoUp, CD or SoUp, without Rhie-Chow.  facevelr is faceVelR; cc the
     cell centroids (numel, 3); the mesh must carry face centres (xm)."""
 
     def __init__(self, system: "_sv.GpuSystem", mesh, facevelr, cc, icod: int = ORTHOGONAL,
@@ -313,9 +314,9 @@ class VelPlan(DifPlan):
             raise _sv.SolverError(rc, "sfr_gpu_vel_plan_create: " + _sv.last_error())
         self.h = h
 
-    def _vopts(self, fso, fvisc, fres, type_simple, time, under):
+    def _vopts(self, fso, fvisc, fres, type_simple, time, under, adv=1):
         o = VelOptsC(icod=self.icod, fso=int(fso), fvisc=int(fvisc), fres=int(fres),
-                     type_simple=type_simple, under=under)
+                     type_simple=type_simple, under=under, adv=int(adv))
         if time is not None:
             o.time_flag = 1
             o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
@@ -323,9 +324,9 @@ class VelPlan(DifPlan):
 
     def assemble(self, lvel, prop, pres, gradpres, vel, gradvel, dfield, fso=True,
                  fvisc=False, fres=True, type_simple=SIMPLE, time=None, under=0.7,
-                 forces=True, matrix=True, calrcell=True):
+                 forces=True, matrix=True, calrcell=True, adv=FOUP):
         """One call with host arrays: returns (ad3, b3, rcell3, dfield), each
-        component block after the other (u, v, w)."""
+        component block after the other (u, v, w).  adv: FOUP, CD or SOUP."""
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         arrs = [_c(a, np.float64) for a in (pres, gradpres, vel, gradvel)]
         df = np.array(dfield, dtype=np.float64, copy=True, order="C")
@@ -333,7 +334,7 @@ class VelPlan(DifPlan):
         b3 = np.empty(3 * self.neq) if forces else None
         rc3 = np.empty(3 * self.numel) if calrcell else None
         lv = _loads_c(lvel)
-        o = self._vopts(fso, fvisc, fres, type_simple, time, under)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv)
         rc = _lib().sfr_gpu_vel_assemble(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), *[_ptr(a) for a in arrs],
             _ptr(df), _ptr(ad3), _ptr(b3), _ptr(rc3), int(forces), int(matrix), int(calrcell))
@@ -347,10 +348,10 @@ class VelPlan(DifPlan):
                         d_gradvel: int, d_dfield: int, d_ad3: int = 0, d_b3: int = 0,
                         d_rcell3: int = 0, fso=True, fvisc=False, fres=True,
                         type_simple=SIMPLE, time=None, under=0.7, forces=True, matrix=True,
-                        calrcell=True, stream: int = 0):
+                        calrcell=True, stream: int = 0, adv=FOUP):
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         lv = _loads_c(lvel)
-        o = self._vopts(fso, fvisc, fres, type_simple, time, under)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv)
         rc = _lib().sfr_gpu_vel_assemble_device(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), d_pres, d_gradpres, d_vel,
             d_gradvel, d_dfield, d_ad3 or None, d_b3 or None, d_rcell3 or None, int(forces),

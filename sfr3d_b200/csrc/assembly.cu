@@ -674,6 +674,7 @@ __global__ void __launch_bounds__(256, 2)
 struct VelOpts {
   int fso, fvisc, fres, simplec, time_flag, time_type, forces, matrix, calrcell;
   double dt, dt0, under;
+  int adv;  // 1 FoUp, 2 CD, 3 SoUp
 };
 
 // moveWall, not Dirichlet (CellLib.c:7715-7770)
@@ -763,7 +764,24 @@ __global__ void __launch_bounds__(256, 2)
       const double cv = xmul(xmul(density, wfn), area);
       la[f] = xsub(dfd, cv < 0.0 ? cv : 0.0);
       sP = xadd(sP, cv);
-      const double cvz = xmul(cv, 0.0);  // FoUp: no deferred correction, cvc = 0
+      // advectiveScheme (CellLib.c:6394-6480) with cv in the place of wfn:
+      // FoUp cvc = 0; CD deferredCd (CellLib.c:5113); SoUp upwindLinearV1
+      // (CellLib.c:5072) from the upwind cell's gradient, r = xm - cc
+      double cvc[3] = {0.0, 0.0, 0.0};
+      if (o.adv == 2) {
+        for (int i = 0; i < 3; ++i)
+          cvc[i] = xsub(xadd(xmul(am1, velC[i]), xmul(alpha, velV[i])),
+                        cv < 0.0 ? velV[i] : velC[i]);
+      } else if (o.adv == 3) {
+        double rr[3];
+        const bool down = cv < 0.0;
+        for (int j = 0; j < 3; ++j) rr[j] = __ldcs(g + ((down ? 16 : 13) + j) * fs);
+        for (int i = 0; i < 3; ++i) {
+          double gu[3];
+          for (int j = 0; j < 3; ++j) gu[j] = down ? gradvel[v9 + 3 * i + j] : gvC[3 * i + j];
+          cvc[i] = dot3(gu, rr);
+        }
+      }
       double gvc[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -773,7 +791,7 @@ __global__ void __launch_bounds__(256, 2)
         const double du = xsub(xdiv(xsub(velV[i], velC[i]), mk), dot3(gf, ksi));
         for (int j = 0; j < 3; ++j) gvc[3 * i + j] = xadd(gf[j], xmul(du, ksi[j]));
         const double dfdc = xmul(visc, dot3(gvc + 3 * i, t));
-        pp[i] = xadd(pp[i], xsub(dfdc, cvz));  // p += dfdc - cv cvc
+        pp[i] = xadd(pp[i], xsub(dfdc, xmul(cv, cvc[i])));  // p += dfdc - cv cvc
       }
       // facePressure (CellLib.c:7499), interior
       double pFace;
@@ -1488,9 +1506,11 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if (rc != SFR_OK) return rc;
   if (calrcell && p->free_cells > 0)
     SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
+  if (o->adv < 0 || o->adv > 3)
+    return bad("adv: FoUp (0 or 1), CD (2) or SoUp (3); TVD, NVD and LUST are not built");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
-                  o->dt, o->dt0, o->under};
+                  o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =

@@ -224,6 +224,44 @@ def test_vel_oracle_matches_reference_live():
             assert bits_equal(x, y)
 
 
+def test_vel_oracle_advection_schemes_match_reference_live():
+    """CD and SoUp (advectiveScheme, CellLib.c:6394-6480): the deferred
+    correction p -= cv cvc, on every layout, against the reference's own
+    systFormSimpleVel."""
+    s = S.poisson_jittered(5, seed=6)
+    m = s.mesh()
+    rng = np.random.default_rng(7)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+            O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1))]
+    for adv, icod, fso, ts in itertools.product((O.CD, O.SOUP), (1, 4), (0, 1),
+                                                (O.SIMPLE, O.SIMPLEC)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)),
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=icod, fso=bool(fso),
+                         type_simple=ts, under=0.7, adv=adv)
+        for name, (st, un, ia, ja, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (adv, icod, fso, ts, name)
+        # the schemes change b (the deferred correction), not the matrix
+        f = O.vel_assemble(O.VelCase(**{**case.__dict__, "adv": O.FOUP}), O.CSRD, True,
+                           s.ia, s.ja, s.neq)
+        c = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+        assert bits_equal(f[1], c[1]) and not np.array_equal(f[3], c[3])
+
+
 def test_vel_oracle_rejects_what_it_does_not_restate():
     s = S.poisson_uniform(4, seed=1)
     m = s.mesh()
@@ -239,5 +277,6 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     assert run(lvel=[O.Load(O.OUTLET, ())]) == -2
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
     assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
+    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4) == -1  # TVD not restated
     assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
                           O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1

@@ -504,6 +504,44 @@ def test_vel_matches_oracle(cuda, box, icod):
         gs.close()
 
 
+@pytest.mark.parametrize("adv", [O.CD, O.SOUP])
+def test_vel_advection_schemes_match_oracle(cuda, box, adv):
+    s, m, lay = box
+    rng = np.random.default_rng(60 + adv)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    cc = _centres(m)
+    fv = m.face_r([1, 1, 2, 1, 3, 1])
+    for name in ("csrd_full", "csrc_unsym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.VelPlan(gs, m, fv, cc, icod=4)
+        for fso, ts in itertools.product((0, 1), (A.SIMPLE, A.SIMPLEC)):
+            case = O.VelCase(mesh=m, cc=cc, facevelr=fv, facepresr=m.face_r([0] * 6),
+                             lvel=VLOADS, prop=prop, pres=rng.standard_normal(m.numel),
+                             gradpres=rng.standard_normal((m.numel, 3)),
+                             vel=rng.standard_normal((m.numel, 3)),
+                             gradvel=rng.standard_normal((m.numel, 3, 3)),
+                             dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, fso=bool(fso),
+                             type_simple=ts, under=0.7, adv=adv)
+            want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
+            assert want[0] == 0
+            ad3, b3, rc3, df = plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres,
+                                             case.vel, case.gradvel, case.dfield, fso=fso,
+                                             type_simple=ts, under=0.7, adv=adv)
+            al, ad, au = A.get_values(gs)
+            a = al if au is None else np.concatenate([al, au])
+            what = (name, adv, fso, ts)
+            assert bits_equal(a, want[1]), what
+            assert bits_equal(ad3, want[2]) and bits_equal(b3, want[3]), what
+            assert bits_equal(rc3, want[4]) and bits_equal(df, want[5]), what
+        with pytest.raises(sv.SolverError):
+            plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres, case.vel,
+                          case.gradvel, case.dfield, adv=4)
+        plan.close()
+        gs.close()
+
+
 def test_vel_assembled_momentum_solves_like_reference(cuda):
     """A lid-driven cavity's momentum system assembled and solved (u, v, w
     with their own diagonals) on the device."""
