@@ -389,10 +389,24 @@ typedef struct {
                           FoUp, 2 CD (deferred central), 3 SoUp (linear upwind) */
   double dt, dt0;
   double under;        /* under-relaxation of the velocity (alphaVel) */
+  int32_t fturb;       /* Turbulence.fTurb: effective viscosity mu + eddy viscosity
+                          (fields bound by sfr_gpu_vel_turbulence) */
+  int32_t fstruc;      /* Turbulence.fTurbStruct: the residual stress tensor's face
+                          integral (turbStructIntegral, CellLib.c:7586) */
 } sfr_vel_opts;
 
 int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
                             sfr_dif_plan **out);
+
+/* The turbulence fields later momentum calls read (CellSimple.c:207-314,
+ * 237-240): eddy[numel] eddy viscosity and stress[numel*6] the residual
+ * stress tensor (xx, yy, zz, xy, yz, xz), either may be NULL.  on_device = 1:
+ * device arrays, kept by pointer and read by every later call; 0: host
+ * arrays, copied now into the plan.  The wall model (Turbulence.fWall) is not
+ * built: walls use the effective viscosity, as the reference does without
+ * it (Loads.c:300-313). */
+int sfr_gpu_vel_turbulence(sfr_dif_plan *p, const double *eddy, const double *stress,
+                           int32_t on_device);
 
 /* One call on device arrays: pres (numel), gradpres, vel, dfield (numel*3),
  * gradvel (numel*9, row i = grad u_i) in; dfield (the new D), ad3 and b3

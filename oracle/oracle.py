@@ -595,6 +595,8 @@ class VelCase:
     mat: np.ndarray | None = None
     caltype: np.ndarray | None = None
     adv: int = FOUP
+    eddy: np.ndarray | None = None     # (numel,) eddy viscosity: Turbulence.fTurb
+    stress: np.ndarray | None = None   # (numel, 6) residual stress: fTurbStruct
 
     def material(self):
         mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
@@ -609,7 +611,8 @@ class _VelOpts(ctypes.Structure):
                 ("fres", ctypes.c_int), ("type_simple", ctypes.c_int),
                 ("time_flag", ctypes.c_int), ("time_type", ctypes.c_int),
                 ("adv", ctypes.c_int),
-                ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double)]
+                ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double),
+                ("fturb", ctypes.c_int), ("fstruc", ctypes.c_int), ("eddy", _P), ("stress", _P)]
 
 
 def _vel_out(storage, unsym, neq, ia, ja, numel, fill):
@@ -643,6 +646,9 @@ def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix
                  fres=int(case.fres), type_simple=case.type_simple,
                  time_flag=int(case.time_flag), time_type=case.time_type, adv=case.adv,
                  dt=case.dt, dt0=case.dt0, under=case.under)
+    turb = [None if a is None else _c(a, np.float64) for a in (case.eddy, case.stress)]
+    o.fturb, o.fstruc = int(turb[0] is not None), int(turb[1] is not None)
+    o.eddy, o.stress = [None if a is None else _p(a) for a in turb]
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
     a, ad, b, rc_ = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
     dfield = np.array(case.dfield, dtype=np.float64, copy=True, order="C")
@@ -669,7 +675,7 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         lib.sfr_ref_syst_form_simple_vel.restype = ctypes.c_int
         lib.sfr_ref_syst_form_simple_vel.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
-            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 9 + [_P])
+            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 11 + [_P] * 3)
         lib._vel_typed = True
     cal, mat = case.material()
     cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
@@ -678,6 +684,8 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
     dfield = cp(case.dfield, np.float64)
     vt = _load_arrays(case.lvel)
     sec = ctypes.c_double()
+    eddy = None if case.eddy is None else cp(case.eddy, np.float64)
+    stress = None if case.stress is None else cp(case.stress, np.float64)
     arrs = [cp(m.nelcon, np.int32), cp(m.nviz, np.int16), cp(m.cellface, np.int32),
             cp(m.owner, np.int32), cp(m.volume, np.float64), cp(m.dcca, np.float64),
             cp(m.xmcc, np.float64), cp(case.cc, np.float64), cp(m.mksi, np.float64),
@@ -694,5 +702,7 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         *[_p(x) for x in vt], case.icod, int(case.fso), int(case.fvisc), int(case.fres),
         case.type_simple, int(case.time_flag), case.time_type, case.dt, case.dt0, case.under,
         neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym), nthreads,
-        case.adv, ctypes.byref(sec))
+        case.adv, int(eddy is not None), int(stress is not None),
+        None if eddy is None else _p(eddy), None if stress is None else _p(stress),
+        ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value

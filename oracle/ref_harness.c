@@ -389,7 +389,9 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int type_simple, int time_flag, int time_type, double dt,
                                  double dt0, double under, int neq, int nad, int storage,
                                  int forces, int matrix, int calrcell, int unsym,
-                                 int nthreads, int advcod, double *seconds)
+                                 int nthreads, int advcod, int fturb, int fstruc,
+                                 const double *eddy_in, const double *stress_in,
+                                 double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -421,6 +423,11 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   memset(&mm, 0, sizeof(mm));
   memset(&ddt, 0, sizeof(ddt));
   adv.iCod1 = (short)(advcod > 0 ? advcod : FOUP);
+  tmodel.fTurb = fturb != 0;
+  tmodel.fTurbStruct = fstruc != 0;
+  tmodel.fWall = false;
+  if (eddy_in) memcpy(eddy, eddy_in, sizeof(double) * (size_t)numel);
+  if (stress_in) memcpy(stressr, stress_in, sizeof(double) * (size_t)numel * 6);
   diff.iCod = (short)icod;
   mm.fRes = fres != 0;
   mm.fRhieChowInt = false;

@@ -1006,6 +1006,28 @@ static void move_wall(const double vC[3], const double vB[3], const double n[3],
                 (vC[1] - vB[1]) * n[1] * n[2]);
 }
 
+/* turbStructIntegral (CellLib.c:7586-7626); rv NULL on a boundary face */
+static void struct_integral(const double *rc, const double *rv, const double *n, double *p,
+                            double area, double g1, double g2)
+{
+  const double third = 3.33333333333333333333E-1; /* D1DIV3, Define.h:179 */
+  double s[6], tmp;
+  int k;
+  if (!rv) {
+    tmp = third * (rc[0] + rc[1] + rc[2]);
+    for (k = 0; k < 3; k++) s[k] = rc[k] - tmp;
+    for (k = 3; k < 6; k++) s[k] = rc[k];
+  } else {
+    for (k = 0; k < 3; k++) s[k] = g1 * rc[k] + g2 * rv[k];
+    tmp = third * (s[0] + s[1] + s[2]);
+    for (k = 0; k < 3; k++) s[k] -= tmp;
+    for (k = 3; k < 6; k++) s[k] = g1 * rc[k] + g2 * rv[k];
+  }
+  p[0] -= area * (s[0] * n[0] + s[3] * n[1] + s[5] * n[2]);
+  p[1] -= area * (s[3] * n[0] + s[1] * n[1] + s[4] * n[2]);
+  p[2] -= area * (s[5] * n[0] + s[4] * n[1] + s[2] * n[2]);
+}
+
 int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
                      const double *xm, const orc_load *lvel, int nlvel,
                      const orc_vel_opts *o, const double *prop, const double *pres,
@@ -1041,7 +1063,7 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
     row = m->id[nel] - 1;
     rhoC = prop[lm * ORC_MAXPROP + ORC_DENSITY];
     muC = prop[lm * ORC_MAXPROP + 0];
-    effC = muC + 0.0e0; /* laminar: no eddy viscosity */
+    effC = muC + (o->fturb ? o->eddy[nel] : 0.0e0); /* CellSimple.c:207-209 */
     presC = pres[nel];
     for (i = 0; i < 3; i++) {
       for (j = 0; j < 3; j++) gvC[i][j] = gradvel[9 * (long)nel + 3 * i + j];
@@ -1064,7 +1086,7 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
         const int nb = viz[f];
         const int lmv = m->mat[nb] - 1;
         const double rhoV = prop[lmv * ORC_MAXPROP + ORC_DENSITY];
-        const double effV = prop[lmv * ORC_MAXPROP + 0] + 0.0e0;
+        const double effV = prop[lmv * ORC_MAXPROP + 0] + (o->fturb ? o->eddy[nb] : 0.0e0);
         const double presV = pres[nb];
         double velV[3], gpV[3], duDksi[3], gvV[3][3], ccV[3], lXm[3], v[3];
         double alpha, am1, visc, modE, dfd, density, wfn, cv, gf[3][3], wf[3], gvc[3][3];
@@ -1136,12 +1158,16 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
           for (i = 0; i < 3; i++)
             p[i] += aP * (gvc[0][i] * nrm[0] + gvc[1][i] * nrm[1] + gvc[2][i] * nrm[2]);
         }
+        if (o->fstruc)
+          struct_integral(o->stress + 6 * (long)nel, o->stress + 6 * (long)nb, nrm, p, area,
+                          am1, alpha);
       } else {
         double tmp;
         lA[f] = 0.0e0;
         /* facePressure, boundary: the cell's own pressure on the face */
         tmp = presC * area;
         for (i = 0; i < 3; i++) pf[i] += tmp * nrm[i];
+        if (o->fstruc) struct_integral(o->stress + 6 * (long)nel, 0, nrm, p, area, 0.0, 0.0);
         for (j = 0; j < 3; j++) s[j] = area * nrm[j];
         if (dif_scheme(s, ksi, e, t, o->icod)) return -1;
         if (fr[f]) {

@@ -154,6 +154,9 @@ typedef struct {
                         (advectiveScheme, CellLib.c:6394-6480) */
   double dt, dt0;
   double under;      /* underU (alphaVel) */
+  int fturb, fstruc; /* Turbulence.fTurb / fTurbStruct (no wall model) */
+  const double *eddy;   /* numel eddy viscosity (fturb) */
+  const double *stress; /* numel*6 residual stress xx yy zz xy yz xz (fstruc) */
 } orc_vel_opts;
 
 /* m->facer is faceVelR (velocity loads; a cell flagged there has no

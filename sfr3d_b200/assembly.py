@@ -42,7 +42,7 @@ class VelOptsC(ctypes.Structure):
     _fields_ = [("icod", _I32), ("fso", _I32), ("fvisc", _I32), ("fres", _I32),
                 ("type_simple", _I32), ("time_flag", _I32), ("time_type", _I32),
                 ("adv", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
-                ("under", ctypes.c_double)]
+                ("under", ctypes.c_double), ("fturb", _I32), ("fstruc", _I32)]
 
 
 class LoadC(ctypes.Structure):
@@ -73,6 +73,7 @@ def _lib():
                                                    + [_I32] * 3 + [_P])
         L.sfr_gpu_vel_plan_create.argtypes = [_P, ctypes.POINTER(DifMeshC), _I32,
                                               ctypes.POINTER(_P)]
+        L.sfr_gpu_vel_turbulence.argtypes = [_P, _P, _P, _I32]
         L.sfr_gpu_vel_assemble.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)] + [_P] * 9
                                            + [_I32] * 3)
         L.sfr_gpu_vel_assemble_device.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)]
@@ -314,9 +315,24 @@ class VelPlan(DifPlan):
             raise _sv.SolverError(rc, "sfr_gpu_vel_plan_create: " + _sv.last_error())
         self.h = h
 
-    def _vopts(self, fso, fvisc, fres, type_simple, time, under, adv=1):
+    def turbulence(self, eddy=None, stress=None, on_device: bool = False) -> None:
+        """Bind the eddy viscosity (numel) and residual stress (numel, 6)
+        that later calls read when fturb / fstruc are set: host arrays
+        (copied now) or device pointers (ints, kept)."""
+        if on_device:
+            rc = _lib().sfr_gpu_vel_turbulence(self.h, eddy or None, stress or None, 1)
+        else:
+            e = None if eddy is None else _c(eddy, np.float64)
+            st = None if stress is None else _c(stress, np.float64)
+            rc = _lib().sfr_gpu_vel_turbulence(self.h, _ptr(e), _ptr(st), 0)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_vel_turbulence: " + _sv.last_error())
+
+    def _vopts(self, fso, fvisc, fres, type_simple, time, under, adv=1, fturb=False,
+               fstruc=False):
         o = VelOptsC(icod=self.icod, fso=int(fso), fvisc=int(fvisc), fres=int(fres),
-                     type_simple=type_simple, under=under, adv=int(adv))
+                     type_simple=type_simple, under=under, adv=int(adv), fturb=int(fturb),
+                     fstruc=int(fstruc))
         if time is not None:
             o.time_flag = 1
             o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
@@ -324,9 +340,10 @@ class VelPlan(DifPlan):
 
     def assemble(self, lvel, prop, pres, gradpres, vel, gradvel, dfield, fso=True,
                  fvisc=False, fres=True, type_simple=SIMPLE, time=None, under=0.7,
-                 forces=True, matrix=True, calrcell=True, adv=FOUP):
+                 forces=True, matrix=True, calrcell=True, adv=FOUP, fturb=False, fstruc=False):
         """One call with host arrays: returns (ad3, b3, rcell3, dfield), each
-        component block after the other (u, v, w).  adv: FOUP, CD or SOUP."""
+        component block after the other (u, v, w).  adv: FOUP, CD or SOUP;
+        fturb / fstruc read the fields bound by ``turbulence``."""
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         arrs = [_c(a, np.float64) for a in (pres, gradpres, vel, gradvel)]
         df = np.array(dfield, dtype=np.float64, copy=True, order="C")
@@ -334,7 +351,7 @@ class VelPlan(DifPlan):
         b3 = np.empty(3 * self.neq) if forces else None
         rc3 = np.empty(3 * self.numel) if calrcell else None
         lv = _loads_c(lvel)
-        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc)
         rc = _lib().sfr_gpu_vel_assemble(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), *[_ptr(a) for a in arrs],
             _ptr(df), _ptr(ad3), _ptr(b3), _ptr(rc3), int(forces), int(matrix), int(calrcell))
@@ -348,10 +365,10 @@ class VelPlan(DifPlan):
                         d_gradvel: int, d_dfield: int, d_ad3: int = 0, d_b3: int = 0,
                         d_rcell3: int = 0, fso=True, fvisc=False, fres=True,
                         type_simple=SIMPLE, time=None, under=0.7, forces=True, matrix=True,
-                        calrcell=True, stream: int = 0, adv=FOUP):
+                        calrcell=True, stream: int = 0, adv=FOUP, fturb=False, fstruc=False):
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         lv = _loads_c(lvel)
-        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv)
+        o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc)
         rc = _lib().sfr_gpu_vel_assemble_device(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), d_pres, d_gradpres, d_vel,
             d_gradvel, d_dfield, d_ad3 or None, d_b3 or None, d_rcell3 or None, int(forces),

@@ -675,7 +675,31 @@ struct VelOpts {
   int fso, fvisc, fres, simplec, time_flag, time_type, forces, matrix, calrcell;
   double dt, dt0, under;
   int adv;  // 1 FoUp, 2 CD, 3 SoUp
+  int fturb, fstruc;
+  const double *eddy, *stress;  // numel, numel*6 (device)
 };
+
+// turbStructIntegral (CellLib.c:7586-7626): p -= area (s n), s the face's
+// residual stress without its trace (interior: g1 Rc + g2 Rv)
+__device__ __forceinline__ void struct_integral(const double *rc, const double *rv,
+                                                const double n[3], double p[3], double area,
+                                                double g1, double g2) {
+  constexpr double kThird = 3.33333333333333333333E-1;
+  double s[6];
+  if (!rv) {
+    const double tmp = xmul(kThird, xadd(xadd(rc[0], rc[1]), rc[2]));
+    for (int k = 0; k < 3; ++k) s[k] = xsub(rc[k], tmp);
+    for (int k = 3; k < 6; ++k) s[k] = rc[k];
+  } else {
+    for (int k = 0; k < 6; ++k) s[k] = xadd(xmul(g1, rc[k]), xmul(g2, rv[k]));
+    const double tmp = xmul(kThird, xadd(xadd(s[0], s[1]), s[2]));
+    for (int k = 0; k < 3; ++k) s[k] = xsub(s[k], tmp);
+  }
+  const double r0[3] = {s[0], s[3], s[5]}, r1[3] = {s[3], s[1], s[4]}, r2[3] = {s[5], s[4], s[2]};
+  p[0] = xsub(p[0], xmul(area, dot3(r0, n)));
+  p[1] = xsub(p[1], xmul(area, dot3(r1, n)));
+  p[2] = xsub(p[2], xmul(area, dot3(r2, n)));
+}
 
 // moveWall, not Dirichlet (CellLib.c:7715-7770)
 __device__ __forceinline__ void move_wall(const double vC[3], const double vB[3],
@@ -719,7 +743,7 @@ __global__ void __launch_bounds__(256, 2)
   const size_t fs = p.fstride;
   const int mc = mat[cell] - 1;
   const double rhoC = mtab[mc], muC = mtab[nmat + mc];
-  const double effC = xadd(muC, 0.0);  // laminar: no eddy viscosity
+  const double effC = xadd(muC, o.fturb ? o.eddy[cell] : 0.0);
   const size_t c3 = 3 * static_cast<size_t>(cell), c9 = 9 * static_cast<size_t>(cell);
   const double presC = pres[cell];
   double velC[3], gpC[3], gvC[9];
@@ -744,7 +768,7 @@ __global__ void __launch_bounds__(256, 2)
       const int c = nb & (kFlagP - 1);
       const size_t v3 = 3 * static_cast<size_t>(c), v9 = 9 * static_cast<size_t>(c);
       const int mv = mat[c] - 1;
-      const double rhoV = mtab[mv], effV = xadd(mtab[nmat + mv], 0.0);
+      const double rhoV = mtab[mv], effV = xadd(mtab[nmat + mv], o.fturb ? o.eddy[c] : 0.0);
       const double alpha = __ldcs(g), modE = __ldcs(g + fs), mk = __ldcs(g + 2 * fs);
       const double am1 = xsub(1.0, alpha);
       double ksi[3], t[3], velV[3], wf[3];
@@ -822,10 +846,16 @@ __global__ void __launch_bounds__(256, 2)
           pp[i] = xadd(pp[i], xmul(aP, dot3(col, n)));
         }
       }
+      if (o.fstruc)
+        struct_integral(o.stress + 6 * static_cast<size_t>(cell),
+                        o.stress + 6 * static_cast<size_t>(c), n, pp, area, am1, alpha);
     } else {
       const double dcca = __ldcs(g + fs);
       const double tmp = xmul(presC, area);
       for (int j = 0; j < 3; ++j) pf[j] = xadd(pf[j], xmul(tmp, n[j]));
+      if (o.fstruc)
+        struct_integral(o.stress + 6 * static_cast<size_t>(cell), nullptr, n, pp, area, 0.0,
+                        0.0);
       if (nb <= -2) {
         const DevLoad &L = loads[-nb - 2];
         if (L.type == 8 || L.type == 14) {  // MOVEWALL, STATICWALL
@@ -950,6 +980,10 @@ struct sfr_dif_plan {
   double *h_fields = nullptr;    // diffusion: density | cdiff | u0 | gradu0; pressure:
                                  // pres | gradpres | vel | dfield
   double *h_b0 = nullptr, *h_b = nullptr, *h_rcell = nullptr;
+  // momentum plans: the turbulence fields (bound device arrays, or the plan's
+  // own copies of host arrays)
+  const double *t_eddy = nullptr, *t_stress = nullptr;
+  double *own_eddy = nullptr, *own_stress = nullptr;
 };
 
 namespace {
@@ -995,6 +1029,8 @@ void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->h_b0);
   cudaFree(p->h_b);
   cudaFree(p->h_rcell);
+  cudaFree(p->own_eddy);
+  cudaFree(p->own_stress);
 }
 
 void fill_load(sfr::DevLoad *d, const sfr_load &L) {
@@ -1508,9 +1544,12 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
     SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
   if (o->adv < 0 || o->adv > 3)
     return bad("adv: FoUp (0 or 1), CD (2) or SoUp (3); TVD, NVD and LUST are not built");
+  if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
+    return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
-                  o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv};
+                  o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv, o->fturb != 0,
+                  o->fstruc != 0, p->t_eddy, p->t_stress};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =
@@ -1580,6 +1619,31 @@ int sfr_gpu_dif_update_cells(sfr_dif_plan *p, const double *d_x, double *d_u, in
   sfr::update_cells_kernel<<<(p->numel + 255) / 256, 256, 0, st>>>(p->d_id, p->numel, p->s->n,
                                                                      d_x, d_u, add != 0);
   SFR_CUA(cudaGetLastError());
+  return SFR_OK;
+}
+
+int sfr_gpu_vel_turbulence(sfr_dif_plan *p, const double *eddy, const double *stress,
+                           int32_t on_device) {
+  if (!p) return bad("NULL argument");
+  if (p->kind != 2) return bad("not a momentum plan");
+  SFR_CUA(cudaSetDevice(p->device));
+  if (on_device) {
+    p->t_eddy = eddy;
+    p->t_stress = stress;
+    return SFR_OK;
+  }
+  const size_t ne = p->numel;
+  p->t_eddy = p->t_stress = nullptr;
+  if (eddy) {
+    if (!p->own_eddy) SFR_CUA(cudaMalloc(&p->own_eddy, sizeof(double) * ne));
+    SFR_CUA(cudaMemcpy(p->own_eddy, eddy, sizeof(double) * ne, cudaMemcpyHostToDevice));
+    p->t_eddy = p->own_eddy;
+  }
+  if (stress) {
+    if (!p->own_stress) SFR_CUA(cudaMalloc(&p->own_stress, sizeof(double) * ne * 6));
+    SFR_CUA(cudaMemcpy(p->own_stress, stress, sizeof(double) * ne * 6, cudaMemcpyHostToDevice));
+    p->t_stress = p->own_stress;
+  }
   return SFR_OK;
 }
 

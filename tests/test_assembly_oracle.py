@@ -262,6 +262,49 @@ def test_vel_oracle_advection_schemes_match_reference_live():
         assert bits_equal(f[1], c[1]) and not np.array_equal(f[3], c[3])
 
 
+def test_vel_oracle_turbulence_matches_reference_live():
+    """An eddy viscosity field (effective viscosity mu + nu_t, the walls' too)
+    and the residual stress tensor's face integral (turbStructIntegral),
+    without a wall model, against the reference's own systFormSimpleVel."""
+    s = S.poisson_jittered(5, seed=8)
+    m = s.mesh()
+    rng = np.random.default_rng(9)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+            O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1))]
+    eddy = rng.uniform(0.0, 5e-3, m.numel)
+    stress = rng.standard_normal((m.numel, 6)) * 1e-2
+    for (te, ts_), adv, fvisc in itertools.product(((True, False), (False, True), (True, True)),
+                                                   (O.FOUP, O.SOUP), (0, 1)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop, mat=mat,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)),
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, fvisc=bool(fvisc),
+                         under=0.7, adv=adv, eddy=eddy if te else None,
+                         stress=stress if ts_ else None)
+        for name, (st, un, ia, ja, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (te, ts_, adv, fvisc, name)
+    # the fields change the system
+    lam = O.vel_assemble(O.VelCase(**{**case.__dict__, "eddy": None, "stress": None}),
+                         O.CSRD, True, s.ia, s.ja, s.neq)
+    tur = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    assert not np.array_equal(lam[1], tur[1]) and not np.array_equal(lam[3], tur[3])
+
+
 def test_vel_oracle_rejects_what_it_does_not_restate():
     s = S.poisson_uniform(4, seed=1)
     m = s.mesh()

@@ -542,6 +542,56 @@ def test_vel_advection_schemes_match_oracle(cuda, box, adv):
         gs.close()
 
 
+def test_vel_turbulence_matches_oracle(cuda, box):
+    """Eddy viscosity and the residual stress integral: bound as host
+    arrays or as device arrays, bit-identical to the oracle."""
+    import torch
+    s, m, lay = box
+    rng = np.random.default_rng(70)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    cc = _centres(m)
+    fv = m.face_r([1, 1, 2, 1, 3, 1])
+    eddy = rng.uniform(0.0, 5e-3, m.numel)
+    stress = rng.standard_normal((m.numel, 6)) * 1e-2
+    d_eddy = torch.tensor(eddy, device="cuda")
+    d_stress = torch.tensor(stress, device="cuda")
+    for name in ("csrd_full", "csrd_sym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.VelPlan(gs, m, fv, cc, icod=4)
+        with pytest.raises(sv.SolverError):  # nothing bound yet
+            plan.assemble(_aloads(VLOADS), prop, np.zeros(m.numel), np.zeros((m.numel, 3)),
+                          np.zeros((m.numel, 3)), np.zeros((m.numel, 3, 3)),
+                          np.ones((m.numel, 3)), fturb=True)
+        for on_device, (te, ts_) in itertools.product((False, True),
+                                                      ((True, False), (True, True))):
+            if on_device:
+                plan.turbulence(d_eddy.data_ptr(), d_stress.data_ptr(), on_device=True)
+            else:
+                plan.turbulence(eddy, stress)
+            case = O.VelCase(mesh=m, cc=cc, facevelr=fv, facepresr=m.face_r([0] * 6),
+                             lvel=VLOADS, prop=prop, pres=rng.standard_normal(m.numel),
+                             gradpres=rng.standard_normal((m.numel, 3)),
+                             vel=rng.standard_normal((m.numel, 3)),
+                             gradvel=rng.standard_normal((m.numel, 3, 3)),
+                             dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, fvisc=True,
+                             under=0.7, adv=O.SOUP, eddy=eddy if te else None,
+                             stress=stress if ts_ else None)
+            want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
+            assert want[0] == 0
+            ad3, b3, rc3, df = plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres,
+                                             case.vel, case.gradvel, case.dfield, fvisc=True,
+                                             under=0.7, adv=O.SOUP, fturb=te, fstruc=ts_)
+            al, ad, au = A.get_values(gs)
+            what = (name, on_device, te, ts_)
+            assert bits_equal(al, want[1]), what
+            assert bits_equal(ad3, want[2]) and bits_equal(b3, want[3]), what
+            assert bits_equal(rc3, want[4]) and bits_equal(df, want[5]), what
+        plan.close()
+        gs.close()
+
+
 def test_vel_assembled_momentum_solves_like_reference(cuda):
     """A lid-driven cavity's momentum system assembled and solved (u, v, w
     with their own diagonals) on the device."""
