@@ -681,7 +681,7 @@ struct VelOpts {
 
 // turbStructIntegral (CellLib.c:7586-7626): p -= area (s n), s the face's
 // residual stress without its trace (interior: g1 Rc + g2 Rv)
-__device__ __forceinline__ void struct_integral(const double *rc, const double *rv,
+__device__ __noinline__ void struct_integral(const double *rc, const double *rv,
                                                 const double n[3], double p[3], double area,
                                                 double g1, double g2) {
   constexpr double kThird = 3.33333333333333333333E-1;
@@ -726,7 +726,33 @@ __device__ __forceinline__ void move_wall(const double vC[3], const double vB[3]
 // One row of cellSimpleVel3D (CellSimple.c:106-727), laminar, first-order
 // upwind, face velocity without Rhie-Chow; three diagonals and forces.
 // mtab: density then viscosity of each material.
-template <int kMV>
+// The deferred correction of advectiveScheme (CellLib.c:6394-6480) with cv
+// in the place of wfn: CD deferredCd (CellLib.c:5113); SoUp upwindLinearV1
+// (CellLib.c:5072) from the upwind cell's gradient, r = xm - cc (plan words
+// 13-15 for this cell, 16-18 for the neighbour).  Out of line: the main
+// path keeps its registers.
+__device__ __noinline__ void advection_correction(int adv, double cv, double am1, double alpha,
+                                                  const double velC[3], const double velV[3],
+                                                  const double gvC[9], const double *gvV,
+                                                  const double *g, size_t fs, double cvc[3]) {
+  if (adv == 2) {
+    for (int i = 0; i < 3; ++i)
+      cvc[i] = xsub(xadd(xmul(am1, velC[i]), xmul(alpha, velV[i])), cv < 0.0 ? velV[i] : velC[i]);
+  } else if (adv == 3) {
+    double rr[3];
+    const bool down = cv < 0.0;
+    for (int j = 0; j < 3; ++j) rr[j] = __ldcs(g + ((down ? 16 : 13) + j) * fs);
+    for (int i = 0; i < 3; ++i) {
+      double gu[3];
+      for (int j = 0; j < 3; ++j) gu[j] = down ? gvV[3 * i + j] : gvC[3 * i + j];
+      cvc[i] = dot3(gu, rr);
+    }
+  }
+}
+
+// kExt: the deferred advection corrections and the turbulence fields; the
+// laminar first-order-upwind instantiation carries none of that code.
+template <int kMV, bool kExt>
 __global__ void __launch_bounds__(256, 2)
     vel_assemble_kernel(PlanDev p, const DevLoad *__restrict__ loads, VelOpts o,
                         const int16_t *__restrict__ mat, const double *__restrict__ mtab, int nmat,
@@ -743,7 +769,7 @@ __global__ void __launch_bounds__(256, 2)
   const size_t fs = p.fstride;
   const int mc = mat[cell] - 1;
   const double rhoC = mtab[mc], muC = mtab[nmat + mc];
-  const double effC = xadd(muC, o.fturb ? o.eddy[cell] : 0.0);
+  const double effC = xadd(muC, kExt && o.fturb ? o.eddy[cell] : 0.0);
   const size_t c3 = 3 * static_cast<size_t>(cell), c9 = 9 * static_cast<size_t>(cell);
   const double presC = pres[cell];
   double velC[3], gpC[3], gvC[9];
@@ -768,7 +794,8 @@ __global__ void __launch_bounds__(256, 2)
       const int c = nb & (kFlagP - 1);
       const size_t v3 = 3 * static_cast<size_t>(c), v9 = 9 * static_cast<size_t>(c);
       const int mv = mat[c] - 1;
-      const double rhoV = mtab[mv], effV = xadd(mtab[nmat + mv], o.fturb ? o.eddy[c] : 0.0);
+      const double rhoV = mtab[mv],
+                   effV = xadd(mtab[nmat + mv], kExt && o.fturb ? o.eddy[c] : 0.0);
       const double alpha = __ldcs(g), modE = __ldcs(g + fs), mk = __ldcs(g + 2 * fs);
       const double am1 = xsub(1.0, alpha);
       double ksi[3], t[3], velV[3], wf[3];
@@ -792,20 +819,8 @@ __global__ void __launch_bounds__(256, 2)
       // FoUp cvc = 0; CD deferredCd (CellLib.c:5113); SoUp upwindLinearV1
       // (CellLib.c:5072) from the upwind cell's gradient, r = xm - cc
       double cvc[3] = {0.0, 0.0, 0.0};
-      if (o.adv == 2) {
-        for (int i = 0; i < 3; ++i)
-          cvc[i] = xsub(xadd(xmul(am1, velC[i]), xmul(alpha, velV[i])),
-                        cv < 0.0 ? velV[i] : velC[i]);
-      } else if (o.adv == 3) {
-        double rr[3];
-        const bool down = cv < 0.0;
-        for (int j = 0; j < 3; ++j) rr[j] = __ldcs(g + ((down ? 16 : 13) + j) * fs);
-        for (int i = 0; i < 3; ++i) {
-          double gu[3];
-          for (int j = 0; j < 3; ++j) gu[j] = down ? gradvel[v9 + 3 * i + j] : gvC[3 * i + j];
-          cvc[i] = dot3(gu, rr);
-        }
-      }
+      if (kExt && o.adv != 1)
+        advection_correction(o.adv, cv, am1, alpha, velC, velV, gvC, gradvel + v9, g, fs, cvc);
       double gvc[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -846,14 +861,14 @@ __global__ void __launch_bounds__(256, 2)
           pp[i] = xadd(pp[i], xmul(aP, dot3(col, n)));
         }
       }
-      if (o.fstruc)
+      if (kExt && o.fstruc)
         struct_integral(o.stress + 6 * static_cast<size_t>(cell),
                         o.stress + 6 * static_cast<size_t>(c), n, pp, area, am1, alpha);
     } else {
       const double dcca = __ldcs(g + fs);
       const double tmp = xmul(presC, area);
       for (int j = 0; j < 3; ++j) pf[j] = xadd(pf[j], xmul(tmp, n[j]));
-      if (o.fstruc)
+      if (kExt && o.fstruc)
         struct_integral(o.stress + 6 * static_cast<size_t>(cell), nullptr, n, pp, area, 0.0,
                         0.0);
       if (nb <= -2) {
@@ -1559,10 +1574,12 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
                                    d_gradpres, d_vel, d_gradvel, d_dfield, s->d_stage,
                                    s->d_diag, d_ad3, d_b3, d_rcell3, p->numel);
   };
+  const bool ext = vo.adv != 1 || vo.fturb || vo.fstruc;
   if (p->d.maxviz == 6)
-    launch(sfr::vel_assemble_kernel<6>);
+    ext ? launch(sfr::vel_assemble_kernel<6, true>) : launch(sfr::vel_assemble_kernel<6, false>);
   else
-    launch(sfr::vel_assemble_kernel<sfr::kMaxViz>);
+    ext ? launch(sfr::vel_assemble_kernel<sfr::kMaxViz, true>)
+        : launch(sfr::vel_assemble_kernel<sfr::kMaxViz, false>);
   SFR_CUA(cudaGetLastError());
   if (matrix) return sfr::values_refreshed(s, st, false);
   return SFR_OK;
