@@ -385,14 +385,16 @@ typedef struct {
   int32_t fres;        /* MomentumModel.fRes */
   int32_t type_simple; /* 1 SIMPLE, 2 SIMPLEC */
   int32_t time_flag, time_type;
-  int32_t adv;         /* Advection.iCod1 (advectiveScheme, CellLib.c:6394-6480): 0 or 1
-                          FoUp, 2 CD (deferred central), 3 SoUp (linear upwind) */
+  int32_t adv;         /* Advection.iCod1 (advectiveScheme, CellLib.c:6394-6650): 0 or 1
+                          FoUp, 2 CD (deferred central), 3 SoUp (linear upwind), 6 LUST
+                          (deferredLust, CellLib.c:5162, weight adv_beta) */
   double dt, dt0;
   double under;        /* under-relaxation of the velocity (alphaVel) */
   int32_t fturb;       /* Turbulence.fTurb: effective viscosity mu + eddy viscosity
                           (fields bound by sfr_gpu_vel_turbulence) */
   int32_t fstruc;      /* Turbulence.fTurbStruct: the residual stress tensor's face
                           integral (turbStructIntegral, CellLib.c:7586) */
+  double adv_beta;     /* Advection.par[0]: LUST's linear-upwind weight */
 } sfr_vel_opts;
 
 int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,

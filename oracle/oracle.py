@@ -561,7 +561,7 @@ def ref_pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
 # ------------------------------------------------------ momentum assembly --
 # systFormSimpleVel (CellLoopInc.c:98-470) -> cellSimpleVel3D (CellSimple.c:106)
 SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
-FOUP, CD, SOUP = 1, 2, 3  # advection schemes, Define.h:267-269
+FOUP, CD, SOUP, LUST = 1, 2, 3, 6  # advection schemes, Define.h:267-272
 
 
 @dataclass
@@ -597,6 +597,7 @@ class VelCase:
     adv: int = FOUP
     eddy: np.ndarray | None = None     # (numel,) eddy viscosity: Turbulence.fTurb
     stress: np.ndarray | None = None   # (numel, 6) residual stress: fTurbStruct
+    adv_beta: float = 0.25             # Advection.par[0]: LUST weight
 
     def material(self):
         mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
@@ -612,7 +613,8 @@ class _VelOpts(ctypes.Structure):
                 ("time_flag", ctypes.c_int), ("time_type", ctypes.c_int),
                 ("adv", ctypes.c_int),
                 ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double),
-                ("fturb", ctypes.c_int), ("fstruc", ctypes.c_int), ("eddy", _P), ("stress", _P)]
+                ("fturb", ctypes.c_int), ("fstruc", ctypes.c_int), ("eddy", _P), ("stress", _P),
+                ("adv_beta", ctypes.c_double)]
 
 
 def _vel_out(storage, unsym, neq, ia, ja, numel, fill):
@@ -649,6 +651,7 @@ def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix
     turb = [None if a is None else _c(a, np.float64) for a in (case.eddy, case.stress)]
     o.fturb, o.fstruc = int(turb[0] is not None), int(turb[1] is not None)
     o.eddy, o.stress = [None if a is None else _p(a) for a in turb]
+    o.adv_beta = case.adv_beta
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
     a, ad, b, rc_ = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
     dfield = np.array(case.dfield, dtype=np.float64, copy=True, order="C")
@@ -675,7 +678,8 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         lib.sfr_ref_syst_form_simple_vel.restype = ctypes.c_int
         lib.sfr_ref_syst_form_simple_vel.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
-            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 11 + [_P] * 3)
+            + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 11 + [_P] * 2
+            + [ctypes.c_double, _P])
         lib._vel_typed = True
     cal, mat = case.material()
     cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
@@ -704,5 +708,5 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         neq, nad, storage, int(forces), int(matrix), int(calrcell), int(unsym), nthreads,
         case.adv, int(eddy is not None), int(stress is not None),
         None if eddy is None else _p(eddy), None if stress is None else _p(stress),
-        ctypes.byref(sec))
+        case.adv_beta, ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value

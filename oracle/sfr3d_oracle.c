@@ -1043,7 +1043,7 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
   if (mv < 1 || mv > MAXF - 1 || storage == ORC_ELLPACK) return -1;
   /* any other typeSimple leaves D as the first neighbour's copy */
   if (o->type_simple != 1 && o->type_simple != 2) return -1;
-  if (o->adv < 0 || o->adv > 3) return -1; /* TVD, NVD and LUST not restated */
+  if (o->adv < 0 || (o->adv > 3 && o->adv != 6)) return -1; /* TVD, NVD not restated */
   for (nel = 0; nel < numel; nel++) {
     double lA[MAXF + 3], ksi[3], nrm[3], s[3], e[3], t[3];
     double p[3] = {0.0, 0.0, 0.0}, pf[3] = {0.0, 0.0, 0.0}, sPc[3] = {0.0, 0.0, 0.0};
@@ -1137,6 +1137,24 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
                 cvc[i] = gvV[i][0] * rV[0] + gvV[i][1] * rV[1] + gvV[i][2] * rV[2];
               else
                 cvc[i] = gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1] + gvC[i][2] * xmcc[2];
+            } else if (o->adv == 6) { /* deferredLust, CellLib.c:5162-5198 */
+              double gf, up, ul, uf1, uf2, cd;
+              if (cv < 0.e0) {
+                gf = gvV[i][0] * rV[0] + gvV[i][1] * rV[1];
+                gf += gvV[i][2] * rV[2];
+                up = velV[i];
+              } else {
+                gf = gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1];
+                gf += gvC[i][2] * xmcc[2];
+                up = velC[i];
+              }
+              ul = up + gf;
+              uf1 = velC[i] + gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1];
+              uf2 = velV[i] + gvV[i][0] * rV[0] + gvV[i][1] * rV[1];
+              uf1 += gvC[i][2] * xmcc[2];
+              uf2 += gvV[i][2] * rV[2];
+              cd = am1 * uf1 + alpha * uf2;
+              cvc[i] = o->adv_beta * ul + (1.e0 - o->adv_beta) * cd - up;
             }
           }
           for (i = 0; i < 3; i++) p[i] += dfdc[i] - cv * cvc[i];

@@ -157,6 +157,7 @@ typedef struct {
   int fturb, fstruc; /* Turbulence.fTurb / fTurbStruct (no wall model) */
   const double *eddy;   /* numel eddy viscosity (fturb) */
   const double *stress; /* numel*6 residual stress xx yy zz xy yz xz (fstruc) */
+  double adv_beta;      /* Advection.par[0]: LUST weight (adv 6) */
 } orc_vel_opts;
 
 /* m->facer is faceVelR (velocity loads; a cell flagged there has no

@@ -674,9 +674,10 @@ __global__ void __launch_bounds__(256, 2)
 struct VelOpts {
   int fso, fvisc, fres, simplec, time_flag, time_type, forces, matrix, calrcell;
   double dt, dt0, under;
-  int adv;  // 1 FoUp, 2 CD, 3 SoUp
+  int adv;  // 1 FoUp, 2 CD, 3 SoUp, 6 LUST
   int fturb, fstruc;
   const double *eddy, *stress;  // numel, numel*6 (device)
+  double beta;  // LUST weight
 };
 
 // turbStructIntegral (CellLib.c:7586-7626): p -= area (s n), s the face's
@@ -732,9 +733,10 @@ __device__ __forceinline__ void move_wall(const double vC[3], const double vB[3]
 // 13-15 for this cell, 16-18 for the neighbour).  Out of line: the main
 // path keeps its registers.
 __device__ __noinline__ void advection_correction(int adv, double cv, double am1, double alpha,
-                                                  const double velC[3], const double velV[3],
-                                                  const double gvC[9], const double *gvV,
-                                                  const double *g, size_t fs, double cvc[3]) {
+                                                  double beta, const double velC[3],
+                                                  const double velV[3], const double gvC[9],
+                                                  const double *gvV, const double *g, size_t fs,
+                                                  double cvc[3]) {
   if (adv == 2) {
     for (int i = 0; i < 3; ++i)
       cvc[i] = xsub(xadd(xmul(am1, velC[i]), xmul(alpha, velV[i])), cv < 0.0 ? velV[i] : velC[i]);
@@ -746,6 +748,24 @@ __device__ __noinline__ void advection_correction(int adv, double cv, double am1
       double gu[3];
       for (int j = 0; j < 3; ++j) gu[j] = down ? gvV[3 * i + j] : gvC[3 * i + j];
       cvc[i] = dot3(gu, rr);
+    }
+  } else if (adv == 6) {  // deferredLust (CellLib.c:5162-5198)
+    double rC[3], rV[3];
+    for (int j = 0; j < 3; ++j) {
+      rC[j] = __ldcs(g + (13 + j) * fs);
+      rV[j] = __ldcs(g + (16 + j) * fs);
+    }
+    const bool down = cv < 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const double *gc = gvC + 3 * i, *gv = gvV + 3 * i;
+      const double up = down ? velV[i] : velC[i];
+      const double ul = xadd(up, down ? dot3(gv, rV) : dot3(gc, rC));
+      double uf1 = xadd(xadd(velC[i], xmul(gc[0], rC[0])), xmul(gc[1], rC[1]));
+      double uf2 = xadd(xadd(velV[i], xmul(gv[0], rV[0])), xmul(gv[1], rV[1]));
+      uf1 = xadd(uf1, xmul(gc[2], rC[2]));
+      uf2 = xadd(uf2, xmul(gv[2], rV[2]));
+      const double cd = xadd(xmul(am1, uf1), xmul(alpha, uf2));
+      cvc[i] = xsub(xadd(xmul(beta, ul), xmul(xsub(1.0, beta), cd)), up);
     }
   }
 }
@@ -820,7 +840,8 @@ __global__ void __launch_bounds__(256, 2)
       // (CellLib.c:5072) from the upwind cell's gradient, r = xm - cc
       double cvc[3] = {0.0, 0.0, 0.0};
       if (kExt && o.adv != 1)
-        advection_correction(o.adv, cv, am1, alpha, velC, velV, gvC, gradvel + v9, g, fs, cvc);
+        advection_correction(o.adv, cv, am1, alpha, o.beta, velC, velV, gvC, gradvel + v9, g, fs,
+                             cvc);
       double gvc[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -1557,14 +1578,14 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if (rc != SFR_OK) return rc;
   if (calrcell && p->free_cells > 0)
     SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
-  if (o->adv < 0 || o->adv > 3)
-    return bad("adv: FoUp (0 or 1), CD (2) or SoUp (3); TVD, NVD and LUST are not built");
+  if (o->adv < 0 || (o->adv > 3 && o->adv != 6))
+    return bad("adv: FoUp (0 or 1), CD (2), SoUp (3) or LUST (6); TVD and NVD are not built");
   if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
     return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
                   o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv, o->fturb != 0,
-                  o->fstruc != 0, p->t_eddy, p->t_stress};
+                  o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =

@@ -239,7 +239,7 @@ def test_vel_oracle_advection_schemes_match_reference_live():
     prop[0, :2] = (1e-3, 1.0)
     lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
             O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1))]
-    for adv, icod, fso, ts in itertools.product((O.CD, O.SOUP), (1, 4), (0, 1),
+    for adv, icod, fso, ts in itertools.product((O.CD, O.SOUP, O.LUST), (1, 4), (0, 1),
                                                 (O.SIMPLE, O.SIMPLEC)):
         case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
                          facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop,
@@ -248,7 +248,7 @@ def test_vel_oracle_advection_schemes_match_reference_live():
                          vel=rng.standard_normal((m.numel, 3)),
                          gradvel=rng.standard_normal((m.numel, 3, 3)),
                          dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=icod, fso=bool(fso),
-                         type_simple=ts, under=0.7, adv=adv)
+                         type_simple=ts, under=0.7, adv=adv, adv_beta=0.25 + 0.1 * icod)
         for name, (st, un, ia, ja, _al, _au) in lay.items():
             r1 = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
             r2 = O.ref_vel_assemble(case, st, un, ia, ja, s.neq, fill=3.0)
@@ -321,5 +321,6 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
     assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
     assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4) == -1  # TVD not restated
+    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=5) == -1  # NVD not restated
     assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
                           O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1
