@@ -386,7 +386,8 @@ typedef struct {
   int32_t type_simple; /* 1 SIMPLE, 2 SIMPLEC */
   int32_t time_flag, time_type;
   int32_t adv;         /* Advection.iCod1 (advectiveScheme, CellLib.c:6394-6650): 0 or 1
-                          FoUp, 2 CD (deferred central), 3 SoUp (linear upwind), 6 LUST
+                          FoUp, 2 CD (deferred central), 3 SoUp (linear upwind), 5 NVD
+                          (faceBaseNvd, CellLib.c:4900, function adv_fn), 6 LUST
                           (deferredLust, CellLib.c:5162, weight adv_beta) */
   double dt, dt0;
   double under;        /* under-relaxation of the velocity (alphaVel) */
@@ -395,6 +396,9 @@ typedef struct {
   int32_t fstruc;      /* Turbulence.fTurbStruct: the residual stress tensor's face
                           integral (turbStructIntegral, CellLib.c:7586) */
   double adv_beta;     /* Advection.par[0]: LUST's linear-upwind weight */
+  int32_t adv_fn;      /* Advection.iCod2 for NVD: 1 BCD, 2 MUSCL, 3 SMART, 4 ModSMART,
+                          5 SuperBee, 6 ModSuperBee, 7 STOIC, 8 MinMod, 9 ModBCD (nvd,
+                          CellLib.c; MUSCL and STOIC weigh 0, as there) */
 } sfr_vel_opts;
 
 int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,

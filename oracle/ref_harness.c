@@ -391,7 +391,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int forces, int matrix, int calrcell, int unsym,
                                  int nthreads, int advcod, int fturb, int fstruc,
                                  const double *eddy_in, const double *stress_in,
-                                 double adv_beta, double *seconds)
+                                 double adv_beta, int adv_fn, double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -424,6 +424,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   memset(&ddt, 0, sizeof(ddt));
   adv.iCod1 = (short)(advcod > 0 ? advcod : FOUP);
   adv.par[0] = adv_beta;
+  adv.iCod2 = (short)adv_fn;
   tmodel.fTurb = fturb != 0;
   tmodel.fTurbStruct = fstruc != 0;
   tmodel.fWall = false;

@@ -1006,6 +1006,42 @@ static void move_wall(const double vC[3], const double vB[3], const double n[3],
                 (vC[1] - vB[1]) * n[1] * n[2]);
 }
 
+/* nvd (CellLib.c): the weights of NVD function fn at phi~, as its table
+ * gives them; MUSCL (2) and STOIC (7) have empty bodies there: (0, 0) */
+static void nvd_table(double ph, int fn, double *w)
+{
+  const double third = 3.33333333333333333333E-1, two3 = 6.66666666666666666666E-1;
+  w[0] = 0.0;
+  w[1] = 0.0;
+  if (fn == 2 || fn == 7) return;
+  w[0] = 1.0;
+  if (fn == 1) {
+    if (ph >= 0 && ph <= 1.e0) { w[0] = 0.5; w[1] = 0.5; }
+  } else if (fn == 3) {
+    if (ph >= 0 && ph <= 5.0 / 6.0) { w[0] = 3.0 / 4.0; w[1] = 3.0 / 8.0; }
+    else if (ph > 5.0 / 6.0 && ph <= 1.0) { w[0] = 0.0; w[1] = 1.0; }
+  } else if (fn == 4) {
+    if (ph >= 0 && ph <= 1.0 / 6.0) { w[0] = 3.0; w[1] = 0.0; }
+    else if (ph > 1.0 / 6.0 && ph <= 0.7) { w[0] = 3.0 / 4.0; w[1] = 3.0 / 8.0; }
+    else if (ph > 0.7 && ph <= 1.0) { w[0] = third; w[1] = two3; }
+  } else if (fn == 5) {
+    if (ph >= 0 && ph <= 5.e-1) { w[0] = 0.5; w[1] = 0.5; }
+    else if (ph > 5e-1 && ph <= two3) { w[0] = 1.5; w[1] = 0.0; }
+    else if (ph > two3 && ph <= 1.e0) { w[0] = 0.0; w[1] = 1.0; }
+  } else if (fn == 6) {
+    if (ph >= 0 && ph <= third) { w[0] = 2.0; w[1] = 0.0; }
+    else if (ph > third && ph <= 0.5) { w[0] = 0.5; w[1] = 0.5; }
+    else if (ph > 0.5 && ph <= two3) { w[0] = 1.5; w[1] = 0.0; }
+    else if (ph > two3 && ph <= 1) { w[0] = 0.0; w[1] = 1.0; }
+  } else if (fn == 8) {
+    if (ph >= 0 && ph <= 5.e-1) { w[0] = 1.5; w[1] = 0.0; }
+    else if (ph > 5e-1 && ph <= 1.0) { w[0] = 0.5; w[1] = 0.5; }
+  } else if (fn == 9) {
+    if (ph >= 0.e0 && ph <= 1.0 / 4.0) { w[0] = 2.5; w[1] = 0.0; }
+    else if (ph > 1.0 / 4.0 && ph <= 1.e0) { w[0] = 0.5; w[1] = 0.5; }
+  }
+}
+
 /* turbStructIntegral (CellLib.c:7586-7626); rv NULL on a boundary face */
 static void struct_integral(const double *rc, const double *rv, const double *n, double *p,
                             double area, double g1, double g2)
@@ -1043,7 +1079,8 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
   if (mv < 1 || mv > MAXF - 1 || storage == ORC_ELLPACK) return -1;
   /* any other typeSimple leaves D as the first neighbour's copy */
   if (o->type_simple != 1 && o->type_simple != 2) return -1;
-  if (o->adv < 0 || (o->adv > 3 && o->adv != 6)) return -1; /* TVD, NVD not restated */
+  if (o->adv < 0 || o->adv == 4 || o->adv > 6) return -1; /* TVD not restated */
+  if (o->adv == 5 && (o->adv_fn < 1 || o->adv_fn > 9)) return -1;
   for (nel = 0; nel < numel; nel++) {
     double lA[MAXF + 3], ksi[3], nrm[3], s[3], e[3], t[3];
     double p[3] = {0.0, 0.0, 0.0}, pf[3] = {0.0, 0.0, 0.0}, sPc[3] = {0.0, 0.0, 0.0};
@@ -1137,6 +1174,25 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
                 cvc[i] = gvV[i][0] * rV[0] + gvV[i][1] * rV[1] + gvV[i][2] * rV[2];
               else
                 cvc[i] = gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1] + gvC[i][2] * xmcc[2];
+            } else if (o->adv == 5) { /* faceBaseNvd, CellLib.c:4900-4937 */
+              double gf, phi, w[2];
+              if (cv < 0.e0) {
+                gf = gvV[i][0] * ksi[0] + gvV[i][1] * ksi[1];
+                gf += gvV[i][2] * ksi[2];
+                gf = -2.e0 * gf * mk + 1.e-32;
+                phi = (velV[i] - velC[i]) / gf + 1.e0;
+                nvd_table(phi, o->adv_fn, w);
+                cvc[i] = (w[0] - 1.0) * velV[i] + w[1] * velC[i] +
+                         (1.0 - w[0] - w[1]) * (velC[i] - gf);
+              } else {
+                gf = gvC[i][0] * ksi[0] + gvC[i][1] * ksi[1];
+                gf += gvC[i][2] * ksi[2];
+                gf = 2.e0 * gf * mk + 1.e-32;
+                phi = (velC[i] - velV[i]) / gf + 1.e0;
+                nvd_table(phi, o->adv_fn, w);
+                cvc[i] = (w[0] - 1.0) * velC[i] + w[1] * velV[i] +
+                         (1.0 - w[0] - w[1]) * (velV[i] - gf);
+              }
             } else if (o->adv == 6) { /* deferredLust, CellLib.c:5162-5198 */
               double gf, up, ul, uf1, uf2, cd;
               if (cv < 0.e0) {

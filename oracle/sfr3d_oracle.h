@@ -158,6 +158,7 @@ typedef struct {
   const double *eddy;   /* numel eddy viscosity (fturb) */
   const double *stress; /* numel*6 residual stress xx yy zz xy yz xz (fstruc) */
   double adv_beta;      /* Advection.par[0]: LUST weight (adv 6) */
+  int adv_fn;           /* Advection.iCod2: NVD function 1..9 (adv 5) */
 } orc_vel_opts;
 
 /* m->facer is faceVelR (velocity loads; a cell flagged there has no

@@ -678,7 +678,50 @@ struct VelOpts {
   int fturb, fstruc;
   const double *eddy, *stress;  // numel, numel*6 (device)
   double beta;  // LUST weight
+  int nvd;      // NVD function
 };
+
+// nvd (CellLib.c): the two weights of an NVD function at phi~; the
+// reference's table, MUSCL and STOIC left at (0, 0) as it leaves them
+__host__ __device__ inline void nvd_weights(double ph, int fn, double *p0, double *p1) {
+  constexpr double k13 = 3.33333333333333333333E-1, k23 = 6.66666666666666666666E-1;
+  double a = 1.0, b = 0.0;
+  switch (fn) {
+    case 1: if (ph >= 0 && ph <= 1.0) { a = 0.5; b = 0.5; } break;
+    case 3:
+      if (ph >= 0 && ph <= 5.0 / 6.0) { a = 3.0 / 4.0; b = 3.0 / 8.0; }
+      else if (ph > 5.0 / 6.0 && ph <= 1.0) { a = 0.0; b = 1.0; }
+      break;
+    case 4:
+      if (ph >= 0 && ph <= 1.0 / 6.0) { a = 3.0; b = 0.0; }
+      else if (ph > 1.0 / 6.0 && ph <= 0.7) { a = 3.0 / 4.0; b = 3.0 / 8.0; }
+      else if (ph > 0.7 && ph <= 1.0) { a = k13; b = k23; }
+      break;
+    case 5:
+      if (ph >= 0 && ph <= 0.5) { a = 0.5; b = 0.5; }
+      else if (ph > 0.5 && ph <= k23) { a = 1.5; b = 0.0; }
+      else if (ph > k23 && ph <= 1.0) { a = 0.0; b = 1.0; }
+      break;
+    case 6:
+      if (ph >= 0 && ph <= k13) { a = 2.0; b = 0.0; }
+      else if (ph > k13 && ph <= 0.5) { a = 0.5; b = 0.5; }
+      else if (ph > 0.5 && ph <= k23) { a = 1.5; b = 0.0; }
+      else if (ph > k23 && ph <= 1.0) { a = 0.0; b = 1.0; }
+      break;
+    case 8:
+      if (ph >= 0 && ph <= 0.5) { a = 1.5; b = 0.0; }
+      else if (ph > 0.5 && ph <= 1.0) { a = 0.5; b = 0.5; }
+      break;
+    case 9:
+      if (ph >= 0 && ph <= 0.25) { a = 2.5; b = 0.0; }
+      else if (ph > 0.25 && ph <= 1.0) { a = 0.5; b = 0.5; }
+      break;
+    default: a = 0.0; b = 0.0; break;  // 2 MUSCL, 7 STOIC
+  }
+  *p0 = a;
+  *p1 = b;
+}
+
 
 // turbStructIntegral (CellLib.c:7586-7626): p -= area (s n), s the face's
 // residual stress without its trace (interior: g1 Rc + g2 Rv)
@@ -733,7 +776,7 @@ __device__ __forceinline__ void move_wall(const double vC[3], const double vB[3]
 // 13-15 for this cell, 16-18 for the neighbour).  Out of line: the main
 // path keeps its registers.
 __device__ __noinline__ void advection_correction(int adv, double cv, double am1, double alpha,
-                                                  double beta, const double velC[3],
+                                                  double beta, int nvd, const double velC[3],
                                                   const double velV[3], const double gvC[9],
                                                   const double *gvV, const double *g, size_t fs,
                                                   double cvc[3]) {
@@ -748,6 +791,22 @@ __device__ __noinline__ void advection_correction(int adv, double cv, double am1
       double gu[3];
       for (int j = 0; j < 3; ++j) gu[j] = down ? gvV[3 * i + j] : gvC[3 * i + j];
       cvc[i] = dot3(gu, rr);
+    }
+  } else if (adv == 5) {  // faceBaseNvd (CellLib.c:4900-4937), the cell as uP
+    double ksi[3];
+    for (int j = 0; j < 3; ++j) ksi[j] = __ldcs(g + (3 + j) * fs);
+    const double mk = __ldcs(g + 2 * fs);
+    const bool down = cv < 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const double uP = velC[i], uV = velV[i];
+      const double gf0 = dot3(down ? gvV + 3 * i : gvC + 3 * i, ksi);
+      const double gf = xadd(xmul(xmul(down ? -2.0 : 2.0, gf0), mk), 1.e-32);
+      const double phi = xadd(xdiv(down ? xsub(uV, uP) : xsub(uP, uV), gf), 1.0);
+      double p0, p1;
+      nvd_weights(phi, nvd, &p0, &p1);
+      const double a = down ? uV : uP, b = down ? uP : uV;
+      cvc[i] = xadd(xadd(xmul(xsub(p0, 1.0), a), xmul(p1, b)),
+                    xmul(xsub(xsub(1.0, p0), p1), xsub(b, gf)));
     }
   } else if (adv == 6) {  // deferredLust (CellLib.c:5162-5198)
     double rC[3], rV[3];
@@ -840,8 +899,8 @@ __global__ void __launch_bounds__(256, 2)
       // (CellLib.c:5072) from the upwind cell's gradient, r = xm - cc
       double cvc[3] = {0.0, 0.0, 0.0};
       if (kExt && o.adv != 1)
-        advection_correction(o.adv, cv, am1, alpha, o.beta, velC, velV, gvC, gradvel + v9, g, fs,
-                             cvc);
+        advection_correction(o.adv, cv, am1, alpha, o.beta, o.nvd, velC, velV, gvC, gradvel + v9,
+                             g, fs, cvc);
       double gvc[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -1578,14 +1637,15 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if (rc != SFR_OK) return rc;
   if (calrcell && p->free_cells > 0)
     SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
-  if (o->adv < 0 || (o->adv > 3 && o->adv != 6))
-    return bad("adv: FoUp (0 or 1), CD (2), SoUp (3) or LUST (6); TVD and NVD are not built");
+  if (o->adv < 0 || o->adv == 4 || o->adv > 6)
+    return bad("adv: FoUp (0 or 1), CD (2), SoUp (3), NVD (5) or LUST (6); TVD is not built");
+  if (o->adv == 5 && (o->adv_fn < 1 || o->adv_fn > 9)) return bad("adv_fn: NVD function 1..9");
   if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
     return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
                   o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv, o->fturb != 0,
-                  o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta};
+                  o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta, o->adv_fn};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =

@@ -255,7 +255,25 @@ def test_vel_oracle_advection_schemes_match_reference_live():
             assert r1[0] == r2[0] == 0
             for x, y in zip(r1[1:], r2[1:6]):
                 assert bits_equal(x, y), (adv, icod, fso, ts, name)
-        # the schemes change b (the deferred correction), not the matrix
+        # NVD with each of its functions (MUSCL and STOIC weigh 0, as in the reference)
+    st, un, ia_, ja_, _al, _au = lay["csrd_full"]
+    for fn in range(1, 10):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.3,
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7,
+                         adv=O.NVD, adv_fn=fn)
+        for name in ("csrd_full", "csrc_unsym"):
+            st, un, ia_, ja_, _al, _au = lay[name]
+            r1 = O.vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), ("nvd", fn, name)
+    # the schemes change b (the deferred correction), not the matrix
         f = O.vel_assemble(O.VelCase(**{**case.__dict__, "adv": O.FOUP}), O.CSRD, True,
                            s.ia, s.ja, s.neq)
         c = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
@@ -321,6 +339,6 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
     assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
     assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4) == -1  # TVD not restated
-    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=5) == -1  # NVD not restated
+    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=5, adv_fn=10) == -1  # no such function
     assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
                           O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1

@@ -504,7 +504,7 @@ def test_vel_matches_oracle(cuda, box, icod):
         gs.close()
 
 
-@pytest.mark.parametrize("adv", [O.CD, O.SOUP, O.LUST])
+@pytest.mark.parametrize("adv", [O.CD, O.SOUP, O.LUST, O.NVD])
 def test_vel_advection_schemes_match_oracle(cuda, box, adv):
     s, m, lay = box
     rng = np.random.default_rng(60 + adv)
@@ -523,12 +523,14 @@ def test_vel_advection_schemes_match_oracle(cuda, box, adv):
                              vel=rng.standard_normal((m.numel, 3)),
                              gradvel=rng.standard_normal((m.numel, 3, 3)),
                              dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, fso=bool(fso),
-                             type_simple=ts, under=0.7, adv=adv, adv_beta=0.3)
+                             type_simple=ts, under=0.7, adv=adv, adv_beta=0.3,
+                             adv_fn=3 + fso + 2 * (ts == A.SIMPLEC))
             want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
             assert want[0] == 0
             ad3, b3, rc3, df = plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres,
                                              case.vel, case.gradvel, case.dfield, fso=fso,
-                                             type_simple=ts, under=0.7, adv=adv, adv_beta=0.3)
+                                             type_simple=ts, under=0.7, adv=adv, adv_beta=0.3,
+                                             adv_fn=case.adv_fn)
             al, ad, au = A.get_values(gs)
             a = al if au is None else np.concatenate([al, au])
             what = (name, adv, fso, ts)
