@@ -387,7 +387,8 @@ typedef struct {
   int32_t time_flag, time_type;
   int32_t adv;         /* Advection.iCod1 (advectiveScheme, CellLib.c:6394-6650): 0 or 1
                           FoUp, 2 CD (deferred central), 3 SoUp (linear upwind), 5 NVD
-                          (faceBaseNvd, CellLib.c:4900, function adv_fn), 6 LUST
+                          (faceBaseNvd, CellLib.c:4900, function adv_fn), 4 TVD (faceBaseTvdV1,
+                          CellLib.c:4845, limiter adv_fn 1..5), 6 LUST
                           (deferredLust, CellLib.c:5162, weight adv_beta) */
   double dt, dt0;
   double under;        /* under-relaxation of the velocity (alphaVel) */

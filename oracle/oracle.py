@@ -561,7 +561,7 @@ def ref_pres_assemble(case: PresCase, storage, unsym, ia, ja, neq, forces=True,
 # ------------------------------------------------------ momentum assembly --
 # systFormSimpleVel (CellLoopInc.c:98-470) -> cellSimpleVel3D (CellSimple.c:106)
 SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
-FOUP, CD, SOUP, NVD, LUST = 1, 2, 3, 5, 6  # advection schemes, Define.h:267-272
+FOUP, CD, SOUP, TVD, NVD, LUST = 1, 2, 3, 4, 5, 6  # advection schemes, Define.h:267-272
 
 
 @dataclass

@@ -1079,7 +1079,8 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
   if (mv < 1 || mv > MAXF - 1 || storage == ORC_ELLPACK) return -1;
   /* any other typeSimple leaves D as the first neighbour's copy */
   if (o->type_simple != 1 && o->type_simple != 2) return -1;
-  if (o->adv < 0 || o->adv == 4 || o->adv > 6) return -1; /* TVD not restated */
+  if (o->adv < 0 || o->adv > 6) return -1;
+  if (o->adv == 4 && (o->adv_fn < 1 || o->adv_fn > 5)) return -1;
   if (o->adv == 5 && (o->adv_fn < 1 || o->adv_fn > 9)) return -1;
   for (nel = 0; nel < numel; nel++) {
     double lA[MAXF + 3], ksi[3], nrm[3], s[3], e[3], t[3];
@@ -1174,6 +1175,36 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
                 cvc[i] = gvV[i][0] * rV[0] + gvV[i][1] * rV[1] + gvV[i][2] * rV[2];
               else
                 cvc[i] = gvC[i][0] * xmcc[0] + gvC[i][1] * xmcc[1] + gvC[i][2] * xmcc[2];
+            } else if (o->adv == 4) { /* faceBaseTvdV1, CellLib.c:4845-4875 */
+              double du, gf, r, lim = 0.e0, a, b, c;
+              const double *vs = m->vskew + 3 * face;
+              if (cv < 0.e0) {
+                du = velC[i] - velV[i] + 1.e-14;
+                gf = gvV[i][0] * ksi[0] + gvV[i][1] * ksi[1];
+                gf += gvV[i][2] * ksi[2];
+                gf = -2.e0 * gf * mk;
+              } else {
+                du = velV[i] - velC[i] + 1.e-14;
+                gf = gvC[i][0] * ksi[0] + gvC[i][1] * ksi[1];
+                gf += gvC[i][2] * ksi[2];
+                gf = 2.e0 * gf * mk;
+              }
+              r = gf / du - 1.0e0;
+              /* limitFaceBase, CellLib.c:4482-4530 (min/max of Define.h:455-456) */
+              switch (o->adv_fn) {
+                case 1: a = fabs(r); lim = (r + a) / (1.0e0 + a); break;
+                case 2: if (r > 0.e0) { a = r * r; lim = (r + a) / (1.0e0 + a); } break;
+                case 3: a = r < 1.e0 ? r : 1.e0; lim = 0.e0 > a ? 0.e0 : a; break;
+                case 4: a = r < 2.e0 ? r : 2.e0; lim = 0.e0 > a ? 0.e0 : a; break;
+                default:
+                  a = 2.e0 * r < 1.e0 ? 2.e0 * r : 1.e0;
+                  b = r < 2.e0 ? r : 2.e0;
+                  c = a > b ? a : b;
+                  lim = 0.e0 > c ? 0.e0 : c;
+                  break;
+              }
+              cvc[i] = 0.5e0 * lim * du;
+              cvc[i] -= gvc[i][0] * vs[0] + gvc[i][1] * vs[1] + gvc[i][2] * vs[2];
             } else if (o->adv == 5) { /* faceBaseNvd, CellLib.c:4900-4937 */
               double gf, phi, w[2];
               if (cv < 0.e0) {

@@ -293,7 +293,7 @@ class PresPlan(DifPlan):
 
 
 SIMPLE, SIMPLEC = 1, 2  # Define.h:223-224
-FOUP, CD, SOUP, NVD, LUST = 1, 2, 3, 5, 6  # advection schemes (Advection.iCod1), Define.h:267-272
+FOUP, CD, SOUP, TVD, NVD, LUST = 1, 2, 3, 4, 5, 6  # advection schemes (Advection.iCod1), Define.h:267-272
 
 
 class VelPlan(DifPlan):

@@ -37,7 +37,7 @@ namespace {
 
 constexpr int kMaxViz = 8;        // face slots per cell handled
 constexpr int kGeo = 9;           // geometry fields per (face, row): diffusion, pressure
-constexpr int kGeoVel = 19;       // momentum
+constexpr int kGeoVel = 22;       // momentum
 constexpr int kMaxLoads = 32;     // entries of the load table
 constexpr int32_t kFlagP = 0x40000000;  // neighbour whose equation id is -1
 
@@ -230,11 +230,13 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
           g[3 + j] = ksi[j];
           g[6 + j] = t[j];
         }
-        if (kind == 2) {  // [9..11] normal, 12 area, [13..15] xmcc, [16..18] xm - c_V
+        if (kind == 2) {  // [9..11] normal, 12 area, [13..15] xmcc, [16..18] xm - c_V,
+                          // [19..21] the face's skew vector (TVD)
           for (int j = 0; j < 3; ++j) {
             g[9 + j] = nrm[j];
             g[13 + j] = m.xmcc[3 * q + j];
             g[16 + j] = xsub(m.xm[3 * face + j], m.cc[3 * static_cast<size_t>(viz) + j]);
+            g[19 + j] = m.vskew[3 * face + j];
           }
           g[12] = area;
         }
@@ -792,6 +794,35 @@ __device__ __noinline__ void advection_correction(int adv, double cv, double am1
       for (int j = 0; j < 3; ++j) gu[j] = down ? gvV[3 * i + j] : gvC[3 * i + j];
       cvc[i] = dot3(gu, rr);
     }
+  } else if (adv == 4) {  // faceBaseTvdV1 (CellLib.c:4845-4875) with limitFaceBase
+    double ksi[3];
+    for (int j = 0; j < 3; ++j) ksi[j] = __ldcs(g + (3 + j) * fs);
+    const double mk = __ldcs(g + 2 * fs);
+    const bool down = cv < 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const double du = xadd(down ? xsub(velC[i], velV[i]) : xsub(velV[i], velC[i]), 1.e-14);
+      const double gf0 = dot3(down ? gvV + 3 * i : gvC + 3 * i, ksi);
+      const double gf = xmul(xmul(down ? -2.0 : 2.0, gf0), mk);
+      const double r = xsub(xdiv(gf, du), 1.0);
+      double lim = 0.0;  // limitFaceBase (CellLib.c:4482-4530); min/max as Define.h:455-456
+      if (nvd == 1) {
+        const double a = fabs(r);
+        lim = xdiv(xadd(r, a), xadd(1.0, a));
+      } else if (nvd == 2) {
+        if (r > 0.0) {
+          const double a = xmul(r, r);
+          lim = xdiv(xadd(r, a), xadd(1.0, a));
+        }
+      } else if (nvd == 3 || nvd == 4) {
+        const double cap = nvd == 3 ? 1.0 : 2.0, mn = r < cap ? r : cap;
+        lim = 0.0 > mn ? 0.0 : mn;
+      } else if (nvd == 5) {
+        const double r2 = xmul(2.0, r);
+        const double a = r2 < 1.0 ? r2 : 1.0, b = r < 2.0 ? r : 2.0, c = a > b ? a : b;
+        lim = 0.0 > c ? 0.0 : c;
+      }
+      cvc[i] = xmul(xmul(0.5, lim), du);
+    }
   } else if (adv == 5) {  // faceBaseNvd (CellLib.c:4900-4937), the cell as uP
     double ksi[3];
     for (int j = 0; j < 3; ++j) ksi[j] = __ldcs(g + (3 + j) * fs);
@@ -910,6 +941,10 @@ __global__ void __launch_bounds__(256, 2)
         const double du = xsub(xdiv(xsub(velV[i], velC[i]), mk), dot3(gf, ksi));
         for (int j = 0; j < 3; ++j) gvc[3 * i + j] = xadd(gf[j], xmul(du, ksi[j]));
         const double dfdc = xmul(visc, dot3(gvc + 3 * i, t));
+        if (kExt && o.adv == 4) {  // TVD: minus the compact gradient along the skew vector
+          const double vs[3] = {__ldcs(g + 19 * fs), __ldcs(g + 20 * fs), __ldcs(g + 21 * fs)};
+          cvc[i] = xsub(cvc[i], dot3(gvc + 3 * i, vs));
+        }
         pp[i] = xadd(pp[i], xsub(dfdc, xmul(cv, cvc[i])));  // p += dfdc - cv cvc
       }
       // facePressure (CellLib.c:7499), interior
@@ -1637,9 +1672,10 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if (rc != SFR_OK) return rc;
   if (calrcell && p->free_cells > 0)
     SFR_CUA(cudaMemsetAsync(d_rcell3, 0, sizeof(double) * 3 * p->numel, st));
-  if (o->adv < 0 || o->adv == 4 || o->adv > 6)
-    return bad("adv: FoUp (0 or 1), CD (2), SoUp (3), NVD (5) or LUST (6); TVD is not built");
+  if (o->adv < 0 || o->adv > 6)
+    return bad("adv: FoUp (0 or 1), CD (2), SoUp (3), TVD (4), NVD (5) or LUST (6)");
   if (o->adv == 5 && (o->adv_fn < 1 || o->adv_fn > 9)) return bad("adv_fn: NVD function 1..9");
+  if (o->adv == 4 && (o->adv_fn < 1 || o->adv_fn > 5)) return bad("adv_fn: TVD limiter 1..5");
   if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
     return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,

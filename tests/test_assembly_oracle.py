@@ -255,9 +255,10 @@ def test_vel_oracle_advection_schemes_match_reference_live():
             assert r1[0] == r2[0] == 0
             for x, y in zip(r1[1:], r2[1:6]):
                 assert bits_equal(x, y), (adv, icod, fso, ts, name)
-        # NVD with each of its functions (MUSCL and STOIC weigh 0, as in the reference)
+        # NVD with each of its functions (MUSCL and STOIC weigh 0, as in the reference),
+    # TVD with each of its limiters
     st, un, ia_, ja_, _al, _au = lay["csrd_full"]
-    for fn in range(1, 10):
+    for adv, fn in [(O.NVD, k) for k in range(1, 10)] + [(O.TVD, k) for k in range(1, 6)]:
         case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 2, 1, 3, 1]),
                          facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop,
                          pres=rng.standard_normal(m.numel),
@@ -265,14 +266,14 @@ def test_vel_oracle_advection_schemes_match_reference_live():
                          vel=rng.standard_normal((m.numel, 3)),
                          gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.3,
                          dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7,
-                         adv=O.NVD, adv_fn=fn)
+                         adv=adv, adv_fn=fn)
         for name in ("csrd_full", "csrc_unsym"):
             st, un, ia_, ja_, _al, _au = lay[name]
             r1 = O.vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
             r2 = O.ref_vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
             assert r1[0] == r2[0] == 0
             for x, y in zip(r1[1:], r2[1:6]):
-                assert bits_equal(x, y), ("nvd", fn, name)
+                assert bits_equal(x, y), (adv, fn, name)
     # the schemes change b (the deferred correction), not the matrix
         f = O.vel_assemble(O.VelCase(**{**case.__dict__, "adv": O.FOUP}), O.CSRD, True,
                            s.ia, s.ja, s.neq)
@@ -338,7 +339,8 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     assert run(lvel=[O.Load(O.OUTLET, ())]) == -2
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
     assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
-    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4) == -1  # TVD not restated
+    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4, adv_fn=6) == -1  # no such limiter
+    assert run(lvel=[O.Load(O.STATICWALL, ())], adv=7) == -1  # no such scheme
     assert run(lvel=[O.Load(O.STATICWALL, ())], adv=5, adv_fn=10) == -1  # no such function
     assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
                           O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1

@@ -504,7 +504,7 @@ def test_vel_matches_oracle(cuda, box, icod):
         gs.close()
 
 
-@pytest.mark.parametrize("adv", [O.CD, O.SOUP, O.LUST, O.NVD])
+@pytest.mark.parametrize("adv", [O.CD, O.SOUP, O.LUST, O.NVD, O.TVD])
 def test_vel_advection_schemes_match_oracle(cuda, box, adv):
     s, m, lay = box
     rng = np.random.default_rng(60 + adv)
@@ -524,7 +524,8 @@ def test_vel_advection_schemes_match_oracle(cuda, box, adv):
                              gradvel=rng.standard_normal((m.numel, 3, 3)),
                              dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, fso=bool(fso),
                              type_simple=ts, under=0.7, adv=adv, adv_beta=0.3,
-                             adv_fn=3 + fso + 2 * (ts == A.SIMPLEC))
+                             adv_fn=(3 + fso + 2 * (ts == A.SIMPLEC)) if adv != O.TVD
+                             else 1 + fso + 2 * (ts == A.SIMPLEC))
             want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
             assert want[0] == 0
             ad3, b3, rc3, df = plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres,
@@ -539,7 +540,7 @@ def test_vel_advection_schemes_match_oracle(cuda, box, adv):
             assert bits_equal(rc3, want[4]) and bits_equal(df, want[5]), what
         with pytest.raises(sv.SolverError):
             plan.assemble(_aloads(VLOADS), prop, case.pres, case.gradpres, case.vel,
-                          case.gradvel, case.dfield, adv=4)
+                          case.gradvel, case.dfield, adv=7)
         plan.close()
         gs.close()
 
