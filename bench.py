@@ -298,6 +298,10 @@ def run_ours(args):
                      "inner_iters": mi[-1].inner_iters,
                      "refinements": mi[-1].refinements,
                      "status": mi[-1].status,
+                     "stopping_test": "reference's PCG criterion on the FP64 true residual: "
+                                      "sqrt|(r, M^-1 r)| < 1e-10 sqrt|(b, M^-1 b)| (Cg.c:145)",
+                     "true_relres_Mnorm": (mi[-1].norm_r_m / (mi[-1].conv / 1e-10)
+                                           if mi[-1].conv > 0 else None),
                      "true_relres_2norm": mi[-1].relres,
                      "err_vs_fp64_x": float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64)),
                      "speedup_vs_fp64": ms_step / max(m_ms, 1e-9),
@@ -371,7 +375,10 @@ def run_ours(args):
     # CPU baseline: the reference's own pcgOmp on this host (rank 0, N = 1)
     cpu = None
     if not args.no_cpu and extras:
-        cpu = cpu_baseline(s, iters, n)
+        xs_gpu = {"fp64": x.cpu().numpy()}
+        if mixed and "ms" in mixed:
+            xs_gpu["mixed"] = xm.cpu().numpy()
+        cpu = cpu_baseline(s, iters, n, xs_gpu)
 
     if rank != 0:
         if world > 1:
@@ -1047,10 +1054,12 @@ def cpu_other_krylov(O, s, n, threads):
     return out
 
 
-def cpu_baseline(s, iters_full, n):
+def cpu_baseline(s, iters_full, n, xs_gpu=None):
     """The reference's pcgOmp on the bench system (cpu_pcg_baseline), plus
-    its other Krylov methods on the other_krylov workloads."""
-    res = cpu_pcg_baseline(s, iters_full)
+    its other Krylov methods on the other_krylov workloads.  xs_gpu: the
+    GPU's solutions ({"fp64": x, "mixed": x}), whose error against the
+    reference's solution is reported (computed outside every timed region)."""
+    res = cpu_pcg_baseline(s, iters_full, xs_gpu)
     if "unavailable" not in res:
         from oracle import oracle as O
         res["other_krylov"] = cpu_other_krylov(O, s, n, res["cores"])
@@ -1058,7 +1067,7 @@ def cpu_baseline(s, iters_full, n):
     return res
 
 
-def cpu_pcg_baseline(s, iters_full):
+def cpu_pcg_baseline(s, iters_full, xs_gpu=None):
     """The reference's own pcgOmp (Cg.c:490) with all host threads on the
     same system in CSRC symmetric storage (the reference's default): a full
     solve when one takes under 30 s, else a bounded sample scaled to the
@@ -1077,10 +1086,19 @@ def cpu_pcg_baseline(s, iters_full):
     if per_it * iters_full < 30:
         r = O.ref_solve(O.PCG, O.CSRC, False, il, jl, al, s.ad, s.b[0], tol=1e-10,
                         maxit=100000, nthreads=threads)
-        return {"value": r.seconds * 1e3, "unit": "ms", "cores": threads, "kind": "reference",
-                "sample": f"one full pcgOmp solve (CSRC symmetric, {threads} threads), "
-                          f"{r.iters} iterations",
-                "ms_per_iteration": r.seconds / r.iters * 1e3}
+        out = {"value": r.seconds * 1e3, "unit": "ms", "cores": threads, "kind": "reference",
+               "sample": f"one full pcgOmp solve (CSRC symmetric, {threads} threads), "
+                         f"{r.iters} iterations",
+               "ms_per_iteration": r.seconds / r.iters * 1e3,
+               "iterations": r.iters}
+        if xs_gpu:
+            import numpy as np
+            nref = float(np.linalg.norm(r.x))
+            out["err_vs_oracle_x"] = {
+                k: float(np.linalg.norm(v - r.x) / nref) for k, v in xs_gpu.items()}
+            out["err_vs_oracle_x"]["what"] = ("||x_gpu - x_ref||_2 / ||x_ref||_2 against this "
+                                              "pcgOmp solve; FP64 bar 1e-12")
+        return out
     n_it = max(100, int(30 / per_it))
     r = O.ref_solve(O.PCG, O.CSRC, False, il, jl, al, s.ad, s.b[0], tol=1e-10,
                     maxit=n_it, nthreads=threads)

@@ -226,10 +226,12 @@ int sfr_gpu_dot(const double *d_a, const double *d_b, int32_t n,
  * while another allocator holds the memory).  No counterpart in the
  * reference.  Never calls cudaMalloc/cudaFree: its scratch is a fixed
  * 4,752-byte device array (592 block partials, result, counter) that every
- * GPU loading the library keeps until exit.  The first call on a device
- * looks up that array's address; make it before any stream capture.  Calls
- * share the array, so calls that overlap on the GPU race.  n < 0 is
- * rejected with SFR_BAD_INPUT. */
+ * GPU loading the library keeps until exit.  Same launch shape as
+ * sfr_gpu_dot, so the same bits.  The first call on a device looks up that
+ * array's address and keeps it (cudaDeviceReset is not supported after
+ * it); make it before any stream capture.  Calls share the array, so calls
+ * that overlap on the GPU race.  n < 0, or a GPU with more than 148 SMs
+ * (more partials than the array holds), is rejected with SFR_BAD_INPUT. */
 int sfr_gpu_dot_noalloc(const double *d_a, const double *d_b, int32_t n,
                         double *dot_out, void *stream);
 

@@ -158,6 +158,9 @@ int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
 int dot_host(const double *d_a, const double *d_b, int32_t n, double *h_out,
              cudaStream_t st);
 int num_sms(int device);
+// Blocks of the standalone dot / SpMV+dot kernels (256 threads each) for n
+// elements on `device`: 4 per SM of the device, at most one per 256 elements.
+int stat_grid(int device, int64_t n);
 // adjoint.cu: dJ/d(value source) and dJ/d(ad) from lam and x (device arrays)
 int adjoint_gradients(sfr_system *s, const double *d_lam, const double *d_x, double *d_gsrc,
                       double *d_gad, cudaStream_t st);

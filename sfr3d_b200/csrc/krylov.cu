@@ -599,9 +599,19 @@ int num_sms(int device) {
   return v;
 }
 
+// standalone kernels: 4 blocks of 256 threads per SM (the device's own SM
+// count); the scratch holds partials for GPUs of up to 256 SMs
+constexpr int kStatBlocksPerSm = 4;
+constexpr int kStatGrid = kStatBlocksPerSm * 256;
+
+int stat_grid(int device, int64_t n) {
+  const int64_t cap = static_cast<int64_t>(kStatBlocksPerSm) * std::max(1, num_sms(device));
+  const int64_t want = (std::max<int64_t>(n, 0) + 255) / 256;
+  return static_cast<int>(std::max<int64_t>(1, std::min({cap, want, int64_t{kStatGrid}})));
+}
+
 namespace {
 
-constexpr int kStatGrid = 4 * 148;  // standalone kernels: 4 blocks per SM
 // automatic engine choice: the graph engine from this many rows up
 constexpr int kGraphEngineRows = 100000;
 
@@ -630,9 +640,8 @@ int scratch_for(int device, Scratch **s) {
 }
 
 int grid_for_slices(int nslices, int device) {
-  const int sms = std::max(1, num_sms(device));
   const int want = (nslices + 7) / 8;  // 8 warps per 256-thread block
-  return std::max(1, std::min(want, kStatGrid > 4 * sms ? 4 * sms : kStatGrid));
+  return std::max(1, std::min(want, stat_grid(device, INT64_MAX)));
 }
 
 template <typename F>
@@ -682,7 +691,7 @@ int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot, c
   Scratch *sc = nullptr;
   int rc = scratch_for(dev, &sc);
   if (rc != SFR_OK) return rc;
-  const int grid = std::max(1, std::min(kStatGrid, (n + 255) / 256));
+  const int grid = stat_grid(dev, n);
   dot_kernel<<<grid, 256, 0, st>>>(d_a, d_b, n, sc->part, sc->counter, d_dot);
   return cudaGetLastError() == cudaSuccess ? SFR_OK : SFR_CUDA_ERROR;
 }

@@ -12,20 +12,23 @@
 // Limits and rules:
 //   * The scratch is 594 doubles (4,752 bytes) held by every GPU that loads
 //     the library until the process exits: 592 block partials, one result,
-//     one arrival counter.  The launch uses at most 592 blocks (the same
-//     launch shape as sfr_gpu_dot, so both return the same bits); a request
-//     that would need more blocks, or a negative length, is rejected with
-//     SFR_BAD_INPUT before anything runs.
+//     one arrival counter.  The launch takes the same shape as sfr_gpu_dot
+//     (4 blocks of 256 threads per SM, at most one block per 256 elements),
+//     so both return the same bits; 592 partials cover a GPU of up to 148
+//     SMs (a B200).  On a GPU with more SMs, or for a negative length, the
+//     call returns SFR_BAD_INPUT, with the reason in sfr_last_error(),
+//     before anything runs.
 //   * The first call on a device looks up the array's device address (one
-//     cudaGetSymbolAddress with that device current).  Make that first call
-//     before any stream capture starts.
+//     cudaGetSymbolAddress with that device current) and keeps it for the
+//     life of the process.  Make that first call before any stream capture
+//     starts.  cudaDeviceReset is not supported afterwards: the kept address
+//     would go stale.
 //   * Every call shares the one array and it keeps the last call's contents;
 //     the arrival counter is cleared at the start of each call.  Calls whose
 //     kernels overlap on the GPU (different streams, or different host
 //     threads) race on the array: serialise them.
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <mutex>
 
 #include "internal.h"
@@ -62,12 +65,21 @@ int scratch_address(int device, double **out) {
 extern "C" int sfr_gpu_dot_noalloc(const double *d_a, const double *d_b, int32_t n,
                                    double *dot_out, void *stream) {
   if (!d_a || !d_b || !dot_out) return SFR_BAD_INPUT;
-  if (n < 0) return SFR_BAD_INPUT;
-  const int grid = std::max(1, std::min(kNoAllocBlocks, (n + kNoAllocThreads - 1) / kNoAllocThreads));
-  if (grid + 2 > kNoAllocSlots) return SFR_BAD_INPUT;  // beyond the fixed scratch
+  if (n < 0) {
+    sfr::set_last_error("sfr_gpu_dot_noalloc: negative length");
+    return SFR_BAD_INPUT;
+  }
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return SFR_CUDA_ERROR;
   if (device < 0 || device >= kMaxDevices) return SFR_BAD_INPUT;
+  // sfr_gpu_dot's launch shape; its partials must fit the fixed scratch
+  const int grid = sfr::stat_grid(device, n);
+  static_assert(kNoAllocThreads == 256, "the launch shape of sfr_gpu_dot");
+  if (grid > kNoAllocBlocks) {
+    sfr::set_last_error("sfr_gpu_dot_noalloc: the device has more SMs than the fixed scratch "
+                        "holds partials for (148)");
+    return SFR_BAD_INPUT;
+  }
   double *scratch = nullptr;
   const int rc = scratch_address(device, &scratch);
   if (rc != SFR_OK) return rc;

@@ -22,7 +22,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("REF", "/root/reference")
+# the reference checkout: $SFR3D_REFERENCE, else "reference" beside the repository
+REF = os.environ.get("SFR3D_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+if not os.path.isdir(os.path.join(REF, "src")):
+    sys.exit(f"make_cavity_golden: no reference checkout at {REF} (set SFR3D_REFERENCE)")
 WORK = os.path.join(ROOT, "oracle", "_ref", "cavity")
 
 
