@@ -65,6 +65,8 @@ def parse_args(argv=None):
     ap.add_argument("--threads", type=int, default=0, help="graph-engine block size (0: default)")
     ap.add_argument("--spw", type=int, default=0, help="SELL slices per warp (0: default)")
     ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (untimed) before the timed solves")
     return ap.parse_args(argv)
 
 
@@ -263,6 +265,15 @@ def run_ours(args):
         barrier()
         return [a.elapsed_time(c) for a, c in ev], infos
 
+    # the autotuner picks the engine and launch shape on this system
+    # (untimed); the timed solves below take its choice
+    tune = None
+    if args.engine == 0 and not args.no_tune:
+        tune = {"headline_fp64": g.autotune(sv.PCG, s.b[0], tol=1e-10, maxit=args.maxit)}
+        if not args.no_mixed:
+            tune["headline_mixed"] = g.autotune(sv.PCG, s.b[0], tol=1e-10, maxit=args.maxit,
+                                                precision=sv.MIXED)
+
     gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
     clocks = ClockSampler(gpu_uuid if gpu_uuid.startswith("GPU-") else f"GPU-{gpu_uuid}")
     clocks.start()
@@ -327,7 +338,7 @@ def run_ours(args):
         assembly["momentum"] = momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["simple_step"] = simple_step_leg(np, torch, sv, s, n)
         partitioned = partitioned_leg(np, sv, s, n, ms_step, x.cpu().numpy())
-        momentum = momentum_leg(np, torch, sv, S, n, local)
+        momentum = momentum_leg(np, torch, sv, S, n, local, tune=not args.no_tune)
         batch = batch_leg(sv, S)
         adjoint = adjoint_leg(np, sv, S)
         if mixed and "ms" in mixed and momentum:
@@ -350,6 +361,8 @@ def run_ours(args):
         h_x = torch.zeros(N, dtype=torch.float64).pin_memory()
         L = sv.lib()
         L.sfr_set_exit_on_failure(0)
+        # the drop-in tunes the pattern's first solve (a warm-up call)
+        L.sfr_set_autotune(0 if args.no_tune or args.engine != 0 else 1)
 
         def call():
             return L.sfr_solverC(None, N, N, len(jl), 0, h_ia.data_ptr(), h_ja.data_ptr(),
@@ -370,6 +383,7 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h_al.numel() * 8 + h_ad.numel() * 8 + h_b.numel() * 8),
                "d2h_bytes_per_step": int(h_x.numel() * 8),
                "api": "sfr_solverC (solverC drop-in), CSRD symmetric storage, FP64"}
+        L.sfr_set_autotune(0)
         sv.release_cache()
 
     # CPU baseline: the reference's own pcgOmp on this host (rank 0, N = 1)
@@ -434,6 +448,7 @@ def run_ours(args):
         "other_krylov": other,
         "assembly": assembly,
         "target_mixed_batched_vs_fp64": target,
+        "autotune": tune,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": args.steps * pcg_kernel_launches(iters),
@@ -520,13 +535,18 @@ def partitioned_leg(np, sv, s, n, fp64_ms, x64):
     return out
 
 
-def momentum_leg(np, torch, sv, S, n, device):
+def momentum_leg(np, torch, sv, S, n, device, tune=True):
     """128^3 momentum (Peclet 50, nu 1e-3, dt 1e-2), three right-hand sides:
-    FP64 one right-hand side at a time vs one K = 3 mixed launch."""
+    FP64 one right-hand side at a time vs one K = 3 mixed launch.  With
+    `tune`, the K = 3 solves run on the autotuner's choice (tuned untimed)."""
     m = S.momentum(n, nrhs=3, seed=3)
     g = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=device)
     g.set_values(m.al, m.ad)
     out = {"workload": f"momentum {n}^3 Peclet 50, 3 RHS, Jacobi-BiCGSTAB to 1e-10"}
+    if tune:
+        out["autotune"] = {
+            "k3_fp64": g.autotune(sv.PBICGSTAB, m.b, tol=1e-10),
+            "k3_mixed": g.autotune(sv.PBICGSTAB, m.b, tol=1e-10, precision=sv.MIXED)}
     for _ in range(2):  # warm-up: graphs built, clocks up
         for k in range(3):
             g.solve(sv.PBICGSTAB, m.b[k], tol=1e-10)
@@ -568,6 +588,7 @@ def batch_leg(sv, S):
         ms = g.autotune(sv.PCG, bs, tol=1e-10, precision=prec)
         _, infos = g.solve(sv.PCG, bs, tol=1e-10, precision=prec)
         out[name] = {"ms": infos[0].seconds * 1e3, "autotune_best_ms": ms,
+                     "autotune": g.tune_report(),
                      "max_iters": max(i.iters for i in infos),
                      "all_converged": all(i.status == sv.OK for i in infos)}
     out["grid_blocks"] = g.stats()["grid"]

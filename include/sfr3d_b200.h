@@ -149,6 +149,38 @@ int sfr_gpu_solve_multi_device(sfr_system *s, int32_t solver, int32_t k, const d
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
                        int32_t slices_per_warp);
 
+/* Result of sfr_gpu_autotune. */
+typedef struct {
+  int32_t engine;           /* chosen engine: 1 persistent, 2 graph, 4 resident */
+  int32_t threads;          /* graph engine block size */
+  int32_t slices_per_warp;  /* graph engine SpMV phases: 0 one wave, else slices per warp */
+  double ms;                /* the choice's solve time (ms, CUDA events) */
+  int32_t default_engine, default_threads, default_slices_per_warp;
+  double default_ms;        /* the automatic choice's solve time (0 when not measured) */
+  int32_t candidates;       /* candidates timed (0: taken from a cache) */
+  int32_t source;           /* 0 measured, 1 this handle's table, 2 the SFR_TUNE_CACHE file */
+} sfr_tune_result;
+
+/* Autotune how this system's solves of one kind (solver, k right-hand
+ * sides, own or per-RHS diagonals, precision) run: the engine (persistent,
+ * graph, resident) and the graph engine's block size and SELL slices per
+ * warp, each candidate timed on the caller's own right-hand sides b (k*neq
+ * host doubles; ad_k NULL or k*neq per-RHS diagonals).  The automatic choice
+ * is kept unless a candidate is more than 2 % faster.  The choice is kept in
+ * the handle -- later solves with engine 0 (automatic) take it -- and, when
+ * the environment variable SFR_TUNE_CACHE names a file, appended there and
+ * read back by later tunes of the same system size, pattern, storage, kind
+ * of solve and GPU, so the choice is fixed across processes.  No
+ * counterpart in the reference, whose OpenMP solvers balance rows by
+ * nonzeros (partitionCsrByNonzeros, Csr.c:1827-1942).  PCG and BiCGSTAB
+ * only (SFR_UNSUPPORTED otherwise). */
+int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const double *ad_k,
+                     const double *b, double tol, uint32_t maxit, int32_t precision,
+                     sfr_tune_result *out);
+/* Forget this handle's autotuned choices (the automatic choice by size
+ * applies again). */
+int sfr_gpu_autotune_clear(sfr_system *s);
+
 /* Solve A^T x = b (host arrays) with the same Krylov path.  The reference
  * has no transpose solve; this serves the adjoint below. */
 int sfr_gpu_solve_transpose(sfr_system *s, int32_t solver, const double *b,
@@ -194,11 +226,29 @@ int sfr_gpu_batch_solve(sfr_batch *b, int32_t solver, const double *const *bv,
                         int32_t newx, int32_t precision, sfr_solve_info *info);
 /* Work weights of the systems (blocks are shared out in proportion). */
 int sfr_gpu_batch_set_weights(sfr_batch *b, const double *w);
-/* Measure per-system iterations on bv, weight teams by slices x iterations,
- * keep whichever plan solves faster; *ms_out = its solve time. */
+/* Autotune the launch plan on bv: the batch takes as long as its slowest
+ * team, so the blocks are shared out to equalise the teams' times, which
+ * each team measures inside the launch.  Plans tried: the default (blocks by
+ * slices x n^(1/3)), blocks by slices x measured iterations, then up to three
+ * plans from a fitted model t_s(B) = f_s + w_s / B of each team's time
+ * against its block count.  The fastest plan measured is kept for later
+ * solves; *ms_out = its solve time.  The reference balances its OpenMP rows
+ * by nonzeros (partitionCsrByNonzeros, Csr.c:1827-1942); here the balance is
+ * by measured time. */
 int sfr_gpu_batch_autotune(sfr_batch *b, int32_t solver,
                            const double *const *bv, double tol,
                            uint32_t maxit, int32_t precision, double *ms_out);
+/* Report of the last sfr_gpu_batch_autotune. */
+typedef struct {
+  double default_ms;   /* blocks by the default work estimate */
+  double weighted_ms;  /* blocks by slices x measured iterations */
+  double tuned_ms;     /* the plan kept (fastest measured) */
+  int32_t plans;       /* plans measured */
+  int32_t kept;        /* 0 default, 1 weighted, 2.. a model round */
+  int32_t grid;        /* blocks of the kept plan */
+  int32_t max_team_blocks, min_team_blocks;
+} sfr_batch_tune;
+int sfr_gpu_batch_tune_report(const sfr_batch *b, sfr_batch_tune *out);
 int sfr_gpu_batch_stats(const sfr_batch *b, int32_t *grid, int64_t *rows,
                         int64_t *bytes);
 int sfr_gpu_batch_destroy(sfr_batch *b);
@@ -607,6 +657,10 @@ void sfr_set_reliable_delta(double delta);
 int sfr_set_solver_reliable_delta(int32_t solver, double delta);
 /* Precision used by sfr_solverC (SFR_FP64 default). */
 void sfr_set_precision(int32_t precision);
+/* flag != 0: sfr_solverC autotunes (sfr_gpu_autotune) the first PCG or
+ * BiCGSTAB solve of each pattern it caches, on that call's own right-hand
+ * side, and every later call takes the choice.  Off by default. */
+void sfr_set_autotune(int32_t flag);
 /* Release every pattern sfr_solverC cached. */
 void sfr_solverC_release(void);
 

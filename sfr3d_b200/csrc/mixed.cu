@@ -179,6 +179,7 @@ __device__ void finish(const MixedArgs &a, const Team &t, const int (&iters)[K],
       o.bnorm = bnorm[k];
       o.refinements = refine[k];
       o.inner_iters = iters[k];
+      o.team_ms = (global_ns() - t.t0) * 1e-6;
       a.out[t.sys * K + k] = o;
     }
   }

@@ -18,7 +18,15 @@ struct SolveOut {
   double bnorm;        // ||b||_2
   int refinements;     // mixed: reliable updates (FP64 residual recomputations)
   int inner_iters;     // mixed: FP32 iterations
+  double team_ms;      // batched launch: the team's time from launch to its result
 };
+
+// The GPU's nanosecond clock (comparable across SMs).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Rows owned by this thread: warps of the block walk the block's slices, a
 // lane takes one row of its slice.  Defines s_ (slice) and row_ (row < n).
@@ -43,11 +51,13 @@ struct Team {
   int sys;      // system index (0 for a single system)
   int row_end;  // rows of the system end here (global row numbering)
   GridSync gs;  // the team's barrier
+  unsigned long long t0;  // this block's start (global_ns)
 };
 
 __device__ __forceinline__ Team make_team(const TeamTable &tt, const GridSync &global,
                                           int nslices, int n) {
   Team t;
+  t.t0 = global_ns();
   t.gs = global;
   if (!tt.block) {
     block_slices(nslices, &t.s0, &t.s1);

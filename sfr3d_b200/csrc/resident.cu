@@ -455,6 +455,7 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
     o.bnorm = bnorm;
     o.refinements = refine;
     o.inner_iters = static_cast<int>(iters);
+    o.team_ms = 0.0;
     *a.out = o;
   }
 }

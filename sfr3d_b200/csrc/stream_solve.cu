@@ -585,6 +585,7 @@ __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
       o.bnorm = st->bnorm[k];
       o.refinements = st->refine[k];
       o.inner_iters = st->iters[k];
+      o.team_ms = 0.0;
       st->out[k] = o;
     }
   }

@@ -54,6 +54,23 @@ class SolveInfo:
         return cls(**{f: getattr(c, f) for f, _ in SolveInfoC._fields_})
 
 
+class TuneResultC(ctypes.Structure):
+    _fields_ = [("engine", _I32), ("threads", _I32), ("slices_per_warp", _I32),
+                ("ms", ctypes.c_double), ("default_engine", _I32),
+                ("default_threads", _I32), ("default_slices_per_warp", _I32),
+                ("default_ms", ctypes.c_double), ("candidates", _I32), ("source", _I32)]
+
+
+class BatchTuneC(ctypes.Structure):
+    _fields_ = [("default_ms", ctypes.c_double), ("weighted_ms", ctypes.c_double),
+                ("tuned_ms", ctypes.c_double), ("plans", _I32), ("kept", _I32),
+                ("grid", _I32), ("max_team_blocks", _I32), ("min_team_blocks", _I32)]
+
+
+def _struct_dict(c):
+    return {name: getattr(c, name) for name, _ in c._fields_}
+
+
 class SolverError(RuntimeError):
     def __init__(self, status: int, what: str):
         super().__init__(f"{what}: {status_string(status)} ({last_error()})")
@@ -105,6 +122,10 @@ def lib() -> ctypes.CDLL:
     L.sfr_gpu_batch_autotune.argtypes = [_P, _I32, _P, ctypes.c_double,
                                          ctypes.c_uint32, _I32, _P]
     L.sfr_gpu_batch_stats.argtypes = [_P, _P, _P, _P]
+    L.sfr_gpu_batch_tune_report.argtypes = [_P, _P]
+    L.sfr_gpu_autotune.argtypes = [_P, _I32, _I32, _P, _P, ctypes.c_double, ctypes.c_uint32,
+                                   _I32, _P]
+    L.sfr_gpu_autotune_clear.argtypes = [_P]
     L.sfr_gpu_batch_destroy.argtypes = [_P]
     L.sfr_set_exit_on_failure.argtypes = [_I32]
     L.sfr_set_exit_on_failure.restype = None
@@ -117,6 +138,8 @@ def lib() -> ctypes.CDLL:
     L.sfr_write_coo_b.argtypes = [ctypes.c_char_p, _P, _I32]
     L.sfr_gpu_write_coo.argtypes = [_P, ctypes.c_char_p, _P, _P, _I32]
     L.sfr_set_precision.restype = None
+    L.sfr_set_autotune.argtypes = [_I32]
+    L.sfr_set_autotune.restype = None
     L.sfr_solverC_set_group.argtypes = [_P]
     L.sfr_solverC_release.restype = None
     L.sfr_solverC_release.argtypes = []
@@ -193,6 +216,26 @@ class GpuSystem:
         rc = lib().sfr_gpu_set_engine(self.h, engine, threads, slices_per_warp)
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_engine")
+
+    def autotune(self, solver: int, b, ad_k=None, tol: float = 1e-10, maxit: int = 100000,
+                 precision: int = FP64) -> dict:
+        """Time the engines and graph launch shapes on this system's solve
+        of b ((neq,) or (k, neq)) and keep the fastest for later automatic
+        solves of that kind (sfr_gpu_autotune).  Returns the report as a dict:
+        engine, threads, slices_per_warp, ms, the default_* choice and its
+        time, candidates timed and source (0 measured, 1 handle, 2 file)."""
+        b = _f64(b)
+        k = 1 if b.ndim == 1 else b.shape[0]
+        ad_k = _f64(ad_k)
+        out = TuneResultC()
+        rc = lib().sfr_gpu_autotune(self.h, solver, k, _ptr(ad_k), _ptr(b), tol, maxit,
+                                    precision, ctypes.byref(out))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_autotune: " + last_error())
+        return _struct_dict(out)
+
+    def autotune_clear(self):
+        lib().sfr_gpu_autotune_clear(self.h)
 
     def set_values(self, al, ad, au=None):
         al, ad, au = _f64(al), _f64(ad), _f64(au)
@@ -414,6 +457,14 @@ class GpuBatch:
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_batch_autotune")
         return ms.value
+
+    def tune_report(self) -> dict:
+        """The last autotune's plans and times (sfr_gpu_batch_tune_report)."""
+        out = BatchTuneC()
+        rc = lib().sfr_gpu_batch_tune_report(self.h, ctypes.byref(out))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_batch_tune_report")
+        return _struct_dict(out)
 
     def stats(self):
         g, r, b = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()

@@ -1,0 +1,120 @@
+"""Autotuners: sfr_gpu_autotune (engine and graph launch shape of one
+system's solves) and sfr_gpu_batch_autotune (blocks per system of a batched
+launch).
+
+What is checked:
+  * the tuned choice is deterministic for a fixed system: a second tune of
+    the same handle returns the kept choice, and with SFR_TUNE_CACHE a new
+    handle of the same system reads the same choice back from the file;
+  * solves on the tuned choice still meet the FP64 bar against the oracle
+    (1e-12 relative in x, iterations +-1) and repeat bit for bit;
+  * the batch tuner keeps the fastest plan it measured and the tuned batch
+    meets the same FP64 bar.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from helpers import bits_equal, rel
+from oracle import oracle as O
+from sfr3d_b200 import solver as sv
+from sfr3d_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def test_autotune_choice_is_kept_and_solves_at_parity(cuda, tmp_path, monkeypatch):
+    s = S.poisson_jittered(48, seed=21)  # 110,592 rows: the graph engine by default
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("SFR_TUNE_CACHE", str(cache))
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    g.set_values(s.al, s.ad)
+    first = g.autotune(sv.PCG, s.b[0], tol=TOL)
+    assert first["source"] == 0 and first["candidates"] >= 6, first
+    assert first["default_engine"] == sv.ENGINE_GRAPH
+    assert first["ms"] <= first["default_ms"]
+    again = g.autotune(sv.PCG, s.b[0], tol=TOL)
+    assert again["source"] == 1
+    assert (again["engine"], again["threads"], again["slices_per_warp"]) == \
+        (first["engine"], first["threads"], first["slices_per_warp"])
+    # the file holds the choice: a new handle of the same system reads it
+    assert cache.read_text().count(" -> engine=") == 1
+    h = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    h.set_values(s.al, s.ad)
+    third = h.autotune(sv.PCG, s.b[0], tol=TOL)
+    assert third["source"] == 2
+    assert (third["engine"], third["threads"], third["slices_per_warp"]) == \
+        (first["engine"], first["threads"], first["slices_per_warp"])
+    h.close()
+    # solves on the tuned choice: the FP64 bar, and the same bits twice
+    ref = O.pcg(O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=TOL)
+    x1, i1 = g.solve(sv.PCG, s.b[0], tol=TOL)
+    x2, i2 = g.solve(sv.PCG, s.b[0], tol=TOL)
+    assert i1.status == sv.OK and abs(i1.iters - ref.iters) <= 1
+    assert rel(x1, ref.x) < 1e-12
+    assert bits_equal(x1, x2) and i1.iters == i2.iters
+    g.close()
+
+
+@pytest.mark.parametrize("engine,threads,spw", [(2, 128, 0), (2, 256, 2), (2, 256, 8),
+                                                (1, 0, 0)])
+def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw):
+    """Whatever the tuner picks, the arithmetic is the reference's: every
+    candidate engine and launch shape solves at the FP64 bar."""
+    s = S.poisson_jittered(40, seed=22)
+    g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+    g.set_values(s.al, s.ad)
+    g.set_engine(engine, threads, spw if spw else -1)
+    ref = O.pcg(O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=TOL)
+    x, info = g.solve(sv.PCG, s.b[0], tol=TOL)
+    assert info.status == sv.OK and abs(info.iters - ref.iters) <= 1
+    assert rel(x, ref.x) < 1e-12
+    m = S.momentum(24, nrhs=3, seed=23)
+    gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
+    gm.set_values(m.al, m.ad)
+    gm.set_engine(engine, threads, spw if spw else -1)
+    xs, infos = gm.solve_multi(sv.PBICGSTAB, m.b, tol=TOL)
+    for k in range(3):
+        refk = O.pbicgstab(O.CSRD, True, m.ia, m.ja, m.al, m.ad, m.b[k], tol=TOL)
+        assert infos[k].status == sv.OK and abs(infos[k].iters - refk.iters) <= 1
+        assert rel(xs[k], refk.x) < 1e-12
+    g.close()
+    gm.close()
+
+
+def test_autotune_mixed_k3_momentum(cuda):
+    m = S.momentum(40, nrhs=3, seed=24)
+    g = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
+    g.set_values(m.al, m.ad)
+    rep = g.autotune(sv.PBICGSTAB, m.b, tol=TOL, precision=sv.MIXED)
+    assert rep["source"] == 0 and rep["ms"] <= rep["default_ms"]
+    xs, infos = g.solve_multi(sv.PBICGSTAB, m.b, tol=TOL, precision=sv.MIXED)
+    for k in range(3):
+        assert infos[k].status == sv.OK
+        r = m.b[k] - O.matvec(O.CSRD, True, m.ia, m.ja, m.al, m.ad, xs[k])
+        assert np.linalg.norm(r) < TOL * np.linalg.norm(m.b[k])
+    g.close()
+
+
+def test_batch_autotune_keeps_the_fastest_plan(cuda):
+    systems = S.poisson_batch(16, 6, 40, seed=25)
+    g = sv.GpuBatch([(s.neq, s.ia, s.ja) for s in systems], sv.CSRD, True)
+    g.set_values([s.al for s in systems], [s.ad for s in systems])
+    bs = [s.b[0] for s in systems]
+    ms = g.autotune(sv.PCG, bs, tol=TOL)
+    rep = g.tune_report()
+    assert rep["plans"] >= 2
+    assert rep["tuned_ms"] == pytest.approx(ms)
+    assert rep["tuned_ms"] <= min(rep["default_ms"], rep["weighted_ms"])
+    assert rep["min_team_blocks"] >= 1 and rep["grid"] >= len(systems)
+    xs, infos = g.solve(sv.PCG, bs, tol=TOL)
+    for s, x, info in zip(systems, xs, infos):
+        ref = O.pcg(O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=TOL)
+        assert info.status == sv.OK and abs(info.iters - ref.iters) <= 1
+        assert rel(x, ref.x) < 1e-12
+    g.close()
