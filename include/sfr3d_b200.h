@@ -149,13 +149,21 @@ int sfr_gpu_solve_multi_device(sfr_system *s, int32_t solver, int32_t k, const d
 int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
                        int32_t slices_per_warp);
 
+/* Graph engine: in the iteration's SpMV phases each warp prefetches into
+ * L2 (cp.async.bulk.prefetch.L2, one request for a slice's values and one
+ * for its slot columns) the SELL slice it reaches `rounds` rounds later, so
+ * that DRAM reads of the matrix overlap the current slice's gathers.  0
+ * (the default) turns it off; at most 8. */
+int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
+
 /* Result of sfr_gpu_autotune. */
 typedef struct {
   int32_t engine;           /* chosen engine: 1 persistent, 2 graph, 4 resident */
   int32_t threads;          /* graph engine block size */
   int32_t slices_per_warp;  /* graph engine SpMV phases: 0 one wave, else slices per warp */
+  int32_t prefetch;         /* graph engine SpMV-phase L2 prefetch distance (rounds) */
   double ms;                /* the choice's solve time (ms, CUDA events) */
-  int32_t default_engine, default_threads, default_slices_per_warp;
+  int32_t default_engine, default_threads, default_slices_per_warp, default_prefetch;
   double default_ms;        /* the automatic choice's solve time (0 when not measured) */
   int32_t candidates;       /* candidates timed (0: taken from a cache) */
   int32_t source;           /* 0 measured, 1 this handle's table, 2 the SFR_TUNE_CACHE file */

@@ -1,13 +1,15 @@
 // Autotuner of one system's solve: the engine and the graph engine's launch
 // shape, chosen by timing each candidate on the caller's own system.
 //
-// Candidates (PCG and BiCGSTAB, any K, FP64 or mixed):
-//   * the graph engine at 256 and 128 threads a block, with the SpMV phases
-//     as one wave of resident blocks or at 2 or 8 SELL slices (64 or 256
-//     rows) per warp;
-//   * the persistent engine (the whole solve in one cooperative launch);
-//   * the resident engine, for mixed PCG with one right-hand side when the
-//     system fits it.
+// Candidates (PCG and BiCGSTAB, any K, FP64 or mixed), searched in two
+// stages:
+//   1. the graph engine at 256 and 128 threads a block, with the SpMV phases
+//      as one wave of resident blocks or at 2 or 8 SELL slices (64 or 256
+//      rows) per warp; the persistent engine (the whole solve in one
+//      cooperative launch); the resident engine, for mixed PCG with one
+//      right-hand side when the system fits it;
+//   2. when the graph engine leads: its best shape with the SpMV phases'
+//      L2 prefetch 1, 2 or 4 rounds ahead.
 // Each candidate solves the caller's right-hand side once untimed (the graph
 // is built and the clocks are up), then twice timed with CUDA events; its
 // time is the faster of the two.  The automatic choice is kept unless a
@@ -47,9 +49,10 @@ const Tuned *find_tuned(const sfr_system *s, int32_t solver, int32_t k, int32_t 
 namespace {
 
 struct Candidate {
-  int engine, threads, spw;
+  int engine, threads, spw, pf;
   bool operator==(const Candidate &o) const {
-    return engine == o.engine && (engine != 2 || (threads == o.threads && spw == o.spw));
+    return engine == o.engine &&
+           (engine != 2 || (threads == o.threads && spw == o.spw && pf == o.pf));
   }
 };
 
@@ -65,7 +68,7 @@ std::string cache_key(const sfr_system *s, int32_t solver, int32_t k, int32_t pr
     if (c == ' ' || c == '\t') c = '_';
   char buf[512];
   std::snprintf(buf, sizeof(buf),
-                "sfr-tune-v1 gpu=%s sms=%d n=%d slots=%lld nsrc=%d storage=%d unsym=%d "
+                "sfr-tune-v2 gpu=%s sms=%d n=%d slots=%lld nsrc=%d storage=%d unsym=%d "
                 "off16=%d solver=%d k=%d precision=%d own_diag=%d",
                 gpu.c_str(), prop.multiProcessorCount, s->n,
                 static_cast<long long>(s->A.nslots), s->nsrc, s->storage, s->unsym,
@@ -85,14 +88,16 @@ bool file_lookup(const std::string &key, Tuned *t) {
   const std::string head = key + " -> ";
   while (std::fgets(line.data(), static_cast<int>(line.size()), f)) {
     if (std::strncmp(line.data(), head.c_str(), head.size()) != 0) continue;
-    int e = 0, th = 0, sp = 0;
+    int e = 0, th = 0, sp = 0, pf = 0;
     double ms = 0.0;
-    if (std::sscanf(line.data() + head.size(), "engine=%d threads=%d spw=%d ms=%lf", &e, &th,
-                    &sp, &ms) == 4 &&
-        (e == 1 || e == 2 || e == 4) && (th == 128 || th == 256) && sp >= 0 && sp <= 64) {
+    if (std::sscanf(line.data() + head.size(), "engine=%d threads=%d spw=%d pf=%d ms=%lf", &e,
+                    &th, &sp, &pf, &ms) == 5 &&
+        (e == 1 || e == 2 || e == 4) && (th == 128 || th == 256) && sp >= 0 && sp <= 64 &&
+        pf >= 0 && pf <= 8) {
       t->engine = e;
       t->threads = th;
       t->spw = sp;
+      t->pf = pf;
       t->ms = ms;
       found = true;
     }
@@ -107,8 +112,8 @@ void file_store(const std::string &key, const Tuned &t) {
   std::lock_guard<std::mutex> lk(g_file_mu);
   FILE *f = std::fopen(path, "a");
   if (!f) return;
-  std::fprintf(f, "%s -> engine=%d threads=%d spw=%d ms=%.6f\n", key.c_str(), t.engine,
-               t.threads, t.spw, t.ms);
+  std::fprintf(f, "%s -> engine=%d threads=%d spw=%d pf=%d ms=%.6f\n", key.c_str(), t.engine,
+               t.threads, t.spw, t.pf, t.ms);
   std::fclose(f);
 }
 
@@ -129,10 +134,12 @@ void fill(sfr_tune_result *out, const Tuned &t, const Candidate &def, double def
   out->engine = t.engine;
   out->threads = t.threads;
   out->slices_per_warp = t.spw;
+  out->prefetch = t.pf;
   out->ms = t.ms;
   out->default_engine = def.engine;
   out->default_threads = def.threads;
   out->default_slices_per_warp = def.spw;
+  out->default_prefetch = def.pf;
   out->default_ms = def_ms;
   out->candidates = n;
   out->source = source;
@@ -155,7 +162,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   if (cudaSetDevice(s->device) != cudaSuccess) return SFR_CUDA_ERROR;
   const bool own_diag = ad_k == nullptr;
   const Candidate def{auto_engine(s, solver, k, precision, own_diag), s->graph_threads,
-                      s->graph_spw};
+                      s->graph_spw, s->graph_pf};
   if (const Tuned *t = find_tuned(s, solver, k, precision, own_diag)) {
     fill(out, *t, def, 0.0, 0, 1);
     return SFR_OK;
@@ -173,15 +180,14 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   }
 
   std::vector<Candidate> cands{def};
+  auto add = [&](const Candidate &c) {
+    if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+  };
   for (int th : {256, 128})
-    for (int sp : {0, 2, 8}) {
-      const Candidate c{2, th, sp};
-      if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
-    }
-  if (!(def == Candidate{1, 0, 0})) cands.push_back({1, 0, 0});
-  if (precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag && resident_fits(s) &&
-      !(def == Candidate{4, 0, 0}))
-    cands.push_back({4, 0, 0});
+    for (int sp : {0, 2, 8}) add({2, th, sp, 0});
+  add({1, 0, 0, 0});
+  if (precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag && resident_fits(s))
+    add({4, 0, 0, 0});
 
   // device copies of the right-hand sides (and diagonals); a scratch x
   const size_t total = static_cast<size_t>(s->n) * k;
@@ -205,30 +211,47 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   std::vector<sfr_solve_info> info(k);
   int hard = SFR_OK;
   int timed = 0;
-  for (size_t c = 0; c < cands.size() && hard == SFR_OK; ++c) {
-    s->engine = cands[c].engine;
-    s->graph_threads = cands[c].threads ? cands[c].threads : threads0;
-    s->graph_spw = cands[c].spw;
-    double best = std::numeric_limits<double>::infinity();
-    bool ok = true;
-    for (int rep = 0; rep < 3 && ok; ++rep) {
-      const int rc = solve_device(s, solver, k, d_ad, d_b, d_x, tol, maxit, 1, precision,
-                                  s->stream, info.data());
-      if (rc == SFR_CUDA_ERROR || rc == SFR_TIMEOUT) {
-        hard = rc;
-        ok = false;
-      } else if (rc != SFR_OK) {
-        ok = false;  // this candidate does not serve the solve (unsupported, no convergence)
-      } else if (rep > 0) {
-        best = std::min(best, info[0].seconds * 1e3);
+  const int32_t pf0 = s->graph_pf;
+  // time candidates [from, cands.size())
+  auto measure = [&](size_t from) {
+    ms.resize(cands.size(), std::numeric_limits<double>::infinity());
+    for (size_t c = from; c < cands.size() && hard == SFR_OK; ++c) {
+      s->engine = cands[c].engine;
+      s->graph_threads = cands[c].threads ? cands[c].threads : threads0;
+      s->graph_spw = cands[c].spw;
+      s->graph_pf = cands[c].pf;
+      double best = std::numeric_limits<double>::infinity();
+      bool ok = true;
+      for (int rep = 0; rep < 3 && ok; ++rep) {
+        const int rc = solve_device(s, solver, k, d_ad, d_b, d_x, tol, maxit, 1, precision,
+                                    s->stream, info.data());
+        if (rc == SFR_CUDA_ERROR || rc == SFR_TIMEOUT) {
+          hard = rc;
+          ok = false;
+        } else if (rc != SFR_OK) {
+          ok = false;  // this candidate does not serve the solve (unsupported, no convergence)
+        } else if (rep > 0) {
+          best = std::min(best, info[0].seconds * 1e3);
+        }
+      }
+      if (ok) {
+        ms[c] = best;
+        ++timed;
       }
     }
-    if (ok) {
-      ms[c] = best;
-      ++timed;
-    }
+  };
+  measure(0);
+  // stage 2: the L2 prefetch distance on the best graph shape of stage 1
+  const size_t stage1 = cands.size();
+  size_t lead = 0;
+  for (size_t j = 1; j < stage1; ++j)
+    if (ms[j] < ms[lead]) lead = j;
+  if (hard == SFR_OK && cands[lead].engine == 2) {
+    for (int pf : {1, 2, 4}) add({2, cands[lead].threads, cands[lead].spw, pf});
+    measure(stage1);
   }
   s->engine = engine0;
+  s->graph_pf = pf0;
   s->graph_threads = threads0;
   s->graph_spw = spw0;
   release();
@@ -244,6 +267,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   t.engine = cands[pick].engine;
   t.threads = cands[pick].threads ? cands[pick].threads : threads0;
   t.spw = cands[pick].spw;
+  t.pf = cands[pick].pf;
   t.ms = ms[pick];
   store(s, t);
   file_store(key, t);

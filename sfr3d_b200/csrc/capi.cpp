@@ -388,11 +388,18 @@ int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads, int32_t s
   return SFR_OK;
 }
 
+int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds) {
+  if (!s || rounds < 0 || rounds > 8) return SFR_BAD_INPUT;
+  s->graph_pf = rounds;
+  return SFR_OK;
+}
+
 int sfr_gpu_destroy(sfr_system *s) {
   if (!s) return SFR_OK;
   cudaSetDevice(s->device);
   if (s->tview) sfr_gpu_destroy(s->tview);
   sfr::release_stream_engine(s);
+  sfr::release_minres_graph(s);
   io_release(s);
   if (!s->borrowed) {
     sfr::free_sell(&s->A);

@@ -204,6 +204,16 @@ struct SlotCols {
   const int16_t *off;  // null when the bandwidth does not fit 16 bits
 };
 
+// The slot columns a kernel instantiation reads: 16-bit offsets (I =
+// int16_t) or absolute indices (I = int).  Separate instantiations keep each
+// SpMV phase at the register count of one index form.
+template <typename I>
+__device__ __forceinline__ const I *cols_of(const SlotCols &c);
+template <>
+__device__ __forceinline__ const int *cols_of<int>(const SlotCols &c) { return c.col; }
+template <>
+__device__ __forceinline__ const int16_t *cols_of<int16_t>(const SlotCols &c) { return c.off; }
+
 // y_k[row] = diag*v(row) + sum_e val_e * v(col_e) for K vectors given by a
 // gather functor g(k, col), accumulated in Acc: exact FP64 (kExact: the
 // reference's rounding, one rounding per product and per sum), or with FMA.
@@ -279,6 +289,57 @@ __device__ __forceinline__ void row_product_t(const int *sptr, const SlotCols &c
   else
     row_product_t<K, Acc, kExact, V, DV, G, int>(sptr, cols.col, valp, diagp, s, lane, act, g, y);
 }
+
+// Totals of NV values over `G` block partials, fixed order, all threads of
+// the (last) block.  Result in sm[0..NV).
+template <int NV>
+__device__ __forceinline__ void block_totals(const double *part, int G, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double s[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    s[v] = 0.0;
+    for (int b = threadIdx.x; b < G; b += blockDim.x) s[v] += ld_vec(part + v * G + b);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = warp_sum(s[v]);
+    if (lane == 0) sm[32 + v * 32 + warp] = w;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double w = lane < nw ? sm[32 + v * 32 + lane] : 0.0;
+      w = warp_sum(w);
+      if (lane == 0) sm[v] = w;
+    }
+  }
+  __syncthreads();
+}
+
+// Block partials -> counter; true in the last block, with the totals in
+// sm[0..NV) for every thread of that block.  The counter is reset there.
+template <int NV>
+__device__ __forceinline__ bool last_block(const double (&acc)[NV], double *part,
+                                           unsigned *counter, double *sm) {
+  __shared__ bool s_last;
+  block_partials<NV>(acc, part, gridDim.x, sm + 32 + NV * 32);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  block_totals<NV>(part, gridDim.x, sm);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+// Shared memory a last_block reduction of NV values needs.
+#define SFR_SHARED_RED(NV) __shared__ double sm[32 + 2 * (NV) * 32]
 
 // Block-contiguous slice range of this block.
 __device__ __forceinline__ void block_slices(int nslices, int *first, int *last) {

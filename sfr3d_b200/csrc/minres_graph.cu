@@ -1,0 +1,519 @@
+// MINRES (Iters.c:309-558, pminres) with its scalar recurrence on the device:
+// the whole solve is one CUDA graph whose iteration loop is a conditional
+// WHILE node, like the graph engine's PCG (stream_solve.cu), so no dot
+// product travels to the host.
+//
+// One iteration is three kernels:
+//   a. p = A z0 and (z0, p); the last block forms alpha = (z0, p) / beta^2
+//      and the three-term coefficients t1 = 1/beta, t2 = -alpha/beta,
+//      t3 = -beta/beta_old;
+//   b. p = t1 p + t2 v + t3 v0, z = M p and (z, p); the last block runs the
+//      rest of the reference's scalar step -- beta, delta, ro2, ro3, symOrtho
+//      (Iters.c:1171-1211, with its branch tests as written: |b| is compared
+//      with a, not |a|), u1..u4, |r| = |s| |r| -- decides convergence,
+//      breakdown (a non-finite u) or maxIt, and clears the WHILE condition;
+//   c. w = u1 z0 + u2 w0 + u3 w00, x += u4 w (skipped after a breakdown, as
+//      the reference breaks before its update).
+// The reference rotates its vectors (v0 <- v <- p, z0 <- z, w00 <- w0 <- w)
+// by pointer swaps, with periods 3 and 2; the graph body unrolls six
+// iterations, each with its own fixed roles, and the kernels of iterations
+// after the stop return at once.
+//
+// Every scalar is computed with the reference's operations in its order,
+// each rounded once (no FMA contraction, IEEE division and square root), and
+// every vector element with the reference's C expression, so the recurrence
+// differs from the reference only through the dot products' summation order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "common.cuh"
+#include "internal.h"
+#include "persist.cuh"
+
+namespace sfr {
+
+namespace {
+
+constexpr int kMrThreads = 256;
+constexpr int kMrUnroll = 6;  // vector roles rotate with periods 3 and 2
+constexpr int kMrCounters = 8;
+
+struct MrState {
+  // per call
+  double tol;
+  unsigned maxit;
+  int newx;
+  // recurrence
+  double conv, beta, beta_old, alpha, t1, t2, t3;
+  double c, c_old, s, s_old, ro1, neta, norm_r;
+  double u1, u2, u3, u4;
+  unsigned j;
+  int active, upd, status, iters;
+  // post-processing (Iters.c:540-557 with the solver's common epilogue)
+  double xKx, norm_x, norm_r_true, norm_r_m;
+};
+
+struct MrArgs {
+  int n, nslices;
+  const int *sptr;
+  SlotCols cols;
+  const double *val;
+  double *ad, *b, *x, *m;        // the graph's own copies of the diagonal, b and x
+  double *V[3], *Z[2], *W[3];    // v0/v/p, z0/z, w00/w0/w by rotation
+  double *part;
+  unsigned *counter;
+  MrState *st;
+  cudaGraphConditionalHandle hwhile;
+};
+
+#define SFR_MR_FOR_ROWS(i) \
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
+
+// Iters.c:1171-1211 (symOrtho): no branch taken leaves c, s, r as they were.
+__device__ void sym_ortho_dev(double a, double b, double *c, double *s, double *r) {
+  const double ma = fabs(a), mb = fabs(b);
+  const double sa = a > 0.0 ? 1.0 : -1.0, sb = b > 0.0 ? 1.0 : -1.0;
+  if (b == 0.0) {
+    *s = 0.0;
+    *r = ma;
+    *c = a == 0.0 ? 1.0 : sa;
+  } else if (a == 0.0) {
+    *c = 0.0;
+    *s = sb;
+    *r = mb;
+  } else if (mb > a) {
+    const double t = xdiv(a, b);
+    *s = xdiv(sb, xsqrt(xadd(1.0, xmul(t, t))));
+    *c = xmul(*s, t);
+    *r = xdiv(b, *s);
+  } else if (ma > mb) {
+    const double t = xdiv(b, a);
+    *c = xdiv(sa, xsqrt(xadd(1.0, xmul(t, t))));
+    *s = xmul(*c, t);
+    *r = xdiv(a, *c);
+  }
+}
+
+// m = 1/ad, x0, z = M^1/2 b; conv = tol ||z||  (Iters.c:355-372)
+__global__ void __launch_bounds__(kMrThreads) k_mr_setup1(const MrArgs a) {
+  SFR_SHARED_RED(1);
+  MrState *st = a.st;
+  const int newx = st->newx;
+  double acc[1] = {0.0};
+  double *z = a.Z[1];
+  SFR_MR_FOR_ROWS(i) {
+    const double mi = 1.0 / a.ad[i];
+    a.m[i] = mi;
+    if (newx) a.x[i] = 0.0;
+    const double zi = xmul(a.b[i], sqrt(mi));
+    z[i] = zi;
+    acc[0] += zi * zi;
+  }
+  if (!last_block<1>(acc, a.part, a.counter + 0, sm)) return;
+  if (threadIdx.x == 0) st->conv = xmul(st->tol, xsqrt(sm[0]));
+}
+
+// v = b - A x, v0 = w0 = w00 = 0, z0 = M v; beta = sqrt|(v, z0)|
+// (Iters.c:374-398), with the iteration-0 roles.
+template <typename I>
+__global__ void __launch_bounds__(kMrThreads) k_mr_setup2(const MrArgs a) {
+  SFR_SHARED_RED(1);
+  MrState *st = a.st;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int all[1] = {1};
+  const double *const diag[1] = {a.ad};
+  double acc[1] = {0.0};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[1];
+    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val, diag, s_, lane, all,
+                                 [&](int, int c) { return ld_ro(a.x + c); }, y);
+    const double vi = xsub(a.b[row_], y[0]);
+    a.V[1][row_] = vi;  // v
+    a.V[0][row_] = 0.0; // v0
+    a.W[1][row_] = 0.0; // w0
+    a.W[0][row_] = 0.0; // w00
+    const double zi = xmul(vi, a.m[row_]);
+    a.Z[0][row_] = zi;  // z0
+    acc[0] += vi * zi;
+  }
+  if (!last_block<1>(acc, a.part, a.counter + 1, sm)) return;
+  if (threadIdx.x == 0) {
+    const double beta = xsqrt(fabs(sm[0]));
+    st->beta = beta;
+    st->beta_old = beta;
+    st->norm_r = beta;
+    st->neta = beta;
+    st->c_old = 1.0;
+    st->c = 1.0;
+    st->s_old = 0.0;
+    st->s = 0.0;
+    st->ro1 = 1.0;
+    st->j = 0;
+    st->upd = 0;
+    st->status = SFR_OK;
+    st->active = st->maxit > 0 ? 1 : 0;
+    if (!st->active) {
+      st->status = SFR_MAXIT;
+      st->iters = 1;
+      cudaGraphSetConditional(a.hwhile, 0u);
+    }
+  }
+}
+
+// a: p = A z0, alpha and the three-term coefficients (Iters.c:402-411)
+template <typename I>
+__global__ void __launch_bounds__(kMrThreads) k_mr_a(const MrArgs a, int u) {
+  SFR_SHARED_RED(1);
+  MrState *st = a.st;
+  if (!st->active) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  const double *z0 = a.Z[u % 2];
+  double *p = a.V[(u + 2) % 3];
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int all[1] = {1};
+  const double *const diag[1] = {a.ad};
+  double acc[1] = {0.0};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[1];
+    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val, diag, s_, lane, all,
+                                 [&](int, int c) { return ld_ro(z0 + c); }, y);
+    st_vec(p + row_, y[0]);
+    acc[0] += ld_ro(z0 + row_) * y[0];
+  }
+  if (!last_block<1>(acc, a.part, a.counter + 2, sm)) return;
+  if (threadIdx.x == 0) {
+    const double beta = st->beta;
+    const double t1 = xdiv(1.0, xmul(beta, beta));
+    const double alpha = xmul(sm[0], t1);
+    st->alpha = alpha;
+    st->t1 = xdiv(1.0, beta);
+    st->t2 = xdiv(-alpha, beta);
+    st->t3 = xdiv(-beta, st->beta_old);
+  }
+}
+
+// b: the new Lanczos vector and the scalar step (Iters.c:413-470)
+__global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
+  SFR_SHARED_RED(1);
+  MrState *st = a.st;
+  if (!st->active) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->upd = 0;
+    return;
+  }
+  const double t1 = st->t1, t2 = st->t2, t3 = st->t3;
+  const double *v0 = a.V[u % 3], *v = a.V[(u + 1) % 3];
+  double *p = a.V[(u + 2) % 3];
+  double *z = a.Z[(u + 1) % 2];
+  double acc[1] = {0.0};
+  SFR_MR_FOR_ROWS(i) {
+    const double pi = xadd(xadd(xmul(t1, ld_vec(p + i)), xmul(t2, ld_ro(v + i))),
+                           xmul(t3, ld_ro(v0 + i)));
+    p[i] = pi;
+    const double zi = xmul(pi, ld_ro(a.m + i));
+    z[i] = zi;
+    acc[0] += zi * pi;
+  }
+  if (!last_block<1>(acc, a.part, a.counter + 3, sm)) return;
+  if (threadIdx.x == 0) {
+    const unsigned j = st->j;
+    const double alpha = st->alpha;
+    const double beta_old = st->beta;
+    const double beta = xsqrt(sm[0]);
+    double c = st->c, s = st->s, ro1 = st->ro1;
+    const double c_old = st->c_old, s_old = st->s_old;
+    const double delta = xsub(xmul(c, alpha), xmul(xmul(c_old, s), beta_old));
+    const double ro2 = xadd(xmul(s, alpha), xmul(xmul(c_old, c), beta_old));
+    const double ro3 = xmul(s_old, beta_old);
+    st->c_old = c;
+    st->s_old = s;
+    sym_ortho_dev(delta, beta, &c, &s, &ro1);
+    st->c = c;
+    st->s = s;
+    st->ro1 = ro1;
+    st->beta_old = beta_old;
+    st->beta = beta;
+    const double u1 = xdiv(1.0, xmul(beta_old, ro1));
+    const double u2 = xdiv(-ro2, ro1);
+    const double u3 = xdiv(-ro3, ro1);
+    const double u4 = xmul(c, st->neta);
+    if (!isfinite(u1) || !isfinite(u2) || !isfinite(u3) || !isfinite(u4)) {
+      st->status = SFR_BREAKDOWN;
+      st->upd = 0;
+      st->active = 0;
+      st->iters = static_cast<int>(min(j + 1, st->maxit)) + 1;
+    } else {
+      st->u1 = u1;
+      st->u2 = u2;
+      st->u3 = u3;
+      st->u4 = u4;
+      st->upd = 1;
+      const double norm_r = xmul(fabs(s), st->norm_r);
+      st->norm_r = norm_r;
+      if (norm_r < st->conv) {
+        st->active = 0;
+        st->iters = static_cast<int>(j) + 1;
+      } else {
+        st->neta = xmul(-s, st->neta);
+        if (j + 1 >= st->maxit) {
+          st->active = 0;
+          st->status = SFR_MAXIT;
+          st->iters = static_cast<int>(st->maxit) + 1;
+        }
+      }
+    }
+    st->j = j + 1;
+    if (!st->active) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
+// c: w = u1 z0 + u2 w0 + u3 w00, x += u4 w  (Iters.c:482-497)
+__global__ void __launch_bounds__(kMrThreads) k_mr_c(const MrArgs a, int u) {
+  MrState *st = a.st;
+  if (!st->upd) return;
+  const double u1 = st->u1, u2 = st->u2, u3 = st->u3, u4 = st->u4;
+  const double *z0 = a.Z[u % 2];
+  const double *w00 = a.W[u % 3], *w0 = a.W[(u + 1) % 3];
+  double *w = a.W[(u + 2) % 3];
+  SFR_MR_FOR_ROWS(i) {
+    const double wi = xadd(xadd(xmul(u1, ld_ro(z0 + i)), xmul(u2, ld_ro(w0 + i))),
+                           xmul(u3, ld_ro(w00 + i)));
+    w[i] = wi;
+    a.x[i] = xadd(a.x[i], xmul(u4, wi));
+  }
+}
+
+// post-processing: xKx, ||x||, ||b - A x||, ||M^1/2 (b - A x)||
+template <typename I>
+__global__ void __launch_bounds__(kMrThreads) k_mr_post(const MrArgs a) {
+  SFR_SHARED_RED(4);
+  MrState *st = a.st;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int all[1] = {1};
+  const double *const diag[1] = {a.ad};
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[1];
+    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val, diag, s_, lane, all,
+                                 [&](int, int c) { return ld_ro(a.x + c); }, y);
+    const double xi = a.x[row_];
+    const double ri = xsub(a.b[row_], y[0]);
+    const double ti = xmul(ri, sqrt(fabs(a.m[row_])));
+    acc[0] += xi * y[0];
+    acc[1] += xi * xi;
+    acc[2] += ri * ri;
+    acc[3] += ti * ti;
+  }
+  if (!last_block<4>(acc, a.part, a.counter + 4, sm)) return;
+  if (threadIdx.x == 0) {
+    st->xKx = sm[0];
+    st->norm_x = sqrt(sm[1]);
+    st->norm_r_true = sqrt(sm[2]);
+    st->norm_r_m = sqrt(sm[3]);
+  }
+}
+
+#define SFR_TRY(expr)                 \
+  do {                                \
+    cudaError_t e_ = (expr);          \
+    if (e_ != cudaSuccess) return e_; \
+  } while (0)
+
+struct MrGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void *ws = nullptr;
+  MrArgs args{};
+  int gs = 0, gv = 0;
+};
+
+std::map<const sfr_system *, std::unique_ptr<MrGraph>> g_mr;
+
+void free_mr(MrGraph *g) {
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  cudaFree(g->ws);
+  *g = MrGraph{};
+}
+
+cudaError_t node(cudaGraph_t g, cudaGraphNode_t *prev, void *func, int grid, void **params) {
+  cudaKernelNodeParams p{};
+  p.func = func;
+  p.gridDim = dim3(grid);
+  p.blockDim = dim3(kMrThreads);
+  p.kernelParams = params;
+  cudaGraphNode_t nd;
+  const cudaError_t e = cudaGraphAddKernelNode(&nd, g, *prev ? prev : nullptr, *prev ? 1 : 0, &p);
+  if (e == cudaSuccess) *prev = nd;
+  return e;
+}
+
+template <typename I>
+cudaError_t build(sfr_system *s, MrGraph *g) {
+  const int n = s->n;
+  const size_t vb = (sizeof(double) * static_cast<size_t>(std::max(n, 1)) + 255) & ~size_t{255};
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mr_a<I>, kMrThreads, 0) !=
+          cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  const int sms = std::max(1, num_sms(s->device));
+  g->gs = std::max(1, std::min((s->A.nslices + 7) / 8, occ * sms));
+  g->gv = std::max(1, std::min(sms * (2048 / kMrThreads), (n + kMrThreads - 1) / kMrThreads));
+  const int gmax = std::max(g->gs, g->gv);
+  const size_t part_b = (sizeof(double) * 4 * static_cast<size_t>(gmax) + 255) & ~size_t{255};
+  const size_t total = vb * 12 + part_b + 256 + sizeof(MrState);
+  SFR_TRY(cudaMalloc(&g->ws, total));
+  SFR_TRY(cudaMemset(g->ws, 0, total));
+  char *base = static_cast<char *>(g->ws);
+  auto V = [&](int i) { return reinterpret_cast<double *>(base + vb * i); };
+  MrArgs &a = g->args;
+  a.n = n;
+  a.nslices = s->A.nslices;
+  a.sptr = s->A.sptr;
+  a.cols = SlotCols{s->A.col, s->A.off};
+  a.val = s->A.val;
+  a.ad = V(0);
+  a.b = V(1);
+  a.x = V(2);
+  a.m = V(3);
+  for (int i = 0; i < 3; ++i) a.V[i] = V(4 + i);
+  for (int i = 0; i < 2; ++i) a.Z[i] = V(7 + i);
+  for (int i = 0; i < 3; ++i) a.W[i] = V(9 + i);
+  a.part = reinterpret_cast<double *>(base + vb * 12);
+  a.counter = reinterpret_cast<unsigned *>(base + vb * 12 + part_b);
+  a.st = reinterpret_cast<MrState *>(base + vb * 12 + part_b + 256);
+
+  SFR_TRY(cudaGraphCreate(&g->graph, 0));
+  SFR_TRY(cudaGraphConditionalHandleCreate(&a.hwhile, g->graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNode_t prev = nullptr;
+  {
+    cudaMemsetParams mp{};
+    mp.dst = a.counter;
+    mp.value = 0;
+    mp.elementSize = sizeof(unsigned);
+    mp.width = kMrCounters;
+    mp.height = 1;
+    SFR_TRY(cudaGraphAddMemsetNode(&prev, g->graph, nullptr, 0, &mp));
+  }
+  void *p1[1] = {&a};
+  SFR_TRY(node(g->graph, &prev, (void *)k_mr_setup1, g->gv, p1));
+  SFR_TRY(node(g->graph, &prev, (void *)k_mr_setup2<I>, g->gs, p1));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = a.hwhile;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wn;
+  SFR_TRY(cudaGraphAddNode(&wn, g->graph, &prev, 1, &cp));
+  prev = wn;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphNode_t bp = nullptr;
+  int us[kMrUnroll];
+  void *pu[kMrUnroll][2];
+  for (int u = 0; u < kMrUnroll; ++u) {
+    us[u] = u;
+    pu[u][0] = &a;
+    pu[u][1] = &us[u];
+    SFR_TRY(node(body, &bp, (void *)k_mr_a<I>, g->gs, pu[u]));
+    SFR_TRY(node(body, &bp, (void *)k_mr_b, g->gv, pu[u]));
+    SFR_TRY(node(body, &bp, (void *)k_mr_c, g->gv, pu[u]));
+  }
+  SFR_TRY(node(g->graph, &prev, (void *)k_mr_post<I>, g->gs, p1));
+  SFR_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  return cudaSuccess;
+}
+
+}  // namespace
+
+int solve_minres_graph(sfr_system *s, const double *d_diag, const double *d_b, double *d_x,
+                       double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
+                       sfr_solve_info *info) {
+  auto &slot = g_mr[s];
+  if (!slot) {
+    slot = std::make_unique<MrGraph>();
+    const cudaError_t be = s->A.off ? build<int16_t>(s, slot.get()) : build<int>(s, slot.get());
+    if (be != cudaSuccess) {
+      set_last_error(cudaGetErrorString(be));
+      free_mr(slot.get());
+      g_mr.erase(s);
+      return SFR_CUDA_ERROR;
+    }
+  }
+  MrGraph *g = slot.get();
+  const MrArgs &a = g->args;
+  const size_t vb = sizeof(double) * static_cast<size_t>(s->n);
+  MrState call{};
+  call.tol = tol;
+  call.maxit = maxit;
+  call.newx = newx;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess) return SFR_CUDA_ERROR;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return SFR_CUDA_ERROR;
+  }
+  cudaError_t err = cudaEventRecord(e0, st);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(a.ad, d_diag ? d_diag : s->d_diag, vb, cudaMemcpyDeviceToDevice, st);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(a.b, d_b, vb, cudaMemcpyDeviceToDevice, st);
+  if (err == cudaSuccess && !newx)
+    err = cudaMemcpyAsync(a.x, d_x, vb, cudaMemcpyDeviceToDevice, st);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(a.st, &call, offsetof(MrState, conv), cudaMemcpyHostToDevice, st);
+  if (err == cudaSuccess) err = cudaGraphLaunch(g->exec, st);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_x, a.x, vb, cudaMemcpyDeviceToDevice, st);
+  if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+  MrState out{};
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(&out, a.st, sizeof(MrState), cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  float ms = 0.f;
+  if (err == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) {
+    set_last_error(cudaGetErrorString(err));
+    return SFR_CUDA_ERROR;
+  }
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->iters = out.iters;
+    info->status = out.status;
+    info->xKx = out.xKx;
+    info->norm_x = out.norm_x;
+    info->norm_r = out.norm_r_true;
+    info->norm_r_m = out.norm_r_m;
+    info->conv = out.conv;
+    info->seconds = ms * 1e-3;
+    info->refinements = 0;
+    info->inner_iters = out.iters;
+    info->relres = std::nan("");
+  }
+  return out.status;
+}
+
+void release_minres_graph(const sfr_system *s) {
+  auto it = g_mr.find(s);
+  if (it == g_mr.end()) return;
+  free_mr(it->second.get());
+  g_mr.erase(it);
+}
+
+}  // namespace sfr

@@ -58,17 +58,11 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   // the right-hand sides share one diagonal: diag64, m, dc and m32 of every
   // k point at k = 0's arrays, which k_setup fills once
   int shared_diag;
+  // SpMV phases of the iteration: a warp prefetches into L2 the slice it
+  // reaches `pf` rounds later (0: off)
+  int pf;
 };
 
-// The slot columns a kernel instantiation reads: 16-bit offsets (I =
-// int16_t) or absolute indices (I = int).  Separate instantiations keep each
-// SpMV phase at the register count of one index form.
-template <typename I>
-__device__ __forceinline__ const I *cols_of(const SlotCols &c);
-template <>
-__device__ __forceinline__ const int *cols_of<int>(const SlotCols &c) { return c.col; }
-template <>
-__device__ __forceinline__ const int16_t *cols_of<int16_t>(const SlotCols &c) { return c.off; }
 
 // Per-call scalars, copied into the state before each launch.
 struct SCall {
@@ -100,55 +94,28 @@ __device__ __forceinline__ float2 ld2ro(const float *p) { return *reinterpret_ca
 __device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
 
-// Totals of NV values over `G` block partials, fixed order, all threads of
-// the (last) block.  Result in sm[0..NV).
-template <int NV>
-__device__ __forceinline__ void block_totals(const double *part, int G, double *sm) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double s[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    s[v] = 0.0;
-    for (int b = threadIdx.x; b < G; b += blockDim.x) s[v] += ld_vec(part + v * G + b);
-  }
-  __syncthreads();
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    const double w = warp_sum(s[v]);
-    if (lane == 0) sm[32 + v * 32 + warp] = w;
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double w = lane < nw ? sm[32 + v * 32 + lane] : 0.0;
-      w = warp_sum(w);
-      if (lane == 0) sm[v] = w;
-    }
-  }
-  __syncthreads();
-}
 
-// Block partials -> counter; true in the last block, with the totals in
-// sm[0..NV) for every thread of that block.  The counter is reset there.
-template <int NV>
-__device__ __forceinline__ bool last_block(const double (&acc)[NV], double *part,
-                                           unsigned *counter, double *sm) {
-  __shared__ bool s_last;
-  block_partials<NV>(acc, part, gridDim.x, sm + 32 + NV * 32);
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last) return false;
-  __threadfence();
-  block_totals<NV>(part, gridDim.x, sm);
-  if (threadIdx.x == 0) *counter = 0u;
-  return true;
+// L2 prefetch for an iteration's SpMV phase: lane 0 of each warp asks for
+// the slice the warp reaches `pf` rounds later (a round: every warp of the
+// block one slice further), within the block's own slices.  A slice's slot
+// columns and values are each one contiguous run (slot-major, 32 rows a
+// slot), so one bulk prefetch covers each: values at 256 B (FP64) / 128 B
+// (FP32) and columns at 64 B boundaries, sizes multiples of 64 B -- both
+// within cp.async.bulk's 16-byte rule.
+template <typename I, typename V>
+__device__ __forceinline__ void prefetch_slice_ahead(int pf, const int *sptr, const I *cols,
+                                                     const V *vals, int s, int s1) {
+  if (pf <= 0 || (threadIdx.x & 31) != 0) return;
+  const int t = s + pf * static_cast<int>(blockDim.x >> 5);
+  if (t >= s1) return;
+  const int b = __ldg(sptr + t);
+  const int e = __ldg(sptr + t + 1);
+  if (e <= b) return;
+  const unsigned nv = static_cast<unsigned>(e - b) * sizeof(V);
+  const unsigned nc = static_cast<unsigned>(e - b) * sizeof(I);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(vals + b), "r"(nv) : "memory");
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(cols + b), "r"(nc) : "memory");
 }
-
-#define SFR_SHARED_RED(NV) __shared__ double sm[32 + 2 * (NV) * 32]
 
 template <int K>
 __device__ __forceinline__ void load_active(const SState<K> *st, int (&act)[K]) {
@@ -279,6 +246,7 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
   for (int k = 0; k < K; ++k) acc[k] = 0.0;
   if (!kMixed) {
     SFR_FOR_OWN_ROWS(s0, s1) {
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.p0[k] + c); }, y);
@@ -292,6 +260,7 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
   } else {
     const double *const *dc = a.dc;
     SFR_FOR_OWN_ROWS(s0, s1) {
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
       double y[K];
       row_product_t<K, double, false, float, double>(
           a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
@@ -657,6 +626,7 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     if (!kMixed) {
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
@@ -673,6 +643,7 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
       // diagonally dominant, and FP64 accumulation of K right-hand sides
       // costs two FP32 -> FP64 conversions a slot and right-hand side (the
       // SpMV phase then ran slower than the FP64 one)
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
       float y[K];
       {
         const double *const *dc = a.dc;
@@ -864,6 +835,7 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
   SFR_FOR_OWN_ROWS(s0, s1) {
     if (!kMixed) {
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
                                    [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
@@ -879,6 +851,7 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
       // diagonally dominant, and FP64 accumulation of K right-hand sides
       // costs two FP32 -> FP64 conversions a slot and right-hand side (the
       // SpMV phase then ran slower than the FP64 one)
+      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
       float y[K];
       {
         const double *const *dc = a.dc;
@@ -1047,9 +1020,10 @@ __global__ void __launch_bounds__(256) k_bicg_c(const SArgs<K> a, SState<K> *st)
 struct GraphKey {
   int solver, k, precision, threads, spw;
   int shared_diag;  // the K right-hand sides share one diagonal
+  int pf;           // SpMV-phase L2 prefetch distance
   bool operator<(const GraphKey &o) const {
-    return std::tie(solver, k, precision, threads, spw, shared_diag) <
-           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag);
+    return std::tie(solver, k, precision, threads, spw, shared_diag, pf) <
+           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag, o.pf);
   }
 };
 
@@ -1137,7 +1111,7 @@ int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
 // SMs idle while the phase's last blocks finish.
 template <int K, typename I>
 cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int spw,
-                    int shared_diag, CachedGraph *cg) {
+                    int shared_diag, int pf, CachedGraph *cg) {
   const int n = s->n;
   const int64_t np = padded(n);
   const bool mixed = precision == SFR_MIXED;
@@ -1215,6 +1189,7 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
     }
   }
   a.shared_diag = shared_diag;
+  a.pf = pf;
   a.part = cg->part;
   a.counter = cg->counter;
   return cudaSuccess;
@@ -1223,8 +1198,8 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
 // The graph for one (solver, K, precision, launch shape).
 template <int K, typename I>
 cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
-                        int shared_diag, CachedGraph *cg) {
-  SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, shared_diag, cg)));
+                        int shared_diag, int pf, CachedGraph *cg) {
+  SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, shared_diag, pf, cg)));
   SFR_TRY(cudaGraphCreate(&cg->graph, 0));
   cudaGraph_t g = cg->graph;
   const bool mixed = precision == SFR_MIXED;
@@ -1399,12 +1374,12 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
 template <int K>
 int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, double *d_x,
         double tol, uint32_t maxit, int newx, int precision, double delta, int threads, int spw,
-        bool loop, cudaStream_t st, SolveOut *out, float *ms) {
+        int pf, bool loop, cudaStream_t st, SolveOut *out, float *ms) {
   const int n = s->n;
   if (maxit == 0) return SFR_BAD_INPUT;
   EngineCache &ec = g_engines[s];
   const int shared_diag = K > 1 && !d_diag_k ? 1 : 0;
-  GraphKey key{solver, K, precision, threads, spw, shared_diag};
+  GraphKey key{solver, K, precision, threads, spw, shared_diag, pf};
   auto it = ec.graphs.find(key);
   if (it == ec.graphs.end()) {
     if (ec.graphs.size() >= kMaxGraphsPerSystem) {  // drop the least recently used
@@ -1416,8 +1391,9 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
     }
     auto cg = std::make_unique<CachedGraph>();
     const cudaError_t be =
-        s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, cg.get())
-                 : build_graph<K, int>(s, solver, precision, threads, spw, shared_diag, cg.get());
+        s->A.off
+            ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, pf, cg.get())
+            : build_graph<K, int>(s, solver, precision, threads, spw, shared_diag, pf, cg.get());
     if (be != cudaSuccess) {
       set_last_error(cudaGetErrorString(be));
       free_graph(cg.get());
@@ -1476,19 +1452,20 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
 
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
-                 int32_t precision, double delta, int threads, int spw, bool loop,
+                 int32_t precision, double delta, int threads, int spw, int pf, bool loop,
                  cudaStream_t st, sfr_solve_info *info) {
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
   if (threads != 128 && threads != 256) return SFR_BAD_INPUT;
   if (spw < 0 || spw > 64) return SFR_BAD_INPUT;
+  if (pf < 0 || pf > 8) return SFR_BAD_INPUT;
   SolveOut out[kMaxK];
   float ms = 0.f;
   int rc;
   switch (k) {
-    case 1: rc = run<1>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
-    case 2: rc = run<2>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
-    case 3: rc = run<3>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
-    default: rc = run<4>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, loop, st, out, &ms); break;
+    case 1: rc = run<1>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
+    case 2: rc = run<2>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
+    case 3: rc = run<3>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
+    default: rc = run<4>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
   }
   if (rc != SFR_OK) return rc;
   int worst = SFR_OK;

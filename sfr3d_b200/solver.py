@@ -56,9 +56,10 @@ class SolveInfo:
 
 class TuneResultC(ctypes.Structure):
     _fields_ = [("engine", _I32), ("threads", _I32), ("slices_per_warp", _I32),
-                ("ms", ctypes.c_double), ("default_engine", _I32),
+                ("prefetch", _I32), ("ms", ctypes.c_double), ("default_engine", _I32),
                 ("default_threads", _I32), ("default_slices_per_warp", _I32),
-                ("default_ms", ctypes.c_double), ("candidates", _I32), ("source", _I32)]
+                ("default_prefetch", _I32), ("default_ms", ctypes.c_double),
+                ("candidates", _I32), ("source", _I32)]
 
 
 class BatchTuneC(ctypes.Structure):
@@ -104,6 +105,7 @@ def lib() -> ctypes.CDLL:
                                   ctypes.c_double, ctypes.c_uint32, _I32, _P]
     L.sfr_gpu_destroy.argtypes = [_P]
     L.sfr_gpu_set_engine.argtypes = [_P, _I32, _I32, _I32]
+    L.sfr_gpu_set_prefetch.argtypes = [_P, _I32]
     L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_transpose.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_dot.argtypes = [_P, _P, _P, _P, _P]
@@ -216,6 +218,13 @@ class GpuSystem:
         rc = lib().sfr_gpu_set_engine(self.h, engine, threads, slices_per_warp)
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_engine")
+
+    def set_prefetch(self, rounds: int):
+        """Graph engine: L2 prefetch of the SELL slice each warp reaches
+        `rounds` rounds later in the SpMV phases (0 off)."""
+        rc = lib().sfr_gpu_set_prefetch(self.h, rounds)
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_prefetch")
 
     def autotune(self, solver: int, b, ad_k=None, tol: float = 1e-10, maxit: int = 100000,
                  precision: int = FP64) -> dict:
