@@ -8,8 +8,10 @@
 //      rows) per warp; the persistent engine (the whole solve in one
 //      cooperative launch); the resident engine, for mixed PCG with one
 //      right-hand side when the system fits it;
-//   2. when the graph engine leads: its best shape with the SpMV phases'
-//      L2 prefetch 1, 2 or 4 rounds ahead.
+//      for FP64 PCG with one right-hand side, also the graph engine with the
+//      fused iteration (one cooperative kernel an iteration, k_pcg_fused);
+//   2. when the graph engine leads with three kernels an iteration: its best
+//      shape with the SpMV phases' L2 prefetch 1, 2 or 4 rounds ahead.
 // Each candidate solves the caller's right-hand side once untimed (the graph
 // is built and the clocks are up), then twice timed with CUDA events; its
 // time is the faster of the two.  The automatic choice is kept unless a
@@ -49,10 +51,10 @@ const Tuned *find_tuned(const sfr_system *s, int32_t solver, int32_t k, int32_t 
 namespace {
 
 struct Candidate {
-  int engine, threads, spw, pf;
+  int engine, threads, spw, pf, fused;
   bool operator==(const Candidate &o) const {
-    return engine == o.engine &&
-           (engine != 2 || (threads == o.threads && spw == o.spw && pf == o.pf));
+    return engine == o.engine && (engine != 2 || (threads == o.threads && spw == o.spw &&
+                                                  pf == o.pf && fused == o.fused));
   }
 };
 
@@ -68,7 +70,7 @@ std::string cache_key(const sfr_system *s, int32_t solver, int32_t k, int32_t pr
     if (c == ' ' || c == '\t') c = '_';
   char buf[512];
   std::snprintf(buf, sizeof(buf),
-                "sfr-tune-v2 gpu=%s sms=%d n=%d slots=%lld nsrc=%d storage=%d unsym=%d "
+                "sfr-tune-v3 gpu=%s sms=%d n=%d slots=%lld nsrc=%d storage=%d unsym=%d "
                 "off16=%d solver=%d k=%d precision=%d own_diag=%d",
                 gpu.c_str(), prop.multiProcessorCount, s->n,
                 static_cast<long long>(s->A.nslots), s->nsrc, s->storage, s->unsym,
@@ -88,16 +90,18 @@ bool file_lookup(const std::string &key, Tuned *t) {
   const std::string head = key + " -> ";
   while (std::fgets(line.data(), static_cast<int>(line.size()), f)) {
     if (std::strncmp(line.data(), head.c_str(), head.size()) != 0) continue;
-    int e = 0, th = 0, sp = 0, pf = 0;
+    int e = 0, th = 0, sp = 0, pf = 0, fu = 0;
     double ms = 0.0;
-    if (std::sscanf(line.data() + head.size(), "engine=%d threads=%d spw=%d pf=%d ms=%lf", &e,
-                    &th, &sp, &pf, &ms) == 5 &&
+    if (std::sscanf(line.data() + head.size(),
+                    "engine=%d threads=%d spw=%d pf=%d fused=%d ms=%lf", &e, &th, &sp, &pf, &fu,
+                    &ms) == 6 &&
         (e == 1 || e == 2 || e == 4) && (th == 128 || th == 256) && sp >= 0 && sp <= 64 &&
-        pf >= 0 && pf <= 8) {
+        pf >= 0 && pf <= 8 && (fu == 0 || fu == 1)) {
       t->engine = e;
       t->threads = th;
       t->spw = sp;
       t->pf = pf;
+      t->fused = fu;
       t->ms = ms;
       found = true;
     }
@@ -112,8 +116,8 @@ void file_store(const std::string &key, const Tuned &t) {
   std::lock_guard<std::mutex> lk(g_file_mu);
   FILE *f = std::fopen(path, "a");
   if (!f) return;
-  std::fprintf(f, "%s -> engine=%d threads=%d spw=%d pf=%d ms=%.6f\n", key.c_str(), t.engine,
-               t.threads, t.spw, t.pf, t.ms);
+  std::fprintf(f, "%s -> engine=%d threads=%d spw=%d pf=%d fused=%d ms=%.6f\n", key.c_str(),
+               t.engine, t.threads, t.spw, t.pf, t.fused, t.ms);
   std::fclose(f);
 }
 
@@ -135,11 +139,13 @@ void fill(sfr_tune_result *out, const Tuned &t, const Candidate &def, double def
   out->threads = t.threads;
   out->slices_per_warp = t.spw;
   out->prefetch = t.pf;
+  out->fused = t.fused;
   out->ms = t.ms;
   out->default_engine = def.engine;
   out->default_threads = def.threads;
   out->default_slices_per_warp = def.spw;
   out->default_prefetch = def.pf;
+  out->default_fused = def.fused;
   out->default_ms = def_ms;
   out->candidates = n;
   out->source = source;
@@ -162,7 +168,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   if (cudaSetDevice(s->device) != cudaSuccess) return SFR_CUDA_ERROR;
   const bool own_diag = ad_k == nullptr;
   const Candidate def{auto_engine(s, solver, k, precision, own_diag), s->graph_threads,
-                      s->graph_spw, s->graph_pf};
+                      s->graph_spw, s->graph_pf, s->graph_fused};
   if (const Tuned *t = find_tuned(s, solver, k, precision, own_diag)) {
     fill(out, *t, def, 0.0, 0, 1);
     return SFR_OK;
@@ -184,10 +190,11 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
     if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
   };
   for (int th : {256, 128})
-    for (int sp : {0, 2, 8}) add({2, th, sp, 0});
-  add({1, 0, 0, 0});
+    for (int sp : {0, 2, 8}) add({2, th, sp, 0, 0});
+  if (precision == SFR_FP64 && solver == SFR_PCG && k == 1) add({2, 256, 0, 0, 1});
+  add({1, 0, 0, 0, 0});
   if (precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag && resident_fits(s))
-    add({4, 0, 0, 0});
+    add({4, 0, 0, 0, 0});
 
   // device copies of the right-hand sides (and diagonals); a scratch x
   const size_t total = static_cast<size_t>(s->n) * k;
@@ -211,7 +218,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   std::vector<sfr_solve_info> info(k);
   int hard = SFR_OK;
   int timed = 0;
-  const int32_t pf0 = s->graph_pf;
+  const int32_t pf0 = s->graph_pf, fused0 = s->graph_fused;
   // time candidates [from, cands.size())
   auto measure = [&](size_t from) {
     ms.resize(cands.size(), std::numeric_limits<double>::infinity());
@@ -220,6 +227,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
       s->graph_threads = cands[c].threads ? cands[c].threads : threads0;
       s->graph_spw = cands[c].spw;
       s->graph_pf = cands[c].pf;
+      s->graph_fused = cands[c].fused;
       double best = std::numeric_limits<double>::infinity();
       bool ok = true;
       for (int rep = 0; rep < 3 && ok; ++rep) {
@@ -246,12 +254,13 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   size_t lead = 0;
   for (size_t j = 1; j < stage1; ++j)
     if (ms[j] < ms[lead]) lead = j;
-  if (hard == SFR_OK && cands[lead].engine == 2) {
-    for (int pf : {1, 2, 4}) add({2, cands[lead].threads, cands[lead].spw, pf});
+  if (hard == SFR_OK && cands[lead].engine == 2 && !cands[lead].fused) {
+    for (int pf : {1, 2, 4}) add({2, cands[lead].threads, cands[lead].spw, pf, 0});
     measure(stage1);
   }
   s->engine = engine0;
   s->graph_pf = pf0;
+  s->graph_fused = fused0;
   s->graph_threads = threads0;
   s->graph_spw = spw0;
   release();
@@ -268,6 +277,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   t.threads = cands[pick].threads ? cands[pick].threads : threads0;
   t.spw = cands[pick].spw;
   t.pf = cands[pick].pf;
+  t.fused = cands[pick].fused;
   t.ms = ms[pick];
   store(s, t);
   file_store(key, t);

@@ -394,12 +394,19 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds) {
   return SFR_OK;
 }
 
+int sfr_gpu_set_fused(sfr_system *s, int32_t flag) {
+  if (!s) return SFR_BAD_INPUT;
+  s->graph_fused = flag != 0 ? 1 : 0;
+  return SFR_OK;
+}
+
 int sfr_gpu_destroy(sfr_system *s) {
   if (!s) return SFR_OK;
   cudaSetDevice(s->device);
   if (s->tview) sfr_gpu_destroy(s->tview);
   sfr::release_stream_engine(s);
   sfr::release_minres_graph(s);
+  sfr::release_bicgstabl2_graph(s);
   io_release(s);
   if (!s->borrowed) {
     sfr::free_sell(&s->A);

@@ -51,7 +51,7 @@ struct SolveOut;  // device-side result record (krylov.cu)
 // (autotune.cpp); the automatic engine choice (engine 0) takes it.
 struct Tuned {
   int32_t solver = 0, k = 0, precision = 0, own_diag = 0;  // the kind of solve
-  int32_t engine = 0, threads = 0, spw = 0, pf = 0;       // the choice
+  int32_t engine = 0, threads = 0, spw = 0, pf = 0, fused = 0;  // the choice
   double ms = 0.0;
 };
 
@@ -102,6 +102,7 @@ struct sfr_system {
   int32_t graph_threads = 256;   // graph engine launch shape
   int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
   int32_t graph_pf = 0;          // SpMV-phase L2 prefetch distance (rounds); 0: off
+  int32_t graph_fused = 0;       // FP64 PCG, one RHS: one cooperative kernel an iteration
   std::vector<sfr::Tuned> tuned; // autotuned choices, used when engine == 0
   int64_t bytes = 0;
 };
@@ -158,12 +159,17 @@ int solve_minres_graph(sfr_system *s, const double *d_diag, const double *d_b, d
                        double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
                        sfr_solve_info *info);
 void release_minres_graph(const sfr_system *s);
+// BiCGSTAB(2) the same way (bicgl2_graph.cu)
+int solve_bicgstabl2_graph(sfr_system *s, const double *d_diag, const double *d_b, double *d_x,
+                           double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
+                           sfr_solve_info *info);
+void release_bicgstabl2_graph(const sfr_system *s);
 
 // Graph engine (stream_solve.cu)
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
-                 int32_t precision, double delta, int threads, int spw, int pf, bool loop,
-                 cudaStream_t st, sfr_solve_info *info);
+                 int32_t precision, double delta, int threads, int spw, int pf, int fused,
+                 bool loop, cudaStream_t st, sfr_solve_info *info);
 void release_stream_engine(const sfr_system *s);
 double reliable_delta(int32_t solver);
 double reliable_delta_resident();  // the resident engine's PCG factor

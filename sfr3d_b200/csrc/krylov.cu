@@ -880,7 +880,7 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   }
   if (solver != SFR_PCG && solver != SFR_PBICGSTAB) return SFR_UNSUPPORTED;
   int engine = s->engine;
-  int threads = s->graph_threads, spw = s->graph_spw, pf = s->graph_pf;
+  int threads = s->graph_threads, spw = s->graph_spw, pf = s->graph_pf, fused = s->graph_fused;
   const bool resident_case = precision == SFR_MIXED && solver == SFR_PCG && k == 1 && !d_diag_k;
   bool tuned = false;
   if (engine == 0) {
@@ -889,6 +889,7 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
       threads = t->threads;
       spw = t->spw;
       pf = t->pf;
+      fused = t->fused;
       tuned = true;
     }
   }
@@ -901,7 +902,7 @@ int solve_device(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   if (engine == 0 || engine == 4) engine = s->n >= kGraphEngineRows ? 2 : 1;
   if (engine == 2 || engine == 3)
     return solve_stream(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, precision,
-                        reliable_delta(solver), threads, spw, pf, engine == 3, st, info);
+                        reliable_delta(solver), threads, spw, pf, fused, engine == 3, st, info);
   if (precision == SFR_MIXED)
     return solve_mixed(s, solver, k, d_diag_k, d_b, d_x, tol, maxit, newx, st, info);
   if (precision != SFR_FP64) return SFR_UNSUPPORTED;

@@ -423,6 +423,118 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
   }
 }
 
+// One whole FP64 PCG iteration (one right-hand side) in one cooperative
+// launch: the three phases above with two grid barriers between them instead
+// of kernel boundaries.  A block keeps q = A p of its own rows in shared
+// memory from phase A to phase B, and then z = M r in the same words from
+// phase B to phase C, so neither q nor z crosses HBM; the block's p is still
+// in cache when phase C rewrites it.  Each barrier's dot product is reduced
+// by every block over all block partials in the same fixed order, so every
+// block holds the same alpha, beta and stop decision.  Every row is computed
+// with the same expressions as in k_pcg_a/b/c (bit-identical rows).
+// The barriers are bounded: a wait that gives up records SFR_TIMEOUT, every
+// block leaves, and the solve stops with that status.
+template <typename I>
+__global__ void __launch_bounds__(256) k_pcg_fused(const SArgs<1> a, SState<1> *st,
+                                                   GridSync gs) {
+  __shared__ double sm[32 * 2];
+  extern __shared__ double qz[];  // this block's rows: q, then z
+  if (!st->any) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int row0 = s0 * kWarp;
+  const int all[1] = {1};
+  const unsigned j = st->j;
+  const double d = st->d[0];
+  const int G = gridDim.x;
+  auto fail = [&](int status, unsigned iters) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->active[0] = 0;
+      st->status[0] = status;
+      st->iters[0] = static_cast<int>(iters);
+      st->any = 0;
+      if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+    }
+  };
+  // phase A: q = A p, (p, q)
+  double acc[1] = {0.0};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[1];
+    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
+                                 [&](int, int c) { return ld_ro(a.p0[0] + c); }, y);
+    qz[row_ - row0] = y[0];
+    acc[0] += y[0] * ld_ro(a.p0[0] + row_);
+  }
+  block_partials<1>(acc, a.part, G, sm);
+  if (!grid_sync(gs)) {
+    fail(SFR_TIMEOUT, j + 1);
+    return;
+  }
+  double tot[1];
+  grid_totals<1>(a.part, G, G, tot, sm);
+  const double alpha = d / tot[0];
+  if (!isfinite(alpha)) {
+    fail(SFR_BREAKDOWN, j + 1);
+    return;
+  }
+  // phase B: x += alpha p, r -= alpha q, z = M r, (r, z)
+  acc[0] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    const double p = ld_ro(a.p0[0] + row_);
+    const double xv = xadd(ld_vec(a.x[0] + row_), xmul(alpha, p));
+    const double rv = xsub(ld_vec(a.r[0] + row_), xmul(alpha, qz[row_ - row0]));
+    const double zv = xmul(rv, ld_ro(a.m[0] + row_));
+    st_vec(a.x[0] + row_, xv);
+    st_vec(a.r[0] + row_, rv);
+    qz[row_ - row0] = zv;
+    acc[0] += rv * zv;
+  }
+  block_partials<1>(acc, a.part + G, G, sm);
+  if (!grid_sync(gs)) {
+    fail(SFR_TIMEOUT, j + 1);
+    return;
+  }
+  grid_totals<1>(a.part + G, G, G, tot, sm);
+  const double di = tot[0];
+  const double beta = di / d;
+  bool stop = false;
+  int status = SFR_OK;
+  unsigned iters = 0;
+  if (sqrt(fabs(di)) < st->conv[0]) {
+    stop = true;
+    iters = j + 1;
+  } else if (!isfinite(beta)) {
+    stop = true;
+    status = SFR_BREAKDOWN;
+    iters = j + 1;
+  } else if (j + 1 >= st->call.maxit) {
+    stop = true;
+    status = SFR_MAXIT;
+    iters = j + 2;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->alpha[0] = alpha;
+    st->beta[0] = beta;
+    st->d[0] = di;
+    st->j = j + 1;
+    if (stop) {
+      st->active[0] = 0;
+      st->status[0] = status;
+      st->iters[0] = static_cast<int>(iters);
+      st->any = 0;
+      if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+    }
+  }
+  if (stop) return;
+  // phase C: p = z + beta p
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    const double p = ld_ro(a.p0[0] + row_);
+    st_vec(a.p0[0] + row_, xadd(qz[row_ - row0], xmul(beta, p)));
+  }
+}
+
 // reliable update, part 1: x += xs (FP64) for the flagged right-hand sides
 template <int K>
 __global__ void __launch_bounds__(256) k_fold(const SArgs<K> a, SState<K> *st, int all) {
@@ -1021,9 +1133,10 @@ struct GraphKey {
   int solver, k, precision, threads, spw;
   int shared_diag;  // the K right-hand sides share one diagonal
   int pf;           // SpMV-phase L2 prefetch distance
+  int fused;        // FP64 PCG, one right-hand side: one cooperative kernel an iteration
   bool operator<(const GraphKey &o) const {
-    return std::tie(solver, k, precision, threads, spw, shared_diag, pf) <
-           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag, o.pf);
+    return std::tie(solver, k, precision, threads, spw, shared_diag, pf, fused) <
+           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag, o.pf, o.fused);
   }
 };
 
@@ -1039,6 +1152,8 @@ struct CachedGraph {
   std::vector<char> args;   // SArgs<K> (host copy, also baked into the nodes)
   cudaGraphConditionalHandle hwhile = 0, hif = 0, hif2 = 0;
   int grid_s = 0, grid_v = 0, threads = 256;
+  int grid_f = 0;        // fused iteration: co-resident blocks
+  size_t smem_f = 0;     // fused iteration: dynamic shared memory a block
   uint64_t last_use = 0;
   int64_t bytes = 0;
 };
@@ -1195,10 +1310,47 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
   return cudaSuccess;
 }
 
+// Launch shape of the fused PCG iteration: the most co-resident 256-thread
+// blocks whose shared memory (8 bytes a row of the block's slices) still lets
+// them all be resident at once.  0 when no shape fits.
+template <typename I>
+int fused_shape(sfr_system *s, size_t *smem) {
+  const int sms = std::max(1, num_sms(s->device));
+  const int nsl = s->A.nslices;
+  const int maxg = std::max(1, (nsl + 7) / 8);
+  for (int per_sm = 8; per_sm >= 1; --per_sm) {
+    const int G = std::min(maxg, per_sm * sms);
+    const size_t bytes = static_cast<size_t>((nsl + G - 1) / G) * kWarp * sizeof(double);
+    if (bytes > 200 * 1024) continue;
+    if (cudaFuncSetAttribute(k_pcg_fused<I>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(bytes)) != cudaSuccess)
+      continue;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_fused<I>, 256, bytes) !=
+        cudaSuccess)
+      continue;
+    if (occ * sms >= G) {
+      *smem = bytes;
+      return G;
+    }
+  }
+  return 0;
+}
+
+GridSync fused_barrier(const CachedGraph *cg) {
+  GridSync g;
+  g.count = cg->counter + 12;
+  g.gen = cg->counter + 13;
+  g.err = reinterpret_cast<int *>(cg->counter + 14);
+  g.nblocks = static_cast<unsigned>(cg->grid_f);
+  g.spin_limit = 1u << 22;
+  return g;
+}
+
 // The graph for one (solver, K, precision, launch shape).
 template <int K, typename I>
 cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, int spw,
-                        int shared_diag, int pf, CachedGraph *cg) {
+                        int shared_diag, int pf, int fused, CachedGraph *cg) {
   SFR_TRY((prepare<K, I>(s, solver, precision, threads, spw, shared_diag, pf, cg)));
   SFR_TRY(cudaGraphCreate(&cg->graph, 0));
   cudaGraph_t g = cg->graph;
@@ -1255,9 +1407,26 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
       SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false, I>, gs, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, false, I>, gs, threads, p2));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, false>, gv, threads, p2));
+      if (fused && K == 1) {
+        // one cooperative kernel an iteration (k_pcg_fused)
+        GridSync gsync = fused_barrier(cg);
+        void *pf3[3] = {&a, &ps, &gsync};
+        cudaKernelNodeParams kp{};
+        kp.func = (void *)k_pcg_fused<I>;
+        kp.gridDim = dim3(cg->grid_f);
+        kp.blockDim = dim3(256);
+        kp.sharedMemBytes = static_cast<unsigned>(cg->smem_f);
+        kp.kernelParams = pf3;
+        cudaGraphNode_t fn;
+        SFR_TRY(cudaGraphAddKernelNode(&fn, body, nullptr, 0, &kp));
+        cudaKernelNodeAttrValue coop{};
+        coop.cooperative = 1;
+        SFR_TRY(cudaGraphKernelNodeSetAttribute(fn, cudaLaunchAttributeCooperative, &coop));
+      } else {
+        SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, false, I>, gs, threads, p2));
+        SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, false>, gv, threads, p2));
+        SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, false>, gv, threads, p2));
+      }
     }
   } else {
     if (mixed) {
@@ -1311,7 +1480,7 @@ void free_graph(CachedGraph *cg) {
 // of finished solves return at once).  For profilers, which cannot look into
 // graphs with conditional nodes; never the production path.
 template <int K, typename I>
-cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
+cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint32_t maxit,
                         cudaStream_t st) {
   SArgs<K> a = *reinterpret_cast<const SArgs<K> *>(cg->args.data());
   a.in_graph = 0;
@@ -1334,6 +1503,15 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
       k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
       k_pcg_start<K, false, I><<<gs, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
+        if constexpr (K == 1) {
+          if (fused) {
+            GridSync gsync = fused_barrier(cg);
+            void *pf3[3] = {&a, &ps, &gsync};
+            SFR_TRY(cudaLaunchCooperativeKernel((void *)k_pcg_fused<I>, dim3(cg->grid_f),
+                                                dim3(256), pf3, cg->smem_f, st));
+            continue;
+          }
+        }
         k_pcg_a<K, false, I><<<gs, t, 0, st>>>(a, ps);
         k_pcg_b<K, false><<<gv, t, 0, st>>>(a, ps);
         k_pcg_c<K, false><<<gv, t, 0, st>>>(a, ps);
@@ -1374,12 +1552,21 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, uint32_t maxit,
 template <int K>
 int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, double *d_x,
         double tol, uint32_t maxit, int newx, int precision, double delta, int threads, int spw,
-        int pf, bool loop, cudaStream_t st, SolveOut *out, float *ms) {
+        int pf, int fused, bool loop, cudaStream_t st, SolveOut *out, float *ms) {
   const int n = s->n;
   if (maxit == 0) return SFR_BAD_INPUT;
   EngineCache &ec = g_engines[s];
   const int shared_diag = K > 1 && !d_diag_k ? 1 : 0;
-  GraphKey key{solver, K, precision, threads, spw, shared_diag, pf};
+  // the fused iteration serves FP64 PCG with one right-hand side when a
+  // co-resident shape exists; other solves take the three-kernel iteration
+  fused = fused && K == 1 && solver == SFR_PCG && precision == SFR_FP64 ? 1 : 0;
+  size_t smem_f = 0;
+  int grid_f = 0;
+  if (fused) {
+    grid_f = s->A.off ? fused_shape<int16_t>(s, &smem_f) : fused_shape<int>(s, &smem_f);
+    if (grid_f <= 0) fused = 0;
+  }
+  GraphKey key{solver, K, precision, threads, spw, shared_diag, pf, fused};
   auto it = ec.graphs.find(key);
   if (it == ec.graphs.end()) {
     if (ec.graphs.size() >= kMaxGraphsPerSystem) {  // drop the least recently used
@@ -1390,10 +1577,13 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
       ec.graphs.erase(lru);
     }
     auto cg = std::make_unique<CachedGraph>();
+    cg->grid_f = grid_f;
+    cg->smem_f = smem_f;
     const cudaError_t be =
-        s->A.off
-            ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, pf, cg.get())
-            : build_graph<K, int>(s, solver, precision, threads, spw, shared_diag, pf, cg.get());
+        s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, pf,
+                                           fused, cg.get())
+                 : build_graph<K, int>(s, solver, precision, threads, spw, shared_diag, pf,
+                                       fused, cg.get());
     if (be != cudaSuccess) {
       set_last_error(cudaGetErrorString(be));
       free_graph(cg.get());
@@ -1428,8 +1618,8 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
     err = cudaMemcpyAsync(cg->d_state, &call, sizeof(call), cudaMemcpyHostToDevice, st);
   if (err == cudaSuccess)
     err = !loop     ? cudaGraphLaunch(cg->exec, st)
-          : s->A.off ? launch_loop<K, int16_t>(cg, solver, mixed, maxit, st)
-                     : launch_loop<K, int>(cg, solver, mixed, maxit, st);
+          : s->A.off ? launch_loop<K, int16_t>(cg, solver, mixed, fused, maxit, st)
+                     : launch_loop<K, int>(cg, solver, mixed, fused, maxit, st);
   for (int k = 0; k < K && err == cudaSuccess; ++k)
     err = cudaMemcpyAsync(d_x + static_cast<size_t>(k) * n, a.x[k], vb, cudaMemcpyDeviceToDevice,
                           st);
@@ -1452,8 +1642,8 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
 
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,
-                 int32_t precision, double delta, int threads, int spw, int pf, bool loop,
-                 cudaStream_t st, sfr_solve_info *info) {
+                 int32_t precision, double delta, int threads, int spw, int pf, int fused,
+                 bool loop, cudaStream_t st, sfr_solve_info *info) {
   if (k < 1 || k > kMaxK) return SFR_BAD_INPUT;
   if (threads != 128 && threads != 256) return SFR_BAD_INPUT;
   if (spw < 0 || spw > 64) return SFR_BAD_INPUT;
@@ -1462,10 +1652,10 @@ int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_
   float ms = 0.f;
   int rc;
   switch (k) {
-    case 1: rc = run<1>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
-    case 2: rc = run<2>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
-    case 3: rc = run<3>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
-    default: rc = run<4>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, loop, st, out, &ms); break;
+    case 1: rc = run<1>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, fused, loop, st, out, &ms); break;
+    case 2: rc = run<2>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, fused, loop, st, out, &ms); break;
+    case 3: rc = run<3>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, fused, loop, st, out, &ms); break;
+    default: rc = run<4>(s, solver, d_diag_k, d_b, d_x, tol, maxit, newx, precision, delta, threads, spw, pf, fused, loop, st, out, &ms); break;
   }
   if (rc != SFR_OK) return rc;
   int worst = SFR_OK;

@@ -56,9 +56,10 @@ class SolveInfo:
 
 class TuneResultC(ctypes.Structure):
     _fields_ = [("engine", _I32), ("threads", _I32), ("slices_per_warp", _I32),
-                ("prefetch", _I32), ("ms", ctypes.c_double), ("default_engine", _I32),
-                ("default_threads", _I32), ("default_slices_per_warp", _I32),
-                ("default_prefetch", _I32), ("default_ms", ctypes.c_double),
+                ("prefetch", _I32), ("fused", _I32), ("ms", ctypes.c_double),
+                ("default_engine", _I32), ("default_threads", _I32),
+                ("default_slices_per_warp", _I32), ("default_prefetch", _I32),
+                ("default_fused", _I32), ("default_ms", ctypes.c_double),
                 ("candidates", _I32), ("source", _I32)]
 
 
@@ -106,6 +107,7 @@ def lib() -> ctypes.CDLL:
     L.sfr_gpu_destroy.argtypes = [_P]
     L.sfr_gpu_set_engine.argtypes = [_P, _I32, _I32, _I32]
     L.sfr_gpu_set_prefetch.argtypes = [_P, _I32]
+    L.sfr_gpu_set_fused.argtypes = [_P, _I32]
     L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_transpose.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_dot.argtypes = [_P, _P, _P, _P, _P]
@@ -225,6 +227,13 @@ class GpuSystem:
         rc = lib().sfr_gpu_set_prefetch(self.h, rounds)
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_prefetch")
+
+    def set_fused(self, flag: bool):
+        """Graph engine, FP64 PCG with one right-hand side: one cooperative
+        kernel an iteration (sfr_gpu_set_fused)."""
+        rc = lib().sfr_gpu_set_fused(self.h, int(bool(flag)))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_fused")
 
     def autotune(self, solver: int, b, ad_k=None, tol: float = 1e-10, maxit: int = 100000,
                  precision: int = FP64) -> dict:

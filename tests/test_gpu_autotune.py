@@ -61,24 +61,34 @@ def test_autotune_choice_is_kept_and_solves_at_parity(cuda, tmp_path, monkeypatc
     g.close()
 
 
-@pytest.mark.parametrize("engine,threads,spw", [(2, 128, 0), (2, 256, 2), (2, 256, 8),
-                                                (1, 0, 0)])
-def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw):
+@pytest.mark.parametrize("engine,threads,spw,pf,fused",
+                         [(2, 128, 0, 0, 0), (2, 256, 2, 0, 0), (2, 256, 8, 0, 0),
+                          (2, 256, 0, 2, 0), (2, 256, 0, 0, 1), (3, 256, 0, 0, 1),
+                          (1, 0, 0, 0, 0)])
+def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf, fused):
     """Whatever the tuner picks, the arithmetic is the reference's: every
-    candidate engine and launch shape solves at the FP64 bar."""
+    candidate engine and launch shape (the L2 prefetch, the fused one-kernel
+    PCG iteration, also launched from a host loop) solves at the FP64 bar."""
     s = S.poisson_jittered(40, seed=22)
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     g.set_values(s.al, s.ad)
     g.set_engine(engine, threads, spw if spw else -1)
+    g.set_prefetch(pf)
+    g.set_fused(bool(fused))
     ref = O.pcg(O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=TOL)
-    x, info = g.solve(sv.PCG, s.b[0], tol=TOL)
+    maxit = ref.iters + 5 if engine == 3 else 100000  # the host loop runs exactly maxit
+    x, info = g.solve(sv.PCG, s.b[0], tol=TOL, maxit=maxit)
     assert info.status == sv.OK and abs(info.iters - ref.iters) <= 1
     assert rel(x, ref.x) < 1e-12
+    x2, info2 = g.solve(sv.PCG, s.b[0], tol=TOL, maxit=maxit)
+    assert bits_equal(x, x2) and info2.iters == info.iters
     m = S.momentum(24, nrhs=3, seed=23)
     gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
     gm.set_values(m.al, m.ad)
     gm.set_engine(engine, threads, spw if spw else -1)
-    xs, infos = gm.solve_multi(sv.PBICGSTAB, m.b, tol=TOL)
+    gm.set_prefetch(pf)
+    gm.set_fused(bool(fused))
+    xs, infos = gm.solve_multi(sv.PBICGSTAB, m.b, tol=TOL, maxit=200 if engine == 3 else 100000)
     for k in range(3):
         refk = O.pbicgstab(O.CSRD, True, m.ia, m.ja, m.al, m.ad, m.b[k], tol=TOL)
         assert infos[k].status == sv.OK and abs(infos[k].iters - refk.iters) <= 1
