@@ -167,9 +167,9 @@ def pcg_alg_bytes(n, nnz_off, iters):
     return (iters + 2) * spmv_alg_bytes(n, nnz_off) + iters * 88 * n
 
 
-def pcg_kernel_launches(iters):
-    # setup, start, three kernels per iteration, post-processing
-    return 3 * iters + 3
+def pcg_kernel_launches(iters, fused=False):
+    # setup, start, three kernels (fused: one) per iteration, post-processing
+    return (1 if fused else 3) * iters + 3
 
 
 # --------------------------------------------------------------- ours ----
@@ -425,7 +425,9 @@ def run_ours(args):
 
     alg = pcg_alg_bytes(N, nnz, iters)
     achieved = alg / (ms_step * 1e-3) / 1e9
-    tr = committed_traffic("pcg_fp64_iteration")
+    # the timed solves' engine: the autotuner's choice, or the flags given
+    fused = bool(tune["headline_fp64"]["fused"]) if tune else bool(args.fused)
+    tr = committed_traffic("pcg_fp64_fused_iteration" if fused else "pcg_fp64_iteration")
     traffic = None
     if tr is not None and tr[1] == "per_iteration_128":
         traffic = tr[0] * (N / 128 ** 3) * iters
@@ -447,14 +449,20 @@ def run_ours(args):
                                f"permuted + RCM; Jacobi-PCG FP64 to 1e-10 (M-norm)",
                    "rows": N, "nnz_offdiag": nnz, "iterations": iters,
                    "format": "SELL-32 from CSRD: FP64 values, 16-bit column offsets",
-                   "engine": "CUDA graph, device-side WHILE loop (3 kernels per iteration)",
+                   "engine": ("CUDA graph, device-side WHILE loop, one cooperative kernel per "
+                              "iteration (k_pcg_fused: SpMV+dot, grid barrier, x/r/z update+dot, "
+                              "grid barrier, p update; q and z kept in shared memory)"
+                              if fused else
+                              "CUDA graph, device-side WHILE loop (3 kernels per iteration)"),
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
         "iterations": iters,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "PCG solve graph (one launch per solve: k_pcg_a SpMV+dot, "
-                               "k_pcg_b update+dot, k_pcg_c direction per iteration)",
+                     "kernel": ("PCG solve graph (one launch per solve: k_pcg_fused per "
+                                "iteration)" if fused else
+                                "PCG solve graph (one launch per solve: k_pcg_a SpMV+dot, "
+                                "k_pcg_b update+dot, k_pcg_c direction per iteration)"),
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": alg,
                      "alg_bytes_rule": "(iters+2)*(12 nnz_off + 4(N+1) + 24N) + iters*88N",
@@ -475,7 +483,7 @@ def run_ours(args):
         "autotune": tune,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": args.steps * pcg_kernel_launches(iters),
+        "gpu_launches": args.steps * pcg_kernel_launches(iters, fused),
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }

@@ -3,7 +3,8 @@
 // WHILE node, like the graph engine's PCG (stream_solve.cu), so no dot
 // product travels to the host.
 //
-// One iteration is three kernels:
+// One iteration is one cooperative kernel (k_mr_fused, when a co-resident
+// launch shape exists) or three kernels:
 //   a. p = A z0 and (z0, p); the last block forms alpha = (z0, p) / beta^2
 //      and the three-term coefficients t1 = 1/beta, t2 = -alpha/beta,
 //      t3 = -beta/beta_old;
@@ -42,7 +43,7 @@ namespace {
 
 constexpr int kMrThreads = 256;
 constexpr int kMrUnroll = 6;  // vector roles rotate with periods 3 and 2
-constexpr int kMrCounters = 8;
+constexpr int kMrCounters = 16;  // 0-4 last-block counters, 12-14 the grid barrier
 
 struct MrState {
   // per call
@@ -206,6 +207,59 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_a(const MrArgs a, int u) {
   }
 }
 
+// The scalar part of one iteration (Iters.c:431-470) on a copy of the state:
+// zp = (z, p) of the new Lanczos vector.  Sets beta, the rotation, u1..u4,
+// |r|, the stop decision (convergence, breakdown -- a non-finite u, before
+// the update, as the reference breaks -- or maxIt) and j + 1.
+__device__ void mr_step(MrState &q, double alpha, double zp) {
+  const unsigned j = q.j;
+  const double beta_old = q.beta;
+  const double beta = xsqrt(zp);
+  double c = q.c, s = q.s, ro1 = q.ro1;
+  const double c_old = q.c_old, s_old = q.s_old;
+  const double delta = xsub(xmul(c, alpha), xmul(xmul(c_old, s), beta_old));
+  const double ro2 = xadd(xmul(s, alpha), xmul(xmul(c_old, c), beta_old));
+  const double ro3 = xmul(s_old, beta_old);
+  q.c_old = c;
+  q.s_old = s;
+  sym_ortho_dev(delta, beta, &c, &s, &ro1);
+  q.c = c;
+  q.s = s;
+  q.ro1 = ro1;
+  q.beta_old = beta_old;
+  q.beta = beta;
+  const double u1 = xdiv(1.0, xmul(beta_old, ro1));
+  const double u2 = xdiv(-ro2, ro1);
+  const double u3 = xdiv(-ro3, ro1);
+  const double u4 = xmul(c, q.neta);
+  if (!isfinite(u1) || !isfinite(u2) || !isfinite(u3) || !isfinite(u4)) {
+    q.status = SFR_BREAKDOWN;
+    q.upd = 0;
+    q.active = 0;
+    q.iters = static_cast<int>(min(j + 1, q.maxit)) + 1;
+  } else {
+    q.u1 = u1;
+    q.u2 = u2;
+    q.u3 = u3;
+    q.u4 = u4;
+    q.upd = 1;
+    const double norm_r = xmul(fabs(s), q.norm_r);
+    q.norm_r = norm_r;
+    if (norm_r < q.conv) {
+      q.active = 0;
+      q.iters = static_cast<int>(j) + 1;
+    } else {
+      q.neta = xmul(-s, q.neta);
+      if (j + 1 >= q.maxit) {
+        q.active = 0;
+        q.status = SFR_MAXIT;
+        q.iters = static_cast<int>(q.maxit) + 1;
+      }
+    }
+  }
+  q.j = j + 1;
+}
+
 // b: the new Lanczos vector and the scalar step (Iters.c:413-470)
 __global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
   SFR_SHARED_RED(1);
@@ -229,54 +283,10 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
   }
   if (!last_block<1>(acc, a.part, a.counter + 3, sm)) return;
   if (threadIdx.x == 0) {
-    const unsigned j = st->j;
-    const double alpha = st->alpha;
-    const double beta_old = st->beta;
-    const double beta = xsqrt(sm[0]);
-    double c = st->c, s = st->s, ro1 = st->ro1;
-    const double c_old = st->c_old, s_old = st->s_old;
-    const double delta = xsub(xmul(c, alpha), xmul(xmul(c_old, s), beta_old));
-    const double ro2 = xadd(xmul(s, alpha), xmul(xmul(c_old, c), beta_old));
-    const double ro3 = xmul(s_old, beta_old);
-    st->c_old = c;
-    st->s_old = s;
-    sym_ortho_dev(delta, beta, &c, &s, &ro1);
-    st->c = c;
-    st->s = s;
-    st->ro1 = ro1;
-    st->beta_old = beta_old;
-    st->beta = beta;
-    const double u1 = xdiv(1.0, xmul(beta_old, ro1));
-    const double u2 = xdiv(-ro2, ro1);
-    const double u3 = xdiv(-ro3, ro1);
-    const double u4 = xmul(c, st->neta);
-    if (!isfinite(u1) || !isfinite(u2) || !isfinite(u3) || !isfinite(u4)) {
-      st->status = SFR_BREAKDOWN;
-      st->upd = 0;
-      st->active = 0;
-      st->iters = static_cast<int>(min(j + 1, st->maxit)) + 1;
-    } else {
-      st->u1 = u1;
-      st->u2 = u2;
-      st->u3 = u3;
-      st->u4 = u4;
-      st->upd = 1;
-      const double norm_r = xmul(fabs(s), st->norm_r);
-      st->norm_r = norm_r;
-      if (norm_r < st->conv) {
-        st->active = 0;
-        st->iters = static_cast<int>(j) + 1;
-      } else {
-        st->neta = xmul(-s, st->neta);
-        if (j + 1 >= st->maxit) {
-          st->active = 0;
-          st->status = SFR_MAXIT;
-          st->iters = static_cast<int>(st->maxit) + 1;
-        }
-      }
-    }
-    st->j = j + 1;
-    if (!st->active) cudaGraphSetConditional(a.hwhile, 0u);
+    MrState q = *st;
+    mr_step(q, q.alpha, sm[0]);
+    *st = q;
+    if (!q.active) cudaGraphSetConditional(a.hwhile, 0u);
   }
 }
 
@@ -293,6 +303,106 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_c(const MrArgs a, int u) {
                            xmul(u3, ld_ro(w00 + i)));
     w[i] = wi;
     a.x[i] = xadd(a.x[i], xmul(u4, wi));
+  }
+}
+
+// One whole iteration in one cooperative launch: a, b and c above with two
+// grid barriers between them.  A block keeps A z0 and z0 of its own rows in
+// shared memory from phase a to phases b and c.  Each barrier's dot product
+// is reduced by every block over all block partials in the same fixed
+// order, and every block runs the scalar step itself on those totals, so all
+// blocks take the same decisions; block 0 writes the state back.  Bounded
+// barriers: a wait that gives up records SFR_TIMEOUT and the solve stops.
+template <typename I>
+__global__ void __launch_bounds__(kMrThreads) k_mr_fused(const MrArgs a, int u, GridSync gs) {
+  __shared__ double sm[64];
+  __shared__ MrState q;
+  extern __shared__ double rows[];  // per own row: A z0, then z0
+  MrState *st = a.st;
+  if (!st->active) return;
+  const int n = a.n;
+  const int lane = threadIdx.x & 31;
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  const int row0 = s0 * kWarp;
+  const int nrow = (s1 - s0) * kWarp;
+  const int G = gridDim.x;
+  const double *z0 = a.Z[u % 2];
+  const double *v0 = a.V[u % 3], *v = a.V[(u + 1) % 3];
+  double *p = a.V[(u + 2) % 3];
+  double *z = a.Z[(u + 1) % 2];
+  const double *w00 = a.W[u % 3], *w0 = a.W[(u + 1) % 3];
+  double *w = a.W[(u + 2) % 3];
+  if (threadIdx.x == 0) q = *st;
+  __syncthreads();
+  auto fail = [&](int status) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->active = 0;
+      st->upd = 0;
+      st->status = status;
+      st->iters = static_cast<int>(q.j) + 1;
+      cudaGraphSetConditional(a.hwhile, 0u);
+    }
+  };
+  // a: A z0, (z0, A z0)
+  const int all[1] = {1};
+  const double *const diag[1] = {a.ad};
+  double acc[1] = {0.0};
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    double y[1];
+    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val, diag, s_, lane, all,
+                                 [&](int, int c) { return ld_ro(z0 + c); }, y);
+    const double zr = ld_ro(z0 + row_);
+    rows[row_ - row0] = y[0];
+    rows[nrow + row_ - row0] = zr;
+    acc[0] += zr * y[0];
+  }
+  block_partials<1>(acc, a.part, G, sm);
+  if (!grid_sync(gs)) {
+    fail(SFR_TIMEOUT);
+    return;
+  }
+  double tot[1];
+  grid_totals<1>(a.part, G, G, tot, sm);
+  const double beta = q.beta;
+  const double alpha = xmul(tot[0], xdiv(1.0, xmul(beta, beta)));
+  const double t1 = xdiv(1.0, beta), t2 = xdiv(-alpha, beta), t3 = xdiv(-beta, q.beta_old);
+  // b: p = t1 A z0 + t2 v + t3 v0, z = M p, (z, p)
+  acc[0] = 0.0;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    const double pi = xadd(xadd(xmul(t1, rows[row_ - row0]), xmul(t2, ld_ro(v + row_))),
+                           xmul(t3, ld_ro(v0 + row_)));
+    st_vec(p + row_, pi);
+    const double zi = xmul(pi, ld_ro(a.m + row_));
+    st_vec(z + row_, zi);
+    acc[0] += zi * pi;
+  }
+  block_partials<1>(acc, a.part + G, G, sm);
+  if (!grid_sync(gs)) {
+    fail(SFR_TIMEOUT);
+    return;
+  }
+  grid_totals<1>(a.part + G, G, G, tot, sm);
+  if (threadIdx.x == 0) {
+    q.alpha = alpha;
+    q.t1 = t1;
+    q.t2 = t2;
+    q.t3 = t3;
+    mr_step(q, alpha, tot[0]);
+    if (blockIdx.x == 0) {
+      *st = q;
+      if (!q.active) cudaGraphSetConditional(a.hwhile, 0u);
+    }
+  }
+  __syncthreads();
+  if (!q.upd) return;
+  // c: w = u1 z0 + u2 w0 + u3 w00, x += u4 w
+  const double u1 = q.u1, u2 = q.u2, u3 = q.u3, u4 = q.u4;
+  SFR_FOR_OWN_ROWS(s0, s1) {
+    const double wi = xadd(xadd(xmul(u1, rows[nrow + row_ - row0]), xmul(u2, ld_ro(w0 + row_))),
+                           xmul(u3, ld_ro(w00 + row_)));
+    st_vec(w + row_, wi);
+    st_vec(a.x + row_, xadd(ld_vec(a.x + row_), xmul(u4, wi)));
   }
 }
 
@@ -341,7 +451,36 @@ struct MrGraph {
   void *ws = nullptr;
   MrArgs args{};
   int gs = 0, gv = 0;
+  int gf = 0;         // fused iteration: co-resident blocks (0: three kernels)
+  size_t smem_f = 0;  // fused iteration: dynamic shared memory a block
 };
+
+// The fused iteration's launch shape: the most co-resident blocks whose
+// shared memory (16 bytes a row of the block's slices) still lets them all
+// be resident at once; 0 when none does.
+template <typename I>
+int mr_fused_shape(const sfr_system *s, size_t *smem) {
+  const int sms = std::max(1, num_sms(s->device));
+  const int nsl = s->A.nslices;
+  const int maxg = std::max(1, (nsl + 7) / 8);
+  for (int per_sm = 8; per_sm >= 1; --per_sm) {
+    const int G = std::min(maxg, per_sm * sms);
+    const size_t bytes = static_cast<size_t>((nsl + G - 1) / G) * kWarp * 2 * sizeof(double);
+    if (bytes > 200 * 1024) continue;
+    if (cudaFuncSetAttribute(k_mr_fused<I>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(bytes)) != cudaSuccess)
+      continue;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mr_fused<I>, kMrThreads, bytes) !=
+        cudaSuccess)
+      continue;
+    if (occ * sms >= G) {
+      *smem = bytes;
+      return G;
+    }
+  }
+  return 0;
+}
 
 std::map<const sfr_system *, std::unique_ptr<MrGraph>> g_mr;
 
@@ -426,14 +565,38 @@ cudaError_t build(sfr_system *s, MrGraph *g) {
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   cudaGraphNode_t bp = nullptr;
   int us[kMrUnroll];
-  void *pu[kMrUnroll][2];
+  void *pu[kMrUnroll][3];
+  g->gf = mr_fused_shape<I>(s, &g->smem_f);
+  GridSync gsync;
+  gsync.count = a.counter + 12;
+  gsync.gen = a.counter + 13;
+  gsync.err = reinterpret_cast<int *>(a.counter + 14);
+  gsync.nblocks = static_cast<unsigned>(g->gf);
+  gsync.spin_limit = 1u << 22;
   for (int u = 0; u < kMrUnroll; ++u) {
     us[u] = u;
     pu[u][0] = &a;
     pu[u][1] = &us[u];
-    SFR_TRY(node(body, &bp, (void *)k_mr_a<I>, g->gs, pu[u]));
-    SFR_TRY(node(body, &bp, (void *)k_mr_b, g->gv, pu[u]));
-    SFR_TRY(node(body, &bp, (void *)k_mr_c, g->gv, pu[u]));
+    pu[u][2] = &gsync;
+    if (g->gf > 0) {
+      // one cooperative kernel an iteration
+      cudaKernelNodeParams kp{};
+      kp.func = (void *)k_mr_fused<I>;
+      kp.gridDim = dim3(g->gf);
+      kp.blockDim = dim3(kMrThreads);
+      kp.sharedMemBytes = static_cast<unsigned>(g->smem_f);
+      kp.kernelParams = pu[u];
+      cudaGraphNode_t fn;
+      SFR_TRY(cudaGraphAddKernelNode(&fn, body, bp ? &bp : nullptr, bp ? 1 : 0, &kp));
+      cudaKernelNodeAttrValue coop{};
+      coop.cooperative = 1;
+      SFR_TRY(cudaGraphKernelNodeSetAttribute(fn, cudaLaunchAttributeCooperative, &coop));
+      bp = fn;
+    } else {
+      SFR_TRY(node(body, &bp, (void *)k_mr_a<I>, g->gs, pu[u]));
+      SFR_TRY(node(body, &bp, (void *)k_mr_b, g->gv, pu[u]));
+      SFR_TRY(node(body, &bp, (void *)k_mr_c, g->gv, pu[u]));
+    }
   }
   SFR_TRY(node(g->graph, &prev, (void *)k_mr_post<I>, g->gs, p1));
   SFR_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
