@@ -156,13 +156,15 @@ int sfr_gpu_set_engine(sfr_system *s, int32_t engine, int32_t threads,
  * (the default) turns it off; at most 8. */
 int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
 
-/* Graph engine, FP64 PCG with one right-hand side: flag != 0 runs each
+/* Graph engine, FP64 PCG with one right-hand side: mode 1 runs each
  * iteration as one cooperative kernel (SpMV and dot, grid barrier, x/r/z
  * update and dot, grid barrier, p update) that keeps q = A p and then
- * z = M r of a block's rows in shared memory instead of HBM.  Solves it does
- * not serve (other solvers, K > 1, mixed precision, or no co-resident
- * shape) take the three-kernel iteration.  0 (the default) turns it off. */
-int sfr_gpu_set_fused(sfr_system *s, int32_t flag);
+ * z = M r of a block's rows in shared memory instead of HBM; mode 2 is the
+ * same kernel held to 40 registers so that six blocks fit an SM.  Solves it
+ * does not serve (other solvers, K > 1, mixed precision, or no co-resident
+ * shape) take the three-kernel iteration.  0 (the default) turns it off;
+ * other values are SFR_BAD_INPUT. */
+int sfr_gpu_set_fused(sfr_system *s, int32_t mode);
 
 /* Result of sfr_gpu_autotune. */
 typedef struct {
@@ -170,7 +172,7 @@ typedef struct {
   int32_t threads;          /* graph engine block size */
   int32_t slices_per_warp;  /* graph engine SpMV phases: 0 one wave, else slices per warp */
   int32_t prefetch;         /* graph engine SpMV-phase L2 prefetch distance (rounds) */
-  int32_t fused;            /* graph engine FP64 PCG: one kernel an iteration */
+  int32_t fused;            /* graph engine FP64 PCG: one kernel an iteration (mode) */
   double ms;                /* the choice's solve time (ms, CUDA events) */
   int32_t default_engine, default_threads, default_slices_per_warp, default_prefetch,
       default_fused;

@@ -228,10 +228,11 @@ class GpuSystem:
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_prefetch")
 
-    def set_fused(self, flag: bool):
+    def set_fused(self, mode: int):
         """Graph engine, FP64 PCG with one right-hand side: one cooperative
-        kernel an iteration (sfr_gpu_set_fused)."""
-        rc = lib().sfr_gpu_set_fused(self.h, int(bool(flag)))
+        kernel an iteration (sfr_gpu_set_fused; 1, or 2 for the 40-register
+        form, 0 off)."""
+        rc = lib().sfr_gpu_set_fused(self.h, int(mode))
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_fused")
 

@@ -63,7 +63,8 @@ def test_autotune_choice_is_kept_and_solves_at_parity(cuda, tmp_path, monkeypatc
 
 @pytest.mark.parametrize("engine,threads,spw,pf,fused",
                          [(2, 128, 0, 0, 0), (2, 256, 2, 0, 0), (2, 256, 8, 0, 0),
-                          (2, 256, 0, 2, 0), (2, 256, 0, 0, 1), (3, 256, 0, 0, 1),
+                          (2, 256, 0, 2, 0), (2, 256, 0, 0, 1), (2, 256, 0, 0, 2),
+                          (3, 256, 0, 0, 1),
                           (1, 0, 0, 0, 0)])
 def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf, fused):
     """Whatever the tuner picks, the arithmetic is the reference's: every
@@ -74,7 +75,7 @@ def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf
     g.set_values(s.al, s.ad)
     g.set_engine(engine, threads, spw if spw else -1)
     g.set_prefetch(pf)
-    g.set_fused(bool(fused))
+    g.set_fused(fused)
     ref = O.pcg(O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=TOL)
     maxit = ref.iters + 5 if engine == 3 else 100000  # the host loop runs exactly maxit
     x, info = g.solve(sv.PCG, s.b[0], tol=TOL, maxit=maxit)
@@ -87,7 +88,7 @@ def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf
     gm.set_values(m.al, m.ad)
     gm.set_engine(engine, threads, spw if spw else -1)
     gm.set_prefetch(pf)
-    gm.set_fused(bool(fused))
+    gm.set_fused(fused)
     xs, infos = gm.solve_multi(sv.PBICGSTAB, m.b, tol=TOL, maxit=200 if engine == 3 else 100000)
     for k in range(3):
         refk = O.pbicgstab(O.CSRD, True, m.ia, m.ja, m.al, m.ad, m.b[k], tol=TOL)
