@@ -3,8 +3,11 @@
 // WHILE node, like the graph engine's PCG (stream_solve.cu), so no dot
 // product travels to the host.
 //
-// One iteration is one cooperative kernel (k_mr_fused, when a co-resident
-// launch shape exists) or three kernels:
+// One iteration is three kernels, or, with the handle's fused-iteration
+// option (sfr_gpu_set_fused) and a co-resident launch shape, one cooperative
+// kernel (k_mr_fused; at 128^3 it measured slower, 126 against 97 us an
+// iteration: 55 registers and 57 KB of shared memory a block leave four
+// blocks an SM for the SpMV phase).  The three kernels:
 //   a. p = A z0 and (z0, p); the last block forms alpha = (z0, p) / beta^2
 //      and the three-term coefficients t1 = 1/beta, t2 = -alpha/beta,
 //      t3 = -beta/beta_old;
@@ -75,6 +78,17 @@ struct MrArgs {
 
 #define SFR_MR_FOR_ROWS(i) \
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+
+// Row pairs (2i, 2i+1) with 16-byte loads; every vector of the graph's
+// workspace has room for an even count, and its padding entries stay 0.
+#define SFR_MR_FOR_PAIRS(i)                                                          \
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; 2 * i < a.n;                  \
+       i += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ double2 ld2(const double *p) {
+  return *reinterpret_cast<const double2 *>(p);
+}
+__device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
 
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
@@ -273,13 +287,18 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
   double *p = a.V[(u + 2) % 3];
   double *z = a.Z[(u + 1) % 2];
   double acc[1] = {0.0};
-  SFR_MR_FOR_ROWS(i) {
-    const double pi = xadd(xadd(xmul(t1, ld_vec(p + i)), xmul(t2, ld_ro(v + i))),
-                           xmul(t3, ld_ro(v0 + i)));
-    p[i] = pi;
-    const double zi = xmul(pi, ld_ro(a.m + i));
-    z[i] = zi;
-    acc[0] += zi * pi;
+  SFR_MR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const double2 pv = ld2(p + r), vv = ld2(v + r), v0v = ld2(v0 + r), mv = ld2(a.m + r);
+    double2 pn, zn;
+    pn.x = xadd(xadd(xmul(t1, pv.x), xmul(t2, vv.x)), xmul(t3, v0v.x));
+    pn.y = xadd(xadd(xmul(t1, pv.y), xmul(t2, vv.y)), xmul(t3, v0v.y));
+    zn.x = xmul(pn.x, mv.x);
+    zn.y = xmul(pn.y, mv.y);
+    st2(p + r, pn);
+    st2(z + r, zn);
+    acc[0] += zn.x * pn.x;
+    if (r + 1 < a.n) acc[0] += zn.y * pn.y;
   }
   if (!last_block<1>(acc, a.part, a.counter + 3, sm)) return;
   if (threadIdx.x == 0) {
@@ -298,11 +317,16 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_c(const MrArgs a, int u) {
   const double *z0 = a.Z[u % 2];
   const double *w00 = a.W[u % 3], *w0 = a.W[(u + 1) % 3];
   double *w = a.W[(u + 2) % 3];
-  SFR_MR_FOR_ROWS(i) {
-    const double wi = xadd(xadd(xmul(u1, ld_ro(z0 + i)), xmul(u2, ld_ro(w0 + i))),
-                           xmul(u3, ld_ro(w00 + i)));
-    w[i] = wi;
-    a.x[i] = xadd(a.x[i], xmul(u4, wi));
+  SFR_MR_FOR_PAIRS(i) {
+    const int r = 2 * i;
+    const double2 zv = ld2(z0 + r), w0v = ld2(w0 + r), w00v = ld2(w00 + r);
+    double2 xv = ld2(a.x + r), wn;
+    wn.x = xadd(xadd(xmul(u1, zv.x), xmul(u2, w0v.x)), xmul(u3, w00v.x));
+    wn.y = xadd(xadd(xmul(u1, zv.y), xmul(u2, w0v.y)), xmul(u3, w00v.y));
+    xv.x = xadd(xv.x, xmul(u4, wn.x));
+    xv.y = xadd(xv.y, xmul(u4, wn.y));
+    st2(w + r, wn);
+    st2(a.x + r, xv);
   }
 }
 
@@ -453,6 +477,7 @@ struct MrGraph {
   int gs = 0, gv = 0;
   int gf = 0;         // fused iteration: co-resident blocks (0: three kernels)
   size_t smem_f = 0;  // fused iteration: dynamic shared memory a block
+  int fused = 0;      // the handle's fused-iteration option this graph was built for
 };
 
 // The fused iteration's launch shape: the most co-resident blocks whose
@@ -504,7 +529,8 @@ cudaError_t node(cudaGraph_t g, cudaGraphNode_t *prev, void *func, int grid, voi
 }
 
 template <typename I>
-cudaError_t build(sfr_system *s, MrGraph *g) {
+cudaError_t build(sfr_system *s, int fused, MrGraph *g) {
+  g->fused = fused;
   const int n = s->n;
   const size_t vb = (sizeof(double) * static_cast<size_t>(std::max(n, 1)) + 255) & ~size_t{255};
   int occ = 0;
@@ -514,7 +540,8 @@ cudaError_t build(sfr_system *s, MrGraph *g) {
     occ = 1;
   const int sms = std::max(1, num_sms(s->device));
   g->gs = std::max(1, std::min((s->A.nslices + 7) / 8, occ * sms));
-  g->gv = std::max(1, std::min(sms * (2048 / kMrThreads), (n + kMrThreads - 1) / kMrThreads));
+  const int npairs = (n + 1) / 2;  // the vector phases move row pairs
+  g->gv = std::max(1, std::min(sms * (2048 / kMrThreads), (npairs + kMrThreads - 1) / kMrThreads));
   const int gmax = std::max(g->gs, g->gv);
   const size_t part_b = (sizeof(double) * 4 * static_cast<size_t>(gmax) + 255) & ~size_t{255};
   const size_t total = vb * 12 + part_b + 256 + sizeof(MrState);
@@ -566,7 +593,7 @@ cudaError_t build(sfr_system *s, MrGraph *g) {
   cudaGraphNode_t bp = nullptr;
   int us[kMrUnroll];
   void *pu[kMrUnroll][3];
-  g->gf = mr_fused_shape<I>(s, &g->smem_f);
+  g->gf = fused ? mr_fused_shape<I>(s, &g->smem_f) : 0;
   GridSync gsync;
   gsync.count = a.counter + 12;
   gsync.gen = a.counter + 13;
@@ -609,9 +636,15 @@ int solve_minres_graph(sfr_system *s, const double *d_diag, const double *d_b, d
                        double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
                        sfr_solve_info *info) {
   auto &slot = g_mr[s];
+  const int fused = s->graph_fused ? 1 : 0;
+  if (slot && slot->fused != fused) {
+    free_mr(slot.get());
+    slot.reset();
+  }
   if (!slot) {
     slot = std::make_unique<MrGraph>();
-    const cudaError_t be = s->A.off ? build<int16_t>(s, slot.get()) : build<int>(s, slot.get());
+    const cudaError_t be =
+        s->A.off ? build<int16_t>(s, fused, slot.get()) : build<int>(s, fused, slot.get());
     if (be != cudaSuccess) {
       set_last_error(cudaGetErrorString(be));
       free_mr(slot.get());

@@ -434,11 +434,9 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
 // with the same expressions as in k_pcg_a/b/c (bit-identical rows).
 // The barriers are bounded: a wait that gives up records SFR_TIMEOUT, every
 // block leaves, and the solve stops with that status.
-// kMinBlocks: the blocks an SM should hold -- 5 (at most 51 registers,
-// fused mode 1) or 6 (at most 40 registers, fused mode 2).
-template <typename I, int kMinBlocks>
-__global__ void __launch_bounds__(256, kMinBlocks) k_pcg_fused(const SArgs<1> a, SState<1> *st,
-                                                               GridSync gs) {
+template <typename I>
+__device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
+                                               const GridSync &gs) {
   __shared__ double sm[32 * 2];
   extern __shared__ double qz[];  // this block's rows: q, then z
   if (!st->any) return;
@@ -535,6 +533,24 @@ __global__ void __launch_bounds__(256, kMinBlocks) k_pcg_fused(const SArgs<1> a,
     const double p = ld_ro(a.p0[0] + row_);
     st_vec(a.p0[0] + row_, xadd(qz[row_ - row0], xmul(beta, p)));
   }
+}
+
+// The fused iteration as launched: mode 1 leaves the register count to the
+// compiler (48), mode 2 holds it to 40 so that six blocks fit an SM.
+template <typename I, int kMode>
+__global__ void __launch_bounds__(256) k_pcg_fused(const SArgs<1> a, SState<1> *st, GridSync gs) {
+  pcg_fused_body<I>(a, st, gs);
+}
+template <typename I>
+__global__ void __launch_bounds__(256, 6) k_pcg_fused_r40(const SArgs<1> a, SState<1> *st,
+                                                          GridSync gs) {
+  pcg_fused_body<I>(a, st, gs);
+}
+
+// The fused kernel of a mode.
+template <typename I>
+const void *fused_kernel(int mode) {
+  return mode == 2 ? (const void *)k_pcg_fused_r40<I> : (const void *)k_pcg_fused<I, 1>;
 }
 
 // reliable update, part 1: x += xs (FP64) for the flagged right-hand sides
@@ -1315,8 +1331,9 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
 // Launch shape of the fused PCG iteration: the most co-resident 256-thread
 // blocks whose shared memory (8 bytes a row of the block's slices) still lets
 // them all be resident at once.  0 when no shape fits.
-template <typename I, int kMinBlocks>
-int fused_shape(sfr_system *s, size_t *smem) {
+template <typename I>
+int fused_shape(sfr_system *s, int mode, size_t *smem) {
+  const void *kern = fused_kernel<I>(mode);
   const int sms = std::max(1, num_sms(s->device));
   const int nsl = s->A.nslices;
   const int maxg = std::max(1, (nsl + 7) / 8);
@@ -1324,13 +1341,11 @@ int fused_shape(sfr_system *s, size_t *smem) {
     const int G = std::min(maxg, per_sm * sms);
     const size_t bytes = static_cast<size_t>((nsl + G - 1) / G) * kWarp * sizeof(double);
     if (bytes > 200 * 1024) continue;
-    if (cudaFuncSetAttribute(k_pcg_fused<I, kMinBlocks>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(bytes)) != cudaSuccess)
       continue;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_fused<I, kMinBlocks>, 256,
-                                                      bytes) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, bytes) != cudaSuccess)
       continue;
     if (occ * sms >= G) {
       *smem = bytes;
@@ -1415,7 +1430,7 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
         GridSync gsync = fused_barrier(cg);
         void *pf3[3] = {&a, &ps, &gsync};
         cudaKernelNodeParams kp{};
-        kp.func = fused == 2 ? (void *)k_pcg_fused<I, 6> : (void *)k_pcg_fused<I, 5>;
+        kp.func = const_cast<void *>(fused_kernel<I>(fused));
         kp.gridDim = dim3(cg->grid_f);
         kp.blockDim = dim3(256);
         kp.sharedMemBytes = static_cast<unsigned>(cg->smem_f);
@@ -1510,9 +1525,8 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
           if (fused) {
             GridSync gsync = fused_barrier(cg);
             void *pf3[3] = {&a, &ps, &gsync};
-            SFR_TRY(cudaLaunchCooperativeKernel(
-                fused == 2 ? (void *)k_pcg_fused<I, 6> : (void *)k_pcg_fused<I, 5>,
-                dim3(cg->grid_f), dim3(256), pf3, cg->smem_f, st));
+            SFR_TRY(cudaLaunchCooperativeKernel(fused_kernel<I>(fused), dim3(cg->grid_f),
+                                                dim3(256), pf3, cg->smem_f, st));
             continue;
           }
         }
@@ -1566,10 +1580,9 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
   fused = K == 1 && solver == SFR_PCG && precision == SFR_FP64 ? fused : 0;
   size_t smem_f = 0;
   int grid_f = 0;
-  if (fused == 2)
-    grid_f = s->A.off ? fused_shape<int16_t, 6>(s, &smem_f) : fused_shape<int, 6>(s, &smem_f);
-  else if (fused)
-    grid_f = s->A.off ? fused_shape<int16_t, 5>(s, &smem_f) : fused_shape<int, 5>(s, &smem_f);
+  if (fused)
+    grid_f = s->A.off ? fused_shape<int16_t>(s, fused, &smem_f)
+                      : fused_shape<int>(s, fused, &smem_f);
   if (fused && grid_f <= 0) fused = 0;
   GraphKey key{solver, K, precision, threads, spw, shared_diag, pf, fused};
   auto it = ec.graphs.find(key);
