@@ -42,6 +42,8 @@ extern "C" {
 #define SFR_CSRD 2
 #define SFR_CSRC 3
 #define SFR_ELLPACK 4
+#define SFR_CSRDCOO 5 /* MPI: CSRD lower part, ghost columns in COO (symmetric) */
+#define SFR_CSRCCOO 6 /* MPI: CSRC, ghost columns in COO */
 
 /* status codes */
 #define SFR_OK 0
@@ -626,7 +628,28 @@ int sfr_dist_group_info(const sfr_dist_group *g, int32_t *kind, int32_t *nranks,
 int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nEqNov,
                         int32_t nAd, int32_t nAdR, const int32_t *ia, const int32_t *ja,
                         int32_t unsym, const sfr_interface *iNeq, sfr_dist **out);
-/* al[nAd + nAdR], ad[nEqNov] (host). */
+/* The same for every MPI storage the reference's dataStruct builds
+ * (Datastruct.c:115-420) and setMatVec multiplies (Solv.c:749-897):
+ *   SFR_CSRD     unsym: full rows over local columns (mpiMatVecCsrD);
+ *                sym: strict-lower square part, ghost columns in CSR at
+ *                ia + nEqNov + 1 (mpiMatVecCsrDSym);
+ *   SFR_CSRC     the CSRD-sym pattern; unsym values al | au | ghost values
+ *                (mpiMatVecCsrC, HccaBlas.c:4394), sym as CSRD sym;
+ *   SFR_CSRDCOO  symmetric: the square part as CSRD sym, the ghost columns
+ *                in COO (rows at ia + 2 (nEqNov + 1), CSR pointers at
+ *                ia + nEqNov + 1) added after the rest of the row
+ *                (mpiMatVecCsrDcooSym, HccaBlas.c:2928);
+ *   SFR_CSRCCOO  the same with CSRC values (mpiMatVecCsrCcoo, :4611);
+ *   SFR_ELLPACK  ia = {width, nEqNov * width}, every row `width` slots over
+ *                local columns (mpiMatVecEllPack, :5094).
+ * Each row keeps the reference's summation order.  SFR_UNSUPPORTED for
+ * CSRDCOO unsym and other storages. */
+int sfr_gpu_dist_create_storage(sfr_dist_group *g, int32_t rank, int32_t storage, int32_t nEq,
+                                int32_t nEqNov, int32_t nAd, int32_t nAdR, const int32_t *ia,
+                                const int32_t *ja, int32_t unsym, const sfr_interface *iNeq,
+                                sfr_dist **out);
+/* al (every value the storage holds: nAd + nAdR, 2 nAd + nAdR for CSRC /
+ * CSRCCOO unsym, nEqNov * width for ELLPACK), ad[nEqNov] (host). */
 int sfr_gpu_dist_set_values(sfr_dist *d, const double *al, const double *ad);
 /* mpiPcg (Cg.c:256-442) or mpiPbicgstab (Bicgstab.c:298-520) over every
  * rank this process holds: parts[nlocal] in rank order (all ranks for a

@@ -192,15 +192,16 @@ class _Rank(ctypes.Structure):
                 ("nAdR", ctypes.c_int), ("unsym", ctypes.c_int), ("ia", _P), ("ja", _P),
                 ("al", _P), ("ad", _P), ("nRcvs", ctypes.c_int), ("nSends", ctypes.c_int),
                 ("nVizPart", ctypes.c_int), ("iaSends", _P), ("iaRcvs", _P), ("fMap", _P),
-                ("vizPart", _P)]
+                ("vizPart", _P), ("storage", ctypes.c_int)]
 
 
 def mpi_solve(solver, ranks, al, ad, b, x0=None, tol=1e-10, maxit=100000,
               newx=True) -> tuple[list, SolveResult]:
     """Restatement of mpiPcg (Cg.c:256-442) / mpiPbicgstab (Bicgstab.c:298-520)
     with the ranks simulated in one process.  ranks[r] has the attributes
-    unsym, nEq, nEqNov, nAd, nAdR, ia, ja, iaSends, iaRcvs, fMap, vizPart (the
-    reference's MPI CSRD and Interface); al[r], ad[r], b[r] its values and
+    unsym, nEq, nEqNov, nAd, nAdR, ia, ja, iaSends, iaRcvs, fMap, vizPart and
+    optionally storage (the reference's MPI layout -- CSRD by default, or
+    CSRC, ELLPACK, CSRDCOO, CSRCCOO -- and its Interface); al[r], ad[r], b[r] its values and
     rows of b; x0[r] its nEq entries.  Returns ([x_r], SolveResult) with
     SolveResult.x the concatenated rows."""
     lib = oracle_lib()
@@ -223,7 +224,7 @@ def mpi_solve(solver, ranks, al, ad, b, x0=None, tol=1e-10, maxit=100000,
         nrcv = q.nEq - q.nEqNov
         arr[r] = _Rank(q.nEq, q.nEqNov, q.nAd, q.nAdR, int(bool(q.unsym)), _p(ia), _p(ja),
                        _p(a), _p(d), nrcv, len(fm) - nrcv, len(vz), _p(ias), _p(iar),
-                       _p(fm), _p(vz))
+                       _p(fm), _p(vz), int(getattr(q, "storage", CSRD)))
         xs.append(np.zeros(q.nEq) if x0 is None else np.array(x0[r], dtype=np.float64))
     bp = (_P * n)(*[_p(keep[9 * r + 8]) for r in range(n)])
     xp = (_P * n)(*[_p(x) for x in xs])

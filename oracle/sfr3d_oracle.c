@@ -1446,7 +1446,7 @@ static void comunicate(const orc_comm *c, double *const *v)
   }
 }
 
-/* mpiMatVecCsrD / mpiMatVecCsrDSym of every rank, after comunicateNeq */
+/* The storage's MPI product of every rank, after comunicateNeq */
 static void mpi_matvec(const orc_comm *c, double *const *x, double *const *y)
 {
   int r, i, k;
@@ -1455,23 +1455,50 @@ static void mpi_matvec(const orc_comm *c, double *const *x, double *const *y)
     const orc_rank *q = &c->rk[r];
     const double *xr = x[r];
     double *yr = y[r];
-    if (q->unsym) {
+    const int split = (q->storage == 3 || q->storage == 6) && q->unsym;
+    if (q->storage == 4) {
+      /* mpiMatVecEllPack: ia[0] slots a row, row-major (MAT2D) */
+      const int w = q->ia[0];
+      for (i = 0; i < q->nEqNov; i++) {
+        double ti = q->ad[i] * xr[i];
+        for (k = 0; k < w; k++) ti += q->al[i * w + k] * xr[q->ja[i * w + k]];
+        yr[i] = ti;
+      }
+    } else if (q->storage == 5 || q->storage == 6) {
+      /* mpiMatVecCsrDcooSym / mpiMatVecCsrCcoo: the square part with the
+       * mirrored scatter, then the ghost terms in COO order */
+      const double *au = split ? q->al + q->nAd : q->al;
+      const int *iar = q->ia + 2 * (q->nEqNov + 1), *jar = q->ja + q->nAd;
+      const double *ar = q->al + (split ? 2 * q->nAd : q->nAd);
+      for (i = 0; i < q->nEqNov; i++) {
+        const double xi = xr[i];
+        double tmp = q->ad[i] * xi;
+        for (k = q->ia[i]; k < q->ia[i + 1]; k++) {
+          const int j = q->ja[k];
+          tmp += q->al[k] * xr[j];
+          yr[j] += au[k] * xi;
+        }
+        yr[i] = tmp;
+      }
+      for (k = 0; k < q->nAdR; k++) yr[iar[k]] += ar[k] * xr[jar[k]];
+    } else if (q->unsym && q->storage != 3) {
       for (i = 0; i < q->nEqNov; i++) {
         double tmp = q->ad[i] * xr[i];
         for (k = q->ia[i]; k < q->ia[i + 1]; k++) tmp += q->al[k] * xr[q->ja[k]];
         yr[i] = tmp;
       }
     } else {
+      /* mpiMatVecCsrDSym, or mpiMatVecCsrC (au = al + nAd) */
       const int *iar = q->ia + q->nEqNov + 1, *jar = q->ja + q->nAd;
-      const double *ar = q->al + q->nAd;
+      const double *au = split ? q->al + q->nAd : q->al;
+      const double *ar = q->al + (split ? 2 * q->nAd : q->nAd);
       for (i = 0; i < q->nEqNov; i++) {
         const double xi = xr[i];
         double tmp = q->ad[i] * xi;
         for (k = q->ia[i]; k < q->ia[i + 1]; k++) {
           const int j = q->ja[k];
-          const double s = q->al[k];
-          tmp += s * xr[j];
-          yr[j] += s * xi;
+          tmp += q->al[k] * xr[j];
+          yr[j] += au[k] * xi;
         }
         for (k = iar[i]; k < iar[i + 1]; k++) tmp += ar[k] * xr[jar[k]];
         yr[i] = tmp;

@@ -189,12 +189,17 @@ typedef struct {
   int nRcvs, nSends, nVizPart;
   const int *iaSends, *iaRcvs, *fMap;
   const short *vizPart;
+  /* storage code (Define.h:407-412): 0 or 2 CSRD, 3 CSRC, 4 ELLPACK,
+   * 5 CSRDCOO, 6 CSRCCOO; the layouts of Datastruct.c:115-420 */
+  int storage;
 } orc_rank;
 
 /* mpiPcg (Cg.c:256-442, solver 1) or mpiPbicgstab (Bicgstab.c:298-520,
  * solver 2) with nranks ranks simulated in this process: comunicateNeq
- * (ParallelMpi.c:3346-3418) before every product, mpiMatVecCsrD
- * (HccaBlas.c:4096-4130) or mpiMatVecCsrDSym (HccaBlas.c:2846-2895), and
+ * (ParallelMpi.c:3346-3418) before every product, the storage's product
+ * -- mpiMatVecCsrD (HccaBlas.c:4096-4130), mpiMatVecCsrDSym (:2846-2895),
+ * mpiMatVecCsrC (:4394-4440), mpiMatVecCsrDcooSym (:2928-2975),
+ * mpiMatVecCsrCcoo (:4611-4670) or mpiMatVecEllPack (:5094-5150) -- and
  * each dot a rank's left-to-right sum, summed over the ranks in rank order
  * (the MPI_Allreduce of dot, HccaBlas.c:393-437).  b[r][nEqNov], x[r][nEq].
  * Returns the status; -1 on a bad interface. */

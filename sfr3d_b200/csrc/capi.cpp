@@ -706,24 +706,38 @@ int solverC_mpi(int32_t nEq, int32_t nEqNov, int32_t nAd, int32_t nAdR, int32_t 
                 bool fLog, bool newX, bool unSym, const char *name) {
   int32_t kind = 0, nranks = 0, rank = 0;
   sfr_dist_group_info(g_group, &kind, &nranks, &rank);
-  if (storage != SFR_CSRD || (solver != SFR_PCG && solver != SFR_PBICGSTAB) || !iNeq ||
-      kind != 1) {
-    fprintf(stderr, "Opcao %d e invalida!!\n", storage != SFR_CSRD ? storage : solver);
+  const bool known_storage = storage == SFR_CSRD || storage == SFR_CSRC ||
+                             storage == SFR_ELLPACK || storage == SFR_CSRDCOO ||
+                             storage == SFR_CSRCCOO;
+  if (!known_storage || (storage == SFR_CSRDCOO && unSym) ||
+      (solver != SFR_PCG && solver != SFR_PBICGSTAB) || !iNeq || kind != 1) {
+    fprintf(stderr, "Opcao %d e invalida!!\n", !known_storage ? storage : solver);
     fprintf(stderr, "Arquivo:%s\nFonte:  %s\n", __FILE__, "sfr_solverC (MPI)");
     if (g_exit_on_failure) exit(EXIT_FAILURE);
     return SFR_UNSUPPORTED;
   }
-  const int32_t n_ia = unSym ? nEqNov + 1 : 2 * (nEqNov + 1);
-  const uint64_t h = pattern_hash(ia, ja, n_ia, static_cast<int64_t>(nAd) + nAdR) ^
-                     (static_cast<uint64_t>(nEq) << 32);
+  // the pattern arrays of the storage (Datastruct.c:115-420)
+  int64_t n_ia = 0, n_ja = static_cast<int64_t>(nAd) + nAdR;
+  if (storage == SFR_ELLPACK) {
+    n_ia = 2;
+    n_ja = static_cast<int64_t>(nEqNov) * ia[0];
+  } else if (storage == SFR_CSRD && unSym) {
+    n_ia = nEqNov + 1;
+  } else {
+    n_ia = 2 * (static_cast<int64_t>(nEqNov) + 1) +
+           (storage == SFR_CSRDCOO || storage == SFR_CSRCCOO ? nAdR : 0);
+  }
+  const uint64_t h = pattern_hash(ia, ja, static_cast<int32_t>(n_ia), n_ja) ^
+                     (static_cast<uint64_t>(nEq) << 32) ^ (static_cast<uint64_t>(storage) << 56);
   PatternKey key{ia, ja, nEqNov, storage, unSym ? 1 : 0};
   DistCached &c = g_dist_cache[key];
   int rc = SFR_OK;
   if (!c.d || c.hash != h) {
     if (c.d) sfr_gpu_dist_destroy(c.d);
     c.d = nullptr;
-    rc = sfr_gpu_dist_create(g_group, rank, nEq, nEqNov, nAd, nAdR, ia, ja, unSym ? 1 : 0,
-                             static_cast<const sfr_interface *>(iNeq), &c.d);
+    rc = sfr_gpu_dist_create_storage(g_group, rank, storage, nEq, nEqNov, nAd, nAdR, ia, ja,
+                                     unSym ? 1 : 0, static_cast<const sfr_interface *>(iNeq),
+                                     &c.d);
     if (rc != SFR_OK) g_dist_cache.erase(key);
     else c.hash = h;
   }

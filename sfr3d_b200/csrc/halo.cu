@@ -874,6 +874,14 @@ int sfr_dist_group_info(const sfr_dist_group *g, int32_t *kind, int32_t *nranks,
 int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nEqNov,
                         int32_t nAd, int32_t nAdR, const int32_t *ia, const int32_t *ja,
                         int32_t unsym, const sfr_interface *iNeq, sfr_dist **out) {
+  return sfr_gpu_dist_create_storage(g, rank, SFR_CSRD, nEq, nEqNov, nAd, nAdR, ia, ja, unsym,
+                                     iNeq, out);
+}
+
+int sfr_gpu_dist_create_storage(sfr_dist_group *g, int32_t rank, int32_t storage, int32_t nEq,
+                                int32_t nEqNov, int32_t nAd, int32_t nAdR, const int32_t *ia,
+                                const int32_t *ja, int32_t unsym, const sfr_interface *iNeq,
+                                sfr_dist **out) {
   if (!out) return fail("out is NULL");
   *out = nullptr;
   if (!g || !ia || !iNeq) return fail("group, ia or iNeq is NULL");
@@ -881,7 +889,13 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
     return fail("rank does not belong to this group in this process");
   if (g->kind == 0 && g->members[rank]) return fail("rank already created in this group");
   if (nEqNov <= 0 || nEq < nEqNov || nAd < 0 || nAdR < 0) return fail("bad sizes");
-  if (unsym && nAdR != 0) return fail("unsymmetric CSRD keeps ghost columns in its rows: nAdR must be 0");
+  const bool coo = storage == SFR_CSRDCOO || storage == SFR_CSRCCOO;
+  if (storage != SFR_CSRD && storage != SFR_CSRC && storage != SFR_ELLPACK && !coo)
+    return fail("storage must be CSRD, CSRC, ELLPACK, CSRDCOO or CSRCCOO", SFR_UNSUPPORTED);
+  if (storage == SFR_CSRDCOO && unsym)
+    return fail("CSRDCOO is symmetric storage (Datastruct.c:199)", SFR_UNSUPPORTED);
+  if (storage == SFR_CSRD && unsym && nAdR != 0)
+    return fail("unsymmetric CSRD keeps ghost columns in its rows: nAdR must be 0");
   const int nghost = nEq - nEqNov;
   if (iNeq->nRcvs > nghost) return fail("nRcvs exceeds the ghost count");
   const int nviz = iNeq->nVizPart;
@@ -921,63 +935,105 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
   }
   // the rows (columns local, ghosts included), in the reference's order
   const int ncols = nEq;
-  const int32_t base = ia[0];
-  if (base != 0) return fail("ia[0] must be 0");
-  for (int i = 0; i < nEqNov; ++i)
-    if (ia[i + 1] < ia[i]) return fail("ia not monotone");
-  if (ia[nEqNov] != nAd) return fail("ia[nEqNov] != nAd");
-  const int32_t *iar_m = unsym ? nullptr : ia + nEqNov + 1;
-  if (!unsym) {
-    if (iar_m[0] != 0) return fail("the rectangular part's ia must start at 0");
-    for (int i = 0; i < nEqNov; ++i)
-      if (iar_m[i + 1] < iar_m[i]) return fail("rectangular ia not monotone");
-    if (iar_m[nEqNov] != nAdR) return fail("rectangular ia[nEqNov] != nAdR");
-  }
-  if (nAd + nAdR > 0 && !ja) return fail("ja is NULL");
-  for (int k = 0; k < nAd + nAdR; ++k)
-    if (ja[k] < 0 || ja[k] >= ncols) return fail("ja out of range");
   std::vector<int64_t> ptr(nEqNov + 1, 0);
   std::vector<int32_t> col, src;
-  if (unsym) {
-    col.assign(ja, ja + nAd);
-    src.resize(nAd);
-    for (int k = 0; k < nAd; ++k) src[k] = k;
-    for (int i = 0; i <= nEqNov; ++i) ptr[i] = ia[i];
+  int64_t nsrc = 0;
+  if (storage == SFR_ELLPACK) {
+    // ia = {width, nEqNov * width}; ja and the values row-major, every slot
+    // in order, padded slots included (mpiMatVecEllPack, HccaBlas.c:5094)
+    const int width = ia[0];
+    if (width <= 0 || ia[1] != static_cast<int64_t>(nEqNov) * width)
+      return fail("ELLPACK ia must be {width, nEqNov * width}");
+    if (!ja) return fail("ja is NULL");
+    nsrc = static_cast<int64_t>(nEqNov) * width;
+    for (int64_t k = 0; k < nsrc; ++k)
+      if (ja[k] < 0 || ja[k] >= ncols) return fail("ja out of range");
+    col.assign(ja, ja + nsrc);
+    src.resize(nsrc);
+    for (int64_t k = 0; k < nsrc; ++k) src[k] = static_cast<int32_t>(k);
+    for (int i = 0; i <= nEqNov; ++i) ptr[i] = static_cast<int64_t>(i) * width;
   } else {
-    // row i: its strict-lower square entries, its ghost columns, then the
-    // mirrored entries of later rows in increasing row order (the order
-    // mpiMatVecCsrDSym, HccaBlas.c:2872-2890, accumulates them)
+    const int32_t base = ia[0];
+    if (base != 0) return fail("ia[0] must be 0");
     for (int i = 0; i < nEqNov; ++i)
-      for (int k = ia[i]; k < ia[i + 1]; ++k)
-        if (ja[k] >= i) return fail("square part not strictly lower");
-    std::vector<int64_t> up(nEqNov + 1, 0);
-    for (int k = 0; k < nAd; ++k) ++up[ja[k] + 1];
-    for (int i = 0; i < nEqNov; ++i) up[i + 1] += up[i];
-    std::vector<int32_t> upc(nAd), ups(nAd);
-    std::vector<int64_t> fill(up.begin(), up.end() - 1);
-    for (int i = 0; i < nEqNov; ++i)
-      for (int k = ia[i]; k < ia[i + 1]; ++k) {
-        const int64_t q = fill[ja[k]]++;
-        upc[q] = i;
-        ups[q] = k;
+      if (ia[i + 1] < ia[i]) return fail("ia not monotone");
+    if (ia[nEqNov] != nAd) return fail("ia[nEqNov] != nAd");
+    const bool full_rows = storage == SFR_CSRD && unsym;
+    // the rectangular (ghost-column) part: CSR at ia + nEqNov + 1; COO rows
+    // at ia + 2 (nEqNov + 1) (Datastruct.c:129-260, 336-420)
+    const int32_t *iar_m = full_rows ? nullptr : ia + nEqNov + 1;
+    const int32_t *coo_row = coo ? ia + 2 * (nEqNov + 1) : nullptr;
+    if (!full_rows) {
+      if (iar_m[0] != 0) return fail("the rectangular part's ia must start at 0");
+      for (int i = 0; i < nEqNov; ++i)
+        if (iar_m[i + 1] < iar_m[i]) return fail("rectangular ia not monotone");
+      if (iar_m[nEqNov] != nAdR) return fail("rectangular ia[nEqNov] != nAdR");
+      if (coo)
+        for (int i = 0; i < nEqNov; ++i)
+          for (int k = iar_m[i]; k < iar_m[i + 1]; ++k)
+            if (coo_row[k] != i) return fail("COO rows disagree with the rectangular ia");
+    }
+    if (nAd + nAdR > 0 && !ja) return fail("ja is NULL");
+    for (int k = 0; k < nAd + nAdR; ++k)
+      if (ja[k] < 0 || ja[k] >= ncols) return fail("ja out of range");
+    if (full_rows) {
+      nsrc = nAd;
+      col.assign(ja, ja + nAd);
+      src.resize(nAd);
+      for (int k = 0; k < nAd; ++k) src[k] = k;
+      for (int i = 0; i <= nEqNov; ++i) ptr[i] = ia[i];
+    } else {
+      // strict-lower square part + mirrored entries of later rows + ghost
+      // columns.  The mirrored value is al[k] (symmetric) or au[k] = a[nAd+k]
+      // (CSRC unsymmetric); the ghost values follow the square part's.
+      // Order of a row (the reference's accumulation):
+      //   CSR ghosts (mpiMatVecCsrDSym HccaBlas.c:2872-2890, mpiMatVecCsrC
+      //   :4394): own lower entries, own ghost columns, mirrored entries;
+      //   COO ghosts (mpiMatVecCsrDcooSym :2928, mpiMatVecCsrCcoo :4611):
+      //   own lower entries, mirrored entries, then the ghost terms, which
+      //   the reference adds after every row, in COO order.
+      const bool split = storage == SFR_CSRC || storage == SFR_CSRCCOO;
+      const int64_t mirror_off = split && unsym ? nAd : 0;
+      const int64_t rect_off = split && unsym ? 2 * static_cast<int64_t>(nAd) : nAd;
+      nsrc = rect_off + nAdR;
+      for (int i = 0; i < nEqNov; ++i)
+        for (int k = ia[i]; k < ia[i + 1]; ++k)
+          if (ja[k] >= i) return fail("square part not strictly lower");
+      std::vector<int64_t> up(nEqNov + 1, 0);
+      for (int k = 0; k < nAd; ++k) ++up[ja[k] + 1];
+      for (int i = 0; i < nEqNov; ++i) up[i + 1] += up[i];
+      std::vector<int32_t> upc(nAd), ups(nAd);
+      std::vector<int64_t> fill(up.begin(), up.end() - 1);
+      for (int i = 0; i < nEqNov; ++i)
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+          const int64_t q = fill[ja[k]]++;
+          upc[q] = i;
+          ups[q] = k;
+        }
+      for (int i = 0; i < nEqNov; ++i) {
+        for (int k = ia[i]; k < ia[i + 1]; ++k) {
+          col.push_back(ja[k]);
+          src.push_back(k);
+        }
+        auto ghosts = [&]() -> bool {
+          for (int k = iar_m[i]; k < iar_m[i + 1]; ++k) {
+            if (ja[nAd + k] < nEqNov) return false;
+            col.push_back(ja[nAd + k]);
+            src.push_back(static_cast<int32_t>(rect_off + k));
+          }
+          return true;
+        };
+        if (!coo && !ghosts()) return fail("rectangular part names an owned column");
+        for (int64_t u = up[i]; u < up[i + 1]; ++u) {
+          col.push_back(upc[u]);
+          src.push_back(static_cast<int32_t>(mirror_off + ups[u]));
+        }
+        if (coo && !ghosts()) return fail("rectangular part names an owned column");
+        ptr[i + 1] = static_cast<int64_t>(col.size());
       }
-    for (int i = 0; i < nEqNov; ++i) {
-      for (int k = ia[i]; k < ia[i + 1]; ++k) {
-        col.push_back(ja[k]);
-        src.push_back(k);
-      }
-      for (int k = iar_m[i]; k < iar_m[i + 1]; ++k) {
-        if (ja[nAd + k] < nEqNov) return fail("rectangular part names an owned column");
-        col.push_back(ja[nAd + k]);
-        src.push_back(nAd + k);
-      }
-      for (int64_t u = up[i]; u < up[i + 1]; ++u) {
-        col.push_back(upc[u]);
-        src.push_back(ups[u]);
-      }
-      ptr[i + 1] = static_cast<int64_t>(col.size());
     }
   }
+  if (nsrc > INT32_MAX) return fail("too many values");
   // SELL-32 of the rows
   sfr::HostSell h;
   h.n = nEqNov;
@@ -1026,7 +1082,7 @@ int sfr_gpu_dist_create(sfr_dist_group *g, int32_t rank, int32_t nEq, int32_t nE
   d->unsym = unsym ? 1 : 0;
   d->nad = nAd;
   d->nadr = nAdR;
-  d->nsrc = nAd + nAdR;
+  d->nsrc = static_cast<int>(nsrc);
   d->nslots = total;
   d->nrcv = nrcv;
   d->nsnd = nsnd;

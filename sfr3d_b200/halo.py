@@ -54,6 +54,9 @@ def _lib() -> ctypes.CDLL:
     L.sfr_dist_group_info.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_dist_create.argtypes = [_P, _I32, _I32, _I32, _I32, _I32, _P, _P, _I32,
                                       ctypes.POINTER(InterfaceC), ctypes.POINTER(_P)]
+    L.sfr_gpu_dist_create_storage.argtypes = [_P, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P,
+                                              _I32, ctypes.POINTER(InterfaceC),
+                                              ctypes.POINTER(_P)]
     L.sfr_gpu_dist_set_values.argtypes = [_P, _P, _P]
     L.sfr_gpu_dist_solve.argtypes = [_P, _I32, _P, _I32, _P, _P, ctypes.c_double,
                                      ctypes.c_uint32, _I32, ctypes.POINTER(_sv.SolveInfoC)]
@@ -85,6 +88,9 @@ class Layout:
     iaRcvs: np.ndarray
     fMap: np.ndarray
     vizPart: np.ndarray
+    # the reference's storage code of ia/ja (Define.h:407-412): CSRD from
+    # `partition`; `as_storage` gives the others
+    storage: int = _sv.CSRD
 
     @property
     def nRcvs(self) -> int:
@@ -118,6 +124,87 @@ class Layout:
                           iaSends=_sv._ptr(self.iaSends), iaRcvs=_sv._ptr(self.iaRcvs),
                           fMap=_sv._ptr(self.fMap), xb=None, nVizPart=len(self.vizPart),
                           vizPart=_sv._ptr(self.vizPart))
+
+
+def value_count(lay: Layout) -> int:
+    """Values of a layout's storage: nAd + nAdR; 2 nAd + nAdR for unsymmetric
+    CSRC / CSRCCOO (al | au | ghost values); nEqNov x width for ELLPACK."""
+    if lay.storage == _sv.ELLPACK:
+        return int(lay.ia[1])
+    if lay.storage in (_sv.CSRC, CSRCCOO) and lay.unsym:
+        return 2 * lay.nAd + lay.nAdR
+    return lay.nAd + lay.nAdR
+
+
+CSRDCOO, CSRCCOO = 5, 6  # Define.h:411-412
+
+
+def as_storage(lay: Layout, storage: int, unsym: bool, ia, ja, al, ad):
+    """This rank's share of a global system in another of the reference's MPI
+    storages (Datastruct.c:115-420), with its values.
+
+    `lay` comes from ``partition(..., unsym=False)`` (the strict-lower square
+    part and the ghost columns in CSR) for CSRC, CSRDCOO and CSRCCOO, and from
+    ``partition(..., unsym=True)`` (full rows) for ELLPACK.  ia/ja/al are the
+    global system's full CSRD rows (all off-diagonals), ad its diagonal;
+    `unsym` picks separate upper values (CSRC, CSRCCOO).  Returns (Layout,
+    al, ad) for DistSystem.set_values."""
+    ia = np.asarray(ia, np.int64)
+    ja = np.asarray(ja, np.int64)
+    al = np.asarray(al, np.float64)
+    n = len(ia) - 1
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(ia))
+    keys = rows * n + ja[: len(rows)]
+    order = np.argsort(keys)
+    skeys, svals = keys[order], al[: len(rows)][order]
+
+    def A(gi, gj):
+        q = np.asarray(gi, np.int64) * n + np.asarray(gj, np.int64)
+        pos = np.searchsorted(skeys, q)
+        if np.any(pos >= len(skeys)) or np.any(skeys[np.minimum(pos, len(skeys) - 1)] != q):
+            raise ValueError("the pattern is not structurally symmetric")
+        return svals[pos]
+
+    g = lay.l2g.astype(np.int64)
+    adr = np.asarray(ad, np.float64)[g[:lay.nEqNov]].copy()
+    fields = {k: getattr(lay, k) for k in ("rank", "nEq", "nEqNov", "src", "l2g", "iaSends",
+                                           "iaRcvs", "fMap", "vizPart")}
+    if storage == _sv.ELLPACK:
+        if not lay.unsym:
+            raise ValueError("ELLPACK takes the full-row layout (partition(..., unsym=True))")
+        lens = np.diff(lay.ia)
+        w = int(lens.max()) if len(lens) else 1
+        eja = np.repeat(np.arange(lay.nEqNov, dtype=np.int32), w).reshape(lay.nEqNov, w)
+        ea = np.zeros((lay.nEqNov, w))
+        for i in range(lay.nEqNov):
+            k0, k1 = int(lay.ia[i]), int(lay.ia[i + 1])
+            eja[i, : k1 - k0] = lay.ja[k0:k1]
+            ea[i, : k1 - k0] = A(np.full(k1 - k0, g[i]), g[lay.ja[k0:k1]])
+        out = Layout(unsym=True, nAd=lay.nEqNov * w, nAdR=0,
+                     ia=np.array([w, lay.nEqNov * w], np.int32), ja=eja.ravel(),
+                     storage=_sv.ELLPACK, **fields)
+        return out, ea.ravel(), adr
+    if lay.unsym:
+        raise ValueError("CSRC and the COO storages take partition(..., unsym=False)")
+    if storage == CSRDCOO and unsym:
+        raise ValueError("CSRDCOO is symmetric storage")
+    n1 = lay.nEqNov + 1
+    low_rows = np.repeat(np.arange(lay.nEqNov, dtype=np.int64), np.diff(lay.ia[:n1]))
+    low_cols = lay.ja[: lay.nAd].astype(np.int64)
+    rect = lay.ia[n1: 2 * n1]
+    rect_rows = np.repeat(np.arange(lay.nEqNov, dtype=np.int64), np.diff(rect))
+    rect_cols = lay.ja[lay.nAd: lay.nAd + lay.nAdR].astype(np.int64)
+    lower = A(g[low_rows], g[low_cols])
+    upper = A(g[low_cols], g[low_rows])
+    ghost = A(g[rect_rows], g[rect_cols])
+    split = storage in (_sv.CSRC, CSRCCOO) and unsym
+    vals = np.concatenate([lower, upper, ghost] if split else [lower, ghost])
+    new_ia = lay.ia.copy()
+    if storage in (CSRDCOO, CSRCCOO):
+        new_ia = np.concatenate([lay.ia[: 2 * n1], rect_rows.astype(np.int32)]).astype(np.int32)
+    out = Layout(unsym=bool(split), nAd=lay.nAd, nAdR=lay.nAdR, ia=new_ia, ja=lay.ja.copy(),
+                 storage=storage, **fields)
+    return out, vals, adr
 
 
 def partition(neq, ia, ja, unsym, nparts, part=None) -> list[Layout]:
@@ -280,18 +367,18 @@ class DistSystem:
         self.layout = layout
         self._iface = layout.interface()
         self._h = _P()
-        rc = _lib().sfr_gpu_dist_create(group._h, layout.rank, layout.nEq, layout.nEqNov,
-                                        layout.nAd, layout.nAdR, _sv._ptr(layout.ia),
-                                        _sv._ptr(layout.ja), int(layout.unsym),
-                                        ctypes.byref(self._iface), ctypes.byref(self._h))
+        rc = _lib().sfr_gpu_dist_create_storage(
+            group._h, layout.rank, int(layout.storage), layout.nEq, layout.nEqNov, layout.nAd,
+            layout.nAdR, _sv._ptr(layout.ia), _sv._ptr(layout.ja), int(layout.unsym),
+            ctypes.byref(self._iface), ctypes.byref(self._h))
         if rc != 0:
-            raise _sv.SolverError(rc, "sfr_gpu_dist_create")
+            raise _sv.SolverError(rc, "sfr_gpu_dist_create_storage: " + _sv.last_error())
         group.members.append(self)
 
     def set_values(self, al, ad) -> None:
         al, ad = _sv._f64(al), _sv._f64(ad)
-        if len(al) != self.layout.nAd + self.layout.nAdR or len(ad) != self.layout.nEqNov:
-            raise ValueError("al must hold nAd + nAdR values and ad nEqNov")
+        if len(al) != value_count(self.layout) or len(ad) != self.layout.nEqNov:
+            raise ValueError("al must hold the storage's values and ad nEqNov")
         rc = _lib().sfr_gpu_dist_set_values(self._h, _sv._ptr(al), _sv._ptr(ad))
         if rc != 0:
             raise _sv.SolverError(rc, "sfr_gpu_dist_set_values")

@@ -196,3 +196,37 @@ def test_solverC_mpi_branch_on_an_nccl_group(tmp_path, solver, head):
         H.set_solverC_group(None)
         SV.release_cache()
         g.close()
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 4])
+@pytest.mark.parametrize("storage,unsym", [(SV.CSRC, True), (SV.CSRC, False),
+                                           (H.CSRDCOO, False), (H.CSRCCOO, True),
+                                           (H.CSRCCOO, False), (SV.ELLPACK, True)])
+def test_other_mpi_storages_match_the_oracle(storage, unsym, nparts):
+    """The reference's other MPI storages (CSRC, CSRD+COO, CSRC+COO,
+    ELLPACK; Datastruct.c:115-420) on the local group against the oracle's
+    restatement of their products (mpiMatVecCsrC, mpiMatVecCsrDcooSym,
+    mpiMatVecCsrCcoo, mpiMatVecEllPack) at the same ranks."""
+    if unsym:
+        sysx = S.momentum(16, peclet=50.0, nrhs=1, seed=9)
+        solver = O.PBICGSTAB
+    else:
+        sysx = S.poisson_jittered(20, seed=9)
+        solver = O.PCG
+    ia, ja, al, ad, b = sysx.ia, sysx.ja, sysx.al, sysx.ad, sysx.b[0]
+    full = storage == SV.ELLPACK
+    base = H.partition(sysx.neq, *((ia, ja) if full else sysx.csrd_lower()[:2]), full, nparts)
+    conv = [H.as_storage(lay, storage, unsym, ia, ja, al, ad) for lay in base]
+    lays = [c[0] for c in conv]
+    b_r = [lay.rows(b) for lay in base]
+    _, ref = O.mpi_solve(solver, lays, [c[1] for c in conv], [c[2] for c in conv], b_r,
+                         tol=1e-10)
+    g = H.LocalGroup(nparts, 0)
+    systems = [H.DistSystem(g, lay) for lay in lays]
+    for sy, c in zip(systems, conv):
+        sy.set_values(c[1], c[2])
+    xs, info = H.solve(g, systems, solver, b_r, tol=1e-10)
+    g.close()
+    assert info.status == 0 and ref.status == 0
+    assert abs(info.iters - ref.iters) <= 1
+    assert _rel(_global(lays, xs, sysx.neq), ref.x) < 1e-12

@@ -280,3 +280,69 @@ def test_gloo_two_ranks_exchange_the_halo(tmp_path, plant):
     else:
         assert all(int(r["nmsg"]) == 0 for r in res)
         assert all(bool(r["ok"]) for r in res)
+
+
+# ---- the reference's other MPI storages (Datastruct.c:115-420) -----------
+
+def _momentum(n=8, seed=6):
+    m = S.momentum(n, nrhs=1, seed=seed)
+    return m, m.ia, m.ja, m.al, m.ad, m.b[0]
+
+
+@pytest.mark.parametrize("storage,unsym", [(SV.CSRC, True), (SV.CSRC, False),
+                                           (H.CSRDCOO, False), (H.CSRCCOO, True),
+                                           (H.CSRCCOO, False), (SV.ELLPACK, True)])
+def test_other_storages_at_one_rank_are_the_serial_solver(storage, unsym):
+    """At one rank nothing is exchanged, and mpiMatVecCsrC, mpiMatVecCsrDcooSym,
+    mpiMatVecCsrCcoo and mpiMatVecEllPack take the serial products' steps:
+    the oracle's restatement is bit-identical to the reference's own serial
+    solver on the same arrays."""
+    sysx, ia, ja, al, ad, b = (_momentum() if unsym else _poisson(8))
+    solver = O.PBICGSTAB if unsym else O.PCG
+    lay = H.partition(sysx.neq, *((ia, ja) if storage == SV.ELLPACK
+                                  else sysx.csrd_lower()[:2]),
+                      storage == SV.ELLPACK, 1)[0]
+    st, a_r, ad_r = H.as_storage(lay, storage, unsym, ia, ja, al, ad)
+    _, got = O.mpi_solve(solver, [st], [a_r], [ad_r], [lay.rows(b)], tol=1e-10)
+    # the reference's serial storage with the same arrays (COO parts are
+    # empty at one rank: the CSRD / CSRC products)
+    serial = {H.CSRDCOO: SV.CSRD, H.CSRCCOO: SV.CSRC}.get(storage, storage)
+    if serial == SV.ELLPACK:
+        sia, sja, sal = st.ia, st.ja, a_r
+    else:
+        sia, sja = st.ia[:st.nEqNov + 1], st.ja[:st.nAd]
+        sal = a_r[: 2 * st.nAd] if unsym and serial == SV.CSRC else a_r[:st.nAd]
+    sun = unsym if serial == SV.CSRC else (serial == SV.ELLPACK)
+    want = O.ref_solve(solver, serial, sun, sia, sja, sal, ad_r, lay.rows(b), tol=1e-10) \
+        if O.ref_available() else None
+    if want is None:
+        pytest.skip("oracle/_ref not built")
+    assert got.iters == want.iters and got.status == want.status == 0
+    assert np.array_equal(got.x.view(np.int64), want.x.view(np.int64))
+
+
+@pytest.mark.parametrize("nparts", [2, 4])
+@pytest.mark.parametrize("storage,unsym", [(SV.CSRC, True), (SV.CSRC, False),
+                                           (H.CSRDCOO, False), (H.CSRCCOO, True),
+                                           (SV.ELLPACK, True)])
+def test_other_storages_over_ranks_solve_the_same_system(storage, unsym, nparts):
+    """Over several ranks each storage sums its ghost terms in its own order;
+    the solve agrees with the serial solve within the summation-order
+    spread (x 1e-10, iterations +-2)."""
+    sysx, ia, ja, al, ad, b = (_momentum() if unsym else _poisson(8))
+    solver = O.PBICGSTAB if unsym else O.PCG
+    lays = H.partition(sysx.neq, *((ia, ja) if storage == SV.ELLPACK
+                                   else sysx.csrd_lower()[:2]),
+                       storage == SV.ELLPACK, nparts)
+    conv = [H.as_storage(lay, storage, unsym, ia, ja, al, ad) for lay in lays]
+    _, got = O.mpi_solve(solver, [c[0] for c in conv], [c[1] for c in conv],
+                         [c[2] for c in conv], [lay.rows(b) for lay in lays], tol=1e-10)
+    ser = (O.pbicgstab if unsym else O.pcg)(O.CSRD, True, ia, ja, al, ad, b, tol=1e-10)
+    x = np.zeros(sysx.neq)
+    off = 0
+    for lay in lays:
+        x[lay.l2g[:lay.nEqNov]] = got.x[off:off + lay.nEqNov]
+        off += lay.nEqNov
+    assert got.status == 0
+    assert abs(got.iters - ser.iters) <= 2
+    assert np.linalg.norm(x - ser.x) <= 1e-10 * np.linalg.norm(ser.x)
