@@ -187,9 +187,17 @@ def test_solverC_mpi_branch_on_an_nccl_group(tmp_path, solver, head):
         assert line.startswith(head)
         assert abs(int(line.split("iteration")[1].split()[0]) - ref.iters) <= 1
         assert _rel(x[:lay.nEqNov], ref.x) < 1e-12
-        # a storage the MPI branch lacks is the reference's invalid option
+        if not unsym:
+            # CSRC symmetric keeps CSRD's symmetric arrays: the same solve
+            x2 = np.zeros(lay.nEq)
+            rc = SV.solverC(lay.nEq, lay.nEqNov, lay.nAd, lay.nAdR, lay.ia, lay.ja, a, d, None,
+                            b, x2, 1e-10, 100000, SV.CSRC, solver, newX=True, unSym=False,
+                            iNeq=iface)
+            assert rc == 0 and np.array_equal(x2, x)
+        # a storage the reference does not build under MPI (CSRDCOO is
+        # symmetric only) is its invalid option
         rc = SV.solverC(lay.nEq, lay.nEqNov, lay.nAd, lay.nAdR, lay.ia, lay.ja, a, d, None, b,
-                        x, 1e-10, 100000, SV.CSRC, solver, newX=True, unSym=unsym,
+                        x, 1e-10, 100000, H.CSRDCOO, solver, newX=True, unSym=True,
                         iNeq=iface)
         assert rc == SV.UNSUPPORTED
     finally:
