@@ -3,11 +3,11 @@
 // WHILE node, like the graph engine's PCG (stream_solve.cu), so no dot
 // product travels to the host.
 //
-// One iteration is three kernels, or, with the handle's fused-iteration
+// One iteration is two kernels, or, with the handle's fused-iteration
 // option (sfr_gpu_set_fused) and a co-resident launch shape, one cooperative
 // kernel (k_mr_fused; at 128^3 it measured slower, 126 against 97 us an
-// iteration: 55 registers and 57 KB of shared memory a block leave four
-// blocks an SM for the SpMV phase).  The three kernels:
+// iteration for three kernels: 55 registers and 57 KB of shared memory a
+// block leave four blocks an SM for the SpMV phase).  The steps:
 //   a. p = A z0 and (z0, p); the last block forms alpha = (z0, p) / beta^2
 //      and the three-term coefficients t1 = 1/beta, t2 = -alpha/beta,
 //      t3 = -beta/beta_old;
@@ -17,7 +17,9 @@
 //      with a, not |a|), u1..u4, |r| = |s| |r| -- decides convergence,
 //      breakdown (a non-finite u) or maxIt, and clears the WHILE condition;
 //   c. w = u1 z0 + u2 w0 + u3 w00, x += u4 w (skipped after a breakdown, as
-//      the reference breaks before its update).
+//      the reference breaks before its update), done by the next
+//      iteration's kernel a for its own rows before its product, and after
+//      the loop by a tail kernel.
 // The reference rotates its vectors (v0 <- v <- p, z0 <- z, w00 <- w0 <- w)
 // by pointer swaps, with periods 3 and 2; the graph body unrolls six
 // iterations, each with its own fixed roles, and the kernels of iterations
@@ -187,7 +189,22 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_setup2(const MrArgs a) {
   }
 }
 
-// a: p = A z0, alpha and the three-term coefficients (Iters.c:402-411)
+// The previous iteration's w = u1 z0 + u2 w0 + u3 w00, x += u4 w
+// (Iters.c:482-497) for one row, with that iteration's roles (pu).
+__device__ __forceinline__ void mr_update_row(const MrArgs &a, const MrState *st, int pu,
+                                              int row) {
+  const double *z0 = a.Z[pu % 2];
+  const double *w00 = a.W[pu % 3], *w0 = a.W[(pu + 1) % 3];
+  double *w = a.W[(pu + 2) % 3];
+  const double wi = xadd(xadd(xmul(st->u1, ld_ro(z0 + row)), xmul(st->u2, ld_ro(w0 + row))),
+                         xmul(st->u3, ld_ro(w00 + row)));
+  st_vec(w + row, wi);
+  st_vec(a.x + row, xadd(ld_vec(a.x + row), xmul(st->u4, wi)));
+}
+
+// a: the previous iteration's w and x update for this warp's rows (it waits
+// for no reduction; its streaming loads overlap the product's gathers), then
+// p = A z0, alpha and the three-term coefficients (Iters.c:402-411)
 template <typename I>
 __global__ void __launch_bounds__(kMrThreads) k_mr_a(const MrArgs a, int u) {
   SFR_SHARED_RED(1);
@@ -197,12 +214,15 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_a(const MrArgs a, int u) {
   const int lane = threadIdx.x & 31;
   const double *z0 = a.Z[u % 2];
   double *p = a.V[(u + 2) % 3];
+  const bool pending = st->upd != 0;
+  const int pu = (u + kMrUnroll - 1) % kMrUnroll;
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
   const int all[1] = {1};
   const double *const diag[1] = {a.ad};
   double acc[1] = {0.0};
   SFR_FOR_OWN_ROWS(s0, s1) {
+    if (pending) mr_update_row(a, st, pu, row_);
     double y[1];
     row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val, diag, s_, lane, all,
                                  [&](int, int c) { return ld_ro(z0 + c); }, y);
@@ -278,10 +298,7 @@ __device__ void mr_step(MrState &q, double alpha, double zp) {
 __global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
   SFR_SHARED_RED(1);
   MrState *st = a.st;
-  if (!st->active) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->upd = 0;
-    return;
-  }
+  if (!st->active) return;
   const double t1 = st->t1, t2 = st->t2, t3 = st->t3;
   const double *v0 = a.V[u % 3], *v = a.V[(u + 1) % 3];
   double *p = a.V[(u + 2) % 3];
@@ -309,25 +326,14 @@ __global__ void __launch_bounds__(kMrThreads) k_mr_b(const MrArgs a, int u) {
   }
 }
 
-// c: w = u1 z0 + u2 w0 + u3 w00, x += u4 w  (Iters.c:482-497)
-__global__ void __launch_bounds__(kMrThreads) k_mr_c(const MrArgs a, int u) {
-  MrState *st = a.st;
-  if (!st->upd) return;
-  const double u1 = st->u1, u2 = st->u2, u3 = st->u3, u4 = st->u4;
-  const double *z0 = a.Z[u % 2];
-  const double *w00 = a.W[u % 3], *w0 = a.W[(u + 1) % 3];
-  double *w = a.W[(u + 2) % 3];
-  SFR_MR_FOR_PAIRS(i) {
-    const int r = 2 * i;
-    const double2 zv = ld2(z0 + r), w0v = ld2(w0 + r), w00v = ld2(w00 + r);
-    double2 xv = ld2(a.x + r), wn;
-    wn.x = xadd(xadd(xmul(u1, zv.x), xmul(u2, w0v.x)), xmul(u3, w00v.x));
-    wn.y = xadd(xadd(xmul(u1, zv.y), xmul(u2, w0v.y)), xmul(u3, w00v.y));
-    xv.x = xadd(xv.x, xmul(u4, wn.x));
-    xv.y = xadd(xv.y, xmul(u4, wn.y));
-    st2(w + r, wn);
-    st2(a.x + r, xv);
-  }
+// After the loop: the last iteration's w and x update (the reference breaks
+// after it on convergence and at maxIt, before it on a breakdown), with that
+// iteration's roles.
+__global__ void __launch_bounds__(kMrThreads) k_mr_tail(const MrArgs a) {
+  const MrState *st = a.st;
+  if (!st->upd || st->j == 0) return;
+  const int pu = static_cast<int>((st->j - 1) % kMrUnroll);
+  SFR_MR_FOR_ROWS(i) mr_update_row(a, st, pu, i);
 }
 
 // One whole iteration in one cooperative launch: a, b and c above with two
@@ -622,9 +628,11 @@ cudaError_t build(sfr_system *s, int fused, MrGraph *g) {
     } else {
       SFR_TRY(node(body, &bp, (void *)k_mr_a<I>, g->gs, pu[u]));
       SFR_TRY(node(body, &bp, (void *)k_mr_b, g->gv, pu[u]));
-      SFR_TRY(node(body, &bp, (void *)k_mr_c, g->gv, pu[u]));
     }
   }
+  // the fused kernel updates w and x itself; the two-kernel body leaves the
+  // last iteration's update to the tail
+  if (!g->gf) SFR_TRY(node(g->graph, &prev, (void *)k_mr_tail, g->gv, p1));
   SFR_TRY(node(g->graph, &prev, (void *)k_mr_post<I>, g->gs, p1));
   SFR_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
   return cudaSuccess;
