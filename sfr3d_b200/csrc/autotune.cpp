@@ -96,7 +96,7 @@ bool file_lookup(const std::string &key, Tuned *t) {
                     "engine=%d threads=%d spw=%d pf=%d fused=%d ms=%lf", &e, &th, &sp, &pf, &fu,
                     &ms) == 6 &&
         (e == 1 || e == 2 || e == 4) && (th == 128 || th == 256) && sp >= 0 && sp <= 64 &&
-        pf >= 0 && pf <= 8 && fu >= 0 && fu <= 2) {
+        pf >= 0 && pf <= 8 && fu >= 0 && fu <= 3) {
       t->engine = e;
       t->threads = th;
       t->spw = sp;
@@ -192,8 +192,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   for (int th : {256, 128})
     for (int sp : {0, 2, 8}) add({2, th, sp, 0, 0});
   if (precision == SFR_FP64 && solver == SFR_PCG && k == 1) {
-    add({2, 256, 0, 0, 1});
-    add({2, 256, 0, 0, 2});
+    for (int mode : {1, 2, 3}) add({2, 256, 0, 0, mode});
   }
   add({1, 0, 0, 0, 0});
   if (precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag && resident_fits(s))

@@ -396,7 +396,7 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds) {
 
 int sfr_gpu_set_fused(sfr_system *s, int32_t flag) {
   if (!s) return SFR_BAD_INPUT;
-  if (flag < 0 || flag > 2) return SFR_BAD_INPUT;
+  if (flag < 0 || flag > 3) return SFR_BAD_INPUT;
   s->graph_fused = flag;
   return SFR_OK;
 }

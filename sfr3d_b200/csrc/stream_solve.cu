@@ -423,6 +423,99 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
   }
 }
 
+// Partial sums between the blocks of a co-resident grid without a counter:
+// each block stores its total in its own word with the two lowest bits of the
+// FP64 pattern replaced by the epoch's tag (epoch & 3, at most 3 units in the
+// last place), and every block polls every block's word until all carry the
+// tag -- the values travel in the polled words, so an exchange is one L2
+// round trip.  Three buffers rotate (epoch % 3): a word is rewritten only
+// three epochs after its last use, by which time every block has read it,
+// and the tag of that last use differs from the new one.  Every block sums
+// the G totals in the same fixed order, so all hold the same bits.  The
+// buffers start zeroed, and epochs start at 1, so a zero word never carries
+// the tag of a buffer's first use.  Only the partial sums cross: no other
+// global data is ordered by it.  A wait gives up after spin_limit polls and
+// records SFR_TIMEOUT in *err.
+struct TagExchange {
+  unsigned long long *words;  // 3 * G, zero at the start of a solve
+  int *err;
+  unsigned spin_limit;
+};
+
+constexpr int kTagMaxPerThread = 4;  // G <= 4 * blockDim.x
+
+__device__ __forceinline__ bool tag_exchange(const TagExchange &x, unsigned epoch, double v,
+                                             double *total, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int G = gridDim.x, T = blockDim.x;
+  const double wsum = warp_sum(v);
+  if (lane == 0) sm[warp] = wsum;
+  __syncthreads();
+  const unsigned tag = epoch & 3u;
+  unsigned long long *buf = x.words + static_cast<size_t>(epoch % 3u) * G;
+  if (warp == 0) {
+    const double bt = warp_sum(lane < nw ? sm[lane] : 0.0);
+    if (lane == 0)
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[blockIdx.x])
+          .store((static_cast<unsigned long long>(__double_as_longlong(bt)) & ~3ull) | tag,
+                 cuda::memory_order_relaxed);
+  }
+  double got[kTagMaxPerThread];
+  int seen = 0, need = 0;
+#pragma unroll
+  for (int k = 0; k < kTagMaxPerThread; ++k) {
+    got[k] = 0.0;
+    if (static_cast<int>(threadIdx.x) + k * T < G) need |= 1 << k;
+  }
+  cuda::atomic_ref<int, cuda::thread_scope_device> err(*x.err);
+  bool ok = true;
+  for (unsigned spins = 0;; ++spins) {
+#pragma unroll
+    for (int k = 0; k < kTagMaxPerThread; ++k)
+      if ((need & ~seen) & (1 << k)) {
+        const unsigned long long u =
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(
+                buf[threadIdx.x + k * T])
+                .load(cuda::memory_order_relaxed);
+        if ((u & 3ull) == tag) {
+          got[k] = __longlong_as_double(static_cast<long long>(u));
+          seen |= 1 << k;
+        }
+      }
+    if (__syncthreads_and(seen == need)) break;
+    if ((spins & 63u) == 63u &&
+        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
+      ok = false;
+      break;
+    }
+    if (spins > x.spin_limit) {
+      if (threadIdx.x == 0) {
+        int expected = 0;
+        err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+      }
+      ok = false;
+      break;
+    }
+  }
+  // totals in a fixed order: per thread its blocks t, t+T, ..., then the
+  // threads' sums by the same tree in every block
+  double t = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTagMaxPerThread; ++k) t += got[k];
+  const double ws = warp_sum(t);
+  __syncthreads();
+  if (lane == 0) sm[warp] = ws;
+  __syncthreads();
+  if (warp == 0) {
+    const double tt = warp_sum(lane < nw ? sm[lane] : 0.0);
+    if (lane == 0) sm[32] = tt;
+  }
+  __syncthreads();
+  *total = sm[32];
+  __syncthreads();
+  return ok;
+}
+
 // One whole FP64 PCG iteration (one right-hand side) in one cooperative
 // launch: the three phases above with two grid barriers between them instead
 // of kernel boundaries.  A block keeps q = A p of its own rows in shared
@@ -434,10 +527,12 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
 // with the same expressions as in k_pcg_a/b/c (bit-identical rows).
 // The barriers are bounded: a wait that gives up records SFR_TIMEOUT, every
 // block leaves, and the solve stops with that status.
-template <typename I>
+// kTagged: the barriers are tag_exchange (mode 3) instead of grid_sync with
+// the partials read back after it.
+template <typename I, bool kTagged>
 __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
-                                               const GridSync &gs) {
-  __shared__ double sm[32 * 2];
+                                               const GridSync &gs, const TagExchange &tx) {
+  __shared__ double sm[33 * 2];
   extern __shared__ double qz[];  // this block's rows: q, then z
   if (!st->any) return;
   const int n = a.n;
@@ -467,13 +562,20 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
     qz[row_ - row0] = y[0];
     acc[0] += y[0] * ld_ro(a.p0[0] + row_);
   }
-  block_partials<1>(acc, a.part, G, sm);
-  if (!grid_sync(gs)) {
-    fail(SFR_TIMEOUT, j + 1);
-    return;
-  }
   double tot[1];
-  grid_totals<1>(a.part, G, G, tot, sm);
+  if (kTagged) {
+    if (!tag_exchange(tx, 2 * j + 1, acc[0], &tot[0], sm)) {
+      fail(SFR_TIMEOUT, j + 1);
+      return;
+    }
+  } else {
+    block_partials<1>(acc, a.part, G, sm);
+    if (!grid_sync(gs)) {
+      fail(SFR_TIMEOUT, j + 1);
+      return;
+    }
+    grid_totals<1>(a.part, G, G, tot, sm);
+  }
   const double alpha = d / tot[0];
   if (!isfinite(alpha)) {
     fail(SFR_BREAKDOWN, j + 1);
@@ -491,12 +593,19 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
     qz[row_ - row0] = zv;
     acc[0] += rv * zv;
   }
-  block_partials<1>(acc, a.part + G, G, sm);
-  if (!grid_sync(gs)) {
-    fail(SFR_TIMEOUT, j + 1);
-    return;
+  if (kTagged) {
+    if (!tag_exchange(tx, 2 * j + 2, acc[0], &tot[0], sm)) {
+      fail(SFR_TIMEOUT, j + 1);
+      return;
+    }
+  } else {
+    block_partials<1>(acc, a.part + G, G, sm);
+    if (!grid_sync(gs)) {
+      fail(SFR_TIMEOUT, j + 1);
+      return;
+    }
+    grid_totals<1>(a.part + G, G, G, tot, sm);
   }
-  grid_totals<1>(a.part + G, G, G, tot, sm);
   const double di = tot[0];
   const double beta = di / d;
   bool stop = false;
@@ -536,21 +645,25 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
 }
 
 // The fused iteration as launched: mode 1 leaves the register count to the
-// compiler (48), mode 2 holds it to 40 so that six blocks fit an SM.
+// compiler (48), mode 2 holds it to 40 so that six blocks fit an SM, mode 3
+// is mode 1 with the tagged exchanges.
 template <typename I, int kMode>
-__global__ void __launch_bounds__(256) k_pcg_fused(const SArgs<1> a, SState<1> *st, GridSync gs) {
-  pcg_fused_body<I>(a, st, gs);
+__global__ void __launch_bounds__(256) k_pcg_fused(const SArgs<1> a, SState<1> *st, GridSync gs,
+                                                   TagExchange tx) {
+  pcg_fused_body<I, kMode == 3>(a, st, gs, tx);
 }
 template <typename I>
 __global__ void __launch_bounds__(256, 6) k_pcg_fused_r40(const SArgs<1> a, SState<1> *st,
-                                                          GridSync gs) {
-  pcg_fused_body<I>(a, st, gs);
+                                                          GridSync gs, TagExchange tx) {
+  pcg_fused_body<I, false>(a, st, gs, tx);
 }
 
 // The fused kernel of a mode.
 template <typename I>
 const void *fused_kernel(int mode) {
-  return mode == 2 ? (const void *)k_pcg_fused_r40<I> : (const void *)k_pcg_fused<I, 1>;
+  return mode == 2   ? (const void *)k_pcg_fused_r40<I>
+         : mode == 3 ? (const void *)k_pcg_fused<I, 3>
+                     : (const void *)k_pcg_fused<I, 1>;
 }
 
 // reliable update, part 1: x += xs (FP64) for the flagged right-hand sides
@@ -1172,6 +1285,7 @@ struct CachedGraph {
   int grid_s = 0, grid_v = 0, threads = 256;
   int grid_f = 0;        // fused iteration: co-resident blocks
   size_t smem_f = 0;     // fused iteration: dynamic shared memory a block
+  unsigned long long *tagw = nullptr;  // fused mode 3: the exchange words (3 * grid_f)
   uint64_t last_use = 0;
   int64_t bytes = 0;
 };
@@ -1338,7 +1452,8 @@ int fused_shape(sfr_system *s, int mode, size_t *smem) {
   const int nsl = s->A.nslices;
   const int maxg = std::max(1, (nsl + 7) / 8);
   for (int per_sm = 8; per_sm >= 1; --per_sm) {
-    const int G = std::min(maxg, per_sm * sms);
+    int G = std::min(maxg, per_sm * sms);
+    if (mode == 3) G = std::min(G, kTagMaxPerThread * 256);  // the exchange's reach
     const size_t bytes = static_cast<size_t>((nsl + G - 1) / G) * kWarp * sizeof(double);
     if (bytes > 200 * 1024) continue;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1353,6 +1468,14 @@ int fused_shape(sfr_system *s, int mode, size_t *smem) {
     }
   }
   return 0;
+}
+
+TagExchange fused_exchange(const CachedGraph *cg) {
+  TagExchange t;
+  t.words = cg->tagw;
+  t.err = reinterpret_cast<int *>(cg->counter + 14);
+  t.spin_limit = 1u << 22;
+  return t;
 }
 
 GridSync fused_barrier(const CachedGraph *cg) {
@@ -1405,6 +1528,20 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
     mp.pitch = 0;
     SFR_TRY(cudaGraphAddMemsetNode(&prev, g, nullptr, 0, &mp));
   }
+  if (fused == 3 && cg->grid_f > 0) {
+    // the fused iteration's exchange words start every solve at zero
+    SFR_TRY(cudaMalloc(&cg->tagw, sizeof(unsigned long long) * 3 * cg->grid_f));
+    cudaMemsetParams mt{};
+    mt.dst = cg->tagw;
+    mt.value = 0;
+    mt.elementSize = sizeof(unsigned);
+    mt.width = 6 * static_cast<size_t>(cg->grid_f);
+    mt.height = 1;
+    mt.pitch = 0;
+    cudaGraphNode_t mn;
+    SFR_TRY(cudaGraphAddMemsetNode(&mn, g, &prev, 1, &mt));
+    prev = mn;
+  }
   cudaGraph_t body = nullptr, ifbody = nullptr;
   if (solver == SFR_PCG) {
     if (mixed) {
@@ -1428,7 +1565,8 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
       if (fused && K == 1) {
         // one cooperative kernel an iteration (k_pcg_fused)
         GridSync gsync = fused_barrier(cg);
-        void *pf3[3] = {&a, &ps, &gsync};
+        TagExchange tx = fused_exchange(cg);
+        void *pf3[4] = {&a, &ps, &gsync, &tx};
         cudaKernelNodeParams kp{};
         kp.func = const_cast<void *>(fused_kernel<I>(fused));
         kp.gridDim = dim3(cg->grid_f);
@@ -1491,6 +1629,7 @@ void free_graph(CachedGraph *cg) {
   cudaFree(cg->ws);
   cudaFree(cg->part);
   cudaFree(cg->counter);
+  cudaFree(cg->tagw);
   *cg = CachedGraph{};
 }
 
@@ -1505,6 +1644,8 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
   auto *ps = static_cast<SState<K> *>(cg->d_state);
   const int gs = cg->grid_s, gv = cg->grid_v, t = cg->threads;
   SFR_TRY(cudaMemsetAsync(cg->counter, 0, sizeof(unsigned) * kCounters, st));
+  if (cg->tagw)
+    SFR_TRY(cudaMemsetAsync(cg->tagw, 0, sizeof(unsigned long long) * 3 * cg->grid_f, st));
   if (solver == SFR_PCG) {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
@@ -1524,7 +1665,8 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
         if constexpr (K == 1) {
           if (fused) {
             GridSync gsync = fused_barrier(cg);
-            void *pf3[3] = {&a, &ps, &gsync};
+            TagExchange tx = fused_exchange(cg);
+            void *pf3[4] = {&a, &ps, &gsync, &tx};
             SFR_TRY(cudaLaunchCooperativeKernel(fused_kernel<I>(fused), dim3(cg->grid_f),
                                                 dim3(256), pf3, cg->smem_f, st));
             continue;

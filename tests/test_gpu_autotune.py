@@ -64,7 +64,7 @@ def test_autotune_choice_is_kept_and_solves_at_parity(cuda, tmp_path, monkeypatc
 @pytest.mark.parametrize("engine,threads,spw,pf,fused",
                          [(2, 128, 0, 0, 0), (2, 256, 2, 0, 0), (2, 256, 8, 0, 0),
                           (2, 256, 0, 2, 0), (2, 256, 0, 0, 1), (2, 256, 0, 0, 2),
-                          (3, 256, 0, 0, 1),
+                          (2, 256, 0, 0, 3), (3, 256, 0, 0, 1), (3, 256, 0, 0, 3),
                           (1, 0, 0, 0, 0)])
 def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf, fused):
     """Whatever the tuner picks, the arithmetic is the reference's: every
