@@ -162,10 +162,10 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
  * iteration as one cooperative kernel (SpMV and dot, grid barrier, x/r/z
  * update and dot, grid barrier, p update) that keeps q = A p and then
  * z = M r of a block's rows in shared memory instead of HBM; mode 2 is the
- * same kernel held to 40 registers so that six blocks fit an SM; mode 3
- * replaces the counter barriers by a tagged exchange (every block polls
- * every block's partial sum, which carries the epoch in its two lowest
- * bits: one L2 round trip).  Solves it
+ * same kernel held to 40 registers so that six blocks fit an SM; in mode 3
+ * the last block to arrive at a barrier sums the partials once and
+ * broadcasts the total in one epoch-tagged word that the others poll.
+ * Solves it
  * does not serve (other solvers, K > 1, mixed precision, or no co-resident
  * shape) take the three-kernel iteration.  0 (the default) turns it off;
  * other values are SFR_BAD_INPUT. */

@@ -423,95 +423,86 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
   }
 }
 
-// Partial sums between the blocks of a co-resident grid without a counter:
-// each block stores its total in its own word with the two lowest bits of the
-// FP64 pattern replaced by the epoch's tag (epoch & 3, at most 3 units in the
-// last place), and every block polls every block's word until all carry the
-// tag -- the values travel in the polled words, so an exchange is one L2
-// round trip.  Three buffers rotate (epoch % 3): a word is rewritten only
-// three epochs after its last use, by which time every block has read it,
-// and the tag of that last use differs from the new one.  Every block sums
-// the G totals in the same fixed order, so all hold the same bits.  The
-// buffers start zeroed, and epochs start at 1, so a zero word never carries
-// the tag of a buffer's first use.  Only the partial sums cross: no other
-// global data is ordered by it.  A wait gives up after spin_limit polls and
-// records SFR_TIMEOUT in *err.
+// Partial sums of a co-resident grid, reduced once and broadcast: every block
+// stores its total in part[b], then arrives at one counter; the last block
+// to arrive sums the G totals in block order and publishes the sum in one
+// word whose two lowest bits carry the epoch's tag (epoch & 3, at most 3
+// units in the last place), after resetting the counter; every other block
+// polls that word (acquire) until it carries the tag.  So the G partials are read once
+// (by the last block) instead of by every block, and the waiters' one poll
+// brings the value.  The word is rewritten every epoch; a waiter for epoch e
+// finds there epoch e-1's sum (another tag) until e's arrives.  It starts
+// each solve at zero and epochs start at 1.  Only the partial sums cross: no
+// other global data is ordered by it.  A wait gives up after spin_limit polls
+// and records SFR_TIMEOUT in *err.
 struct TagExchange {
-  unsigned long long *words;  // 3 * G, zero at the start of a solve
+  unsigned long long *word;  // the broadcast word, zero at the start of a solve
+  unsigned *count;           // arrivals, zero between exchanges
   int *err;
   unsigned spin_limit;
 };
 
-constexpr int kTagMaxPerThread = 4;  // G <= 4 * blockDim.x
-
 __device__ __forceinline__ bool tag_exchange(const TagExchange &x, unsigned epoch, double v,
-                                             double *total, double *sm) {
+                                             double *part, double *total, double *sm) {
+  __shared__ int s_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int G = gridDim.x, T = blockDim.x;
+  const int G = gridDim.x;
   const double wsum = warp_sum(v);
   if (lane == 0) sm[warp] = wsum;
   __syncthreads();
   const unsigned tag = epoch & 3u;
-  unsigned long long *buf = x.words + static_cast<size_t>(epoch % 3u) * G;
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> word(*x.word);
+  cuda::atomic_ref<int, cuda::thread_scope_device> err(*x.err);
   if (warp == 0) {
     const double bt = warp_sum(lane < nw ? sm[lane] : 0.0);
-    if (lane == 0)
-      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[blockIdx.x])
-          .store((static_cast<unsigned long long>(__double_as_longlong(bt)) & ~3ull) | tag,
-                 cuda::memory_order_relaxed);
-  }
-  double got[kTagMaxPerThread];
-  int seen = 0, need = 0;
-#pragma unroll
-  for (int k = 0; k < kTagMaxPerThread; ++k) {
-    got[k] = 0.0;
-    if (static_cast<int>(threadIdx.x) + k * T < G) need |= 1 << k;
-  }
-  cuda::atomic_ref<int, cuda::thread_scope_device> err(*x.err);
-  bool ok = true;
-  for (unsigned spins = 0;; ++spins) {
-#pragma unroll
-    for (int k = 0; k < kTagMaxPerThread; ++k)
-      if ((need & ~seen) & (1 << k)) {
-        const unsigned long long u =
-            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(
-                buf[threadIdx.x + k * T])
-                .load(cuda::memory_order_relaxed);
-        if ((u & 3ull) == tag) {
-          got[k] = __longlong_as_double(static_cast<long long>(u));
-          seen |= 1 << k;
-        }
-      }
-    if (__syncthreads_and(seen == need)) break;
-    if ((spins & 63u) == 63u &&
-        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
-      ok = false;
-      break;
+    if (lane == 0) {
+      st_vec(part + blockIdx.x, bt);
+      __threadfence();
+      s_last = atomicAdd(x.count, 1u) == static_cast<unsigned>(G) - 1u;
     }
-    if (spins > x.spin_limit) {
-      if (threadIdx.x == 0) {
+  }
+  __syncthreads();
+  bool ok = true;
+  if (s_last) {
+    __threadfence();
+    if (warp == 0) {
+      double t = 0.0;
+      for (int b = lane; b < G; b += 32) t += ld_vec(part + b);
+      t = warp_sum(t);
+      if (lane == 0) {
+        *x.count = 0u;
+        const unsigned long long u =
+            (static_cast<unsigned long long>(__double_as_longlong(t)) & ~3ull) | tag;
+        word.store(u, cuda::memory_order_release);
+        sm[32] = __longlong_as_double(static_cast<long long>(u));
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    for (unsigned spins = 0;; ++spins) {
+      // acquire: the counter's reset before the publication is visible to
+      // this block's next arrival
+      const unsigned long long u = word.load(cuda::memory_order_acquire);
+      if ((u & 3ull) == tag) {
+        sm[32] = __longlong_as_double(static_cast<long long>(u));
+        break;
+      }
+      if (err.load(cuda::memory_order_relaxed) != 0) {
+        ok = false;
+        break;
+      }
+      if (spins > x.spin_limit) {
         int expected = 0;
         err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+        ok = false;
+        break;
       }
-      ok = false;
-      break;
     }
+    if (!ok) sm[33] = 1.0;
   }
-  // totals in a fixed order: per thread its blocks t, t+T, ..., then the
-  // threads' sums by the same tree in every block
-  double t = 0.0;
-#pragma unroll
-  for (int k = 0; k < kTagMaxPerThread; ++k) t += got[k];
-  const double ws = warp_sum(t);
-  __syncthreads();
-  if (lane == 0) sm[warp] = ws;
-  __syncthreads();
-  if (warp == 0) {
-    const double tt = warp_sum(lane < nw ? sm[lane] : 0.0);
-    if (lane == 0) sm[32] = tt;
-  }
+  if (threadIdx.x == 0 && ok) sm[33] = 0.0;
   __syncthreads();
   *total = sm[32];
+  ok = sm[33] == 0.0;
   __syncthreads();
   return ok;
 }
@@ -527,12 +518,12 @@ __device__ __forceinline__ bool tag_exchange(const TagExchange &x, unsigned epoc
 // with the same expressions as in k_pcg_a/b/c (bit-identical rows).
 // The barriers are bounded: a wait that gives up records SFR_TIMEOUT, every
 // block leaves, and the solve stops with that status.
-// kTagged: the barriers are tag_exchange (mode 3) instead of grid_sync with
-// the partials read back after it.
+// kTagged: the barriers are tag_exchange (mode 3: the last block reduces and
+// broadcasts) instead of grid_sync with every block reading the partials.
 template <typename I, bool kTagged>
 __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
                                                const GridSync &gs, const TagExchange &tx) {
-  __shared__ double sm[33 * 2];
+  __shared__ double sm[34 * 2];
   extern __shared__ double qz[];  // this block's rows: q, then z
   if (!st->any) return;
   const int n = a.n;
@@ -564,7 +555,7 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
   }
   double tot[1];
   if (kTagged) {
-    if (!tag_exchange(tx, 2 * j + 1, acc[0], &tot[0], sm)) {
+    if (!tag_exchange(tx, 2 * j + 1, acc[0], a.part, &tot[0], sm)) {
       fail(SFR_TIMEOUT, j + 1);
       return;
     }
@@ -594,7 +585,7 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
     acc[0] += rv * zv;
   }
   if (kTagged) {
-    if (!tag_exchange(tx, 2 * j + 2, acc[0], &tot[0], sm)) {
+    if (!tag_exchange(tx, 2 * j + 2, acc[0], a.part + G, &tot[0], sm)) {
       fail(SFR_TIMEOUT, j + 1);
       return;
     }
@@ -1285,7 +1276,7 @@ struct CachedGraph {
   int grid_s = 0, grid_v = 0, threads = 256;
   int grid_f = 0;        // fused iteration: co-resident blocks
   size_t smem_f = 0;     // fused iteration: dynamic shared memory a block
-  unsigned long long *tagw = nullptr;  // fused mode 3: the exchange words (3 * grid_f)
+  unsigned long long *tagw = nullptr;  // fused mode 3: the broadcast word
   uint64_t last_use = 0;
   int64_t bytes = 0;
 };
@@ -1452,8 +1443,7 @@ int fused_shape(sfr_system *s, int mode, size_t *smem) {
   const int nsl = s->A.nslices;
   const int maxg = std::max(1, (nsl + 7) / 8);
   for (int per_sm = 8; per_sm >= 1; --per_sm) {
-    int G = std::min(maxg, per_sm * sms);
-    if (mode == 3) G = std::min(G, kTagMaxPerThread * 256);  // the exchange's reach
+    const int G = std::min(maxg, per_sm * sms);
     const size_t bytes = static_cast<size_t>((nsl + G - 1) / G) * kWarp * sizeof(double);
     if (bytes > 200 * 1024) continue;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1472,7 +1462,8 @@ int fused_shape(sfr_system *s, int mode, size_t *smem) {
 
 TagExchange fused_exchange(const CachedGraph *cg) {
   TagExchange t;
-  t.words = cg->tagw;
+  t.word = cg->tagw;
+  t.count = cg->counter + 11;
   t.err = reinterpret_cast<int *>(cg->counter + 14);
   t.spin_limit = 1u << 22;
   return t;
@@ -1530,12 +1521,12 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   }
   if (fused == 3 && cg->grid_f > 0) {
     // the fused iteration's exchange words start every solve at zero
-    SFR_TRY(cudaMalloc(&cg->tagw, sizeof(unsigned long long) * 3 * cg->grid_f));
+    SFR_TRY(cudaMalloc(&cg->tagw, sizeof(unsigned long long)));
     cudaMemsetParams mt{};
     mt.dst = cg->tagw;
     mt.value = 0;
     mt.elementSize = sizeof(unsigned);
-    mt.width = 6 * static_cast<size_t>(cg->grid_f);
+    mt.width = 2;
     mt.height = 1;
     mt.pitch = 0;
     cudaGraphNode_t mn;
@@ -1644,8 +1635,7 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
   auto *ps = static_cast<SState<K> *>(cg->d_state);
   const int gs = cg->grid_s, gv = cg->grid_v, t = cg->threads;
   SFR_TRY(cudaMemsetAsync(cg->counter, 0, sizeof(unsigned) * kCounters, st));
-  if (cg->tagw)
-    SFR_TRY(cudaMemsetAsync(cg->tagw, 0, sizeof(unsigned long long) * 3 * cg->grid_f, st));
+  if (cg->tagw) SFR_TRY(cudaMemsetAsync(cg->tagw, 0, sizeof(unsigned long long), st));
   if (solver == SFR_PCG) {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
