@@ -447,14 +447,17 @@ int sfr_gpu_pres_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
  * (CellSimple.c:106-727) placed by csrSimple (Csr.c:1024): the u, v, w
  * systems share the off-diagonals and carry their own diagonals, forces and
  * residuals; the momentum D field (V / a_P, or V / (a_P - sum a_N) for
- * SIMPLEC) comes out for the pressure correction.  Restated for laminar flow
- * (no eddy viscosity, structural stress or wall model), first-order upwind
- * advection (FoUp: no deferred correction) and face velocities without
- * Rhie-Chow (with it on, the reference's serial loop reads D fields it has
- * already overwritten, so its result depends on the cell order); velocity
- * loads MOVEWALL, STATICWALL and constant INLET (the others are
- * SFR_UNSUPPORTED).  mesh->facer is faceVelR; mesh->cc and mesh->xm are
- * required.  CSRD or CSRC. */
+ * SIMPLEC) comes out for the pressure correction.  Restated without a wall
+ * model (an eddy viscosity field and the residual stress integral are bound
+ * by sfr_gpu_vel_turbulence), with the advection schemes of adv below and
+ * face velocities without Rhie-Chow (with it on, the reference's serial loop
+ * reads D fields it has already overwritten, so its result depends on the
+ * cell order).  Velocity loads: MOVEWALL, STATICWALL, constant INLET,
+ * OUTLET, OPEN, INLETTOTALPRES and INLETSTAICTPRES, whose inflow direction is
+ * the load's par[0..2] (the reference's getLoads copies no parameter for
+ * that type, Loads.c:148-150, and its pLoadSimple reads an uninitialised
+ * array); an INLET given as a function is SFR_UNSUPPORTED.  mesh->facer is
+ * faceVelR; mesh->cc and mesh->xm are required.  CSRD or CSRC. */
 typedef struct {
   int32_t icod;        /* Diffusion.iCod: 1..4 */
   int32_t fso;         /* MomentumModel.fSoPressure: second-order face pressure */

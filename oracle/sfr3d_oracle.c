@@ -1307,8 +1307,66 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
             p[0] -= mflux * tA[0];
             p[1] -= mflux * tA[1];
             p[2] -= mflux * tA[2];
-          } else if (ld->type == 7 || ld->type == 9 || ld->type == 10 || ld->type == 13) {
-            return -2; /* OUTLET, INLETSTAICTPRES, OPEN, INLETTOTALPRES */
+          } else if (ld->type == 7 || ld->type == 10) { /* OUTLET, OPEN */
+            const double wfn = dot3c(velC, nrm);
+            if (ld->type == 10 && wfn < 0.e0) {
+              /* OPEN inflow (Loads.c:604-627): the cell's own direction */
+              const double mflux = ld->density * wfn * area;
+              double modv = velC[0] * velC[0] + velC[1] * velC[1];
+              double aP;
+              modv += velC[2] * velC[2];
+              modv = 1.e0 / sqrt(modv);
+              aP = mflux * wfn * modv;
+              for (k = 0; k < 3; k++) p[k] -= aP * velC[k];
+            } else {
+              /* OUTLET (Loads.c:436-518) and OPEN outflow (Loads.c:531-600) */
+              const double mflux = rhoC * wfn * area;
+              double ef[3], prod[3], gvf[3][3], mod, tf;
+              if (ld->type == 7) { /* stress (CellLib.c:7013), lambda = 0 */
+                const double tr = gvC[0][0] + gvC[1][1] + gvC[2][2];
+                double ss[6];
+                ss[0] = 2.e0 * muC * gvC[0][0] + 0.0 * tr;
+                ss[1] = 2.e0 * muC * gvC[1][1] + 0.0 * tr;
+                ss[2] = 2.e0 * muC * gvC[2][2] + 0.0 * tr;
+                ss[3] = muC * (gvC[1][0] + gvC[0][1]);
+                ss[4] = muC * (gvC[2][1] + gvC[1][2]);
+                ss[5] = muC * (gvC[2][0] + gvC[0][2]);
+                p[0] += ss[0] * s[0] + ss[3] * s[1] + ss[5] * s[2];
+                p[1] += ss[3] * s[0] + ss[1] * s[1] + ss[4] * s[2];
+                p[2] += ss[5] * s[0] + ss[4] * s[1] + ss[2] * s[2];
+              }
+              /* gradFaceNull (CellLib.c:5477-5600): the cell gradient less
+               * its part along the centroid-to-face direction */
+              mod = sqrt(xmcc[0] * xmcc[0] + xmcc[1] * xmcc[1] + xmcc[2] * xmcc[2]);
+              for (j = 0; j < 3; j++) ef[j] = xmcc[j] / mod;
+              for (i = 0; i < 3; i++)
+                prod[i] = gvC[i][0] * ef[0] + gvC[i][1] * ef[1] + gvC[i][2] * ef[2];
+              for (i = 0; i < 3; i++)
+                for (j = 0; j < 3; j++) gvf[i][j] = gvC[i][j] - prod[i] * ef[j];
+              for (i = 0; i < 3; i++) {
+                tf = gvf[i][0] * xmcc[0] + gvf[i][1] * xmcc[1] + gvf[i][2] * xmcc[2];
+                p[i] -= mflux * tf;
+              }
+              for (i = 0; i < 3; i++) sPc[i] += mflux;
+            }
+          } else if (ld->type == 9) {
+            /* INLETSTAICTPRES (Loads.c:364-392).  getLoads copies nothing
+             * for this type (Loads.c:148-150), so the reference reads an
+             * uninitialised par[]; this restatement reads the load's own
+             * par[0..2] as the inflow direction. */
+            const double wfn = dot3c(velC, nrm);
+            const double dn = ld->par[0] * nrm[0] + ld->par[1] * nrm[1] + ld->par[2] * nrm[2];
+            const double t3 = wfn / dn, mflux = rhoC * wfn * area;
+            for (k = 0; k < 3; k++) p[k] -= mflux * ld->par[k] * t3;
+          } else if (ld->type == 13) {
+            /* INLETTOTALPRES (Loads.c:634-672): density par[0], direction
+             * par[2..4] (getLoads copies 5 parameters) */
+            const double rho = ld->par[0];
+            const double ev[3] = {ld->par[2], ld->par[3], ld->par[4]};
+            const double t0 = dot3c(velC, nrm), t1 = dot3c(ev, nrm) * area;
+            const double mflux = rho * t0 * area;
+            const double modv = mflux / (rho * t1), tm = mflux * modv;
+            for (k = 0; k < 3; k++) p[k] -= tm * ev[k];
           }
         }
       }

@@ -167,9 +167,11 @@ typedef struct {
  * nmat x MAXPROP (DYNAMICVISCOSITY 0, DENSITY 1); vel, gradpres, dfield
  * numel*3; gradvel numel*9 (row i = grad u_i).  dfield is updated in place
  * cell by cell as the reference does.  a: al (al|au for unsym CSRC); ad and
- * b: 3*neq (u, v, w blocks); rcell 3*numel.  Returns 0, -1 for input the
- * reference cannot take, -2 for loads outside MOVEWALL, STATICWALL and
- * constant INLET. */
+ * b: 3*neq (u, v, w blocks); rcell 3*numel.  Velocity loads: MOVEWALL,
+ * STATICWALL, constant INLET, OUTLET, OPEN, INLETTOTALPRES and
+ * INLETSTAICTPRES (whose direction is the load's own par[0..2]: the
+ * reference reads an uninitialised array there).  Returns 0, -1 for input
+ * the reference cannot take, -2 for an INLET given as a function. */
 int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
                      const double *xm, const orc_load *lvel, int nlvel,
                      const orc_vel_opts *o, const double *prop, const double *pres,

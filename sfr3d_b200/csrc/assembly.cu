@@ -270,12 +270,13 @@ __global__ void plan_kernel(MeshDev m, PatternDev P, PlanDev p, int icod, int ki
           g[3 + j] = nrm[j];
           g[6 + j] = 0.0;
         }
-      } else if (kind == 2) {  // faceVelR's load; [9..11] normal, 12 area
+      } else if (kind == 2) {  // faceVelR's load; [9..11] normal, 12 area, [13..15] xmcc
         nbv = ld > 0 ? -(ld - 1) - 2 : -1;
         for (int j = 0; j < 3; ++j) {
           g[3 + j] = ksi[j];
           g[6 + j] = 0.0;
           g[9 + j] = nrm[j];
+          g[13 + j] = m.xmcc[3 * q + j];
         }
         g[12] = m.area[face];
       } else {
@@ -1010,6 +1011,58 @@ __global__ void __launch_bounds__(256, 2)
           pp[1] = xadd(pp[1], dot3(r1, sa));
           pp[2] = xadd(pp[2], dot3(r2, sa));
           for (int k = 0; k < 3; ++k) pp[k] = xsub(pp[k], xmul(mflux, tA[k]));
+        } else if (L.type == 7 || L.type == 10) {  // OUTLET, OPEN
+          const double wfn = dot3(velC, n);
+          if (L.type == 10 && wfn < 0.0) {
+            // OPEN inflow (Loads.c:604-627): along the cell's own velocity
+            const double mflux = xmul(xmul(L.density, wfn), area);
+            const double aP = xmul(xmul(mflux, wfn), xdiv(1.0, xsqrt(dot3(velC, velC))));
+            for (int k = 0; k < 3; ++k) pp[k] = xsub(pp[k], xmul(aP, velC[k]));
+          } else {
+            // OUTLET (Loads.c:436-518), OPEN outflow (Loads.c:531-600)
+            const double mflux = xmul(xmul(rhoC, wfn), area);
+            if (L.type == 7) {  // stress (CellLib.c:7013), lambda = 0
+              const double tr = xadd(xadd(gvC[0], gvC[4]), gvC[8]);
+              const double nu2 = xmul(2.0, muC), z = xmul(0.0, tr);
+              const double ss[6] = {xadd(xmul(nu2, gvC[0]), z), xadd(xmul(nu2, gvC[4]), z),
+                                    xadd(xmul(nu2, gvC[8]), z), xmul(muC, xadd(gvC[3], gvC[1])),
+                                    xmul(muC, xadd(gvC[7], gvC[5])),
+                                    xmul(muC, xadd(gvC[6], gvC[2]))};
+              const double sa[3] = {xmul(area, n[0]), xmul(area, n[1]), xmul(area, n[2])};
+              const double r0[3] = {ss[0], ss[3], ss[5]}, r1[3] = {ss[3], ss[1], ss[4]},
+                           r2[3] = {ss[5], ss[4], ss[2]};
+              pp[0] = xadd(pp[0], dot3(r0, sa));
+              pp[1] = xadd(pp[1], dot3(r1, sa));
+              pp[2] = xadd(pp[2], dot3(r2, sa));
+            }
+            // gradFaceNull (CellLib.c:5477-5600): the cell gradient less its
+            // part along the centroid-to-face direction, applied to xmcc
+            const double xc[3] = {__ldcs(g + 13 * fs), __ldcs(g + 14 * fs), __ldcs(g + 15 * fs)};
+            const double mod = xsqrt(dot3(xc, xc));
+            const double ef[3] = {xdiv(xc[0], mod), xdiv(xc[1], mod), xdiv(xc[2], mod)};
+            for (int i = 0; i < 3; ++i) {
+              const double prod = dot3(gvC + 3 * i, ef);
+              double gf[3];
+              for (int j = 0; j < 3; ++j) gf[j] = xsub(gvC[3 * i + j], xmul(prod, ef[j]));
+              pp[i] = xsub(pp[i], xmul(mflux, dot3(gf, xc)));
+              sPc[i] = xadd(sPc[i], mflux);
+            }
+          }
+        } else if (L.type == 9) {
+          // INLETSTAICTPRES (Loads.c:364-392), the load's par[0..2] as the
+          // inflow direction (the reference's getLoads copies none for it)
+          const double wfn = dot3(velC, n);
+          const double dir[3] = {L.par[0], L.par[1], L.par[2]};
+          const double t3 = xdiv(wfn, dot3(dir, n));
+          const double mflux = xmul(xmul(rhoC, wfn), area);
+          for (int k = 0; k < 3; ++k) pp[k] = xsub(pp[k], xmul(xmul(mflux, dir[k]), t3));
+        } else if (L.type == 13) {
+          // INLETTOTALPRES (Loads.c:634-672): density par[0], direction par[2..4]
+          const double ev[3] = {L.par[2], L.par[3], L.par[4]};
+          const double t1 = xmul(dot3(ev, n), area);
+          const double mflux = xmul(xmul(L.par[0], dot3(velC, n)), area);
+          const double tm = xmul(mflux, xdiv(mflux, xmul(L.par[0], t1)));
+          for (int k = 0; k < 3; ++k) pp[k] = xsub(pp[k], xmul(tm, ev[k]));
         }
       }
     }
@@ -1233,9 +1286,11 @@ int stage_pres_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
   return stage_table(p, h, st);
 }
 
-// Momentum: pLoadSimple with fCalVel (Loads.c:265-720) for the loads this
-// kernel restates (MOVEWALL, STATICWALL, constant INLET); prop: nmat x
-// MAXPROP (DYNAMICVISCOSITY 0, DENSITY 1).
+// Momentum: pLoadSimple with fCalVel (Loads.c:265-720): MOVEWALL,
+// STATICWALL, constant INLET, OUTLET, OPEN, INLETSTAICTPRES and
+// INLETTOTALPRES (getLoads copies par[0..4] of the last two, Loads.c:148-155,
+// and OPEN reads Loads.density); prop: nmat x MAXPROP (DYNAMICVISCOSITY 0,
+// DENSITY 1).
 int stage_vel_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel, const double *prop,
                      cudaStream_t st) {
   if (nlvel < 0 || nlvel > sfr::kMaxLoads || (nlvel > 0 && !lvel))
@@ -1245,9 +1300,6 @@ int stage_vel_tables(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel, const
     if (!(p->used_loads & (1u << l))) continue;
     if (l >= nlvel) return bad("a boundary face names a velocity load beyond nlvel");
     const sfr_load &L = lvel[l];
-    if (L.type == 7 || L.type == 9 || L.type == 10 || L.type == 13)
-      return unsupported("OUTLET, INLETSTAICTPRES, OPEN and INLETTOTALPRES velocity loads are "
-                         "not assembled on the device");
     if (L.type == 6 && L.var != 0)
       return unsupported("loads given as functions (nTypeVar 1) are not assembled on the device");
     if (L.type == 6 && (L.np < 3 || L.np > 20)) return bad("an INLET load needs 3..20 parameters");

@@ -324,6 +324,88 @@ def test_vel_oracle_turbulence_matches_reference_live():
     assert not np.array_equal(lam[1], tur[1]) and not np.array_equal(lam[3], tur[3])
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_vel_oracle_outflow_loads_match_reference_live():
+    """OUTLET (stress plus the null normal gradient, sP += m), OPEN (outflow
+    as OUTLET without the stress, inflow along the cell's own velocity) and
+    INLETTOTALPRES (pLoadSimple, Loads.c:436-672) against the reference's
+    own systFormSimpleVel, on every layout, with the cell velocities of
+    both signs on each side."""
+    s = S.poisson_jittered(5, seed=10)
+    m = s.mesh()
+    rng = np.random.default_rng(11)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.OUTLET, ()), O.Load(O.OPEN, (0.0,), density=1.1),
+            O.Load(O.INLETTOTALPRES, (1.05, 2.0, 0.6, -0.5, 0.4))]
+    for sides, icod, ts, adv in itertools.product(([1, 2, 3, 4, 1, 3], [4, 3, 2, 1, 2, 2]),
+                                                  (1, 4), (O.SIMPLE, O.SIMPLEC),
+                                                  (O.FOUP, O.SOUP)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r(sides),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop, mat=mat,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)),
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=icod, fvisc=True,
+                         type_simple=ts, under=0.7, adv=adv)
+        for name, (st, un, ia_, ja_, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (sides, icod, ts, adv, name)
+    # the outflow loads change the diagonal (sP += m) and b against a wall
+    wall = O.vel_assemble(O.VelCase(**{**case.__dict__, "lvel": [lvel[0]] * 4}), O.CSRD, True,
+                          s.ia, s.ja, s.neq)
+    out = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    assert not np.array_equal(wall[2], out[2]) and not np.array_equal(wall[3], out[3])
+
+
+def test_vel_oracle_inlet_static_pressure_direction():
+    """INLETSTAICTPRES (Loads.c:364-392): the reference's getLoads copies no
+    parameters for this type (Loads.c:148-150) and reads an uninitialised
+    array, so no run of it pins the branch; the restatement takes the load's
+    own par[0..2] as the inflow direction.  Checked here by its algebra: the
+    force is -m (t . n)^-1 (v . n) t on each inflow face, t the direction."""
+    s = S.poisson_uniform(4, seed=12)
+    m = s.mesh()
+    rng = np.random.default_rng(13)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.3)
+    t = (0.7, -0.2, 0.3)
+    base = dict(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 0, 0, 0, 0, 0]),
+                facepresr=m.face_r([0] * 6), prop=prop, pres=np.zeros(m.numel),
+                gradpres=np.zeros((m.numel, 3)), vel=rng.standard_normal((m.numel, 3)),
+                gradvel=np.zeros((m.numel, 3, 3)), dfield=np.ones((m.numel, 3)), under=1.0)
+    wall = O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.CSRD, True,
+                          s.ia, s.ja, s.neq)
+    isp = O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.INLETSTAICTPRES, t + (1.0,))]),
+                         O.CSRD, True, s.ia, s.ja, s.neq)
+    none = O.vel_assemble(O.VelCase(**{**base, "facevelr": m.face_r([0] * 6)},
+                                    lvel=[O.Load(O.STATICWALL, ())]), O.CSRD, True,
+                          s.ia, s.ja, s.neq)
+    assert wall[0] == isp[0] == none[0] == 0
+    # the load touches b only: no diagonal share, as the reference's branch
+    assert np.array_equal(isp[1], none[1]) and np.array_equal(isp[2], none[2])
+    db = (isp[3] - none[3]).reshape(3, s.neq)
+    for c in np.flatnonzero(m.nelcon[:, 0] == -1):
+        face = m.cellface[c, 0] - 1
+        ch = 1.0 if m.owner[face, 0] - 1 == c else -1.0  # the normal out of cell c
+        nrm = ch * np.asarray(m.normal[face])
+        row = m.id[c] - 1
+        v = base["vel"][c]
+        wfn = v @ nrm
+        want = -1.3 * wfn * m.area[face] * (wfn / (np.asarray(t) @ nrm)) * np.asarray(t)
+        np.testing.assert_allclose(db[:, row], want, rtol=1e-12, atol=1e-14)
+
+
 def test_vel_oracle_rejects_what_it_does_not_restate():
     s = S.poisson_uniform(4, seed=1)
     m = s.mesh()
@@ -336,7 +418,7 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     run = lambda **kw: O.vel_assemble(O.VelCase(**{**base, **kw}), O.CSRD, True,  # noqa: E731
                                       s.ia, s.ja, s.neq)[0]
     assert run(lvel=[O.Load(O.STATICWALL, ())]) == 0
-    assert run(lvel=[O.Load(O.OUTLET, ())]) == -2
+    assert run(lvel=[O.Load(O.OUTLET, ())]) == 0
     assert run(lvel=[O.Load(O.INLET, (1.0, 0.0, 0.0, 1.0), var=1)]) == -2
     assert run(lvel=[O.Load(O.STATICWALL, ())], type_simple=3) == -1
     assert run(lvel=[O.Load(O.STATICWALL, ())], adv=4, adv_fn=6) == -1  # no such limiter
