@@ -259,6 +259,118 @@ __device__ __forceinline__ void row_product_t(const int *sptr, const I *colp, co
   }
 }
 
+// L2 prefetch for an iteration's SpMV phase: lane 0 of each warp asks for
+// the slice the warp reaches `pf` rounds later (a round: every warp of the
+// block one slice further), within the block's own slices.  A slice's slot
+// columns and values are each one contiguous run (slot-major, 32 rows a
+// slot), so one bulk prefetch covers each: values at 256 B (FP64) / 128 B
+// (FP32) and columns at 64 B boundaries, sizes multiples of 64 B -- both
+// within cp.async.bulk's 16-byte rule.
+template <typename I, typename V>
+__device__ __forceinline__ void prefetch_slice_ahead(int pf, const int *sptr, const I *cols,
+                                                     const V *vals, int s, int s1) {
+  if (pf <= 0 || (threadIdx.x & 31) != 0) return;
+  const int t = s + pf * static_cast<int>(blockDim.x >> 5);
+  if (t >= s1) return;
+  const int b = __ldg(sptr + t);
+  const int e = __ldg(sptr + t + 1);
+  if (e <= b) return;
+  const unsigned nv = static_cast<unsigned>(e - b) * sizeof(V);
+  const unsigned nc = static_cast<unsigned>(e - b) * sizeof(I);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(vals + b), "r"(nv) : "memory");
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(cols + b), "r"(nc) : "memory");
+}
+
+// A warp's slices s0 + warp, s0 + warp + warps, ... (< s1) of a K-vector
+// SpMV phase, with the loads of each slice ordered for latency: the next
+// slice's extent is read one slice ahead, and every load that does not
+// depend on a column index -- the row's own operands of the phase (pre(k,
+// row), e.g. r and r0 for a dot), the diagonal and each vector at the row --
+// is issued with the slot columns and values, before the first gather.  A
+// slice then costs two dependent memory round trips (columns, then gathers)
+// instead of four.  The arithmetic is row_product_t's: diagonal product
+// first, then each slot's product in order.  post(k, row, y_k, pre_k) runs
+// for each active k of every row below n.  pf: prefetch_slice_ahead's
+// distance (0: off).
+template <int K, typename Acc, bool kExact, typename V, typename DV, typename I, typename G,
+          typename Pre, typename Post>
+__device__ __forceinline__ void slice_rows(int n, const int *sptr, const I *colp,
+                                           const V *valp, const DV *const *diagp, int s0,
+                                           int s1, int pf, const int (&act)[K], G g, Pre pre,
+                                           Post post) {
+  using E = decltype(pre(0, 0));
+  const int lane = threadIdx.x & 31;
+  const int step = static_cast<int>(blockDim.x >> 5);
+  int s = s0 + static_cast<int>(threadIdx.x >> 5);
+  if (s >= s1) return;
+  int base = __ldg(sptr + s), end = __ldg(sptr + s + 1);
+  for (; s < s1; s += step) {
+    prefetch_slice_ahead(pf, sptr, colp, valp, s, s1);
+    const int row = s * kWarp + lane;
+    int nbase = 0, nend = 0;
+    if (s + step < s1) {
+      nbase = __ldg(sptr + s + step);
+      nend = __ldg(sptr + s + step + 1);
+    }
+    if (row < n) {
+      E ex[K];
+      Acc y[K], dv[K], gv[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) {
+          ex[k] = pre(k, row);
+          dv[k] = static_cast<Acc>(ld_vec(diagp[k] + row));
+          gv[k] = static_cast<Acc>(g(k, row));
+        }
+      const int w = (end - base) >> 5;
+      const I *c = colp + base + lane;
+      const V *v = valp + base + lane;
+      int jj[6];
+      Acc vv[6];
+#pragma unroll
+      for (int u = 0; u < 6; ++u)
+        if (u < w) {
+          jj[u] = slot_col(c, u * kWarp, row);
+          vv[u] = static_cast<Acc>(ld_stream(v + u * kWarp));
+        }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) y[k] = kExact ? xmul(dv[k], gv[k]) : dv[k] * gv[k];
+      for (int e0 = 0; e0 < w; e0 += 6) {
+        if (e0 > 0) {
+#pragma unroll
+          for (int u = 0; u < 6; ++u)
+            if (e0 + u < w) {
+              jj[u] = slot_col(c, (e0 + u) * kWarp, row);
+              vv[u] = static_cast<Acc>(ld_stream(v + (e0 + u) * kWarp));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 6; ++u)
+          if (e0 + u < w) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (act[k]) {
+                const Acc t = static_cast<Acc>(g(k, jj[u]));
+                y[k] = kExact ? xadd(y[k], xmul(vv[u], t)) : fma(vv[u], t, y[k]);
+              }
+          }
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) post(k, row, y[k], ex[k]);
+    }
+    base = nbase;
+    end = nend;
+  }
+}
+
+// Two operands of a row, the usual pre() result of slice_rows.
+template <typename T>
+struct RowPair {
+  T a, b;
+};
+
 template <int K, bool kExact, typename V, typename G, typename I = int>
 __device__ __forceinline__ void row_product(const int *sptr, const I *colp, const V *valp,
                                             const V *const *diagp, int s, int lane,

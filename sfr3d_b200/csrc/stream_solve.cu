@@ -38,6 +38,23 @@ namespace {
 
 constexpr int kCounters = 16;
 
+// The iteration's SpMV phases (k_pcg_a, k_bicg_a1, k_bicg_a2) trade a
+// warp's loads in flight against warps resident.  slice_rows issues every
+// load of a slice that does not depend on a column before the first gather
+// (two dependent round trips a slice); it pays for that in registers.
+// Measured at 128^3 (momentum K = 3, Poisson K = 1):
+//   K = 1: slice_rows, uncapped (the three-kernel PCG 125.0 ms against
+//          130.5 ms with row_product);
+//   K > 1, FP32 operator: slice_rows capped at 4 blocks of 256 an SM
+//          (64 registers; BiCGSTAB 4.67 ms against 5.16 ms);
+//   K > 1, FP64: row_product (5.40 ms; slice_rows needs 97 registers and
+//          ran 6.52 ms uncapped, 5.91 ms capped at 3 blocks, 7.23 ms at 4).
+template <int K, bool kMixed>
+struct SpmvShape {
+  static constexpr bool kSliceRows = K == 1 || kMixed;
+  static constexpr int kMinBlocks = (K > 1 && kMixed) ? 4 : 0;  // 0: no cap
+};
+
 template <int K>
 struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   int n, nslices, npairs;
@@ -94,28 +111,6 @@ __device__ __forceinline__ float2 ld2ro(const float *p) { return *reinterpret_ca
 __device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
 
-
-// L2 prefetch for an iteration's SpMV phase: lane 0 of each warp asks for
-// the slice the warp reaches `pf` rounds later (a round: every warp of the
-// block one slice further), within the block's own slices.  A slice's slot
-// columns and values are each one contiguous run (slot-major, 32 rows a
-// slot), so one bulk prefetch covers each: values at 256 B (FP64) / 128 B
-// (FP32) and columns at 64 B boundaries, sizes multiples of 64 B -- both
-// within cp.async.bulk's 16-byte rule.
-template <typename I, typename V>
-__device__ __forceinline__ void prefetch_slice_ahead(int pf, const int *sptr, const I *cols,
-                                                     const V *vals, int s, int s1) {
-  if (pf <= 0 || (threadIdx.x & 31) != 0) return;
-  const int t = s + pf * static_cast<int>(blockDim.x >> 5);
-  if (t >= s1) return;
-  const int b = __ldg(sptr + t);
-  const int e = __ldg(sptr + t + 1);
-  if (e <= b) return;
-  const unsigned nv = static_cast<unsigned>(e - b) * sizeof(V);
-  const unsigned nc = static_cast<unsigned>(e - b) * sizeof(I);
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(vals + b), "r"(nv) : "memory");
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(cols + b), "r"(nc) : "memory");
-}
 
 template <int K>
 __device__ __forceinline__ void load_active(const SState<K> *st, int (&act)[K]) {
@@ -231,7 +226,7 @@ __global__ void __launch_bounds__(256) k_pcg_start(const SArgs<K> a, SState<K> *
 
 // phase A: q = A p, (q, p)  (Cg.c:105-109)
 template <int K, bool kMixed, typename I>
-__global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) {
+__global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_pcg_a(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(K);
   if (!st->any) return;
   const int n = a.n;
@@ -244,7 +239,7 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) acc[k] = 0.0;
-  if (!kMixed) {
+  if (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
     SFR_FOR_OWN_ROWS(s0, s1) {
       prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
@@ -257,22 +252,25 @@ __global__ void __launch_bounds__(256) k_pcg_a(const SArgs<K> a, SState<K> *st) 
         acc[k] += y[k] * ld_ro(a.p0[k] + row_);
       }
     }
+  } else if (!kMixed) {
+    slice_rows<K, double, true, double, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.p0[k] + c); },
+        [&](int k, int row) { return ld_ro(a.p0[k] + row); },
+        [&](int k, int row, double y, double pk) {
+          st_vec(a.q[k] + row, y);
+          acc[k] += y * pk;
+        });
   } else {
-    const double *const *dc = a.dc;
-    SFR_FOR_OWN_ROWS(s0, s1) {
-      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
-      double y[K];
-      row_product_t<K, double, false, float, double>(
-          a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
-          [&](int k, int c) { return ld_ro(a.fp0[k] + c); }, y);
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (!act[k]) continue;
-        const float yf = __double2float_rn(y[k]);
-        st_vec(a.fq[k] + row_, yf);
-        acc[k] += static_cast<double>(yf) * static_cast<double>(ld_ro(a.fp0[k] + row_));
-      }
-    }
+    slice_rows<K, double, false, float, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.fp0[k] + c); },
+        [&](int k, int row) { return ld_ro(a.fp0[k] + row); },
+        [&](int k, int row, double y, float pk) {
+          const float yf = __double2float_rn(y);
+          st_vec(a.fq[k] + row, yf);
+          acc[k] += static_cast<double>(yf) * static_cast<double>(pk);
+        });
   }
   if (!last_block<K>(acc, a.part, a.counter + 2, sm)) return;
   if (threadIdx.x == 0) {
@@ -846,7 +844,7 @@ __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> 
 
 // A1: v = A z ; rr0 = (r, r0) ; alpha = rr0 / (v, r0)
 template <int K, bool kMixed, typename I>
-__global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st) {
+__global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bicg_a1(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
   const int n = a.n;
@@ -858,8 +856,8 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    if (!kMixed) {
+  if (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
+    SFR_FOR_OWN_ROWS(s0, s1) {
       prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
@@ -872,28 +870,32 @@ __global__ void __launch_bounds__(256) k_bicg_a1(const SArgs<K> a, SState<K> *st
         acc[2 * k] += ld_ro(a.r[k] + row_) * r0k;
         acc[2 * k + 1] += y[k] * r0k;
       }
-    } else {
-      // FP32 accumulation: the momentum systems BiCGSTAB serves are
-      // diagonally dominant, and FP64 accumulation of K right-hand sides
-      // costs two FP32 -> FP64 conversions a slot and right-hand side (the
-      // SpMV phase then ran slower than the FP64 one)
-      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
-      float y[K];
-      {
-        const double *const *dc = a.dc;
-        row_product_t<K, float, false, float, double>(
-            a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
-            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (!act[k]) continue;
-        st_vec(a.fq[k] + row_, y[k]);
-        const double r0k = ld_ro(a.fr0[k] + row_);
-        acc[2 * k] += static_cast<double>(ld_ro(a.fr[k] + row_)) * r0k;
-        acc[2 * k + 1] += static_cast<double>(y[k]) * r0k;
-      }
     }
+  } else if (!kMixed) {
+    slice_rows<K, double, true, double, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.z[k] + c); },
+        [&](int k, int row) { return RowPair<double>{ld_ro(a.r[k] + row), ld_ro(a.r0[k] + row)}; },
+        [&](int k, int row, double y, RowPair<double> e) {
+          st_vec(a.q[k] + row, y);
+          acc[2 * k] += e.a * e.b;
+          acc[2 * k + 1] += y * e.b;
+        });
+  } else {
+    // FP32 accumulation: the momentum systems BiCGSTAB serves are
+    // diagonally dominant, and FP64 accumulation of K right-hand sides
+    // costs two FP32 -> FP64 conversions a slot and right-hand side (the
+    // SpMV phase then ran slower than the FP64 one)
+    slice_rows<K, float, false, float, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.fz[k] + c); },
+        [&](int k, int row) { return RowPair<float>{ld_ro(a.fr[k] + row), ld_ro(a.fr0[k] + row)}; },
+        [&](int k, int row, float y, RowPair<float> e) {
+          st_vec(a.fq[k] + row, y);
+          const double r0k = e.b;
+          acc[2 * k] += static_cast<double>(e.a) * r0k;
+          acc[2 * k + 1] += static_cast<double>(y) * r0k;
+        });
   }
   if (!last_block<2 * K>(acc, a.part, a.counter + 2, sm)) return;
   if (threadIdx.x == 0) {
@@ -1055,7 +1057,7 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
 
 // A2: t = A z ; w = (t, s) / (t, t)
 template <int K, bool kMixed, typename I>
-__global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st) {
+__global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bicg_a2(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
   const int n = a.n;
@@ -1067,8 +1069,8 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    if (!kMixed) {
+  if (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
+    SFR_FOR_OWN_ROWS(s0, s1) {
       prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
@@ -1080,27 +1082,28 @@ __global__ void __launch_bounds__(256) k_bicg_a2(const SArgs<K> a, SState<K> *st
         acc[2 * k] += y[k] * ld_ro(a.r[k] + row_);
         acc[2 * k + 1] += y[k] * y[k];
       }
-    } else {
-      // FP32 accumulation: the momentum systems BiCGSTAB serves are
-      // diagonally dominant, and FP64 accumulation of K right-hand sides
-      // costs two FP32 -> FP64 conversions a slot and right-hand side (the
-      // SpMV phase then ran slower than the FP64 one)
-      prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val32, s_, s1);
-      float y[K];
-      {
-        const double *const *dc = a.dc;
-        row_product_t<K, float, false, float, double>(
-            a.sptr, cols_of<I>(a.cols), a.val32, dc, s_, lane, act,
-            [&](int k, int c) { return ld_ro(a.fz[k] + c); }, y);
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (!act[k]) continue;
-        st_vec(a.ft[k] + row_, y[k]);
-        acc[2 * k] += static_cast<double>(y[k]) * static_cast<double>(ld_ro(a.fr[k] + row_));
-        acc[2 * k + 1] += static_cast<double>(y[k]) * static_cast<double>(y[k]);
-      }
     }
+  } else if (!kMixed) {
+    slice_rows<K, double, true, double, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.z[k] + c); },
+        [&](int k, int row) { return ld_ro(a.r[k] + row); },
+        [&](int k, int row, double y, double rk) {
+          st_vec(a.t[k] + row, y);
+          acc[2 * k] += y * rk;
+          acc[2 * k + 1] += y * y;
+        });
+  } else {
+    // FP32 accumulation, as in phase A1
+    slice_rows<K, float, false, float, double, I>(
+        n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.pf, act,
+        [&](int k, int c) { return ld_ro(a.fz[k] + c); },
+        [&](int k, int row) { return ld_ro(a.fr[k] + row); },
+        [&](int k, int row, float y, float rk) {
+          st_vec(a.ft[k] + row, y);
+          acc[2 * k] += static_cast<double>(y) * static_cast<double>(rk);
+          acc[2 * k + 1] += static_cast<double>(y) * static_cast<double>(y);
+        });
   }
   if (!last_block<2 * K>(acc, a.part, a.counter + 5, sm)) return;
   if (threadIdx.x == 0) {
