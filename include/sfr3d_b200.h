@@ -171,6 +171,16 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
  * other values are SFR_BAD_INPUT. */
 int sfr_gpu_set_fused(sfr_system *s, int32_t mode);
 
+/* Graph engine, BiCGSTAB: 1 stages each warp's SELL slices (slot values and
+ * columns) in shared memory with bulk copies issued three slices ahead, so
+ * the SpMV phases wait on memory only for their gathers; it applies when the
+ * columns fit 16-bit offsets and no slice is wider than 8 slots.  0 (the
+ * default) reads the slices from global memory: on the 128^3 momentum
+ * systems staging measured even with FP32 values and slower with FP64 (the
+ * staged FP64 phases need more registers, so fewer blocks fit an SM).  The
+ * arithmetic is the same either way.  Other values are SFR_BAD_INPUT. */
+int sfr_gpu_set_staging(sfr_system *s, int32_t flag);
+
 /* Result of sfr_gpu_autotune. */
 typedef struct {
   int32_t engine;           /* chosen engine: 1 persistent, 2 graph, 4 resident */

@@ -394,6 +394,12 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds) {
   return SFR_OK;
 }
 
+int sfr_gpu_set_staging(sfr_system *s, int32_t flag) {
+  if (!s || flag < 0 || flag > 1) return SFR_BAD_INPUT;
+  s->graph_stage = flag;
+  return SFR_OK;
+}
+
 int sfr_gpu_set_fused(sfr_system *s, int32_t flag) {
   if (!s) return SFR_BAD_INPUT;
   if (flag < 0 || flag > 3) return SFR_BAD_INPUT;

@@ -365,6 +365,176 @@ __device__ __forceinline__ void slice_rows(int n, const int *sptr, const I *colp
   }
 }
 
+// ----------------------------------------------------------------------
+// Slices staged in shared memory by the bulk-copy (TMA) engine.
+//
+// A slice's slot values and slot columns are each one contiguous run
+// (slot-major, 32 rows a slot) that starts at sptr[s], a multiple of 32
+// elements: 128 B for FP32 values, 256 B for FP64, 64 B for 16-bit columns,
+// so both copies start and end on 16-byte boundaries as cp.async.bulk
+// requires (the arrays themselves are cudaMalloc'd, 256-byte aligned).
+// Each warp owns kStages stage buffers with one mbarrier each; lane 0
+// copies the warp's slice kStages slices ahead into a free stage, and the
+// warp reads the slice from shared memory once that stage's mbarrier phase
+// completes.  The matrix stream then runs behind the warp's arithmetic, and
+// only the gathers wait on memory.  No multicast, no tensor map.
+// ----------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// Order this thread's mbarrier inits and generic-proxy accesses of shared
+// memory before later async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes,
+                                              uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Column of a staged slot (shared memory): absolute, or row + offset.
+__device__ __forceinline__ int smem_col(const int *c, int k, int) { return c[k]; }
+__device__ __forceinline__ int smem_col(const int16_t *c, int k, int row) {
+  return row + static_cast<int>(c[k]);
+}
+
+// Bytes of one warp's stages: kStages mbarriers (padded to 16 bytes), then
+// kStages value buffers, then kStages column buffers of `cap` slots each
+// (cap a multiple of 32).
+template <typename V, typename I, int kStages>
+__host__ __device__ constexpr int staged_warp_bytes(int cap) {
+  return ((kStages * 8 + 15) / 16) * 16 + kStages * cap * static_cast<int>(sizeof(V) + sizeof(I));
+}
+
+// slice_rows with the slices staged in shared memory (`smem`: the block's
+// dynamic shared memory, staged_warp_bytes per warp; cap: slots a stage
+// holds, at least the widest slice's).  The same arithmetic, rows and
+// post() calls as slice_rows.  A stage whose copy has not landed after
+// `spin_limit` polls sets *err to SFR_TIMEOUT and the warp goes on (its
+// results are then meaningless and the caller reports the error).
+template <int K, typename Acc, bool kExact, typename V, typename DV, typename I, int kStages,
+          typename G, typename Pre, typename Post>
+__device__ __forceinline__ void slice_rows_staged(int n, const int *sptr, const I *colp,
+                                                  const V *valp, const DV *const *diagp, int s0,
+                                                  int s1, int cap, char *smem, int *err,
+                                                  const int (&act)[K], G g, Pre pre,
+                                                  Post post) {
+  using E = decltype(pre(0, 0));
+  constexpr unsigned kSpinLimit = 1u << 24;
+  const int lane = threadIdx.x & 31;
+  const int warp = static_cast<int>(threadIdx.x >> 5);
+  const int step = static_cast<int>(blockDim.x >> 5);
+  char *base = smem + static_cast<size_t>(warp) * staged_warp_bytes<V, I, kStages>(cap);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base);
+  V *vs = reinterpret_cast<V *>(base + ((kStages * 8 + 15) / 16) * 16);
+  I *cs = reinterpret_cast<I *>(vs + kStages * cap);
+  const int first = s0 + warp;
+  if (first >= s1) return;
+  // lane 0: one slice into stage `stg`
+  auto issue = [&](int s, int stg) {
+    const int b = __ldg(sptr + s);
+    const unsigned cnt = static_cast<unsigned>(__ldg(sptr + s + 1) - b);
+    mbar_arrive_expect_tx(bar + stg, cnt * static_cast<unsigned>(sizeof(V) + sizeof(I)));
+    if (cnt > 0) {
+      bulk_copy_g2s(vs + stg * cap, valp + b, cnt * static_cast<unsigned>(sizeof(V)), bar + stg);
+      bulk_copy_g2s(cs + stg * cap, colp + b, cnt * static_cast<unsigned>(sizeof(I)), bar + stg);
+    }
+  };
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < kStages; ++q) mbar_init(bar + q, 1);
+    fence_proxy_async_smem();
+#pragma unroll
+    for (int q = 0; q < kStages; ++q)
+      if (first + q * step < s1) issue(first + q * step, q);
+  }
+  __syncwarp();
+  int i = 0;
+  for (int s = first; s < s1; s += step, ++i) {
+    const int stg = i % kStages;
+    const unsigned parity = static_cast<unsigned>(i / kStages) & 1u;
+    const int row = s * kWarp + lane;
+    const int w = (__ldg(sptr + s + 1) - __ldg(sptr + s)) >> 5;
+    E ex[K];
+    Acc dv[K], gv[K];
+    if (row < n) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) {
+          ex[k] = pre(k, row);
+          dv[k] = static_cast<Acc>(ld_vec(diagp[k] + row));
+          gv[k] = static_cast<Acc>(g(k, row));
+        }
+    }
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar + stg, parity)) {
+      if (++spins > kSpinLimit) {
+        atomicCAS(err, 0, SFR_TIMEOUT);
+        break;
+      }
+    }
+    if (row < n) {
+      const I *c = cs + stg * cap + lane;
+      const V *v = vs + stg * cap + lane;
+      Acc y[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) y[k] = kExact ? xmul(dv[k], gv[k]) : dv[k] * gv[k];
+      for (int e0 = 0; e0 < w; e0 += 6) {
+        int jj[6];
+        Acc vv[6];
+#pragma unroll
+        for (int u = 0; u < 6; ++u)
+          if (e0 + u < w) {
+            jj[u] = smem_col(c, (e0 + u) * kWarp, row);
+            vv[u] = static_cast<Acc>(v[(e0 + u) * kWarp]);
+          }
+#pragma unroll
+        for (int u = 0; u < 6; ++u)
+          if (e0 + u < w) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              if (act[k]) {
+                const Acc t = static_cast<Acc>(g(k, jj[u]));
+                y[k] = kExact ? xadd(y[k], xmul(vv[u], t)) : fma(vv[u], t, y[k]);
+              }
+          }
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (act[k]) post(k, row, y[k], ex[k]);
+    }
+    __syncwarp();  // every lane is done with stage stg
+    if (lane == 0 && s + kStages * step < s1) {
+      fence_proxy_async_smem();
+      issue(s + kStages * step, stg);
+    }
+  }
+}
+
 // Two operands of a row, the usual pre() result of slice_rows.
 template <typename T>
 struct RowPair {

@@ -76,6 +76,7 @@ int upload_sell(const HostSell &h, DevSell *d, int64_t *bytes) {
   d->n = h.n;
   d->nslices = h.nslices;
   d->nslots = h.sptr.empty() ? 0 : h.sptr.back();
+  d->max_width = h.max_width;
   if (upload(&d->sptr, h.sptr, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
   if (upload(&d->col, h.col, bytes) != cudaSuccess) return SFR_CUDA_ERROR;
   if (upload(&d->src, h.src, bytes) != cudaSuccess) return SFR_CUDA_ERROR;

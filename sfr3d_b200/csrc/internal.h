@@ -43,6 +43,7 @@ struct DevSell {
                            // bandwidth exceeds 32767
   double *val = nullptr;  // FP64 values
   float *val32 = nullptr; // FP32 copy (mixed precision)
+  int32_t max_width = 0;  // slots of the widest slice
 };
 
 struct SolveOut;  // device-side result record (krylov.cu)
@@ -103,6 +104,7 @@ struct sfr_system {
   int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
   int32_t graph_pf = 0;          // SpMV-phase L2 prefetch distance (rounds); 0: off
   int32_t graph_fused = 0;       // FP64 PCG, one RHS: one cooperative kernel an iteration
+  int32_t graph_stage = 0;       // BiCGSTAB SpMV phases: slices staged in shared memory
   std::vector<sfr::Tuned> tuned; // autotuned choices, used when engine == 0
   int64_t bytes = 0;
 };

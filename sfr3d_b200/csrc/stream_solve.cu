@@ -78,6 +78,11 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   // SpMV phases of the iteration: a warp prefetches into L2 the slice it
   // reaches `pf` rounds later (0: off)
   int pf;
+  // BiCGSTAB's SpMV phases with the slices staged in shared memory by bulk
+  // copies (kernels instantiated with kStages > 0): slots a stage holds, and
+  // the word a stage wait that gave up sets
+  int stage_cap;
+  int *stage_err;
 };
 
 
@@ -787,6 +792,7 @@ __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
       o.refinements = st->refine[k];
       o.inner_iters = st->iters[k];
       o.team_ms = 0.0;
+      if (a.stage_err && *a.stage_err != 0) o.status = SFR_TIMEOUT;  // a stage wait gave up
       st->out[k] = o;
     }
   }
@@ -843,7 +849,7 @@ __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> 
 }
 
 // A1: v = A z ; rr0 = (r, r0) ; alpha = rr0 / (v, r0)
-template <int K, bool kMixed, typename I>
+template <int K, bool kMixed, typename I, int kStages = 0>
 __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bicg_a1(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
@@ -856,12 +862,45 @@ __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bic
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  if (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
+  auto g64 = [&](int k, int c) { return ld_ro(a.z[k] + c); };
+  auto pre64 = [&](int k, int row) {
+    return RowPair<double>{ld_ro(a.r[k] + row), ld_ro(a.r0[k] + row)};
+  };
+  auto post64 = [&](int k, int row, double y, RowPair<double> e) {
+    st_vec(a.q[k] + row, y);
+    acc[2 * k] += e.a * e.b;
+    acc[2 * k + 1] += y * e.b;
+  };
+  // FP32 accumulation: the momentum systems BiCGSTAB serves are diagonally
+  // dominant, and FP64 accumulation of K right-hand sides costs two FP32 ->
+  // FP64 conversions a slot and right-hand side (the SpMV phase then ran
+  // slower than the FP64 one)
+  auto g32 = [&](int k, int c) { return ld_ro(a.fz[k] + c); };
+  auto pre32 = [&](int k, int row) {
+    return RowPair<float>{ld_ro(a.fr[k] + row), ld_ro(a.fr0[k] + row)};
+  };
+  auto post32 = [&](int k, int row, float y, RowPair<float> e) {
+    st_vec(a.fq[k] + row, y);
+    const double r0k = e.b;
+    acc[2 * k] += static_cast<double>(e.a) * r0k;
+    acc[2 * k + 1] += static_cast<double>(y) * r0k;
+  };
+  if constexpr (kStages > 0) {
+    extern __shared__ __align__(16) char stage_smem[];
+    if constexpr (!kMixed)
+      slice_rows_staged<K, double, true, double, double, I, kStages>(
+          n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.stage_cap, stage_smem,
+          a.stage_err, act, g64, pre64, post64);
+    else
+      slice_rows_staged<K, float, false, float, double, I, kStages>(
+          n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.stage_cap, stage_smem,
+          a.stage_err, act, g32, pre32, post32);
+  } else if constexpr (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
     SFR_FOR_OWN_ROWS(s0, s1) {
       prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
-                                   [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
+                                   g64, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -871,31 +910,13 @@ __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bic
         acc[2 * k + 1] += y[k] * r0k;
       }
     }
-  } else if (!kMixed) {
-    slice_rows<K, double, true, double, double, I>(
-        n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.pf, act,
-        [&](int k, int c) { return ld_ro(a.z[k] + c); },
-        [&](int k, int row) { return RowPair<double>{ld_ro(a.r[k] + row), ld_ro(a.r0[k] + row)}; },
-        [&](int k, int row, double y, RowPair<double> e) {
-          st_vec(a.q[k] + row, y);
-          acc[2 * k] += e.a * e.b;
-          acc[2 * k + 1] += y * e.b;
-        });
+  } else if constexpr (!kMixed) {
+    slice_rows<K, double, true, double, double, I>(n, a.sptr, cols_of<I>(a.cols), a.val64,
+                                                   a.diag64, s0, s1, a.pf, act, g64, pre64,
+                                                   post64);
   } else {
-    // FP32 accumulation: the momentum systems BiCGSTAB serves are
-    // diagonally dominant, and FP64 accumulation of K right-hand sides
-    // costs two FP32 -> FP64 conversions a slot and right-hand side (the
-    // SpMV phase then ran slower than the FP64 one)
-    slice_rows<K, float, false, float, double, I>(
-        n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.pf, act,
-        [&](int k, int c) { return ld_ro(a.fz[k] + c); },
-        [&](int k, int row) { return RowPair<float>{ld_ro(a.fr[k] + row), ld_ro(a.fr0[k] + row)}; },
-        [&](int k, int row, float y, RowPair<float> e) {
-          st_vec(a.fq[k] + row, y);
-          const double r0k = e.b;
-          acc[2 * k] += static_cast<double>(e.a) * r0k;
-          acc[2 * k + 1] += static_cast<double>(y) * r0k;
-        });
+    slice_rows<K, float, false, float, double, I>(n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc,
+                                                  s0, s1, a.pf, act, g32, pre32, post32);
   }
   if (!last_block<2 * K>(acc, a.part, a.counter + 2, sm)) return;
   if (threadIdx.x == 0) {
@@ -1056,7 +1077,7 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
 }
 
 // A2: t = A z ; w = (t, s) / (t, t)
-template <int K, bool kMixed, typename I>
+template <int K, bool kMixed, typename I, int kStages = 0>
 __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bicg_a2(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   if (!st->any) return;
@@ -1069,12 +1090,37 @@ __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bic
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  if (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
+  auto g64 = [&](int k, int c) { return ld_ro(a.z[k] + c); };
+  auto pre64 = [&](int k, int row) { return ld_ro(a.r[k] + row); };
+  auto post64 = [&](int k, int row, double y, double rk) {
+    st_vec(a.t[k] + row, y);
+    acc[2 * k] += y * rk;
+    acc[2 * k + 1] += y * y;
+  };
+  // FP32 accumulation, as in phase A1
+  auto g32 = [&](int k, int c) { return ld_ro(a.fz[k] + c); };
+  auto pre32 = [&](int k, int row) { return ld_ro(a.fr[k] + row); };
+  auto post32 = [&](int k, int row, float y, float rk) {
+    st_vec(a.ft[k] + row, y);
+    acc[2 * k] += static_cast<double>(y) * static_cast<double>(rk);
+    acc[2 * k + 1] += static_cast<double>(y) * static_cast<double>(y);
+  };
+  if constexpr (kStages > 0) {
+    extern __shared__ __align__(16) char stage_smem[];
+    if constexpr (!kMixed)
+      slice_rows_staged<K, double, true, double, double, I, kStages>(
+          n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.stage_cap, stage_smem,
+          a.stage_err, act, g64, pre64, post64);
+    else
+      slice_rows_staged<K, float, false, float, double, I, kStages>(
+          n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.stage_cap, stage_smem,
+          a.stage_err, act, g32, pre32, post32);
+  } else if constexpr (!kMixed && !SpmvShape<K, kMixed>::kSliceRows) {
     SFR_FOR_OWN_ROWS(s0, s1) {
       prefetch_slice_ahead(a.pf, a.sptr, cols_of<I>(a.cols), a.val64, s_, s1);
       double y[K];
       row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, act,
-                                   [&](int k, int c) { return ld_ro(a.z[k] + c); }, y);
+                                   g64, y);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!act[k]) continue;
@@ -1083,27 +1129,13 @@ __global__ void __launch_bounds__(256, (SpmvShape<K, kMixed>::kMinBlocks)) k_bic
         acc[2 * k + 1] += y[k] * y[k];
       }
     }
-  } else if (!kMixed) {
-    slice_rows<K, double, true, double, double, I>(
-        n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, a.pf, act,
-        [&](int k, int c) { return ld_ro(a.z[k] + c); },
-        [&](int k, int row) { return ld_ro(a.r[k] + row); },
-        [&](int k, int row, double y, double rk) {
-          st_vec(a.t[k] + row, y);
-          acc[2 * k] += y * rk;
-          acc[2 * k + 1] += y * y;
-        });
+  } else if constexpr (!kMixed) {
+    slice_rows<K, double, true, double, double, I>(n, a.sptr, cols_of<I>(a.cols), a.val64,
+                                                   a.diag64, s0, s1, a.pf, act, g64, pre64,
+                                                   post64);
   } else {
-    // FP32 accumulation, as in phase A1
-    slice_rows<K, float, false, float, double, I>(
-        n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc, s0, s1, a.pf, act,
-        [&](int k, int c) { return ld_ro(a.fz[k] + c); },
-        [&](int k, int row) { return ld_ro(a.fr[k] + row); },
-        [&](int k, int row, float y, float rk) {
-          st_vec(a.ft[k] + row, y);
-          acc[2 * k] += static_cast<double>(y) * static_cast<double>(rk);
-          acc[2 * k + 1] += static_cast<double>(y) * static_cast<double>(y);
-        });
+    slice_rows<K, float, false, float, double, I>(n, a.sptr, cols_of<I>(a.cols), a.val32, a.dc,
+                                                  s0, s1, a.pf, act, g32, pre32, post32);
   }
   if (!last_block<2 * K>(acc, a.part, a.counter + 5, sm)) return;
   if (threadIdx.x == 0) {
@@ -1259,9 +1291,11 @@ struct GraphKey {
   int shared_diag;  // the K right-hand sides share one diagonal
   int pf;           // SpMV-phase L2 prefetch distance
   int fused;        // FP64 PCG, one right-hand side: one cooperative kernel an iteration
+  int staged;       // BiCGSTAB: SpMV phases with slices staged in shared memory
   bool operator<(const GraphKey &o) const {
-    return std::tie(solver, k, precision, threads, spw, shared_diag, pf, fused) <
-           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag, o.pf, o.fused);
+    return std::tie(solver, k, precision, threads, spw, shared_diag, pf, fused, staged) <
+           std::tie(o.solver, o.k, o.precision, o.threads, o.spw, o.shared_diag, o.pf, o.fused,
+                    o.staged);
   }
 };
 
@@ -1277,9 +1311,12 @@ struct CachedGraph {
   std::vector<char> args;   // SArgs<K> (host copy, also baked into the nodes)
   cudaGraphConditionalHandle hwhile = 0, hif = 0, hif2 = 0;
   int grid_s = 0, grid_v = 0, threads = 256;
+  int grid_o = 0;        // once-a-solve and refresh kernels: one wave of their own
   int grid_f = 0;        // fused iteration: co-resident blocks
   size_t smem_f = 0;     // fused iteration: dynamic shared memory a block
   unsigned long long *tagw = nullptr;  // fused mode 3: the broadcast word
+  bool staged = false;   // BiCGSTAB SpMV phases staged through shared memory
+  size_t smem_s = 0;     // their dynamic shared memory a block
   uint64_t last_use = 0;
   int64_t bytes = 0;
 };
@@ -1292,12 +1329,12 @@ std::map<const sfr_system *, EngineCache> g_engines;
 constexpr size_t kMaxGraphsPerSystem = 4;
 
 cudaError_t add_kernel(cudaGraph_t g, cudaGraphNode_t *prev, void *func, int grid, int threads,
-                       void **params) {
+                       void **params, size_t smem = 0) {
   cudaKernelNodeParams p{};
   p.func = func;
   p.gridDim = dim3(grid);
   p.blockDim = dim3(threads);
-  p.sharedMemBytes = 0;
+  p.sharedMemBytes = static_cast<unsigned>(smem);
   p.kernelParams = params;
   cudaGraphNode_t node;
   cudaError_t e = cudaGraphAddKernelNode(&node, g, *prev ? prev : nullptr, *prev ? 1 : 0, &p);
@@ -1332,16 +1369,39 @@ constexpr int kVecs32 = 10;       // (unused) m32 r z q p0 p1 xs r0 t
 
 inline int64_t padded(int n) { return (static_cast<int64_t>(n) + 3) & ~static_cast<int64_t>(3); }
 
-// Allocate the graph's workspace and fill its by-value arguments.
+// Stages a warp keeps in flight when BiCGSTAB's SpMV phases stage their
+// slices through shared memory, and the widest slice (slots) they take.
+constexpr int kStageDepth = 3;
+constexpr int kStageMaxWidth = 8;
+
+// BiCGSTAB's SpMV-phase kernels (A1, A2) of a graph.
+template <int K, typename I>
+void bicg_spmv_kernels(bool mixed, bool staged, const void **a1, const void **a2) {
+  if constexpr (std::is_same<I, int16_t>::value) {
+    if (staged) {
+      *a1 = mixed ? (const void *)k_bicg_a1<K, true, I, kStageDepth>
+                  : (const void *)k_bicg_a1<K, false, I, kStageDepth>;
+      *a2 = mixed ? (const void *)k_bicg_a2<K, true, I, kStageDepth>
+                  : (const void *)k_bicg_a2<K, false, I, kStageDepth>;
+      return;
+    }
+  }
+  *a1 = mixed ? (const void *)k_bicg_a1<K, true, I> : (const void *)k_bicg_a1<K, false, I>;
+  *a2 = mixed ? (const void *)k_bicg_a2<K, true, I> : (const void *)k_bicg_a2<K, false, I>;
+}
+
 // Blocks of the iteration's SpMV kernel that fit on the GPU at once.
 template <int K, typename I>
-int resident_blocks(sfr_system *s, int solver, bool mixed, int threads) {
-  const void *kern =
-      solver == SFR_PCG
-          ? (mixed ? (const void *)k_pcg_a<K, true, I> : (const void *)k_pcg_a<K, false, I>)
-          : (mixed ? (const void *)k_bicg_a1<K, true, I> : (const void *)k_bicg_a1<K, false, I>);
+int resident_blocks(sfr_system *s, int solver, bool mixed, int threads, bool staged,
+                    size_t smem) {
+  const void *kern = nullptr, *unused = nullptr;
+  if (solver == SFR_PCG)
+    kern = mixed ? (const void *)k_pcg_a<K, true, I> : (const void *)k_pcg_a<K, false, I>;
+  else
+    bicg_spmv_kernels<K, I>(mixed, staged, &kern, &unused);
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, staged ? smem : 0) !=
+          cudaSuccess ||
       occ < 1)
     occ = 1;
   return occ * std::max(1, num_sms(s->device));
@@ -1358,11 +1418,45 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
   const bool mixed = precision == SFR_MIXED;
   const int warps = threads / kWarp;
   cg->threads = threads;
+  const int cap = s->A.max_width * kWarp;
+  if (cg->staged) {
+    cg->smem_s = static_cast<size_t>(warps) *
+                 (mixed ? staged_warp_bytes<float, int16_t, kStageDepth>(cap)
+                        : staged_warp_bytes<double, int16_t, kStageDepth>(cap));
+    const void *k1 = nullptr, *k2 = nullptr;
+    bicg_spmv_kernels<K, I>(mixed, true, &k1, &k2);
+    SFR_TRY(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(cg->smem_s)));
+    SFR_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(cg->smem_s)));
+  }
   if (spw > 0)
     cg->grid_s = std::max(1, (s->A.nslices + warps * spw - 1) / (warps * spw));
   else
-    cg->grid_s = std::max(1, std::min((s->A.nslices + warps - 1) / warps,
-                                      resident_blocks<K, I>(s, solver, mixed, threads)));
+    cg->grid_s = std::max(
+        1, std::min((s->A.nslices + warps - 1) / warps,
+                    resident_blocks<K, I>(s, solver, mixed, threads, cg->staged, cg->smem_s)));
+  {
+    // start, refresh and post read the matrix like the SpMV phases but hold
+    // more registers: one wave of their own, not the SpMV phase's grid
+    const void *once[3] = {(const void *)k_post<K, I>,
+                           solver == SFR_PCG
+                               ? (mixed ? (const void *)k_pcg_start<K, true, I>
+                                        : (const void *)k_pcg_start<K, false, I>)
+                               : (mixed ? (const void *)k_bicg_start<K, true, I>
+                                        : (const void *)k_bicg_start<K, false, I>),
+                           solver == SFR_PCG ? (const void *)k_pcg_refresh<K, I>
+                                             : (const void *)k_bicg_refresh<K, I>};
+    int occ = 64;
+    for (const void *k : once) {
+      int o = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, threads, 0) != cudaSuccess || o < 1)
+        o = 1;
+      occ = std::min(occ, o);
+    }
+    cg->grid_o = spw > 0 ? cg->grid_s
+                         : std::max(1, std::min(cg->grid_s, occ * std::max(1, num_sms(s->device))));
+  }
   const int npairs = (n + 1) / 2;
   const int wave = std::max(1, num_sms(s->device)) * (2048 / threads);
   cg->grid_v = std::max(1, std::min(wave, (npairs + threads - 1) / threads));
@@ -1431,6 +1525,8 @@ cudaError_t prepare(sfr_system *s, int solver, int precision, int threads, int s
   }
   a.shared_diag = shared_diag;
   a.pf = pf;
+  a.stage_cap = cg->staged ? cap : 0;
+  a.stage_err = reinterpret_cast<int *>(cg->counter + 15);
   a.part = cg->part;
   a.counter = cg->counter;
   return cudaSuccess;
@@ -1509,7 +1605,10 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   void *pf_all[3] = {&a, &ps, &one};
   void *pr1[3] = {&a, &ps, &stage1};
   void *pr2[3] = {&a, &ps, &stage2};
-  const int gs = cg->grid_s, gv = cg->grid_v;
+  const int gs = cg->grid_s, gv = cg->grid_v, go = cg->grid_o;
+  const void *a1k = nullptr, *a2k = nullptr;
+  bicg_spmv_kernels<K, I>(mixed, cg->staged, &a1k, &a2k);
+  const size_t ssm = cg->staged ? cg->smem_s : 0;
 
   cudaGraphNode_t prev = nullptr;
   {
@@ -1540,7 +1639,7 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   if (solver == SFR_PCG) {
     if (mixed) {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, true, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, true, I>, go, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, true, I>, gs, threads, p2));
@@ -1548,12 +1647,12 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
       SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
       cudaGraphNode_t ip = nullptr;
       SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K, I>, go, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_pcg_start<K, false, I>, go, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
       if (fused && K == 1) {
@@ -1581,37 +1680,37 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   } else {
     if (mixed) {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, true, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, true, I>, go, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, true, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a1k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, true>, gv, threads, p2));
       SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
       cudaGraphNode_t ip = nullptr;
       SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K, I>, gs, threads, pr1));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, true, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K, I>, go, threads, pr1));
+      SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a2k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, true>, gv, threads, p2));
       cudaGraph_t ifbody2 = nullptr;
       SFR_TRY(add_conditional(body, &bp, cg->hif2, cudaGraphCondTypeIf, &ifbody2));
       cudaGraphNode_t ip2 = nullptr;
       SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K, I>, gs, threads, pr2));
+      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K, I>, go, threads, pr2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, false, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(g, &prev, (void *)k_bicg_start<K, false, I>, go, threads, p2));
       SFR_TRY(add_conditional(g, &prev, cg->hwhile, cudaGraphCondTypeWhile, &body));
       cudaGraphNode_t bp = nullptr;
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a1<K, false, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a1k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, false>, gv, threads, p2));
-      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_a2<K, false, I>, gs, threads, p2));
+      SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a2k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, false>, gv, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, false>, gv, threads, p2));
     }
   }
-  SFR_TRY(add_kernel(g, &prev, (void *)k_post<K, I>, gs, threads, p2));
+  SFR_TRY(add_kernel(g, &prev, (void *)k_post<K, I>, go, threads, p2));
   SFR_TRY(cudaGraphInstantiate(&cg->exec, g, 0));
   return cudaSuccess;
 }
@@ -1636,24 +1735,28 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
   SArgs<K> a = *reinterpret_cast<const SArgs<K> *>(cg->args.data());
   a.in_graph = 0;
   auto *ps = static_cast<SState<K> *>(cg->d_state);
-  const int gs = cg->grid_s, gv = cg->grid_v, t = cg->threads;
+  const int gs = cg->grid_s, gv = cg->grid_v, go = cg->grid_o, t = cg->threads;
+  const void *a1k = nullptr, *a2k = nullptr;
+  bicg_spmv_kernels<K, I>(mixed, cg->staged, &a1k, &a2k);
+  const size_t ssm = cg->staged ? cg->smem_s : 0;
+  void *pa[2] = {&a, &ps};
   SFR_TRY(cudaMemsetAsync(cg->counter, 0, sizeof(unsigned) * kCounters, st));
   if (cg->tagw) SFR_TRY(cudaMemsetAsync(cg->tagw, 0, sizeof(unsigned long long), st));
   if (solver == SFR_PCG) {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
-      k_pcg_start<K, true, I><<<gs, t, 0, st>>>(a, ps);
+      k_pcg_start<K, true, I><<<go, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
         k_pcg_a<K, true, I><<<gs, t, 0, st>>>(a, ps);
         k_pcg_b<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_pcg_refresh<K, I><<<gs, t, 0, st>>>(a, ps);
+        k_pcg_refresh<K, I><<<go, t, 0, st>>>(a, ps);
         k_pcg_c<K, true><<<gv, t, 0, st>>>(a, ps);
       }
       k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
     } else {
       k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
-      k_pcg_start<K, false, I><<<gs, t, 0, st>>>(a, ps);
+      k_pcg_start<K, false, I><<<go, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
         if constexpr (K == 1) {
           if (fused) {
@@ -1673,32 +1776,32 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
   } else {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
-      k_bicg_start<K, true, I><<<gs, t, 0, st>>>(a, ps);
+      k_bicg_start<K, true, I><<<go, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_bicg_a1<K, true, I><<<gs, t, 0, st>>>(a, ps);
+        SFR_TRY(cudaLaunchKernel(a1k, dim3(gs), dim3(t), pa, ssm, st));
         k_bicg_b1<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_bicg_refresh<K, I><<<gs, t, 0, st>>>(a, ps, 1);
-        k_bicg_a2<K, true, I><<<gs, t, 0, st>>>(a, ps);
+        k_bicg_refresh<K, I><<<go, t, 0, st>>>(a, ps, 1);
+        SFR_TRY(cudaLaunchKernel(a2k, dim3(gs), dim3(t), pa, ssm, st));
         k_bicg_b2<K, true><<<gv, t, 0, st>>>(a, ps);
         k_fold<K><<<gv, t, 0, st>>>(a, ps, 0);
-        k_bicg_refresh<K, I><<<gs, t, 0, st>>>(a, ps, 2);
+        k_bicg_refresh<K, I><<<go, t, 0, st>>>(a, ps, 2);
         k_bicg_c<K, true><<<gv, t, 0, st>>>(a, ps);
       }
       k_fold<K><<<gv, t, 0, st>>>(a, ps, 1);
     } else {
       k_setup<K, false><<<gv, t, 0, st>>>(a, ps);
-      k_bicg_start<K, false, I><<<gs, t, 0, st>>>(a, ps);
+      k_bicg_start<K, false, I><<<go, t, 0, st>>>(a, ps);
       for (uint32_t it = 0; it < maxit; ++it) {
-        k_bicg_a1<K, false, I><<<gs, t, 0, st>>>(a, ps);
+        SFR_TRY(cudaLaunchKernel(a1k, dim3(gs), dim3(t), pa, ssm, st));
         k_bicg_b1<K, false><<<gv, t, 0, st>>>(a, ps);
-        k_bicg_a2<K, false, I><<<gs, t, 0, st>>>(a, ps);
+        SFR_TRY(cudaLaunchKernel(a2k, dim3(gs), dim3(t), pa, ssm, st));
         k_bicg_b2<K, false><<<gv, t, 0, st>>>(a, ps);
         k_bicg_c<K, false><<<gv, t, 0, st>>>(a, ps);
       }
     }
   }
-  k_post<K, I><<<gs, t, 0, st>>>(a, ps);
+  k_post<K, I><<<go, t, 0, st>>>(a, ps);
   return cudaGetLastError();
 }
 
@@ -1719,7 +1822,13 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
     grid_f = s->A.off ? fused_shape<int16_t>(s, fused, &smem_f)
                       : fused_shape<int>(s, fused, &smem_f);
   if (fused && grid_f <= 0) fused = 0;
-  GraphKey key{solver, K, precision, threads, spw, shared_diag, pf, fused};
+  // BiCGSTAB's SpMV phases stage their slices through shared memory when
+  // the columns are 16-bit offsets and no slice is wider than a stage
+  const int staged = solver != SFR_PCG && s->graph_stage && s->A.off &&
+                             s->A.max_width <= kStageMaxWidth
+                         ? 1
+                         : 0;
+  GraphKey key{solver, K, precision, threads, spw, shared_diag, pf, fused, staged};
   auto it = ec.graphs.find(key);
   if (it == ec.graphs.end()) {
     if (ec.graphs.size() >= kMaxGraphsPerSystem) {  // drop the least recently used
@@ -1732,6 +1841,7 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
     auto cg = std::make_unique<CachedGraph>();
     cg->grid_f = grid_f;
     cg->smem_f = smem_f;
+    cg->staged = staged != 0;
     const cudaError_t be =
         s->A.off ? build_graph<K, int16_t>(s, solver, precision, threads, spw, shared_diag, pf,
                                            fused, cg.get())

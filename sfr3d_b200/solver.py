@@ -108,6 +108,7 @@ def lib() -> ctypes.CDLL:
     L.sfr_gpu_set_engine.argtypes = [_P, _I32, _I32, _I32]
     L.sfr_gpu_set_prefetch.argtypes = [_P, _I32]
     L.sfr_gpu_set_fused.argtypes = [_P, _I32]
+    L.sfr_gpu_set_staging.argtypes = [_P, _I32]
     L.sfr_gpu_spmv.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_transpose.argtypes = [_P, _P, _P, _P]
     L.sfr_gpu_spmv_dot.argtypes = [_P, _P, _P, _P, _P]
@@ -231,10 +232,17 @@ class GpuSystem:
     def set_fused(self, mode: int):
         """Graph engine, FP64 PCG with one right-hand side: one cooperative
         kernel an iteration (sfr_gpu_set_fused; 1, or 2 for the 40-register
-        form, 0 off)."""
+        form, 3 the tagged exchange, 0 off)."""
         rc = lib().sfr_gpu_set_fused(self.h, int(mode))
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_fused")
+
+    def set_staging(self, flag: int):
+        """Graph engine, BiCGSTAB: SpMV-phase slices staged in shared memory
+        by bulk copies (sfr_gpu_set_staging; 1 on, 0 off, the default)."""
+        rc = lib().sfr_gpu_set_staging(self.h, int(flag))
+        if rc != OK:
+            raise SolverError(rc, "sfr_gpu_set_staging")
 
     def autotune(self, solver: int, b, ad_k=None, tol: float = 1e-10, maxit: int = 100000,
                  precision: int = FP64) -> dict:
