@@ -547,15 +547,17 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
       if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
     }
   };
-  // phase A: q = A p, (p, q)
+  // phase A: q = A p, (p, q); each slice's column-independent loads go out
+  // with its columns (slice_rows: 114.6 -> 106.9 ms a 128^3 solve in mode 3)
   double acc[1] = {0.0};
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    double y[1];
-    row_product<1, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
-                                 [&](int, int c) { return ld_ro(a.p0[0] + c); }, y);
-    qz[row_ - row0] = y[0];
-    acc[0] += y[0] * ld_ro(a.p0[0] + row_);
-  }
+  slice_rows<1, double, true, double, double, I>(
+      n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, 0, all,
+      [&](int, int c) { return ld_ro(a.p0[0] + c); },
+      [&](int, int row) { return ld_ro(a.p0[0] + row); },
+      [&](int, int row, double y, double pk) {
+        qz[row - row0] = y;
+        acc[0] += y * pk;
+      });
   double tot[1];
   if (kTagged) {
     if (!tag_exchange(tx, 2 * j + 1, acc[0], a.part, &tot[0], sm)) {
