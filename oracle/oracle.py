@@ -713,3 +713,112 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         None if eddy is None else _p(eddy), None if stress is None else _p(stress),
         case.adv_beta, case.adv_fn, ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value
+
+
+# ------------------------------------------------ gradient reconstruction --
+# rcGradU (CellLoop.c:4544-4790): Green-Gauss cell or least squares
+RCGRADGAUSSC, RCGRADGAUSSN, RCLSQUARE, RCLSQUAREQR = 1, 2, 3, 4  # Define.h:377-380
+CONVECTIONHEAT = 11
+FLUXPRESC = 16
+
+
+@dataclass
+class GradCase:
+    """One rcGradU call: the mesh arrays, faceR of the field (its face loads),
+    the loads, the material table (COEFDIF column 0), u (numel, ndf) and the
+    previous gradient gradu (numel, ndf, 3), row k = grad u_k."""
+    mesh: object
+    facer: np.ndarray
+    loads: list
+    prop: np.ndarray
+    u: np.ndarray
+    gradu: np.ndarray
+    type: int = RCLSQUARE
+    mat: np.ndarray | None = None
+
+    @property
+    def ndf(self) -> int:
+        u = np.asarray(self.u)
+        return 1 if u.ndim == 1 else int(u.shape[1])
+
+    def material(self):
+        mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
+               else _c(self.mat, np.int16))
+        nmat = len(np.asarray(self.prop).reshape(-1, MAXPROP))
+        return np.ones(nmat, np.int16), mat
+
+
+def _grad_mesh(case: GradCase):
+    m = case.mesh
+    cal, mat = case.material()
+    keep = dict(
+        nelcon=_c(m.nelcon, np.int32), nface=_c(m.nviz, np.int16),
+        cellface=_c(m.cellface, np.int32), owner=_c(m.owner, np.int32),
+        volume=_c(m.volume, np.float64), dcca=_c(m.dcca, np.float64),
+        xmcc=_c(m.xmcc, np.float64), mksi=_c(m.mksi, np.float64),
+        ksi=_c(m.ksi, np.float64), area=_c(m.area, np.float64),
+        normal=_c(m.normal, np.float64), vskew=_c(m.vskew, np.float64),
+        caltype=cal, mat=mat, id=_c(m.id, np.int32), facer=_c(case.facer, np.int16))
+    dm = _DifMesh(numel=m.numel, maxviz=m.nelcon.shape[1],
+                  **{k: _p(v) for k, v in keep.items()})
+    return dm, keep
+
+
+def ls_matrix(case: GradCase) -> np.ndarray:
+    """leastSquareMatrix (RCLSQUARE) of every cell: (numel, 3, maxviz)."""
+    lib = oracle_lib()
+    lib.orc_ls_matrix.restype = None
+    lib.orc_ls_matrix.argtypes = [ctypes.POINTER(_DifMesh), _P]
+    dm, _keep = _grad_mesh(case)
+    out = np.zeros((case.mesh.numel, 3, case.mesh.nelcon.shape[1]))
+    lib.orc_ls_matrix(ctypes.byref(dm), _p(out))
+    return out
+
+
+def rc_grad(case: GradCase):
+    """The C restatement: (rc, gradu (numel, ndf, 3))."""
+    lib = oracle_lib()
+    lib.orc_rc_grad.restype = ctypes.c_int
+    lib.orc_rc_grad.argtypes = [ctypes.POINTER(_DifMesh), _P, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, _P, _P, _P, _P]
+    dm, _keep = _grad_mesh(case)
+    ndf = case.ndf
+    lsq = ls_matrix(case) if case.type == RCLSQUARE else np.zeros(1)
+    g = np.array(case.gradu, dtype=np.float64, copy=True, order="C").reshape(case.mesh.numel,
+                                                                            ndf, 3)
+    u = _c(case.u, np.float64)
+    rc = lib.orc_rc_grad(ctypes.byref(dm), _load_table(case.loads), len(case.loads), case.type,
+                         ndf, _p(_c(case.prop, np.float64)), _p(lsq), _p(u), _p(g))
+    return rc, g
+
+
+def ref_rc_grad(case: GradCase, nthreads=0):
+    """The reference's own rcLeastSquare + rcGradU: (rc, gradu, lsq, seconds)."""
+    m = case.mesh
+    lib = ref_lib()
+    if not getattr(lib, "_grad_typed", False):
+        lib.sfr_ref_rc_grad.restype = ctypes.c_int
+        lib.sfr_ref_rc_grad.argtypes = ([ctypes.c_int, ctypes.c_int] + [_P] * 20 + [ctypes.c_int]
+                                        + [_P] * 5 + [ctypes.c_int] * 2 + [_P] * 3
+                                        + [ctypes.c_int, _P])
+        lib._grad_typed = True
+    cal, mat = case.material()
+    cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
+    ndf = case.ndf
+    g = cp(case.gradu, np.float64).reshape(m.numel, ndf, 3)
+    u = cp(case.u, np.float64)
+    lsq = np.zeros((m.numel, 3, m.nelcon.shape[1]))
+    cc = m.xm[m.cellface[:, 0] - 1] - m.xmcc[:, 0, :]
+    arrs = [cp(m.nelcon, np.int32), cp(m.nviz, np.int16), cp(m.cellface, np.int32),
+            cp(m.owner, np.int32), cp(m.volume, np.float64), cp(m.dcca, np.float64),
+            cp(m.xmcc, np.float64), cp(cc, np.float64), cp(m.mksi, np.float64),
+            cp(m.ksi, np.float64), cp(m.eta, np.float64), cp(m.area, np.float64),
+            cp(m.normal, np.float64), cp(m.xm, np.float64), cp(m.mvskew, np.float64),
+            cp(m.vskew, np.float64), cal.copy(), mat.copy(), cp(case.prop, np.float64),
+            cp(case.facer, np.int16)]
+    vt = _load_arrays(case.loads)
+    sec = ctypes.c_double()
+    rc = lib.sfr_ref_rc_grad(m.numel, m.nelcon.shape[1], *[_p(x) for x in arrs],
+                             len(case.loads), *[_p(x) for x in vt], case.type, ndf, _p(u),
+                             _p(g), _p(lsq), nthreads, ctypes.byref(sec))
+    return rc, g, lsq, sec.value

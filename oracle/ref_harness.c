@@ -463,3 +463,71 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   free(wallpar);
   return rc;
 }
+
+/*
+ * The reference's own gradient reconstruction: rcLeastSquare
+ * (CellLoop.c:4830-4880) for the least-squares matrices, then rcGradU
+ * (CellLoop.c:4544-4790) as the SIMPLE driver calls it for the velocity or
+ * the pressure (Simple.c:2797-2858), with rcGrad {type, no limiter}, one
+ * process, no density fields.  Every cell is a hexahedron (geomType only
+ * picks the node table the Green-Gauss nodal variant would use).  gradu
+ * (numel*ndf*3) is read as the previous gradient and overwritten; lsq
+ * (numel*3*maxviz) receives the least-squares matrices when type is
+ * RCLSQUARE.  nthreads > 1 turns on its OpenMP cell loop.
+ */
+int sfr_ref_rc_grad(int numel, int maxviz, int *nelcon, short *nface, int *cellface, int *owner,
+                    double *volume, double *dcca, double *xmcc, double *cc, double *mksi,
+                    double *ksi, double *eta, double *area, double *normal, double *xm,
+                    double *mvskew, double *vskew, short *caltype, short *mat, double *prop,
+                    short *facer, int nloads, const int *ltype, const int *lvar,
+                    const int *lnp, const double *lpar, const double *ldens, int type, int ndf,
+                    double *u, double *gradu, double *lsq, int nthreads, double *seconds)
+{
+  INT *el = calloc((size_t)numel * 8, sizeof(INT));
+  short *nen = malloc((size_t)numel * sizeof(short));
+  short *gtype = malloc((size_t)numel * sizeof(short));
+  double *lsqr = calloc((size_t)numel * 6, sizeof(double));
+  double *lsqm = calloc((size_t)numel * 3 * maxviz, sizeof(double));
+  Loads *ld = calloc((size_t)(nloads > 0 ? nloads : 1), sizeof(Loads));
+  RcGrad rc;
+  int i, code = 0;
+  double t0;
+
+  fileLogExc = stderr;
+  fileLogDebug = stderr;
+  mpiVar.nPrcs = 1;
+  mpiVar.myId = 0;
+  ompVar.fGrad = nthreads > 1;
+  ompVar.nThreadsGrad = (short)(nthreads > 1 ? nthreads : 1);
+  for (i = 0; i < numel; i++) {
+    nen[i] = 8;
+    gtype[i] = HEXACELL;
+  }
+  fill_loads(ld, nloads, ltype, lvar, lnp, lpar, ldens);
+  memset(&rc, 0, sizeof(rc));
+  rc.type = (short)type;
+  rc.fLimiter = false;
+  if (type == RCLSQUARE || type == RCLSQUAREQR)
+    rcLeastSquare(cellface, owner, mksi, ksi, lsqm, lsqr, nface, numel, (short)maxviz,
+                  (short)type, 3);
+  g_armed = 1;
+  if (setjmp(g_jump) == 0) {
+    t0 = omp_get_wtime();
+    rcGradU(NULL, ld, el, nelcon, NULL, nen, nface, cellface, owner, volume, dcca, xmcc, cc,
+            mksi, ksi, eta, area, normal, xm, mvskew, vskew, gtype, prop, caltype, mat, NULL,
+            lsqm, lsqr, facer, u, gradu, NULL, NULL, NULL, 0.0, &rc, 8, (short)maxviz,
+            (short)ndf, 3, NULL, NULL, numel, numel, 0, 0, false);
+    if (seconds) *seconds = omp_get_wtime() - t0;
+    g_armed = 0;
+  } else {
+    code = g_exit_code ? g_exit_code : -1;
+  }
+  if (lsq) memcpy(lsq, lsqm, sizeof(double) * (size_t)numel * 3 * maxviz);
+  free(el);
+  free(nen);
+  free(gtype);
+  free(lsqr);
+  free(lsqm);
+  free(ld);
+  return code;
+}

@@ -1704,3 +1704,260 @@ done:
   comm_free(&c);
   return rc;
 }
+
+/* ======================================================================
+ * Gradient reconstruction: rcGradU (CellLoop.c:4544-4790) with
+ * greenGaussCell (CellLib.c:2481-2780) or leastSquare (CellLib.c:2931-3215)
+ * and the least-squares matrices of rcLeastSquare / leastSquareMatrix
+ * (CellLoop.c:4830-4880, CellLib.c:3500-3590); ndm = 3.
+ * ====================================================================== */
+
+enum {
+  GR_DIRICHLET = 1, GR_NEUMANN = 2, GR_ROBIN = 3, GR_SINBC = 4, GR_INLET = 6, GR_OUTLET = 7,
+  GR_MOVEWALL = 8, GR_INLETSTATIC = 9, GR_OPEN = 10, GR_CONVECTIONHEAT = 11,
+  GR_STATICWALL = 14, GR_FLUXPRES = 15, GR_FLUXPRESC = 16
+};
+
+/* the ch-signed ksi and |ksi| of a cell's faces */
+static void cell_ksi(const orc_dif_mesh *m, int nel, int nf, double ksi[][3], double *mk)
+{
+  int f, j;
+  for (f = 0; f < nf; f++) {
+    const long q = (long)nel * m->maxviz + f;
+    const int face = m->cellface[q] - 1;
+    const double ch = (m->owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+    mk[f] = m->mksi[face];
+    for (j = 0; j < 3; j++) ksi[f][j] = ch * m->ksi[3 * face + j];
+  }
+}
+
+void orc_ls_matrix(const orc_dif_mesh *m, double *lsq)
+{
+  const int mv = m->maxviz;
+  int nel, f;
+  for (nel = 0; nel < m->numel; nel++) {
+    double ksi[32][3], mk[32], dx[32][3], w[32], a[6] = {0, 0, 0, 0, 0, 0}, inv[6], det;
+    const int nf = m->nface[nel];
+    cell_ksi(m, nel, nf, ksi, mk);
+    for (f = 0; f < nf; f++) {
+      w[f] = 1.e0 / pow(mk[f], 2);
+      dx[f][0] = ksi[f][0] * mk[f];
+      dx[f][1] = ksi[f][1] * mk[f];
+      dx[f][2] = ksi[f][2] * mk[f];
+      a[0] += w[f] * dx[f][0] * dx[f][0];
+      a[1] += w[f] * dx[f][0] * dx[f][1];
+      a[2] += w[f] * dx[f][0] * dx[f][2];
+      a[3] += w[f] * dx[f][1] * dx[f][1];
+      a[4] += w[f] * dx[f][1] * dx[f][2];
+      a[5] += w[f] * dx[f][2] * dx[f][2];
+    }
+    det = a[0] * a[3] * a[5] + 2.e0 * a[1] * a[4] * a[2] -
+          (a[2] * a[2] * a[3] + a[4] * a[4] * a[0] + a[1] * a[1] * a[5]);
+    det = 1.e0 / det;
+    inv[0] = (a[3] * a[5] - a[4] * a[4]) * det;
+    inv[1] = -(a[1] * a[5] - a[2] * a[4]) * det;
+    inv[2] = (a[1] * a[4] - a[2] * a[3]) * det;
+    inv[3] = (a[0] * a[5] - a[2] * a[2]) * det;
+    inv[4] = -(a[0] * a[4] - a[1] * a[2]) * det;
+    inv[5] = (a[0] * a[3] - a[1] * a[1]) * det;
+    for (f = 0; f < nf; f++) {
+      double *l = lsq + (long)nel * 3 * mv;
+      l[0 * mv + f] = w[f] * (dx[f][0] * inv[0] + dx[f][1] * inv[1] + dx[f][2] * inv[2]);
+      l[1 * mv + f] = w[f] * (dx[f][0] * inv[1] + dx[f][1] * inv[3] + dx[f][2] * inv[4]);
+      l[2 * mv + f] = w[f] * (dx[f][0] * inv[2] + dx[f][1] * inv[4] + dx[f][2] * inv[5]);
+    }
+  }
+}
+
+/* getLoads (Loads.c:122-169) for the types the gradient reads: -2 for a
+ * function-valued load */
+static int gr_par(const orc_load *ld, double *par)
+{
+  int i;
+  if ((ld->type == GR_DIRICHLET || ld->type == GR_INLET) && ld->var != 0) return -2;
+  for (i = 0; i < ORC_MAXLOADPAR; i++) par[i] = ld->par[i];
+  return 0;
+}
+
+int orc_rc_grad(const orc_dif_mesh *m, const orc_load *loads, int nloads, int type, int ndf,
+                const double *prop, const double *lsq, const double *u, double *gradu)
+{
+  const int mv = m->maxviz;
+  int nel;
+  if (type != ORC_RCGRADGAUSSC && type != ORC_RCLSQUARE) return -1;
+  if (ndf != 1 && ndf != 3) return -1;
+  if (mv < 1 || mv > 31) return -1;
+  for (nel = 0; nel < m->numel; nel++) {
+    const int nf = m->nface[nel];
+    const short *fr = m->facer + (long)nel * (mv + 1);
+    const double coefdif = prop[(m->mat[nel] - 1) * ORC_MAXPROP + 0];
+    double *g = gradu + (long)nel * ndf * 3;
+    double uC[3], par[ORC_MAXLOADPAR];
+    int f, k, j, i;
+    if (nf < 1 || nf > mv) return -1;
+    for (k = 0; k < ndf; k++) uC[k] = u[(long)nel * ndf + k];
+    for (f = 0; f < nf; f++)
+      if (m->nelcon[(long)nel * mv + f] - 1 == -2 && fr[f] > 0) {
+        const orc_load *ld;
+        if (fr[f] > nloads) return -1;
+        ld = &loads[fr[f] - 1];
+        if (ld->type == GR_SINBC) return -2;
+        if ((ld->type == GR_DIRICHLET || ld->type == GR_INLET) && ld->var != 0) return -2;
+      }
+    if (type == ORC_RCGRADGAUSSC) {
+      double uf[32][3];
+      const double invVol = 1.e0 / m->volume[nel];
+      for (f = 0; f < nf; f++) {
+        const long q = (long)nel * mv + f;
+        const int viz = m->nelcon[q] - 1;
+        const double *xmcc = m->xmcc + 3 * q;
+        if (viz > -1) {
+          const int face = m->cellface[q] - 1;
+          const long q0 = (long)nel * mv;
+          const int face0 = m->cellface[q0] - 1;
+          double v[3], alpha, am1;
+          /* interpolFace, INTPOLFACELINEAR (CellLib.c:7174-7200), called with
+           * the cell's skew and xmcc arrays themselves (CellLib.c:2513, 2640), so
+           * every face reads its first face's vSkew and xmcc; |ksi| is the
+           * face's own */
+          for (j = 0; j < 3; j++) v[j] = m->vskew[3 * face0 + j] + m->xmcc[3 * q0 + j];
+          alpha = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / m->mksi[face];
+          am1 = 1.0e0 - alpha;
+          for (k = 0; k < ndf; k++) uf[f][k] = am1 * uC[k] + alpha * u[(long)viz * ndf + k];
+        } else if (fr[f] > 0) {
+          const orc_load *ld = &loads[fr[f] - 1];
+          const int ty = ld->type;
+          if (ndf == 1) {
+            if (ty == GR_DIRICHLET || ty == GR_INLET) {
+              gr_par(ld, par);
+              uf[f][0] = par[0];
+            } else if (ty == GR_FLUXPRES) {
+              /* gradPbBuoyant without buoyancy: gradPb = 0 */
+              uf[f][0] = uC[0] + (0.0 * xmcc[0] + 0.0 * xmcc[1] + 0.0 * xmcc[2]);
+            } else if (ty == GR_FLUXPRESC) {
+              uf[f][0] = uC[0];
+            } else if (ty == GR_NEUMANN) {
+              if (coefdif == 0.e0) return -1; /* uf left undefined */
+              gr_par(ld, par);
+              uf[f][0] = uC[0] + (par[0] / coefdif) * m->dcca[q];
+            } else if (ty == GR_ROBIN || ty == GR_CONVECTIONHEAT) {
+              uf[f][0] = uC[0];
+              for (j = 0; j < 3; j++) uf[f][0] += g[j] * xmcc[j];
+            } else if (ty == GR_OUTLET) {
+              uf[f][0] = uC[0];
+            } else {
+              return -1; /* no branch sets the face value */
+            }
+          } else {
+            int set = 0;
+            if (ty == GR_DIRICHLET || ty == GR_MOVEWALL) {
+              gr_par(ld, par);
+              for (k = 0; k < 3; k++) uf[f][k] = par[k];
+              set = 1;
+            }
+            /* a second chain: the reference's `if` here is not an `else if` */
+            if (ty == GR_STATICWALL) {
+              for (k = 0; k < 3; k++) uf[f][k] = 0.e0;
+              set = 1;
+            } else if (ty == GR_INLET) {
+              gr_par(ld, par);
+              for (k = 0; k < 3; k++) uf[f][k] = par[k];
+              set = 1;
+            } else if (ty == GR_NEUMANN) {
+              if (coefdif == 0.e0) return -1;
+              gr_par(ld, par);
+              for (k = 0; k < 3; k++) uf[f][k] = uC[k] + (par[k] / coefdif) * m->dcca[q];
+              set = 1;
+            } else if (ty == GR_ROBIN || ty == GR_CONVECTIONHEAT) {
+              return -1; /* the reference stops: not implemented */
+            } else if (ty == GR_OUTLET || ty == GR_INLETSTATIC || ty == GR_OPEN) {
+              for (k = 0; k < 3; k++) uf[f][k] = uC[k];
+              set = 1;
+            }
+            if (!set) return -1;
+          }
+        } else {
+          for (k = 0; k < ndf; k++) {
+            uf[f][k] = uC[k];
+            for (j = 0; j < 3; j++) uf[f][k] += g[3 * k + j] * xmcc[j];
+          }
+        }
+      }
+      for (k = 0; k < ndf; k++)
+        for (j = 0; j < 3; j++) {
+          double tmp = 0.e0;
+          for (f = 0; f < nf; f++) {
+            const int face = m->cellface[(long)nel * mv + f] - 1;
+            const double ch = (m->owner[2 * face] - 1 == nel) ? 1.0 : -1.0;
+            tmp += uf[f][k] * m->area[face] * (ch * m->normal[3 * face + j]);
+          }
+          g[3 * k + j] = tmp * invVol;
+        }
+    } else {
+      const double *l = lsq + (long)nel * 3 * mv;
+      double du[32][3];
+      int it = 1, pass;
+      for (i = 0; i < ndf * 3; i++) g[i] = 0.e0;
+      for (pass = 0; pass < it; pass++) {
+        for (f = 0; f < nf; f++) {
+          const long q = (long)nel * mv + f;
+          const int viz = m->nelcon[q] - 1;
+          const double *xmcc = m->xmcc + 3 * q;
+          for (k = 0; k < ndf; k++) du[f][k] = 0.e0;
+          if (viz > -1) {
+            for (k = 0; k < ndf; k++) du[f][k] = u[(long)viz * ndf + k] - uC[k];
+          } else if (fr[f] > 0) {
+            const orc_load *ld = &loads[fr[f] - 1];
+            const int ty = ld->type;
+            if (ndf == 1) {
+              if (ty == GR_DIRICHLET || ty == GR_MOVEWALL || ty == GR_INLET) {
+                gr_par(ld, par);
+                du[f][0] = par[0] - uC[0];
+              } else if (ty == GR_FLUXPRES) {
+                du[f][0] = 0.0 * xmcc[0] + 0.0 * xmcc[1] + 0.0 * xmcc[2];
+              } else if (ty == GR_NEUMANN) {
+                if (coefdif != 0.e0) {
+                  gr_par(ld, par);
+                  du[f][0] = (par[0] / coefdif) * m->dcca[q];
+                }
+              } else if (ty == GR_ROBIN || ty == GR_CONVECTIONHEAT) {
+                if (pass == 0) it = 2;
+                du[f][0] = 0.e0;
+                for (j = 0; j < 3; j++) du[f][0] += g[j] * xmcc[j];
+              }
+              /* FLUXPRESC, OUTLET, INLETSTAICTPRES, OPEN and the rest: 0 */
+            } else {
+              if (ty == GR_DIRICHLET || ty == GR_MOVEWALL) {
+                gr_par(ld, par);
+                for (k = 0; k < 3; k++) du[f][k] = par[k] - uC[k];
+              } else if (fr[f] == GR_STATICWALL) {
+                /* the reference compares the load's index, not its type,
+                 * with STATICWALL (CellLib.c:3118) */
+                for (k = 0; k < 3; k++) du[f][k] = -uC[k];
+              } else if (ty == GR_INLET) {
+                gr_par(ld, par);
+                for (k = 0; k < 3; k++) du[f][k] = par[k] - uC[k];
+              } else if (ty == GR_ROBIN || ty == GR_CONVECTIONHEAT) {
+                return -1; /* the reference stops: not implemented */
+              }
+              /* the rest: 0 */
+            }
+          } else {
+            if (pass == 0) it = 2;
+            for (k = 0; k < ndf; k++) {
+              du[f][k] = 0.e0;
+              for (j = 0; j < 3; j++) du[f][k] += g[3 * k + j] * xmcc[j];
+            }
+          }
+        }
+        for (k = 0; k < ndf; k++)
+          for (i = 0; i < 3; i++) {
+            double tmp = 0.e0;
+            for (f = 0; f < nf; f++) tmp += l[i * mv + f] * du[f][k];
+            g[3 * k + i] = tmp;
+          }
+      }
+    }
+  }
+  return 0;
+}

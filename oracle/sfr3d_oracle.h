@@ -180,6 +180,31 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
                      const int *ia, const int *ja, double *a, double *ad, double *b,
                      double *rcell, int forces, int matrix, int calrcell);
 
+/* ---- gradient reconstruction (rcGradU, CellLoop.c:4544-4790) ---------- */
+
+#define ORC_RCGRADGAUSSC 1 /* Define.h:377 */
+#define ORC_RCLSQUARE 3    /* Define.h:379 */
+
+/* leastSquareMatrix with RCLSQUARE, ndm = 3 (CellLib.c:3500-3590), for
+ * every cell as rcLeastSquare stores it (CellLoop.c:4830-4880):
+ * lsq[(cell * 3 + i) * maxviz + face]. */
+void orc_ls_matrix(const orc_dif_mesh *m, double *lsq);
+
+/* rcGradU with rcGrad.type ORC_RCGRADGAUSSC (greenGaussCell, CellLib.c:
+ * 2481-2780) or ORC_RCLSQUARE (leastSquare, CellLib.c:2931-3215), no
+ * limiter, ndm = 3, ndf 1 or 3.  m->facer holds the field's face loads
+ * (faceRpres, faceRvel, ...); prop nmat x MAXPROP (COEFDIF 0, read by
+ * NEUMANN faces); lsq from orc_ls_matrix (least squares only); u numel*ndf;
+ * gradu numel*ndf*3, row k = grad u_k: in, the previous gradient (faces
+ * without a load extrapolate with it under Green-Gauss), out, the new one.
+ * FLUXPRES is restated without buoyancy (gradPbBuoyant's zero branch).
+ * Returns 0, -1 for input whose face value the reference leaves undefined
+ * (a load type its branch does not handle, NEUMANN with zero COEFDIF under
+ * Green-Gauss, ROBIN with ndf = 3), -2 for loads given as functions and
+ * SINBC. */
+int orc_rc_grad(const orc_dif_mesh *m, const orc_load *loads, int nloads, int type, int ndf,
+                const double *prop, const double *lsq, const double *u, double *gradu);
+
 /* ---- the MPI path: row-partitioned PCG and BiCGSTAB ------------------- */
 
 /* One rank's layout and interface (Interface, Mesh.h:212-222; the MPI CSRD of

@@ -426,3 +426,99 @@ def test_vel_oracle_rejects_what_it_does_not_restate():
     assert run(lvel=[O.Load(O.STATICWALL, ())], adv=5, adv_fn=10) == -1  # no such function
     assert O.vel_assemble(O.VelCase(**base, lvel=[O.Load(O.STATICWALL, ())]), O.ELLPACK, False,
                           O.ell_ia(s.neq, 6), s.ell()[0], s.neq)[0] == -1
+
+
+# ---------------------------------------------------- gradient reconstruction
+GRAD_SCALAR_LOADS = [O.Load(O.DIRICHLET, (0.3,)), O.Load(O.NEUMANN, (0.2,)),
+                     O.Load(O.OUTLET, ()), O.Load(O.ROBIN, (2.0, 1.5)),
+                     O.Load(O.FLUXPRES, ()), O.Load(O.FLUXPRESC, ())]
+GRAD_VEL_LOADS = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+                  O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1)), O.Load(O.OUTLET, ()),
+                  O.Load(O.OPEN, (0.0,), density=1.1), O.Load(O.DIRICHLET, (0.1, 0.2, 0.3))]
+
+
+def _grad_cases(m, rng, typ, ndf):
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (0.7, 1.3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    if ndf == 1:
+        loads = GRAD_SCALAR_LOADS
+        tables = [[1, 2, 0, 3, 1, 0], [5, 6, 2, 0, 4, 1]]
+        if typ == O.RCLSQUARE:
+            tables.append([4, 3, 5, 6, 2, 1])
+    else:
+        loads = GRAD_VEL_LOADS
+        tables = [[1, 2, 3, 4, 0, 1], [6, 5, 1, 1, 2, 0]]
+    for sides in tables:
+        u = rng.standard_normal(m.numel) if ndf == 1 else rng.standard_normal((m.numel, 3))
+        yield sides, O.GradCase(mesh=m, facer=m.face_r(sides), loads=loads, prop=prop, u=u,
+                                gradu=rng.standard_normal((m.numel, ndf, 3)), type=typ,
+                                mat=mat)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+@pytest.mark.parametrize("typ", [O.RCGRADGAUSSC, O.RCLSQUARE])
+@pytest.mark.parametrize("ndf", [1, 3])
+def test_rc_grad_oracle_matches_reference_live(typ, ndf):
+    """rcGradU (Green-Gauss cell or least squares, no limiter) against the
+    reference's own rcLeastSquare + rcGradU, bit for bit: the field's face
+    loads of every kind each branch takes, faces without a load (the
+    previous gradient, or the two-pass least squares), two materials; the
+    least-squares matrices too, and the OpenMP cell loop gives the same
+    gradient."""
+    s = S.poisson_jittered(5, seed=30)
+    m = s.mesh()
+    rng = np.random.default_rng(31 + typ + ndf)
+    for sides, case in _grad_cases(m, rng, typ, ndf):
+        r1, g1 = O.rc_grad(case)
+        r2, g2, lsq, _sec = O.ref_rc_grad(case)
+        assert r1 == r2 == 0, sides
+        assert bits_equal(g1, g2), (sides, np.abs(g1 - g2).max())
+        if typ == O.RCLSQUARE:
+            assert bits_equal(O.ls_matrix(case), lsq)
+        r3, g3, _lsq, _sec = O.ref_rc_grad(case, nthreads=4)
+        assert r3 == 0 and bits_equal(g1, g3)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_rc_grad_least_squares_staticwall_index_quirk():
+    """leastSquare with ndf > 1 compares the load's index, not its type, with
+    STATICWALL (CellLib.c:3118): a STATICWALL load elsewhere in the table
+    contributes nothing, while whatever load sits at index 14 pins the face
+    to zero.  The restatement keeps both, against the reference."""
+    s = S.poisson_jittered(4, seed=32)
+    m = s.mesh()
+    rng = np.random.default_rng(33)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (0.7, 1.0)
+    loads = [O.Load(O.OUTLET, ())] * 13 + [O.Load(O.OPEN, (0.0,), density=1.0),
+                                           O.Load(O.STATICWALL, ())]
+    for sides in ([14, 15, 1, 14, 15, 0], [15, 15, 15, 15, 15, 15]):
+        case = O.GradCase(mesh=m, facer=m.face_r(sides), loads=loads, prop=prop,
+                          u=rng.standard_normal((m.numel, 3)),
+                          gradu=rng.standard_normal((m.numel, 3, 3)), type=O.RCLSQUARE)
+        r1, g1 = O.rc_grad(case)
+        r2, g2, _lsq, _sec = O.ref_rc_grad(case)
+        assert r1 == r2 == 0 and bits_equal(g1, g2), sides
+
+
+def test_rc_grad_oracle_rejects_what_the_reference_leaves_undefined():
+    s = S.poisson_uniform(4, seed=34)
+    m = s.mesh()
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (0.7, 1.0)
+    run = lambda loads, typ, ndf, p=prop: O.rc_grad(O.GradCase(  # noqa: E731
+        mesh=m, facer=m.face_r([1, 0, 0, 0, 0, 0]), loads=loads, prop=p,
+        u=np.zeros(m.numel) if ndf == 1 else np.zeros((m.numel, 3)),
+        gradu=np.zeros((m.numel, ndf, 3)), type=typ))[0]
+    assert run([O.Load(O.DIRICHLET, (1.0,))], O.RCGRADGAUSSC, 1) == 0
+    assert run([O.Load(O.DIRICHLET, (1.0,), var=1)], O.RCLSQUARE, 1) == -2
+    assert run([O.Load(O.SINBC, (1.0, 1.0, 0.0) * 3)], O.RCGRADGAUSSC, 1) == -2
+    assert run([O.Load(O.STATICWALL, ())], O.RCGRADGAUSSC, 1) == -1  # no face value
+    assert run([O.Load(O.ROBIN, (1.0, 1.0))], O.RCLSQUARE, 3) == -1  # the reference stops
+    zero = prop.copy()
+    zero[0, 0] = 0.0
+    assert run([O.Load(O.NEUMANN, (1.0,))], O.RCGRADGAUSSC, 1, zero) == -1
+    assert run([O.Load(O.NEUMANN, (1.0,))], O.RCLSQUARE, 1, zero) == 0  # du stays 0
+    assert run([O.Load(O.STATICWALL, ())], O.RCLSQUARE + 1, 1) == -1  # QR: not restated
