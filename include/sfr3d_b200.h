@@ -529,6 +529,47 @@ int sfr_gpu_vel_assemble(sfr_dif_plan *p, const sfr_load *lvel, int32_t nlvel,
  * calls are not). */
 int sfr_gpu_dif_plan_destroy(sfr_dif_plan *p);
 
+/* ---- gradient reconstruction ------------------------------------------ */
+/* rcGradU (CellLoop.c:4544-4790) on the device: the Green-Gauss cell kernel
+ * (type 1, RCGRADGAUSSC: greenGaussCell, CellLib.c:2481-2780) or least
+ * squares (type 3, RCLSQUARE: leastSquare, CellLib.c:2931-3215, with the
+ * matrices of rcLeastSquare / leastSquareMatrix, CellLib.c:3500-3590), no
+ * limiter, ndm = 3, for a scalar (ndf 1: the pressure) or the velocity
+ * (ndf 3), bit-identical to the reference's.  The SIMPLE driver calls it for
+ * the velocity and the pressure before each assembly (Simple.c:2797-2858);
+ * here the gradient is formed where the field is.  Types 2 (Green-Gauss
+ * nodal) and 4 (QR least squares) are SFR_UNSUPPORTED.
+ *
+ * The plan reads from mesh: nelcon, nviz, cellface, owner, volume, dcca,
+ * xmcc, mksi, ksi, area, normal, vskew, mat, nmat and facer, which holds the
+ * FIELD's face loads (faceRpres for the pressure, faceRvel for the
+ * velocity).  Two reference behaviours are kept: greenGaussCell
+ * interpolates every face with its cell's FIRST face's vSkew and xmcc
+ * (CellLib.c:2513, 2640), and leastSquare with ndf 3 sets a face to -u_C
+ * when its load is the 14th of the table, whatever its type, rather than
+ * for STATICWALL loads (CellLib.c:3118). */
+typedef struct sfr_grad_plan sfr_grad_plan;
+int sfr_gpu_grad_plan_create(int32_t device, const sfr_dif_mesh *mesh, int32_t type,
+                             sfr_grad_plan **out);
+
+/* gradu (numel * ndf * 3, row k = grad u_k) is read as the previous
+ * gradient and overwritten with the new one; u is numel * ndf.  prop is the
+ * nmat x MAXPROP material table (COEFDIF, column 0, is read by NEUMANN
+ * faces).  A face value the reference's branch leaves undefined (a load
+ * type the branch has no case for, NEUMANN with COEFDIF 0 under
+ * Green-Gauss, ROBIN with ndf 3) is SFR_BAD_INPUT; SINBC and loads given as
+ * functions SFR_UNSUPPORTED.  FLUXPRES faces are taken without buoyancy.
+ * Device arrays, on `stream` (NULL: the plan's own). */
+int sfr_gpu_grad_device(sfr_grad_plan *p, const sfr_load *loads, int32_t nloads,
+                        const double *prop, int32_t ndf, const double *d_u, double *d_gradu,
+                        void *stream);
+
+/* The same with host arrays (copied in and back; synchronous). */
+int sfr_gpu_grad(sfr_grad_plan *p, const sfr_load *loads, int32_t nloads, const double *prop,
+                 int32_t ndf, const double *u, double *gradu);
+
+int sfr_gpu_grad_plan_destroy(sfr_grad_plan *p);
+
 /* Copy the system's values back in the reference's layout: al (nad, or the
  * neq*width ELLPACK slots), ad (neq) and, for unsym CSRC, au (nad).  Any
  * pointer may be NULL. */

@@ -385,6 +385,69 @@ class VelPlan(DifPlan):
             self.system.values_version += 1
 
 
+RCGRADGAUSSC, RCLSQUARE = 1, 3  # rcGrad.type (Define.h:377-380)
+
+
+class GradPlan:
+    """rcGradU on the device (sfr_gpu_grad_*): Green-Gauss cell
+    (RCGRADGAUSSC) or least squares (RCLSQUARE) over ``mesh`` with the
+    field's face loads ``facer`` (faceRpres, faceRvel, ...).  ``mat`` gives
+    each cell's material (1-based; COEFDIF of ``prop`` column 0 is read by
+    NEUMANN faces)."""
+
+    def __init__(self, mesh, facer, type: int = RCLSQUARE, mat=None, nmat: int = 1,
+                 device: int = 0):
+        self.numel = int(mesh.numel)
+        self.type = type
+        L = _lib()
+        if not getattr(L, "_grad_typed", False):
+            L.sfr_gpu_grad_plan_create.argtypes = [_I32, ctypes.POINTER(DifMeshC), _I32,
+                                                   ctypes.POINTER(_P)]
+            L.sfr_gpu_grad.argtypes = [_P, _P, _I32, _P, _I32, _P, _P]
+            L.sfr_gpu_grad_device.argtypes = [_P, _P, _I32, _P, _I32, _P, _P, _P]
+            L.sfr_gpu_grad_plan_destroy.argtypes = [_P]
+            L._grad_typed = True
+        m, _keep = _mesh_c(mesh, facer, None, mat, nmat=nmat)
+        h = _P()
+        rc = L.sfr_gpu_grad_plan_create(device, ctypes.byref(m), type, ctypes.byref(h))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_grad_plan_create: " + _sv.last_error())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().sfr_gpu_grad_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def grad(self, loads, prop, u, gradu):
+        """One rcGradU call with host arrays: u (numel,) or (numel, 3), gradu
+        (numel, ndf, 3) the previous gradient; returns the new one."""
+        u = _c(u, np.float64)
+        ndf = 1 if u.ndim == 1 else int(u.shape[1])
+        g = np.array(gradu, dtype=np.float64, copy=True, order="C").reshape(self.numel, ndf, 3)
+        lt = _loads_c(loads)
+        pr = _c(prop, np.float64)
+        rc = _lib().sfr_gpu_grad(self.h, lt, len(loads), _ptr(pr), ndf, _ptr(u), _ptr(g))
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_grad: " + _sv.last_error())
+        return g
+
+    def grad_device(self, loads, prop, ndf: int, d_u: int, d_gradu: int, stream: int = 0):
+        """The same on device arrays (torch data_ptr values), on ``stream``."""
+        lt = _loads_c(loads)
+        pr = _c(prop, np.float64)
+        rc = _lib().sfr_gpu_grad_device(self.h, lt, len(loads), _ptr(pr), ndf, d_u, d_gradu,
+                                        stream or None)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_grad_device: " + _sv.last_error())
+
+
 def get_values(system: "_sv.GpuSystem"):
     """(al, ad, au) of the system in the reference's layout, copied back
     (au is None unless the storage is unsym CSRC)."""

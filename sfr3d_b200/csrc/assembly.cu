@@ -109,8 +109,6 @@ struct FuseDev {
   float *diag32;
 };
 
-__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
   return xadd(xadd(xmul(a[0], b[0]), xmul(a[1], b[1])), xmul(a[2], b[2]));
 }

@@ -74,7 +74,6 @@ struct BlArgs {
 #define SFR_BL_FOR_ROWS(i) \
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
 
-__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 
 // y = A g over this warp's rows (the reference's row rounding); defines y0
 // for the body.  The diagonal is the graph's copy of the caller's.

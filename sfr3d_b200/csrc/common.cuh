@@ -49,6 +49,10 @@ __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+// IEEE division and square root, correctly rounded (what the host's / and
+// sqrt give)
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
 
 // ----------------------------------------------------------------------
 // Deterministic reductions: fixed shuffle tree inside a warp, fixed tree

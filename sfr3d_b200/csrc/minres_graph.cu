@@ -92,8 +92,6 @@ __device__ __forceinline__ double2 ld2(const double *p) {
 }
 __device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
 
-__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ double xsqrt(double a) { return __dsqrt_rn(a); }
 
 // Iters.c:1171-1211 (symOrtho): no branch taken leaves c, s, r as they were.
 __device__ void sym_ortho_dev(double a, double b, double *c, double *s, double *r) {

@@ -713,3 +713,81 @@ def test_vel_validation(cuda, box):
     assert e.value.status == sv.BAD_INPUT
     plan.assemble([A.Load(A.STATICWALL, ())], prop, z1, z3, z3, z9, z3)
     plan.close()
+
+
+# ---------------------------------------------------- gradient reconstruction
+GSCALAR = [O.Load(O.DIRICHLET, (0.3,)), O.Load(O.NEUMANN, (0.2,)), O.Load(O.OUTLET, ()),
+           O.Load(O.ROBIN, (2.0, 1.5)), O.Load(O.FLUXPRES, ()), O.Load(O.FLUXPRESC, ())]
+GVEL = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+        O.Load(O.INLET, (0.5, 0.1, 0.0, 1.1)), O.Load(O.OUTLET, ()),
+        O.Load(O.OPEN, (0.0,), density=1.1), O.Load(O.DIRICHLET, (0.1, 0.2, 0.3))]
+
+
+@pytest.mark.parametrize("typ", [O.RCGRADGAUSSC, O.RCLSQUARE])
+@pytest.mark.parametrize("ndf", [1, 3])
+def test_rc_grad_matches_oracle(cuda, box, typ, ndf):
+    """rcGradU on the device, bit for bit against the oracle (itself pinned
+    to the reference's rcGradU): every load kind each branch takes, faces
+    without a load, two materials; host and device-array calls."""
+    torch = cuda
+    s, m, lay = box
+    rng = np.random.default_rng(60 + typ + ndf)
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (0.7, 1.3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    loads = GSCALAR if ndf == 1 else GVEL
+    tables = ([[1, 2, 0, 3, 1, 0], [5, 6, 2, 0, 4, 1]] if ndf == 1
+              else [[1, 2, 3, 4, 0, 1], [6, 5, 1, 1, 2, 0]])
+    for sides in tables:
+        fr = m.face_r(sides)
+        plan = A.GradPlan(m, fr, type=typ, mat=mat, nmat=2)
+        for _ in range(2):
+            u = rng.standard_normal(m.numel) if ndf == 1 else rng.standard_normal((m.numel, 3))
+            g0 = rng.standard_normal((m.numel, ndf, 3))
+            case = O.GradCase(mesh=m, facer=fr, loads=loads, prop=prop, u=u, gradu=g0, type=typ,
+                              mat=mat)
+            rc, want = O.rc_grad(case)
+            assert rc == 0
+            got = plan.grad(_aloads(loads), prop, u, g0)
+            assert bits_equal(got, want), (sides, np.abs(got - want).max())
+            du = torch.tensor(np.ascontiguousarray(u), device="cuda")
+            dg = torch.tensor(g0, device="cuda")
+            plan.grad_device(_aloads(loads), prop, ndf, du.data_ptr(), dg.data_ptr())
+            torch.cuda.synchronize()
+            assert bits_equal(dg.cpu().numpy(), want)
+        plan.close()
+
+
+def test_rc_grad_validation(cuda, box):
+    s, m, lay = box
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (0.7, 1.0)
+    fr = m.face_r([1, 0, 0, 0, 0, 0])
+    with pytest.raises(sv.SolverError) as e:
+        A.GradPlan(m, fr, type=2)
+    assert e.value.status == sv.UNSUPPORTED
+    gg = A.GradPlan(m, fr, type=A.RCGRADGAUSSC)
+    ls = A.GradPlan(m, fr, type=A.RCLSQUARE)
+    u1, g1 = np.zeros(m.numel), np.zeros((m.numel, 1, 3))
+    u3, g3 = np.zeros((m.numel, 3)), np.zeros((m.numel, 3, 3))
+    with pytest.raises(sv.SolverError) as e:  # no face value under Green-Gauss
+        gg.grad([A.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0))], prop, u1, g1)
+    assert e.value.status == sv.BAD_INPUT
+    with pytest.raises(sv.SolverError) as e:
+        ls.grad([A.Load(O.ROBIN, (1.0, 1.0))], prop, u3, g3)  # the reference stops
+    assert e.value.status == sv.BAD_INPUT
+    with pytest.raises(sv.SolverError) as e:
+        ls.grad([A.Load(O.DIRICHLET, (1.0,), var=1)], prop, u1, g1)
+    assert e.value.status == sv.UNSUPPORTED
+    with pytest.raises(sv.SolverError) as e:
+        ls.grad([], prop, u1, g1)  # a face names load 1
+    assert e.value.status == sv.BAD_INPUT
+    zero = prop.copy()
+    zero[0, 0] = 0.0
+    with pytest.raises(sv.SolverError) as e:
+        gg.grad([A.Load(O.NEUMANN, (1.0,))], zero, u1, g1)
+    assert e.value.status == sv.BAD_INPUT
+    ls.grad([A.Load(O.NEUMANN, (1.0,))], zero, u1, g1)  # leastSquare: du stays 0
+    gg.close()
+    ls.close()
