@@ -362,6 +362,7 @@ def run_ours(args):
         assembly["pressure"] = pressure_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["momentum"] = momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind)
         assembly["simple_step"] = simple_step_leg(np, torch, sv, s, n)
+        assembly["gradient"] = gradient_leg(np, torch, s, n, peak, peak_kind)
         partitioned = partitioned_leg(np, sv, s, n, ms_step, x.cpu().numpy())
         momentum = momentum_leg(np, torch, sv, S, n, local, tune=not args.no_tune)
         batch = batch_leg(sv, S)
@@ -1113,6 +1114,54 @@ def momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind):
             "kernel": "vel_assemble_kernel<6 faces> + the gather/compensation refresh"}
 
 
+# algorithmic bytes per cell of the least-squares gradient kernel (6 faces):
+# per face the neighbour word (4) and 7 doubles (the matrix column, xmcc,
+# dcca), the cell's face count and material (4), its own u (8 ndf; the
+# neighbours' u come from cache), the previous gradient read and the new one
+# written (2 * 24 ndf)
+def grad_alg_bytes(ndf):
+    return 6 * (4 + 56) + 4 + 8 * ndf + 48 * ndf
+
+
+def gradient_inputs(np, s):
+    """The cavity fields and face loads of a SIMPLE step: velocity (MOVEWALL
+    lid, STATICWALL walls) and pressure (fixed on x = 0)."""
+    from sfr3d_b200 import assembly as A
+    m = s.mesh()
+    rng = np.random.default_rng(13)
+    prop = np.zeros((1, 10))
+    prop[0, :2] = (1e-3, 1.0)
+    vel = rng.standard_normal((m.numel, 3)) * 0.1
+    pres = rng.standard_normal(m.numel) * 1e-2
+    lvel = [A.Load(A.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), A.Load(A.STATICWALL, ())]
+    lpres = [A.Load(A.DIRICHLET, (0.0,))]
+    return m, prop, vel, pres, lvel, lpres
+
+
+def gradient_leg(np, torch, s, n, peak, peak_kind):
+    """rcGradU on the device, least squares (the cavity deck's rcGrad): the
+    velocity gradient (ndf 3) and the pressure gradient (ndf 1) of the same
+    mesh, each on device arrays."""
+    from sfr3d_b200 import assembly as A
+    m, prop, vel, pres, lvel, lpres = gradient_inputs(np, s)
+    out = {"workload": f"rcGradU least squares, {n}^3 = {m.numel} cells, cavity loads",
+           "peak_source": f"{peak_kind} hbm_gbs",
+           "kernel": "least_squares_kernel<ndf> (one thread a cell, 6 faces)"}
+    st = torch.cuda.Stream()
+    for name, sides, loads, u, ndf in (("velocity", PRES_SIDES_VEL, lvel, vel, 3),
+                                       ("pressure", PRES_SIDES_PRES, lpres, pres, 1)):
+        plan = A.GradPlan(m, m.face_r(sides), type=A.RCLSQUARE)
+        du = torch.tensor(np.ascontiguousarray(u), device="cuda")
+        dg = torch.zeros((m.numel, ndf, 3), dtype=torch.float64, device="cuda")
+        ms = time_calls(torch, lambda: plan.grad_device(loads, prop, ndf, du.data_ptr(),
+                                                        dg.data_ptr(), st.cuda_stream), st)
+        plan.close()
+        gbs = grad_alg_bytes(ndf) * m.numel / (ms * 1e-3) / 1e9
+        out[name] = {"ndf": ndf, "device_ms": ms, "alg_bytes_per_cell": grad_alg_bytes(ndf),
+                     "GB/s": gbs, "frac": gbs / peak}
+    return out
+
+
 def simple_step_leg(np, torch, sv, s, n):
     """The linear-algebra half of one SIMPLE iteration kept on the device:
     momentum assembly, the u, v, w BiCGSTAB solves in one batched launch,
@@ -1216,6 +1265,19 @@ def cpu_assembly(O, s):
     rp = O.ref_solve(O.PCG, O.CSRD, True, s.ia, s.ja, pr[1], pr[2], pr[3], tol=1e-10,
                      nthreads=threads)
     step_ms = (time.perf_counter() - t0) * 1e3
+    # the reference's rcGradU (least squares) on the same fields and loads
+    m, gprop, gvel, gpres, _lv, _lp = gradient_inputs(np, s)
+    grad_cpu = {"threads": threads,
+                "sample": "one full rcGradU call (least squares) with its OpenMP cell loop "
+                          "on all host threads"}
+    for name, sides, loads, u, ndf in (
+            ("velocity", PRES_SIDES_VEL,
+             [O.Load(O.MOVEWALL, (1.0, 0.0, 0.0, 0.0)), O.Load(O.STATICWALL, ())], gvel, 3),
+            ("pressure", PRES_SIDES_PRES, [O.Load(O.DIRICHLET, (0.0,))], gpres, 1)):
+        gcase = O.GradCase(mesh=m, facer=m.face_r(sides), loads=loads, prop=gprop, u=u,
+                           gradu=np.zeros((m.numel, ndf, 3)), type=O.RCLSQUARE)
+        grc, _g, _lsq, gsec = O.ref_rc_grad(gcase, nthreads=threads)
+        grad_cpu[name] = {"ms": gsec * 1e3, "status": grc}
     return {"ms": sec * 1e3, "threads": 1, "status": rc,
             "simple_step": {"ms": step_ms, "threads": threads, "momentum_iters": mom_iters,
                             "pressure_iters": rp.iters, "status": [vr[0], pr[0], rp.status],
@@ -1227,7 +1289,8 @@ def cpu_assembly(O, s):
                                    "loop on all host threads"},
             "momentum": {"ms": vsec * 1e3, "threads": threads, "status": vrc,
                          "sample": "one full systFormSimpleVel call with its OpenMP cell "
-                                   "loop on all host threads"}}
+                                   "loop on all host threads"},
+            "gradient": grad_cpu}
 
 
 def adjoint_leg(np, sv, S):
