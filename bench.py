@@ -56,7 +56,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the momentum, batched and adjoint legs")
     ap.add_argument("--profile", choices=["none", "spmv", "solve", "bicgstab", "assembly",
-                                          "pressure", "momentum", "partitioned"],
+                                          "pressure", "momentum", "partitioned", "gradient"],
                     default="none",
                     help="short launch sequence for ncu (no JSON line)")
     ap.add_argument("--engine", type=int, default=0,
@@ -241,6 +241,16 @@ def run_ours(args):
                 for _ in range(args.warmup + args.steps):
                     call()
                 close()
+            elif args.profile == "gradient":
+                from sfr3d_b200 import assembly as A
+                m, prop, vel, _pres, lvel, _lpres = gradient_inputs(np, s)
+                plan = A.GradPlan(m, m.face_r(PRES_SIDES_VEL), type=A.RCLSQUARE)
+                du = torch.tensor(np.ascontiguousarray(vel), device="cuda")
+                dg = torch.zeros((m.numel, 3, 3), dtype=torch.float64, device="cuda")
+                for _ in range(args.warmup + args.steps):
+                    plan.grad_device(lvel, prop, 3, du.data_ptr(), dg.data_ptr(), sptr)
+                torch.cuda.synchronize()
+                plan.close()
             elif args.profile == "partitioned":
                 from sfr3d_b200 import halo as H
                 lays = H.partition(N, s.ia, s.ja, True, 2)
@@ -1115,12 +1125,13 @@ def momentum_assembly_leg(np, torch, sv, s, n, peak, peak_kind):
 
 
 # algorithmic bytes per cell of the least-squares gradient kernel (6 faces):
-# per face the neighbour word (4) and 7 doubles (the matrix column, xmcc,
-# dcca), the cell's face count and material (4), its own u (8 ndf; the
-# neighbours' u come from cache), the previous gradient read and the new one
-# written (2 * 24 ndf)
+# per face the neighbour word (4) and the cell matrix's column for it (3
+# doubles; xmcc and dcca are read on boundary faces only), the cell's face
+# count and material (4), its own u (8 ndf; the neighbours' u come from
+# cache) and the new gradient written (24 ndf; least squares starts from zero
+# and does not read the previous one)
 def grad_alg_bytes(ndf):
-    return 6 * (4 + 56) + 4 + 8 * ndf + 48 * ndf
+    return 6 * (4 + 24) + 4 + 8 * ndf + 24 * ndf
 
 
 def gradient_inputs(np, s):
