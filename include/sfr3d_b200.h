@@ -490,6 +490,9 @@ typedef struct {
   int32_t adv_fn;      /* Advection.iCod2 for NVD: 1 BCD, 2 MUSCL, 3 SMART, 4 ModSMART,
                           5 SuperBee, 6 ModSuperBee, 7 STOIC, 8 MinMod, 9 ModBCD (nvd,
                           CellLib.c; MUSCL and STOIC weigh 0, as there) */
+  int32_t fwall;       /* Turbulence.fWall: walls (MOVEWALL, STATICWALL) take the wall
+                          model's viscosity mu yPlus / uPlus (mu where yPlus <= 0.01)
+                          from the field bound by sfr_gpu_vel_wall (Loads.c:300-313) */
 } sfr_vel_opts;
 
 int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,
@@ -499,11 +502,16 @@ int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t ico
  * 237-240): eddy[numel] eddy viscosity and stress[numel*6] the residual
  * stress tensor (xx, yy, zz, xy, yz, xz), either may be NULL.  on_device = 1:
  * device arrays, kept by pointer and read by every later call; 0: host
- * arrays, copied now into the plan.  The wall model (Turbulence.fWall) is not
- * built: walls use the effective viscosity, as the reference does without
- * it (Loads.c:300-313). */
+ * arrays, copied now into the plan.  Without the wall model (fwall, bound by
+ * sfr_gpu_vel_wall) walls use the effective viscosity (Loads.c:300-313). */
 int sfr_gpu_vel_turbulence(sfr_dif_plan *p, const double *eddy, const double *stress,
                            int32_t on_device);
+
+/* The wall model's per-cell parameters that momentum calls with fwall read
+ * (wallPar of systFormSimpleVel, CellLoopInc.c:322-324): wallpar[numel*4]
+ * = yPlus, uPlus, uFri, stressW per cell (the turbulence module computes
+ * them); on_device as for sfr_gpu_vel_turbulence.  NULL unbinds. */
+int sfr_gpu_vel_wall(sfr_dif_plan *p, const double *wallpar, int32_t on_device);
 
 /* One call on device arrays: pres (numel), gradpres, vel, dfield (numel*3),
  * gradvel (numel*9, row i = grad u_i) in; dfield (the new D), ad3 and b3

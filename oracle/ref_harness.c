@@ -391,7 +391,8 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int forces, int matrix, int calrcell, int unsym,
                                  int nthreads, int advcod, int fturb, int fstruc,
                                  const double *eddy_in, const double *stress_in,
-                                 double adv_beta, int adv_fn, double *seconds)
+                                 double adv_beta, int adv_fn, int fwall,
+                                 const double *wallpar_in, double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -427,7 +428,8 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   adv.iCod2 = (short)adv_fn;
   tmodel.fTurb = fturb != 0;
   tmodel.fTurbStruct = fstruc != 0;
-  tmodel.fWall = false;
+  tmodel.fWall = fwall != 0;
+  if (wallpar_in) memcpy(wallpar, wallpar_in, sizeof(double) * (size_t)numel * NWALLPAR);
   if (eddy_in) memcpy(eddy, eddy_in, sizeof(double) * (size_t)numel);
   if (stress_in) memcpy(stressr, stress_in, sizeof(double) * (size_t)numel * 6);
   diff.iCod = (short)icod;

@@ -1282,9 +1282,14 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
           if (l < 0 || l >= nlvel) return -1;
           ld = &lvel[l];
           if (ld->type == 8 || ld->type == 14) { /* MOVEWALL, STATICWALL */
+            double visc = effC;
+            if (o->fwall) { /* Loads.c:300-313: the wall model's viscosity */
+              const double yp = o->wallpar[4 * (long)nel], up = o->wallpar[4 * (long)nel + 1];
+              visc = yp > 0.01e0 ? muC * yp / up : muC;
+            }
             if (ld->type == 8)
               for (j = 0; j < 3; j++) tA[j] = ld->par[j];
-            move_wall(velC, tA, nrm, sPc, p, m->dcca[q], effC, area);
+            move_wall(velC, tA, nrm, sPc, p, m->dcca[q], visc, area);
           } else if (ld->type == 6) { /* INLET */
             double wfn, ss[6], tr, mflux;
             if (ld->var != 0) return -2;

@@ -154,11 +154,13 @@ typedef struct {
                         (advectiveScheme, CellLib.c:6394-6480) */
   double dt, dt0;
   double under;      /* underU (alphaVel) */
-  int fturb, fstruc; /* Turbulence.fTurb / fTurbStruct (no wall model) */
+  int fturb, fstruc; /* Turbulence.fTurb / fTurbStruct */
   const double *eddy;   /* numel eddy viscosity (fturb) */
   const double *stress; /* numel*6 residual stress xx yy zz xy yz xz (fstruc) */
   double adv_beta;      /* Advection.par[0]: LUST weight (adv 6) */
   int adv_fn;           /* Advection.iCod2: NVD function 1..9 (adv 5) */
+  int fwall;            /* Turbulence.fWall: the wall model's viscosity on walls */
+  const double *wallpar; /* numel*NWALLPAR (yPlus, uPlus, uFri, stressW) (fwall) */
 } orc_vel_opts;
 
 /* m->facer is faceVelR (velocity loads; a cell flagged there has no

@@ -43,7 +43,7 @@ class VelOptsC(ctypes.Structure):
                 ("type_simple", _I32), ("time_flag", _I32), ("time_type", _I32),
                 ("adv", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
                 ("under", ctypes.c_double), ("fturb", _I32), ("fstruc", _I32),
-                ("adv_beta", ctypes.c_double), ("adv_fn", _I32)]
+                ("adv_beta", ctypes.c_double), ("adv_fn", _I32), ("fwall", _I32)]
 
 
 class LoadC(ctypes.Structure):
@@ -75,6 +75,7 @@ def _lib():
         L.sfr_gpu_vel_plan_create.argtypes = [_P, ctypes.POINTER(DifMeshC), _I32,
                                               ctypes.POINTER(_P)]
         L.sfr_gpu_vel_turbulence.argtypes = [_P, _P, _P, _I32]
+        L.sfr_gpu_vel_wall.argtypes = [_P, _P, _I32]
         L.sfr_gpu_vel_assemble.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)] + [_P] * 9
                                            + [_I32] * 3)
         L.sfr_gpu_vel_assemble_device.argtypes = ([_P, _P, _I32, ctypes.POINTER(VelOptsC)]
@@ -329,11 +330,24 @@ class VelPlan(DifPlan):
         if rc != _sv.OK:
             raise _sv.SolverError(rc, "sfr_gpu_vel_turbulence: " + _sv.last_error())
 
+    def wall(self, wallpar=None, on_device: bool = False) -> None:
+        """Bind the wall model's parameters (numel, 4: yPlus, uPlus, uFri,
+        stressW) that later calls with fwall read: a host array (copied now)
+        or a device pointer (int, kept)."""
+        if on_device:
+            rc = _lib().sfr_gpu_vel_wall(self.h, wallpar or None, 1)
+        else:
+            w = None if wallpar is None else _c(wallpar, np.float64)
+            rc = _lib().sfr_gpu_vel_wall(self.h, _ptr(w), 0)
+        if rc != _sv.OK:
+            raise _sv.SolverError(rc, "sfr_gpu_vel_wall: " + _sv.last_error())
+
     def _vopts(self, fso, fvisc, fres, type_simple, time, under, adv=1, fturb=False,
-               fstruc=False, adv_beta=0.25, adv_fn=1):
+               fstruc=False, adv_beta=0.25, adv_fn=1, fwall=False):
         o = VelOptsC(icod=self.icod, fso=int(fso), fvisc=int(fvisc), fres=int(fres),
                      type_simple=type_simple, under=under, adv=int(adv), fturb=int(fturb),
-                     fstruc=int(fstruc), adv_beta=float(adv_beta), adv_fn=int(adv_fn))
+                     fstruc=int(fstruc), adv_beta=float(adv_beta), adv_fn=int(adv_fn),
+                     fwall=int(fwall))
         if time is not None:
             o.time_flag = 1
             o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
@@ -342,7 +356,7 @@ class VelPlan(DifPlan):
     def assemble(self, lvel, prop, pres, gradpres, vel, gradvel, dfield, fso=True,
                  fvisc=False, fres=True, type_simple=SIMPLE, time=None, under=0.7,
                  forces=True, matrix=True, calrcell=True, adv=FOUP, fturb=False, fstruc=False,
-                 adv_beta=0.25, adv_fn=1):
+                 adv_beta=0.25, adv_fn=1, fwall=False):
         """One call with host arrays: returns (ad3, b3, rcell3, dfield), each
         component block after the other (u, v, w).  adv: FOUP, CD, SOUP or LUST
         (weight adv_beta);
@@ -355,7 +369,7 @@ class VelPlan(DifPlan):
         rc3 = np.empty(3 * self.numel) if calrcell else None
         lv = _loads_c(lvel)
         o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc, adv_beta,
-                        adv_fn)
+                        adv_fn, fwall)
         rc = _lib().sfr_gpu_vel_assemble(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), *[_ptr(a) for a in arrs],
             _ptr(df), _ptr(ad3), _ptr(b3), _ptr(rc3), int(forces), int(matrix), int(calrcell))
@@ -370,11 +384,11 @@ class VelPlan(DifPlan):
                         d_rcell3: int = 0, fso=True, fvisc=False, fres=True,
                         type_simple=SIMPLE, time=None, under=0.7, forces=True, matrix=True,
                         calrcell=True, stream: int = 0, adv=FOUP, fturb=False, fstruc=False,
-                        adv_beta=0.25, adv_fn=1):
+                        adv_beta=0.25, adv_fn=1, fwall=False):
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         lv = _loads_c(lvel)
         o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc, adv_beta,
-                        adv_fn)
+                        adv_fn, fwall)
         rc = _lib().sfr_gpu_vel_assemble_device(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), d_pres, d_gradpres, d_vel,
             d_gradvel, d_dfield, d_ad3 or None, d_b3 or None, d_rcell3 or None, int(forces),

@@ -680,6 +680,8 @@ struct VelOpts {
   const double *eddy, *stress;  // numel, numel*6 (device)
   double beta;  // LUST weight
   int nvd;      // NVD function
+  int fwall;    // the wall model's viscosity on walls
+  const double *wall;  // numel*4: yPlus, uPlus, uFri, stressW (device)
 };
 
 // nvd (CellLib.c): the two weights of an NVD function at phi~; the
@@ -990,7 +992,13 @@ __global__ void __launch_bounds__(256, 2)
         if (L.type == 8 || L.type == 14) {  // MOVEWALL, STATICWALL
           const double vB[3] = {L.type == 8 ? L.par[0] : 0.0, L.type == 8 ? L.par[1] : 0.0,
                                 L.type == 8 ? L.par[2] : 0.0};
-          move_wall(velC, vB, n, sPc, pp, dcca, effC, area);
+          double visc = effC;
+          if (kExt && o.fwall) {  // the wall model's viscosity (Loads.c:300-313)
+            const double yp = o.wall[4 * static_cast<size_t>(cell)];
+            const double up = o.wall[4 * static_cast<size_t>(cell) + 1];
+            visc = yp > 0.01e0 ? xdiv(xmul(muC, yp), up) : muC;
+          }
+          move_wall(velC, vB, n, sPc, pp, dcca, visc, area);
         } else if (L.type == 6) {  // INLET
           const double tA[3] = {L.par[0], L.par[1], L.par[2]};
           double wfn = xadd(xmul(tA[0], n[0]), xmul(tA[1], n[1]));
@@ -1165,6 +1173,8 @@ struct sfr_dif_plan {
   // own copies of host arrays)
   const double *t_eddy = nullptr, *t_stress = nullptr;
   double *own_eddy = nullptr, *own_stress = nullptr;
+  const double *t_wall = nullptr;  // the wall model's per-cell parameters
+  double *own_wall = nullptr;
 };
 
 namespace {
@@ -1212,6 +1222,7 @@ void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->h_rcell);
   cudaFree(p->own_eddy);
   cudaFree(p->own_stress);
+  cudaFree(p->own_wall);
 }
 
 void fill_load(sfr::DevLoad *d, const sfr_load &L) {
@@ -1728,10 +1739,12 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if (o->adv == 4 && (o->adv_fn < 1 || o->adv_fn > 5)) return bad("adv_fn: TVD limiter 1..5");
   if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
     return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
+  if (o->fwall && !p->t_wall) return bad("fwall set without the field bound by sfr_gpu_vel_wall");
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
                   o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv, o->fturb != 0,
-                  o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta, o->adv_fn};
+                  o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta, o->adv_fn,
+                  o->fwall != 0, p->t_wall};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =
@@ -1741,7 +1754,7 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
                                    d_gradpres, d_vel, d_gradvel, d_dfield, s->d_stage,
                                    s->d_diag, d_ad3, d_b3, d_rcell3, p->numel);
   };
-  const bool ext = vo.adv != 1 || vo.fturb || vo.fstruc;
+  const bool ext = vo.adv != 1 || vo.fturb || vo.fstruc || vo.fwall;
   if (p->d.maxviz == 6)
     ext ? launch(sfr::vel_assemble_kernel<6, true>) : launch(sfr::vel_assemble_kernel<6, false>);
   else
@@ -1828,6 +1841,21 @@ int sfr_gpu_vel_turbulence(sfr_dif_plan *p, const double *eddy, const double *st
     SFR_CUA(cudaMemcpy(p->own_stress, stress, sizeof(double) * ne * 6, cudaMemcpyHostToDevice));
     p->t_stress = p->own_stress;
   }
+  return SFR_OK;
+}
+
+int sfr_gpu_vel_wall(sfr_dif_plan *p, const double *wallpar, int32_t on_device) {
+  if (!p) return bad("NULL argument");
+  if (p->kind != 2) return bad("not a momentum plan");
+  SFR_CUA(cudaSetDevice(p->device));
+  if (on_device || !wallpar) {
+    p->t_wall = wallpar;
+    return SFR_OK;
+  }
+  const size_t bytes = sizeof(double) * 4 * static_cast<size_t>(p->numel);
+  if (!p->own_wall) SFR_CUA(cudaMalloc(&p->own_wall, bytes));
+  SFR_CUA(cudaMemcpy(p->own_wall, wallpar, bytes, cudaMemcpyHostToDevice));
+  p->t_wall = p->own_wall;
   return SFR_OK;
 }
 

@@ -406,6 +406,52 @@ def test_vel_oracle_inlet_static_pressure_direction():
         np.testing.assert_allclose(db[:, row], want, rtol=1e-12, atol=1e-14)
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_vel_oracle_wall_model_matches_reference_live():
+    """The wall model's viscosity on MOVEWALL / STATICWALL faces
+    (Turbulence.fWall, Loads.c:300-313): mu yPlus / uPlus where yPlus > 0.01,
+    else mu, from a given per-cell (yPlus, uPlus, uFri, stressW) field, with
+    and without an eddy viscosity, against the reference's own
+    systFormSimpleVel on every layout."""
+    s = S.poisson_jittered(5, seed=14)
+    m = s.mesh()
+    rng = np.random.default_rng(15)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+            O.Load(O.OUTLET, ())]
+    wall = np.stack([rng.uniform(0.0, 40.0, m.numel), rng.uniform(1.0, 20.0, m.numel),
+                     rng.uniform(0.0, 1.0, m.numel), rng.uniform(0.0, 1.0, m.numel)], axis=1)
+    wall[::3, 0] = rng.uniform(0.0, 0.01, len(wall[::3]))  # below the threshold: mu
+    for eddy, adv in itertools.product((None, rng.uniform(0.0, 5e-3, m.numel)),
+                                       (O.FOUP, O.SOUP)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 2, 1, 3, 1, 2]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop, mat=mat,
+                         pres=rng.standard_normal(m.numel),
+                         gradpres=rng.standard_normal((m.numel, 3)),
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)),
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7, adv=adv,
+                         eddy=eddy, wallpar=wall)
+        for name, (st, un, ia_, ja_, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (eddy is None, adv, name)
+    # the wall model changes the walls' diagonal share
+    off = O.vel_assemble(O.VelCase(**{**case.__dict__, "wallpar": None}), O.CSRD, True, s.ia,
+                         s.ja, s.neq)
+    on = O.vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+    assert not np.array_equal(off[2], on[2])
+
+
 def test_vel_oracle_rejects_what_it_does_not_restate():
     s = S.poisson_uniform(4, seed=1)
     m = s.mesh()

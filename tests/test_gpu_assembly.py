@@ -595,6 +595,66 @@ def test_vel_turbulence_matches_oracle(cuda, box):
         gs.close()
 
 
+def test_vel_wall_model_matches_oracle(cuda, box):
+    """The wall model's viscosity on walls (fwall), with the parameters bound
+    as a host array or a device array, with and without an eddy viscosity:
+    bit-identical to the oracle (itself pinned to the reference)."""
+    import torch
+    s, m, lay = box
+    rng = np.random.default_rng(72)
+    prop = np.zeros((2, O.MAXPROP))
+    prop[:, 0] = (1e-3, 2e-3)
+    prop[:, 1] = (1.0, 1.2)
+    mat = rng.integers(1, 3, m.numel).astype(np.int16)
+    cc = _centres(m)
+    fv = m.face_r([1, 2, 1, 3, 1, 2])
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0)),
+            O.Load(O.OUTLET, ())]
+    wall = np.stack([rng.uniform(0.0, 40.0, m.numel), rng.uniform(1.0, 20.0, m.numel),
+                     rng.uniform(0.0, 1.0, m.numel), rng.uniform(0.0, 1.0, m.numel)], axis=1)
+    wall[::3, 0] = rng.uniform(0.0, 0.01, len(wall[::3]))
+    eddy = rng.uniform(0.0, 5e-3, m.numel)
+    d_wall = torch.tensor(wall, device="cuda")
+    for name in ("csrd_full", "csrc_unsym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.VelPlan(gs, m, fv, cc, icod=4, mat=mat, nmat=2)
+        with pytest.raises(sv.SolverError):  # nothing bound yet
+            plan.assemble(_aloads(lvel), prop, np.zeros(m.numel), np.zeros((m.numel, 3)),
+                          np.zeros((m.numel, 3)), np.zeros((m.numel, 3, 3)),
+                          np.ones((m.numel, 3)), fwall=True)
+        plan.turbulence(eddy)
+        for on_device, te in itertools.product((False, True), (False, True)):
+            if on_device:
+                plan.wall(d_wall.data_ptr(), on_device=True)
+            else:
+                plan.wall(wall)
+            case = O.VelCase(mesh=m, cc=cc, facevelr=fv, facepresr=m.face_r([0] * 6),
+                             lvel=lvel, prop=prop, mat=mat, pres=rng.standard_normal(m.numel),
+                             gradpres=rng.standard_normal((m.numel, 3)),
+                             vel=rng.standard_normal((m.numel, 3)),
+                             gradvel=rng.standard_normal((m.numel, 3, 3)),
+                             dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7,
+                             eddy=eddy if te else None, wallpar=wall)
+            want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
+            assert want[0] == 0
+            n = gs._nsrc()
+            split = st == sv.CSRC and un
+            gs.set_values(np.zeros(n // 2 if split else n), np.zeros(s.neq),
+                          np.zeros(n // 2) if split else None)
+            ad3, b3, rc3, df = plan.assemble(_aloads(lvel), prop, case.pres, case.gradpres,
+                                             case.vel, case.gradvel, case.dfield, under=0.7,
+                                             fturb=te, fwall=True)
+            al, ad, au = A.get_values(gs)
+            a = al if au is None else np.concatenate([al, au])
+            what = (name, on_device, te)
+            assert bits_equal(a, want[1]), what
+            assert bits_equal(ad3, want[2]) and bits_equal(b3, want[3]), what
+            assert bits_equal(rc3, want[4]) and bits_equal(df, want[5]), what
+        plan.close()
+        gs.close()
+
+
 def test_vel_assembled_momentum_solves_like_reference(cuda):
     """A lid-driven cavity's momentum system assembled and solved (u, v, w
     with their own diagonals) on the device."""
