@@ -493,6 +493,13 @@ typedef struct {
   int32_t fwall;       /* Turbulence.fWall: walls (MOVEWALL, STATICWALL) take the wall
                           model's viscosity mu yPlus / uPlus (mu where yPlus <= 0.01)
                           from the field bound by sfr_gpu_vel_wall (Loads.c:300-313) */
+  int32_t rhie;        /* MomentumModel.fRhieChowInt: 1 Rhie-Chow face velocities
+                          (interpolFaceVel, CellLib.c:6853-6960) reading the D field
+                          as it was at the call's start, for every cell -- a defined,
+                          order-independent form; the reference's serial loop reads
+                          the D it has already rewritten for lower-numbered
+                          neighbours, so its result depends on the cell order.
+                          0 off; other values SFR_UNSUPPORTED */
 } sfr_vel_opts;
 
 int sfr_gpu_vel_plan_create(sfr_system *s, const sfr_dif_mesh *mesh, int32_t icod,

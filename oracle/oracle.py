@@ -601,6 +601,7 @@ class VelCase:
     adv_beta: float = 0.25             # Advection.par[0]: LUST weight
     adv_fn: int = 1                    # Advection.iCod2: NVD function (1 BCD .. 9 ModBCD)
     wallpar: np.ndarray | None = None  # (numel, 4) yPlus, uPlus, uFri, stressW: Turbulence.fWall
+    rhie: int = 0                      # fRhieChowInt: 1 D from the call's start, 2 serial order
 
     def material(self):
         mat = (np.ones(self.mesh.numel, np.int16) if self.mat is None
@@ -618,7 +619,7 @@ class _VelOpts(ctypes.Structure):
                 ("dt", ctypes.c_double), ("dt0", ctypes.c_double), ("under", ctypes.c_double),
                 ("fturb", ctypes.c_int), ("fstruc", ctypes.c_int), ("eddy", _P), ("stress", _P),
                 ("adv_beta", ctypes.c_double), ("adv_fn", ctypes.c_int),
-                ("fwall", ctypes.c_int), ("wallpar", _P)]
+                ("fwall", ctypes.c_int), ("wallpar", _P), ("rhie", ctypes.c_int)]
 
 
 def _vel_out(storage, unsym, neq, ia, ja, numel, fill):
@@ -659,6 +660,7 @@ def vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, matrix
     o.adv_fn = case.adv_fn
     wall = None if case.wallpar is None else _c(case.wallpar, np.float64)
     o.fwall, o.wallpar = int(wall is not None), None if wall is None else _p(wall)
+    o.rhie = int(case.rhie)
     ia, ja = _c(ia, np.int32), _c(ja, np.int32)
     a, ad, b, rc_ = _vel_out(storage, unsym, neq, ia, ja, m.numel, fill)
     dfield = np.array(case.dfield, dtype=np.float64, copy=True, order="C")
@@ -686,7 +688,7 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         lib.sfr_ref_syst_form_simple_vel.argtypes = (
             [ctypes.c_int, ctypes.c_int] + [_P] * 33 + [ctypes.c_int] + [_P] * 5
             + [ctypes.c_int] * 7 + [ctypes.c_double] * 3 + [ctypes.c_int] * 11 + [_P] * 2
-            + [ctypes.c_double, ctypes.c_int, ctypes.c_int, _P, _P])
+            + [ctypes.c_double, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P])
         lib._vel_typed = True
     cal, mat = case.material()
     cp = lambda x, dt: np.array(x, dtype=dt, copy=True, order="C")  # noqa: E731
@@ -716,7 +718,8 @@ def ref_vel_assemble(case: VelCase, storage, unsym, ia, ja, neq, forces=True, ma
         case.adv, int(eddy is not None), int(stress is not None),
         None if eddy is None else _p(eddy), None if stress is None else _p(stress),
         case.adv_beta, case.adv_fn, int(case.wallpar is not None),
-        None if case.wallpar is None else _p(cp(case.wallpar, np.float64)), ctypes.byref(sec))
+        None if case.wallpar is None else _p(cp(case.wallpar, np.float64)), int(case.rhie),
+        ctypes.byref(sec))
     return rc, a, ad, b, rcell, dfield, sec.value
 
 

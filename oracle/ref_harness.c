@@ -392,7 +392,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
                                  int nthreads, int advcod, int fturb, int fstruc,
                                  const double *eddy_in, const double *stress_in,
                                  double adv_beta, int adv_fn, int fwall,
-                                 const double *wallpar_in, double *seconds)
+                                 const double *wallpar_in, int rhie, double *seconds)
 {
   INT *el = calloc((size_t)numel * 8, sizeof(INT));
   short *nen = malloc((size_t)numel * sizeof(short));
@@ -434,7 +434,7 @@ int sfr_ref_syst_form_simple_vel(int numel, int maxviz, int *nelcon, short *nfac
   if (stress_in) memcpy(stressr, stress_in, sizeof(double) * (size_t)numel * 6);
   diff.iCod = (short)icod;
   mm.fRes = fres != 0;
-  mm.fRhieChowInt = false;
+  mm.fRhieChowInt = rhie != 0;
   mm.fViscosity = fvisc != 0;
   mm.fSoPressure = fso != 0;
   ddt.flag = time_flag != 0;

@@ -1064,13 +1064,15 @@ static void struct_integral(const double *rc, const double *rv, const double *n,
   p[2] -= area * (s[5] * n[0] + s[4] * n[1] + s[2] * n[2]);
 }
 
-int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
-                     const double *xm, const orc_load *lvel, int nlvel,
-                     const orc_vel_opts *o, const double *prop, const double *pres,
-                     const double *gradpres, const double *vel, const double *gradvel,
-                     double *dfield, int storage, int unsym, int neq, int nad,
-                     const int *ia, const int *ja, double *a, double *ad, double *b,
-                     double *rcell, int forces, int matrix, int calrcell)
+/* dsnap: the D field at the call's start (Rhie-Chow), else NULL */
+static int vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
+                        const double *xm, const orc_load *lvel, int nlvel,
+                        const orc_vel_opts *o, const double *prop, const double *pres,
+                        const double *gradpres, const double *vel, const double *gradvel,
+                        double *dfield, int storage, int unsym, int neq, int nad,
+                        const int *ia, const int *ja, double *a, double *ad, double *b,
+                        double *rcell, int forces, int matrix, int calrcell,
+                        const double *dsnap)
 {
   enum { MAXF = 32 };
   const int mv = m->maxviz, numel = m->numel;
@@ -1152,6 +1154,21 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
         }
         density = am1 * rhoC + alpha * rhoV;
         wfn = wf[0] * nrm[0] + wf[1] * nrm[1] + wf[2] * nrm[2];
+        if (o->rhie) {
+          /* interpolFaceVel, ndm = 3 (CellLib.c:6853-6960) with the face D
+           * of CellSimple.c:339-350, both D values from the call's start */
+          const double *dd = dsnap ? dsnap : dfield;
+          double dF[3], gp[3], g0, g1, nk;
+          for (j = 0; j < 3; j++) {
+            dF[j] = am1 * dd[3 * (long)nel + j] + alpha * dd[3 * (long)nb + j];
+            gp[j] = am1 * gpC[j] + alpha * gpV[j];
+          }
+          g0 = (presV - presC) / mk;
+          nk = dF[0] * ksi[0] * nrm[0] + dF[1] * ksi[1] * nrm[1] + dF[2] * ksi[2] * nrm[2];
+          g1 = gp[0] * ksi[0] + gp[1] * ksi[1] + gp[2] * ksi[2];
+          g1 = (g1 - g0) * nk;
+          wfn += g1;
+        }
         for (i = 0; i < 3; i++) {
           gk = gf[i][0] * ksi[0] + gf[i][1] * ksi[1] + gf[i][2] * ksi[2];
           du = duDksi[i] - gk;
@@ -1430,6 +1447,28 @@ int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double
     }
   }
   return 0;
+}
+
+int orc_vel_assemble(const orc_dif_mesh *m, const short *facepresr, const double *cc,
+                     const double *xm, const orc_load *lvel, int nlvel,
+                     const orc_vel_opts *o, const double *prop, const double *pres,
+                     const double *gradpres, const double *vel, const double *gradvel,
+                     double *dfield, int storage, int unsym, int neq, int nad,
+                     const int *ia, const int *ja, double *a, double *ad, double *b,
+                     double *rcell, int forces, int matrix, int calrcell)
+{
+  double *dsnap = NULL;
+  int rc, i;
+  if (o->rhie == 1) { /* the D field every face velocity reads: the call's start */
+    dsnap = (double *)malloc(sizeof(double) * 3 * (size_t)(m->numel > 0 ? m->numel : 1));
+    if (!dsnap) return -1;
+    for (i = 0; i < 3 * m->numel; i++) dsnap[i] = dfield[i];
+  }
+  rc = vel_assemble(m, facepresr, cc, xm, lvel, nlvel, o, prop, pres, gradpres, vel, gradvel,
+                    dfield, storage, unsym, neq, nad, ia, ja, a, ad, b, rcell, forces, matrix,
+                    calrcell, dsnap);
+  free(dsnap);
+  return rc;
 }
 
 /* ---- the MPI path (test infrastructure) ------------------------------- */

@@ -161,6 +161,11 @@ typedef struct {
   int adv_fn;           /* Advection.iCod2: NVD function 1..9 (adv 5) */
   int fwall;            /* Turbulence.fWall: the wall model's viscosity on walls */
   const double *wallpar; /* numel*NWALLPAR (yPlus, uPlus, uFri, stressW) (fwall) */
+  int rhie;             /* MomentumModel.fRhieChowInt: 1 order-independent, every
+                           cell's face velocity reads the D field as it was at the
+                           call's start; 2 the reference's serial loop, which reads
+                           the D it has already rewritten for lower-numbered
+                           neighbours (CellLoopInc.c:301, 364) */
 } orc_vel_opts;
 
 /* m->facer is faceVelR (velocity loads; a cell flagged there has no

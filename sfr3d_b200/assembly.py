@@ -43,7 +43,8 @@ class VelOptsC(ctypes.Structure):
                 ("type_simple", _I32), ("time_flag", _I32), ("time_type", _I32),
                 ("adv", _I32), ("dt", ctypes.c_double), ("dt0", ctypes.c_double),
                 ("under", ctypes.c_double), ("fturb", _I32), ("fstruc", _I32),
-                ("adv_beta", ctypes.c_double), ("adv_fn", _I32), ("fwall", _I32)]
+                ("adv_beta", ctypes.c_double), ("adv_fn", _I32), ("fwall", _I32),
+                ("rhie", _I32)]
 
 
 class LoadC(ctypes.Structure):
@@ -343,11 +344,11 @@ class VelPlan(DifPlan):
             raise _sv.SolverError(rc, "sfr_gpu_vel_wall: " + _sv.last_error())
 
     def _vopts(self, fso, fvisc, fres, type_simple, time, under, adv=1, fturb=False,
-               fstruc=False, adv_beta=0.25, adv_fn=1, fwall=False):
+               fstruc=False, adv_beta=0.25, adv_fn=1, fwall=False, rhie=0):
         o = VelOptsC(icod=self.icod, fso=int(fso), fvisc=int(fvisc), fres=int(fres),
                      type_simple=type_simple, under=under, adv=int(adv), fturb=int(fturb),
                      fstruc=int(fstruc), adv_beta=float(adv_beta), adv_fn=int(adv_fn),
-                     fwall=int(fwall))
+                     fwall=int(fwall), rhie=int(rhie))
         if time is not None:
             o.time_flag = 1
             o.time_type, o.dt, o.dt0 = int(time[0]), float(time[1]), float(time[2])
@@ -356,7 +357,7 @@ class VelPlan(DifPlan):
     def assemble(self, lvel, prop, pres, gradpres, vel, gradvel, dfield, fso=True,
                  fvisc=False, fres=True, type_simple=SIMPLE, time=None, under=0.7,
                  forces=True, matrix=True, calrcell=True, adv=FOUP, fturb=False, fstruc=False,
-                 adv_beta=0.25, adv_fn=1, fwall=False):
+                 adv_beta=0.25, adv_fn=1, fwall=False, rhie=0):
         """One call with host arrays: returns (ad3, b3, rcell3, dfield), each
         component block after the other (u, v, w).  adv: FOUP, CD, SOUP or LUST
         (weight adv_beta);
@@ -369,7 +370,7 @@ class VelPlan(DifPlan):
         rc3 = np.empty(3 * self.numel) if calrcell else None
         lv = _loads_c(lvel)
         o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc, adv_beta,
-                        adv_fn, fwall)
+                        adv_fn, fwall, rhie)
         rc = _lib().sfr_gpu_vel_assemble(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), *[_ptr(a) for a in arrs],
             _ptr(df), _ptr(ad3), _ptr(b3), _ptr(rc3), int(forces), int(matrix), int(calrcell))
@@ -384,11 +385,11 @@ class VelPlan(DifPlan):
                         d_rcell3: int = 0, fso=True, fvisc=False, fres=True,
                         type_simple=SIMPLE, time=None, under=0.7, forces=True, matrix=True,
                         calrcell=True, stream: int = 0, adv=FOUP, fturb=False, fstruc=False,
-                        adv_beta=0.25, adv_fn=1, fwall=False):
+                        adv_beta=0.25, adv_fn=1, fwall=False, rhie=0):
         prop = np.ascontiguousarray(prop, np.float64).reshape(-1, MAXPROP)
         lv = _loads_c(lvel)
         o = self._vopts(fso, fvisc, fres, type_simple, time, under, adv, fturb, fstruc, adv_beta,
-                        adv_fn, fwall)
+                        adv_fn, fwall, rhie)
         rc = _lib().sfr_gpu_vel_assemble_device(
             self.h, lv, len(lvel), ctypes.byref(o), _ptr(prop), d_pres, d_gradpres, d_vel,
             d_gradvel, d_dfield, d_ad3 or None, d_b3 or None, d_rcell3 or None, int(forces),

@@ -682,6 +682,8 @@ struct VelOpts {
   int nvd;      // NVD function
   int fwall;    // the wall model's viscosity on walls
   const double *wall;  // numel*4: yPlus, uPlus, uFri, stressW (device)
+  int rhie;     // Rhie-Chow face velocity, D from the call's start
+  const double *dold;  // numel*3: that D (a copy made before the launch)
 };
 
 // nvd (CellLib.c): the two weights of an NVD function at phi~; the
@@ -922,7 +924,20 @@ __global__ void __launch_bounds__(256, 2)
                               : xdiv(1.0, xadd(xdiv(alpha, effC), xdiv(am1, effV)));
       const double dfd = xdiv(xmul(visc, modE), mk);
       const double density = xadd(xmul(am1, rhoC), xmul(alpha, rhoV));
-      const double wfn = dot3(wf, n);
+      double wfn = dot3(wf, n);
+      if (kExt && o.rhie) {
+        // interpolFaceVel, ndm = 3 (CellLib.c:6853-6960) with the face D of
+        // CellSimple.c:339-350, both D values as they were at the call's start
+        double dF[3], gp[3];
+        for (int j = 0; j < 3; ++j) {
+          dF[j] = xadd(xmul(am1, o.dold[c3 + j]), xmul(alpha, o.dold[v3 + j]));
+          gp[j] = xadd(xmul(am1, gpC[j]), xmul(alpha, gradp[v3 + j]));
+        }
+        const double g0 = xdiv(xsub(pres[c], presC), mk);
+        const double nk = xadd(xadd(xmul(xmul(dF[0], ksi[0]), n[0]), xmul(xmul(dF[1], ksi[1]), n[1])),
+                               xmul(xmul(dF[2], ksi[2]), n[2]));
+        wfn = xadd(wfn, xmul(xsub(dot3(gp, ksi), g0), nk));
+      }
       const double cv = xmul(xmul(density, wfn), area);
       la[f] = xsub(dfd, cv < 0.0 ? cv : 0.0);
       sP = xadd(sP, cv);
@@ -1175,6 +1190,7 @@ struct sfr_dif_plan {
   double *own_eddy = nullptr, *own_stress = nullptr;
   const double *t_wall = nullptr;  // the wall model's per-cell parameters
   double *own_wall = nullptr;
+  double *dsnap = nullptr;         // Rhie-Chow: the D field at a call's start
 };
 
 namespace {
@@ -1223,6 +1239,7 @@ void free_plan_buffers(sfr_dif_plan *p) {
   cudaFree(p->own_eddy);
   cudaFree(p->own_stress);
   cudaFree(p->own_wall);
+  cudaFree(p->dsnap);
 }
 
 void fill_load(sfr::DevLoad *d, const sfr_load &L) {
@@ -1740,11 +1757,20 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
   if ((o->fturb && !p->t_eddy) || (o->fstruc && !p->t_stress))
     return bad("fturb / fstruc set without the field bound by sfr_gpu_vel_turbulence");
   if (o->fwall && !p->t_wall) return bad("fwall set without the field bound by sfr_gpu_vel_wall");
+  if (o->rhie < 0 || o->rhie > 1)
+    return unsupported("rhie: 0 off, 1 D from the call's start (the reference's serial order, in "
+                       "which a cell reads its lower-numbered neighbours' new D, is not restated "
+                       "on the device)");
+  if (o->rhie) {  // every face velocity reads D as it was before this call
+    if (!p->dsnap) SFR_CUA(cudaMalloc(&p->dsnap, sizeof(double) * 3 * p->numel));
+    SFR_CUA(cudaMemcpyAsync(p->dsnap, d_dfield, sizeof(double) * 3 * p->numel,
+                            cudaMemcpyDeviceToDevice, st));
+  }
   sfr::VelOpts vo{o->fso != 0, o->fvisc != 0, o->fres != 0, o->type_simple == 2,
                   o->time_flag != 0, o->time_type, forces != 0, matrix != 0, calrcell != 0,
                   o->dt, o->dt0, o->under, o->adv == 0 ? 1 : o->adv, o->fturb != 0,
                   o->fstruc != 0, p->t_eddy, p->t_stress, o->adv_beta, o->adv_fn,
-                  o->fwall != 0, p->t_wall};
+                  o->fwall != 0, p->t_wall, o->rhie != 0, p->dsnap};
   const int blocks = (s->n + 255) / 256;
   const auto *loads_d = reinterpret_cast<const sfr::DevLoad *>(p->d_table);
   const auto *mtab =
@@ -1754,7 +1780,7 @@ int sfr_gpu_vel_assemble_device(sfr_dif_plan *p, const sfr_load *lvel, int32_t n
                                    d_gradpres, d_vel, d_gradvel, d_dfield, s->d_stage,
                                    s->d_diag, d_ad3, d_b3, d_rcell3, p->numel);
   };
-  const bool ext = vo.adv != 1 || vo.fturb || vo.fstruc || vo.fwall;
+  const bool ext = vo.adv != 1 || vo.fturb || vo.fstruc || vo.fwall || vo.rhie;
   if (p->d.maxviz == 6)
     ext ? launch(sfr::vel_assemble_kernel<6, true>) : launch(sfr::vel_assemble_kernel<6, false>);
   else

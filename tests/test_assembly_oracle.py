@@ -452,6 +452,56 @@ def test_vel_oracle_wall_model_matches_reference_live():
     assert not np.array_equal(off[2], on[2])
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (needs the reference)")
+def test_vel_oracle_rhie_chow_matches_reference_live():
+    """Rhie-Chow face velocities in the momentum system (fRhieChowInt,
+    interpolFaceVel, CellLib.c:6853-6960).  The reference's serial loop
+    rewrites each cell's D as it goes, so a cell reads the new D of its
+    lower-numbered neighbours and the old D of the others.  The oracle's
+    serial mode (rhie 2) reads D the same way and matches the reference's
+    systFormSimpleVel bit for bit on every cell and layout; the defined,
+    order-independent variant the device runs (rhie 1: every D from the
+    call's start) matches it wherever the two read the same D -- the first
+    cell, which has no lower-numbered neighbour -- and differs elsewhere."""
+    s = S.poisson_jittered(5, seed=16)
+    m = s.mesh()
+    rng = np.random.default_rng(17)
+    lay = layouts(s)
+    ia, ja, _ = s.csrc()
+    lay["csrc_unsym"] = (O.CSRC, True, ia, ja, None, None)
+    del lay["ellpack"]
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0))]
+    for adv, ts in itertools.product((O.FOUP, O.SOUP), (O.SIMPLE, O.SIMPLEC)):
+        case = O.VelCase(mesh=m, cc=_cell_centres(m), facevelr=m.face_r([1, 1, 1, 1, 1, 2]),
+                         facepresr=m.face_r([0] * 6), lvel=lvel, prop=prop,
+                         pres=rng.standard_normal(m.numel) * 0.1,
+                         gradpres=rng.standard_normal((m.numel, 3)) * 0.1,
+                         vel=rng.standard_normal((m.numel, 3)),
+                         gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.1,
+                         dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7, adv=adv,
+                         type_simple=ts, rhie=2)
+        for name, (st, un, ia_, ja_, _al, _au) in lay.items():
+            r1 = O.vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            r2 = O.ref_vel_assemble(case, st, un, ia_, ja_, s.neq, fill=3.0)
+            assert r1[0] == r2[0] == 0
+            for x, y in zip(r1[1:], r2[1:6]):
+                assert bits_equal(x, y), (adv, ts, name)
+        # the order-independent variant against the reference's serial result
+        r1 = O.vel_assemble(O.VelCase(**{**case.__dict__, "rhie": 1}), O.CSRD, True, s.ia, s.ja,
+                            s.neq)
+        r2 = O.ref_vel_assemble(case, O.CSRD, True, s.ia, s.ja, s.neq)
+        N, row0 = s.neq, m.id[0] - 1
+        assert bits_equal(r1[1][s.ia[row0]:s.ia[row0 + 1]], r2[1][s.ia[row0]:s.ia[row0 + 1]])
+        for k in range(3):
+            assert r1[2][k * N + row0] == r2[2][k * N + row0]
+            assert r1[3][k * N + row0] == r2[3][k * N + row0]
+            assert r1[4][k * m.numel] == r2[4][k * m.numel]
+        assert bits_equal(r1[5][0], r2[5][0])
+        assert not bits_equal(r1[5], r2[5])  # the other cells read other D values
+
+
 def test_vel_oracle_rejects_what_it_does_not_restate():
     s = S.poisson_uniform(4, seed=1)
     m = s.mesh()

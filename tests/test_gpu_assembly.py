@@ -655,6 +655,54 @@ def test_vel_wall_model_matches_oracle(cuda, box):
         gs.close()
 
 
+@pytest.mark.parametrize("adv", [O.FOUP, O.SOUP, O.TVD])
+def test_vel_rhie_chow_matches_oracle(cuda, box, adv):
+    """Rhie-Chow face velocities (rhie 1: every cell reads the D field as it
+    was at the call's start) on the device, bit for bit against the oracle's
+    same form, on every CSR layout; the new D field comes out as before.
+    The reference's serial order (rhie 2) is SFR_UNSUPPORTED on the device."""
+    s, m, lay = box
+    rng = np.random.default_rng(74 + adv)
+    prop = np.zeros((1, O.MAXPROP))
+    prop[0, :2] = (1e-3, 1.0)
+    cc = _centres(m)
+    fv = m.face_r([1, 1, 1, 1, 1, 2])
+    lvel = [O.Load(O.STATICWALL, ()), O.Load(O.MOVEWALL, (1.0, 0.2, -0.1, 0.0))]
+    for name in ("csrd_full", "csrd_sym", "csrc_sym", "csrc_unsym"):
+        st, un, ia, ja, _al, _au = lay[name]
+        gs = sv.GpuSystem(s.neq, ia, ja, st, un)
+        plan = A.VelPlan(gs, m, fv, cc, icod=4)
+        for ts in (A.SIMPLE, A.SIMPLEC):
+            case = O.VelCase(mesh=m, cc=cc, facevelr=fv, facepresr=m.face_r([0] * 6), lvel=lvel,
+                             prop=prop, pres=rng.standard_normal(m.numel) * 0.1,
+                             gradpres=rng.standard_normal((m.numel, 3)) * 0.1,
+                             vel=rng.standard_normal((m.numel, 3)),
+                             gradvel=rng.standard_normal((m.numel, 3, 3)) * 0.1,
+                             dfield=rng.uniform(0.1, 1, (m.numel, 3)), icod=4, under=0.7,
+                             adv=adv, adv_fn=1, type_simple=ts, rhie=1)
+            want = O.vel_assemble(case, st, un, ia, ja, s.neq, fill=0.0)
+            assert want[0] == 0
+            n = gs._nsrc()
+            split = st == sv.CSRC and un
+            gs.set_values(np.zeros(n // 2 if split else n), np.zeros(s.neq),
+                          np.zeros(n // 2) if split else None)
+            ad3, b3, rc3, df = plan.assemble(_aloads(lvel), prop, case.pres, case.gradpres,
+                                             case.vel, case.gradvel, case.dfield, under=0.7,
+                                             adv=adv, adv_fn=1, type_simple=ts, rhie=1)
+            al, ad, au = A.get_values(gs)
+            a = al if au is None else np.concatenate([al, au])
+            what = (name, ts)
+            assert bits_equal(a, want[1]), what
+            assert bits_equal(ad3, want[2]) and bits_equal(b3, want[3]), what
+            assert bits_equal(rc3, want[4]) and bits_equal(df, want[5]), what
+        with pytest.raises(sv.SolverError) as e:
+            plan.assemble(_aloads(lvel), prop, case.pres, case.gradpres, case.vel,
+                          case.gradvel, case.dfield, rhie=2)
+        assert e.value.status == sv.UNSUPPORTED
+        plan.close()
+        gs.close()
+
+
 def test_vel_assembled_momentum_solves_like_reference(cuda):
     """A lid-driven cavity's momentum system assembled and solved (u, v, w
     with their own diagonals) on the device."""
