@@ -1175,11 +1175,14 @@ def gradient_leg(np, torch, s, n, peak, peak_kind):
 
 def simple_step_leg(np, torch, sv, s, n):
     """The linear-algebra half of one SIMPLE iteration kept on the device:
-    momentum assembly, the u, v, w BiCGSTAB solves in one batched launch,
-    the pressure-correction assembly from the new D field, and its PCG solve
+    the velocity and pressure gradients (rcGradU, least squares), momentum
+    assembly, the u, v, w BiCGSTAB solves in one batched launch, the
+    pressure-correction assembly from the new D field, and its PCG solve
     (FP64 and mixed), with no host transfer between the steps."""
     from sfr3d_b200 import assembly as A
     m, prop, cc, f = vel_inputs(np, s)
+    gvel_plan = A.GradPlan(m, m.face_r(PRES_SIDES_VEL), type=A.RCLSQUARE)
+    gpres_plan = A.GradPlan(m, m.face_r(PRES_SIDES_PRES), type=A.RCLSQUARE)
     gv = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     gp = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     vplan = A.VelPlan(gv, m, m.face_r(PRES_SIDES_VEL), cc)
@@ -1192,13 +1195,19 @@ def simple_step_leg(np, torch, sv, s, n):
     d_ad3, d_b3, d_x3, d_bp, d_xp = z(3 * N), z(3 * N), z(3 * N), z(N), z(N)
     st = torch.cuda.Stream()
     sp = st.cuda_stream
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    out = {"workload": f"{n}^3 cavity: systFormSimpleVel + 3 momentum BiCGSTAB (one batched "
-                       "launch) + systFormSimplePres from the new D + pressure PCG, to 1e-10, "
-                       "all on the device"}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    out = {"workload": f"{n}^3 cavity: rcGradU (velocity, pressure; least squares) + "
+                       "systFormSimpleVel + 3 momentum BiCGSTAB (one batched launch) + "
+                       "systFormSimplePres from the new D + pressure PCG, to 1e-10, all on the "
+                       "device"}
     for prec, tag in ((sv.FP64, "fp64"), (sv.MIXED, "mixed")):
         for rep in range(2):  # the second pass is timed (graphs built, clocks up)
             with torch.cuda.stream(st):
+                ev[5].record(st)
+                gvel_plan.grad_device(lvel, prop, 3, dev["vel"].data_ptr(),
+                                      dev["gradvel"].data_ptr(), sp)
+                gpres_plan.grad_device(lpres, prop, 1, dev["pres"].data_ptr(),
+                                       dev["gradpres"].data_ptr(), sp)
                 ev[0].record(st)
                 vplan.assemble_device(lvel, prop, dev["pres"].data_ptr(),
                                       dev["gradpres"].data_ptr(), dev["vel"].data_ptr(),
@@ -1221,13 +1230,16 @@ def simple_step_leg(np, torch, sv, s, n):
                 ev[4].record(st)
             st.synchronize()
         t = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
-        out[tag] = {"total_ms": sum(t), "momentum_assembly_ms": t[0],
+        tg = ev[5].elapsed_time(ev[0])
+        out[tag] = {"total_ms": sum(t) + tg, "gradients_ms": tg, "momentum_assembly_ms": t[0],
                     "momentum_solves_ms": t[1], "pressure_assembly_ms": t[2],
                     "pressure_solve_ms": t[3], "momentum_iters": [i.iters for i in iv],
                     "pressure_iters": ip.iters,
                     "status": [i.status for i in iv] + [ip.status]}
     vplan.close()
     pplan.close()
+    gvel_plan.close()
+    gpres_plan.close()
     gv.close()
     gp.close()
     return out
@@ -1261,8 +1273,15 @@ def cpu_assembly(O, s):
     vrc, *_, vsec = O.ref_vel_assemble(vcase, O.CSRD, True, s.ia, s.ja, s.neq,
                                        nthreads=threads)
     # the same SIMPLE linear-algebra step on the host, the reference's way:
-    # its own assembly routines and its OpenMP solvers
+    # its own gradient reconstruction, assembly routines and OpenMP solvers
     t0 = time.perf_counter()
+    _grc, gvel, _l, _s = O.ref_rc_grad(O.GradCase(
+        mesh=m, facer=m.face_r(PRES_SIDES_VEL), loads=vcase.lvel, prop=prop, u=vcase.vel,
+        gradu=np.zeros((m.numel, 3, 3)), type=O.RCLSQUARE), nthreads=threads)
+    _grc, gpres, _l, _s = O.ref_rc_grad(O.GradCase(
+        mesh=m, facer=m.face_r(PRES_SIDES_PRES), loads=pcase.lpres, prop=prop, u=vcase.pres,
+        gradu=np.zeros((m.numel, 1, 3)), type=O.RCLSQUARE), nthreads=threads)
+    vcase = O.VelCase(**{**vcase.__dict__, "gradvel": gvel, "gradpres": gpres.reshape(-1, 3)})
     vr = O.ref_vel_assemble(O.VelCase(**{**vcase.__dict__, "fres": False}), O.CSRD, True,
                             s.ia, s.ja, s.neq, nthreads=threads, calrcell=False)
     N = s.neq
@@ -1271,7 +1290,8 @@ def cpu_assembly(O, s):
         r = O.ref_solve(O.PBICGSTAB, O.CSRD, True, s.ia, s.ja, vr[1], vr[2][k * N:(k + 1) * N],
                         vr[3][k * N:(k + 1) * N], tol=1e-10, nthreads=threads)
         mom_iters.append(r.iters)
-    pc2 = O.PresCase(**{**pcase.__dict__, "dfield": vr[5]})
+    pc2 = O.PresCase(**{**pcase.__dict__, "dfield": vr[5], "pres": vcase.pres,
+                        "gradpres": gpres.reshape(-1, 3), "vel": vcase.vel})
     pr = O.ref_pres_assemble(pc2, O.CSRD, True, s.ia, s.ja, N, nthreads=threads, calrcell=False)
     rp = O.ref_solve(O.PCG, O.CSRD, True, s.ia, s.ja, pr[1], pr[2], pr[3], tol=1e-10,
                      nthreads=threads)
@@ -1292,8 +1312,9 @@ def cpu_assembly(O, s):
     return {"ms": sec * 1e3, "threads": 1, "status": rc,
             "simple_step": {"ms": step_ms, "threads": threads, "momentum_iters": mom_iters,
                             "pressure_iters": rp.iters, "status": [vr[0], pr[0], rp.status],
-                            "sample": "systFormSimpleVel + 3 pbicgstabOmp + systFormSimplePres "
-                                      "+ pcgOmp, the device step's inputs"},
+                            "sample": "rcGradU (velocity, pressure) + systFormSimpleVel + 3 "
+                                      "pbicgstabOmp + systFormSimplePres + pcgOmp, the device "
+                                      "step's inputs"},
             "sample": "one full systFormDif call (the reference's loop is serial)",
             "pressure": {"ms": psec * 1e3, "threads": threads, "status": prc,
                          "sample": "one full systFormSimplePres call with its OpenMP cell "
