@@ -616,6 +616,19 @@ const char *sfr_last_error(void);
  * returns SFR_OK when the device can run it. */
 int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor);
 
+/* Self-test of the bounded device-side waits that replace the reference's
+ * blocking MPI collectives inside the solvers (no counterpart in the
+ * reference, whose MPI_Allreduce waits without a limit).  Four co-resident
+ * blocks meet once at one of the waits the engines use: kind 0 the grid
+ * barrier (persistent engine, fused iteration modes 1-2), kind 1 the
+ * fused iteration's tagged exchange (modes 3-6), kind 2 the resident
+ * engine's exchange.  The last `absent` blocks (0-3) leave before the wait.
+ * Returns SFR_OK when the wait completed (absent = 0) and SFR_TIMEOUT when
+ * it gave up after `spin_limit` polls because a participant never arrived;
+ * either way every block has left and the context stays usable.  Allocates
+ * 64 bytes (768 for kind 2) of device memory for the call. */
+int sfr_gpu_wait_selftest(int32_t kind, int32_t absent, uint32_t spin_limit, void *stream);
+
 /* ---- row partition over several GPUs (the reference's MPI path) ------ */
 
 /* The reference's interface map (Interface, include/Mesh.h:212-222), with

@@ -119,6 +119,14 @@ int sfr_gpu_check_device(int32_t device, int32_t *major, int32_t *minor) {
   return (ma == 10 && mi == 0) ? SFR_OK : SFR_UNSUPPORTED;
 }
 
+int sfr_gpu_wait_selftest(int32_t kind, int32_t absent, uint32_t spin_limit, void *stream) {
+  if (spin_limit == 0) return SFR_BAD_INPUT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (kind == 0 || kind == 1) return sfr::wait_selftest_fused(kind, absent, spin_limit, st);
+  if (kind == 2) return sfr::wait_selftest_resident(absent, spin_limit, st);
+  return SFR_BAD_INPUT;
+}
+
 int sfr_gpu_create(int32_t neq, int32_t nad, const int32_t *ia, const int32_t *ja,
                    int32_t storage, int32_t unsym, int32_t device, sfr_system **out) {
   if (!out) return SFR_BAD_INPUT;

@@ -146,6 +146,11 @@ int enqueue_team_mixed(sfr_system *s, int32_t solver, const double *d_b, double 
 // Resident engine (resident.cu): mixed PCG, one right-hand side, the
 // system's own diagonal.  resident_fits: the pattern and size allow it;
 // solve_resident returns SFR_UNSUPPORTED when the diagonal is not positive.
+// Self-tests of the bounded device-side waits (sfr_gpu_wait_selftest):
+// kind 0 grid_sync, 1 the fused iteration's tagged exchange; the resident
+// engine's exchange.
+int wait_selftest_fused(int32_t kind, int32_t absent, uint32_t spin_limit, cudaStream_t st);
+int wait_selftest_resident(int32_t absent, uint32_t spin_limit, cudaStream_t st);
 bool resident_fits(sfr_system *s);
 int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, uint32_t maxit,
                    int32_t newx, cudaStream_t st, sfr_solve_info *info);

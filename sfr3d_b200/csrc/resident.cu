@@ -551,7 +551,46 @@ size_t block_smem(int nslices, int grid, int device, int per_row) {
   return std::max<size_t>(bytes, 16);
 }
 
+// Self-test of the exchange's bounded wait: the grid exchanges one partial
+// sum, except its last `absent` blocks, which leave before publishing, so
+// the others' polls of their words run out and record SFR_TIMEOUT.
+__global__ void k_res_wait_selftest(int absent, ExSync f) {
+  __shared__ double red[32 * 2];
+  if (static_cast<int>(blockIdx.x) >= static_cast<int>(gridDim.x) - absent) return;
+  unsigned epoch = 0;
+  const double acc[1] = {1.0};
+  double tot[1];
+  (void)exchange<1, false>(f, epoch, acc, tot, red);
+}
+
 }  // namespace
+
+int wait_selftest_resident(int32_t absent, uint32_t spin_limit, cudaStream_t st) {
+  constexpr int kGrid = 4;
+  if (absent < 0 || absent >= kGrid) return SFR_BAD_INPUT;
+  const size_t slots = sizeof(ExSlot) * 3 * kGrid;
+  char *buf = nullptr;
+  if (cudaMalloc(&buf, slots + 64) != cudaSuccess) return SFR_CUDA_ERROR;
+  ExSync f;
+  f.slots = reinterpret_cast<ExSlot *>(buf);
+  f.err = reinterpret_cast<int *>(buf + slots);
+  f.nblocks = kGrid;
+  f.spin_limit = spin_limit;
+  void *params[] = {&absent, &f};
+  int err = 0;
+  cudaError_t ce = cudaMemsetAsync(buf, 0, slots + 64, st);
+  if (ce == cudaSuccess)
+    ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_res_wait_selftest), dim3(kGrid),
+                                     dim3(128), params, 0, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&err, f.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (ce != cudaSuccess) {
+    set_last_error(cudaGetErrorString(ce));
+    return SFR_CUDA_ERROR;
+  }
+  return err;
+}
 
 bool resident_fits(sfr_system *s) {
   if (!s->A.off) return false;  // bandwidth above 32767: no 16-bit column offsets

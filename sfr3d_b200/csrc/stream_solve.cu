@@ -662,6 +662,21 @@ const void *fused_kernel(int mode) {
                      : (const void *)k_pcg_fused<I, 1>;
 }
 
+// Self-test of the bounded waits: the grid meets once at a grid_sync (kind
+// 0) or a tag_exchange (kind 1), except its last `absent` blocks, which
+// leave before it, so the others' wait on them runs out and records
+// SFR_TIMEOUT.
+__global__ void k_wait_selftest(int kind, int absent, GridSync gs, TagExchange tx, double *part) {
+  __shared__ double sm[34];
+  if (static_cast<int>(blockIdx.x) >= static_cast<int>(gridDim.x) - absent) return;
+  if (kind == 0) {
+    (void)grid_sync(gs);
+  } else {
+    double tot = 0.0;
+    (void)tag_exchange(tx, 1u, 1.0, part, &tot, sm);
+  }
+}
+
 // reliable update, part 1: x += xs (FP64) for the flagged right-hand sides
 template <int K>
 __global__ void __launch_bounds__(256) k_fold(const SArgs<K> a, SState<K> *st, int all) {
@@ -1904,6 +1919,42 @@ int run(sfr_system *s, int solver, const double *d_diag_k, const double *d_b, do
 }
 
 }  // namespace
+
+int wait_selftest_fused(int32_t kind, int32_t absent, uint32_t spin_limit, cudaStream_t st) {
+  constexpr int kGrid = 4;
+  if ((kind != 0 && kind != 1) || absent < 0 || absent >= kGrid) return SFR_BAD_INPUT;
+  // control words: grid_sync count, generation and error (0-2), the tagged
+  // word (bytes 16-23), the exchange's arrivals (6), the block partials
+  // (bytes 32-63)
+  unsigned *ctl = nullptr;
+  if (cudaMalloc(&ctl, 64) != cudaSuccess) return SFR_CUDA_ERROR;
+  GridSync gs;
+  gs.count = ctl;
+  gs.gen = ctl + 1;
+  gs.err = reinterpret_cast<int *>(ctl + 2);
+  gs.nblocks = kGrid;
+  gs.spin_limit = spin_limit;
+  TagExchange tx;
+  tx.word = reinterpret_cast<unsigned long long *>(ctl + 4);
+  tx.count = ctl + 6;
+  tx.err = gs.err;
+  tx.spin_limit = spin_limit;
+  double *part = reinterpret_cast<double *>(ctl + 8);
+  void *params[] = {&kind, &absent, &gs, &tx, &part};
+  int err = 0;
+  cudaError_t ce = cudaMemsetAsync(ctl, 0, 64, st);
+  if (ce == cudaSuccess)
+    ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_wait_selftest), dim3(kGrid),
+                                     dim3(128), params, 0, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&err, gs.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  cudaFree(ctl);
+  if (ce != cudaSuccess) {
+    set_last_error(cudaGetErrorString(ce));
+    return SFR_CUDA_ERROR;
+  }
+  return err;
+}
 
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,
                  const double *d_b, double *d_x, double tol, uint32_t maxit, int32_t newx,

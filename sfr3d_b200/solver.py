@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
     L.sfr_status_string.argtypes = [ctypes.c_int]
     L.sfr_last_error.restype = ctypes.c_char_p
     L.sfr_gpu_check_device.argtypes = [_I32, _P, _P]
+    L.sfr_gpu_wait_selftest.argtypes = [_I32, _I32, ctypes.c_uint32, _P]
     L.sfr_gpu_create.argtypes = [_I32, _I32, _P, _P, _I32, _I32, _I32,
                                  ctypes.POINTER(_P)]
     L.sfr_gpu_set_values.argtypes = [_P, _P, _P, _P]
@@ -176,6 +177,17 @@ def check_device(device: int = 0) -> tuple[int, int, int]:
     ma, mi = ctypes.c_int32(), ctypes.c_int32()
     rc = lib().sfr_gpu_check_device(device, ctypes.byref(ma), ctypes.byref(mi))
     return rc, ma.value, mi.value
+
+
+# the device-side waits sfr_gpu_wait_selftest exercises
+WAIT_GRID_BARRIER, WAIT_TAG_EXCHANGE, WAIT_RESIDENT_EXCHANGE = 0, 1, 2
+
+
+def wait_selftest(kind: int, absent: int, spin_limit: int, stream=None) -> int:
+    """Run one of the engines' bounded waits on four blocks of which
+    `absent` never arrive; SFR_OK when it completed, SFR_TIMEOUT when it
+    gave up after `spin_limit` polls."""
+    return lib().sfr_gpu_wait_selftest(kind, absent, spin_limit, stream)
 
 
 class GpuSystem:
