@@ -10,8 +10,8 @@
 // residual, the FP32 solution increment, A p and (when it fits) the
 // diagonal correction in shared memory (16 bytes a row).  The global traffic
 // of an inner iteration is the operator (from L2), the gathers of p and the
-// update of p; one exchange of partial sums and one barrier separate its two
-// phases.
+// update of p; one exchange of partial sums separates its two phases, and a
+// wait on the blocks whose p the next SpMV phase gathers ends it.
 //
 // Arithmetic.  PCG with the Jacobi preconditioner M = diag(1/ad) (Cg.c:47-209,
 // PreCond.c:18-26) is CG on the symmetrically scaled system
@@ -178,6 +178,93 @@ __device__ __forceinline__ bool exchange_barrier(const ExSync &f, unsigned &epoc
   return exchange<1, true>(f, epoch, z, t, sm);
 }
 
+// The wait after an iteration's update of p.  The next SpMV phase of a
+// block gathers p only at the columns of its own rows, so it needs the
+// updates of the blocks that own those columns -- for a banded (RCM-ordered)
+// matrix a few neighbouring blocks -- and not of the whole grid: the global
+// exchange after each SpMV phase already keeps every block from rewriting p
+// while another still reads it.  Each block publishes the number of updates
+// it has finished in its own 64-byte slot (release) and polls (acquire) the
+// slots of the blocks it gathers from.  Bounded like the exchanges.
+struct NbSync {
+  unsigned *ticks;  // 16 words a block, zero at launch; word 0 counts updates
+};
+
+// The range [red_i[0], red_i[1]] of blocks owning the columns this block's
+// rows gather from (block_slices's partition of nslices slices over
+// gridDim.x blocks), in shared memory.
+__device__ __forceinline__ void gather_blocks(const int *sm_sp, const int16_t *off, int s0,
+                                              int s1, int nslices, int *red_i) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  int cmin = s0 * kWarp, cmax = s1 * kWarp - 1;
+  for (int s = s0 + warp; s < s1; s += nw) {
+    const int base = sm_sp[s - s0], end = sm_sp[s - s0 + 1];
+    const int row = s * kWarp + lane;
+    for (int e = base + lane; e < end; e += kWarp) {
+      const int c = row + static_cast<int>(__ldcg(off + e));  // slot e is lane's
+      cmin = min(cmin, c);
+      cmax = max(cmax, c);
+    }
+  }
+  if (threadIdx.x == 0) {
+    red_i[0] = cmin;
+    red_i[1] = cmax;
+  }
+  __syncthreads();
+  atomicMin(red_i, cmin);
+  atomicMax(red_i + 1, cmax);
+  __syncthreads();
+  const long long G = gridDim.x, ns = nslices;
+  auto owner = [&](int col) {
+    const long long sl = col / kWarp;
+    return static_cast<int>(((sl + 1) * G + ns - 1) / ns - 1);
+  };
+  const int lo = min(owner(red_i[0]), static_cast<int>(blockIdx.x));
+  const int hi = max(owner(red_i[1]), static_cast<int>(blockIdx.x));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    red_i[0] = lo;
+    red_i[1] = hi;
+  }
+  __syncthreads();
+}
+
+// Publishes this block's `tick`-th update of p and waits until every block in
+// [lo, hi] has published its own.
+__device__ __forceinline__ bool neighbour_wait(const NbSync &nb, const ExSync &f, unsigned tick,
+                                               int lo, int hi) {
+  __syncthreads();  // the block's writes of p come before the release
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device>(nb.ticks[16 * blockIdx.x])
+        .store(tick, cuda::memory_order_release);
+  }
+  const int t = lo + static_cast<int>(threadIdx.x);
+  const bool watcher = t <= hi && t != static_cast<int>(blockIdx.x);
+  int seen = !watcher;
+  int ok = 1;
+  cuda::atomic_ref<int, cuda::thread_scope_device> err(*f.err);
+  for (unsigned spins = 0;; ++spins) {
+    if (!seen)
+      seen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(nb.ticks[16 * t])
+                 .load(cuda::memory_order_acquire) >= tick;
+    if (__syncthreads_and(seen)) break;
+    if ((spins & 63u) == 63u &&
+        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
+      ok = 0;
+      break;
+    }
+    if (spins > f.spin_limit) {
+      if (threadIdx.x == 0) {
+        int expected = 0;
+        err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+      }
+      ok = 0;
+      break;
+    }
+  }
+  return ok != 0;
+}
+
 struct ResArgs {
   int n, nslices;
   const int *sptr;
@@ -194,6 +281,7 @@ struct ResArgs {
   double *x;
   float *p;  // search direction, nslices * 32 entries (padding rows stay 0)
   ExSync ex;
+  NbSync nb;  // ticks null: the update of p ends with a full barrier
   SolveOut *out;
   double tol, rdelta;
   unsigned maxit;
@@ -290,12 +378,12 @@ __device__ __forceinline__ void fold(const ResArgs &a, int s0, int s1, int r0, f
   }
 }
 
-// Iteration j (one exchange of partial sums, one barrier):
+// Iteration j (one exchange of partial sums, one wait on the neighbours):
 //   q = A_s p ; (p, q), (r, q), (q, q), (r, r)                 [exchange]
 //   alpha = (r, r) / (p, q)
 //   (r', r') = (r, r) - 2 alpha (r, q) + alpha^2 (q, q)   for r' = r - alpha q
 //   (refresh when due)
-//   r = r - alpha q ; xs += alpha p ; p = r + beta p            [barrier]
+//   r = r - alpha q ; xs += alpha p ; p = r + beta p            [wait]
 // The norm of the next residual follows from dot products the SpMV phase
 // already forms, so the residual update needs no exchange of its own; it is
 // accumulated in FP64 and only decides beta and when to refresh.  The next
@@ -320,6 +408,12 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
   for (int i = threadIdx.x; i <= s1 - s0; i += kT) sm_sp[i] = __ldg(a.sptr + s0 + i);
   if (kDeltaShared)
     for (int lr = threadIdx.x; lr < rows; lr += kT) sm_d[lr] = __ldcg(a.delta + r0 + lr);
+  __syncthreads();
+  // the blocks whose p this block's SpMV phases gather
+  __shared__ int nb_range[2];
+  nb_range[0] = 0;
+  nb_range[1] = kT;  // no neighbour waits unless the range is computed
+  if (a.nb.ticks) gather_blocks(sm_sp, a.off, s0, s1, a.nslices, nb_range);
 
   // setup: x0, (b, M b), (b, b)
   double bm = 0.0, bnorm = 0.0;
@@ -417,7 +511,12 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
         st_vec(a.p + row, fmaf(bf, pr, ri));
       }
       a_pend = 0.0f;
-      if (!exchange_barrier(a.ex, epoch, red)) return;
+      // one update of p an iteration: iteration j publishes its (j + 1)-th
+      if (nb_range[1] - nb_range[0] < kT) {
+        if (!neighbour_wait(a.nb, a.ex, j + 1, nb_range[0], nb_range[1])) return;
+      } else if (!exchange_barrier(a.ex, epoch, red)) {
+        return;
+      }
     }
   }
   if (act) {  // iteration cap
@@ -631,7 +730,8 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   const size_t part_bytes = align(sizeof(ExSlot) * 3 * static_cast<size_t>(grid));
   const size_t ctl_bytes = 256;
   const size_t out_bytes = align(sizeof(SolveOut));
-  rc = ensure_workspace(s, p_bytes + part_bytes + ctl_bytes + out_bytes);
+  const size_t tick_bytes = align(64 * static_cast<size_t>(grid));
+  rc = ensure_workspace(s, p_bytes + part_bytes + ctl_bytes + out_bytes + tick_bytes);
   if (rc != SFR_OK) return rc;
   char *base = static_cast<char *>(s->ws.base);
 
@@ -656,6 +756,7 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   a.ex.nblocks = grid;
   a.ex.spin_limit = 1u << 22;
   a.out = reinterpret_cast<SolveOut *>(base + part_bytes + ctl_bytes);
+  a.nb.ticks = reinterpret_cast<unsigned *>(base + part_bytes + ctl_bytes + out_bytes);
   a.tol = tol;
   a.rdelta = reliable_delta_resident();
   a.maxit = maxit;
@@ -664,7 +765,8 @@ int solve_resident(sfr_system *s, const double *d_b, double *d_x, double tol, ui
   // padding rows of p must read as 0; epochs restart at 0 in every launch,
   // with every exchange word untagged
   if (cudaMemsetAsync(a.p, 0, p_bytes, st) != cudaSuccess) return SFR_CUDA_ERROR;
-  if (cudaMemsetAsync(a.ex.slots, 0, part_bytes + ctl_bytes, st) != cudaSuccess)
+  if (cudaMemsetAsync(a.ex.slots, 0, part_bytes + ctl_bytes, st) != cudaSuccess ||
+      cudaMemsetAsync(a.nb.ticks, 0, tick_bytes, st) != cudaSuccess)
     return SFR_CUDA_ERROR;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return SFR_CUDA_ERROR;
