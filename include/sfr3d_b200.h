@@ -164,8 +164,10 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
  * z = M r of a block's rows in shared memory instead of HBM; mode 2 is the
  * same kernel held to 40 registers so that six blocks fit an SM; in mode 3
  * the last block to arrive at a barrier sums the partials once and
- * broadcasts the total in one epoch-tagged word that the others poll.
- * Solves it
+ * broadcasts the total in one epoch-tagged word that the others poll; mode
+ * 4 runs mode 3's iteration in a loop inside one cooperative launch for the
+ * whole solve, each block waiting after its update of p only on the blocks
+ * whose p its next SpMV phase gathers.  Solves it
  * does not serve (other solvers, K > 1, mixed precision, or no co-resident
  * shape) take the three-kernel iteration.  0 (the default) turns it off;
  * other values are SFR_BAD_INPUT. */

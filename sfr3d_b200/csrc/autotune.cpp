@@ -192,7 +192,7 @@ extern "C" int sfr_gpu_autotune(sfr_system *s, int32_t solver, int32_t k, const 
   for (int th : {256, 128})
     for (int sp : {0, 2, 8}) add({2, th, sp, 0, 0});
   if (precision == SFR_FP64 && solver == SFR_PCG && k == 1) {
-    for (int mode : {1, 2, 3}) add({2, 256, 0, 0, mode});
+    for (int mode : {1, 2, 3, 4}) add({2, 256, 0, 0, mode});
   }
   add({1, 0, 0, 0, 0});
   if (precision == SFR_MIXED && solver == SFR_PCG && k == 1 && own_diag && resident_fits(s))

@@ -410,7 +410,7 @@ int sfr_gpu_set_staging(sfr_system *s, int32_t flag) {
 
 int sfr_gpu_set_fused(sfr_system *s, int32_t flag) {
   if (!s) return SFR_BAD_INPUT;
-  if (flag < 0 || flag > 3) return SFR_BAD_INPUT;
+  if (flag < 0 || flag > 4) return SFR_BAD_INPUT;
   s->graph_fused = flag;
   return SFR_OK;
 }

@@ -157,6 +157,61 @@ __device__ __forceinline__ bool grid_sync(const GridSync &g) {
 }
 
 // ----------------------------------------------------------------------
+// Wait on the blocks a phase gathers from.  A block whose next phase reads a
+// vector only at its rows' columns needs the updates of the blocks owning
+// those columns -- for a banded (RCM-ordered) matrix a few neighbouring
+// blocks -- not of the whole grid.  Each block publishes the number of
+// updates it has finished in its own 64-byte slot of `ticks` (16 words a
+// block, zero at launch; release) and polls the slots of blocks [lo, hi]
+// (acquire; thread t watches block lo + t, so hi - lo < blockDim.x).  The
+// caller keeps the blocks from rewriting the vector while another still
+// reads it (a global exchange between the reads and the next writes).
+// Bounded: after spin_limit polls a block records SFR_TIMEOUT in *err; a
+// block that sees *err set stops waiting.  Returns false on either.
+// ----------------------------------------------------------------------
+__device__ __forceinline__ bool neighbour_wait(unsigned *ticks, int *err_word,
+                                               unsigned spin_limit, unsigned tick, int lo,
+                                               int hi) {
+  __syncthreads();  // the block's writes come before the release
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device>(ticks[16 * blockIdx.x])
+        .store(tick, cuda::memory_order_release);
+  }
+  const int t = lo + static_cast<int>(threadIdx.x);
+  const bool watcher = t <= hi && t != static_cast<int>(blockIdx.x);
+  int seen = !watcher;
+  int ok = 1;
+  cuda::atomic_ref<int, cuda::thread_scope_device> err(*err_word);
+  for (unsigned spins = 0;; ++spins) {
+    if (!seen)
+      seen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(ticks[16 * t])
+                 .load(cuda::memory_order_acquire) >= tick;
+    if (__syncthreads_and(seen)) break;
+    if ((spins & 63u) == 63u &&
+        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
+      ok = 0;
+      break;
+    }
+    if (spins > spin_limit) {
+      if (threadIdx.x == 0) {
+        int expected = 0;
+        err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
+      }
+      ok = 0;
+      break;
+    }
+  }
+  return ok != 0;
+}
+
+// The block owning row `row` under block_slices's partition of nslices
+// slices over gridDim.x blocks.
+__device__ __forceinline__ int owner_block(int row, int nslices) {
+  const long long G = gridDim.x, ns = nslices, sl = row / 32;
+  return static_cast<int>(((sl + 1) * G + ns - 1) / ns - 1);
+}
+
+// ----------------------------------------------------------------------
 // Sliced ELLPACK (SELL-32) view.  Rows are grouped in slices of 32; slice s
 // holds w_s = (sptr[s+1]-sptr[s])/32 slots, stored slot-major so that lane l
 // of a warp reads row 32s+l.  Slot k of a row is its k-th off-diagonal in the

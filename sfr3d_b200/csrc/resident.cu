@@ -178,14 +178,10 @@ __device__ __forceinline__ bool exchange_barrier(const ExSync &f, unsigned &epoc
   return exchange<1, true>(f, epoch, z, t, sm);
 }
 
-// The wait after an iteration's update of p.  The next SpMV phase of a
-// block gathers p only at the columns of its own rows, so it needs the
-// updates of the blocks that own those columns -- for a banded (RCM-ordered)
-// matrix a few neighbouring blocks -- and not of the whole grid: the global
-// exchange after each SpMV phase already keeps every block from rewriting p
-// while another still reads it.  Each block publishes the number of updates
-// it has finished in its own 64-byte slot (release) and polls (acquire) the
-// slots of the blocks it gathers from.  Bounded like the exchanges.
+// The wait after an iteration's update of p (neighbour_wait, common.cuh):
+// the next SpMV phase of a block gathers p only at the columns of its own
+// rows, and the global exchange after each SpMV phase already keeps every
+// block from rewriting p while another still reads it.
 struct NbSync {
   unsigned *ticks;  // 16 words a block, zero at launch; word 0 counts updates
 };
@@ -214,55 +210,14 @@ __device__ __forceinline__ void gather_blocks(const int *sm_sp, const int16_t *o
   atomicMin(red_i, cmin);
   atomicMax(red_i + 1, cmax);
   __syncthreads();
-  const long long G = gridDim.x, ns = nslices;
-  auto owner = [&](int col) {
-    const long long sl = col / kWarp;
-    return static_cast<int>(((sl + 1) * G + ns - 1) / ns - 1);
-  };
-  const int lo = min(owner(red_i[0]), static_cast<int>(blockIdx.x));
-  const int hi = max(owner(red_i[1]), static_cast<int>(blockIdx.x));
+  const int lo = min(owner_block(red_i[0], nslices), static_cast<int>(blockIdx.x));
+  const int hi = max(owner_block(red_i[1], nslices), static_cast<int>(blockIdx.x));
   __syncthreads();
   if (threadIdx.x == 0) {
     red_i[0] = lo;
     red_i[1] = hi;
   }
   __syncthreads();
-}
-
-// Publishes this block's `tick`-th update of p and waits until every block in
-// [lo, hi] has published its own.
-__device__ __forceinline__ bool neighbour_wait(const NbSync &nb, const ExSync &f, unsigned tick,
-                                               int lo, int hi) {
-  __syncthreads();  // the block's writes of p come before the release
-  if (threadIdx.x == 0) {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device>(nb.ticks[16 * blockIdx.x])
-        .store(tick, cuda::memory_order_release);
-  }
-  const int t = lo + static_cast<int>(threadIdx.x);
-  const bool watcher = t <= hi && t != static_cast<int>(blockIdx.x);
-  int seen = !watcher;
-  int ok = 1;
-  cuda::atomic_ref<int, cuda::thread_scope_device> err(*f.err);
-  for (unsigned spins = 0;; ++spins) {
-    if (!seen)
-      seen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(nb.ticks[16 * t])
-                 .load(cuda::memory_order_acquire) >= tick;
-    if (__syncthreads_and(seen)) break;
-    if ((spins & 63u) == 63u &&
-        __syncthreads_or(threadIdx.x == 0 && err.load(cuda::memory_order_relaxed) != 0)) {
-      ok = 0;
-      break;
-    }
-    if (spins > f.spin_limit) {
-      if (threadIdx.x == 0) {
-        int expected = 0;
-        err.compare_exchange_strong(expected, SFR_TIMEOUT, cuda::memory_order_relaxed);
-      }
-      ok = 0;
-      break;
-    }
-  }
-  return ok != 0;
 }
 
 struct ResArgs {
@@ -513,7 +468,9 @@ __global__ void __launch_bounds__(kT, 1) pcg_resident_kernel(ResArgs a) {
       a_pend = 0.0f;
       // one update of p an iteration: iteration j publishes its (j + 1)-th
       if (nb_range[1] - nb_range[0] < kT) {
-        if (!neighbour_wait(a.nb, a.ex, j + 1, nb_range[0], nb_range[1])) return;
+        if (!neighbour_wait(a.nb.ticks, a.ex.err, a.ex.spin_limit, j + 1, nb_range[0],
+                            nb_range[1]))
+          return;
       } else if (!exchange_barrier(a.ex, epoch, red)) {
         return;
       }

@@ -523,30 +523,38 @@ __device__ __forceinline__ bool tag_exchange(const TagExchange &x, unsigned epoc
 // block leaves, and the solve stops with that status.
 // kTagged: the barriers are tag_exchange (mode 3: the last block reduces and
 // broadcasts) instead of grid_sync with every block reading the partials.
+// Iteration j from d = (r, z); returns true with d = the new (r, z) when the
+// solve goes on, false when it stopped (converged, breakdown, iteration cap
+// or a wait that gave up), with the state recorded by block 0.
+
+// Stops the fused solve with `status` after `iters` iterations (block 0
+// records it).
+__device__ __forceinline__ void fused_stop(const SArgs<1> &a, SState<1> *st, int status,
+                                           unsigned iters) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->active[0] = 0;
+    st->status[0] = status;
+    st->iters[0] = static_cast<int>(iters);
+    st->any = 0;
+    if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
+  }
+}
+
 template <typename I, bool kTagged>
-__device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
-                                               const GridSync &gs, const TagExchange &tx) {
+__device__ __forceinline__ bool pcg_fused_body(const SArgs<1> &a, SState<1> *st,
+                                               const GridSync &gs, const TagExchange &tx,
+                                               const unsigned j, double &d_io) {
   __shared__ double sm[34 * 2];
   extern __shared__ double qz[];  // this block's rows: q, then z
-  if (!st->any) return;
   const int n = a.n;
   const int lane = threadIdx.x & 31;
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
   const int row0 = s0 * kWarp;
   const int all[1] = {1};
-  const unsigned j = st->j;
-  const double d = st->d[0];
+  const double d = d_io;
   const int G = gridDim.x;
-  auto fail = [&](int status, unsigned iters) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      st->active[0] = 0;
-      st->status[0] = status;
-      st->iters[0] = static_cast<int>(iters);
-      st->any = 0;
-      if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
-    }
-  };
+  auto fail = [&](int status, unsigned iters) { fused_stop(a, st, status, iters); };
   // phase A: q = A p, (p, q); each slice's column-independent loads go out
   // with its columns (slice_rows: 114.6 -> 106.9 ms a 128^3 solve in mode 3)
   double acc[1] = {0.0};
@@ -562,20 +570,20 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
   if (kTagged) {
     if (!tag_exchange(tx, 2 * j + 1, acc[0], a.part, &tot[0], sm)) {
       fail(SFR_TIMEOUT, j + 1);
-      return;
+      return false;
     }
   } else {
     block_partials<1>(acc, a.part, G, sm);
     if (!grid_sync(gs)) {
       fail(SFR_TIMEOUT, j + 1);
-      return;
+      return false;
     }
     grid_totals<1>(a.part, G, G, tot, sm);
   }
   const double alpha = d / tot[0];
   if (!isfinite(alpha)) {
     fail(SFR_BREAKDOWN, j + 1);
-    return;
+    return false;
   }
   // phase B: x += alpha p, r -= alpha q, z = M r, (r, z)
   acc[0] = 0.0;
@@ -592,13 +600,13 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
   if (kTagged) {
     if (!tag_exchange(tx, 2 * j + 2, acc[0], a.part + G, &tot[0], sm)) {
       fail(SFR_TIMEOUT, j + 1);
-      return;
+      return false;
     }
   } else {
     block_partials<1>(acc, a.part + G, G, sm);
     if (!grid_sync(gs)) {
       fail(SFR_TIMEOUT, j + 1);
-      return;
+      return false;
     }
     grid_totals<1>(a.part + G, G, G, tot, sm);
   }
@@ -632,12 +640,14 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
       if (a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
     }
   }
-  if (stop) return;
+  if (stop) return false;
   // phase C: p = z + beta p
   SFR_FOR_OWN_ROWS(s0, s1) {
     const double p = ld_ro(a.p0[0] + row_);
     st_vec(a.p0[0] + row_, xadd(qz[row_ - row0], xmul(beta, p)));
   }
+  d_io = di;
+  return true;
 }
 
 // The fused iteration as launched: mode 1 leaves the register count to the
@@ -645,13 +655,75 @@ __device__ __forceinline__ void pcg_fused_body(const SArgs<1> &a, SState<1> *st,
 // is mode 1 with the tagged exchanges.
 template <typename I, int kMode>
 __global__ void __launch_bounds__(256) k_pcg_fused(const SArgs<1> a, SState<1> *st, GridSync gs,
-                                                   TagExchange tx) {
-  pcg_fused_body<I, kMode == 3>(a, st, gs, tx);
+                                                   TagExchange tx, unsigned *) {
+  if (!st->any) return;
+  double d = st->d[0];
+  (void)pcg_fused_body<I, kMode == 3>(a, st, gs, tx, st->j, d);
 }
 template <typename I>
 __global__ void __launch_bounds__(256, 6) k_pcg_fused_r40(const SArgs<1> a, SState<1> *st,
-                                                          GridSync gs, TagExchange tx) {
-  pcg_fused_body<I, false>(a, st, gs, tx);
+                                                          GridSync gs, TagExchange tx, unsigned *) {
+  if (!st->any) return;
+  double d = st->d[0];
+  (void)pcg_fused_body<I, false>(a, st, gs, tx, st->j, d);
+}
+
+// Mode 4: the whole solve in one cooperative launch, mode 3's iteration in a
+// loop.  The kernel boundary that published p between iterations becomes a
+// wait on the blocks whose p the next SpMV phase gathers (neighbour_wait;
+// the two exchanges inside an iteration keep every block from rewriting p
+// while another still reads it).  A block finds those blocks once, from the
+// columns of its slices.
+template <typename I>
+__global__ void __launch_bounds__(256) k_pcg_fused_loop(const SArgs<1> a, SState<1> *st,
+                                                        GridSync gs, TagExchange tx,
+                                                        unsigned *ticks) {
+  __shared__ int range[2];
+  int s0, s1;
+  block_slices(a.nslices, &s0, &s1);
+  {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    int cmin = s0 * kWarp, cmax = s1 * kWarp - 1;
+    const I *cols = cols_of<I>(a.cols);
+    for (int s = s0 + static_cast<int>(threadIdx.x >> 5); s < s1; s += nw) {
+      const int base = __ldg(a.sptr + s), w = (__ldg(a.sptr + s + 1) - base) >> 5;
+      const int row = s * kWarp + lane;
+      for (int k = 0; k < w; ++k) {
+        const int c = slot_col(cols + base + lane, k * kWarp, row);
+        cmin = min(cmin, c);
+        cmax = max(cmax, c);
+      }
+    }
+    if (threadIdx.x == 0) {
+      range[0] = cmin;
+      range[1] = cmax;
+    }
+    __syncthreads();
+    atomicMin(range, cmin);
+    atomicMax(range + 1, cmax);
+    __syncthreads();
+    const int lo = min(owner_block(range[0], a.nslices), static_cast<int>(blockIdx.x));
+    const int hi = max(owner_block(range[1], a.nslices), static_cast<int>(blockIdx.x));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      range[0] = lo;
+      range[1] = hi;
+    }
+    __syncthreads();
+  }
+  if (!st->any) return;
+  unsigned j = st->j;
+  double d = st->d[0];
+  const bool local = range[1] - range[0] < static_cast<int>(blockDim.x);
+  while (pcg_fused_body<I, true>(a, st, gs, tx, j, d)) {
+    const bool ok = local ? neighbour_wait(ticks, tx.err, tx.spin_limit, j + 1, range[0], range[1])
+                          : grid_sync(gs);
+    if (!ok) {
+      fused_stop(a, st, SFR_TIMEOUT, j + 1);
+      return;
+    }
+    ++j;
+  }
 }
 
 // The fused kernel of a mode.
@@ -659,6 +731,7 @@ template <typename I>
 const void *fused_kernel(int mode) {
   return mode == 2   ? (const void *)k_pcg_fused_r40<I>
          : mode == 3 ? (const void *)k_pcg_fused<I, 3>
+         : mode == 4 ? (const void *)k_pcg_fused_loop<I>
                      : (const void *)k_pcg_fused<I, 1>;
 }
 
@@ -1331,7 +1404,9 @@ struct CachedGraph {
   int grid_o = 0;        // once-a-solve and refresh kernels: one wave of their own
   int grid_f = 0;        // fused iteration: co-resident blocks
   size_t smem_f = 0;     // fused iteration: dynamic shared memory a block
-  unsigned long long *tagw = nullptr;  // fused mode 3: the broadcast word
+  unsigned long long *tagw = nullptr;  // fused modes 3-4: the broadcast word
+  unsigned *ticks = nullptr;           // fused mode 4: update counts (inside tagw's allocation)
+  size_t tag_bytes = 0;                // tagw's allocation
   bool staged = false;   // BiCGSTAB SpMV phases staged through shared memory
   size_t smem_s = 0;     // their dynamic shared memory a block
   uint64_t last_use = 0;
@@ -1638,14 +1713,18 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
     mp.pitch = 0;
     SFR_TRY(cudaGraphAddMemsetNode(&prev, g, nullptr, 0, &mp));
   }
-  if (fused == 3 && cg->grid_f > 0) {
-    // the fused iteration's exchange words start every solve at zero
-    SFR_TRY(cudaMalloc(&cg->tagw, sizeof(unsigned long long)));
+  if (fused >= 3 && cg->grid_f > 0) {
+    // the fused iteration's exchange words (and mode 4's update counts, 64
+    // bytes a block) start every solve at zero
+    const size_t words = fused == 4 ? 16 + 16 * static_cast<size_t>(cg->grid_f) : 2;
+    SFR_TRY(cudaMalloc(&cg->tagw, sizeof(unsigned) * words));
+    cg->tag_bytes = sizeof(unsigned) * words;
+    if (fused == 4) cg->ticks = reinterpret_cast<unsigned *>(cg->tagw) + 16;
     cudaMemsetParams mt{};
     mt.dst = cg->tagw;
     mt.value = 0;
     mt.elementSize = sizeof(unsigned);
-    mt.width = 2;
+    mt.width = words;
     mt.height = 1;
     mt.pitch = 0;
     cudaGraphNode_t mn;
@@ -1676,7 +1755,8 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
         // one cooperative kernel an iteration (k_pcg_fused)
         GridSync gsync = fused_barrier(cg);
         TagExchange tx = fused_exchange(cg);
-        void *pf3[4] = {&a, &ps, &gsync, &tx};
+        unsigned *ticks = cg->ticks;
+        void *pf3[5] = {&a, &ps, &gsync, &tx, &ticks};
         cudaKernelNodeParams kp{};
         kp.func = const_cast<void *>(fused_kernel<I>(fused));
         kp.gridDim = dim3(cg->grid_f);
@@ -1758,7 +1838,7 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
   const size_t ssm = cg->staged ? cg->smem_s : 0;
   void *pa[2] = {&a, &ps};
   SFR_TRY(cudaMemsetAsync(cg->counter, 0, sizeof(unsigned) * kCounters, st));
-  if (cg->tagw) SFR_TRY(cudaMemsetAsync(cg->tagw, 0, sizeof(unsigned long long), st));
+  if (cg->tagw) SFR_TRY(cudaMemsetAsync(cg->tagw, 0, cg->tag_bytes, st));
   if (solver == SFR_PCG) {
     if (mixed) {
       k_setup<K, true><<<gv, t, 0, st>>>(a, ps);
@@ -1779,9 +1859,11 @@ cudaError_t launch_loop(CachedGraph *cg, int solver, bool mixed, int fused, uint
           if (fused) {
             GridSync gsync = fused_barrier(cg);
             TagExchange tx = fused_exchange(cg);
-            void *pf3[4] = {&a, &ps, &gsync, &tx};
+            unsigned *ticks = cg->ticks;
+            void *pf3[5] = {&a, &ps, &gsync, &tx, &ticks};
             SFR_TRY(cudaLaunchCooperativeKernel(fused_kernel<I>(fused), dim3(cg->grid_f),
                                                 dim3(256), pf3, cg->smem_f, st));
+            if (fused == 4) break;  // the whole loop in one launch
             continue;
           }
         }

@@ -64,8 +64,8 @@ def test_autotune_choice_is_kept_and_solves_at_parity(cuda, tmp_path, monkeypatc
 @pytest.mark.parametrize("engine,threads,spw,pf,fused",
                          [(2, 128, 0, 0, 0), (2, 256, 2, 0, 0), (2, 256, 8, 0, 0),
                           (2, 256, 0, 2, 0), (2, 256, 0, 0, 1), (2, 256, 0, 0, 2),
-                          (2, 256, 0, 0, 3), (3, 256, 0, 0, 1), (3, 256, 0, 0, 3),
-                          (1, 0, 0, 0, 0)])
+                          (2, 256, 0, 0, 3), (2, 256, 0, 0, 4), (3, 256, 0, 0, 1),
+                          (3, 256, 0, 0, 3), (3, 256, 0, 0, 4), (1, 0, 0, 0, 0)])
 def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf, fused):
     """Whatever the tuner picks, the arithmetic is the reference's: every
     candidate engine and launch shape (the L2 prefetch, the fused one-kernel
@@ -96,6 +96,24 @@ def test_every_candidate_shape_meets_the_fp64_bar(cuda, engine, threads, spw, pf
         assert rel(xs[k], refk.x) < 1e-12
     g.close()
     gm.close()
+
+
+def test_fused_loop_matches_fused_iteration_bit_for_bit(cuda):
+    """Mode 4 runs mode 3's iteration in one launch on the same blocks, with a
+    wait on the neighbouring blocks where the kernel boundary was: the same
+    arithmetic in the same order, so the same bits and iteration count."""
+    s = S.poisson_jittered(40, seed=25)
+    out = {}
+    for mode in (3, 4):
+        g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+        g.set_values(s.al, s.ad)
+        g.set_engine(2, 256, -1)
+        g.set_fused(mode)
+        out[mode] = g.solve(sv.PCG, s.b[0], tol=TOL)
+        g.close()
+    (x3, i3), (x4, i4) = out[3], out[4]
+    assert i3.status == sv.OK and i4.status == sv.OK and i3.iters == i4.iters
+    assert bits_equal(x3, x4)
 
 
 def test_autotune_mixed_k3_momentum(cuda):

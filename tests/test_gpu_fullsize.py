@@ -61,16 +61,21 @@ def m_residual(s, x, b):
     return float(np.sqrt(abs(np.dot(r, r / s.ad)))), float(np.sqrt(abs(np.dot(b, b / s.ad))))
 
 
-def test_pressure128_fp64_graph_engine(cuda, pressure128):
+@pytest.mark.parametrize("fused", [0, 3, 4])
+def test_pressure128_fp64_graph_engine(cuda, pressure128, fused):
+    """The three-kernel iteration, the fused one-kernel iteration (mode 3)
+    and the whole solve in one launch (mode 4), which the autotuner chooses
+    between for this system."""
     s, ref = pressure128
     g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
     g.set_values(s.al, s.ad)
     g.set_engine(sv.ENGINE_GRAPH)
+    g.set_fused(fused)
     x, info = g.solve(sv.PCG, s.b[0], tol=TOL)
     g.close()
     err = rel(x, ref.x)
-    print(f"128^3 FP64 PCG: {info.iters} iterations (reference {ref.iters}), "
-          f"error vs reference {err:.2e}")
+    print(f"128^3 FP64 PCG (fused mode {fused}): {info.iters} iterations (reference "
+          f"{ref.iters}), error vs reference {err:.2e}")
     assert info.status == sv.OK
     assert abs(info.iters - ref.iters) <= 1
     assert err < TOL_X
