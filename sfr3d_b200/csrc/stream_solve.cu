@@ -673,11 +673,13 @@ __global__ void __launch_bounds__(256, 6) k_pcg_fused_r40(const SArgs<1> a, SSta
 // wait on the blocks whose p the next SpMV phase gathers (neighbour_wait;
 // the two exchanges inside an iteration keep every block from rewriting p
 // while another still reads it).  A block finds those blocks once, from the
-// columns of its slices.
+// columns of its slices.  Held to four blocks an SM (64 registers): 91.9 ms
+// a 128^3 solve, against 97.2 ms with the compiler's own choice at the same
+// register count, 103.2 ms at three blocks and 119.4 ms at five.
 template <typename I>
-__global__ void __launch_bounds__(256) k_pcg_fused_loop(const SArgs<1> a, SState<1> *st,
-                                                        GridSync gs, TagExchange tx,
-                                                        unsigned *ticks) {
+__global__ void __launch_bounds__(256, 4) k_pcg_fused_loop(const SArgs<1> a, SState<1> *st,
+                                                           GridSync gs, TagExchange tx,
+                                                           unsigned *ticks) {
   __shared__ int range[2];
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
