@@ -168,8 +168,11 @@ def pcg_alg_bytes(n, nnz_off, iters):
     return (iters + 2) * spmv_alg_bytes(n, nnz_off) + iters * 88 * n
 
 
-def pcg_kernel_launches(iters, fused=False):
-    # setup, start, three kernels (fused: one) per iteration, post-processing
+def pcg_kernel_launches(iters, fused=0):
+    # setup, start, three kernels per iteration (fused modes 1-3: one; mode 4:
+    # one for the whole loop), post-processing
+    if fused == 4:
+        return 4
     return (1 if fused else 3) * iters + 3
 
 
@@ -438,8 +441,9 @@ def run_ours(args):
     alg = pcg_alg_bytes(N, nnz, iters)
     achieved = alg / (ms_step * 1e-3) / 1e9
     # the timed solves' engine: the autotuner's choice, or the flags given
-    fused = bool(tune["headline_fp64"]["fused"]) if tune else bool(args.fused)
-    tr = committed_traffic("pcg_fp64_fused_iteration" if fused else "pcg_fp64_iteration")
+    fused = int(tune["headline_fp64"]["fused"]) if tune else int(args.fused)
+    tr = committed_traffic("pcg_fp64_fused_loop_iteration" if fused == 4
+                           else "pcg_fp64_fused_iteration" if fused else "pcg_fp64_iteration")
     traffic = None
     if tr is not None and tr[1] == "per_iteration_128":
         traffic = tr[0] * (N / 128 ** 3) * iters
@@ -461,17 +465,23 @@ def run_ours(args):
                                f"permuted + RCM; Jacobi-PCG FP64 to 1e-10 (M-norm)",
                    "rows": N, "nnz_offdiag": nnz, "iterations": iters,
                    "format": "SELL-32 from CSRD: FP64 values, 16-bit column offsets",
-                   "engine": ("CUDA graph, device-side WHILE loop, one cooperative kernel per "
+                   "engine": ("CUDA graph, one cooperative kernel for the whole solve "
+                              "(k_pcg_fused_loop: per iteration SpMV+dot, exchange, x/r/z "
+                              "update+dot, exchange, p update, wait on the neighbouring blocks; "
+                              "q and z kept in shared memory)" if fused == 4 else
+                              "CUDA graph, device-side WHILE loop, one cooperative kernel per "
                               "iteration (k_pcg_fused: SpMV+dot, grid barrier, x/r/z update+dot, "
                               "grid barrier, p update; q and z kept in shared memory)"
                               if fused else
                               "CUDA graph, device-side WHILE loop (3 kernels per iteration)"),
+                   "fused_mode": fused,
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
         "iterations": iters,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": ("PCG solve graph (one launch per solve: k_pcg_fused per "
+                     "kernel": ("k_pcg_fused_loop (one launch per solve)" if fused == 4 else
+                                "PCG solve graph (one launch per solve: k_pcg_fused per "
                                 "iteration)" if fused else
                                 "PCG solve graph (one launch per solve: k_pcg_a SpMV+dot, "
                                 "k_pcg_b update+dot, k_pcg_c direction per iteration)"),

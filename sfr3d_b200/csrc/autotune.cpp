@@ -96,7 +96,7 @@ bool file_lookup(const std::string &key, Tuned *t) {
                     "engine=%d threads=%d spw=%d pf=%d fused=%d ms=%lf", &e, &th, &sp, &pf, &fu,
                     &ms) == 6 &&
         (e == 1 || e == 2 || e == 4) && (th == 128 || th == 256) && sp >= 0 && sp <= 64 &&
-        pf >= 0 && pf <= 8 && fu >= 0 && fu <= 3) {
+        pf >= 0 && pf <= 8 && fu >= 0 && fu <= 4) {
       t->engine = e;
       t->threads = th;
       t->spw = sp;
