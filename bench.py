@@ -480,6 +480,8 @@ def run_ours(args):
         "iterations": iters,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "frac_on_traffic": (None if traffic is None
+                                         else traffic / (ms_step * 1e-3) / 1e9 / peak),
                      "kernel": ("k_pcg_fused_loop (one launch per solve)" if fused == 4 else
                                 "PCG solve graph (one launch per solve: k_pcg_fused per "
                                 "iteration)" if fused else
@@ -489,7 +491,11 @@ def run_ours(args):
                      "alg_bytes_per_launch": alg,
                      "alg_bytes_rule": "(iters+2)*(12 nnz_off + 4(N+1) + 24N) + iters*88N",
                      "alg_bytes_note": "32-bit column indices, as the CSRD formula counts them; "
-                                       "the SpMV phases read 16-bit offsets (2 B a slot less)"},
+                                       "the SpMV phases read 16-bit offsets (2 B a slot less), "
+                                       "and the fused iterations keep q and z on chip, so the "
+                                       "algorithmic fraction can exceed 1; frac_on_traffic is "
+                                       "the ncu DRAM bytes of the same iterations over the "
+                                       "same time"},
         "spmv": {"kernel": "spmv_kernel", "ms": spmv_ms, "alg_bytes": sb, "GB/s": spmv_gbs,
                  "frac": spmv_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
                  "traffic": None if sp_tr is None else sp_tr[0] * (N / 128 ** 3),

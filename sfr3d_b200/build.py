@@ -29,7 +29,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["krylov.cu", "mixed.cu", "stream_solve.cu", "batched.cu", "device_mem.cu", "halo.cu",
                 "noalloc.cu", "adjoint.cu", "resident.cu", "krylov_ext.cu",
-                "assembly.cu", "minres_graph.cu", "bicgl2_graph.cu", "gradient.cu"]
+                "assembly.cu", "minres_graph.cu", "bicgl2_graph.cu", "gmres_graph.cu",
+                "gradient.cu"]
 HOST_SOURCES = ["capi.cpp", "sell_build.cpp", "partition.cpp", "autotune.cpp"]
 SYSTEM_SOURCES = ["systems.cpp"]
 

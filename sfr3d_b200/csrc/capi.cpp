@@ -422,6 +422,7 @@ int sfr_gpu_destroy(sfr_system *s) {
   sfr::release_stream_engine(s);
   sfr::release_minres_graph(s);
   sfr::release_bicgstabl2_graph(s);
+  sfr::release_gmres_graph(s);
   io_release(s);
   if (!s->borrowed) {
     sfr::free_sell(&s->A);

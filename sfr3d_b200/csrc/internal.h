@@ -171,6 +171,10 @@ int solve_bicgstabl2_graph(sfr_system *s, const double *d_diag, const double *d_
                            double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
                            sfr_solve_info *info);
 void release_bicgstabl2_graph(const sfr_system *s);
+int solve_gmres_graph(sfr_system *s, const double *d_diag, const double *d_b, double *d_x,
+                      double tol, uint32_t maxit, int32_t newx, cudaStream_t st,
+                      sfr_solve_info *info);
+void release_gmres_graph(const sfr_system *s);
 
 // Graph engine (stream_solve.cu)
 int solve_stream(sfr_system *s, int32_t solver, int32_t k, const double *d_diag_k,

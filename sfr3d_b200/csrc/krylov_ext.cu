@@ -2,9 +2,9 @@
 // BiCGSTAB(2) (Bicgstab.c:1172-1460), restarted GMRES(15) (Iters.c:587-800)
 // and MINRES (Iters.c:309-558), all with the Jacobi preconditioner, FP64.
 //
-// GMRES runs as a host loop over device work (so do MINRES and BiCGSTAB(2)
-// with engine 3; otherwise each is one CUDA graph, minres_graph.cu and
-// bicgl2_graph.cu): the SpMV with the reference's row rounding
+// With engine 3 the three run as host loops over device work (otherwise
+// each is one CUDA graph: minres_graph.cu, bicgl2_graph.cu,
+// gmres_graph.cu): the SpMV with the reference's row rounding
 // (spmv_kernel), deterministic dot products (fixed block
 // partition, fixed reduction tree), and element-wise updates that round in
 // the order of the reference's expressions (no FMA contraction).  The scalar
@@ -519,13 +519,15 @@ int run_gmres(Ext &e, const double *b, double *x, double tol, uint32_t maxit, in
 int solve_ext(sfr_system *s, int32_t solver, const double *d_diag, const double *d_b, double *d_x,
               double tol, uint32_t maxit, int32_t newx, cudaStream_t st, sfr_solve_info *info) {
   if (maxit == 0) return SFR_BAD_INPUT;
-  // MINRES and BiCGSTAB(2) run as one CUDA graph with their recurrences on
-  // the device (minres_graph.cu, bicgl2_graph.cu); engine 3 keeps the host
-  // loops below, for profilers
+  // MINRES, BiCGSTAB(2) and GMRES run as one CUDA graph with their
+  // recurrences on the device (minres_graph.cu, bicgl2_graph.cu,
+  // gmres_graph.cu); engine 3 keeps the host loops below, for profilers
   if (solver == SFR_MINRES && s->engine != 3)
     return solve_minres_graph(s, d_diag, d_b, d_x, tol, maxit, newx, st, info);
   if (solver == SFR_PBICGSTABL2 && s->engine != 3)
     return solve_bicgstabl2_graph(s, d_diag, d_b, d_x, tol, maxit, newx, st, info);
+  if (solver == SFR_GMRES && s->engine != 3)
+    return solve_gmres_graph(s, d_diag, d_b, d_x, tol, maxit, newx, st, info);
   int nv = 0, extra = 0;
   switch (solver) {
     case SFR_MINRES: nv = 9; break;

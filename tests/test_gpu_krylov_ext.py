@@ -109,6 +109,31 @@ def test_warm_start_repeatability_and_caps(cuda, solver):
     g.close()
 
 
+@pytest.mark.parametrize("solver", [sv.PBICGSTABL2, sv.GMRES, sv.MINRES])
+def test_device_graph_and_host_loop_agree(cuda, solver):
+    """Each method runs as one CUDA graph with its scalar recurrence on the
+    device (the default) and as a host loop over device kernels (engine 3).
+    The two differ only in the dot products' summation order, so both stay
+    within the reference's own order spread."""
+    if solver == sv.MINRES:
+        s = S.poisson_jittered(14, seed=35)
+    else:
+        s = S.build(S.params(kind=S.SFR_SYS_CONVDIFF, n=14, lengths=(np.pi,) * 3,
+                             dirichlet=S.ALL_FACES, nrhs=1, rhs_normal=True, peclet=20.0,
+                             nu=1e-3, dt=1e-2, seed=35))
+    ref = reference(solver, O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=1e-10)
+    it_bar, x_bar = bars(solver, O.CSRD, True, s.ia, s.ja, s.al, s.ad, s.b[0], tol=1e-10)
+    for engine in (0, 3):
+        g = sv.GpuSystem(s.neq, s.ia, s.ja, sv.CSRD, True)
+        g.set_values(s.al, s.ad)
+        g.set_engine(engine)
+        x, info = g.solve(solver, s.b[0], tol=1e-10, maxit=100000)
+        g.close()
+        assert info.status == sv.OK, engine
+        assert abs(info.iters - ref.iters) <= it_bar, (engine, info.iters, ref.iters)
+        assert rel(x, ref.x) < x_bar, engine
+
+
 @pytest.mark.parametrize("solver,head", [(sv.PBICGSTABL2, "PBICGSTAB(2): tol"),
                                          (sv.GMRES, "GMRES: tol"),
                                          (sv.MINRES, "PMINRES: tol")])
