@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(256) k_pcg_c(const SArgs<K> a, SState<K> *st) 
 
 // Partial sums of a co-resident grid, reduced once and broadcast: every block
 // stores its total in part[b], then arrives at one counter; the last block
-// to arrive sums the G totals in block order and publishes the sum in one
+// to arrive sums the G totals in a fixed order and publishes the sum in one
 // word whose two lowest bits carry the epoch's tag (epoch & 3, at most 3
 // units in the last place), after resetting the counter; every other block
 // polls that word (acquire) until it carries the tag.  So the G partials are read once
@@ -460,18 +460,37 @@ __device__ __forceinline__ bool tag_exchange(const TagExchange &x, unsigned epoc
     const double bt = warp_sum(lane < nw ? sm[lane] : 0.0);
     if (lane == 0) {
       st_vec(part + blockIdx.x, bt);
-      __threadfence();
-      s_last = atomicAdd(x.count, 1u) == static_cast<unsigned>(G) - 1u;
+      // release: the partial above is visible before the arrival counts
+      s_last = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(*x.count)
+                   .fetch_add(1u, cuda::memory_order_acq_rel) == static_cast<unsigned>(G) - 1u;
     }
   }
   __syncthreads();
   bool ok = true;
   if (s_last) {
-    __threadfence();
+    // every thread of the last block loads its share of the G partials at
+    // once (one L2 round trip), then the block sums them in a fixed order:
+    // thread t's partials t, t + blockDim.x, ... in turn, the warps' shuffle
+    // trees, the warps in order
+    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+    constexpr int kAhead = 5;
+    double pv[kAhead];
+#pragma unroll
+    for (int q = 0; q < kAhead; ++q) {
+      const int b = static_cast<int>(threadIdx.x) + q * static_cast<int>(blockDim.x);
+      pv[q] = b < G ? __ldcg(part + b) : 0.0;
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < kAhead; ++q) t += pv[q];
+    for (int b = static_cast<int>(threadIdx.x) + kAhead * static_cast<int>(blockDim.x); b < G;
+         b += blockDim.x)
+      t += __ldcg(part + b);
+    t = warp_sum(t);
+    if (lane == 0) sm[warp] = t;
+    __syncthreads();
     if (warp == 0) {
-      double t = 0.0;
-      for (int b = lane; b < G; b += 32) t += ld_vec(part + b);
-      t = warp_sum(t);
+      t = warp_sum(lane < nw ? sm[lane] : 0.0);
       if (lane == 0) {
         *x.count = 0u;
         const unsigned long long u =
