@@ -64,9 +64,10 @@ def parse_args(argv=None):
                          "loop (profiling), 4 resident (mixed PCG)")
     ap.add_argument("--threads", type=int, default=0, help="graph-engine block size (0: default)")
     ap.add_argument("--spw", type=int, default=0, help="SELL slices per warp (0: default)")
-    ap.add_argument("--fused", type=int, default=0,
-                    help="graph engine FP64 PCG: one cooperative kernel an iteration "
-                         "(1, or 2 for the 40-register form)")
+    ap.add_argument("--fused", type=int, default=4,
+                    help="graph engine FP64 PCG: 0 three kernels an iteration, 1-3 one "
+                         "cooperative kernel an iteration, 4 (the library's default) the whole "
+                         "solve in one cooperative launch")
     ap.add_argument("--pf", type=int, default=0,
                     help="graph engine SpMV-phase L2 prefetch distance in rounds (0: off)")
     ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
@@ -223,8 +224,7 @@ def run_ours(args):
     g.set_engine(args.engine, args.threads, args.spw)
     if args.pf:
         g.set_prefetch(args.pf)
-    if args.fused:
-        g.set_fused(args.fused)
+    g.set_fused(args.fused)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
     b = torch.tensor(s.b[0], device="cuda")

@@ -169,8 +169,9 @@ int sfr_gpu_set_prefetch(sfr_system *s, int32_t rounds);
  * whole solve, each block waiting after its update of p only on the blocks
  * whose p its next SpMV phase gathers.  Solves it
  * does not serve (other solvers, K > 1, mixed precision, or no co-resident
- * shape) take the three-kernel iteration.  0 (the default) turns it off;
- * other values are SFR_BAD_INPUT. */
+ * shape) take the three-kernel iteration.  4 is the default; 0 turns the
+ * fused iteration off (three kernels an iteration); other values are
+ * SFR_BAD_INPUT. */
 int sfr_gpu_set_fused(sfr_system *s, int32_t mode);
 
 /* Graph engine, BiCGSTAB: 1 stages each warp's SELL slices (slot values and

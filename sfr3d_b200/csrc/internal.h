@@ -103,7 +103,7 @@ struct sfr_system {
   int32_t graph_threads = 256;   // graph engine launch shape
   int32_t graph_spw = 0;         // SELL slices per warp; 0: one wave of resident blocks
   int32_t graph_pf = 0;          // SpMV-phase L2 prefetch distance (rounds); 0: off
-  int32_t graph_fused = 0;       // FP64 PCG, one RHS: one cooperative kernel an iteration
+  int32_t graph_fused = 4;       // FP64 PCG, one RHS: the fused iteration's mode (4: one launch a solve)
   int32_t graph_stage = 0;       // BiCGSTAB SpMV phases: slices staged in shared memory
   std::vector<sfr::Tuned> tuned; // autotuned choices, used when engine == 0
   int64_t bytes = 0;

@@ -242,9 +242,10 @@ class GpuSystem:
             raise SolverError(rc, "sfr_gpu_set_prefetch")
 
     def set_fused(self, mode: int):
-        """Graph engine, FP64 PCG with one right-hand side: one cooperative
-        kernel an iteration (sfr_gpu_set_fused; 1, or 2 for the 40-register
-        form, 3 the tagged exchange, 0 off)."""
+        """Graph engine, FP64 PCG with one right-hand side
+        (sfr_gpu_set_fused): 0 three kernels an iteration, 1-3 one cooperative
+        kernel an iteration (2: held to 40 registers; 3: tagged exchanges),
+        4 (the default) the whole solve in one cooperative launch."""
         rc = lib().sfr_gpu_set_fused(self.h, int(mode))
         if rc != OK:
             raise SolverError(rc, "sfr_gpu_set_fused")

@@ -116,6 +116,53 @@ def test_fused_loop_matches_fused_iteration_bit_for_bit(cuda):
     assert bits_equal(x3, x4)
 
 
+def _with_long_range_couplings(s, c=1e-3):
+    """The CSRD system s with every row i also coupled to row i +- n/2 (value
+    -c, the diagonal raised by c, so the matrix stays symmetric positive
+    definite): the bandwidth is then about n/2."""
+    n = s.neq
+    ia, ja, al = [0], [], []
+    ad = s.ad.copy()
+    for i in range(n):
+        j = i + n // 2 if i < n // 2 else i - n // 2
+        cols = list(s.ja[s.ia[i]:s.ia[i + 1]])
+        vals = list(s.al[s.ia[i]:s.ia[i + 1]])
+        if j != i and j not in cols:
+            k = int(np.searchsorted(cols, j))
+            cols.insert(k, j)
+            vals.insert(k, -c)
+            ad[i] += c
+        ja += cols
+        al += vals
+        ia.append(len(ja))
+    return (np.array(ia, dtype=np.int32), np.array(ja, dtype=np.int32),
+            np.array(al, dtype=np.float64), ad)
+
+
+def test_fused_loop_long_range_couplings_take_the_grid_barrier(cuda):
+    """Mode 4 waits after its update of p only on the blocks its rows gather
+    from; when those span more blocks than a block has threads (here every
+    row reaches n/2 rows away, 592 blocks) it falls back to a grid barrier.
+    The bandwidth also rules out 16-bit column offsets, so this runs the
+    32-bit-column kernel.  Both at the FP64 bar against the oracle."""
+    s = S.poisson_jittered(64, seed=26)
+    ia, ja, al, ad = _with_long_range_couplings(s)
+    ref = O.pcg(O.CSRD, True, ia, ja, al, ad, s.b[0], tol=TOL)
+    out = {}
+    for mode in (3, 4):
+        g = sv.GpuSystem(s.neq, ia, ja, sv.CSRD, True)
+        g.set_values(al, ad)
+        g.set_engine(2, 256, -1)
+        g.set_fused(mode)
+        out[mode] = g.solve(sv.PCG, s.b[0], tol=TOL)
+        g.close()
+    for mode, (x, info) in out.items():
+        assert info.status == sv.OK, mode
+        assert abs(info.iters - ref.iters) <= 1, (mode, info.iters, ref.iters)
+        assert rel(x, ref.x) < 1e-12, mode
+    assert bits_equal(out[3][0], out[4][0])
+
+
 def test_autotune_mixed_k3_momentum(cuda):
     m = S.momentum(40, nrhs=3, seed=24)
     g = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True)
