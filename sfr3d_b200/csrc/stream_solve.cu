@@ -70,7 +70,7 @@ struct SArgs {  // passed by value: every pointer is fixed for the graph's life
   float *m32[K], *fr[K], *fz[K], *fq[K], *fp0[K], *fp1[K], *fxs[K], *fr0[K], *ft[K];
   double *part;
   unsigned *counter;
-  cudaGraphConditionalHandle hwhile, hif, hif2;
+  cudaGraphConditionalHandle hwhile;
   int in_graph;  // 0: plain launch loop (profiling): no conditional handles
   // the right-hand sides share one diagonal: diag64, m, dc and m32 of every
   // k point at k = 0's arrays, which k_setup fills once
@@ -389,7 +389,6 @@ __global__ void __launch_bounds__(256) k_pcg_b(const SArgs<K> a, SState<K> *st) 
     st->j = j + 1;
     st->any = any;
     st->any_upd = any_upd;
-    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif, any_upd ? 1u : 0u);
     if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
   }
 }
@@ -1114,7 +1113,6 @@ __global__ void __launch_bounds__(256) k_bicg_b1(const SArgs<K> a, SState<K> *st
     }
     st->any = any;
     st->any_upd = any_upd;
-    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif, any_upd ? 1u : 0u);
     if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
   }
 }
@@ -1352,7 +1350,6 @@ __global__ void __launch_bounds__(256) k_bicg_b2(const SArgs<K> a, SState<K> *st
     st->j = j + 1;
     st->any = any;
     st->any_upd = any_upd;
-    if (kMixed) if (a.in_graph) cudaGraphSetConditional(a.hif2, any_upd ? 1u : 0u);
     if (!any && a.in_graph) cudaGraphSetConditional(a.hwhile, 0u);
   }
 }
@@ -1420,7 +1417,7 @@ struct CachedGraph {
   double *part = nullptr;
   unsigned *counter = nullptr;
   std::vector<char> args;   // SArgs<K> (host copy, also baked into the nodes)
-  cudaGraphConditionalHandle hwhile = 0, hif = 0, hif2 = 0;
+  cudaGraphConditionalHandle hwhile = 0;
   int grid_s = 0, grid_v = 0, threads = 256;
   int grid_o = 0;        // once-a-solve and refresh kernels: one wave of their own
   int grid_f = 0;        // fused iteration: co-resident blocks
@@ -1700,14 +1697,8 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
   cudaGraph_t g = cg->graph;
   const bool mixed = precision == SFR_MIXED;
   SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hwhile, g, 1, cudaGraphCondAssignDefault));
-  // one handle per conditional node
-  if (mixed) SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hif, g, 0, cudaGraphCondAssignDefault));
-  if (mixed && solver != SFR_PCG)
-    SFR_TRY(cudaGraphConditionalHandleCreate(&cg->hif2, g, 0, cudaGraphCondAssignDefault));
   SArgs<K> &a = *reinterpret_cast<SArgs<K> *>(cg->args.data());
   a.hwhile = cg->hwhile;
-  a.hif = cg->hif;
-  a.hif2 = cg->hif2;
   a.in_graph = 1;
 
   // cudaGraphAddKernelNode copies the argument values these point to
@@ -1752,7 +1743,7 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
     SFR_TRY(cudaGraphAddMemsetNode(&mn, g, &prev, 1, &mt));
     prev = mn;
   }
-  cudaGraph_t body = nullptr, ifbody = nullptr;
+  cudaGraph_t body = nullptr;
   if (solver == SFR_PCG) {
     if (mixed) {
       SFR_TRY(add_kernel(g, &prev, (void *)k_setup<K, true>, gv, threads, p2));
@@ -1761,10 +1752,11 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
       cudaGraphNode_t bp = nullptr;
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_a<K, true, I>, gs, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_b<K, true>, gv, threads, p2));
-      SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
-      cudaGraphNode_t ip = nullptr;
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_pcg_refresh<K, I>, go, threads, p2));
+      // the reliable update as plain kernel nodes that return at once when
+      // no right-hand side is due (a conditional IF node costs more than the
+      // two empty launches)
+      SFR_TRY(add_kernel(body, &bp, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_refresh<K, I>, go, threads, p2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_pcg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
@@ -1803,17 +1795,14 @@ cudaError_t build_graph(sfr_system *s, int solver, int precision, int threads, i
       cudaGraphNode_t bp = nullptr;
       SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a1k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b1<K, true>, gv, threads, p2));
-      SFR_TRY(add_conditional(body, &bp, cg->hif, cudaGraphCondTypeIf, &ifbody));
-      cudaGraphNode_t ip = nullptr;
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody, &ip, (void *)k_bicg_refresh<K, I>, go, threads, pr1));
+      // the reliable updates as plain kernel nodes that return at once when
+      // no right-hand side is due (as in the mixed PCG body)
+      SFR_TRY(add_kernel(body, &bp, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_refresh<K, I>, go, threads, pr1));
       SFR_TRY(add_kernel(body, &bp, const_cast<void *>(a2k), gs, threads, p2, ssm));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_b2<K, true>, gv, threads, p2));
-      cudaGraph_t ifbody2 = nullptr;
-      SFR_TRY(add_conditional(body, &bp, cg->hif2, cudaGraphCondTypeIf, &ifbody2));
-      cudaGraphNode_t ip2 = nullptr;
-      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_fold<K>, gv, threads, pf_sel));
-      SFR_TRY(add_kernel(ifbody2, &ip2, (void *)k_bicg_refresh<K, I>, go, threads, pr2));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_fold<K>, gv, threads, pf_sel));
+      SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_refresh<K, I>, go, threads, pr2));
       SFR_TRY(add_kernel(body, &bp, (void *)k_bicg_c<K, true>, gv, threads, p2));
       SFR_TRY(add_kernel(g, &prev, (void *)k_fold<K>, gv, threads, pf_all));
     } else {
