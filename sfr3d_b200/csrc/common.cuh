@@ -600,6 +600,12 @@ struct RowPair {
   T a, b;
 };
 
+// Three per-row operands of a phase, loaded with the slice (slice_rows's pre)
+template <typename T>
+struct RowTriple {
+  T a, b, c;
+};
+
 template <int K, bool kExact, typename V, typename G, typename I = int>
 __device__ __forceinline__ void row_product(const int *sptr, const I *colp, const V *valp,
                                             const V *const *diagp, int s, int lane,

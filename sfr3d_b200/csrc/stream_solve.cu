@@ -862,7 +862,6 @@ template <int K, typename I>
 __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(4 * K);
   const int n = a.n;
-  const int lane = threadIdx.x & 31;
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
   int all[K];
@@ -871,21 +870,21 @@ __global__ void __launch_bounds__(256) k_post(const SArgs<K> a, SState<K> *st) {
   double acc[4 * K];
 #pragma unroll
   for (int v = 0; v < 4 * K; ++v) acc[v] = 0.0;
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    double y[K];
-    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
-                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double xk = ld_ro(a.x[k] + row_);
-      const double rk = xsub(ld_ro(a.b[k] + row_), y[k]);
-      const double dk = ld_ro(a.diag64[k] + row_);
-      acc[4 * k + 0] += xk * y[k];
-      acc[4 * k + 1] += xk * xk;
-      acc[4 * k + 2] += rk * xmul(rk, 1.0 / dk);
-      acc[4 * k + 3] += rk * rk;
-    }
-  }
+  // the row's x, b and diagonal load with the slice
+  slice_rows<K, double, true, double, double, I>(
+      n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, 0, all,
+      [&](int k, int c) { return ld_ro(a.x[k] + c); },
+      [&](int k, int row) {
+        return RowTriple<double>{ld_ro(a.x[k] + row), ld_ro(a.b[k] + row),
+                                 ld_ro(a.diag64[k] + row)};
+      },
+      [&](int k, int row, double y, RowTriple<double> e) {
+        const double rk = xsub(e.b, y);
+        acc[4 * k + 0] += e.a * y;
+        acc[4 * k + 1] += e.a * e.a;
+        acc[4 * k + 2] += rk * xmul(rk, 1.0 / e.c);
+        acc[4 * k + 3] += rk * rk;
+      });
   if (!last_block<4 * K>(acc, a.part, a.counter + 7, sm)) return;
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -916,7 +915,6 @@ template <int K, bool kMixed, typename I>
 __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> *st) {
   SFR_SHARED_RED(2 * K);
   const int n = a.n;
-  const int lane = threadIdx.x & 31;
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
   int all[K];
@@ -925,29 +923,32 @@ __global__ void __launch_bounds__(256) k_bicg_start(const SArgs<K> a, SState<K> 
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    double y[K];
-    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, all,
-                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double rk = xsub(ld_ro(a.b[k] + row_), y[k]);
-      if (kMixed) {
-        const float rs = __double2float_rn(rk);
-        st_vec(a.fr0[k] + row_, rs);
-        st_vec(a.fp0[k] + row_, rs);
-        st_vec(a.fr[k] + row_, rs);
-        st_vec(a.fz[k] + row_, ld_ro(a.m32[k] + row_) * rs);
-        st_vec(a.fxs[k] + row_, 0.0f);
-      } else {
-        st_vec(a.r0[k] + row_, rk);
-        st_vec(a.p0[k] + row_, rk);
-        st_vec(a.r[k] + row_, rk);
-        st_vec(a.z[k] + row_, xmul(rk, ld_ro(a.m[k] + row_)));
-      }
-      acc[2 * k] += rk * rk;
-    }
-  }
+  // the row's b and M (FP32 M held exactly as a double) load with the slice
+  slice_rows<K, double, true, double, double, I>(
+      n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, 0, all,
+      [&](int k, int c) { return ld_ro(a.x[k] + c); },
+      [&](int k, int row) {
+        return RowPair<double>{ld_ro(a.b[k] + row),
+                               kMixed ? static_cast<double>(ld_ro(a.m32[k] + row))
+                                      : ld_ro(a.m[k] + row)};
+      },
+      [&](int k, int row, double y, RowPair<double> e) {
+        const double rk = xsub(e.a, y);
+        if (kMixed) {
+          const float rs = __double2float_rn(rk);
+          st_vec(a.fr0[k] + row, rs);
+          st_vec(a.fp0[k] + row, rs);
+          st_vec(a.fr[k] + row, rs);
+          st_vec(a.fz[k] + row, static_cast<float>(e.b) * rs);
+          st_vec(a.fxs[k] + row, 0.0f);
+        } else {
+          st_vec(a.r0[k] + row, rk);
+          st_vec(a.p0[k] + row, rk);
+          st_vec(a.r[k] + row, rk);
+          st_vec(a.z[k] + row, xmul(rk, e.b));
+        }
+        acc[2 * k] += rk * rk;
+      });
   if (!last_block<2 * K>(acc, a.part, a.counter + 1, sm)) return;
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -1127,7 +1128,6 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
   SFR_SHARED_RED(2 * K);
   if (!st->any_upd) return;
   const int n = a.n;
-  const int lane = threadIdx.x & 31;
   int s0, s1;
   block_slices(a.nslices, &s0, &s1);
   int sel[K];
@@ -1136,22 +1136,23 @@ __global__ void __launch_bounds__(256) k_bicg_refresh(const SArgs<K> a, SState<K
   double acc[2 * K];
 #pragma unroll
   for (int v = 0; v < 2 * K; ++v) acc[v] = 0.0;
-  SFR_FOR_OWN_ROWS(s0, s1) {
-    double y[K];
-    row_product<K, true, double>(a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s_, lane, sel,
-                                 [&](int k, int c) { return ld_ro(a.x[k] + c); }, y);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (!sel[k]) continue;
-      const double rt = ld_ro(a.b[k] + row_) - y[k];
-      const float rs = __double2float_rn(rt);
-      st_vec(a.fr[k] + row_, rs);
-      st_vec(a.fz[k] + row_, ld_ro(a.m32[k] + row_) * rs);
-      st_vec(a.fxs[k] + row_, 0.0f);
-      acc[2 * k] += rt * rt;
-      acc[2 * k + 1] += static_cast<double>(rs) * static_cast<double>(ld_ro(a.fr0[k] + row_));
-    }
-  }
+  // the row's b, r0 and M (FP32 held exactly as doubles) load with the slice
+  slice_rows<K, double, true, double, double, I>(
+      n, a.sptr, cols_of<I>(a.cols), a.val64, a.diag64, s0, s1, 0, sel,
+      [&](int k, int c) { return ld_ro(a.x[k] + c); },
+      [&](int k, int row) {
+        return RowTriple<double>{ld_ro(a.b[k] + row), static_cast<double>(ld_ro(a.fr0[k] + row)),
+                                 static_cast<double>(ld_ro(a.m32[k] + row))};
+      },
+      [&](int k, int row, double y, RowTriple<double> e) {
+        const double rt = e.a - y;
+        const float rs = __double2float_rn(rt);
+        st_vec(a.fr[k] + row, rs);
+        st_vec(a.fz[k] + row, static_cast<float>(e.c) * rs);
+        st_vec(a.fxs[k] + row, 0.0f);
+        acc[2 * k] += rt * rt;
+        acc[2 * k + 1] += static_cast<double>(rs) * e.b;
+      });
   if (!last_block<2 * K>(acc, a.part, a.counter + 4, sm)) return;
   if (threadIdx.x == 0) {
     const unsigned j = st->j;
