@@ -71,6 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--pf", type=int, default=0,
                     help="graph engine SpMV-phase L2 prefetch distance in rounds (0: off)")
     ap.add_argument("--mixed", action="store_true", help="--profile solve: mixed precision")
+    ap.add_argument("--nrhs", type=int, default=1,
+                    help="--profile bicgstab: right-hand sides sharing the momentum matrix")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (untimed) before the timed solves")
     ap.add_argument("--partitioned", action="store_true",
@@ -266,16 +268,17 @@ def run_ours(args):
                     H.solve(hg, hs, sv.PCG, b_r, tol=1e-10, maxit=args.maxit)
                 hg.close()
             elif args.profile == "bicgstab":
-                m = S.momentum(n, nrhs=1, seed=3)
+                m = S.momentum(n, nrhs=args.nrhs, seed=3)
                 gm = sv.GpuSystem(m.neq, m.ia, m.ja, sv.CSRD, True, device=local)
                 gm.set_values(m.al, m.ad)
                 gm.set_engine(args.engine, args.threads, args.spw)
-                bm = torch.tensor(m.b[0], device="cuda")
+                gm.set_prefetch(args.pf)
+                bm = torch.tensor(m.b.reshape(-1), device="cuda")
                 xm = torch.zeros_like(bm)
                 for _ in range(args.warmup + args.steps):
-                    gm.solve_device(sv.PBICGSTAB, bm.data_ptr(), xm.data_ptr(), tol=1e-10,
-                                    maxit=args.maxit, stream=sptr,
-                                    precision=sv.MIXED if args.mixed else sv.FP64)
+                    gm.solve_multi_device(sv.PBICGSTAB, args.nrhs, bm.data_ptr(), xm.data_ptr(),
+                                          tol=1e-10, maxit=args.maxit, stream=sptr,
+                                          precision=sv.MIXED if args.mixed else sv.FP64)
             else:
                 for _ in range(args.warmup + args.steps):
                     g.solve_device(sv.PCG, b.data_ptr(), x.data_ptr(), tol=1e-10,
