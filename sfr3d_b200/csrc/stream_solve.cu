@@ -16,8 +16,8 @@
 // launch latency dominates; this engine suits large ones.  Both follow the
 // same arithmetic: FP64 rows and updates bit-identical to the reference
 // (Cg.c, Bicgstab.c, HccaBlas.c), or FP32 inner iterations with FP64
-// reliable updates (the true residual and x in FP64; the update kernels sit in
-// a conditional IF node that runs only when a refinement is due).
+// reliable updates (the true residual and x in FP64; the update kernels are
+// plain graph nodes that return at once unless a refinement is due).
 #include <cuda_runtime.h>
 
 #include <algorithm>
