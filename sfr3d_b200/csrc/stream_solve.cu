@@ -1348,6 +1348,15 @@ __global__ void __launch_bounds__(256) k_bicg_b2(const SArgs<K> a, SState<K> *st
       }
       any |= st->active[k];
     }
+    // The refresh reads the FP64 matrix once for all right-hand sides, so
+    // when one is due every other active one is refreshed in the same pass
+    // (a reliable update is valid at any iteration).  Their later triggers
+    // then tend to coincide, and fewer refresh passes are run in all.
+    if (kMixed && K > 1 && any_upd) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (st->active[k]) st->upd[k] = 1;
+    }
     st->j = j + 1;
     st->any = any;
     st->any_upd = any_upd;
